@@ -1,0 +1,139 @@
+/*
+ * pastix_b200.h -- C ABI of the B200 numerical factorization and solve backend
+ * for PaStiX.
+ *
+ * PaStiX keeps its host analysis (ordering, symbolic factorization, blend); its
+ * numerical factorization, triangular solves and iterative refinement run on one
+ * B200 through these entry points.  Only plain C types cross this boundary: the
+ * SolverMatrix integer tables are passed as int64 arrays, values and vectors as
+ * host (or, for the *_device variants, device) pointers.
+ *
+ * Return values are PaStiX error codes (include/pastix/api.h:321-334):
+ * 0 = PASTIX_SUCCESS, 2 = PASTIX_ERR_ALLOC, 3 = PASTIX_ERR_NOTIMPLEMENTED,
+ * 4 = PASTIX_ERR_OUTOFMEMORY, 6 = PASTIX_ERR_INTERNAL, 7 = PASTIX_ERR_BADPARAMETER.
+ *
+ * Threading: one solver instance is not re-entrant (as a pastix_data_t);
+ * separate instances may be used from separate host threads.
+ */
+#ifndef PASTIX_B200_H
+#define PASTIX_B200_H
+
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+/* Factorization kinds, numbered as PaStiX's pastix_factotype_t
+ * (include/pastix/api.h:272-285). */
+enum { B200_FACTO_POTRF = 0, B200_FACTO_SYTRF = 1, B200_FACTO_GETRF = 2 };
+
+/* Arithmetic of the factor.
+ *  FP64   : factor in double, FP64 updates (the drop-in path).
+ *  FP32   : factor in float, FP32 CUDA-core updates.
+ *  TF32   : factor in float, wide updates on tcgen05 tensor cores in TF32
+ *           with FP32 accumulation.
+ *  TF32X3 : as TF32 with split (big + small) operands, three TF32 products per
+ *           update, for close-to-FP32 accuracy.
+ * The solve and refinement vectors are always double. */
+enum { B200_PREC_FP64 = 0, B200_PREC_FP32 = 1, B200_PREC_TF32 = 2, B200_PREC_TF32X3 = 3 };
+
+/* Refinement methods, numbered as PaStiX's pastix_refine_t
+ * (include/pastix/api.h, IPARM_REFINEMENT): GMRES, CG, simple refinement. */
+enum { B200_REFINE_GMRES = 0, B200_REFINE_CG = 1, B200_REFINE_SR = 2 };
+
+/* The SolverMatrix integer structure (blend/solver.h:83-213), 0-based.
+ * cblk arrays hold cblknbr+1 entries (the last is PaStiX's sentinel cblk, whose
+ * fblok is bloknbr and brownum is brownbr); blok arrays hold bloknbr+1 entries
+ * (SolverBlok fields); cblk_fblok[k] = cblktab[k].fblokptr - bloktab.
+ * peritab is ordemesh->peritab (new -> original index). */
+typedef struct b200_symbol_s {
+    int64_t n, cblknbr, bloknbr, brownbr;
+    const int64_t *cblk_fcolnum, *cblk_lcolnum, *cblk_fblok, *cblk_stride;
+    const int64_t *cblk_lcolidx, *cblk_brownum;
+    const int64_t *blok_frownum, *blok_lrownum, *blok_lcblknm, *blok_fcblknm;
+    const int64_t *browtab;
+    const int64_t *peritab;
+} b200_symbol_t;
+
+typedef struct b200_solver_s b200_solver_t;
+
+/* Upload the structure and build the device-side schedules.  Replaces the
+ * structure walk PaStiX does in coeftabInit / solverBackupInit
+ * (sopalin/coeftab.c:70-140, blend/solver_backup.c:60-100) and selects the
+ * kernels that the per-(facto, precision) table sopalinFacto
+ * (sopalin/pastix_task_sopalin.c:41-48) would have picked.  stream may be NULL
+ * (the library then creates its own CUDA stream). */
+int b200_solver_create( const b200_symbol_t *symbol, int facto, int precision, void *stream,
+                        b200_solver_t **solver );
+int b200_solver_destroy( b200_solver_t *solver );
+
+/* Load the permuted blocked CSC (bcsc/bcsc.h:28-53; pastix_subtask_spm2bcsc,
+ * sopalin/pastix_task_sopalin.c:82).  colptr has n+1 entries in the permuted
+ * column numbering; Lvalues holds A (both triangles for a symmetric matrix),
+ * Uvalues holds A^T (LU only, else NULL); anorm is ||A||_F (DPARM_A_NORM).
+ * Host pointers.  The first call fixes the pattern; later calls with the same
+ * colptr/rowtab only replace the values (same-pattern refactorization). */
+int b200_bcsc_load( b200_solver_t *solver, int64_t nnz, const int64_t *colptr,
+                    const int64_t *rowtab, const double *Lvalues, const double *Uvalues,
+                    double anorm );
+
+/* Numerical factorization: bcsc -> coeftab scatter (cpucblk_zfillin,
+ * kernels/cpucblk_zinit.c:229) and the supernodal factorization
+ * (sopalin/sequential_z{potrf,sytrf,getrf}.c).  epsilon_magn_ctrl has the
+ * meaning of DPARM_EPSILON_MAGN_CTRL (sopalin/pastix_task_sopalin.c:401-425):
+ * < 0: |value| is the threshold, 0: sqrt(eps)*||A||_F, > 0: value*||A||_F.
+ * nbpivots (may be NULL) receives the static-pivot count (IPARM_STATIC_PIVOTING).
+ * Returns 6 (PASTIX_ERR_INTERNAL) on a negative pivot in a Cholesky. */
+int b200_numfact( b200_solver_t *solver, double epsilon_magn_ctrl, int64_t *nbpivots );
+
+/* pastix_task_solve (sopalin/pastix_task_solve.c:550): b (n x nrhs, column
+ * major, leading dimension ldb, original ordering, host memory) is overwritten
+ * with x. */
+int b200_solve( b200_solver_t *solver, int64_t nrhs, double *b, int64_t ldb );
+
+/* Same on device memory, asynchronously on the solver's stream (or on stream if
+ * not NULL). */
+int b200_solve_device( b200_solver_t *solver, int64_t nrhs, double *d_b, int64_t ldb, void *stream );
+
+/* pastix_task_refine (refinement/pastix_task_refine.c:226): iterative
+ * refinement in double of x (initial guess, overwritten) for A x = b, with the
+ * factor as preconditioner.  method: B200_REFINE_*; eps: stopping tolerance on
+ * ||b - A x||_2 / ||b||_2 per right-hand side (DPARM_EPSILON_REFINEMENT);
+ * itermax: IPARM_ITERMAX; gmres_im: IPARM_GMRES_IM.  Host pointers.
+ * niter (may be NULL) receives the largest iteration count over the
+ * right-hand sides, berr (may be NULL, nrhs entries) the final backward errors. */
+int b200_refine( b200_solver_t *solver, int64_t nrhs, const double *b, int64_t ldb, double *x,
+                 int64_t ldx, int method, double eps, int64_t itermax, int64_t gmres_im,
+                 int64_t *niter, double *berr );
+
+/* Same on device memory (b and x on the device). */
+int b200_refine_device( b200_solver_t *solver, int64_t nrhs, const double *d_b, int64_t ldb,
+                        double *d_x, int64_t ldx, int method, double eps, int64_t itermax,
+                        int64_t gmres_im, int64_t *niter, double *berr, void *stream );
+
+/* y = alpha A x + beta y with the loaded matrix, in the original ordering, host
+ * pointers (spmMatVec; used for backward errors).  nrhs columns. */
+int b200_spmv( b200_solver_t *solver, int64_t nrhs, double alpha, const double *x, int64_t ldx,
+               double beta, double *y, int64_t ldy );
+
+/* Copy the factor back in PaStiX's coeftab layout: every cblk's 2D block layout
+ * (blend/solver_matrix_gen_utils.h:137-165), cblks concatenated in order, as
+ * double.  U (LU only, else NULL) receives the transposed U factor.  Each array
+ * holds coefnbr entries. */
+int b200_factor_download( b200_solver_t *solver, double *L, double *U );
+
+/* Statistics of the last calls: out[0] numfact ms, out[1] solve ms, out[2]
+ * refine ms, out[3] static pivots, out[4] diag threshold used, out[5] device
+ * bytes held, out[6] number of etree levels, out[7] kernel launches of the last
+ * numfact, out[8] kernel launches of the last solve, out[9] coefnbr. */
+int b200_stats( b200_solver_t *solver, double *out );
+
+/* Short description of a return code. */
+const char *b200_strerror( int code );
+
+#ifdef __cplusplus
+}
+#endif
+
+#endif /* PASTIX_B200_H */

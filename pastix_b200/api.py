@@ -1,0 +1,114 @@
+"""Host mirror of PaStiX's task API for the B200 backend.
+
+The call sequence and parameters follow PaStiX (include/pastix.h:84-95,
+example/simple.c): ``pastix_task_analyze`` runs PaStiX's own analysis (ordering
+with ``pastixOrderGrid``, symbolic factorization, blend); ``pastix_task_numfact``
+builds the bcsc and factors on the GPU; ``pastix_task_solve`` and
+``pastix_task_refine`` solve and refine on the GPU.  iparm/dparm keep PaStiX's
+names and meanings (include/pastix/api.h), plus ``precision`` for the factor
+arithmetic of the B200 backend.
+"""
+from __future__ import annotations
+
+import numpy as np
+
+from . import native
+from .refhost import Analysis
+
+DEFAULT_IPARM = {
+    "FACTORIZATION": "potrf",   # IPARM_FACTORIZATION: potrf / sytrf / getrf
+    "REFINEMENT": "gmres",      # IPARM_REFINEMENT: gmres / cg / sr
+    "ITERMAX": 250,             # IPARM_ITERMAX
+    "GMRES_IM": 25,             # IPARM_GMRES_IM
+    "MIN_BLOCKSIZE": 160,       # IPARM_MIN_BLOCKSIZE
+    "MAX_BLOCKSIZE": 320,       # IPARM_MAX_BLOCKSIZE
+    "PRECISION": "fp64",        # B200 backend: fp64 / fp32 / tf32 / tf32x3
+}
+DEFAULT_DPARM = {
+    "EPSILON_REFINEMENT": 1e-12,  # DPARM_EPSILON_REFINEMENT (double)
+    "EPSILON_MAGN_CTRL": 0.0,     # DPARM_EPSILON_MAGN_CTRL
+}
+
+
+class PastixB200:
+    """One solver instance (the counterpart of a pastix_data_t)."""
+
+    def __init__(self, iparm: dict | None = None, dparm: dict | None = None, stream=None):
+        self.iparm = dict(DEFAULT_IPARM, **(iparm or {}))
+        self.dparm = dict(DEFAULT_DPARM, **(dparm or {}))
+        self.stream = stream
+        self.analysis = None
+        self.structure = None
+        self.solver = None
+        self.out = {}
+
+    # pastix_task_analyze (blend/pastix_task_analyze.c:52)
+    def task_analyze(self, A):
+        ip = {"MIN_BLOCKSIZE": self.iparm["MIN_BLOCKSIZE"], "MAX_BLOCKSIZE": self.iparm["MAX_BLOCKSIZE"]}
+        self.analysis = Analysis(A, self.iparm["FACTORIZATION"], iparm=ip)
+        self.structure = self.analysis.structure()
+        self.out["FACT_THFLOPS"] = self.structure.thflops
+        if self.solver is not None:
+            self.solver.close()
+        self.solver = native.Solver(self.structure, self.iparm["FACTORIZATION"], self.iparm["PRECISION"],
+                                    self.stream)
+        return self
+
+    # pastix_subtask_spm2bcsc (sopalin/pastix_task_sopalin.c:82)
+    def subtask_spm2bcsc(self, values=None):
+        bc = self.analysis.bcsc(values)
+        self.out["A_NORM"] = bc.anorm
+        self.solver.bcsc_load(bc)
+        return bc
+
+    # pastix_task_numfact (sopalin/pastix_task_sopalin.c:563)
+    def task_numfact(self, values=None):
+        self.subtask_spm2bcsc(values)
+        piv = self.solver.numfact(self.dparm["EPSILON_MAGN_CTRL"])
+        st = self.solver.stats()
+        self.out["STATIC_PIVOTING"] = piv
+        self.out["FACT_TIME"] = st["numfact_ms"] / 1e3
+        self.out["FACT_FLOPS"] = self.structure.thflops / max(self.out["FACT_TIME"], 1e-30)
+        return piv
+
+    # pastix_task_solve (sopalin/pastix_task_solve.c:550): b is overwritten with x
+    def task_solve(self, b):
+        x = self.solver.solve(b)
+        self.out["SOLV_TIME"] = self.solver.stats()["solve_ms"] / 1e3
+        return x
+
+    # pastix_task_refine (refinement/pastix_task_refine.c:226)
+    def task_refine(self, b, x):
+        x, nit, berr = self.solver.refine(b, x, self.iparm["REFINEMENT"], self.dparm["EPSILON_REFINEMENT"],
+                                          self.iparm["ITERMAX"], self.iparm["GMRES_IM"])
+        self.out["NBITER"] = nit
+        self.out["RELATIVE_ERROR"] = float(np.max(berr)) if berr.size else 0.0
+        self.out["REFINE_TIME"] = self.solver.stats()["refine_ms"] / 1e3
+        return x
+
+    def close(self):
+        if self.solver is not None:
+            self.solver.close()
+            self.solver = None
+
+
+def backward_error(A, x, b) -> np.ndarray:
+    """||b - A x||_2 / ||b||_2 per column (the refinement metric,
+    refinement/z_refine_gmres.c:148-155), in float64 on the host."""
+    r = b - A.matvec(x)
+    r = r.reshape(A.n, -1)
+    b2 = b.reshape(A.n, -1)
+    return np.linalg.norm(r, axis=0) / np.linalg.norm(b2, axis=0)
+
+
+def normwise_backward_error(A, x, b) -> np.ndarray:
+    """||b - A x||_1 / (||A||_1 ||x||_1) per column (spmCheckAxb, spm/src/z_spm_genrhs.c:384-423)."""
+    r = (b - A.matvec(x)).reshape(A.n, -1)
+    x2 = x.reshape(A.n, -1)
+    return np.abs(r).sum(axis=0) / (A.norm_one() * np.abs(x2).sum(axis=0))
+
+
+def forward_error(x, xtrue) -> np.ndarray:
+    x2 = x.reshape(xtrue.shape[0], -1)
+    t2 = xtrue.reshape(xtrue.shape[0], -1)
+    return np.abs(x2 - t2).max(axis=0) / np.abs(t2).max(axis=0)

@@ -1,0 +1,78 @@
+// Internal types of the B200 supernodal factorization/solve library.
+//
+// Device layout of the factor ("panel layout"): every cblk k owns one
+// column-major panel of stride_k rows and ncols_k columns, leading dimension
+// ld_k = stride_k rounded up to a multiple of 4, starting on a 256-byte
+// boundary.  Its blocks are stacked in the panel in PaStiX's block order
+// (diagonal block first), block b starting at panel row rowoff[b].  This is
+// PaStiX's 1D cblk layout (the !CBLK_LAYOUT_2D case of kernels/cpucblk_zinit.c
+// and kernels/core_zgemmsp.c:1D1D) with a padded leading dimension; the
+// integer structure is PaStiX's SolverMatrix unchanged, and
+// b200_factor_download() converts back to PaStiX's 2D block layout.
+// For LU the transposed U factor has its own arena with the same offsets.
+#pragma once
+
+#include <cstdint>
+#include <cuda_runtime.h>
+#include <vector>
+
+namespace b200 {
+
+constexpr int FACTO_POTRF = 0, FACTO_SYTRF = 1, FACTO_GETRF = 2;
+
+// Structure tables on the device (all 0-based).
+struct DevSym {
+    int n, cblknbr, bloknbr;
+    const int *fcol;      // [cblknbr+1] first column of each cblk
+    const int *ncols;     // [cblknbr]
+    const int *stride;    // [cblknbr]
+    const int *ld;        // [cblknbr] padded leading dimension
+    const int64_t *off;   // [cblknbr] panel offset in elements
+    const int *fblok;     // [cblknbr+1]
+    const int *frow;      // [bloknbr]
+    const int *lrow;      // [bloknbr]
+    const int *rowoff;    // [bloknbr] first panel row of the block inside its cblk
+    const int *fcblk;     // [bloknbr] facing cblk
+};
+
+// One update of the right-looking supernodal factorization: the contribution of
+// cblk k's block j (and the blocks below it) to the facing cblk f
+// (core_zgemmsp_2d2d, kernels/core_zgemmsp.c:396-465, as one GEMM over the
+// stacked rows):  C_f[rows of blocks i >= j (+shift), cols of block j] -=
+// A_k[rows i] * B_k[rows j]^T, K = ncols_k.
+enum : int {
+    UPD_ATOMIC = 1,   // another cblk of the same level updates f: accumulate with atomics
+    UPD_SYM = 2,      // only the lower triangle of the diagonal square is needed
+    UPD_A_U = 4,      // A operand from the U panel (LU, upper side)
+    UPD_B_U = 8,      // B operand from the U panel (LU, lower side)
+    UPD_C_U = 16,     // C is the U panel of f
+    UPD_SCALE_D = 32  // multiply A by D (LDL^T: C -= (L_i D) L_j^T)
+};
+
+struct Upd {
+    int k, j, f;
+    int rowA0;    // panel row of k where the M-range starts
+    int rowB0;    // panel row of k of block j
+    int M, N, K;
+    int colbase;  // column in f of block j's first row
+    int tiles_m, tiles_n;
+    int tile0;    // first tile index of this update inside its launch
+    int flags;
+};
+
+// Off-diagonal row tile of a cblk panel (TRSM and solve tasks).
+struct RowTask {
+    int k;
+    int row0;  // first panel row of the tile (>= ncols_k)
+};
+
+struct Level {
+    int c0, c1;          // cblks (indices into lvl_cblk)
+    int t0, t1;          // row tasks of the off-diagonal panels
+    int u0, u1;          // updates
+    int ntiles;          // GEMM tiles of the level
+    int nmax;            // widest cblk of the level
+    int64_t flops;
+};
+
+}  // namespace b200

@@ -1,0 +1,659 @@
+// Numerical factorization kernels (sm_100a).
+//
+//  scatter_kernel      bcsc -> panel arena (cpucblk_zfillin_fr, kernels/cpucblk_zinit.c:229-309)
+//  diag_factor_kernel  per-cblk diagonal-block POTRF / GETRF / SYTRF with static pivoting
+//                      (core_z{potrf,getrf,sytrf}sp, kernels/core_z*trfsp.c)
+//  panel_trsm_kernel   off-diagonal panel solve (core_ztrsmsp_2d, kernels/core_ztrsmsp.c:147-181)
+//  update_f64_kernel   GEMM + scatter-add into the facing cblk on FP64 tensor cores (DMMA)
+//                      (core_zgemmsp_2d2d, kernels/core_zgemmsp.c:396-465)
+//  update_simt_kernel  the same update for FP32 factors on CUDA cores
+#include "b200_internal.h"
+#include "kernels.h"
+
+#include <algorithm>
+
+namespace b200 {
+
+// ------------------------------------------------------------------ helpers
+
+__device__ __forceinline__ unsigned smem_u32(const void *p) {
+    return static_cast<unsigned>(__cvta_generic_to_shared(p));
+}
+
+// 8-byte asynchronous global->shared copy; src_bytes = 0 fills zeros.
+__device__ __forceinline__ void cp_async8(void *dst, const void *src, bool ok) {
+    asm volatile("cp.async.ca.shared.global [%0], [%1], 8, %2;\n" ::"r"(smem_u32(dst)), "l"(src),
+                 "r"(ok ? 8 : 0));
+}
+__device__ __forceinline__ void cp_async4(void *dst, const void *src, bool ok) {
+    asm volatile("cp.async.ca.shared.global [%0], [%1], 4, %2;\n" ::"r"(smem_u32(dst)), "l"(src),
+                 "r"(ok ? 4 : 0));
+}
+__device__ __forceinline__ void cp_async_commit() { asm volatile("cp.async.commit_group;\n" ::); }
+template <int N>
+__device__ __forceinline__ void cp_async_wait() { asm volatile("cp.async.wait_group %0;\n" ::"n"(N)); }
+
+// Panel row -> destination panel row in the facing cblk f.
+// Block i of k holds panel rows [rowoff[i], rowoff[i]+rows); its global rows
+// start at frow[i].  In f the global row lies in the block fb with
+// frow[fb] <= grow <= lrow[fb]  (is_block_inside_fblock, blend/solver.h:358).
+__device__ __forceinline__ int dest_row(const DevSym &s, int k, int f, int prow) {
+    int lo = s.fblok[k], hi = s.fblok[k + 1] - 1;
+    while (lo < hi) {
+        int mid = (lo + hi + 1) >> 1;
+        if (s.rowoff[mid] <= prow) lo = mid; else hi = mid - 1;
+    }
+    const int grow = s.frow[lo] + (prow - s.rowoff[lo]);
+    int flo = s.fblok[f], fhi = s.fblok[f + 1] - 1;
+    while (flo < fhi) {
+        int mid = (flo + fhi + 1) >> 1;
+        if (s.frow[mid] <= grow) flo = mid; else fhi = mid - 1;
+    }
+    if (grow > s.lrow[flo]) return -1;  // not in the structure of f (cannot happen for a valid symbol)
+    return s.rowoff[flo] + (grow - s.frow[flo]);
+}
+
+// ------------------------------------------------------------------ scatter
+
+template <typename T>
+__global__ void scatter_kernel(int64_t nnz, const int64_t *__restrict__ dest, const double *__restrict__ Lv,
+                               const double *__restrict__ Uv, T *__restrict__ L, T *__restrict__ U) {
+    const int64_t e = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
+    if (e >= nnz) return;
+    int64_t d = dest[e];
+    if (d < 0) return;
+    const bool strict = (d >> 62) & 1;
+    d &= ((int64_t)1 << 62) - 1;
+    L[d] = (T)Lv[e];
+    if (U != nullptr && strict) U[d] = (T)Uv[e];
+}
+
+// ------------------------------------------------------------------ diagonal blocks
+
+constexpr int TP = 33;  // padded leading dimension of 32x32 shared tiles
+
+// Unblocked factorization of a pb x pb tile by one warp (lane = row).
+// POTRF: core_zpotf2sp (kernels/core_zpotrfsp.c:66-100)
+// GETRF: core_zgetf2sp (kernels/core_zgetrfsp.c:64-110)
+// SYTRF: core_zsytf2sp (kernels/core_zsytrfsp.c:63-103)
+template <typename T, int FACTO>
+__device__ void factor_tile(T *t, int pb, int lane, double thr, int *piv, int *err) {
+    for (int c = 0; c < pb; c++) {
+        if (lane == 0) {
+            T d = t[c * (TP + 1)];
+            if (fabs((double)d) < thr) {
+                if (FACTO == FACTO_POTRF) d = (T)thr;
+                else d = (d < (T)0) ? (T)(-thr) : (T)thr;
+                (*piv)++;
+            }
+            if (FACTO == FACTO_POTRF) {
+                if (d < (T)0) { *err = 1; d = -d; }
+                d = sqrt(d);
+            }
+            t[c * (TP + 1)] = d;
+        }
+        __syncwarp();
+        const T d = t[c * (TP + 1)];
+        const T inv = (T)1 / d;
+        if (lane > c && lane < pb) {
+            const T v = t[lane + c * TP];
+            if (FACTO == FACTO_SYTRF) t[c + lane * TP] = v;  // D L^T copy in the upper part
+            t[lane + c * TP] = v * inv;
+        }
+        __syncwarp();
+        if (lane > c && lane < pb) {
+            const T lic = t[lane + c * TP];
+            if (FACTO == FACTO_GETRF) {
+                for (int j = c + 1; j < pb; j++) t[lane + j * TP] -= lic * t[c + j * TP];
+            } else if (FACTO == FACTO_POTRF) {
+                for (int j = c + 1; j <= lane; j++) t[lane + j * TP] -= lic * t[j + c * TP];
+            } else {
+                const T a = -d * lic;
+                for (int j = c + 1; j <= lane; j++) t[lane + j * TP] += a * t[j + c * TP];
+            }
+        }
+        __syncwarp();
+    }
+}
+
+// One CTA (256 threads) factors the diagonal block of one cblk, blocked by 32
+// columns: tile factorization, solve of the rows (and for LU columns) below
+// the tile inside the diagonal block, trailing update.  For LU the diagonal
+// block of the U arena is first added transposed into L (core_zgeadd) and
+// afterwards receives the transposed factor (core_zgetmo).
+template <typename T, int FACTO>
+__global__ void __launch_bounds__(256) diag_factor_kernel(DevSym s, const int *__restrict__ cblks, T *L,
+                                                          T *U, const double *__restrict__ thr_ptr,
+                                                          unsigned long long *npiv, int *err) {
+    __shared__ T tile[32 * TP];
+    __shared__ T xs[64 * TP];
+    __shared__ T ys[64 * TP];
+    __shared__ int s_piv, s_err;
+    const int k = cblks[blockIdx.x];
+    const int n = s.ncols[k], ld = s.ld[k];
+    const double thr = *thr_ptr;
+    T *A = L + s.off[k];
+    const int tid = threadIdx.x, nth = blockDim.x, lane = tid & 31, warp = tid >> 5;
+    if (tid == 0) { s_piv = 0; s_err = 0; }
+    if (FACTO == FACTO_GETRF) {
+        const T *Au = U + s.off[k];
+        for (int idx = tid; idx < n * n; idx += nth) {
+            const int i = idx % n, j = idx / n;
+            A[i + (size_t)j * ld] += Au[j + (size_t)i * ld];
+        }
+    }
+    __syncthreads();
+    for (int p = 0; p < n; p += 32) {
+        const int pb = min(32, n - p);
+        T *Ap = A + p + (size_t)p * ld;
+        for (int idx = tid; idx < 32 * 32; idx += nth) {
+            const int i = idx & 31, j = idx >> 5;
+            tile[i + j * TP] = (i < pb && j < pb) ? Ap[i + (size_t)j * ld] : (T)0;
+        }
+        __syncthreads();
+        if (warp == 0) factor_tile<T, FACTO>(tile, pb, lane, thr, &s_piv, &s_err);
+        __syncthreads();
+        for (int idx = tid; idx < 32 * 32; idx += nth) {
+            const int i = idx & 31, j = idx >> 5;
+            if (i < pb && j < pb && (FACTO != FACTO_POTRF || i >= j)) Ap[i + (size_t)j * ld] = tile[i + j * TP];
+        }
+        const int rest = n - p - pb;
+        if (rest > 0) {
+            // rows below the tile: X op(T) = A
+            for (int r = tid; r < rest; r += nth) {
+                T *row = A + (p + pb + r) + (size_t)p * ld;
+                T x[32];
+#pragma unroll
+                for (int c = 0; c < 32; c++) x[c] = (c < pb) ? row[(size_t)c * ld] : (T)0;
+#pragma unroll
+                for (int c = 0; c < 32; c++) {
+                    if (c < pb) {
+                        T v = x[c];
+                        for (int l = 0; l < c; l++) {
+                            const T tv = (FACTO == FACTO_GETRF) ? tile[l + c * TP] : tile[c + l * TP];
+                            v -= x[l] * tv;
+                        }
+                        if (FACTO != FACTO_SYTRF) v = v / tile[c * (TP + 1)];
+                        x[c] = v;
+                    }
+                }
+#pragma unroll
+                for (int c = 0; c < 32; c++) {
+                    if (c < pb) {
+                        if (FACTO == FACTO_SYTRF) {
+                            A[(p + c) + (size_t)(p + pb + r) * ld] = x[c];          // (L D)^T in the upper part
+                            row[(size_t)c * ld] = x[c] * ((T)1 / tile[c * (TP + 1)]);  // L
+                        } else {
+                            row[(size_t)c * ld] = x[c];
+                        }
+                    }
+                }
+            }
+            if (FACTO == FACTO_GETRF) {
+                // columns right of the tile: Y = L_tile^{-1} A (unit lower)
+                for (int cc = tid; cc < rest; cc += nth) {
+                    T *col = A + p + (size_t)(p + pb + cc) * ld;
+                    T y[32];
+#pragma unroll
+                    for (int l = 0; l < 32; l++) y[l] = (l < pb) ? col[l] : (T)0;
+#pragma unroll
+                    for (int l = 0; l < 32; l++) {
+                        if (l < pb) {
+                            T v = y[l];
+                            for (int m = 0; m < l; m++) v -= tile[l + m * TP] * y[m];
+                            y[l] = v;
+                        }
+                    }
+#pragma unroll
+                    for (int l = 0; l < 32; l++)
+                        if (l < pb) col[l] = y[l];
+                }
+            }
+            __syncthreads();
+            // trailing update of the diagonal block: A22 -= X * B^T
+            const int nt = (rest + 63) / 64;
+            for (int ti = 0; ti < nt; ti++) {
+                for (int tj = 0; tj < nt; tj++) {
+                    if (FACTO != FACTO_GETRF && tj > ti) continue;
+                    const int i0 = p + pb + ti * 64, j0 = p + pb + tj * 64;
+                    for (int idx = tid; idx < 64 * 32; idx += nth) {
+                        const int r = idx & 63, c = idx >> 6;
+                        T xv = 0, yv = 0;
+                        if (c < pb && i0 + r < n) xv = A[(i0 + r) + (size_t)(p + c) * ld];
+                        if (c < pb && j0 + r < n) {
+                            if (FACTO == FACTO_POTRF) yv = A[(j0 + r) + (size_t)(p + c) * ld];
+                            else yv = A[(p + c) + (size_t)(j0 + r) * ld];  // (L D)^T row (SYTRF) / U row (GETRF)
+                        }
+                        xs[r * TP + c] = xv;
+                        ys[r * TP + c] = yv;
+                    }
+                    __syncthreads();
+                    const int tr = tid & 15, tc = tid >> 4;
+                    T acc[4][4];
+#pragma unroll
+                    for (int a = 0; a < 4; a++)
+#pragma unroll
+                        for (int b = 0; b < 4; b++) acc[a][b] = 0;
+                    for (int c = 0; c < pb; c++) {
+                        T xv[4], yv[4];
+#pragma unroll
+                        for (int a = 0; a < 4; a++) xv[a] = xs[(tr + 16 * a) * TP + c];
+#pragma unroll
+                        for (int b = 0; b < 4; b++) yv[b] = ys[(tc + 16 * b) * TP + c];
+#pragma unroll
+                        for (int a = 0; a < 4; a++)
+#pragma unroll
+                            for (int b = 0; b < 4; b++) acc[a][b] += xv[a] * yv[b];
+                    }
+#pragma unroll
+                    for (int a = 0; a < 4; a++) {
+#pragma unroll
+                        for (int b = 0; b < 4; b++) {
+                            const int i = i0 + tr + 16 * a, j = j0 + tc + 16 * b;
+                            if (i < n && j < n && (FACTO == FACTO_GETRF || i >= j)) A[i + (size_t)j * ld] -= acc[a][b];
+                        }
+                    }
+                    __syncthreads();
+                }
+            }
+        }
+        __syncthreads();
+    }
+    if (FACTO == FACTO_GETRF) {
+        T *Au = U + s.off[k];
+        for (int idx = tid; idx < n * n; idx += nth) {
+            const int i = idx % n, j = idx / n;
+            Au[j + (size_t)i * ld] = A[i + (size_t)j * ld];
+        }
+    }
+    if (tid == 0) {
+        if (s_piv) atomicAdd(npiv, (unsigned long long)s_piv);
+        if (s_err) atomicExch(err, 1);
+    }
+}
+
+// ------------------------------------------------------------------ panel TRSM
+
+// X op(T) = B for a tile of TR off-diagonal rows of cblk k, the whole tile held
+// in shared memory.  op(T) is upper triangular:
+//   mode 0: op(T)[l][c] = D[l + c*ld]  (upper part of the diagonal block)
+//   mode 1: op(T)[l][c] = D[c + l*ld]  (lower part, transposed)
+template <typename T>
+__global__ void __launch_bounds__(256) panel_trsm_kernel(DevSym s, const RowTask *__restrict__ tasks, int TR,
+                                                         T *P, const T *Dsrc, int mode, int unit) {
+    extern __shared__ __align__(16) unsigned char smraw[];
+    T *xs = reinterpret_cast<T *>(smraw);  // TR x n, column-major
+    __shared__ T ts[64 * TP];
+    __shared__ T tt[32 * TP];
+    const RowTask t = tasks[blockIdx.x];
+    const int k = t.k, n = s.ncols[k], ld = s.ld[k];
+    const int rows = min(TR, s.stride[k] - t.row0);
+    T *X = P + s.off[k] + t.row0;
+    const T *D = Dsrc + s.off[k];
+    const int tid = threadIdx.x, nth = blockDim.x;
+    for (int idx = tid; idx < TR * n; idx += nth) {
+        const int r = idx % TR, c = idx / TR;
+        xs[idx] = (r < rows) ? X[r + (size_t)c * ld] : (T)0;
+    }
+    __syncthreads();
+    const int NG = nth / TR;      // column groups
+    const int CPG = 32 / NG;      // columns per group (<= 8)
+    const int r = tid % TR, cg = tid / TR;
+    for (int cb = 0; cb < n; cb += 32) {
+        const int w = min(32, n - cb);
+        T acc[8];
+#pragma unroll
+        for (int q = 0; q < 8; q++) acc[q] = 0;
+        for (int l0 = 0; l0 < cb; l0 += 64) {
+            const int lw = min(64, cb - l0);
+            for (int idx = tid; idx < 64 * 32; idx += nth) {
+                const int l = idx >> 5, c = idx & 31;
+                T v = 0;
+                if (l < lw && c < w) v = mode == 0 ? D[(l0 + l) + (size_t)(cb + c) * ld] : D[(cb + c) + (size_t)(l0 + l) * ld];
+                ts[l * TP + c] = v;
+            }
+            __syncthreads();
+            for (int l = 0; l < lw; l++) {
+                const T xv = xs[r + (l0 + l) * TR];
+#pragma unroll
+                for (int q = 0; q < 8; q++)
+                    if (q < CPG) acc[q] += xv * ts[l * TP + cg * CPG + q];
+            }
+            __syncthreads();
+        }
+#pragma unroll
+        for (int q = 0; q < 8; q++) {
+            const int c = cg * CPG + q;
+            if (q < CPG && c < w) xs[r + (cb + c) * TR] -= acc[q];
+        }
+        for (int idx = tid; idx < 32 * 32; idx += nth) {
+            const int l = idx >> 5, c = idx & 31;
+            T v = 0;
+            if (l < w && c < w) v = mode == 0 ? D[(cb + l) + (size_t)(cb + c) * ld] : D[(cb + c) + (size_t)(cb + l) * ld];
+            tt[l * TP + c] = v;
+        }
+        __syncthreads();
+        if (tid < TR) {
+            T x[32];
+#pragma unroll
+            for (int c = 0; c < 32; c++) x[c] = (c < w) ? xs[tid + (cb + c) * TR] : (T)0;
+#pragma unroll
+            for (int c = 0; c < 32; c++) {
+                if (c < w) {
+                    T v = x[c];
+                    for (int l = 0; l < c; l++) v -= x[l] * tt[l * TP + c];
+                    if (!unit) v = v / tt[c * (TP + 1)];
+                    x[c] = v;
+                }
+            }
+#pragma unroll
+            for (int c = 0; c < 32; c++)
+                if (c < w) xs[tid + (cb + c) * TR] = x[c];
+        }
+        __syncthreads();
+    }
+    for (int idx = tid; idx < TR * n; idx += nth) {
+        const int rr = idx % TR, c = idx / TR;
+        if (rr < rows) X[rr + (size_t)c * ld] = xs[idx];
+    }
+}
+
+// ------------------------------------------------------------------ updates
+
+__device__ __forceinline__ int find_update(const Upd *__restrict__ upds, int nupd, int tile) {
+    int lo = 0, hi = nupd - 1;
+    while (lo < hi) {
+        const int mid = (lo + hi + 1) >> 1;
+        if (upds[mid].tile0 <= tile) lo = mid; else hi = mid - 1;
+    }
+    return lo;
+}
+
+__device__ __forceinline__ void tile_coords(const Upd &u, int lt, int &mt, int &nt) {
+    if (u.flags & UPD_SYM) {
+        nt = 0;
+        while (lt >= u.tiles_m - nt) { lt -= u.tiles_m - nt; nt++; }
+        mt = nt + lt;
+    } else {
+        mt = lt % u.tiles_m;
+        nt = lt / u.tiles_m;
+    }
+}
+
+__device__ __forceinline__ void dmma_16x8x4(double (&c)[4], const double (&a)[2], double b) {
+    asm volatile(
+        "mma.sync.aligned.m16n8k4.row.col.f64.f64.f64.f64 {%0,%1,%2,%3}, {%4,%5}, {%6}, {%0,%1,%2,%3};\n"
+        : "+d"(c[0]), "+d"(c[1]), "+d"(c[2]), "+d"(c[3])
+        : "d"(a[0]), "d"(a[1]), "d"(b));
+}
+
+constexpr int UT_M = 64, UT_N = 64, UT_K = 16, UT_STAGES = 3, UT_LDS = UT_M + 4;
+constexpr int UPD_F64_SMEM = 2 * UT_STAGES * UT_K * UT_LDS * sizeof(double);
+
+// 64x64 output tile per CTA, 4 warps (2x2) of 32x32, DMMA m16n8k4, 3-stage
+// cp.async pipeline over K in chunks of 16 columns.
+__global__ void __launch_bounds__(128) update_f64_kernel(DevSym s, const Upd *__restrict__ upds, int nupd,
+                                                         double *L, double *U) {
+    extern __shared__ __align__(16) unsigned char upd_smem[];
+    double(*As)[UT_K][UT_LDS] = reinterpret_cast<double(*)[UT_K][UT_LDS]>(upd_smem);
+    double(*Bs)[UT_K][UT_LDS] = reinterpret_cast<double(*)[UT_K][UT_LDS]>(upd_smem + sizeof(double) * UT_STAGES * UT_K * UT_LDS);
+    __shared__ double Ds[UT_STAGES][UT_K];
+    __shared__ int drow[UT_M];
+    const int tile = blockIdx.x;
+    const Upd u = upds[find_update(upds, nupd, tile)];
+    int mt, nt;
+    tile_coords(u, tile - u.tile0, mt, nt);
+    const int m0 = mt * UT_M, n0 = nt * UT_N;
+    const int k = u.k, ldk = s.ld[k];
+    const double *Ap = ((u.flags & UPD_A_U) ? U : L) + s.off[k] + u.rowA0 + m0;
+    const double *Bp = ((u.flags & UPD_B_U) ? U : L) + s.off[k] + u.rowB0 + n0;
+    const double *Dp = L + s.off[k];
+    const bool scale = (u.flags & UPD_SCALE_D) != 0;
+    const int mrem = u.M - m0, nrem = u.N - n0;
+    const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
+    const int wm = warp & 1, wn = warp >> 1;
+    const int g = lane >> 2, tg = lane & 3;
+
+    auto load_stage = [&](int st, int kc) {
+#pragma unroll
+        for (int i = 0; i < 8; i++) {
+            const int idx = tid + i * 128;
+            const int r = idx & 63, c = idx >> 6;
+            const int kk = kc + c;
+            const bool okA = (r < mrem) && (kk < u.K);
+            const bool okB = (r < nrem) && (kk < u.K);
+            cp_async8(&As[st][c][r], okA ? Ap + r + (size_t)kk * ldk : Ap, okA);
+            cp_async8(&Bs[st][c][r], okB ? Bp + r + (size_t)kk * ldk : Bp, okB);
+        }
+        if (scale && tid < UT_K) {
+            const int kk = kc + tid;
+            Ds[st][tid] = (kk < u.K) ? Dp[(size_t)kk * (ldk + 1)] : 0.0;
+        }
+    };
+
+    double acc[2][4][4];
+#pragma unroll
+    for (int a = 0; a < 2; a++)
+#pragma unroll
+        for (int b = 0; b < 4; b++)
+#pragma unroll
+            for (int e = 0; e < 4; e++) acc[a][b][e] = 0.0;
+
+    const int nk = (u.K + UT_K - 1) / UT_K;
+#pragma unroll
+    for (int st = 0; st < UT_STAGES - 1; st++) {
+        if (st < nk) load_stage(st, st * UT_K);
+        cp_async_commit();
+    }
+    for (int kt = 0; kt < nk; kt++) {
+        cp_async_wait<UT_STAGES - 2>();
+        __syncthreads();
+        const int st = kt % UT_STAGES;
+        const int nxt = kt + UT_STAGES - 1;
+        if (nxt < nk) load_stage(nxt % UT_STAGES, nxt * UT_K);
+        cp_async_commit();
+#pragma unroll
+        for (int k4 = 0; k4 < UT_K; k4 += 4) {
+            double a[2][2], b[4];
+            const double dsc = scale ? Ds[st][k4 + tg] : 1.0;
+#pragma unroll
+            for (int mi = 0; mi < 2; mi++) {
+                const int row = wm * 32 + mi * 16 + g;
+                a[mi][0] = As[st][k4 + tg][row] * dsc;
+                a[mi][1] = As[st][k4 + tg][row + 8] * dsc;
+            }
+#pragma unroll
+            for (int ni = 0; ni < 4; ni++) b[ni] = Bs[st][k4 + tg][wn * 32 + ni * 8 + g];
+#pragma unroll
+            for (int mi = 0; mi < 2; mi++)
+#pragma unroll
+                for (int ni = 0; ni < 4; ni++) dmma_16x8x4(acc[mi][ni], a[mi], b[ni]);
+        }
+    }
+    cp_async_wait<0>();
+    if (tid < UT_M) drow[tid] = (m0 + tid < u.M) ? dest_row(s, k, u.f, u.rowA0 + m0 + tid) : -1;
+    __syncthreads();
+    double *C = ((u.flags & UPD_C_U) ? U : L) + s.off[u.f];
+    const int ldf = s.ld[u.f];
+    const bool atomic = (u.flags & UPD_ATOMIC) != 0;
+    const bool sym = (u.flags & UPD_SYM) != 0;
+#pragma unroll
+    for (int mi = 0; mi < 2; mi++) {
+#pragma unroll
+        for (int ni = 0; ni < 4; ni++) {
+#pragma unroll
+            for (int e = 0; e < 4; e++) {
+                const int row = wm * 32 + mi * 16 + g + (e >> 1) * 8;
+                const int col = wn * 32 + ni * 8 + 2 * tg + (e & 1);
+                if (n0 + col >= u.N) continue;
+                if (sym && m0 + row < n0 + col) continue;
+                const int d = drow[row];
+                if (d < 0) continue;
+                double *p = C + d + (size_t)(u.colbase + n0 + col) * ldf;
+                if (atomic) atomicAdd(p, -acc[mi][ni][e]);
+                else *p -= acc[mi][ni][e];
+            }
+        }
+    }
+}
+
+// FP32 factor update on CUDA cores: 64x64 tile, 256 threads (4x4 each), K chunks of 16.
+__global__ void __launch_bounds__(256) update_simt_f32_kernel(DevSym s, const Upd *__restrict__ upds, int nupd,
+                                                              float *L, float *U) {
+    __shared__ __align__(16) float As[2][UT_K][UT_M + 4];
+    __shared__ __align__(16) float Bs[2][UT_K][UT_N + 4];
+    __shared__ int drow[UT_M];
+    const int tile = blockIdx.x;
+    const Upd u = upds[find_update(upds, nupd, tile)];
+    int mt, nt;
+    tile_coords(u, tile - u.tile0, mt, nt);
+    const int m0 = mt * UT_M, n0 = nt * UT_N;
+    const int k = u.k, ldk = s.ld[k];
+    const float *Ap = ((u.flags & UPD_A_U) ? U : L) + s.off[k] + u.rowA0 + m0;
+    const float *Bp = ((u.flags & UPD_B_U) ? U : L) + s.off[k] + u.rowB0 + n0;
+    const float *Dp = L + s.off[k];
+    const bool scale = (u.flags & UPD_SCALE_D) != 0;
+    const int mrem = u.M - m0, nrem = u.N - n0;
+    const int tid = threadIdx.x;
+    const int tr = tid & 15, tc = tid >> 4;
+    float acc[4][4] = {};
+    const int nk = (u.K + UT_K - 1) / UT_K;
+    auto load_stage = [&](int st, int kc) {
+#pragma unroll
+        for (int i = 0; i < 4; i++) {
+            const int idx = tid + i * 256;
+            const int r = idx & 63, c = idx >> 6;
+            const int kk = kc + c;
+            const bool okA = (r < mrem) && (kk < u.K);
+            const bool okB = (r < nrem) && (kk < u.K);
+            cp_async4(&As[st][c][r], okA ? Ap + r + (size_t)kk * ldk : Ap, okA);
+            cp_async4(&Bs[st][c][r], okB ? Bp + r + (size_t)kk * ldk : Bp, okB);
+        }
+    };
+    load_stage(0, 0);
+    cp_async_commit();
+    for (int kt = 0; kt < nk; kt++) {
+        const int st = kt & 1;
+        if (kt + 1 < nk) load_stage(st ^ 1, (kt + 1) * UT_K);
+        cp_async_commit();
+        cp_async_wait<1>();
+        __syncthreads();
+#pragma unroll
+        for (int c = 0; c < UT_K; c++) {
+            const int kk = kt * UT_K + c;
+            const float dsc = (scale && kk < u.K) ? Dp[(size_t)kk * (ldk + 1)] : 1.0f;
+            float av[4], bv[4];
+#pragma unroll
+            for (int a = 0; a < 4; a++) av[a] = As[st][c][tr + 16 * a] * dsc;
+#pragma unroll
+            for (int b = 0; b < 4; b++) bv[b] = Bs[st][c][tc + 16 * b];
+#pragma unroll
+            for (int a = 0; a < 4; a++)
+#pragma unroll
+                for (int b = 0; b < 4; b++) acc[a][b] = fmaf(av[a], bv[b], acc[a][b]);
+        }
+        __syncthreads();
+    }
+    if (tid < UT_M) drow[tid] = (m0 + tid < u.M) ? dest_row(s, k, u.f, u.rowA0 + m0 + tid) : -1;
+    __syncthreads();
+    float *C = ((u.flags & UPD_C_U) ? U : L) + s.off[u.f];
+    const int ldf = s.ld[u.f];
+    const bool atomic = (u.flags & UPD_ATOMIC) != 0;
+    const bool sym = (u.flags & UPD_SYM) != 0;
+#pragma unroll
+    for (int a = 0; a < 4; a++) {
+#pragma unroll
+        for (int b = 0; b < 4; b++) {
+            const int row = tr + 16 * a, col = tc + 16 * b;
+            if (n0 + col >= u.N) continue;
+            if (sym && m0 + row < n0 + col) continue;
+            const int d = drow[row];
+            if (d < 0) continue;
+            float *p = C + d + (size_t)(u.colbase + n0 + col) * ldf;
+            if (atomic) atomicAdd(p, -acc[a][b]);
+            else *p -= acc[a][b];
+        }
+    }
+}
+
+// ------------------------------------------------------------------ launchers
+
+template <typename T>
+void launch_scatter(int64_t nnz, const int64_t *dest, const double *Lv, const double *Uv, T *L, T *U,
+                    cudaStream_t st) {
+    if (nnz <= 0) return;
+    const int bs = 256;
+    scatter_kernel<T><<<(unsigned)((nnz + bs - 1) / bs), bs, 0, st>>>(nnz, dest, Lv, Uv, L, U);
+}
+
+template <typename T>
+void launch_diag(int facto, const DevSym &s, const int *cblks, int ncblk, T *L, T *U, const double *thr,
+                 unsigned long long *npiv, int *err, cudaStream_t st) {
+    if (ncblk <= 0) return;
+    if (facto == FACTO_POTRF)
+        diag_factor_kernel<T, FACTO_POTRF><<<ncblk, 256, 0, st>>>(s, cblks, L, U, thr, npiv, err);
+    else if (facto == FACTO_GETRF)
+        diag_factor_kernel<T, FACTO_GETRF><<<ncblk, 256, 0, st>>>(s, cblks, L, U, thr, npiv, err);
+    else
+        diag_factor_kernel<T, FACTO_SYTRF><<<ncblk, 256, 0, st>>>(s, cblks, L, U, thr, npiv, err);
+}
+
+template <typename T>
+void launch_trsm(const DevSym &s, const RowTask *tasks, int ntasks, int TR, int nmax, T *P, const T *D, int mode,
+                 int unit, cudaStream_t st) {
+    if (ntasks <= 0) return;
+    const size_t smem = (size_t)TR * nmax * sizeof(T);
+    panel_trsm_kernel<T><<<ntasks, 256, smem, st>>>(s, tasks, TR, P, D, mode, unit);
+}
+
+void launch_update_f64(const DevSym &s, const Upd *upds, int nupd, int ntiles, double *L, double *U,
+                       cudaStream_t st) {
+    if (ntiles <= 0) return;
+    update_f64_kernel<<<ntiles, 128, UPD_F64_SMEM, st>>>(s, upds, nupd, L, U);
+}
+
+void launch_update_f32(const DevSym &s, const Upd *upds, int nupd, int ntiles, float *L, float *U,
+                       cudaStream_t st) {
+    if (ntiles <= 0) return;
+    update_simt_f32_kernel<<<ntiles, 256, 0, st>>>(s, upds, nupd, L, U);
+}
+
+// Raise the dynamic shared-memory limit of a kernel to what the device allows
+// beyond its static shared memory; returns that limit (bytes) or -1.
+template <typename K>
+static int raise_smem(K kernel) {
+    int dev = 0, optin = 0;
+    cudaGetDevice(&dev);
+    cudaDeviceGetAttribute(&optin, cudaDevAttrMaxSharedMemoryPerBlockOptin, dev);
+    cudaFuncAttributes fa;
+    if (cudaFuncGetAttributes(&fa, kernel) != cudaSuccess) return -1;
+    const int dyn = optin - (int)fa.sharedSizeBytes;
+    if (cudaFuncSetAttribute(kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, dyn) != cudaSuccess) return -1;
+    return dyn;
+}
+
+int configure_factor_kernels() {
+    int lim = 1 << 30;
+    int v;
+    if ((v = raise_smem(update_f64_kernel)) < UPD_F64_SMEM) return -1;
+    if ((v = raise_smem(panel_trsm_kernel<double>)) < 0) return -1;
+    lim = std::min(lim, v);
+    if ((v = raise_smem(panel_trsm_kernel<float>)) < 0) return -1;
+    lim = std::min(lim, v);
+    return lim;
+}
+
+template void launch_scatter<double>(int64_t, const int64_t *, const double *, const double *, double *, double *,
+                                     cudaStream_t);
+template void launch_scatter<float>(int64_t, const int64_t *, const double *, const double *, float *, float *,
+                                    cudaStream_t);
+template void launch_diag<double>(int, const DevSym &, const int *, int, double *, double *, const double *,
+                                  unsigned long long *, int *, cudaStream_t);
+template void launch_diag<float>(int, const DevSym &, const int *, int, float *, float *, const double *,
+                                 unsigned long long *, int *, cudaStream_t);
+template void launch_trsm<double>(const DevSym &, const RowTask *, int, int, int, double *, const double *, int, int,
+                                  cudaStream_t);
+template void launch_trsm<float>(const DevSym &, const RowTask *, int, int, int, float *, const float *, int, int,
+                                 cudaStream_t);
+
+}  // namespace b200

@@ -1,0 +1,138 @@
+// FP64 vector kernels of the iterative refinement (sm_100a): bcsc SpMV and the
+// BLAS-1 operations the refinement drivers need, all on n x nrhs column-major
+// blocks with one scalar per column (bcsc/bcsc_zspmv.c, bcsc/bvec_zcompute.c).
+#include "b200_internal.h"
+#include "kernels.h"
+
+namespace b200 {
+
+// y = alpha * A x + beta * y.  The matrix is the bcsc in the permuted basis, read
+// row-wise: for a symmetric matrix the bcsc columns hold both triangles so column
+// i is row i; for a general matrix the values passed are A^T in the same pattern
+// (Uvalues), whose column i is row i of A (bcsc/bcsc_zspmv.c:127-240).
+// One warp per row.
+__global__ void __launch_bounds__(256) spmv_kernel(int n, int nrhs, const int64_t *__restrict__ colptr,
+                                                   const int *__restrict__ rowtab, const double *__restrict__ vals,
+                                                   const double *__restrict__ x, int64_t ldx, double *y, int64_t ldy,
+                                                   double alpha, double beta) {
+    const int warp = (blockIdx.x * blockDim.x + threadIdx.x) >> 5;
+    const int lane = threadIdx.x & 31;
+    if (warp >= n) return;
+    const int64_t e0 = colptr[warp], e1 = colptr[warp + 1];
+    for (int r = 0; r < nrhs; r++) {
+        double acc = 0.0;
+        for (int64_t e = e0 + lane; e < e1; e += 32) acc += vals[e] * x[rowtab[e] + r * ldx];
+#pragma unroll
+        for (int o = 16; o > 0; o >>= 1) acc += __shfl_xor_sync(0xffffffffu, acc, o);
+        if (lane == 0) {
+            double *yp = y + warp + r * ldy;
+            *yp = (beta == 0.0) ? alpha * acc : alpha * acc + beta * *yp;
+        }
+    }
+}
+
+// Column dot products, one CTA per (column, chunk), atomically accumulated.
+__global__ void dots_kernel(int n, const double *__restrict__ x, int64_t ldx, const double *__restrict__ y,
+                            int64_t ldy, double *out) {
+    const int r = blockIdx.y;
+    __shared__ double red[32];
+    double acc = 0.0;
+    for (int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; i < n; i += (int64_t)gridDim.x * blockDim.x)
+        acc += x[i + r * ldx] * y[i + r * ldy];
+#pragma unroll
+    for (int o = 16; o > 0; o >>= 1) acc += __shfl_xor_sync(0xffffffffu, acc, o);
+    if ((threadIdx.x & 31) == 0) red[threadIdx.x >> 5] = acc;
+    __syncthreads();
+    if (threadIdx.x < 32) {
+        acc = (threadIdx.x < (blockDim.x >> 5)) ? red[threadIdx.x] : 0.0;
+#pragma unroll
+        for (int o = 16; o > 0; o >>= 1) acc += __shfl_xor_sync(0xffffffffu, acc, o);
+        if (threadIdx.x == 0) atomicAdd(out + r, acc);
+    }
+}
+
+__global__ void axpys_kernel(int n, int nrhs, const double *__restrict__ a, double sign,
+                             const double *__restrict__ x, int64_t ldx, double *y, int64_t ldy) {
+    const int64_t idx = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
+    if (idx >= (int64_t)n * nrhs) return;
+    const int i = (int)(idx % n), r = (int)(idx / n);
+    y[i + r * ldy] += sign * a[r] * x[i + r * ldx];
+}
+
+__global__ void xpbys_kernel(int n, int nrhs, const double *__restrict__ x, int64_t ldx, const double *__restrict__ b,
+                             double *y, int64_t ldy) {
+    const int64_t idx = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
+    if (idx >= (int64_t)n * nrhs) return;
+    const int i = (int)(idx % n), r = (int)(idx / n);
+    y[i + r * ldy] = x[i + r * ldx] + b[r] * y[i + r * ldy];
+}
+
+__global__ void axpby_kernel(int n, int nrhs, double alpha, const double *__restrict__ x, int64_t ldx, double beta,
+                             double *y, int64_t ldy) {
+    const int64_t idx = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
+    if (idx >= (int64_t)n * nrhs) return;
+    const int i = (int)(idx % n), r = (int)(idx / n);
+    const double yv = (beta == 0.0) ? 0.0 : beta * y[i + r * ldy];
+    y[i + r * ldy] = alpha * x[i + r * ldx] + yv;
+}
+
+__global__ void scal_cols_kernel(int n, int nrhs, const double *__restrict__ s, const double *__restrict__ x,
+                                 int64_t ldx, double *y, int64_t ldy) {
+    const int64_t idx = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
+    if (idx >= (int64_t)n * nrhs) return;
+    const int i = (int)(idx % n), r = (int)(idx / n);
+    y[i + r * ldy] = s[r] * x[i + r * ldx];
+}
+
+static inline unsigned nblk(int64_t tot, int bs) { return (unsigned)((tot + bs - 1) / bs); }
+
+void launch_spmv(int n, int nrhs, const int64_t *colptr, const int *rowtab, const double *vals, const double *x,
+                 int64_t ldx, double *y, int64_t ldy, double alpha, double beta, cudaStream_t st) {
+    if (n <= 0) return;
+    spmv_kernel<<<nblk((int64_t)n * 32, 256), 256, 0, st>>>(n, nrhs, colptr, rowtab, vals, x, ldx, y, ldy, alpha,
+                                                             beta);
+}
+
+void launch_dots(int n, int nrhs, const double *x, int64_t ldx, const double *y, int64_t ldy, double *out,
+                 cudaStream_t st) {
+    if (nrhs <= 0) return;
+    cudaMemsetAsync(out, 0, nrhs * sizeof(double), st);
+    const int bs = 256;
+    int gx = (int)std::min<int64_t>(296, ((int64_t)n + bs - 1) / bs);
+    if (gx < 1) gx = 1;
+    dots_kernel<<<dim3(gx, nrhs), bs, 0, st>>>(n, x, ldx, y, ldy, out);
+}
+
+void launch_axpys(int n, int nrhs, const double *a, double sign, const double *x, int64_t ldx, double *y,
+                  int64_t ldy, cudaStream_t st) {
+    const int64_t tot = (int64_t)n * nrhs;
+    if (tot <= 0) return;
+    axpys_kernel<<<nblk(tot, 256), 256, 0, st>>>(n, nrhs, a, sign, x, ldx, y, ldy);
+}
+
+void launch_xpbys(int n, int nrhs, const double *x, int64_t ldx, const double *b, double *y, int64_t ldy,
+                  cudaStream_t st) {
+    const int64_t tot = (int64_t)n * nrhs;
+    if (tot <= 0) return;
+    xpbys_kernel<<<nblk(tot, 256), 256, 0, st>>>(n, nrhs, x, ldx, b, y, ldy);
+}
+
+void launch_copy(int n, int nrhs, const double *x, int64_t ldx, double *y, int64_t ldy, cudaStream_t st) {
+    launch_axpby(n, nrhs, 1.0, x, ldx, 0.0, y, ldy, st);
+}
+
+void launch_axpby(int n, int nrhs, double alpha, const double *x, int64_t ldx, double beta, double *y, int64_t ldy,
+                  cudaStream_t st) {
+    const int64_t tot = (int64_t)n * nrhs;
+    if (tot <= 0) return;
+    axpby_kernel<<<nblk(tot, 256), 256, 0, st>>>(n, nrhs, alpha, x, ldx, beta, y, ldy);
+}
+
+void launch_scal_cols(int n, int nrhs, const double *s, const double *x, int64_t ldx, double *y, int64_t ldy,
+                      cudaStream_t st) {
+    const int64_t tot = (int64_t)n * nrhs;
+    if (tot <= 0) return;
+    scal_cols_kernel<<<nblk(tot, 256), 256, 0, st>>>(n, nrhs, s, x, ldx, y, ldy);
+}
+
+}  // namespace b200

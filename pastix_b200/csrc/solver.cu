@@ -1,0 +1,1021 @@
+// Host side of the B200 supernodal factorization/solve library: structure upload,
+// level schedules, kernel sequencing (captured into CUDA graphs), the refinement
+// drivers and the C ABI declared in include/pastix_b200.h.
+#include <algorithm>
+#include <chrono>
+#include <cmath>
+#include <cstdio>
+#include <cstring>
+#include <map>
+#include <vector>
+
+#include "b200_internal.h"
+#include "kernels.h"
+#include "pastix_b200.h"
+
+using namespace b200;
+
+namespace {
+
+constexpr int ERR_SUCCESS = 0, ERR_ALLOC = 2, ERR_NOTIMPL = 3, ERR_OOM = 4, ERR_INTERNAL = 6, ERR_BADPARAM = 7;
+
+#define CU(call)                                                                                      \
+    do {                                                                                              \
+        cudaError_t e_ = (call);                                                                      \
+        if (e_ != cudaSuccess) {                                                                      \
+            fprintf(stderr, "pastix_b200: %s failed: %s (%s:%d)\n", #call, cudaGetErrorString(e_),    \
+                    __FILE__, __LINE__);                                                              \
+            return e_ == cudaErrorMemoryAllocation ? ERR_OOM : ERR_INTERNAL;                          \
+        }                                                                                             \
+    } while (0)
+
+#define RET(call)                          \
+    do {                                   \
+        int r_ = (call);                   \
+        if (r_ != ERR_SUCCESS) return r_;  \
+    } while (0)
+
+template <typename T>
+int dalloc(T **p, size_t count) {
+    *p = nullptr;
+    if (count == 0) count = 1;
+    cudaError_t e = cudaMalloc((void **)p, count * sizeof(T));
+    if (e != cudaSuccess) {
+        fprintf(stderr, "pastix_b200: cudaMalloc(%zu bytes) failed: %s\n", count * sizeof(T), cudaGetErrorString(e));
+        return ERR_OOM;
+    }
+    return ERR_SUCCESS;
+}
+
+template <typename T>
+int upload(T **p, const std::vector<T> &h, cudaStream_t st) {
+    RET(dalloc(p, h.size()));
+    if (!h.empty()) CU(cudaMemcpyAsync(*p, h.data(), h.size() * sizeof(T), cudaMemcpyHostToDevice, st));
+    return ERR_SUCCESS;
+}
+
+}  // namespace
+
+struct b200_solver_s {
+    int facto = 0, prec = 0;
+    bool f32 = false;
+    size_t esz = 8;
+    cudaStream_t st = nullptr;
+    bool own_stream = false;
+    int n = 0, cblknbr = 0, bloknbr = 0;
+    int64_t coefnbr = 0;  // PaStiX's coefficient count (sum of stride * ncols)
+    int64_t arena = 0;    // elements of one factor arena (padded layout)
+
+    // host copy of the structure
+    std::vector<int> fcol, ncols, stride, ld, fblok, frow, lrow, rowoff, fcblk, peri;
+    std::vector<int64_t> off;
+
+    // device structure
+    DevSym ds{};
+    std::vector<void *> dev_allocs;
+    void *dL = nullptr, *dU = nullptr;
+    int *d_peri = nullptr;
+    int *d_lvl_cblk = nullptr;
+    RowTask *d_trsm = nullptr, *d_stask = nullptr;
+    Upd *d_upd = nullptr;
+    std::vector<Level> levels;
+    std::vector<int> lvl_tr;            // TRSM rows per task of each level
+    std::vector<int> lvl_s0, lvl_s1;    // solve row tasks of each level
+    int nmax_all = 0;
+    int64_t total_tiles = 0;
+    int trsm_smem = 0;                  // dynamic shared memory available to the panel TRSM
+
+    // bcsc
+    int64_t nnz = -1;
+    int64_t *d_colptr = nullptr;
+    int *d_rowtab = nullptr;
+    double *d_Lv = nullptr, *d_Uv = nullptr;
+    int64_t *d_dest = nullptr;
+    std::vector<int64_t> h_colptr, h_rowtab;
+    double anorm = 0.0;
+
+    // numfact
+    double *d_thr = nullptr;
+    unsigned long long *d_npiv = nullptr;
+    int *d_err = nullptr;
+    cudaGraphExec_t fact_graph = nullptr;
+    bool factored = false;
+    double thr_used = 0.0;
+    int64_t last_npiv = 0;
+
+    // solve / refine workspaces
+    double *d_ws = nullptr;
+    size_t ws_cap = 0;
+    std::map<int, cudaGraphExec_t> solve_graphs;  // keyed by nrhs, on the ws buffer
+    double *d_scal = nullptr;                     // per-column scalars
+    int scal_cap = 0;
+
+    double t_fact = 0, t_solve = 0, t_refine = 0;
+    int launches_fact = 0, launches_solve = 0;
+    cudaEvent_t ev0 = nullptr, ev1 = nullptr;
+
+    template <typename T>
+    int dmalloc(T **p, size_t count) {
+        RET(dalloc(p, count));
+        dev_allocs.push_back((void *)*p);
+        return ERR_SUCCESS;
+    }
+    template <typename T>
+    int dupload(T **p, const std::vector<T> &h) {
+        RET(upload(p, h, st));
+        dev_allocs.push_back((void *)*p);
+        return ERR_SUCCESS;
+    }
+};
+
+namespace {
+
+int build_schedule(b200_solver_t *s) {
+    const int N = s->cblknbr;
+    // level = 1 + max level of the cblks that update it; facing cblks have larger indices
+    std::vector<int> level(N, 0);
+    for (int k = 0; k < N; k++)
+        for (int b = s->fblok[k] + 1; b < s->fblok[k + 1]; b++) {
+            const int f = s->fcblk[b];
+            if (f <= k || f >= N) return ERR_BADPARAM;
+            level[f] = std::max(level[f], level[k] + 1);
+        }
+    const int nlev = N ? *std::max_element(level.begin(), level.end()) + 1 : 0;
+    std::vector<int> cnt(nlev + 1, 0);
+    for (int k = 0; k < N; k++) cnt[level[k] + 1]++;
+    for (int l = 0; l < nlev; l++) cnt[l + 1] += cnt[l];
+    std::vector<int> lvl_cblk(N);
+    {
+        std::vector<int> pos(cnt.begin(), cnt.end() - 1);
+        for (int k = 0; k < N; k++) lvl_cblk[pos[level[k]]++] = k;
+    }
+    std::vector<RowTask> trsm, stask;
+    std::vector<Upd> upds;
+    s->levels.assign(nlev, Level{});
+    s->lvl_tr.assign(nlev, 64);
+    s->lvl_s0.assign(nlev, 0);
+    s->lvl_s1.assign(nlev, 0);
+    std::vector<int> src_count(N, 0), src_last(N, -1);
+    const size_t trsm_smem = (size_t)s->trsm_smem;
+    for (int l = 0; l < nlev; l++) {
+        Level &L = s->levels[l];
+        L.c0 = cnt[l];
+        L.c1 = cnt[l + 1];
+        L.nmax = 0;
+        for (int i = L.c0; i < L.c1; i++) L.nmax = std::max(L.nmax, s->ncols[lvl_cblk[i]]);
+        if (L.nmax > 1024) {
+            fprintf(stderr, "pastix_b200: cblk of %d columns exceeds the supported width 1024\n", L.nmax);
+            return ERR_NOTIMPL;
+        }
+        int TR = 64;
+        while (TR > 16 && (size_t)TR * L.nmax * s->esz > trsm_smem) TR >>= 1;
+        if ((size_t)TR * L.nmax * s->esz > trsm_smem) return ERR_NOTIMPL;
+        s->lvl_tr[l] = TR;
+        L.t0 = (int)trsm.size();
+        s->lvl_s0[l] = (int)stask.size();
+        for (int i = L.c0; i < L.c1; i++) {
+            const int k = lvl_cblk[i];
+            for (int r0 = s->ncols[k]; r0 < s->stride[k]; r0 += TR) trsm.push_back({k, r0});
+            for (int r0 = s->ncols[k]; r0 < s->stride[k]; r0 += 128) stask.push_back({k, r0});
+        }
+        L.t1 = (int)trsm.size();
+        s->lvl_s1[l] = (int)stask.size();
+        // number of sources of this level facing each cblk
+        for (int i = L.c0; i < L.c1; i++) {
+            const int k = lvl_cblk[i];
+            for (int b = s->fblok[k] + 1; b < s->fblok[k + 1]; b++) {
+                const int f = s->fcblk[b];
+                if (src_last[f] != k) {
+                    src_last[f] = k;
+                    src_count[f]++;
+                }
+            }
+        }
+        L.u0 = (int)upds.size();
+        int tile0 = 0;
+        int64_t flops = 0;
+        for (int i = L.c0; i < L.c1; i++) {
+            const int k = lvl_cblk[i];
+            const int nc = s->ncols[k];
+            flops += (int64_t)nc * nc * nc / 3;
+            for (int j = s->fblok[k] + 1; j < s->fblok[k + 1]; j++) {
+                const int f = s->fcblk[j];
+                const int atomic = src_count[f] > 1 ? UPD_ATOMIC : 0;
+                const int nj = s->lrow[j] - s->frow[j] + 1;
+                for (int side = 0; side < (s->facto == FACTO_GETRF ? 2 : 1); side++) {
+                    Upd u{};
+                    u.k = k;
+                    u.j = j;
+                    u.f = f;
+                    u.rowB0 = s->rowoff[j];
+                    if (side == 0) {
+                        u.rowA0 = s->rowoff[j];
+                        u.flags = atomic;
+                        if (s->facto != FACTO_GETRF) u.flags |= UPD_SYM;
+                        if (s->facto == FACTO_SYTRF) u.flags |= UPD_SCALE_D;
+                        if (s->facto == FACTO_GETRF) u.flags |= UPD_B_U;
+                    } else {
+                        if (j + 1 >= s->fblok[k + 1]) continue;
+                        u.rowA0 = s->rowoff[j + 1];
+                        u.flags = atomic | UPD_A_U | UPD_C_U;
+                    }
+                    u.M = s->stride[k] - u.rowA0;
+                    u.N = nj;
+                    u.K = nc;
+                    u.colbase = s->frow[j] - s->fcol[f];
+                    u.tiles_m = (u.M + 63) / 64;
+                    u.tiles_n = (u.N + 63) / 64;
+                    const int nt = (u.flags & UPD_SYM) ? u.tiles_n * u.tiles_m - u.tiles_n * (u.tiles_n - 1) / 2
+                                                       : u.tiles_n * u.tiles_m;
+                    u.tile0 = tile0;
+                    tile0 += nt;
+                    flops += 2LL * u.M * u.N * u.K;
+                    upds.push_back(u);
+                }
+            }
+        }
+        L.u1 = (int)upds.size();
+        L.ntiles = tile0;
+        L.flops = flops;
+        s->total_tiles += tile0;
+        // reset the per-level source counters
+        for (int i = L.c0; i < L.c1; i++) {
+            const int k = lvl_cblk[i];
+            for (int b = s->fblok[k] + 1; b < s->fblok[k + 1]; b++) {
+                src_count[s->fcblk[b]] = 0;
+                src_last[s->fcblk[b]] = -1;
+            }
+        }
+        s->nmax_all = std::max(s->nmax_all, L.nmax);
+    }
+    RET(s->dupload(&s->d_lvl_cblk, lvl_cblk));
+    RET(s->dupload(&s->d_trsm, trsm));
+    RET(s->dupload(&s->d_stask, stask));
+    RET(s->dupload(&s->d_upd, upds));
+    return ERR_SUCCESS;
+}
+
+int ensure_ws(b200_solver_t *s, size_t doubles) {
+    if (doubles <= s->ws_cap) return ERR_SUCCESS;
+    for (auto &kv : s->solve_graphs) cudaGraphExecDestroy(kv.second);
+    s->solve_graphs.clear();
+    if (s->d_ws) cudaFree(s->d_ws);
+    s->d_ws = nullptr;
+    s->ws_cap = 0;
+    RET(dalloc(&s->d_ws, doubles));
+    s->ws_cap = doubles;
+    return ERR_SUCCESS;
+}
+
+int ensure_scal(b200_solver_t *s, int count) {
+    if (count <= s->scal_cap) return ERR_SUCCESS;
+    if (s->d_scal) cudaFree(s->d_scal);
+    s->d_scal = nullptr;
+    RET(dalloc(&s->d_scal, (size_t)count));
+    s->scal_cap = count;
+    return ERR_SUCCESS;
+}
+
+// ---------------------------------------------------------------- numfact
+
+template <typename T>
+int enqueue_numfact(b200_solver_t *s, cudaStream_t st) {
+    T *L = (T *)s->dL, *U = (T *)s->dU;
+    int launches = 0;
+    CU(cudaMemsetAsync(L, 0, s->arena * sizeof(T), st));
+    if (U) CU(cudaMemsetAsync(U, 0, s->arena * sizeof(T), st));
+    CU(cudaMemsetAsync(s->d_npiv, 0, sizeof(unsigned long long), st));
+    CU(cudaMemsetAsync(s->d_err, 0, sizeof(int), st));
+    launch_scatter<T>(s->nnz, s->d_dest, s->d_Lv, s->d_Uv, L, U, st);
+    launches++;
+    for (size_t l = 0; l < s->levels.size(); l++) {
+        const Level &Lv = s->levels[l];
+        launch_diag<T>(s->facto, s->ds, s->d_lvl_cblk + Lv.c0, Lv.c1 - Lv.c0, L, U, s->d_thr, s->d_npiv, s->d_err, st);
+        launches++;
+        const int nt = Lv.t1 - Lv.t0;
+        if (nt > 0) {
+            const int TR = s->lvl_tr[l];
+            if (s->facto == FACTO_POTRF) {
+                launch_trsm<T>(s->ds, s->d_trsm + Lv.t0, nt, TR, Lv.nmax, L, L, 1, 0, st);
+            } else if (s->facto == FACTO_SYTRF) {
+                launch_trsm<T>(s->ds, s->d_trsm + Lv.t0, nt, TR, Lv.nmax, L, L, 0, 0, st);
+            } else {
+                launch_trsm<T>(s->ds, s->d_trsm + Lv.t0, nt, TR, Lv.nmax, L, L, 0, 0, st);
+                launch_trsm<T>(s->ds, s->d_trsm + Lv.t0, nt, TR, Lv.nmax, U, L, 1, 1, st);
+                launches++;
+            }
+            launches++;
+        }
+        if (Lv.ntiles > 0) {
+            if (sizeof(T) == 8)
+                launch_update_f64(s->ds, s->d_upd + Lv.u0, Lv.u1 - Lv.u0, Lv.ntiles, (double *)L, (double *)U, st);
+            else
+                launch_update_f32(s->ds, s->d_upd + Lv.u0, Lv.u1 - Lv.u0, Lv.ntiles, (float *)L, (float *)U, st);
+            launches++;
+        }
+    }
+    CU(cudaGetLastError());
+    s->launches_fact = launches;
+    return ERR_SUCCESS;
+}
+
+// ---------------------------------------------------------------- solve (permuted basis)
+
+template <typename T>
+int enqueue_sweeps(b200_solver_t *s, double *x, int64_t ldx, int nrhs, cudaStream_t st, int *launches) {
+    const T *L = (const T *)s->dL;
+    const T *Ub = (s->facto == FACTO_GETRF) ? (const T *)s->dU : L;
+    const int nlev = (int)s->levels.size();
+    const int unitL = (s->facto != FACTO_POTRF);
+    for (int l = 0; l < nlev; l++) {
+        const Level &Lv = s->levels[l];
+        launch_solve_diag<T>(s->ds, s->d_lvl_cblk + Lv.c0, Lv.c1 - Lv.c0, Lv.nmax, L, x, ldx, nrhs, 0, unitL, st);
+        const int ns = s->lvl_s1[l] - s->lvl_s0[l];
+        launch_solve_offdiag<T>(s->ds, s->d_stask + s->lvl_s0[l], ns, L, x, ldx, nrhs, 0, st);
+        *launches += 1 + (ns > 0);
+    }
+    if (s->facto == FACTO_SYTRF) {
+        launch_solve_scale_diag<T>(s->ds, s->d_lvl_cblk, s->cblknbr, L, x, ldx, nrhs, st);
+        *launches += 1;
+    }
+    const int unitU = (s->facto == FACTO_SYTRF);
+    for (int l = nlev - 1; l >= 0; l--) {
+        const Level &Lv = s->levels[l];
+        const int ns = s->lvl_s1[l] - s->lvl_s0[l];
+        launch_solve_offdiag<T>(s->ds, s->d_stask + s->lvl_s0[l], ns, Ub, x, ldx, nrhs, 1, st);
+        launch_solve_diag<T>(s->ds, s->d_lvl_cblk + Lv.c0, Lv.c1 - Lv.c0, Lv.nmax, Ub, x, ldx, nrhs, 1, unitU, st);
+        *launches += 1 + (ns > 0);
+    }
+    CU(cudaGetLastError());
+    return ERR_SUCCESS;
+}
+
+int sweeps(b200_solver_t *s, double *x, int64_t ldx, int nrhs, cudaStream_t st, int *launches) {
+    return s->f32 ? enqueue_sweeps<float>(s, x, ldx, nrhs, st, launches)
+                  : enqueue_sweeps<double>(s, x, ldx, nrhs, st, launches);
+}
+
+// Full solve of device b (original ordering): permute, sweeps, permute back.
+// Uses ws[0 : n*nrhs] as the permuted block; replayed from a CUDA graph per nrhs
+// when the call runs on the solver's own stream.
+int solve_device(b200_solver_t *s, int nrhs, double *b, int64_t ldb, cudaStream_t st) {
+    const int n = s->n;
+    RET(ensure_ws(s, (size_t)n * nrhs));
+    double *xp = s->d_ws;
+    int launches = 2;
+    launch_permute(n, nrhs, s->d_peri, b, ldb, xp, n, 1, st);
+    RET(sweeps(s, xp, n, nrhs, st, &launches));
+    launch_permute(n, nrhs, s->d_peri, xp, n, b, ldb, 0, st);
+    CU(cudaGetLastError());
+    s->launches_solve = launches;
+    return ERR_SUCCESS;
+}
+
+// ---------------------------------------------------------------- refinement (permuted basis, double)
+
+struct RefineCtx {
+    b200_solver_t *s;
+    cudaStream_t st;
+    int n, nrhs;
+    // A x in the permuted basis with the bcsc
+    int spmv(const double *x, double *y, double alpha, double beta) {
+        const double *vals = (s->facto == FACTO_GETRF) ? s->d_Uv : s->d_Lv;
+        launch_spmv(n, nrhs, s->d_colptr, s->d_rowtab, vals, x, n, y, n, alpha, beta, st);
+        return ERR_SUCCESS;
+    }
+    // z <- M^{-1} z with the factor (sweeps only, already permuted)
+    int spsv(double *z) {
+        int l = 0;
+        return sweeps(s, z, n, nrhs, st, &l);
+    }
+    int dots(const double *x, const double *y, std::vector<double> &out) {
+        launch_dots(n, nrhs, x, n, y, n, s->d_scal, st);
+        out.resize(nrhs);
+        CU(cudaMemcpyAsync(out.data(), s->d_scal, nrhs * sizeof(double), cudaMemcpyDeviceToHost, st));
+        CU(cudaStreamSynchronize(st));
+        return ERR_SUCCESS;
+    }
+    int set_scal(const std::vector<double> &v, int slot) {
+        CU(cudaMemcpyAsync(s->d_scal + (size_t)slot * nrhs, v.data(), nrhs * sizeof(double), cudaMemcpyHostToDevice,
+                           st));
+        return ERR_SUCCESS;
+    }
+    double *scal(int slot) { return s->d_scal + (size_t)slot * nrhs; }
+};
+
+// z_pivot_smp (refinement/z_refine_pivot.c:45-140), all right-hand sides together,
+// each column with its own stopping rule.
+int refine_sr(RefineCtx &c, const double *b, double *x, int itermax, double eps, int64_t *niter,
+              std::vector<double> &berr) {
+    const int n = c.n, R = c.nrhs;
+    double *r = c.s->d_ws + (size_t)2 * n * R, *dx = r + (size_t)n * R;
+    std::vector<double> nb, nr, last(R, 0.0), mask(R, 1.0);
+    RET(c.dots(b, b, nb));
+    for (auto &v : nb) v = std::sqrt(v);
+    int iter = 0;
+    bool any = true;
+    berr.assign(R, 0.0);
+    while (any) {
+        launch_copy(n, R, b, n, r, n, c.st);
+        RET(c.spmv(x, r, -1.0, 1.0));
+        RET(c.dots(r, r, nr));
+        any = false;
+        for (int j = 0; j < R; j++) {
+            const double be = std::sqrt(nr[j]) / (nb[j] > 0 ? nb[j] : 1.0);
+            if (mask[j] == 0.0) continue;
+            berr[j] = be;
+            if (iter == 0) last[j] = 3 * be;
+            if (iter < itermax && be > eps && be <= last[j] / 2.0) {
+                last[j] = be;
+                any = true;
+            } else {
+                mask[j] = 0.0;
+            }
+        }
+        if (!any) break;
+        launch_copy(n, R, r, n, dx, n, c.st);
+        RET(c.spsv(dx));
+        RET(c.set_scal(mask, 0));
+        launch_axpys(n, R, c.scal(0), 1.0, dx, n, x, n, c.st);
+        iter++;
+    }
+    *niter = iter;
+    return ERR_SUCCESS;
+}
+
+// z_grad_smp (refinement/z_refine_grad.c:46-156): preconditioned CG.
+int refine_cg(RefineCtx &c, const double *b, double *x, int itermax, double eps, int64_t *niter,
+              std::vector<double> &berr) {
+    const int n = c.n, R = c.nrhs;
+    const size_t blk = (size_t)n * R;
+    double *gr = c.s->d_ws + 2 * blk, *gp = gr + blk, *gz = gp + blk, *g2 = gz + blk;
+    std::vector<double> nb, nx, nr, beta, alpha, tmp;
+    RET(c.dots(b, b, nb));
+    RET(c.dots(x, x, nx));
+    for (auto &v : nb) v = std::sqrt(v);
+    launch_copy(n, R, b, n, gr, n, c.st);
+    RET(c.spmv(x, gr, -1.0, 1.0));
+    RET(c.dots(gr, gr, nr));
+    std::vector<double> resid(R), active(R, 1.0);
+    bool any = false;
+    for (int j = 0; j < R; j++) {
+        resid[j] = std::sqrt(nr[j]) / (nb[j] > 0 ? nb[j] : 1.0);
+        if (resid[j] > eps) any = true; else active[j] = 0.0;
+    }
+    launch_copy(n, R, gr, n, gz, n, c.st);
+    RET(c.spsv(gz));
+    launch_copy(n, R, gz, n, gp, n, c.st);
+    int iter = 0;
+    while (any && iter < itermax) {
+        iter++;
+        RET(c.spmv(gp, g2, 1.0, 0.0));
+        RET(c.dots(gr, gz, beta));
+        RET(c.dots(g2, gp, alpha));
+        for (int j = 0; j < R; j++) alpha[j] = (active[j] != 0.0 && alpha[j] != 0.0) ? beta[j] / alpha[j] : 0.0;
+        RET(c.set_scal(alpha, 0));
+        launch_axpys(n, R, c.scal(0), 1.0, gp, n, x, n, c.st);
+        launch_axpys(n, R, c.scal(0), -1.0, g2, n, gr, n, c.st);
+        launch_copy(n, R, gr, n, gz, n, c.st);
+        RET(c.spsv(gz));
+        RET(c.dots(gr, gz, tmp));
+        for (int j = 0; j < R; j++) tmp[j] = (beta[j] != 0.0) ? tmp[j] / beta[j] : 0.0;
+        RET(c.set_scal(tmp, 1));
+        launch_xpbys(n, R, gz, n, c.scal(1), gp, n, c.st);
+        RET(c.dots(gr, gr, nr));
+        any = false;
+        for (int j = 0; j < R; j++) {
+            if (active[j] == 0.0) continue;
+            resid[j] = std::sqrt(nr[j]) / (nb[j] > 0 ? nb[j] : 1.0);
+            if (resid[j] > eps) any = true; else active[j] = 0.0;
+        }
+    }
+    berr = resid;
+    *niter = iter;
+    return ERR_SUCCESS;
+}
+
+// z_gmres_smp (refinement/z_refine_gmres.c:46-352): right-preconditioned
+// restarted GMRES(im) with Givens rotations; the Gram-Schmidt projections of all
+// right-hand sides are computed together.
+int refine_gmres(RefineCtx &c, const double *b, double *x, int itermax, int im, double eps, int64_t *niter,
+                 std::vector<double> &berr) {
+    const int n = c.n, R = c.nrhs;
+    const size_t blk = (size_t)n * R;
+    double *V = c.s->d_ws + 2 * blk;               // (im+1) blocks
+    double *W = V + (size_t)(im + 1) * blk;         // im blocks
+    const int im1 = im + 1;
+    std::vector<double> nb, nr, h, tmp;
+    RET(c.dots(b, b, nb));
+    for (auto &v : nb) v = std::sqrt(v);
+    std::vector<std::vector<double>> H(R, std::vector<double>((size_t)im * im1, 0.0));
+    std::vector<std::vector<double>> G(R, std::vector<double>(im1, 0.0)), cs(R, std::vector<double>(im, 0.0)),
+        sn(R, std::vector<double>(im, 0.0));
+    std::vector<double> resid_b(R, 0.0);
+    std::vector<char> done(R, 0);
+    int iters = 0;
+    bool outer = true;
+    while (outer) {
+        launch_copy(n, R, b, n, V, n, c.st);
+        RET(c.spmv(x, V, -1.0, 1.0));
+        RET(c.dots(V, V, nr));
+        bool any = false;
+        std::vector<double> inv(R, 0.0);
+        for (int j = 0; j < R; j++) {
+            const double resid = std::sqrt(nr[j]);
+            resid_b[j] = resid / (nb[j] > 0 ? nb[j] : 1.0);
+            done[j] = resid_b[j] <= eps;
+            if (!done[j]) any = true;
+            inv[j] = (!done[j] && resid > 0) ? 1.0 / resid : 0.0;
+            std::fill(G[j].begin(), G[j].end(), 0.0);
+            G[j][0] = done[j] ? 0.0 : resid;
+            std::fill(H[j].begin(), H[j].end(), 0.0);
+        }
+        if (!any) break;
+        RET(c.set_scal(inv, 0));
+        launch_scal_cols(n, R, c.scal(0), V, n, V, n, c.st);
+        int i = -1;
+        bool inner = true;
+        while (inner) {
+            i++;
+            double *Vi = V + (size_t)i * blk, *Wi = W + (size_t)i * blk, *Vn = V + (size_t)(i + 1) * blk;
+            launch_copy(n, R, Vi, n, Wi, n, c.st);
+            RET(c.spsv(Wi));
+            RET(c.spmv(Wi, Vn, 1.0, 0.0));
+            for (int jj = 0; jj <= i; jj++) {
+                RET(c.dots(Vn, V + (size_t)jj * blk, h));
+                for (int j = 0; j < R; j++) H[j][(size_t)i * im1 + jj] = h[j];
+                RET(c.set_scal(h, 0));
+                launch_axpys(n, R, c.scal(0), -1.0, V + (size_t)jj * blk, n, Vn, n, c.st);
+            }
+            RET(c.dots(Vn, Vn, nr));
+            std::vector<double> sc(R, 1.0);
+            for (int j = 0; j < R; j++) {
+                const double norm = std::sqrt(nr[j]);
+                double *Hi = &H[j][(size_t)i * im1];
+                Hi[i + 1] = norm;
+                sc[j] = norm > 1e-50 ? 1.0 / norm : 1.0;
+                for (int q = 0; q < i; q++) {
+                    const double t = Hi[q];
+                    Hi[q] = cs[j][q] * t + sn[j][q] * Hi[q + 1];
+                    Hi[q + 1] = cs[j][q] * Hi[q + 1] - sn[j][q] * t;
+                }
+                double t = std::sqrt(Hi[i] * Hi[i] + Hi[i + 1] * Hi[i + 1]);
+                if (std::fabs(t) <= eps) t = eps;
+                cs[j][i] = Hi[i] / t;
+                sn[j][i] = Hi[i + 1] / t;
+                G[j][i + 1] = -sn[j][i] * G[j][i];
+                G[j][i] = cs[j][i] * G[j][i];
+                Hi[i] = cs[j][i] * Hi[i] + sn[j][i] * Hi[i + 1];
+                if (!done[j]) resid_b[j] = std::fabs(G[j][i + 1]) / (nb[j] > 0 ? nb[j] : 1.0);
+            }
+            RET(c.set_scal(sc, 0));
+            launch_scal_cols(n, R, c.scal(0), Vn, n, Vn, n, c.st);
+            iters++;
+            bool all_conv = true;
+            for (int j = 0; j < R; j++)
+                if (!done[j] && resid_b[j] > eps) all_conv = false;
+            if (i + 1 >= im || all_conv || iters >= itermax) inner = false;
+        }
+        // y = H^{-1} g (upper triangular, i+1 columns), x += W y
+        for (int j = 0; j < R; j++) {
+            std::vector<double> &g = G[j];
+            for (int q = i; q >= 0; q--) {
+                double v = g[q];
+                for (int p = q + 1; p <= i; p++) v -= H[j][(size_t)p * im1 + q] * g[p];
+                const double d = H[j][(size_t)q * im1 + q];
+                g[q] = (d != 0.0) ? v / d : 0.0;
+            }
+        }
+        for (int q = 0; q <= i; q++) {
+            std::vector<double> y(R);
+            for (int j = 0; j < R; j++) y[j] = G[j][q];
+            RET(c.set_scal(y, 0));
+            launch_axpys(n, R, c.scal(0), 1.0, W + (size_t)q * blk, n, x, n, c.st);
+        }
+        if (iters >= itermax) outer = false;
+    }
+    berr = resid_b;
+    *niter = iters;
+    return ERR_SUCCESS;
+}
+
+int refine_device(b200_solver_t *s, int nrhs, const double *b, int64_t ldb, double *x, int64_t ldx, int method,
+                  double eps, int64_t itermax, int64_t im, int64_t *niter, double *berr, cudaStream_t st) {
+    const int n = s->n;
+    if (im < 1) im = 25;
+    const size_t blk = (size_t)n * nrhs;
+    size_t need = 2 * blk;
+    if (method == B200_REFINE_SR) need += 2 * blk;
+    else if (method == B200_REFINE_CG) need += 4 * blk;
+    else need += (size_t)(2 * im + 1) * blk;
+    RET(ensure_ws(s, need));
+    RET(ensure_scal(s, 2 * nrhs));
+    double *bp = s->d_ws, *xp = s->d_ws + blk;
+    launch_permute(n, nrhs, s->d_peri, b, ldb, bp, n, 1, st);
+    launch_permute(n, nrhs, s->d_peri, x, ldx, xp, n, 1, st);
+    RefineCtx c{s, st, n, nrhs};
+    std::vector<double> be;
+    int64_t it = 0;
+    int rc;
+    if (method == B200_REFINE_SR) rc = refine_sr(c, bp, xp, (int)itermax, eps, &it, be);
+    else if (method == B200_REFINE_CG) rc = refine_cg(c, bp, xp, (int)itermax, eps, &it, be);
+    else rc = refine_gmres(c, bp, xp, (int)itermax, (int)im, eps, &it, be);
+    if (rc) return rc;
+    launch_permute(n, nrhs, s->d_peri, xp, n, x, ldx, 0, st);
+    CU(cudaGetLastError());
+    if (niter) *niter = it;
+    if (berr)
+        for (int j = 0; j < nrhs; j++) berr[j] = be[j];
+    return ERR_SUCCESS;
+}
+
+}  // namespace
+
+// ====================================================================== C ABI
+
+extern "C" {
+
+const char *b200_strerror(int code) {
+    switch (code) {
+        case 0: return "success";
+        case ERR_ALLOC: return "allocation error";
+        case ERR_NOTIMPL: return "not implemented";
+        case ERR_OOM: return "out of device memory";
+        case ERR_INTERNAL: return "internal error (CUDA failure or negative pivot in Cholesky)";
+        case ERR_BADPARAM: return "bad parameter";
+        default: return "unknown error";
+    }
+}
+
+int b200_solver_create(const b200_symbol_t *sym, int facto, int precision, void *stream, b200_solver_t **out) {
+    if (!sym || !out || facto < 0 || facto > 2 || precision < 0 || precision > 3) return ERR_BADPARAM;
+    if (sym->n <= 0 || sym->cblknbr <= 0 || sym->n >= (1LL << 31) || sym->bloknbr >= (1LL << 31)) return ERR_BADPARAM;
+    int dev = 0;
+    CU(cudaGetDevice(&dev));
+    b200_solver_t *s = new b200_solver_t();
+    *out = nullptr;
+    s->facto = facto;
+    s->prec = precision;
+    s->f32 = precision != B200_PREC_FP64;
+    s->esz = s->f32 ? 4 : 8;
+    if (stream) {
+        s->st = (cudaStream_t)stream;
+    } else {
+        if (cudaStreamCreateWithFlags(&s->st, cudaStreamNonBlocking) != cudaSuccess) {
+            delete s;
+            return ERR_INTERNAL;
+        }
+        s->own_stream = true;
+    }
+    const int N = (int)sym->cblknbr, B = (int)sym->bloknbr;
+    s->n = (int)sym->n;
+    s->cblknbr = N;
+    s->bloknbr = B;
+    s->fcol.resize(N + 1);
+    s->ncols.resize(N);
+    s->stride.resize(N);
+    s->ld.resize(N);
+    s->off.resize(N);
+    s->fblok.resize(N + 1);
+    s->frow.resize(B);
+    s->lrow.resize(B);
+    s->rowoff.resize(B);
+    s->fcblk.resize(B);
+    s->peri.resize(s->n);
+    int64_t pos = 0, coef = 0;
+    const int64_t align = s->f32 ? 64 : 32;  // 256-byte panel starts
+    for (int k = 0; k <= N; k++) {
+        s->fcol[k] = (int)sym->cblk_fcolnum[k];
+        s->fblok[k] = (int)sym->cblk_fblok[k];
+    }
+    for (int k = 0; k < N; k++) {
+        s->ncols[k] = (int)(sym->cblk_lcolnum[k] - sym->cblk_fcolnum[k] + 1);
+        s->stride[k] = (int)sym->cblk_stride[k];
+        s->ld[k] = (s->stride[k] + 3) & ~3;
+        pos = (pos + align - 1) / align * align;
+        s->off[k] = pos;
+        pos += (int64_t)s->ld[k] * s->ncols[k];
+        coef += (int64_t)s->stride[k] * s->ncols[k];
+        if (s->fblok[k + 1] <= s->fblok[k] || s->ncols[k] <= 0) {
+            delete s;
+            return ERR_BADPARAM;
+        }
+        int row = 0;
+        for (int b = s->fblok[k]; b < s->fblok[k + 1]; b++) {
+            s->frow[b] = (int)sym->blok_frownum[b];
+            s->lrow[b] = (int)sym->blok_lrownum[b];
+            s->fcblk[b] = (int)sym->blok_fcblknm[b];
+            s->rowoff[b] = row;
+            row += s->lrow[b] - s->frow[b] + 1;
+        }
+        if (row != s->stride[k]) {
+            delete s;
+            return ERR_BADPARAM;
+        }
+    }
+    for (int i = 0; i < s->n; i++) s->peri[i] = (int)sym->peritab[i];
+    s->arena = (pos + align - 1) / align * align;
+    s->coefnbr = coef;
+    int rc = ERR_SUCCESS;
+    s->trsm_smem = configure_factor_kernels();
+    if (s->trsm_smem < 0 || configure_solve_kernels() < 0) {
+        fprintf(stderr, "pastix_b200: cannot configure the shared memory of the kernels\n");
+        rc = ERR_INTERNAL;
+    }
+    int *d_fcol, *d_ncols, *d_stride, *d_ld, *d_fblok, *d_frow, *d_lrow, *d_rowoff, *d_fcblk;
+    int64_t *d_off;
+    if (!rc) rc = s->dupload(&d_fcol, s->fcol);
+    if (!rc) rc = s->dupload(&d_ncols, s->ncols);
+    if (!rc) rc = s->dupload(&d_stride, s->stride);
+    if (!rc) rc = s->dupload(&d_ld, s->ld);
+    if (!rc) rc = s->dupload(&d_off, s->off);
+    if (!rc) rc = s->dupload(&d_fblok, s->fblok);
+    if (!rc) rc = s->dupload(&d_frow, s->frow);
+    if (!rc) rc = s->dupload(&d_lrow, s->lrow);
+    if (!rc) rc = s->dupload(&d_rowoff, s->rowoff);
+    if (!rc) rc = s->dupload(&d_fcblk, s->fcblk);
+    if (!rc) rc = s->dupload(&s->d_peri, s->peri);
+    if (!rc) {
+        s->ds = DevSym{s->n, N, B, d_fcol, d_ncols, d_stride, d_ld, d_off, d_fblok, d_frow, d_lrow, d_rowoff, d_fcblk};
+        rc = build_schedule(s);
+    }
+    if (!rc) rc = dalloc((char **)&s->dL, (size_t)s->arena * s->esz);
+    if (!rc && facto == FACTO_GETRF) rc = dalloc((char **)&s->dU, (size_t)s->arena * s->esz);
+    if (!rc) rc = s->dmalloc(&s->d_thr, 1);
+    if (!rc) rc = s->dmalloc(&s->d_npiv, 1);
+    if (!rc) rc = s->dmalloc(&s->d_err, 1);
+    if (!rc && cudaEventCreate(&s->ev0) != cudaSuccess) rc = ERR_INTERNAL;
+    if (!rc && cudaEventCreate(&s->ev1) != cudaSuccess) rc = ERR_INTERNAL;
+    if (!rc && cudaStreamSynchronize(s->st) != cudaSuccess) rc = ERR_INTERNAL;
+    if (rc) {
+        b200_solver_destroy(s);
+        return rc;
+    }
+    *out = s;
+    return ERR_SUCCESS;
+}
+
+int b200_solver_destroy(b200_solver_t *s) {
+    if (!s) return ERR_SUCCESS;
+    if (s->st) cudaStreamSynchronize(s->st);
+    if (s->fact_graph) cudaGraphExecDestroy(s->fact_graph);
+    for (auto &kv : s->solve_graphs) cudaGraphExecDestroy(kv.second);
+    for (void *p : s->dev_allocs) cudaFree(p);
+    if (s->dL) cudaFree(s->dL);
+    if (s->dU) cudaFree(s->dU);
+    if (s->d_colptr) cudaFree(s->d_colptr);
+    if (s->d_rowtab) cudaFree(s->d_rowtab);
+    if (s->d_Lv) cudaFree(s->d_Lv);
+    if (s->d_Uv) cudaFree(s->d_Uv);
+    if (s->d_dest) cudaFree(s->d_dest);
+    if (s->d_ws) cudaFree(s->d_ws);
+    if (s->d_scal) cudaFree(s->d_scal);
+    if (s->ev0) cudaEventDestroy(s->ev0);
+    if (s->ev1) cudaEventDestroy(s->ev1);
+    if (s->own_stream && s->st) cudaStreamDestroy(s->st);
+    delete s;
+    return ERR_SUCCESS;
+}
+
+int b200_bcsc_load(b200_solver_t *s, int64_t nnz, const int64_t *colptr, const int64_t *rowtab, const double *Lvalues,
+                   const double *Uvalues, double anorm) {
+    if (!s || nnz < 0 || !colptr || !rowtab || !Lvalues) return ERR_BADPARAM;
+    if (s->facto == FACTO_GETRF && !Uvalues) return ERR_BADPARAM;
+    const int n = s->n;
+    if (colptr[0] != 0 || colptr[n] != nnz) return ERR_BADPARAM;
+    bool same = (s->nnz == nnz) && std::equal(colptr, colptr + n + 1, s->h_colptr.begin()) &&
+                std::equal(rowtab, rowtab + nnz, s->h_rowtab.begin());
+    if (!same) {
+        if (s->d_colptr) cudaFree(s->d_colptr);
+        if (s->d_rowtab) cudaFree(s->d_rowtab);
+        if (s->d_Lv) cudaFree(s->d_Lv);
+        if (s->d_Uv) cudaFree(s->d_Uv);
+        if (s->d_dest) cudaFree(s->d_dest);
+        s->d_colptr = nullptr; s->d_rowtab = nullptr; s->d_Lv = nullptr; s->d_Uv = nullptr; s->d_dest = nullptr;
+        if (s->fact_graph) cudaGraphExecDestroy(s->fact_graph);
+        s->fact_graph = nullptr;
+        s->h_colptr.assign(colptr, colptr + n + 1);
+        s->h_rowtab.assign(rowtab, rowtab + nnz);
+        // destination of every bcsc entry in the panel arena (cpucblk_zfillin_fr,
+        // kernels/cpucblk_zinit.c:229-309): rows above the diagonal are skipped,
+        // bit 62 marks strictly-lower entries that also go to the U arena
+        std::vector<int64_t> dest(nnz, -1);
+        std::vector<int> rows32(nnz);
+        for (int k = 0; k < s->cblknbr; k++) {
+            for (int col = s->fcol[k]; col < s->fcol[k] + s->ncols[k] && col < n; col++) {
+                const int jc = col - s->fcol[k];
+                for (int64_t e = colptr[col]; e < colptr[col + 1]; e++) {
+                    const int64_t r = rowtab[e];
+                    if (r < 0 || r >= n) return ERR_BADPARAM;
+                    rows32[e] = (int)r;
+                    if (r < col) continue;
+                    int lo = s->fblok[k], hi = s->fblok[k + 1] - 1;
+                    while (lo < hi) {
+                        const int mid = (lo + hi + 1) >> 1;
+                        if (s->frow[mid] <= r) lo = mid; else hi = mid - 1;
+                    }
+                    if (r < s->frow[lo] || r > s->lrow[lo]) continue;  // dropped, as PaStiX does
+                    int64_t d = s->off[k] + s->rowoff[lo] + (r - s->frow[lo]) + (int64_t)jc * s->ld[k];
+                    if (r > col) d |= (int64_t)1 << 62;
+                    dest[e] = d;
+                }
+            }
+        }
+        RET(dalloc(&s->d_colptr, (size_t)n + 1));
+        RET(dalloc(&s->d_rowtab, (size_t)nnz));
+        RET(dalloc(&s->d_dest, (size_t)nnz));
+        RET(dalloc(&s->d_Lv, (size_t)nnz));
+        if (Uvalues) RET(dalloc(&s->d_Uv, (size_t)nnz));
+        CU(cudaMemcpyAsync(s->d_colptr, colptr, (n + 1) * sizeof(int64_t), cudaMemcpyHostToDevice, s->st));
+        CU(cudaMemcpyAsync(s->d_rowtab, rows32.data(), nnz * sizeof(int), cudaMemcpyHostToDevice, s->st));
+        CU(cudaMemcpyAsync(s->d_dest, dest.data(), nnz * sizeof(int64_t), cudaMemcpyHostToDevice, s->st));
+        CU(cudaStreamSynchronize(s->st));
+        s->nnz = nnz;
+    }
+    CU(cudaMemcpyAsync(s->d_Lv, Lvalues, nnz * sizeof(double), cudaMemcpyHostToDevice, s->st));
+    if (Uvalues && s->d_Uv) CU(cudaMemcpyAsync(s->d_Uv, Uvalues, nnz * sizeof(double), cudaMemcpyHostToDevice, s->st));
+    CU(cudaStreamSynchronize(s->st));
+    s->anorm = anorm;
+    s->factored = false;
+    return ERR_SUCCESS;
+}
+
+int b200_numfact(b200_solver_t *s, double epsilon_magn_ctrl, int64_t *nbpivots) {
+    if (!s || s->nnz < 0) return ERR_BADPARAM;
+    // threshold rule of pastix_subtask_sopalin (sopalin/pastix_task_sopalin.c:401-425)
+    double thr;
+    if (epsilon_magn_ctrl < 0.0) thr = -epsilon_magn_ctrl;
+    else if (epsilon_magn_ctrl == 0.0) {
+        const double eps = s->f32 ? std::ldexp(1.0, -24) : std::ldexp(1.0, -53);  // LAPACK xlamch('e')
+        thr = std::sqrt(eps) * s->anorm;
+    } else thr = epsilon_magn_ctrl * s->anorm;
+    s->thr_used = thr;
+    CU(cudaMemcpyAsync(s->d_thr, &thr, sizeof(double), cudaMemcpyHostToDevice, s->st));
+    if (!s->fact_graph) {
+        cudaGraph_t g;
+        CU(cudaStreamBeginCapture(s->st, cudaStreamCaptureModeThreadLocal));
+        int rc = s->f32 ? enqueue_numfact<float>(s, s->st) : enqueue_numfact<double>(s, s->st);
+        cudaError_t ec = cudaStreamEndCapture(s->st, &g);
+        if (rc) return rc;
+        CU(ec);
+        CU(cudaGraphInstantiate(&s->fact_graph, g, 0));
+        cudaGraphDestroy(g);
+    }
+    CU(cudaEventRecord(s->ev0, s->st));
+    CU(cudaGraphLaunch(s->fact_graph, s->st));
+    CU(cudaEventRecord(s->ev1, s->st));
+    unsigned long long piv = 0;
+    int err = 0;
+    CU(cudaMemcpyAsync(&piv, s->d_npiv, sizeof(piv), cudaMemcpyDeviceToHost, s->st));
+    CU(cudaMemcpyAsync(&err, s->d_err, sizeof(err), cudaMemcpyDeviceToHost, s->st));
+    CU(cudaStreamSynchronize(s->st));
+    float ms = 0;
+    cudaEventElapsedTime(&ms, s->ev0, s->ev1);
+    s->t_fact = ms;
+    s->last_npiv = (int64_t)piv;
+    if (nbpivots) *nbpivots = (int64_t)piv;
+    if (err) {
+        fprintf(stderr, "pastix_b200: negative diagonal term in the Cholesky factorization\n");
+        return ERR_INTERNAL;
+    }
+    s->factored = true;
+    return ERR_SUCCESS;
+}
+
+int b200_solve_device(b200_solver_t *s, int64_t nrhs, double *d_b, int64_t ldb, void *stream) {
+    if (!s || !s->factored || nrhs < 0 || ldb < s->n) return ERR_BADPARAM;
+    if (nrhs == 0) return ERR_SUCCESS;
+    cudaStream_t st = stream ? (cudaStream_t)stream : s->st;
+    return solve_device(s, (int)nrhs, d_b, ldb, st);
+}
+
+int b200_solve(b200_solver_t *s, int64_t nrhs, double *b, int64_t ldb) {
+    if (!s || !s->factored || nrhs < 0 || ldb < s->n || (!b && nrhs)) return ERR_BADPARAM;
+    if (nrhs == 0) return ERR_SUCCESS;
+    const int n = s->n;
+    double *db = nullptr;
+    RET(dalloc(&db, (size_t)n * nrhs));
+    int rc = ERR_SUCCESS;
+    if (cudaMemcpy2DAsync(db, n * sizeof(double), b, ldb * sizeof(double), n * sizeof(double), nrhs,
+                          cudaMemcpyHostToDevice, s->st) != cudaSuccess) rc = ERR_INTERNAL;
+    if (!rc) {
+        cudaEventRecord(s->ev0, s->st);
+        rc = solve_device(s, (int)nrhs, db, n, s->st);
+        cudaEventRecord(s->ev1, s->st);
+    }
+    if (!rc && cudaMemcpy2DAsync(b, ldb * sizeof(double), db, n * sizeof(double), n * sizeof(double), nrhs,
+                                 cudaMemcpyDeviceToHost, s->st) != cudaSuccess) rc = ERR_INTERNAL;
+    if (cudaStreamSynchronize(s->st) != cudaSuccess) rc = ERR_INTERNAL;
+    float ms = 0;
+    if (!rc) cudaEventElapsedTime(&ms, s->ev0, s->ev1);
+    s->t_solve = ms;
+    cudaFree(db);
+    return rc;
+}
+
+int b200_refine_device(b200_solver_t *s, int64_t nrhs, const double *d_b, int64_t ldb, double *d_x, int64_t ldx,
+                       int method, double eps, int64_t itermax, int64_t gmres_im, int64_t *niter, double *berr,
+                       void *stream) {
+    if (!s || !s->factored || nrhs < 0 || ldb < s->n || ldx < s->n || method < 0 || method > 2) return ERR_BADPARAM;
+    if (nrhs == 0) return ERR_SUCCESS;
+    cudaStream_t st = stream ? (cudaStream_t)stream : s->st;
+    auto t0 = std::chrono::steady_clock::now();
+    int rc = refine_device(s, (int)nrhs, d_b, ldb, d_x, ldx, method, eps, itermax, gmres_im, niter, berr, st);
+    if (!rc && cudaStreamSynchronize(st) != cudaSuccess) rc = ERR_INTERNAL;
+    s->t_refine = std::chrono::duration<double, std::milli>(std::chrono::steady_clock::now() - t0).count();
+    return rc;
+}
+
+int b200_refine(b200_solver_t *s, int64_t nrhs, const double *b, int64_t ldb, double *x, int64_t ldx, int method,
+                double eps, int64_t itermax, int64_t gmres_im, int64_t *niter, double *berr) {
+    if (!s || !s->factored || nrhs < 0 || ldb < s->n || ldx < s->n) return ERR_BADPARAM;
+    if (nrhs == 0) return ERR_SUCCESS;
+    const int n = s->n;
+    double *db = nullptr, *dx = nullptr;
+    RET(dalloc(&db, (size_t)n * nrhs));
+    int rc = dalloc(&dx, (size_t)n * nrhs);
+    if (!rc && cudaMemcpy2DAsync(db, n * sizeof(double), b, ldb * sizeof(double), n * sizeof(double), nrhs,
+                                 cudaMemcpyHostToDevice, s->st) != cudaSuccess) rc = ERR_INTERNAL;
+    if (!rc && cudaMemcpy2DAsync(dx, n * sizeof(double), x, ldx * sizeof(double), n * sizeof(double), nrhs,
+                                 cudaMemcpyHostToDevice, s->st) != cudaSuccess) rc = ERR_INTERNAL;
+    if (!rc) rc = b200_refine_device(s, nrhs, db, n, dx, n, method, eps, itermax, gmres_im, niter, berr, s->st);
+    if (!rc && cudaMemcpy2DAsync(x, ldx * sizeof(double), dx, n * sizeof(double), n * sizeof(double), nrhs,
+                                 cudaMemcpyDeviceToHost, s->st) != cudaSuccess) rc = ERR_INTERNAL;
+    if (cudaStreamSynchronize(s->st) != cudaSuccess) rc = ERR_INTERNAL;
+    cudaFree(db);
+    if (dx) cudaFree(dx);
+    return rc;
+}
+
+int b200_spmv(b200_solver_t *s, int64_t nrhs, double alpha, const double *x, int64_t ldx, double beta, double *y,
+              int64_t ldy) {
+    if (!s || s->nnz < 0 || nrhs < 0 || ldx < s->n || ldy < s->n) return ERR_BADPARAM;
+    if (nrhs == 0) return ERR_SUCCESS;
+    const int n = s->n;
+    const size_t blk = (size_t)n * nrhs;
+    double *d = nullptr;
+    RET(dalloc(&d, 4 * blk));
+    double *dx = d, *dy = d + blk, *px = d + 2 * blk, *py = d + 3 * blk;
+    int rc = ERR_SUCCESS;
+    if (cudaMemcpy2DAsync(dx, n * sizeof(double), x, ldx * sizeof(double), n * sizeof(double), nrhs,
+                          cudaMemcpyHostToDevice, s->st) != cudaSuccess) rc = ERR_INTERNAL;
+    if (!rc && cudaMemcpy2DAsync(dy, n * sizeof(double), y, ldy * sizeof(double), n * sizeof(double), nrhs,
+                                 cudaMemcpyHostToDevice, s->st) != cudaSuccess) rc = ERR_INTERNAL;
+    if (!rc) {
+        launch_permute(n, (int)nrhs, s->d_peri, dx, n, px, n, 1, s->st);
+        launch_permute(n, (int)nrhs, s->d_peri, dy, n, py, n, 1, s->st);
+        const double *vals = (s->facto == FACTO_GETRF) ? s->d_Uv : s->d_Lv;
+        launch_spmv(n, (int)nrhs, s->d_colptr, s->d_rowtab, vals, px, n, py, n, alpha, beta, s->st);
+        launch_permute(n, (int)nrhs, s->d_peri, py, n, dy, n, 0, s->st);
+        if (cudaMemcpy2DAsync(y, ldy * sizeof(double), dy, n * sizeof(double), n * sizeof(double), nrhs,
+                              cudaMemcpyDeviceToHost, s->st) != cudaSuccess) rc = ERR_INTERNAL;
+    }
+    if (cudaStreamSynchronize(s->st) != cudaSuccess) rc = ERR_INTERNAL;
+    cudaFree(d);
+    return rc;
+}
+
+int b200_factor_download(b200_solver_t *s, double *L, double *U) {
+    if (!s || !L || !s->factored) return ERR_BADPARAM;
+    std::vector<char> host((size_t)s->arena * s->esz);
+    for (int side = 0; side < 2; side++) {
+        double *out = side == 0 ? L : U;
+        void *src = side == 0 ? s->dL : s->dU;
+        if (!out) continue;
+        if (!src) return ERR_BADPARAM;
+        CU(cudaMemcpyAsync(host.data(), src, host.size(), cudaMemcpyDeviceToHost, s->st));
+        CU(cudaStreamSynchronize(s->st));
+        int64_t pos = 0;
+        for (int k = 0; k < s->cblknbr; k++) {
+            const int nc = s->ncols[k], ld = s->ld[k];
+            for (int b = s->fblok[k]; b < s->fblok[k + 1]; b++) {
+                const int m = s->lrow[b] - s->frow[b] + 1;
+                for (int j = 0; j < nc; j++)
+                    for (int i = 0; i < m; i++) {
+                        const int64_t src_i = s->off[k] + s->rowoff[b] + i + (int64_t)j * ld;
+                        out[pos + i + (int64_t)j * m] =
+                            s->f32 ? (double)((float *)host.data())[src_i] : ((double *)host.data())[src_i];
+                    }
+                pos += (int64_t)m * nc;
+            }
+        }
+    }
+    return ERR_SUCCESS;
+}
+
+int b200_stats(b200_solver_t *s, double *out) {
+    if (!s || !out) return ERR_BADPARAM;
+    out[0] = s->t_fact;
+    out[1] = s->t_solve;
+    out[2] = s->t_refine;
+    out[3] = (double)s->last_npiv;
+    out[4] = s->thr_used;
+    out[5] = (double)s->arena * s->esz * (s->dU ? 2 : 1);
+    out[6] = (double)s->levels.size();
+    out[7] = s->launches_fact;
+    out[8] = s->launches_solve;
+    out[9] = (double)s->coefnbr;
+    return ERR_SUCCESS;
+}
+
+}  // extern "C"

@@ -1,0 +1,166 @@
+"""ctypes binding of libpastix_b200.so (the C ABI of include/pastix_b200.h).
+
+This is the only way the Python layer reaches the GPU path.  There is no CPU
+fallback: if the library is missing, or no CUDA device is present, the calls fail
+with an exception.
+"""
+from __future__ import annotations
+
+import ctypes as C
+import os
+
+import numpy as np
+
+HERE = os.path.dirname(os.path.abspath(__file__))
+LIBPATH = os.path.join(HERE, "lib", "libpastix_b200.so")
+
+FACTO = {"potrf": 0, "sytrf": 1, "getrf": 2}
+PREC = {"fp64": 0, "fp32": 1, "tf32": 2, "tf32x3": 3}
+REFINE = {"gmres": 0, "cg": 1, "sr": 2}
+
+_P = C.c_void_p
+_I64 = C.c_int64
+_lib = None
+
+# exported symbols, in the order of include/pastix_b200.h
+SYMBOLS = ["b200_solver_create", "b200_solver_destroy", "b200_bcsc_load", "b200_numfact", "b200_solve",
+           "b200_solve_device", "b200_refine", "b200_refine_device", "b200_spmv", "b200_factor_download",
+           "b200_stats", "b200_strerror"]
+
+
+class Symbol(C.Structure):
+    _fields_ = [("n", _I64), ("cblknbr", _I64), ("bloknbr", _I64), ("brownbr", _I64)] + [
+        (f, _P) for f in ("cblk_fcolnum", "cblk_lcolnum", "cblk_fblok", "cblk_stride", "cblk_lcolidx",
+                          "cblk_brownum", "blok_frownum", "blok_lrownum", "blok_lcblknm", "blok_fcblknm",
+                          "browtab", "peritab")]
+
+
+class B200Error(RuntimeError):
+    pass
+
+
+def lib():
+    global _lib
+    if _lib is None:
+        if not os.path.exists(LIBPATH):
+            raise B200Error(f"{LIBPATH} is missing: build it with pastix_b200/build.py")
+        L = C.CDLL(LIBPATH)
+        L.b200_solver_create.argtypes = [C.POINTER(Symbol), C.c_int, C.c_int, _P, C.POINTER(_P)]
+        L.b200_solver_destroy.argtypes = [_P]
+        L.b200_bcsc_load.argtypes = [_P, _I64, _P, _P, _P, _P, C.c_double]
+        L.b200_numfact.argtypes = [_P, C.c_double, C.POINTER(_I64)]
+        L.b200_solve.argtypes = [_P, _I64, _P, _I64]
+        L.b200_solve_device.argtypes = [_P, _I64, _P, _I64, _P]
+        L.b200_refine.argtypes = [_P, _I64, _P, _I64, _P, _I64, C.c_int, C.c_double, _I64, _I64,
+                                  C.POINTER(_I64), _P]
+        L.b200_refine_device.argtypes = [_P, _I64, _P, _I64, _P, _I64, C.c_int, C.c_double, _I64, _I64,
+                                         C.POINTER(_I64), _P, _P]
+        L.b200_spmv.argtypes = [_P, _I64, C.c_double, _P, _I64, C.c_double, _P, _I64]
+        L.b200_factor_download.argtypes = [_P, _P, _P]
+        L.b200_stats.argtypes = [_P, _P]
+        L.b200_strerror.restype = C.c_char_p
+        L.b200_strerror.argtypes = [C.c_int]
+        _lib = L
+    return _lib
+
+
+def check(rc: int, what: str):
+    if rc != 0:
+        raise B200Error(f"{what}: {lib().b200_strerror(rc).decode()} (code {rc})")
+
+
+def _p(a):
+    return a.ctypes.data_as(_P) if a is not None else None
+
+
+class Solver:
+    """One factorization instance on the GPU (the B200 counterpart of a
+    pastix_data_t after analysis)."""
+
+    def __init__(self, st, facto="potrf", precision="fp64", stream=None):
+        self.st = st
+        self.facto = FACTO[facto] if isinstance(facto, str) else int(facto)
+        self.precision = PREC[precision] if isinstance(precision, str) else int(precision)
+        self.n = st.n
+        self._keep = [np.ascontiguousarray(a, dtype=np.int64) for a in (
+            st.cblk_fcolnum, st.cblk_lcolnum, st.cblk_fblok, st.cblk_stride, st.cblk_lcolidx, st.cblk_brownum,
+            st.blok_frownum, st.blok_lrownum, st.blok_lcblknm, st.blok_fcblknm,
+            st.browtab if st.browtab.size else np.zeros(1, np.int64), st.peritab)]
+        sym = Symbol(st.n, st.cblknbr, st.bloknbr, st.brownbr, *[a.ctypes.data for a in self._keep])
+        h = _P()
+        check(lib().b200_solver_create(C.byref(sym), self.facto, self.precision, stream, C.byref(h)),
+              "b200_solver_create")
+        self.h = h
+
+    def close(self):
+        if getattr(self, "h", None):
+            lib().b200_solver_destroy(self.h)
+            self.h = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+    def bcsc_load(self, bcsc):
+        colptr = np.ascontiguousarray(bcsc.colptr, dtype=np.int64)
+        rowtab = np.ascontiguousarray(bcsc.rowtab, dtype=np.int64)
+        Lv = np.ascontiguousarray(bcsc.Lvalues, dtype=np.float64)
+        Uv = np.ascontiguousarray(bcsc.Uvalues, dtype=np.float64) if bcsc.Uvalues is not None else None
+        check(lib().b200_bcsc_load(self.h, int(colptr[-1]), _p(colptr), _p(rowtab), _p(Lv), _p(Uv), bcsc.anorm),
+              "b200_bcsc_load")
+
+    def numfact(self, epsilon_magn_ctrl: float = 0.0) -> int:
+        piv = _I64(0)
+        check(lib().b200_numfact(self.h, epsilon_magn_ctrl, C.byref(piv)), "b200_numfact")
+        return int(piv.value)
+
+    def solve(self, b: np.ndarray) -> np.ndarray:
+        x = np.asfortranarray(np.array(b, dtype=np.float64).reshape(self.n, -1))
+        check(lib().b200_solve(self.h, x.shape[1], _p(x), self.n), "b200_solve")
+        return x.reshape(np.shape(b))
+
+    def solve_device(self, d_ptr: int, nrhs: int, ld: int, stream: int | None = None):
+        check(lib().b200_solve_device(self.h, nrhs, _P(d_ptr), ld, _P(stream) if stream else None),
+              "b200_solve_device")
+
+    def refine(self, b, x, method="gmres", eps=1e-12, itermax=250, gmres_im=25):
+        b2 = np.asfortranarray(np.array(b, dtype=np.float64).reshape(self.n, -1))
+        x2 = np.asfortranarray(np.array(x, dtype=np.float64).reshape(self.n, -1))
+        nit = _I64(0)
+        berr = np.zeros(b2.shape[1])
+        m = REFINE[method] if isinstance(method, str) else int(method)
+        check(lib().b200_refine(self.h, b2.shape[1], _p(b2), self.n, _p(x2), self.n, m, eps, itermax, gmres_im,
+                                C.byref(nit), _p(berr)), "b200_refine")
+        return x2.reshape(np.shape(x)), int(nit.value), berr
+
+    def refine_device(self, d_b: int, d_x: int, nrhs: int, method="gmres", eps=1e-12, itermax=250, gmres_im=25,
+                      stream: int | None = None):
+        nit = _I64(0)
+        berr = np.zeros(nrhs)
+        m = REFINE[method] if isinstance(method, str) else int(method)
+        check(lib().b200_refine_device(self.h, nrhs, _P(d_b), self.n, _P(d_x), self.n, m, eps, itermax, gmres_im,
+                                       C.byref(nit), _p(berr), _P(stream) if stream else None),
+              "b200_refine_device")
+        return int(nit.value), berr
+
+    def spmv(self, x, alpha=1.0, beta=0.0, y=None):
+        x2 = np.asfortranarray(np.array(x, dtype=np.float64).reshape(self.n, -1))
+        y2 = np.zeros_like(x2) if y is None else np.asfortranarray(np.array(y, dtype=np.float64).reshape(self.n, -1))
+        check(lib().b200_spmv(self.h, x2.shape[1], alpha, _p(x2), self.n, beta, _p(y2), self.n), "b200_spmv")
+        return y2.reshape(np.shape(x))
+
+    def factor(self):
+        """The factor in PaStiX's coeftab layout (2D blocks), as float64 arrays."""
+        L = np.zeros(self.st.coefnbr)
+        U = np.zeros(self.st.coefnbr) if self.facto == 2 else None
+        check(lib().b200_factor_download(self.h, _p(L), _p(U)), "b200_factor_download")
+        return L, U
+
+    def stats(self) -> dict:
+        out = np.zeros(10)
+        check(lib().b200_stats(self.h, _p(out)), "b200_stats")
+        return dict(numfact_ms=out[0], solve_ms=out[1], refine_ms=out[2], nbpivots=int(out[3]), threshold=out[4],
+                    device_bytes=int(out[5]), levels=int(out[6]), launches_numfact=int(out[7]),
+                    launches_solve=int(out[8]), coefnbr=int(out[9]))
