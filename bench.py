@@ -1,0 +1,425 @@
+"""Benchmark of the B200 supernodal factorization + solve (PaStiX hot path).
+
+Workload (default): 27-point 3D Laplacian on an 80^3 grid (n = 512,000; diagonal
+26 + 1e-3 shift, off-diagonals -1), real double, Cholesky, grid nested-dissection
+ordering through PaStiX's own analysis, 16 right-hand sides b = A x_true with
+x_true uniform[-1, 1] from a fixed seed.  Synthetic data generated in-process.
+
+One step = the hot path from the matrix values resident in HBM to x at backward
+error <= 1e-12: numerical factorization + 16-RHS solve (+ FP64 iterative
+refinement for the mixed-precision path).  Both paths are measured:
+  fp64  : FP64 factor (DMMA updates) + solve          -- the drop-in path
+  mixed : FP32 factor (tensor-core updates) + solve + FP64 CG refinement
+``value`` is the numfact-equivalent throughput of the faster path that meets the
+accuracy target: PaStiX's theoretical flop count (DPARM_FACT_THFLOPS, SI) divided
+by that path's device time per step.
+
+``--impl reference`` times PaStiX's own CPU implementation (static scheduler on
+all host cores) on the same workload.
+"""
+from __future__ import annotations
+
+import argparse
+import json
+import os
+import subprocess
+import sys
+import threading
+import time
+
+import numpy as np
+
+REPO = os.path.dirname(os.path.abspath(__file__))
+sys.path.insert(0, REPO)
+os.environ.setdefault("OPENBLAS_NUM_THREADS", "1")
+
+METRIC = "numfact GFLOP/s & solve p50/p99 at bwd err ≤1e-12: mixed vs FP64, 1 B200"
+BERR_TARGET = 1e-12
+
+
+def parse():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=5)
+    ap.add_argument("--warmup", type=int, default=3)
+    ap.add_argument("--impl", default="b200", choices=["b200", "reference"])
+    ap.add_argument("--nx", type=int, default=80)
+    ap.add_argument("--points", type=int, default=27)
+    ap.add_argument("--nrhs", type=int, default=16)
+    ap.add_argument("--mixed", default="auto", help="precision of the mixed path (fp32, tf32, tf32x3; auto = best built)")
+    ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--cpu-budget", type=float, default=150.0, help="seconds of CPU time for the reference arm")
+    return ap.parse_args()
+
+
+def workload(args):
+    from pastix_b200 import matrices as M
+    shift = 1e-3 if args.points == 27 else 0.0
+    A = M.laplacian(args.nx, args.nx, args.nx, args.points, float(args.points - 1), shift=shift)
+    xt, b = M.rhs_from_xtrue(A, args.nrhs, seed=2024)
+    name = f"{args.points}-point 3D Laplacian {args.nx}^3 (n={A.n}), POTRF, {args.nrhs} RHS"
+    return A, xt, b, name
+
+
+def host_cores() -> int:
+    try:
+        return len(os.sched_getaffinity(0))
+    except Exception:
+        return os.cpu_count() or 1
+
+
+# ------------------------------------------------------------------ clocks
+
+class ClockSampler:
+    """nvidia-smi samples during the timed region (SM clock and throttle reasons)."""
+
+    Q = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
+         "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
+         "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+
+    def __init__(self, index: int):
+        self.index = index
+        self.rows = []
+        self.proc = None
+
+    def start(self):
+        try:
+            self.proc = subprocess.Popen(["nvidia-smi", f"--id={self.index}", f"--query-gpu={self.Q}",
+                                          "--format=csv,noheader,nounits", "-lms", "100"],
+                                         stdout=subprocess.PIPE, stderr=subprocess.DEVNULL, text=True)
+            self.thread = threading.Thread(target=self._read, daemon=True)
+            self.thread.start()
+        except Exception:
+            self.proc = None
+
+    def _read(self):
+        for line in self.proc.stdout:
+            parts = [p.strip() for p in line.split(",")]
+            if len(parts) >= 9:
+                self.rows.append(parts)
+
+    def stop(self) -> dict:
+        if self.proc is None:
+            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["nvidia-smi unavailable"]}
+        time.sleep(0.25)
+        self.proc.terminate()
+        try:
+            self.proc.wait(timeout=5)
+        except Exception:
+            self.proc.kill()
+        self.thread.join(timeout=2)
+        sm = [float(r[1]) for r in self.rows if r[1].replace(".", "").isdigit()]
+        mx = [float(r[2]) for r in self.rows if r[2].replace(".", "").isdigit()]
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        reasons = sorted({names[i] for r in self.rows for i in range(4) if r[5 + i].strip() == "Active"})
+        return {"sm_mhz": float(np.median(sm)) if sm else None, "sm_max_mhz": max(mx) if mx else None,
+                "reasons": reasons, "samples": len(self.rows)}
+
+
+# ------------------------------------------------------------------ peaks
+
+def measured_peaks():
+    try:
+        with open(os.path.join(REPO, "MEASURED_PEAKS.json")) as fh:
+            return json.load(fh)
+    except Exception:
+        return {}
+
+
+def gemm_peak_tflops(dtype: str) -> float:
+    """cuBLAS GEMM throughput on this GPU (best of a few 8192^3 products), the
+    denominator of the tensor roofline for FP64 (DGEMM) and TF32 updates."""
+    import torch
+    n = 8192 if dtype != "fp64" else 6144
+    torch.backends.cuda.matmul.allow_tf32 = dtype == "tf32"
+    dt = torch.float64 if dtype == "fp64" else torch.float32
+    a = torch.randn(n, n, device="cuda", dtype=dt)
+    b = torch.randn(n, n, device="cuda", dtype=dt)
+    for _ in range(2):
+        torch.matmul(a, b)
+    torch.cuda.synchronize()
+    best = 1e30
+    for _ in range(5):
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        e0.record()
+        torch.matmul(a, b)
+        e1.record()
+        e1.synchronize()
+        best = min(best, e0.elapsed_time(e1))
+    torch.backends.cuda.matmul.allow_tf32 = False
+    del a, b
+    torch.cuda.empty_cache()
+    return 2.0 * n ** 3 / (best * 1e-3) / 1e12
+
+
+def ncu_traffic(kernel: str):
+    """DRAM bytes per launch of a kernel from the committed ncu summary, if any."""
+    path = os.path.join(REPO, "profiles", "traffic.json")
+    try:
+        with open(path) as fh:
+            return json.load(fh).get(kernel)
+    except Exception:
+        return None
+
+
+# ------------------------------------------------------------------ reference (CPU) arm
+
+def run_reference(args, A, b, name, ncores, budget_s, steps, warmup):
+    """PaStiX's own CPU numfact + solve, static scheduler on all host cores."""
+    import oracle
+    from pastix_b200.refhost import Analysis
+    an = Analysis(A, "potrf", nthreads=ncores)
+    st = an.structure()
+    rd = oracle.RefDriver(an)
+    facts, solves = [], []
+    t_start = time.time()
+    done = 0
+    for it in range(warmup + steps):
+        rd.numfact(1)  # PastixSchedStatic
+        x = rd.solve(b)
+        s = rd.stats()
+        if it >= warmup:
+            facts.append(s["fact_time"])
+            solves.append(s["solve_time"])
+            done += 1
+        if time.time() - t_start > budget_s and done >= 1:
+            break
+    be = np.linalg.norm(b - A.matvec(x), axis=0) / np.linalg.norm(b, axis=0)
+    return dict(thflops=st.thflops, fact_times=facts, solve_times=solves, berr=float(be.max()), steps=done)
+
+
+# ------------------------------------------------------------------ B200 arm
+
+def run_path(solver, st, A, b, xt, prec, steps, warmup, stream, device_b, device_x, nrhs, refine):
+    """Timed steps on device-resident values: numfact + solve (+ refinement)."""
+    import torch
+    tfact, tsolve, tref, ttot, berrs, iters = [], [], [], [], [], []
+    n = A.n
+    launches0 = solver.stats()["kernel_launches"]
+    ev = lambda: torch.cuda.Event(enable_timing=True)
+    for it in range(warmup + steps):
+        if it == warmup:
+            launches0 = solver.stats()["kernel_launches"]
+        e0, e1, e2, e3 = ev(), ev(), ev(), ev()
+        with torch.cuda.stream(stream):
+            e0.record(stream)
+            solver.numfact(0.0)
+            e1.record(stream)
+            device_x.copy_(device_b)
+            solver.solve_device(device_x.data_ptr(), nrhs, n, stream.cuda_stream)
+            e2.record(stream)
+            nit = 0
+            if refine:
+                nit, be = solver.refine_device(device_b.data_ptr(), device_x.data_ptr(), nrhs, "cg", BERR_TARGET, 50,
+                                               25, stream.cuda_stream)
+            e3.record(stream)
+        e3.synchronize()
+        if it >= warmup:
+            tfact.append(e0.elapsed_time(e1))
+            tsolve.append(e1.elapsed_time(e2))
+            tref.append(e2.elapsed_time(e3))
+            ttot.append(e0.elapsed_time(e3))
+            iters.append(nit)
+    x = device_x.cpu().numpy().reshape(nrhs, n).T
+    berr = np.linalg.norm(b - A.matvec(x), axis=0) / np.linalg.norm(b, axis=0)
+    ferr = np.abs(x - xt).max(axis=0) / np.abs(xt).max(axis=0)
+    launches = solver.stats()["kernel_launches"] - launches0
+    return dict(prec=prec, numfact_ms=float(np.median(tfact)), solve_ms=float(np.median(tsolve)),
+                refine_ms=float(np.median(tref)), step_ms=float(np.median(ttot)), step_ms_all=ttot,
+                berr=float(berr.max()), ferr=float(ferr.max()), refine_iters=int(max(iters) if iters else 0),
+                numfact_gflops=st.thflops / (np.median(tfact) * 1e-3) / 1e9, launches=int(launches))
+
+
+def solve_latency(solver, A, b, stream, device_b, device_x, nrhs, reps=50):
+    """p50/p99 of the device time of one nrhs-column solve with the factor resident."""
+    import torch
+    ts = []
+    for i in range(reps):
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        with torch.cuda.stream(stream):
+            device_x.copy_(device_b)
+            e0.record(stream)
+            solver.solve_device(device_x.data_ptr(), nrhs, A.n, stream.cuda_stream)
+            e1.record(stream)
+        e1.synchronize()
+        ts.append(e0.elapsed_time(e1))
+    return float(np.percentile(ts, 50)), float(np.percentile(ts, 99))
+
+
+def e2e_path(solver, bc, A, b, prec, refine, nrhs, reps=3):
+    """The same step through the C ABI with host buffers: values uploaded,
+    factorization, solve of host b, refinement with host vectors."""
+    ts = []
+    for _ in range(reps):
+        t0 = time.perf_counter()
+        solver.bcsc_load(bc)
+        solver.numfact(0.0)
+        x = solver.solve(b)
+        if refine:
+            x, nit, be = solver.refine(b, x, "cg", BERR_TARGET, 50, 25)
+        ts.append(time.perf_counter() - t0)
+    h2d = bc.Lvalues.nbytes + (bc.Uvalues.nbytes if bc.Uvalues is not None else 0) + b.nbytes * (2 if refine else 1)
+    if refine:
+        h2d += b.nbytes  # initial x of the refinement
+    d2h = b.nbytes * (2 if refine else 1)
+    return float(np.median(ts)), int(h2d), int(d2h)
+
+
+def main():
+    args = parse()
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    rank = int(os.environ.get("RANK", "0"))
+    local_rank = int(os.environ.get("LOCAL_RANK", "0"))
+    ncores = host_cores()
+
+    if args.impl == "reference":
+        if rank != 0:
+            return 0
+        A, xt, b, name = workload(args)
+        steps = max(1, args.steps)
+        warm = min(args.warmup, 1)
+        r = run_reference(args, A, b, name, ncores, args.cpu_budget, steps, warm)
+        ft = float(np.median(r["fact_times"]))
+        val = r["thflops"] / ft / 1e9
+        line = {
+            "metric": METRIC, "value": val, "unit": "GFLOP/s", "n_gpus": args.gpus, "steps": r["steps"],
+            "warmup": warm, "ms_per_step": (ft + float(np.median(r["solve_times"]))) * 1e3,
+            "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f64",
+            "data": "synthetic", "impl": "reference",
+            "config": {"workload": name, "scheduler": "PaStiX static", "threads": ncores,
+                       "nrhs": args.nrhs, "l2": "inputs larger than L2"},
+            "cpu_baseline": {"value": val, "unit": "GFLOP/s", "cores": ncores, "kind": "reference",
+                             "sample": f"{r['steps']} numfact+solve of the full workload (PaStiX static scheduler)"},
+            "e2e": {"value": val, "unit": "GFLOP/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
+            "solve_ms": float(np.median(r["solve_times"])) * 1e3, "berr": r["berr"],
+        }
+        print(json.dumps(line), flush=True)
+        return 0
+
+    import torch
+    from pastix_b200 import native
+    from pastix_b200.refhost import Analysis
+
+    torch.cuda.set_device(local_rank)
+    dist = None
+    if world > 1:
+        import datetime
+        import torch.distributed as dist
+        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=600))
+
+    A, xt, b, name = workload(args)
+    an = Analysis(A, "potrf")
+    st = an.structure()
+    bc = an.bcsc()
+
+    # CPU baseline (reference PaStiX, all host cores), bounded sample: one factorization
+    cpu = None
+    if rank == 0 and not args.no_cpu_baseline:
+        try:
+            r = run_reference(args, A, b, name, ncores, 30.0, 1, 0)
+            cpu = {"value": r["thflops"] / r["fact_times"][0] / 1e9, "unit": "GFLOP/s", "cores": ncores,
+                   "kind": "reference",
+                   "sample": "one PaStiX numfact of the full workload, static scheduler, all host cores"}
+        except Exception as exc:  # the reference library is built where the PaStiX sources are
+            cpu = {"value": None, "unit": "GFLOP/s", "cores": ncores, "kind": "reference",
+                   "sample": f"unavailable: {exc}"}
+
+    mixed_prec = args.mixed
+    if mixed_prec == "auto":
+        mixed_prec = os.environ.get("B200_MIXED", "fp32")
+
+    stream = torch.cuda.Stream()
+    nrhs, n = args.nrhs, A.n
+    device_b = torch.from_numpy(np.ascontiguousarray(b.T)).cuda()  # column-major n x nrhs
+    device_x = torch.empty_like(device_b)
+    results = {}
+    traces = {}
+    solvers = {}
+    for prec, refine in (("fp64", False), (mixed_prec, True)):
+        s = native.Solver(st, "potrf", prec, stream=stream.cuda_stream)
+        s.bcsc_load(bc)
+        solvers[prec] = (s, refine)
+        traces[prec] = s.numfact_trace(0.0)
+
+    clk = ClockSampler(torch.cuda.current_device())
+    if dist is not None:
+        dist.barrier()
+    torch.cuda.synchronize()
+    clk.start()
+    t_wall0 = time.perf_counter()
+    for prec, (s, refine) in solvers.items():
+        results[prec] = run_path(s, st, A, b, xt, prec, args.steps, args.warmup, stream, device_b, device_x, nrhs,
+                                 refine)
+    torch.cuda.synchronize()
+    if dist is not None:
+        dist.barrier()
+    wall = time.perf_counter() - t_wall0
+    clocks = clk.stop()
+
+    ok = {p: r for p, r in results.items() if r["berr"] <= BERR_TARGET}
+    head = min(ok.values(), key=lambda r: r["step_ms"]) if ok else results["fp64"]
+    step_ms = head["step_ms"]
+    if dist is not None:
+        t = torch.tensor([step_ms], device="cuda", dtype=torch.float64)
+        dist.all_reduce(t, op=dist.ReduceOp.MAX)
+        step_ms = float(t.item())
+    value = world * st.thflops / (step_ms * 1e-3) / 1e9
+
+    hs, _ = solvers[head["prec"]]
+    p50, p99 = solve_latency(hs, A, b, stream, device_b, device_x, nrhs)
+    e2e_s, h2d, d2h = e2e_path(hs, bc, A, b, head["prec"], head["prec"] != "fp64", nrhs)
+    e2e_value = world * st.thflops / e2e_s / 1e9
+
+    # roofline of the dominant kernel (the GEMM-scatter update) of the headline path
+    tr = traces[head["prec"]]
+    upd = tr["update"]
+    peak_dtype = "fp64" if head["prec"] == "fp64" else ("tf32" if head["prec"].startswith("tf32") else "fp32")
+    try:
+        peak = gemm_peak_tflops(peak_dtype)
+    except Exception:
+        peak = None
+    achieved = upd["flops"] / (upd["ms"] * 1e-3) / 1e12 if upd["ms"] > 0 else 0.0
+    kname = "update_f64_kernel" if head["prec"] == "fp64" else "update_kernel_" + head["prec"]
+    roofline = {"bound": "tensor", "achieved": achieved, "peak": peak, "unit": "TFLOP/s",
+                "frac": (achieved / peak) if peak else None, "traffic": ncu_traffic(kname),
+                "kernel": kname,
+                "peak_source": f"measured cuBLAS {peak_dtype.upper()} GEMM on this GPU (bench.py)",
+                "share_of_numfact": upd["ms"] / max(sum(v["ms"] for v in tr.values()), 1e-9)}
+
+    if rank == 0:
+        line = {
+            "metric": METRIC, "value": value, "unit": "GFLOP/s", "n_gpus": world, "steps": args.steps,
+            "warmup": args.warmup, "ms_per_step": step_ms, "higher_is_better": True,
+            "scaling": "weak", "vs_baseline": None,
+            "dtype": "f64" if head["prec"] == "fp64" else "f32+f64",
+            "data": "synthetic",
+            "config": {"workload": name, "parallelism": "replicas" if world > 1 else "single GPU",
+                       "headline_path": head["prec"], "nrhs": nrhs, "berr_target": BERR_TARGET,
+                       "l2": f"inputs larger than L2 (factor {st.coefnbr * 8 / 1e9:.2f} GB FP64)",
+                       "thflops": st.thflops, "cblknbr": st.cblknbr, "bloknbr": st.bloknbr},
+            "paths": results,
+            "speedup_mixed_vs_fp64": (results["fp64"]["step_ms"] / results[mixed_prec]["step_ms"]),
+            "solve_latency_ms": {"p50": p50, "p99": p99, "nrhs": nrhs, "path": head["prec"]},
+            "numfact_trace": traces,
+            "roofline": roofline,
+            "cpu_baseline": cpu,
+            "e2e": {"value": e2e_value, "unit": "GFLOP/s", "h2d_bytes_per_step": h2d, "d2h_bytes_per_step": d2h,
+                    "seconds_per_step": e2e_s},
+            "gpu_launches": int(sum(r["launches"] for r in results.values())),
+            "clocks": clocks,
+            "wall_s_timed_region": wall,
+            "measured_peaks": {k: measured_peaks().get(k) for k in ("hbm_gbs", "bf16_tflops")},
+        }
+        for r in results.values():
+            r.pop("step_ms_all", None)
+        print(json.dumps(line), flush=True)
+    for s, _ in solvers.values():
+        s.close()
+    if dist is not None:
+        dist.barrier()
+        dist.destroy_process_group()
+    return 0
+
+
+if __name__ == "__main__":
+    sys.exit(main())

@@ -87,6 +87,15 @@ int b200_bcsc_load( b200_solver_t *solver, int64_t nnz, const int64_t *colptr,
  * Returns 6 (PASTIX_ERR_INTERNAL) on a negative pivot in a Cholesky. */
 int b200_numfact( b200_solver_t *solver, double epsilon_magn_ctrl, int64_t *nbpivots );
 
+/* Per-kernel timing of one factorization, the counterpart of PaStiX's kernel
+ * tracing and flop accounting (kernels/kernels_trace.h:206-300).  Runs
+ * b200_numfact once through the CUDA graph, then once more kernel by kernel
+ * with CUDA events.  ms[4] receives the device time of each kernel class
+ * (0: arena clear + bcsc scatter, 1: diagonal blocks, 2: panel TRSM,
+ * 3: GEMM-scatter updates); flops[4] (may be NULL) their algorithmic flops
+ * (diagonal n^3/3, TRSM m n^2, updates 2 M N K; doubled for LU). */
+int b200_numfact_trace( b200_solver_t *solver, double epsilon_magn_ctrl, double *ms, double *flops );
+
 /* pastix_task_solve (sopalin/pastix_task_solve.c:550): b (n x nrhs, column
  * major, leading dimension ldb, original ordering, host memory) is overwritten
  * with x. */
@@ -126,7 +135,8 @@ int b200_factor_download( b200_solver_t *solver, double *L, double *U );
 /* Statistics of the last calls: out[0] numfact ms, out[1] solve ms, out[2]
  * refine ms, out[3] static pivots, out[4] diag threshold used, out[5] device
  * bytes held, out[6] number of etree levels, out[7] kernel launches of the last
- * numfact, out[8] kernel launches of the last solve, out[9] coefnbr. */
+ * numfact, out[8] kernel launches of the last solve, out[9] coefnbr, out[10]
+ * kernels run by this instance so far.  out holds 11 entries. */
 int b200_stats( b200_solver_t *solver, double *out );
 
 /* Short description of a return code. */

@@ -84,6 +84,8 @@ struct b200_solver_s {
     int nmax_all = 0;
     int64_t total_tiles = 0;
     int trsm_smem = 0;                  // dynamic shared memory available to the panel TRSM
+    double flops_class[4] = {0, 0, 0, 0};  // algorithmic flops per kernel class (see Trace)
+    double bytes_scatter = 0;
 
     // bcsc
     int64_t nnz = -1;
@@ -112,6 +114,7 @@ struct b200_solver_s {
 
     double t_fact = 0, t_solve = 0, t_refine = 0;
     int launches_fact = 0, launches_solve = 0;
+    long long kernel_launches = 0;      // kernels this instance has run (graph replays included)
     cudaEvent_t ev0 = nullptr, ev1 = nullptr;
 
     template <typename T>
@@ -198,6 +201,9 @@ int build_schedule(b200_solver_t *s) {
             const int k = lvl_cblk[i];
             const int nc = s->ncols[k];
             flops += (int64_t)nc * nc * nc / 3;
+            const double m = (double)(s->stride[k] - nc);
+            s->flops_class[1] += (s->facto == FACTO_GETRF ? 2.0 : 1.0) * nc * (double)nc * nc / 3.0;
+            s->flops_class[2] += (s->facto == FACTO_GETRF ? 2.0 : 1.0) * m * nc * nc;
             for (int j = s->fblok[k] + 1; j < s->fblok[k + 1]; j++) {
                 const int f = s->fcblk[j];
                 const int atomic = src_count[f] > 1 ? UPD_ATOMIC : 0;
@@ -229,7 +235,11 @@ int build_schedule(b200_solver_t *s) {
                                                        : u.tiles_n * u.tiles_m;
                     u.tile0 = tile0;
                     tile0 += nt;
-                    flops += 2LL * u.M * u.N * u.K;
+                    // useful work: the lower triangle of the diagonal square for symmetric updates
+                    const double mn = (u.flags & UPD_SYM) ? (double)u.N * (u.M - u.N) + 0.5 * u.N * (u.N + 1.0)
+                                                          : (double)u.M * u.N;
+                    flops += (int64_t)(2.0 * mn * u.K);
+                    s->flops_class[3] += 2.0 * mn * u.K;
                     upds.push_back(u);
                 }
             }
@@ -278,21 +288,58 @@ int ensure_scal(b200_solver_t *s, int count) {
 
 // ---------------------------------------------------------------- numfact
 
+// Per-kernel-class timing of one factorization (kernels_trace,
+// kernels/kernels_trace.h:206-300): class 0 arena clear + bcsc scatter, 1 diagonal
+// blocks, 2 panel TRSM, 3 GEMM-scatter updates.
+struct Trace {
+    std::vector<std::pair<cudaEvent_t, cudaEvent_t>> ev[4];
+    cudaEvent_t open = nullptr;
+    void begin(cudaStream_t st) {
+        cudaEventCreate(&open);
+        cudaEventRecord(open, st);
+    }
+    void end(int cls, cudaStream_t st) {
+        cudaEvent_t e;
+        cudaEventCreate(&e);
+        cudaEventRecord(e, st);
+        ev[cls].push_back({open, e});
+        open = nullptr;
+    }
+    void finish(double *ms) {
+        for (int c = 0; c < 4; c++) {
+            ms[c] = 0;
+            for (auto &pr : ev[c]) {
+                float t = 0;
+                cudaEventElapsedTime(&t, pr.first, pr.second);
+                ms[c] += t;
+                cudaEventDestroy(pr.first);
+                cudaEventDestroy(pr.second);
+            }
+            ev[c].clear();
+        }
+    }
+};
+
 template <typename T>
-int enqueue_numfact(b200_solver_t *s, cudaStream_t st) {
+int enqueue_numfact(b200_solver_t *s, cudaStream_t st, Trace *tr = nullptr) {
     T *L = (T *)s->dL, *U = (T *)s->dU;
     int launches = 0;
+    if (tr) tr->begin(st);
     CU(cudaMemsetAsync(L, 0, s->arena * sizeof(T), st));
     if (U) CU(cudaMemsetAsync(U, 0, s->arena * sizeof(T), st));
     CU(cudaMemsetAsync(s->d_npiv, 0, sizeof(unsigned long long), st));
     CU(cudaMemsetAsync(s->d_err, 0, sizeof(int), st));
     launch_scatter<T>(s->nnz, s->d_dest, s->d_Lv, s->d_Uv, L, U, st);
+    if (tr) tr->end(0, st);
     launches++;
     for (size_t l = 0; l < s->levels.size(); l++) {
         const Level &Lv = s->levels[l];
+        if (tr) tr->begin(st);
         launch_diag<T>(s->facto, s->ds, s->d_lvl_cblk + Lv.c0, Lv.c1 - Lv.c0, L, U, s->d_thr, s->d_npiv, s->d_err, st);
+        if (tr) tr->end(1, st);
         launches++;
         const int nt = Lv.t1 - Lv.t0;
+        if (tr) tr->begin(st);
         if (nt > 0) {
             const int TR = s->lvl_tr[l];
             if (s->facto == FACTO_POTRF) {
@@ -306,6 +353,8 @@ int enqueue_numfact(b200_solver_t *s, cudaStream_t st) {
             }
             launches++;
         }
+        if (tr) tr->end(2, st);
+        if (tr) tr->begin(st);
         if (Lv.ntiles > 0) {
             if (sizeof(T) == 8)
                 launch_update_f64(s->ds, s->d_upd + Lv.u0, Lv.u1 - Lv.u0, Lv.ntiles, (double *)L, (double *)U, st);
@@ -313,6 +362,7 @@ int enqueue_numfact(b200_solver_t *s, cudaStream_t st) {
                 launch_update_f32(s->ds, s->d_upd + Lv.u0, Lv.u1 - Lv.u0, Lv.ntiles, (float *)L, (float *)U, st);
             launches++;
         }
+        if (tr) tr->end(3, st);
     }
     CU(cudaGetLastError());
     s->launches_fact = launches;
@@ -368,6 +418,7 @@ int solve_device(b200_solver_t *s, int nrhs, double *b, int64_t ldb, cudaStream_
     launch_permute(n, nrhs, s->d_peri, xp, n, b, ldb, 0, st);
     CU(cudaGetLastError());
     s->launches_solve = launches;
+    s->kernel_launches += launches;
     return ERR_SUCCESS;
 }
 
@@ -381,15 +432,21 @@ struct RefineCtx {
     int spmv(const double *x, double *y, double alpha, double beta) {
         const double *vals = (s->facto == FACTO_GETRF) ? s->d_Uv : s->d_Lv;
         launch_spmv(n, nrhs, s->d_colptr, s->d_rowtab, vals, x, n, y, n, alpha, beta, st);
+        s->kernel_launches++;
         return ERR_SUCCESS;
     }
     // z <- M^{-1} z with the factor (sweeps only, already permuted)
     int spsv(double *z) {
         int l = 0;
-        return sweeps(s, z, n, nrhs, st, &l);
+        int rc = sweeps(s, z, n, nrhs, st, &l);
+        s->kernel_launches += l;
+        return rc;
     }
+    // one BLAS-1 kernel launched by the caller
+    void count(int k = 1) { s->kernel_launches += k; }
     int dots(const double *x, const double *y, std::vector<double> &out) {
         launch_dots(n, nrhs, x, n, y, n, s->d_scal, st);
+        s->kernel_launches++;
         out.resize(nrhs);
         CU(cudaMemcpyAsync(out.data(), s->d_scal, nrhs * sizeof(double), cudaMemcpyDeviceToHost, st));
         CU(cudaStreamSynchronize(st));
@@ -417,6 +474,7 @@ int refine_sr(RefineCtx &c, const double *b, double *x, int itermax, double eps,
     berr.assign(R, 0.0);
     while (any) {
         launch_copy(n, R, b, n, r, n, c.st);
+        c.count();
         RET(c.spmv(x, r, -1.0, 1.0));
         RET(c.dots(r, r, nr));
         any = false;
@@ -434,9 +492,11 @@ int refine_sr(RefineCtx &c, const double *b, double *x, int itermax, double eps,
         }
         if (!any) break;
         launch_copy(n, R, r, n, dx, n, c.st);
+        c.count();
         RET(c.spsv(dx));
         RET(c.set_scal(mask, 0));
         launch_axpys(n, R, c.scal(0), 1.0, dx, n, x, n, c.st);
+        c.count();
         iter++;
     }
     *niter = iter;
@@ -454,6 +514,7 @@ int refine_cg(RefineCtx &c, const double *b, double *x, int itermax, double eps,
     RET(c.dots(x, x, nx));
     for (auto &v : nb) v = std::sqrt(v);
     launch_copy(n, R, b, n, gr, n, c.st);
+    c.count();
     RET(c.spmv(x, gr, -1.0, 1.0));
     RET(c.dots(gr, gr, nr));
     std::vector<double> resid(R), active(R, 1.0);
@@ -463,8 +524,10 @@ int refine_cg(RefineCtx &c, const double *b, double *x, int itermax, double eps,
         if (resid[j] > eps) any = true; else active[j] = 0.0;
     }
     launch_copy(n, R, gr, n, gz, n, c.st);
+    c.count();
     RET(c.spsv(gz));
     launch_copy(n, R, gz, n, gp, n, c.st);
+    c.count();
     int iter = 0;
     while (any && iter < itermax) {
         iter++;
@@ -474,13 +537,17 @@ int refine_cg(RefineCtx &c, const double *b, double *x, int itermax, double eps,
         for (int j = 0; j < R; j++) alpha[j] = (active[j] != 0.0 && alpha[j] != 0.0) ? beta[j] / alpha[j] : 0.0;
         RET(c.set_scal(alpha, 0));
         launch_axpys(n, R, c.scal(0), 1.0, gp, n, x, n, c.st);
+        c.count();
         launch_axpys(n, R, c.scal(0), -1.0, g2, n, gr, n, c.st);
+        c.count();
         launch_copy(n, R, gr, n, gz, n, c.st);
+        c.count();
         RET(c.spsv(gz));
         RET(c.dots(gr, gz, tmp));
         for (int j = 0; j < R; j++) tmp[j] = (beta[j] != 0.0) ? tmp[j] / beta[j] : 0.0;
         RET(c.set_scal(tmp, 1));
         launch_xpbys(n, R, gz, n, c.scal(1), gp, n, c.st);
+        c.count();
         RET(c.dots(gr, gr, nr));
         any = false;
         for (int j = 0; j < R; j++) {
@@ -516,6 +583,7 @@ int refine_gmres(RefineCtx &c, const double *b, double *x, int itermax, int im, 
     bool outer = true;
     while (outer) {
         launch_copy(n, R, b, n, V, n, c.st);
+        c.count();
         RET(c.spmv(x, V, -1.0, 1.0));
         RET(c.dots(V, V, nr));
         bool any = false;
@@ -533,12 +601,14 @@ int refine_gmres(RefineCtx &c, const double *b, double *x, int itermax, int im, 
         if (!any) break;
         RET(c.set_scal(inv, 0));
         launch_scal_cols(n, R, c.scal(0), V, n, V, n, c.st);
+        c.count();
         int i = -1;
         bool inner = true;
         while (inner) {
             i++;
             double *Vi = V + (size_t)i * blk, *Wi = W + (size_t)i * blk, *Vn = V + (size_t)(i + 1) * blk;
             launch_copy(n, R, Vi, n, Wi, n, c.st);
+            c.count();
             RET(c.spsv(Wi));
             RET(c.spmv(Wi, Vn, 1.0, 0.0));
             for (int jj = 0; jj <= i; jj++) {
@@ -546,6 +616,7 @@ int refine_gmres(RefineCtx &c, const double *b, double *x, int itermax, int im, 
                 for (int j = 0; j < R; j++) H[j][(size_t)i * im1 + jj] = h[j];
                 RET(c.set_scal(h, 0));
                 launch_axpys(n, R, c.scal(0), -1.0, V + (size_t)jj * blk, n, Vn, n, c.st);
+                c.count();
             }
             RET(c.dots(Vn, Vn, nr));
             std::vector<double> sc(R, 1.0);
@@ -570,6 +641,7 @@ int refine_gmres(RefineCtx &c, const double *b, double *x, int itermax, int im, 
             }
             RET(c.set_scal(sc, 0));
             launch_scal_cols(n, R, c.scal(0), Vn, n, Vn, n, c.st);
+            c.count();
             iters++;
             bool all_conv = true;
             for (int j = 0; j < R; j++)
@@ -591,6 +663,7 @@ int refine_gmres(RefineCtx &c, const double *b, double *x, int itermax, int im, 
             for (int j = 0; j < R; j++) y[j] = G[j][q];
             RET(c.set_scal(y, 0));
             launch_axpys(n, R, c.scal(0), 1.0, W + (size_t)q * blk, n, x, n, c.st);
+            c.count();
         }
         if (iters >= itermax) outer = false;
     }
@@ -613,6 +686,7 @@ int refine_device(b200_solver_t *s, int nrhs, const double *b, int64_t ldb, doub
     double *bp = s->d_ws, *xp = s->d_ws + blk;
     launch_permute(n, nrhs, s->d_peri, b, ldb, bp, n, 1, st);
     launch_permute(n, nrhs, s->d_peri, x, ldx, xp, n, 1, st);
+    s->kernel_launches += 3;
     RefineCtx c{s, st, n, nrhs};
     std::vector<double> be;
     int64_t it = 0;
@@ -863,6 +937,7 @@ int b200_numfact(b200_solver_t *s, double epsilon_magn_ctrl, int64_t *nbpivots) 
     }
     CU(cudaEventRecord(s->ev0, s->st));
     CU(cudaGraphLaunch(s->fact_graph, s->st));
+    s->kernel_launches += s->launches_fact;
     CU(cudaEventRecord(s->ev1, s->st));
     unsigned long long piv = 0;
     int err = 0;
@@ -879,6 +954,23 @@ int b200_numfact(b200_solver_t *s, double epsilon_magn_ctrl, int64_t *nbpivots) 
         return ERR_INTERNAL;
     }
     s->factored = true;
+    return ERR_SUCCESS;
+}
+
+int b200_numfact_trace(b200_solver_t *s, double epsilon_magn_ctrl, double *ms, double *flops) {
+    if (!s || s->nnz < 0 || !ms) return ERR_BADPARAM;
+    int64_t piv = 0;
+    RET(b200_numfact(s, epsilon_magn_ctrl, &piv));  // sets the threshold and checks the factorization
+    Trace tr;
+    int rc = s->f32 ? enqueue_numfact<float>(s, s->st, &tr) : enqueue_numfact<double>(s, s->st, &tr);
+    if (rc) return rc;
+    CU(cudaStreamSynchronize(s->st));
+    s->kernel_launches += s->launches_fact;
+    tr.finish(ms);
+    if (flops) {
+        flops[0] = 0.0;
+        for (int c = 1; c < 4; c++) flops[c] = s->flops_class[c];
+    }
     return ERR_SUCCESS;
 }
 
@@ -1015,6 +1107,7 @@ int b200_stats(b200_solver_t *s, double *out) {
     out[7] = s->launches_fact;
     out[8] = s->launches_solve;
     out[9] = (double)s->coefnbr;
+    out[10] = (double)s->kernel_launches;
     return ERR_SUCCESS;
 }
 

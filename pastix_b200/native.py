@@ -23,7 +23,8 @@ _I64 = C.c_int64
 _lib = None
 
 # exported symbols, in the order of include/pastix_b200.h
-SYMBOLS = ["b200_solver_create", "b200_solver_destroy", "b200_bcsc_load", "b200_numfact", "b200_solve",
+SYMBOLS = ["b200_solver_create", "b200_solver_destroy", "b200_bcsc_load", "b200_numfact", "b200_numfact_trace",
+           "b200_solve",
            "b200_solve_device", "b200_refine", "b200_refine_device", "b200_spmv", "b200_factor_download",
            "b200_stats", "b200_strerror"]
 
@@ -49,6 +50,7 @@ def lib():
         L.b200_solver_destroy.argtypes = [_P]
         L.b200_bcsc_load.argtypes = [_P, _I64, _P, _P, _P, _P, C.c_double]
         L.b200_numfact.argtypes = [_P, C.c_double, C.POINTER(_I64)]
+        L.b200_numfact_trace.argtypes = [_P, C.c_double, _P, _P]
         L.b200_solve.argtypes = [_P, _I64, _P, _I64]
         L.b200_solve_device.argtypes = [_P, _I64, _P, _I64, _P]
         L.b200_refine.argtypes = [_P, _I64, _P, _I64, _P, _I64, C.c_int, C.c_double, _I64, _I64,
@@ -116,6 +118,14 @@ class Solver:
         check(lib().b200_numfact(self.h, epsilon_magn_ctrl, C.byref(piv)), "b200_numfact")
         return int(piv.value)
 
+    def numfact_trace(self, epsilon_magn_ctrl: float = 0.0) -> dict:
+        """Device time (ms) and algorithmic flops per kernel class of one factorization."""
+        ms = np.zeros(4)
+        fl = np.zeros(4)
+        check(lib().b200_numfact_trace(self.h, epsilon_magn_ctrl, _p(ms), _p(fl)), "b200_numfact_trace")
+        names = ["scatter", "diag", "trsm", "update"]
+        return {n: dict(ms=float(ms[i]), flops=float(fl[i])) for i, n in enumerate(names)}
+
     def solve(self, b: np.ndarray) -> np.ndarray:
         x = np.asfortranarray(np.array(b, dtype=np.float64).reshape(self.n, -1))
         check(lib().b200_solve(self.h, x.shape[1], _p(x), self.n), "b200_solve")
@@ -159,8 +169,8 @@ class Solver:
         return L, U
 
     def stats(self) -> dict:
-        out = np.zeros(10)
+        out = np.zeros(11)
         check(lib().b200_stats(self.h, _p(out)), "b200_stats")
         return dict(numfact_ms=out[0], solve_ms=out[1], refine_ms=out[2], nbpivots=int(out[3]), threshold=out[4],
                     device_bytes=int(out[5]), levels=int(out[6]), launches_numfact=int(out[7]),
-                    launches_solve=int(out[8]), coefnbr=int(out[9]))
+                    launches_solve=int(out[8]), coefnbr=int(out[9]), kernel_launches=int(out[10]))

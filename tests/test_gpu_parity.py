@@ -1,0 +1,243 @@
+"""GPU parity of the B200 factorization and solves, through the C ABI.
+
+Factors are compared with PaStiX's own factor (golden fixtures) and with the
+oracle restatement on the same analysis; the bar for the FP64 path is a factor
+relative Frobenius difference <= 1e-12 (masked as PaStiX's factors are: lower
+triangle of diagonal blocks for POTRF, strict lower + D for SYTRF, everything for
+LU) and a backward error ||b - A x||_2 / ||b||_2 <= 1e-13.  The FP32-factor paths
+must reach a backward error <= 1e-12 after FP64 refinement.
+"""
+import numpy as np
+import pytest
+
+import oracle
+from golden_util import load, names
+from pastix_b200 import matrices as M
+from pastix_b200 import native
+from pastix_b200.api import PastixB200, backward_error, forward_error
+from pastix_b200.refhost import Analysis
+
+pytestmark = pytest.mark.gpu
+
+FACTOR_TOL = 1e-12
+BERR_FP64 = 1e-13
+BERR_TARGET = 1e-12
+
+
+def factor_diff(orc, facto, Lg, Ug, L, U):
+    mask = orc.factor_mask(facto)
+    d = np.linalg.norm((Lg - L)[mask]) / np.linalg.norm(L[mask])
+    if U is not None:
+        d = max(d, np.linalg.norm(Ug - U) / np.linalg.norm(U))
+    return d
+
+
+def oracle_factor(st, bc, facto, thr):
+    orc = oracle.Oracle(st)
+    L, U = orc.fillin(bc)
+    piv = orc.numfact(facto, L, U, thr)
+    return orc, L, U, piv
+
+
+@pytest.mark.parametrize("name", names())
+def test_factor_and_solve_match_pastix_golden(name):
+    A, st, bc, d = load(name)
+    facto = int(d["facto"])
+    s = native.Solver(st, facto, "fp64")
+    s.bcsc_load(bc)
+    piv = s.numfact(0.0)
+    assert piv == int(d["nbpivots"])
+    assert abs(s.stats()["threshold"] - float(d["threshold"])) <= 1e-15 * float(d["threshold"])
+    Lg, Ug = s.factor()
+    orc = oracle.Oracle(st)
+    assert factor_diff(orc, facto, Lg, Ug, d["L"], d.get("U")) <= FACTOR_TOL
+    x = s.solve(d["b"])
+    assert np.linalg.norm(x - d["x"]) / np.linalg.norm(d["x"]) <= 1e-12
+    assert backward_error(A, x, d["b"]).max() <= BERR_FP64
+    s.close()
+
+
+CASES = [
+    ("potrf", lambda: M.laplacian(20, 20, 20, 7, 6.0)),          # config 1 (n = 8000)
+    ("potrf", lambda: M.laplacian(12, 12, 12, 27, 26.0, shift=1e-3)),
+    ("getrf", lambda: M.convection_diffusion(16, 16, 16, seed=4)),
+    ("sytrf", lambda: M.shifted_laplacian_2d(40, 0.8)),
+    ("potrf", lambda: M.laplacian(30, 7, 5, 7, 6.0)),             # ragged grid
+    ("getrf", lambda: M.convection_diffusion(3, 2, 2, seed=1)),   # tiny: 12 unknowns
+]
+
+
+@pytest.mark.parametrize("facto,make", CASES)
+def test_fp64_factor_matches_oracle(facto, make):
+    A = make()
+    an = Analysis(A, facto)
+    st = an.structure()
+    bc = an.bcsc()
+    s = native.Solver(st, facto, "fp64")
+    s.bcsc_load(bc)
+    piv = s.numfact(0.0)
+    thr = s.stats()["threshold"]
+    orc, L, U, opiv = oracle_factor(st, bc, an.facto, thr)
+    assert piv == opiv
+    Lg, Ug = s.factor()
+    assert factor_diff(orc, an.facto, Lg, Ug, L, U) <= FACTOR_TOL
+    xt, b = M.rhs_from_xtrue(A, 3, seed=9)
+    x = s.solve(b)
+    xo = orc.solve(an.facto, L, U, b)
+    assert np.linalg.norm(x - xo) / np.linalg.norm(xo) <= 1e-12
+    assert backward_error(A, x, b).max() <= BERR_FP64
+    s.close()
+
+
+@pytest.mark.parametrize("facto,make,method", [
+    ("potrf", lambda: M.laplacian(20, 20, 20, 27, 26.0, shift=1e-3), "cg"),
+    ("potrf", lambda: M.laplacian(20, 20, 20, 7, 6.0), "sr"),
+    ("getrf", lambda: M.convection_diffusion(16, 16, 16, seed=5), "gmres"),
+    ("sytrf", lambda: M.shifted_laplacian_2d(40, 0.8), "gmres"),
+])
+def test_fp32_factor_with_fp64_refinement(facto, make, method):
+    A = make()
+    p = PastixB200(iparm={"FACTORIZATION": facto, "PRECISION": "fp32", "REFINEMENT": method})
+    p.task_analyze(A)
+    p.task_numfact()
+    xt, b = M.rhs_from_xtrue(A, 4, seed=3)
+    x0 = p.task_solve(b)
+    assert backward_error(A, x0, b).max() < 1e-4  # an FP32 factor alone
+    x = p.task_refine(b, x0)
+    be = backward_error(A, x, b)
+    assert be.max() <= BERR_TARGET, (be, p.out)
+    assert forward_error(x, xt).max() <= 1e-8
+    p.close()
+
+
+def test_refactorization_same_pattern():
+    """Values change, pattern stays: re-load the bcsc values and factor again."""
+    A = M.laplacian(14, 14, 14, 7, 6.0)
+    an = Analysis(A, "potrf")
+    st = an.structure()
+    s = native.Solver(st, "potrf", "fp64")
+    s.bcsc_load(an.bcsc())
+    s.numfact(0.0)
+    rng = np.random.default_rng(0)
+    scale = rng.uniform(0.9, 1.1, A.n)
+    vals = A.values.copy()
+    cols = np.repeat(np.arange(A.n), np.diff(A.colptr))
+    diag = A.rowind == cols
+    vals[diag] *= scale[cols[diag]]
+    bc2 = an.bcsc(vals)
+    s.bcsc_load(bc2)
+    s.numfact(0.0)
+    orc, L, U, _ = oracle_factor(st, bc2, 0, s.stats()["threshold"])
+    Lg, _ = s.factor()
+    assert factor_diff(orc, 0, Lg, None, L, None) <= FACTOR_TOL
+    A2 = M.CSC(A.n, A.colptr, A.rowind, vals, True, A.grid)
+    xt, b = M.rhs_from_xtrue(A2, 2, seed=1)
+    assert backward_error(A2, s.solve(b), b).max() <= BERR_FP64
+    s.close()
+
+
+def test_multi_rhs_columns_match_single_solves():
+    """Each column of a multi-RHS solve equals the one-column solve (within tolerance)."""
+    A = M.laplacian(16, 16, 16, 27, 26.0, shift=1e-3)
+    an = Analysis(A, "potrf")
+    s = native.Solver(an.structure(), "potrf", "fp64")
+    s.bcsc_load(an.bcsc())
+    s.numfact(0.0)
+    xt, b = M.rhs_from_xtrue(A, 37, seed=2)  # more than one pass of 16 columns
+    X = s.solve(b)
+    for j in (0, 15, 16, 36):
+        xj = s.solve(b[:, j:j + 1])
+        assert np.linalg.norm(X[:, j] - xj[:, 0]) / np.linalg.norm(xj) <= 1e-13
+    s.close()
+
+
+def test_spmv_matches_host():
+    A = M.convection_diffusion(9, 8, 7, seed=2)
+    an = Analysis(A, "getrf")
+    s = native.Solver(an.structure(), "getrf", "fp64")
+    s.bcsc_load(an.bcsc())
+    x = np.asfortranarray(np.random.default_rng(0).standard_normal((A.n, 3)))
+    y = s.spmv(x)
+    assert np.allclose(y, A.matvec(x), rtol=1e-13, atol=1e-13)
+    s.close()
+
+
+def test_negative_pivot_reports_error_and_context_survives():
+    """POTRF on an indefinite matrix returns PASTIX_ERR_INTERNAL; the instance and
+    the CUDA context stay usable."""
+    A = M.shifted_laplacian_2d(20, 3.0)
+    an = Analysis(A, "potrf")
+    s = native.Solver(an.structure(), "potrf", "fp64")
+    s.bcsc_load(an.bcsc())
+    with pytest.raises(native.B200Error):
+        s.numfact(0.0)
+    s.close()
+    A2 = M.laplacian(6, 6, 6, 7, 6.0)
+    an2 = Analysis(A2, "potrf")
+    s2 = native.Solver(an2.structure(), "potrf", "fp64")
+    s2.bcsc_load(an2.bcsc())
+    s2.numfact(0.0)
+    xt, b = M.rhs_from_xtrue(A2, 1, seed=0)
+    assert backward_error(A2, s2.solve(b), b).max() <= BERR_FP64
+    s2.close()
+
+
+def test_static_pivoting_counts_replacements():
+    """A threshold above some pivots replaces them (core_zgetf2sp) and counts them."""
+    A = M.convection_diffusion(8, 8, 8, seed=6)
+    an = Analysis(A, "getrf")
+    st = an.structure()
+    bc = an.bcsc()
+    # pick a threshold (|DPARM_EPSILON_MAGN_CTRL| < 0 form) that replaces some but not all pivots
+    thr = None
+    for cand in (7.0, 7.5, 8.0, 9.0, 10.0):
+        orc, L, U, opiv = oracle_factor(st, bc, 2, cand)
+        if 0 < opiv < A.n // 2:
+            thr = cand
+            break
+    assert thr is not None
+    s = native.Solver(st, "getrf", "fp64")
+    s.bcsc_load(bc)
+    piv = s.numfact(-thr)
+    assert piv == opiv
+    Lg, Ug = s.factor()
+    assert factor_diff(orc, 2, Lg, Ug, L, U) <= 1e-11
+    s.close()
+
+
+def test_bad_parameters():
+    A = M.laplacian(5, 5, 5, 7, 6.0)
+    an = Analysis(A, "potrf")
+    s = native.Solver(an.structure(), "potrf", "fp64")
+    with pytest.raises(native.B200Error):
+        s.numfact(0.0)  # no values loaded yet
+    s.bcsc_load(an.bcsc())
+    s.numfact(0.0)
+    assert native.lib().b200_solve(s.h, 1, None, 1) == 7  # ldb < n
+    x = s.solve(np.zeros((A.n, 0)))
+    assert x.shape == (A.n, 0)
+    s.close()
+
+
+def test_full_size_config2_backward_error():
+    """The 80^3 27-point Laplacian: FP64 factor reaches bwd err <= 1e-13, the FP32
+    factor with CG refinement <= 1e-12 (size-independent properties at full size)."""
+    A = M.laplacian(80, 80, 80, 27, 26.0, shift=1e-3)
+    an = Analysis(A, "potrf")
+    st = an.structure()
+    bc = an.bcsc()
+    xt, b = M.rhs_from_xtrue(A, 16, seed=2024)
+    s = native.Solver(st, "potrf", "fp64")
+    s.bcsc_load(bc)
+    s.numfact(0.0)
+    x = s.solve(b)
+    assert backward_error(A, x, b).max() <= BERR_FP64
+    s.close()
+    s = native.Solver(st, "potrf", "fp32")
+    s.bcsc_load(bc)
+    s.numfact(0.0)
+    x0 = s.solve(b)
+    x, nit, berr = s.refine(b, x0, "cg", BERR_TARGET, 50, 25)
+    assert backward_error(A, x, b).max() <= BERR_TARGET
+    assert forward_error(x, xt).max() <= 1e-9
+    s.close()

@@ -1,0 +1,51 @@
+"""PaStiX's host analysis run through refhost reproduces the committed structure
+bit-exactly, and the flop count of the 20^3 Laplacian."""
+import os
+
+import numpy as np
+import pytest
+
+from golden_util import FIELDS, load, names
+from pastix_b200 import matrices as M
+from pastix_b200 import refhost
+
+pytestmark = pytest.mark.skipif(not os.path.exists(refhost.LIBPATH), reason="PaStiX host library not built")
+
+
+@pytest.mark.parametrize("name", names())
+def test_analysis_reproduces_golden_structure(name):
+    A, st, bc, d = load(name)
+    facto = {0: "potrf", 1: "sytrf", 2: "getrf"}[int(d["facto"])]
+    an = refhost.Analysis(A, facto)
+    st2 = an.structure()
+    for f in FIELDS:
+        a, b = getattr(st2, f), getattr(st, f)
+        if f in ("cblk_brown2d", "cblk_type", "cblk_stride"):
+            a, b = a[:-1], b[:-1]  # PaStiX leaves these unset on the sentinel cblk
+        assert np.array_equal(a, b), f
+    bc2 = an.bcsc()
+    assert np.array_equal(bc2.colptr, bc.colptr) and np.array_equal(bc2.rowtab, bc.rowtab)
+    assert np.array_equal(bc2.Lvalues, bc.Lvalues)
+
+
+def test_thflops_20cube():
+    A = M.laplacian(20, 20, 20, 7, 6.0)
+    st = refhost.Analysis(A, "potrf").structure()
+    assert st.n == 8000
+    assert abs(st.thflops - 3.161e8) / 3.161e8 < 1e-3
+
+
+def test_structure_invariants():
+    A = M.convection_diffusion(10, 10, 10, seed=3)
+    st = refhost.Analysis(A, "getrf").structure()
+    nc = st.cblk_lcolnum[:-1] - st.cblk_fcolnum[:-1] + 1
+    rows = st.blok_lrownum[:-1] - st.blok_frownum[:-1] + 1
+    for k in range(st.cblknbr):
+        b0, b1 = st.cblk_fblok[k], st.cblk_fblok[k + 1]
+        assert st.blok_frownum[b0] == st.cblk_fcolnum[k] and st.blok_lrownum[b0] == st.cblk_lcolnum[k]
+        assert rows[b0:b1].sum() == st.cblk_stride[k]
+        assert np.all(st.blok_fcblknm[b0 + 1:b1] > k)
+        # 2D layout: coefind = rows above * ncols
+        assert np.array_equal(st.blok_coefind[b0:b1], np.concatenate([[0], np.cumsum(rows[b0:b1])[:-1]]) * nc[k])
+    assert np.array_equal(np.sort(st.permtab), np.arange(st.n))
+    assert np.array_equal(st.peritab[st.permtab], np.arange(st.n))
