@@ -105,6 +105,26 @@ int b200_solve( b200_solver_t *solver, int64_t nrhs, double *b, int64_t ldb );
  * not NULL). */
 int b200_solve_device( b200_solver_t *solver, int64_t nrhs, double *d_b, int64_t ldb, void *stream );
 
+/* Maximum n * nrhs of b200_solve_device_noalloc: 4,194,304 doubles (32 MiB). */
+#define B200_NOALLOC_SCRATCH_DOUBLES 4194304
+
+/* Solve on device memory without allocating anything.  It has no counterpart in
+ * PaStiX: it exists for callers that cannot call cudaMalloc when they solve --
+ * a request loop whose device memory is all reserved by a pool, code that must
+ * not trigger the implicit device synchronization of cudaMalloc/cudaFree, or a
+ * process that must keep a fixed footprint.  Same result as b200_solve_device.
+ * The permuted right-hand sides live in one fixed scratch array compiled into
+ * this library (B200_NOALLOC_SCRATCH_DOUBLES doubles), which every GPU that
+ * loads the library holds until the process exits; calls with
+ * n * nrhs > B200_NOALLOC_SCRATCH_DOUBLES are rejected with
+ * PASTIX_ERR_BADPARAMETER.  The first call on a device looks up the array's
+ * device address (cudaGetSymbolAddress), so make that first call before any
+ * stream capture.  All calls share the array: calls that overlap on the GPU
+ * (other streams, other solver instances, other host threads) race and must be
+ * serialized by the caller.  stream may be NULL (the solver's own stream). */
+int b200_solve_device_noalloc( b200_solver_t *solver, int64_t nrhs, double *d_b, int64_t ldb,
+                               void *stream );
+
 /* pastix_task_refine (refinement/pastix_task_refine.c:226): iterative
  * refinement in double of x (initial guess, overwritten) for A x = b, with the
  * factor as preconditioner.  method: B200_REFINE_*; eps: stopping tolerance on

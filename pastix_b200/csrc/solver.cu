@@ -7,6 +7,7 @@
 #include <cstdio>
 #include <cstring>
 #include <map>
+#include <mutex>
 #include <vector>
 
 #include "b200_internal.h"
@@ -705,6 +706,41 @@ int refine_device(b200_solver_t *s, int nrhs, const double *b, int64_t ldb, doub
 
 }  // namespace
 
+// ====================================================================== no-allocation solve
+
+// Scratch of b200_solve_device_noalloc: the permuted right-hand sides.  A
+// file-scope device array, so the entry point never allocates.  In host code
+// the name is only a host-side handle; its device address is looked up once per
+// device with cudaGetSymbolAddress and passed to the kernels.
+static __device__ __align__(256) double g_noalloc_scratch[B200_NOALLOC_SCRATCH_DOUBLES];
+
+namespace {
+constexpr int NOALLOC_MAX_DEVICES = 64;
+std::mutex g_noalloc_mutex;
+double *g_noalloc_addr[NOALLOC_MAX_DEVICES] = {};
+
+// Device address of the scratch array on the current device (looked up on the
+// first call on that device, with that device current).
+int noalloc_scratch(double **out) {
+    int dev = 0;
+    CU(cudaGetDevice(&dev));
+    if (dev < 0 || dev >= NOALLOC_MAX_DEVICES) return ERR_INTERNAL;
+    std::lock_guard<std::mutex> lock(g_noalloc_mutex);
+    if (g_noalloc_addr[dev] == nullptr) {
+        void *p = nullptr;
+        cudaError_t e = cudaGetSymbolAddress(&p, g_noalloc_scratch);
+        if (e != cudaSuccess || p == nullptr) {
+            fprintf(stderr, "pastix_b200: cudaGetSymbolAddress of the no-alloc scratch failed: %s\n",
+                    cudaGetErrorString(e));
+            return ERR_INTERNAL;
+        }
+        g_noalloc_addr[dev] = static_cast<double *>(p);
+    }
+    *out = g_noalloc_addr[dev];
+    return ERR_SUCCESS;
+}
+}  // namespace
+
 // ====================================================================== C ABI
 
 extern "C" {
@@ -979,6 +1015,29 @@ int b200_solve_device(b200_solver_t *s, int64_t nrhs, double *d_b, int64_t ldb, 
     if (nrhs == 0) return ERR_SUCCESS;
     cudaStream_t st = stream ? (cudaStream_t)stream : s->st;
     return solve_device(s, (int)nrhs, d_b, ldb, st);
+}
+
+int b200_solve_device_noalloc(b200_solver_t *s, int64_t nrhs, double *d_b, int64_t ldb, void *stream) {
+    if (!s || !s->factored || nrhs < 0 || ldb < s->n || (!d_b && nrhs)) return ERR_BADPARAM;
+    if (nrhs == 0) return ERR_SUCCESS;
+    const int n = s->n;
+    if ((uint64_t)n * (uint64_t)nrhs > (uint64_t)B200_NOALLOC_SCRATCH_DOUBLES) {
+        fprintf(stderr,
+                "pastix_b200: b200_solve_device_noalloc: n * nrhs = %lld exceeds its fixed scratch of %d doubles\n",
+                (long long)n * (long long)nrhs, B200_NOALLOC_SCRATCH_DOUBLES);
+        return ERR_BADPARAM;
+    }
+    double *xp = nullptr;
+    RET(noalloc_scratch(&xp));
+    cudaStream_t st = stream ? (cudaStream_t)stream : s->st;
+    // every entry of the scratch used here is written by the permutation before it is read
+    int launches = 2;
+    launch_permute(n, (int)nrhs, s->d_peri, d_b, ldb, xp, n, 1, st);
+    RET(sweeps(s, xp, n, (int)nrhs, st, &launches));
+    launch_permute(n, (int)nrhs, s->d_peri, xp, n, d_b, ldb, 0, st);
+    CU(cudaGetLastError());
+    s->kernel_launches += launches;
+    return ERR_SUCCESS;
 }
 
 int b200_solve(b200_solver_t *s, int64_t nrhs, double *b, int64_t ldb) {

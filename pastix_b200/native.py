@@ -25,7 +25,7 @@ _lib = None
 # exported symbols, in the order of include/pastix_b200.h
 SYMBOLS = ["b200_solver_create", "b200_solver_destroy", "b200_bcsc_load", "b200_numfact", "b200_numfact_trace",
            "b200_solve",
-           "b200_solve_device", "b200_refine", "b200_refine_device", "b200_spmv", "b200_factor_download",
+           "b200_solve_device", "b200_solve_device_noalloc", "b200_refine", "b200_refine_device", "b200_spmv", "b200_factor_download",
            "b200_stats", "b200_strerror"]
 
 
@@ -53,6 +53,7 @@ def lib():
         L.b200_numfact_trace.argtypes = [_P, C.c_double, _P, _P]
         L.b200_solve.argtypes = [_P, _I64, _P, _I64]
         L.b200_solve_device.argtypes = [_P, _I64, _P, _I64, _P]
+        L.b200_solve_device_noalloc.argtypes = [_P, _I64, _P, _I64, _P]
         L.b200_refine.argtypes = [_P, _I64, _P, _I64, _P, _I64, C.c_int, C.c_double, _I64, _I64,
                                   C.POINTER(_I64), _P]
         L.b200_refine_device.argtypes = [_P, _I64, _P, _I64, _P, _I64, C.c_int, C.c_double, _I64, _I64,
