@@ -101,11 +101,26 @@ int b200_numfact_trace( b200_solver_t *solver, double epsilon_magn_ctrl, double 
  * with x. */
 int b200_solve( b200_solver_t *solver, int64_t nrhs, double *b, int64_t ldb );
 
+/* Per-kernel timing of the triangular sweeps of one solve of nrhs zero
+ * right-hand sides (in the permuted basis, no permutation): ms[1] diagonal-block
+ * solves, ms[2] off-diagonal tiles (ms[0], ms[3] unused), with CUDA events around
+ * every launch; bytes[4] (may be NULL) the algorithmic traffic of each class
+ * (factor entries read once per sweep, vectors read and written). */
+int b200_solve_trace( b200_solver_t *solver, int64_t nrhs, double *ms, double *bytes );
+
+/* Per-launch device times of the last b200_numfact_trace / b200_solve_trace:
+ * ms[i] and cls[i] for the first min(cap, count) launches, grouped by kind in
+ * launch order within a kind.  Kinds: 0-3 the classes of the trace, 4 sub-panel
+ * diagonal tiles, 5 sub-panel TRSM, 6 sub-panel internal updates, 7 inverses of
+ * the diagonal blocks.  Returns the launch count (or a negative error code). */
+int64_t b200_trace_launches( b200_solver_t *solver, double *ms, int32_t *cls, int64_t cap );
+
 /* Same on device memory, asynchronously on the solver's stream (or on stream if
  * not NULL). */
 int b200_solve_device( b200_solver_t *solver, int64_t nrhs, double *d_b, int64_t ldb, void *stream );
 
-/* Maximum n * nrhs of b200_solve_device_noalloc: 4,194,304 doubles (32 MiB). */
+/* Size of the fixed scratch of b200_solve_device_noalloc: 4,194,304 doubles
+ * (32 MiB); a call needs 2 * n * nrhs of them. */
 #define B200_NOALLOC_SCRATCH_DOUBLES 4194304
 
 /* Solve on device memory without allocating anything.  It has no counterpart in
@@ -116,7 +131,7 @@ int b200_solve_device( b200_solver_t *solver, int64_t nrhs, double *d_b, int64_t
  * The permuted right-hand sides live in one fixed scratch array compiled into
  * this library (B200_NOALLOC_SCRATCH_DOUBLES doubles), which every GPU that
  * loads the library holds until the process exits; calls with
- * n * nrhs > B200_NOALLOC_SCRATCH_DOUBLES are rejected with
+ * 2 * n * nrhs > B200_NOALLOC_SCRATCH_DOUBLES are rejected with
  * PASTIX_ERR_BADPARAMETER.  The first call on a device looks up the array's
  * device address (cudaGetSymbolAddress), so make that first call before any
  * stream capture.  All calls share the array: calls that overlap on the GPU

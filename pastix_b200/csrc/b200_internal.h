@@ -51,6 +51,7 @@ enum : int {
 
 struct Upd {
     int k, j, f;
+    int colK0;    // first column of k in the K-range (0 except for sub-panel self-updates)
     int rowA0;    // panel row of k where the M-range starts
     int rowB0;    // panel row of k of block j
     int M, N, K;
@@ -64,6 +65,23 @@ struct Upd {
 struct RowTask {
     int k;
     int row0;  // first panel row of the tile (>= ncols_k)
+};
+
+// Off-diagonal tile of a cblk panel for the solves: 64 panel rows x 64 columns.
+struct SolveTile {
+    int k;
+    int row0;  // first panel row (>= ncols_k)
+    int col0;  // first column of the cblk
+};
+
+// Task of the sub-panel path for wide cblks: a 64-row tile of cblk k below the
+// 64-column sub-panel starting at column c0; pos is the cblk's slot in the step's
+// scratch of 64x64 inverses.
+struct SubTask {
+    int k;
+    int row0;
+    int c0;
+    int pos;
 };
 
 struct Level {

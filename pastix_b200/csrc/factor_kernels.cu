@@ -116,23 +116,139 @@ __device__ void factor_tile(T *t, int pb, int lane, double thr, int *piv, int *e
     }
 }
 
+// Inverse of the lower triangle of a pb x pb tile by one warp (lane = column of
+// the row being formed): W[i][i] = 1/T[i][i] (1 if unit), W[i][j] =
+// -(1/T[i][i]) sum_{j<=m<i} T[i][m] W[m][j], rows in order.  trans = 1 reads the
+// tile transposed (the lower triangle of T^T is the upper triangle of T).
+template <typename T>
+__device__ void invert_lower_tile(const T *t, T *w, int pb, int lane, int unit, int trans) {
+    for (int i = 0; i < 32; i++) {
+        if (lane <= i) {
+            const int j = lane;
+            T v = 0;
+            if (i < pb) {
+                const T dii = unit ? (T)1 : (trans ? t[i * TP + i] : t[i + i * TP]);
+                if (j == i) {
+                    v = (T)1 / dii;
+                } else {
+                    T acc = 0;
+                    for (int m = j; m < i; m++) acc += (trans ? t[m + i * TP] : t[i + m * TP]) * w[m + j * TP];
+                    v = -acc / dii;
+                }
+            }
+            w[i + j * TP] = v;
+        } else {
+            w[i + lane * TP] = 0;
+        }
+        __syncwarp();
+    }
+}
+
+// 32x32 output tile of a trailing update, computed by one warp:
+// C[i][j] -= sum_c X[i][c] * B(j, c) for c < pb, where X(i, c) = A[(r0+i) + (p+c) ld]
+// and B(j, c) = A[(c0+j) + (p+c) ld] (btrans = 0) or A[(p+c) + (c0+j) ld] (btrans = 1).
+__device__ __forceinline__ void dmma_tile(double (&c)[4], double a0, double a1, double b) {
+    asm volatile(
+        "mma.sync.aligned.m16n8k4.row.col.f64.f64.f64.f64 {%0,%1,%2,%3}, {%4,%5}, {%6}, {%0,%1,%2,%3};\n"
+        : "+d"(c[0]), "+d"(c[1]), "+d"(c[2]), "+d"(c[3])
+        : "d"(a0), "d"(a1), "d"(b));
+}
+
+__device__ void warp_tile_update(double *A, int ld, int n, int p, int pb, int r0, int c0, int btrans, int lower_only,
+                                 int lane, double *) {
+    const int g = lane >> 2, tg = lane & 3;
+    double acc[2][4][4];
+#pragma unroll
+    for (int mi = 0; mi < 2; mi++)
+#pragma unroll
+        for (int ni = 0; ni < 4; ni++)
+#pragma unroll
+            for (int e = 0; e < 4; e++) acc[mi][ni][e] = 0.0;
+    for (int kk = 0; kk < pb; kk += 4) {
+        const int c = kk + tg;
+        const bool okc = c < pb;
+        double a[2][2], b[4];
+#pragma unroll
+        for (int mi = 0; mi < 2; mi++) {
+            const int ra = r0 + mi * 16 + g, rb = ra + 8;
+            a[mi][0] = (okc && ra < n) ? A[ra + (size_t)(p + c) * ld] : 0.0;
+            a[mi][1] = (okc && rb < n) ? A[rb + (size_t)(p + c) * ld] : 0.0;
+        }
+#pragma unroll
+        for (int ni = 0; ni < 4; ni++) {
+            const int j = c0 + ni * 8 + g;
+            b[ni] = (okc && j < n) ? (btrans ? A[(p + c) + (size_t)j * ld] : A[j + (size_t)(p + c) * ld]) : 0.0;
+        }
+#pragma unroll
+        for (int mi = 0; mi < 2; mi++)
+#pragma unroll
+            for (int ni = 0; ni < 4; ni++) dmma_tile(acc[mi][ni], a[mi][0], a[mi][1], b[ni]);
+    }
+#pragma unroll
+    for (int mi = 0; mi < 2; mi++)
+#pragma unroll
+        for (int ni = 0; ni < 4; ni++)
+#pragma unroll
+            for (int e = 0; e < 4; e++) {
+                const int i = r0 + mi * 16 + g + (e >> 1) * 8;
+                const int j = c0 + ni * 8 + 2 * tg + (e & 1);
+                if (i < n && j < n && (!lower_only || i >= j)) A[i + (size_t)j * ld] -= acc[mi][ni][e];
+            }
+}
+
+// FP32 version: lane i owns row r0+i of the tile; B staged in per-warp shared memory.
+__device__ void warp_tile_update(float *A, int ld, int n, int p, int pb, int r0, int c0, int btrans, int lower_only,
+                                 int lane, float *bs) {
+    for (int idx = lane; idx < 32 * 32; idx += 32) {
+        const int j = idx & 31, c = idx >> 5;
+        float v = 0.0f;
+        if (c < pb && c0 + j < n) v = btrans ? A[(p + c) + (size_t)(c0 + j) * ld] : A[(c0 + j) + (size_t)(p + c) * ld];
+        bs[c * 33 + j] = v;
+    }
+    __syncwarp();
+    const int i = r0 + lane;
+    float acc[32];
+#pragma unroll
+    for (int j = 0; j < 32; j++) acc[j] = 0.0f;
+    if (i < n) {
+        for (int c = 0; c < pb; c++) {
+            const float x = A[i + (size_t)(p + c) * ld];
+#pragma unroll
+            for (int j = 0; j < 32; j++) acc[j] = fmaf(x, bs[c * 33 + j], acc[j]);
+        }
+#pragma unroll
+        for (int j = 0; j < 32; j++) {
+            const int jj = c0 + j;
+            if (jj < n && (!lower_only || i >= jj)) A[i + (size_t)jj * ld] -= acc[j];
+        }
+    }
+    __syncwarp();
+}
+
 // One CTA (256 threads) factors the diagonal block of one cblk, blocked by 32
-// columns: tile factorization, solve of the rows (and for LU columns) below
-// the tile inside the diagonal block, trailing update.  For LU the diagonal
-// block of the U arena is first added transposed into L (core_zgeadd) and
-// afterwards receives the transposed factor (core_zgetmo).
+// columns.  Per panel: one warp factors the 32x32 diagonal tile and a second
+// inverts it (lower, and for LU the upper triangle too); the rows (and, for LU,
+// columns) below the tile inside the diagonal block are solved as products with
+// those inverses; every warp then updates its own 32x32 tiles of the trailing
+// block (FP64 tensor cores for double).  The tile inverses are also stored in
+// tinv for the panel TRSM.  For LU the diagonal block of the U arena is first
+// added transposed into L (core_zgeadd) and afterwards receives the transposed
+// factor (core_zgetmo).
 template <typename T, int FACTO>
 __global__ void __launch_bounds__(256) diag_factor_kernel(DevSym s, const int *__restrict__ cblks, T *L,
-                                                          T *U, const double *__restrict__ thr_ptr,
+                                                          T *U, T *tinv, const int64_t *__restrict__ tinv_off,
+                                                          const double *__restrict__ thr_ptr,
                                                           unsigned long long *npiv, int *err) {
     __shared__ T tile[32 * TP];
-    __shared__ T xs[64 * TP];
-    __shared__ T ys[64 * TP];
+    __shared__ T wl[32 * TP];
+    __shared__ T wu[32 * TP];
+    extern __shared__ __align__(16) float diag_wbuf[];  // FP32 only: per-warp 32x33 staging
     __shared__ int s_piv, s_err;
     const int k = cblks[blockIdx.x];
     const int n = s.ncols[k], ld = s.ld[k];
     const double thr = *thr_ptr;
     T *A = L + s.off[k];
+    T *ti = tinv + tinv_off[k];
     const int tid = threadIdx.x, nth = blockDim.x, lane = tid & 31, warp = tid >> 5;
     if (tid == 0) { s_piv = 0; s_err = 0; }
     if (FACTO == FACTO_GETRF) {
@@ -143,7 +259,7 @@ __global__ void __launch_bounds__(256) diag_factor_kernel(DevSym s, const int *_
         }
     }
     __syncthreads();
-    for (int p = 0; p < n; p += 32) {
+    for (int p = 0, pi = 0; p < n; p += 32, pi++) {
         const int pb = min(32, n - p);
         T *Ap = A + p + (size_t)p * ld;
         for (int idx = tid; idx < 32 * 32; idx += nth) {
@@ -153,38 +269,46 @@ __global__ void __launch_bounds__(256) diag_factor_kernel(DevSym s, const int *_
         __syncthreads();
         if (warp == 0) factor_tile<T, FACTO>(tile, pb, lane, thr, &s_piv, &s_err);
         __syncthreads();
+        if (warp == 0) invert_lower_tile<T>(tile, wl, pb, lane, FACTO != FACTO_POTRF, 0);
+        if (FACTO == FACTO_GETRF && warp == 1) invert_lower_tile<T>(tile, wu, pb, lane, 0, 1);  // inv(U^T)
+        __syncthreads();
+        // store the factored tile and its inverse(s)
         for (int idx = tid; idx < 32 * 32; idx += nth) {
             const int i = idx & 31, j = idx >> 5;
             if (i < pb && j < pb && (FACTO != FACTO_POTRF || i >= j)) Ap[i + (size_t)j * ld] = tile[i + j * TP];
+            // panel pi of the tile-inverse store: 32 x pb, after pi full panels (two per panel for LU)
+            if (j < pb) {
+                T *tp = ti + (size_t)pi * 1024 * (FACTO == FACTO_GETRF ? 2 : 1);
+                tp[i + j * 32] = wl[i + j * TP];
+                if (FACTO == FACTO_GETRF) tp[32 * pb + i + j * 32] = wu[i + j * TP];
+            }
         }
         const int rest = n - p - pb;
         if (rest > 0) {
-            // rows below the tile: X op(T) = A
+            // rows below the tile: X = A op(T)^{-1} with the tile inverse
             for (int r = tid; r < rest; r += nth) {
                 T *row = A + (p + pb + r) + (size_t)p * ld;
-                T x[32];
+                T a[32];
 #pragma unroll
-                for (int c = 0; c < 32; c++) x[c] = (c < pb) ? row[(size_t)c * ld] : (T)0;
-#pragma unroll
-                for (int c = 0; c < 32; c++) {
-                    if (c < pb) {
-                        T v = x[c];
-                        for (int l = 0; l < c; l++) {
-                            const T tv = (FACTO == FACTO_GETRF) ? tile[l + c * TP] : tile[c + l * TP];
-                            v -= x[l] * tv;
-                        }
-                        if (FACTO != FACTO_SYTRF) v = v / tile[c * (TP + 1)];
-                        x[c] = v;
-                    }
-                }
+                for (int c = 0; c < 32; c++) a[c] = (c < pb) ? row[(size_t)c * ld] : (T)0;
 #pragma unroll
                 for (int c = 0; c < 32; c++) {
                     if (c < pb) {
-                        if (FACTO == FACTO_SYTRF) {
-                            A[(p + c) + (size_t)(p + pb + r) * ld] = x[c];          // (L D)^T in the upper part
-                            row[(size_t)c * ld] = x[c] * ((T)1 / tile[c * (TP + 1)]);  // L
+                        T v = 0;
+                        if (FACTO == FACTO_GETRF) {
+                            // X = A U^{-1}: (U^{-1})[l][c] = inv(U^T)[c][l]
+#pragma unroll
+                            for (int l = 0; l <= c; l++) v += a[l] * wu[c + l * TP];
                         } else {
-                            row[(size_t)c * ld] = x[c];
+                            // X = A L^{-T}: (L^{-T})[l][c] = inv(L)[c][l]
+#pragma unroll
+                            for (int l = 0; l <= c; l++) v += a[l] * wl[c + l * TP];
+                        }
+                        if (FACTO == FACTO_SYTRF) {
+                            A[(p + c) + (size_t)(p + pb + r) * ld] = v;          // (L D)^T in the upper part
+                            row[(size_t)c * ld] = v * ((T)1 / tile[c * (TP + 1)]);  // L
+                        } else {
+                            row[(size_t)c * ld] = v;
                         }
                     }
                 }
@@ -193,68 +317,37 @@ __global__ void __launch_bounds__(256) diag_factor_kernel(DevSym s, const int *_
                 // columns right of the tile: Y = L_tile^{-1} A (unit lower)
                 for (int cc = tid; cc < rest; cc += nth) {
                     T *col = A + p + (size_t)(p + pb + cc) * ld;
-                    T y[32];
+                    T a[32];
 #pragma unroll
-                    for (int l = 0; l < 32; l++) y[l] = (l < pb) ? col[l] : (T)0;
+                    for (int l = 0; l < 32; l++) a[l] = (l < pb) ? col[l] : (T)0;
 #pragma unroll
                     for (int l = 0; l < 32; l++) {
                         if (l < pb) {
-                            T v = y[l];
-                            for (int m = 0; m < l; m++) v -= tile[l + m * TP] * y[m];
-                            y[l] = v;
+                            T v = 0;
+#pragma unroll
+                            for (int m = 0; m <= l; m++) v += wl[l + m * TP] * a[m];
+                            col[l] = v;
                         }
                     }
-#pragma unroll
-                    for (int l = 0; l < 32; l++)
-                        if (l < pb) col[l] = y[l];
                 }
             }
             __syncthreads();
-            // trailing update of the diagonal block: A22 -= X * B^T
-            const int nt = (rest + 63) / 64;
-            for (int ti = 0; ti < nt; ti++) {
-                for (int tj = 0; tj < nt; tj++) {
-                    if (FACTO != FACTO_GETRF && tj > ti) continue;
-                    const int i0 = p + pb + ti * 64, j0 = p + pb + tj * 64;
-                    for (int idx = tid; idx < 64 * 32; idx += nth) {
-                        const int r = idx & 63, c = idx >> 6;
-                        T xv = 0, yv = 0;
-                        if (c < pb && i0 + r < n) xv = A[(i0 + r) + (size_t)(p + c) * ld];
-                        if (c < pb && j0 + r < n) {
-                            if (FACTO == FACTO_POTRF) yv = A[(j0 + r) + (size_t)(p + c) * ld];
-                            else yv = A[(p + c) + (size_t)(j0 + r) * ld];  // (L D)^T row (SYTRF) / U row (GETRF)
-                        }
-                        xs[r * TP + c] = xv;
-                        ys[r * TP + c] = yv;
-                    }
-                    __syncthreads();
-                    const int tr = tid & 15, tc = tid >> 4;
-                    T acc[4][4];
-#pragma unroll
-                    for (int a = 0; a < 4; a++)
-#pragma unroll
-                        for (int b = 0; b < 4; b++) acc[a][b] = 0;
-                    for (int c = 0; c < pb; c++) {
-                        T xv[4], yv[4];
-#pragma unroll
-                        for (int a = 0; a < 4; a++) xv[a] = xs[(tr + 16 * a) * TP + c];
-#pragma unroll
-                        for (int b = 0; b < 4; b++) yv[b] = ys[(tc + 16 * b) * TP + c];
-#pragma unroll
-                        for (int a = 0; a < 4; a++)
-#pragma unroll
-                            for (int b = 0; b < 4; b++) acc[a][b] += xv[a] * yv[b];
-                    }
-#pragma unroll
-                    for (int a = 0; a < 4; a++) {
-#pragma unroll
-                        for (int b = 0; b < 4; b++) {
-                            const int i = i0 + tr + 16 * a, j = j0 + tc + 16 * b;
-                            if (i < n && j < n && (FACTO == FACTO_GETRF || i >= j)) A[i + (size_t)j * ld] -= acc[a][b];
-                        }
-                    }
-                    __syncthreads();
+            // trailing update, one 32x32 tile per warp at a time
+            const int nt = (rest + 31) / 32;
+            const int ntiles = (FACTO == FACTO_GETRF) ? nt * nt : nt * (nt + 1) / 2;
+            for (int t = warp; t < ntiles; t += 8) {
+                int ti_, tj_;
+                if (FACTO == FACTO_GETRF) {
+                    ti_ = t % nt;
+                    tj_ = t / nt;
+                } else {
+                    tj_ = 0;
+                    int rem = t;
+                    while (rem >= nt - tj_) { rem -= nt - tj_; tj_++; }
+                    ti_ = tj_ + rem;
                 }
+                warp_tile_update(A, ld, n, p, pb, p + pb + ti_ * 32, p + pb + tj_ * 32, FACTO != FACTO_POTRF,
+                                 FACTO != FACTO_GETRF, lane, reinterpret_cast<T *>(diag_wbuf) + warp * 32 * 33);
             }
         }
         __syncthreads();
@@ -280,7 +373,9 @@ __global__ void __launch_bounds__(256) diag_factor_kernel(DevSym s, const int *_
 //   mode 1: op(T)[l][c] = D[c + l*ld]  (lower part, transposed)
 template <typename T>
 __global__ void __launch_bounds__(256) panel_trsm_kernel(DevSym s, const RowTask *__restrict__ tasks, int TR,
-                                                         T *P, const T *Dsrc, int mode, int unit) {
+                                                         T *P, const T *Dsrc, int mode, const T *__restrict__ tinv,
+                                                         const int64_t *__restrict__ tinv_off, int which, int getrf,
+                                                         int scale_d) {
     extern __shared__ __align__(16) unsigned char smraw[];
     T *xs = reinterpret_cast<T *>(smraw);  // TR x n, column-major
     __shared__ T ts[64 * TP];
@@ -326,29 +421,36 @@ __global__ void __launch_bounds__(256) panel_trsm_kernel(DevSym s, const RowTask
             const int c = cg * CPG + q;
             if (q < CPG && c < w) xs[r + (cb + c) * TR] -= acc[q];
         }
-        for (int idx = tid; idx < 32 * 32; idx += nth) {
-            const int l = idx >> 5, c = idx & 31;
-            T v = 0;
-            if (l < w && c < w) v = mode == 0 ? D[(cb + l) + (size_t)(cb + c) * ld] : D[(cb + c) + (size_t)(cb + l) * ld];
-            tt[l * TP + c] = v;
+        // multiplier of this column block: M(l, c) = W[c][l] (W = the stored tile
+        // inverse, inv(L) or inv(U^T)), divided by D[c] for LDL^T
+        {
+            const T *W = tinv + tinv_off[k] + (size_t)(cb >> 5) * 1024 * (getrf ? 2 : 1) + (which ? 32 * w : 0);
+            for (int idx = tid; idx < 32 * 32; idx += nth) {
+                const int l = idx >> 5, c = idx & 31;
+                T v = 0;
+                if (l < w && c < w && c >= l) {
+                    v = W[c + l * 32];
+                    if (scale_d) v = v / D[(size_t)(cb + c) * (ld + 1)];
+                }
+                tt[l * TP + c] = v;
+            }
         }
         __syncthreads();
-        if (tid < TR) {
-            T x[32];
+        {
+            T out[8];
 #pragma unroll
-            for (int c = 0; c < 32; c++) x[c] = (c < w) ? xs[tid + (cb + c) * TR] : (T)0;
-#pragma unroll
-            for (int c = 0; c < 32; c++) {
-                if (c < w) {
-                    T v = x[c];
-                    for (int l = 0; l < c; l++) v -= x[l] * tt[l * TP + c];
-                    if (!unit) v = v / tt[c * (TP + 1)];
-                    x[c] = v;
-                }
+            for (int q = 0; q < 8; q++) {
+                out[q] = 0;
+                const int c = cg * CPG + q;
+                if (q < CPG && c < w)
+                    for (int l = 0; l <= c; l++) out[q] += xs[r + (cb + l) * TR] * tt[l * TP + c];
             }
+            __syncthreads();
 #pragma unroll
-            for (int c = 0; c < 32; c++)
-                if (c < w) xs[tid + (cb + c) * TR] = x[c];
+            for (int q = 0; q < 8; q++) {
+                const int c = cg * CPG + q;
+                if (q < CPG && c < w) xs[r + (cb + c) * TR] = out[q];
+            }
         }
         __syncthreads();
     }
@@ -357,6 +459,265 @@ __global__ void __launch_bounds__(256) panel_trsm_kernel(DevSym s, const RowTask
         if (rr < rows) X[rr + (size_t)c * ld] = xs[idx];
     }
 }
+
+// ------------------------------------------------------------------ sub-panels of wide cblks
+//
+// POTRF / LDL^T of a wide cblk as a sequence of 64-column sub-panels (PaStiX
+// factors the diagonal block with its blocked core_zpotrfsp / core_zsytrfsp and
+// then solves the whole panel; here the same blocked right-looking algorithm is
+// spread over many CTAs): factor the 64x64 diagonal tile of the sub-panel and
+// invert it (one CTA, in shared memory), solve every row below it in the panel
+// as a product with that inverse (one CTA per 64 rows), then update the
+// remaining columns of the panel with the GEMM-scatter kernel (f = k).
+
+constexpr int SP = 64, SPP = 65;
+
+// factor_tile / invert_lower_tile on a tile with leading dimension ldt (shared memory)
+template <typename T, int FACTO>
+__device__ void factor_tile_ld(T *t, int ldt, int pb, int lane, double thr, int *piv, int *err) {
+    for (int c = 0; c < pb; c++) {
+        if (lane == 0) {
+            T d = t[c * (ldt + 1)];
+            if (fabs((double)d) < thr) {
+                if (FACTO == FACTO_POTRF) d = (T)thr;
+                else d = (d < (T)0) ? (T)(-thr) : (T)thr;
+                (*piv)++;
+            }
+            if (FACTO == FACTO_POTRF) {
+                if (d < (T)0) { *err = 1; d = -d; }
+                d = sqrt(d);
+            }
+            t[c * (ldt + 1)] = d;
+        }
+        __syncwarp();
+        const T d = t[c * (ldt + 1)];
+        const T inv = (T)1 / d;
+        T lic = 0;
+        if (lane > c && lane < pb) {
+            const T v = t[lane + c * ldt];
+            lic = v * inv;
+            t[lane + c * ldt] = lic;
+        }
+        __syncwarp();
+        if (lane > c && lane < pb) {
+            const T f = (FACTO == FACTO_POTRF) ? lic : d * lic;
+            for (int j = c + 1; j <= lane; j++) t[lane + j * ldt] -= f * t[j + c * ldt];
+        }
+        __syncwarp();
+    }
+}
+
+template <typename T>
+__device__ void invert_lower_ld(const T *t, int ldt, T *w, int ldw, int pb, int lane, int unit) {
+    for (int i = 0; i < 32; i++) {
+        if (lane <= i) {
+            const int j = lane;
+            T v = 0;
+            if (i < pb) {
+                const T dii = unit ? (T)1 : t[i + i * ldt];
+                if (j == i) {
+                    v = (T)1 / dii;
+                } else {
+                    T acc = 0;
+                    for (int m = j; m < i; m++) acc += t[i + m * ldt] * w[m + j * ldw];
+                    v = -acc / dii;
+                }
+            }
+            w[i + j * ldw] = v;
+        } else {
+            w[i + lane * ldw] = 0;
+        }
+        __syncwarp();
+    }
+}
+
+// 64x64 diagonal tile of a sub-panel, blocked 2 x 32:
+//   L11 = fact(A11); W11 = L11^{-1};  X21 = A21 L11^{-T}  (LDL^T: L21 = X21 D1^{-1});
+//   A22 -= L21 X21^T;  L22 = fact(A22); W22 = L22^{-1};  W21 = -W22 L21 W11.
+// The tile and its inverse W (64x64, lower) are written back.
+template <typename T, int FACTO>
+__global__ void __launch_bounds__(256) subpanel_diag_kernel(DevSym s, const SubTask *__restrict__ tasks, T *L,
+                                                            T *winv, const double *__restrict__ thr_ptr,
+                                                            unsigned long long *npiv, int *err) {
+    extern __shared__ __align__(16) unsigned char sp_smem[];
+    T *a = reinterpret_cast<T *>(sp_smem);   // 64 x 64 tile (ld SPP)
+    T *w = a + SP * SPP;                     // 64 x 64 inverse (ld SPP)
+    __shared__ T x21[32 * 33];               // X21 (LDL^T: L21 D1), then L21 W11
+    __shared__ int s_piv, s_err;
+    const SubTask tk = tasks[blockIdx.x];
+    const int k = tk.k, c0 = tk.c0, ld = s.ld[k];
+    const int n = s.ncols[k], wd = min(SP, n - c0);
+    const int w1 = min(32, wd), w2 = wd - w1;
+    const double thr = *thr_ptr;
+    T *A = L + s.off[k] + c0 + (size_t)c0 * ld;
+    const int tid = threadIdx.x, nth = blockDim.x, lane = tid & 31, warp = tid >> 5;
+    if (tid == 0) { s_piv = 0; s_err = 0; }
+    for (int idx = tid; idx < SP * SP; idx += nth) {
+        const int i = idx & 63, j = idx >> 6;
+        a[i + j * SPP] = (i < wd && j < wd && i >= j) ? A[i + (size_t)j * ld] : (T)0;
+        w[i + j * SPP] = 0;
+    }
+    __syncthreads();
+    if (warp == 0) {
+        factor_tile_ld<T, FACTO>(a, SPP, w1, lane, thr, &s_piv, &s_err);
+        invert_lower_ld<T>(a, SPP, w, SPP, w1, lane, FACTO != FACTO_POTRF);
+    }
+    __syncthreads();
+    if (w2 > 0) {
+        // X21 = A21 W11^T (32 x 32): thread -> (row i, 4 columns)
+        {
+            const int i = tid & 31, cq = (tid >> 5) * 4;
+            T v[4];
+#pragma unroll
+            for (int q = 0; q < 4; q++) {
+                const int c = cq + q;
+                T acc = 0;
+                if (i < w2 && c < w1)
+                    for (int l = 0; l <= c; l++) acc += a[(32 + i) + l * SPP] * w[c + l * SPP];
+                v[q] = acc;
+            }
+            __syncthreads();
+#pragma unroll
+            for (int q = 0; q < 4; q++) {
+                const int c = cq + q;
+                x21[i + c * 33] = v[q];
+                if (i < w2 && c < w1)
+                    a[(32 + i) + c * SPP] = (FACTO == FACTO_SYTRF) ? v[q] / a[c * (SPP + 1)] : v[q];
+            }
+        }
+        __syncthreads();
+        // A22 -= L21 X21^T (lower): thread -> (row i, 4 columns)
+        {
+            const int i = tid & 31, jq = (tid >> 5) * 4;
+#pragma unroll
+            for (int q = 0; q < 4; q++) {
+                const int j = jq + q;
+                if (i < w2 && j <= i) {
+                    T acc = 0;
+                    for (int c = 0; c < w1; c++) acc += a[(32 + i) + c * SPP] * x21[j + c * 33];
+                    a[(32 + i) + (32 + j) * SPP] -= acc;
+                }
+            }
+        }
+        __syncthreads();
+        if (warp == 0) {
+            factor_tile_ld<T, FACTO>(a + 32 * (SPP + 1), SPP, w2, lane, thr, &s_piv, &s_err);
+            invert_lower_ld<T>(a + 32 * (SPP + 1), SPP, w + 32 * (SPP + 1), SPP, w2, lane, FACTO != FACTO_POTRF);
+        }
+        __syncthreads();
+        // T21 = L21 W11 -> x21 ; W21 = -W22 T21
+        {
+            const int i = tid & 31, cq = (tid >> 5) * 4;
+            T v[4];
+#pragma unroll
+            for (int q = 0; q < 4; q++) {
+                const int c = cq + q;
+                T acc = 0;
+                if (i < w2 && c < w1)
+                    for (int l = c; l < w1; l++) acc += a[(32 + i) + l * SPP] * w[l + c * SPP];
+                v[q] = acc;
+            }
+            __syncthreads();
+#pragma unroll
+            for (int q = 0; q < 4; q++) x21[i + (cq + q) * 33] = v[q];
+            __syncthreads();
+#pragma unroll
+            for (int q = 0; q < 4; q++) {
+                const int c = cq + q;
+                T acc = 0;
+                if (i < w2 && c < w1)
+                    for (int m = 0; m <= i; m++) acc += w[(32 + i) + (32 + m) * SPP] * x21[m + c * 33];
+                v[q] = -acc;
+            }
+#pragma unroll
+            for (int q = 0; q < 4; q++)
+                if (i < w2 && cq + q < w1) w[(32 + i) + (cq + q) * SPP] = v[q];
+        }
+        __syncthreads();
+    }
+    T *W = winv + (size_t)tk.pos * SP * SP;
+    for (int idx = tid; idx < SP * SP; idx += nth) {
+        const int i = idx & 63, j = idx >> 6;
+        if (i < wd && j < wd && i >= j) A[i + (size_t)j * ld] = a[i + j * SPP];
+        W[idx] = w[i + j * SPP];
+    }
+    if (tid == 0) {
+        if (s_piv) atomicAdd(npiv, (unsigned long long)s_piv);
+        if (s_err) atomicExch(err, 1);
+    }
+}
+
+// X = A W^T (POTRF) or A W^T D^{-1} (LDL^T) for 64 rows of the panel below the
+// sub-panel's diagonal tile, in place.
+template <typename T, int FACTO>
+__global__ void __launch_bounds__(256) subpanel_trsm_kernel(DevSym s, const SubTask *__restrict__ tasks, T *L,
+                                                            const T *__restrict__ winv) {
+    extern __shared__ __align__(16) unsigned char sp_smem[];
+    T *xa = reinterpret_cast<T *>(sp_smem);
+    T *wt = xa + SP * SPP;
+    __shared__ T dinv[SP];
+    const SubTask tk = tasks[blockIdx.x];
+    const int k = tk.k, c0 = tk.c0, ld = s.ld[k];
+    const int wd = min(SP, s.ncols[k] - c0);
+    const int rows = min(SP, s.stride[k] - tk.row0);
+    T *X = L + s.off[k] + tk.row0 + (size_t)c0 * ld;
+    const T *W = winv + (size_t)tk.pos * SP * SP;
+    const T *Dg = L + s.off[k] + c0 + (size_t)c0 * ld;
+    const int tid = threadIdx.x, nth = blockDim.x;
+    for (int idx = tid; idx < SP * SP; idx += nth) {
+        const int i = idx & 63, j = idx >> 6;
+        xa[i + j * SPP] = (i < rows && j < wd) ? X[i + (size_t)j * ld] : (T)0;
+        wt[i + j * SPP] = (i < wd && j < wd) ? W[idx] : (T)0;
+    }
+    if (tid < SP) dinv[tid] = (FACTO == FACTO_SYTRF && tid < wd) ? (T)1 / Dg[(size_t)tid * (ld + 1)] : (T)1;
+    __syncthreads();
+    // thread: row r = tid & 63, columns cg*16 .. cg*16+15
+    const int r = tid & 63, cg = tid >> 6;
+    T acc[16];
+#pragma unroll
+    for (int q = 0; q < 16; q++) acc[q] = 0;
+    for (int l = 0; l < wd; l++) {
+        const T x = xa[r + l * SPP];
+#pragma unroll
+        for (int q = 0; q < 16; q++) acc[q] += x * wt[(cg * 16 + q) + l * SPP];  // W[c][l]
+    }
+    if (r < rows) {
+#pragma unroll
+        for (int q = 0; q < 16; q++) {
+            const int c = cg * 16 + q;
+            if (c < wd) X[r + (size_t)c * ld] = acc[q] * dinv[c];
+        }
+    }
+}
+
+template <typename T>
+void launch_subpanel_diag(int facto, const DevSym &s, const SubTask *tasks, int ntasks, T *L, T *winv,
+                          const double *thr, unsigned long long *npiv, int *err, cudaStream_t st) {
+    if (ntasks <= 0) return;
+    const size_t smem = 2 * SP * SPP * sizeof(T);
+    if (facto == FACTO_POTRF)
+        subpanel_diag_kernel<T, FACTO_POTRF><<<ntasks, 256, smem, st>>>(s, tasks, L, winv, thr, npiv, err);
+    else
+        subpanel_diag_kernel<T, FACTO_SYTRF><<<ntasks, 256, smem, st>>>(s, tasks, L, winv, thr, npiv, err);
+}
+
+template <typename T>
+void launch_subpanel_trsm(int facto, const DevSym &s, const SubTask *tasks, int ntasks, T *L, const T *winv,
+                          cudaStream_t st) {
+    if (ntasks <= 0) return;
+    const size_t smem = 2 * SP * SPP * sizeof(T);
+    if (facto == FACTO_POTRF) subpanel_trsm_kernel<T, FACTO_POTRF><<<ntasks, 256, smem, st>>>(s, tasks, L, winv);
+    else subpanel_trsm_kernel<T, FACTO_SYTRF><<<ntasks, 256, smem, st>>>(s, tasks, L, winv);
+}
+
+template void launch_subpanel_diag<double>(int, const DevSym &, const SubTask *, int, double *, double *,
+                                           const double *, unsigned long long *, int *, cudaStream_t);
+template void launch_subpanel_diag<float>(int, const DevSym &, const SubTask *, int, float *, float *, const double *,
+                                          unsigned long long *, int *, cudaStream_t);
+template void launch_subpanel_trsm<double>(int, const DevSym &, const SubTask *, int, double *, const double *,
+                                           cudaStream_t);
+template void launch_subpanel_trsm<float>(int, const DevSym &, const SubTask *, int, float *, const float *,
+                                          cudaStream_t);
 
 // ------------------------------------------------------------------ updates
 
@@ -405,9 +766,9 @@ __global__ void __launch_bounds__(128) update_f64_kernel(DevSym s, const Upd *__
     tile_coords(u, tile - u.tile0, mt, nt);
     const int m0 = mt * UT_M, n0 = nt * UT_N;
     const int k = u.k, ldk = s.ld[k];
-    const double *Ap = ((u.flags & UPD_A_U) ? U : L) + s.off[k] + u.rowA0 + m0;
-    const double *Bp = ((u.flags & UPD_B_U) ? U : L) + s.off[k] + u.rowB0 + n0;
-    const double *Dp = L + s.off[k];
+    const double *Ap = ((u.flags & UPD_A_U) ? U : L) + s.off[k] + u.rowA0 + m0 + (size_t)u.colK0 * ldk;
+    const double *Bp = ((u.flags & UPD_B_U) ? U : L) + s.off[k] + u.rowB0 + n0 + (size_t)u.colK0 * ldk;
+    const double *Dp = L + s.off[k] + (size_t)u.colK0 * (ldk + 1);
     const bool scale = (u.flags & UPD_SCALE_D) != 0;
     const int mrem = u.M - m0, nrem = u.N - n0;
     const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
@@ -509,9 +870,9 @@ __global__ void __launch_bounds__(256) update_simt_f32_kernel(DevSym s, const Up
     tile_coords(u, tile - u.tile0, mt, nt);
     const int m0 = mt * UT_M, n0 = nt * UT_N;
     const int k = u.k, ldk = s.ld[k];
-    const float *Ap = ((u.flags & UPD_A_U) ? U : L) + s.off[k] + u.rowA0 + m0;
-    const float *Bp = ((u.flags & UPD_B_U) ? U : L) + s.off[k] + u.rowB0 + n0;
-    const float *Dp = L + s.off[k];
+    const float *Ap = ((u.flags & UPD_A_U) ? U : L) + s.off[k] + u.rowA0 + m0 + (size_t)u.colK0 * ldk;
+    const float *Bp = ((u.flags & UPD_B_U) ? U : L) + s.off[k] + u.rowB0 + n0 + (size_t)u.colK0 * ldk;
+    const float *Dp = L + s.off[k] + (size_t)u.colK0 * (ldk + 1);
     const bool scale = (u.flags & UPD_SCALE_D) != 0;
     const int mrem = u.M - m0, nrem = u.N - n0;
     const int tid = threadIdx.x;
@@ -587,23 +948,24 @@ void launch_scatter(int64_t nnz, const int64_t *dest, const double *Lv, const do
 }
 
 template <typename T>
-void launch_diag(int facto, const DevSym &s, const int *cblks, int ncblk, T *L, T *U, const double *thr,
-                 unsigned long long *npiv, int *err, cudaStream_t st) {
+void launch_diag(int facto, const DevSym &s, const int *cblks, int ncblk, T *L, T *U, T *tinv,
+                 const int64_t *tinv_off, const double *thr, unsigned long long *npiv, int *err, cudaStream_t st) {
     if (ncblk <= 0) return;
+    const size_t smem = (sizeof(T) == 4) ? 8 * 32 * 33 * sizeof(float) : 0;
     if (facto == FACTO_POTRF)
-        diag_factor_kernel<T, FACTO_POTRF><<<ncblk, 256, 0, st>>>(s, cblks, L, U, thr, npiv, err);
+        diag_factor_kernel<T, FACTO_POTRF><<<ncblk, 256, smem, st>>>(s, cblks, L, U, tinv, tinv_off, thr, npiv, err);
     else if (facto == FACTO_GETRF)
-        diag_factor_kernel<T, FACTO_GETRF><<<ncblk, 256, 0, st>>>(s, cblks, L, U, thr, npiv, err);
+        diag_factor_kernel<T, FACTO_GETRF><<<ncblk, 256, smem, st>>>(s, cblks, L, U, tinv, tinv_off, thr, npiv, err);
     else
-        diag_factor_kernel<T, FACTO_SYTRF><<<ncblk, 256, 0, st>>>(s, cblks, L, U, thr, npiv, err);
+        diag_factor_kernel<T, FACTO_SYTRF><<<ncblk, 256, smem, st>>>(s, cblks, L, U, tinv, tinv_off, thr, npiv, err);
 }
 
 template <typename T>
 void launch_trsm(const DevSym &s, const RowTask *tasks, int ntasks, int TR, int nmax, T *P, const T *D, int mode,
-                 int unit, cudaStream_t st) {
+                 const T *tinv, const int64_t *tinv_off, int which, int getrf, int scale_d, cudaStream_t st) {
     if (ntasks <= 0) return;
     const size_t smem = (size_t)TR * nmax * sizeof(T);
-    panel_trsm_kernel<T><<<ntasks, 256, smem, st>>>(s, tasks, TR, P, D, mode, unit);
+    panel_trsm_kernel<T><<<ntasks, 256, smem, st>>>(s, tasks, TR, P, D, mode, tinv, tinv_off, which, getrf, scale_d);
 }
 
 void launch_update_f64(const DevSym &s, const Upd *upds, int nupd, int ntiles, double *L, double *U,
@@ -635,6 +997,11 @@ static int raise_smem(K kernel) {
 int configure_factor_kernels() {
     int lim = 1 << 30;
     int v;
+    if (raise_smem(subpanel_diag_kernel<double, FACTO_POTRF>) < 0 || raise_smem(subpanel_diag_kernel<double, FACTO_SYTRF>) < 0 ||
+        raise_smem(subpanel_diag_kernel<float, FACTO_POTRF>) < 0 || raise_smem(subpanel_diag_kernel<float, FACTO_SYTRF>) < 0 ||
+        raise_smem(subpanel_trsm_kernel<double, FACTO_POTRF>) < 0 || raise_smem(subpanel_trsm_kernel<double, FACTO_SYTRF>) < 0 ||
+        raise_smem(subpanel_trsm_kernel<float, FACTO_POTRF>) < 0 || raise_smem(subpanel_trsm_kernel<float, FACTO_SYTRF>) < 0)
+        return -1;
     if ((v = raise_smem(update_f64_kernel)) < UPD_F64_SMEM) return -1;
     if ((v = raise_smem(panel_trsm_kernel<double>)) < 0) return -1;
     lim = std::min(lim, v);
@@ -647,13 +1014,13 @@ template void launch_scatter<double>(int64_t, const int64_t *, const double *, c
                                      cudaStream_t);
 template void launch_scatter<float>(int64_t, const int64_t *, const double *, const double *, float *, float *,
                                     cudaStream_t);
-template void launch_diag<double>(int, const DevSym &, const int *, int, double *, double *, const double *,
-                                  unsigned long long *, int *, cudaStream_t);
-template void launch_diag<float>(int, const DevSym &, const int *, int, float *, float *, const double *,
-                                 unsigned long long *, int *, cudaStream_t);
-template void launch_trsm<double>(const DevSym &, const RowTask *, int, int, int, double *, const double *, int, int,
-                                  cudaStream_t);
-template void launch_trsm<float>(const DevSym &, const RowTask *, int, int, int, float *, const float *, int, int,
-                                 cudaStream_t);
+template void launch_diag<double>(int, const DevSym &, const int *, int, double *, double *, double *,
+                                  const int64_t *, const double *, unsigned long long *, int *, cudaStream_t);
+template void launch_diag<float>(int, const DevSym &, const int *, int, float *, float *, float *, const int64_t *,
+                                 const double *, unsigned long long *, int *, cudaStream_t);
+template void launch_trsm<double>(const DevSym &, const RowTask *, int, int, int, double *, const double *, int,
+                                  const double *, const int64_t *, int, int, int, cudaStream_t);
+template void launch_trsm<float>(const DevSym &, const RowTask *, int, int, int, float *, const float *, int,
+                                 const float *, const int64_t *, int, int, int, cudaStream_t);
 
 }  // namespace b200

@@ -9,12 +9,22 @@ namespace b200 {
 template <typename T>
 void launch_scatter(int64_t nnz, const int64_t *dest, const double *Lv, const double *Uv, T *L, T *U,
                     cudaStream_t st);
+// tinv: per cblk 32 x ncols (x2 for LU) tile inverses written by the diagonal kernel, read by the TRSM
 template <typename T>
-void launch_diag(int facto, const DevSym &s, const int *cblks, int ncblk, T *L, T *U, const double *thr,
-                 unsigned long long *npiv, int *err, cudaStream_t st);
+void launch_diag(int facto, const DevSym &s, const int *cblks, int ncblk, T *L, T *U, T *tinv,
+                 const int64_t *tinv_off, const double *thr, unsigned long long *npiv, int *err, cudaStream_t st);
+// X op(T) = B: mode 0 upper / 1 lower-transposed for the left-looking part; which = 0 (inv L) or 1 (inv U^T)
+// selects the tile inverse; scale_d divides by D (LDL^T)
 template <typename T>
 void launch_trsm(const DevSym &s, const RowTask *tasks, int ntasks, int TR, int nmax, T *P, const T *D, int mode,
-                 int unit, cudaStream_t st);
+                 const T *tinv, const int64_t *tinv_off, int which, int getrf, int scale_d, cudaStream_t st);
+// sub-panel path of wide POTRF / LDL^T cblks (64-column steps)
+template <typename T>
+void launch_subpanel_diag(int facto, const DevSym &s, const SubTask *tasks, int ntasks, T *L, T *winv,
+                          const double *thr, unsigned long long *npiv, int *err, cudaStream_t st);
+template <typename T>
+void launch_subpanel_trsm(int facto, const DevSym &s, const SubTask *tasks, int ntasks, T *L, const T *winv,
+                          cudaStream_t st);
 void launch_update_f64(const DevSym &s, const Upd *upds, int nupd, int ntiles, double *L, double *U,
                        cudaStream_t st);
 void launch_update_f32(const DevSym &s, const Upd *upds, int nupd, int ntiles, float *L, float *U,
@@ -29,12 +39,29 @@ void launch_solve_diag(const DevSym &s, const int *cblks, int ncblk, int nmax, c
 template <typename T>
 void launch_solve_offdiag(const DevSym &s, const RowTask *tasks, int ntasks, const T *L, double *x, int64_t ldx,
                           int nrhs, int backward, cudaStream_t st);
+// off-diagonal solve on 64x64 tiles with FP64 tensor cores; x and b may be the same buffer
+template <typename T>
+void launch_solve_tiles(const DevSym &s, const SolveTile *tasks, int ntasks, const T *L, const double *x, double *b,
+                        int64_t ldx, int nrhs, int backward, cudaStream_t st);
+// W_k = inverse of the lower-triangular diagonal block of every listed cblk (W: n x n per cblk)
+template <typename T>
+void launch_diag_inverse(const DevSym &s, const int *cblks, int ncblk, const T *L, T *W, const int64_t *woff,
+                         int unit, cudaStream_t st);
+// W_k of cblks with at most 32 columns, copied from the diagonal kernel's tile inverses (which: 0 L, 1 U^T)
+template <typename T>
+void launch_copy_tile_inverse(const DevSym &s, const int *cblks, int ncblk, const T *tinv, const int64_t *toff, T *W,
+                              const int64_t *woff, int which, cudaStream_t st);
+// xout[k] = W_k xin[k] (forward) or W_k^T xin[k] (backward) on 64-row tiles (task row0 < ncols)
+template <typename T>
+void launch_solve_diag_inv(const DevSym &s, const RowTask *tasks, int ntasks, const T *W, const int64_t *woff,
+                           const double *xin, double *xout, int64_t ldx, int nrhs, int backward, cudaStream_t st);
 template <typename T>
 void launch_solve_scale_diag(const DevSym &s, const int *cblks, int ncblk, const T *L, double *x, int64_t ldx,
                              int nrhs, cudaStream_t st);
 void launch_permute(int n, int nrhs, const int *peri, const double *src, int64_t lds, double *dst, int64_t ldd,
                     int forward, cudaStream_t st);
 int configure_solve_kernels();
+int configure_inverse_kernels();
 
 // refinement vectors (refine_kernels.cu)
 void launch_spmv(int n, int nrhs, const int64_t *colptr, const int *rowtab, const double *vals, const double *x,

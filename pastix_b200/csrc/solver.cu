@@ -78,8 +78,36 @@ struct b200_solver_s {
     int *d_peri = nullptr;
     int *d_lvl_cblk = nullptr;
     RowTask *d_trsm = nullptr, *d_stask = nullptr;
+    SolveTile *d_stile = nullptr;
+    std::vector<int> lvl_st0, lvl_st1;  // solve tiles of each level
+    RowTask *d_dtask = nullptr;         // 64-row tiles of the diagonal blocks (solves)
+    std::vector<int> lvl_dt0, lvl_dt1;
+    // inverses of the diagonal blocks: W_L (forward sweep) and, for LU, W_U (backward)
+    int64_t *d_woff = nullptr;
+    int64_t winv_elems = 0;
+    int64_t *d_toff = nullptr;          // tile inverses of the panel TRSM: 32 x ncols (x2 for LU) per cblk
+    int64_t tinv_elems = 0;
+    void *dTinv = nullptr;
+    void *dWL = nullptr, *dWU = nullptr;
     Upd *d_upd = nullptr;
     std::vector<Level> levels;
+    // cblks of each level that go through the one-CTA diagonal kernel (the others take the sub-panel path)
+    int *d_diag_list = nullptr;
+    int *d_inv_small = nullptr, *d_inv_big = nullptr;  // cblks of <= 32 / > 32 columns
+    int n_inv_small = 0, n_inv_big = 0;
+    std::vector<int> lvl_ds0, lvl_ds1;
+    // sub-panel steps of wide POTRF / LDL^T cblks
+    struct SubStep {
+        int d0, d1;   // subpanel diagonal tasks
+        int t0, t1;   // subpanel TRSM tasks
+        int u0, u1;   // internal updates
+        int ntiles;
+    };
+    std::vector<std::vector<SubStep>> lvl_steps;
+    SubTask *d_subtask = nullptr;
+    Upd *d_subupd = nullptr;
+    void *d_subwinv = nullptr;
+    int64_t subwinv_slots = 0;
     std::vector<int> lvl_tr;            // TRSM rows per task of each level
     std::vector<int> lvl_s0, lvl_s1;    // solve row tasks of each level
     int nmax_all = 0;
@@ -116,6 +144,7 @@ struct b200_solver_s {
     double t_fact = 0, t_solve = 0, t_refine = 0;
     int launches_fact = 0, launches_solve = 0;
     long long kernel_launches = 0;      // kernels this instance has run (graph replays included)
+    std::vector<std::pair<int, double>> trace_detail;  // per-launch times of the last trace
     cudaEvent_t ev0 = nullptr, ev1 = nullptr;
 
     template <typename T>
@@ -154,7 +183,21 @@ int build_schedule(b200_solver_t *s) {
         for (int k = 0; k < N; k++) lvl_cblk[pos[level[k]]++] = k;
     }
     std::vector<RowTask> trsm, stask;
+    std::vector<SolveTile> stile;
     std::vector<Upd> upds;
+    std::vector<int> diag_list;
+    std::vector<SubTask> subtasks;
+    std::vector<Upd> subupds;
+    s->lvl_ds0.assign(nlev, 0);
+    s->lvl_ds1.assign(nlev, 0);
+    s->lvl_steps.assign(nlev, {});
+    const int split_min = 96;  // wider POTRF / LDL^T cblks take the sub-panel path
+    auto is_big = [&](int k) { return s->facto != FACTO_GETRF && s->ncols[k] > split_min; };
+    s->lvl_st0.assign(nlev, 0);
+    s->lvl_st1.assign(nlev, 0);
+    s->lvl_dt0.assign(nlev, 0);
+    s->lvl_dt1.assign(nlev, 0);
+    std::vector<RowTask> dtask;
     s->levels.assign(nlev, Level{});
     s->lvl_tr.assign(nlev, 64);
     s->lvl_s0.assign(nlev, 0);
@@ -177,11 +220,77 @@ int build_schedule(b200_solver_t *s) {
         s->lvl_tr[l] = TR;
         L.t0 = (int)trsm.size();
         s->lvl_s0[l] = (int)stask.size();
+        s->lvl_st0[l] = (int)stile.size();
+        s->lvl_dt0[l] = (int)dtask.size();
+        s->lvl_ds0[l] = (int)diag_list.size();
+        for (int i = L.c0; i < L.c1; i++)
+            if (!is_big(lvl_cblk[i])) diag_list.push_back(lvl_cblk[i]);
+        s->lvl_ds1[l] = (int)diag_list.size();
+        {
+            // sub-panel steps: 64 columns each, for every wide cblk of the level
+            int nsteps = 0;
+            for (int i = L.c0; i < L.c1; i++)
+                if (is_big(lvl_cblk[i])) nsteps = std::max(nsteps, (s->ncols[lvl_cblk[i]] + 63) / 64);
+            for (int st = 0; st < nsteps; st++) {
+                b200_solver_s::SubStep ss{};
+                const int c0 = st * 64;
+                int pos = 0;
+                ss.d0 = (int)subtasks.size();
+                std::vector<std::pair<int, int>> members;  // (k, pos)
+                for (int i = L.c0; i < L.c1; i++) {
+                    const int k = lvl_cblk[i];
+                    if (!is_big(k) || c0 >= s->ncols[k]) continue;
+                    members.push_back({k, pos});
+                    subtasks.push_back({k, c0, c0, pos});
+                    pos++;
+                }
+                ss.d1 = (int)subtasks.size();
+                s->subwinv_slots = std::max<int64_t>(s->subwinv_slots, pos);
+                ss.t0 = (int)subtasks.size();
+                for (auto &m : members) {
+                    const int wd = std::min(64, s->ncols[m.first] - c0);  // rows below the sub-panel's tile
+                    for (int r0 = c0 + wd; r0 < s->stride[m.first]; r0 += 64) subtasks.push_back({m.first, r0, c0, m.second});
+                }
+                ss.t1 = (int)subtasks.size();
+                ss.u0 = (int)subupds.size();
+                int t0 = 0;
+                for (auto &m : members) {
+                    const int k = m.first, n = s->ncols[k];
+                    if (c0 + 64 >= n) continue;
+                    Upd u{};
+                    u.k = k;
+                    u.j = -1;
+                    u.f = k;
+                    u.colK0 = c0;
+                    u.rowA0 = c0 + 64;
+                    u.rowB0 = c0 + 64;
+                    u.M = s->stride[k] - (c0 + 64);
+                    u.N = n - (c0 + 64);
+                    u.K = 64;
+                    u.colbase = c0 + 64;
+                    u.flags = UPD_SYM | (s->facto == FACTO_SYTRF ? UPD_SCALE_D : 0);
+                    u.tiles_m = (u.M + 63) / 64;
+                    u.tiles_n = (u.N + 63) / 64;
+                    u.tile0 = t0;
+                    t0 += u.tiles_n * u.tiles_m - u.tiles_n * (u.tiles_n - 1) / 2;
+                    subupds.push_back(u);
+                }
+                ss.u1 = (int)subupds.size();
+                ss.ntiles = t0;
+                s->lvl_steps[l].push_back(ss);
+            }
+        }
         for (int i = L.c0; i < L.c1; i++) {
             const int k = lvl_cblk[i];
-            for (int r0 = s->ncols[k]; r0 < s->stride[k]; r0 += TR) trsm.push_back({k, r0});
+            for (int r0 = 0; r0 < s->ncols[k]; r0 += 64) dtask.push_back({k, r0});
+            if (!is_big(k))
+                for (int r0 = s->ncols[k]; r0 < s->stride[k]; r0 += TR) trsm.push_back({k, r0});
             for (int r0 = s->ncols[k]; r0 < s->stride[k]; r0 += 128) stask.push_back({k, r0});
+            for (int r0 = s->ncols[k]; r0 < s->stride[k]; r0 += 64)
+                for (int c0 = 0; c0 < s->ncols[k]; c0 += 64) stile.push_back({k, r0, c0});
         }
+        s->lvl_st1[l] = (int)stile.size();
+        s->lvl_dt1[l] = (int)dtask.size();
         L.t1 = (int)trsm.size();
         s->lvl_s1[l] = (int)stask.size();
         // number of sources of this level facing each cblk
@@ -262,6 +371,38 @@ int build_schedule(b200_solver_t *s) {
     RET(s->dupload(&s->d_lvl_cblk, lvl_cblk));
     RET(s->dupload(&s->d_trsm, trsm));
     RET(s->dupload(&s->d_stask, stask));
+    RET(s->dupload(&s->d_stile, stile));
+    RET(s->dupload(&s->d_dtask, dtask));
+    RET(s->dupload(&s->d_diag_list, diag_list));
+    {
+        std::vector<int> small, big;
+        for (int k = 0; k < N; k++) (s->ncols[k] <= 32 && !is_big(k) ? small : big).push_back(k);
+        s->n_inv_small = (int)small.size();
+        s->n_inv_big = (int)big.size();
+        RET(s->dupload(&s->d_inv_small, small));
+        RET(s->dupload(&s->d_inv_big, big));
+    }
+    RET(s->dupload(&s->d_subtask, subtasks));
+    RET(s->dupload(&s->d_subupd, subupds));
+    // inverse arena: n_k x n_k per cblk, 256-byte aligned
+    std::vector<int64_t> woff(N);
+    int64_t wpos = 0;
+    const int64_t walign = s->f32 ? 64 : 32;
+    for (int k = 0; k < N; k++) {
+        wpos = (wpos + walign - 1) / walign * walign;
+        woff[k] = wpos;
+        wpos += (int64_t)s->ncols[k] * s->ncols[k];
+    }
+    s->winv_elems = (wpos + walign - 1) / walign * walign;
+    RET(s->dupload(&s->d_woff, woff));
+    std::vector<int64_t> toff(N);
+    int64_t tpos = 0;
+    for (int k = 0; k < N; k++) {
+        toff[k] = tpos;
+        tpos += (int64_t)32 * s->ncols[k] * (s->facto == FACTO_GETRF ? 2 : 1);
+    }
+    s->tinv_elems = tpos;
+    RET(s->dupload(&s->d_toff, toff));
     RET(s->dupload(&s->d_upd, upds));
     return ERR_SUCCESS;
 }
@@ -292,8 +433,13 @@ int ensure_scal(b200_solver_t *s, int count) {
 // Per-kernel-class timing of one factorization (kernels_trace,
 // kernels/kernels_trace.h:206-300): class 0 arena clear + bcsc scatter, 1 diagonal
 // blocks, 2 panel TRSM, 3 GEMM-scatter updates.
+// Fine kernel kinds recorded in the per-launch detail; ids 0-3 are the classes
+// above, 4 subpanel diagonal, 5 subpanel TRSM, 6 subpanel internal update,
+// 7 diagonal-block inverses (summed into classes 1, 2, 2, 1).
 struct Trace {
-    std::vector<std::pair<cudaEvent_t, cudaEvent_t>> ev[4];
+    static constexpr int NK = 8;
+    static int coarse(int c) { return c < 4 ? c : (c == 4 || c == 7) ? 1 : 2; }
+    std::vector<std::pair<cudaEvent_t, cudaEvent_t>> ev[NK];
     cudaEvent_t open = nullptr;
     void begin(cudaStream_t st) {
         cudaEventCreate(&open);
@@ -306,13 +452,16 @@ struct Trace {
         ev[cls].push_back({open, e});
         open = nullptr;
     }
+    std::vector<std::pair<int, double>> *detail = nullptr;  // (class, ms) per launch, in class order
     void finish(double *ms) {
-        for (int c = 0; c < 4; c++) {
-            ms[c] = 0;
+        if (detail) detail->clear();
+        for (int c = 0; c < 4; c++) ms[c] = 0;
+        for (int c = 0; c < NK; c++) {
             for (auto &pr : ev[c]) {
                 float t = 0;
                 cudaEventElapsedTime(&t, pr.first, pr.second);
-                ms[c] += t;
+                ms[coarse(c)] += t;
+                if (detail) detail->push_back({c, (double)t});
                 cudaEventDestroy(pr.first);
                 cudaEventDestroy(pr.second);
             }
@@ -336,25 +485,51 @@ int enqueue_numfact(b200_solver_t *s, cudaStream_t st, Trace *tr = nullptr) {
     for (size_t l = 0; l < s->levels.size(); l++) {
         const Level &Lv = s->levels[l];
         if (tr) tr->begin(st);
-        launch_diag<T>(s->facto, s->ds, s->d_lvl_cblk + Lv.c0, Lv.c1 - Lv.c0, L, U, s->d_thr, s->d_npiv, s->d_err, st);
+        launch_diag<T>(s->facto, s->ds, s->d_diag_list + s->lvl_ds0[l], s->lvl_ds1[l] - s->lvl_ds0[l], L, U,
+                       (T *)s->dTinv, s->d_toff, s->d_thr, s->d_npiv, s->d_err, st);
         if (tr) tr->end(1, st);
         launches++;
         const int nt = Lv.t1 - Lv.t0;
         if (tr) tr->begin(st);
         if (nt > 0) {
             const int TR = s->lvl_tr[l];
+            const T *ti = (const T *)s->dTinv;
             if (s->facto == FACTO_POTRF) {
-                launch_trsm<T>(s->ds, s->d_trsm + Lv.t0, nt, TR, Lv.nmax, L, L, 1, 0, st);
+                launch_trsm<T>(s->ds, s->d_trsm + Lv.t0, nt, TR, Lv.nmax, L, L, 1, ti, s->d_toff, 0, 0, 0, st);
             } else if (s->facto == FACTO_SYTRF) {
-                launch_trsm<T>(s->ds, s->d_trsm + Lv.t0, nt, TR, Lv.nmax, L, L, 0, 0, st);
+                launch_trsm<T>(s->ds, s->d_trsm + Lv.t0, nt, TR, Lv.nmax, L, L, 0, ti, s->d_toff, 0, 0, 1, st);
             } else {
-                launch_trsm<T>(s->ds, s->d_trsm + Lv.t0, nt, TR, Lv.nmax, L, L, 0, 0, st);
-                launch_trsm<T>(s->ds, s->d_trsm + Lv.t0, nt, TR, Lv.nmax, U, L, 1, 1, st);
+                launch_trsm<T>(s->ds, s->d_trsm + Lv.t0, nt, TR, Lv.nmax, L, L, 0, ti, s->d_toff, 1, 1, 0, st);
+                launch_trsm<T>(s->ds, s->d_trsm + Lv.t0, nt, TR, Lv.nmax, U, L, 1, ti, s->d_toff, 0, 1, 0, st);
                 launches++;
             }
             launches++;
         }
         if (tr) tr->end(2, st);
+        // sub-panel steps of the wide cblks
+        for (const auto &ss : s->lvl_steps[l]) {
+            if (tr) tr->begin(st);
+            launch_subpanel_diag<T>(s->facto, s->ds, s->d_subtask + ss.d0, ss.d1 - ss.d0, L, (T *)s->d_subwinv,
+                                    s->d_thr, s->d_npiv, s->d_err, st);
+            launches++;
+            if (tr) tr->end(4, st);
+            if (ss.t1 > ss.t0) {
+                if (tr) tr->begin(st);
+                launch_subpanel_trsm<T>(s->facto, s->ds, s->d_subtask + ss.t0, ss.t1 - ss.t0, L,
+                                        (const T *)s->d_subwinv, st);
+                launches++;
+                if (tr) tr->end(5, st);
+            }
+            if (ss.ntiles > 0) {
+                if (tr) tr->begin(st);
+                if (sizeof(T) == 8)
+                    launch_update_f64(s->ds, s->d_subupd + ss.u0, ss.u1 - ss.u0, ss.ntiles, (double *)L, (double *)U, st);
+                else
+                    launch_update_f32(s->ds, s->d_subupd + ss.u0, ss.u1 - ss.u0, ss.ntiles, (float *)L, (float *)U, st);
+                launches++;
+                if (tr) tr->end(6, st);
+            }
+        }
         if (tr) tr->begin(st);
         if (Lv.ntiles > 0) {
             if (sizeof(T) == 8)
@@ -365,6 +540,19 @@ int enqueue_numfact(b200_solver_t *s, cudaStream_t st, Trace *tr = nullptr) {
         }
         if (tr) tr->end(3, st);
     }
+    // inverses of the diagonal blocks for the solves (W_L of L; for LU also W_U of the stored U^T)
+    if (tr) tr->begin(st);
+    launch_copy_tile_inverse<T>(s->ds, s->d_inv_small, s->n_inv_small, (const T *)s->dTinv, s->d_toff, (T *)s->dWL,
+                                s->d_woff, 0, st);
+    launch_diag_inverse<T>(s->ds, s->d_inv_big, s->n_inv_big, L, (T *)s->dWL, s->d_woff, s->facto != FACTO_POTRF, st);
+    launches += 2;
+    if (s->facto == FACTO_GETRF) {
+        launch_copy_tile_inverse<T>(s->ds, s->d_inv_small, s->n_inv_small, (const T *)s->dTinv, s->d_toff,
+                                    (T *)s->dWU, s->d_woff, 1, st);
+        launch_diag_inverse<T>(s->ds, s->d_inv_big, s->n_inv_big, U, (T *)s->dWU, s->d_woff, 0, st);
+        launches += 2;
+    }
+    if (tr) tr->end(7, st);
     CU(cudaGetLastError());
     s->launches_fact = launches;
     return ERR_SUCCESS;
@@ -372,38 +560,51 @@ int enqueue_numfact(b200_solver_t *s, cudaStream_t st, Trace *tr = nullptr) {
 
 // ---------------------------------------------------------------- solve (permuted basis)
 
+// The two sweeps in the permuted basis.  x holds b on entry and the solution on
+// exit; aux (same shape) receives the forward solution.  Per level, forward:
+// aux_k = W_L,k x_k, then x[ancestor rows] -= P_k aux_k; backward (levels in
+// reverse): aux_k -= P_k^T x[ancestor rows], then x_k = W_B,k^T aux_k.
 template <typename T>
-int enqueue_sweeps(b200_solver_t *s, double *x, int64_t ldx, int nrhs, cudaStream_t st, int *launches) {
+int enqueue_sweeps(b200_solver_t *s, double *x, double *aux, int64_t ldx, int nrhs, cudaStream_t st, int *launches,
+                   Trace *tr = nullptr) {
     const T *L = (const T *)s->dL;
     const T *Ub = (s->facto == FACTO_GETRF) ? (const T *)s->dU : L;
+    const T *WL = (const T *)s->dWL;
+    const T *WB = (s->facto == FACTO_GETRF) ? (const T *)s->dWU : WL;
     const int nlev = (int)s->levels.size();
-    const int unitL = (s->facto != FACTO_POTRF);
     for (int l = 0; l < nlev; l++) {
-        const Level &Lv = s->levels[l];
-        launch_solve_diag<T>(s->ds, s->d_lvl_cblk + Lv.c0, Lv.c1 - Lv.c0, Lv.nmax, L, x, ldx, nrhs, 0, unitL, st);
-        const int ns = s->lvl_s1[l] - s->lvl_s0[l];
-        launch_solve_offdiag<T>(s->ds, s->d_stask + s->lvl_s0[l], ns, L, x, ldx, nrhs, 0, st);
+        const int nd = s->lvl_dt1[l] - s->lvl_dt0[l];
+        if (tr) tr->begin(st);
+        launch_solve_diag_inv<T>(s->ds, s->d_dtask + s->lvl_dt0[l], nd, WL, s->d_woff, x, aux, ldx, nrhs, 0, st);
+        if (tr) tr->end(1, st);
+        const int ns = s->lvl_st1[l] - s->lvl_st0[l];
+        if (tr) tr->begin(st);
+        launch_solve_tiles<T>(s->ds, s->d_stile + s->lvl_st0[l], ns, L, aux, x, ldx, nrhs, 0, st);
+        if (tr) tr->end(2, st);
         *launches += 1 + (ns > 0);
     }
     if (s->facto == FACTO_SYTRF) {
-        launch_solve_scale_diag<T>(s->ds, s->d_lvl_cblk, s->cblknbr, L, x, ldx, nrhs, st);
+        launch_solve_scale_diag<T>(s->ds, s->d_lvl_cblk, s->cblknbr, L, aux, ldx, nrhs, st);
         *launches += 1;
     }
-    const int unitU = (s->facto == FACTO_SYTRF);
     for (int l = nlev - 1; l >= 0; l--) {
-        const Level &Lv = s->levels[l];
-        const int ns = s->lvl_s1[l] - s->lvl_s0[l];
-        launch_solve_offdiag<T>(s->ds, s->d_stask + s->lvl_s0[l], ns, Ub, x, ldx, nrhs, 1, st);
-        launch_solve_diag<T>(s->ds, s->d_lvl_cblk + Lv.c0, Lv.c1 - Lv.c0, Lv.nmax, Ub, x, ldx, nrhs, 1, unitU, st);
+        const int ns = s->lvl_st1[l] - s->lvl_st0[l];
+        if (tr) tr->begin(st);
+        launch_solve_tiles<T>(s->ds, s->d_stile + s->lvl_st0[l], ns, Ub, x, aux, ldx, nrhs, 1, st);
+        if (tr) tr->end(2, st);
+        const int nd = s->lvl_dt1[l] - s->lvl_dt0[l];
+        if (tr) tr->begin(st);
+        launch_solve_diag_inv<T>(s->ds, s->d_dtask + s->lvl_dt0[l], nd, WB, s->d_woff, aux, x, ldx, nrhs, 1, st);
+        if (tr) tr->end(1, st);
         *launches += 1 + (ns > 0);
     }
     CU(cudaGetLastError());
     return ERR_SUCCESS;
 }
 
-int sweeps(b200_solver_t *s, double *x, int64_t ldx, int nrhs, cudaStream_t st, int *launches) {
-    return s->f32 ? enqueue_sweeps<float>(s, x, ldx, nrhs, st, launches)
-                  : enqueue_sweeps<double>(s, x, ldx, nrhs, st, launches);
+int sweeps(b200_solver_t *s, double *x, double *aux, int64_t ldx, int nrhs, cudaStream_t st, int *launches) {
+    return s->f32 ? enqueue_sweeps<float>(s, x, aux, ldx, nrhs, st, launches)
+                  : enqueue_sweeps<double>(s, x, aux, ldx, nrhs, st, launches);
 }
 
 // Full solve of device b (original ordering): permute, sweeps, permute back.
@@ -411,11 +612,11 @@ int sweeps(b200_solver_t *s, double *x, int64_t ldx, int nrhs, cudaStream_t st, 
 // when the call runs on the solver's own stream.
 int solve_device(b200_solver_t *s, int nrhs, double *b, int64_t ldb, cudaStream_t st) {
     const int n = s->n;
-    RET(ensure_ws(s, (size_t)n * nrhs));
-    double *xp = s->d_ws;
+    RET(ensure_ws(s, (size_t)2 * n * nrhs));
+    double *xp = s->d_ws, *aux = s->d_ws + (size_t)n * nrhs;
     int launches = 2;
     launch_permute(n, nrhs, s->d_peri, b, ldb, xp, n, 1, st);
-    RET(sweeps(s, xp, n, nrhs, st, &launches));
+    RET(sweeps(s, xp, aux, n, nrhs, st, &launches));
     launch_permute(n, nrhs, s->d_peri, xp, n, b, ldb, 0, st);
     CU(cudaGetLastError());
     s->launches_solve = launches;
@@ -437,9 +638,10 @@ struct RefineCtx {
         return ERR_SUCCESS;
     }
     // z <- M^{-1} z with the factor (sweeps only, already permuted)
+    double *aux = nullptr;  // n x nrhs scratch of the sweeps
     int spsv(double *z) {
         int l = 0;
-        int rc = sweeps(s, z, n, nrhs, st, &l);
+        int rc = sweeps(s, z, aux, n, nrhs, st, &l);
         s->kernel_launches += l;
         return rc;
     }
@@ -682,6 +884,8 @@ int refine_device(b200_solver_t *s, int nrhs, const double *b, int64_t ldb, doub
     if (method == B200_REFINE_SR) need += 2 * blk;
     else if (method == B200_REFINE_CG) need += 4 * blk;
     else need += (size_t)(2 * im + 1) * blk;
+    const size_t aux_at = need;
+    need += blk;  // scratch of the sweeps
     RET(ensure_ws(s, need));
     RET(ensure_scal(s, 2 * nrhs));
     double *bp = s->d_ws, *xp = s->d_ws + blk;
@@ -689,6 +893,7 @@ int refine_device(b200_solver_t *s, int nrhs, const double *b, int64_t ldb, doub
     launch_permute(n, nrhs, s->d_peri, x, ldx, xp, n, 1, st);
     s->kernel_launches += 3;
     RefineCtx c{s, st, n, nrhs};
+    c.aux = s->d_ws + aux_at;
     std::vector<double> be;
     int64_t it = 0;
     int rc;
@@ -828,7 +1033,7 @@ int b200_solver_create(const b200_symbol_t *sym, int facto, int precision, void 
     s->coefnbr = coef;
     int rc = ERR_SUCCESS;
     s->trsm_smem = configure_factor_kernels();
-    if (s->trsm_smem < 0 || configure_solve_kernels() < 0) {
+    if (s->trsm_smem < 0 || configure_solve_kernels() < 0 || configure_inverse_kernels() < 0) {
         fprintf(stderr, "pastix_b200: cannot configure the shared memory of the kernels\n");
         rc = ERR_INTERNAL;
     }
@@ -851,6 +1056,10 @@ int b200_solver_create(const b200_symbol_t *sym, int facto, int precision, void 
     }
     if (!rc) rc = dalloc((char **)&s->dL, (size_t)s->arena * s->esz);
     if (!rc && facto == FACTO_GETRF) rc = dalloc((char **)&s->dU, (size_t)s->arena * s->esz);
+    if (!rc) rc = dalloc((char **)&s->dWL, (size_t)s->winv_elems * s->esz);
+    if (!rc) rc = dalloc((char **)&s->dTinv, (size_t)s->tinv_elems * s->esz);
+    if (!rc) rc = dalloc((char **)&s->d_subwinv, (size_t)std::max<int64_t>(s->subwinv_slots, 1) * 64 * 64 * s->esz);
+    if (!rc && facto == FACTO_GETRF) rc = dalloc((char **)&s->dWU, (size_t)s->winv_elems * s->esz);
     if (!rc) rc = s->dmalloc(&s->d_thr, 1);
     if (!rc) rc = s->dmalloc(&s->d_npiv, 1);
     if (!rc) rc = s->dmalloc(&s->d_err, 1);
@@ -873,6 +1082,10 @@ int b200_solver_destroy(b200_solver_t *s) {
     for (void *p : s->dev_allocs) cudaFree(p);
     if (s->dL) cudaFree(s->dL);
     if (s->dU) cudaFree(s->dU);
+    if (s->dWL) cudaFree(s->dWL);
+    if (s->dTinv) cudaFree(s->dTinv);
+    if (s->d_subwinv) cudaFree(s->d_subwinv);
+    if (s->dWU) cudaFree(s->dWU);
     if (s->d_colptr) cudaFree(s->d_colptr);
     if (s->d_rowtab) cudaFree(s->d_rowtab);
     if (s->d_Lv) cudaFree(s->d_Lv);
@@ -998,6 +1211,7 @@ int b200_numfact_trace(b200_solver_t *s, double epsilon_magn_ctrl, double *ms, d
     int64_t piv = 0;
     RET(b200_numfact(s, epsilon_magn_ctrl, &piv));  // sets the threshold and checks the factorization
     Trace tr;
+    tr.detail = &s->trace_detail;
     int rc = s->f32 ? enqueue_numfact<float>(s, s->st, &tr) : enqueue_numfact<double>(s, s->st, &tr);
     if (rc) return rc;
     CU(cudaStreamSynchronize(s->st));
@@ -1008,6 +1222,49 @@ int b200_numfact_trace(b200_solver_t *s, double epsilon_magn_ctrl, double *ms, d
         for (int c = 1; c < 4; c++) flops[c] = s->flops_class[c];
     }
     return ERR_SUCCESS;
+}
+
+int b200_solve_trace(b200_solver_t *s, int64_t nrhs, double *ms, double *bytes) {
+    if (!s || !s->factored || nrhs <= 0 || !ms) return ERR_BADPARAM;
+    const int n = s->n;
+    RET(ensure_ws(s, (size_t)2 * n * nrhs));
+    double *xp = s->d_ws, *aux = s->d_ws + (size_t)n * nrhs;
+    CU(cudaMemsetAsync(xp, 0, (size_t)n * nrhs * sizeof(double), s->st));
+    Trace tr;
+    tr.detail = &s->trace_detail;
+    int launches = 0;
+    tr.begin(s->st);
+    tr.end(0, s->st);
+    int rc = s->f32 ? enqueue_sweeps<float>(s, xp, aux, n, (int)nrhs, s->st, &launches, &tr)
+                    : enqueue_sweeps<double>(s, xp, aux, n, (int)nrhs, s->st, &launches, &tr);
+    if (rc) return rc;
+    CU(cudaStreamSynchronize(s->st));
+    s->kernel_launches += launches;
+    tr.finish(ms);
+    if (bytes) {
+        // algorithmic traffic: every factor entry once per sweep (LU: L then U) + vectors
+        double fb = 0, db = 0;
+        for (int k = 0; k < s->cblknbr; k++) {
+            const double nc = s->ncols[k];
+            db += nc * nc * 0.5;
+            fb += (s->stride[k] - nc) * nc;
+        }
+        bytes[0] = 0;
+        bytes[1] = 2.0 * db * s->esz + 4.0 * n * nrhs * 8.0;
+        bytes[2] = 2.0 * fb * s->esz + 4.0 * (double)n * nrhs * 8.0;
+        bytes[3] = 0;
+    }
+    return ERR_SUCCESS;
+}
+
+int64_t b200_trace_launches(b200_solver_t *s, double *ms, int32_t *cls, int64_t cap) {
+    if (!s) return -ERR_BADPARAM;
+    const int64_t cnt = (int64_t)s->trace_detail.size();
+    for (int64_t i = 0; i < cnt && i < cap; i++) {
+        if (ms) ms[i] = s->trace_detail[i].second;
+        if (cls) cls[i] = s->trace_detail[i].first;
+    }
+    return cnt;
 }
 
 int b200_solve_device(b200_solver_t *s, int64_t nrhs, double *d_b, int64_t ldb, void *stream) {
@@ -1021,19 +1278,21 @@ int b200_solve_device_noalloc(b200_solver_t *s, int64_t nrhs, double *d_b, int64
     if (!s || !s->factored || nrhs < 0 || ldb < s->n || (!d_b && nrhs)) return ERR_BADPARAM;
     if (nrhs == 0) return ERR_SUCCESS;
     const int n = s->n;
-    if ((uint64_t)n * (uint64_t)nrhs > (uint64_t)B200_NOALLOC_SCRATCH_DOUBLES) {
+    if (2 * (uint64_t)n * (uint64_t)nrhs > (uint64_t)B200_NOALLOC_SCRATCH_DOUBLES) {
         fprintf(stderr,
-                "pastix_b200: b200_solve_device_noalloc: n * nrhs = %lld exceeds its fixed scratch of %d doubles\n",
-                (long long)n * (long long)nrhs, B200_NOALLOC_SCRATCH_DOUBLES);
+                "pastix_b200: b200_solve_device_noalloc: 2 * n * nrhs = %lld exceeds its fixed scratch of %d doubles\n",
+                2LL * n * (long long)nrhs, B200_NOALLOC_SCRATCH_DOUBLES);
         return ERR_BADPARAM;
     }
     double *xp = nullptr;
     RET(noalloc_scratch(&xp));
+    double *aux = xp + (size_t)n * nrhs;
     cudaStream_t st = stream ? (cudaStream_t)stream : s->st;
-    // every entry of the scratch used here is written by the permutation before it is read
+    // every entry of the scratch used here is written before it is read: the first half
+    // by the permutation, the second by the forward diagonal products
     int launches = 2;
     launch_permute(n, (int)nrhs, s->d_peri, d_b, ldb, xp, n, 1, st);
-    RET(sweeps(s, xp, n, (int)nrhs, st, &launches));
+    RET(sweeps(s, xp, aux, n, (int)nrhs, st, &launches));
     launch_permute(n, (int)nrhs, s->d_peri, xp, n, d_b, ldb, 0, st);
     CU(cudaGetLastError());
     s->kernel_launches += launches;
@@ -1161,7 +1420,7 @@ int b200_stats(b200_solver_t *s, double *out) {
     out[2] = s->t_refine;
     out[3] = (double)s->last_npiv;
     out[4] = s->thr_used;
-    out[5] = (double)s->arena * s->esz * (s->dU ? 2 : 1);
+    out[5] = ((double)s->arena + s->winv_elems) * s->esz * (s->dU ? 2 : 1);
     out[6] = (double)s->levels.size();
     out[7] = s->launches_fact;
     out[8] = s->launches_solve;

@@ -24,7 +24,7 @@ _lib = None
 
 # exported symbols, in the order of include/pastix_b200.h
 SYMBOLS = ["b200_solver_create", "b200_solver_destroy", "b200_bcsc_load", "b200_numfact", "b200_numfact_trace",
-           "b200_solve",
+           "b200_solve_trace", "b200_trace_launches", "b200_solve",
            "b200_solve_device", "b200_solve_device_noalloc", "b200_refine", "b200_refine_device", "b200_spmv", "b200_factor_download",
            "b200_stats", "b200_strerror"]
 
@@ -52,6 +52,9 @@ def lib():
         L.b200_numfact.argtypes = [_P, C.c_double, C.POINTER(_I64)]
         L.b200_numfact_trace.argtypes = [_P, C.c_double, _P, _P]
         L.b200_solve.argtypes = [_P, _I64, _P, _I64]
+        L.b200_solve_trace.argtypes = [_P, _I64, _P, _P]
+        L.b200_trace_launches.argtypes = [_P, _P, _P, _I64]
+        L.b200_trace_launches.restype = _I64
         L.b200_solve_device.argtypes = [_P, _I64, _P, _I64, _P]
         L.b200_solve_device_noalloc.argtypes = [_P, _I64, _P, _I64, _P]
         L.b200_refine.argtypes = [_P, _I64, _P, _I64, _P, _I64, C.c_int, C.c_double, _I64, _I64,
@@ -126,6 +129,22 @@ class Solver:
         check(lib().b200_numfact_trace(self.h, epsilon_magn_ctrl, _p(ms), _p(fl)), "b200_numfact_trace")
         names = ["scatter", "diag", "trsm", "update"]
         return {n: dict(ms=float(ms[i]), flops=float(fl[i])) for i, n in enumerate(names)}
+
+    def solve_trace(self, nrhs: int) -> dict:
+        """Device time (ms) and algorithmic bytes of the sweeps of one nrhs-column solve."""
+        ms = np.zeros(4)
+        by = np.zeros(4)
+        check(lib().b200_solve_trace(self.h, nrhs, _p(ms), _p(by)), "b200_solve_trace")
+        return {"diag": dict(ms=float(ms[1]), bytes=float(by[1])),
+                "offdiag": dict(ms=float(ms[2]), bytes=float(by[2]))}
+
+    def trace_launches(self):
+        """(class, ms) of every launch of the last trace, grouped by class."""
+        cnt = int(lib().b200_trace_launches(self.h, None, None, 0))
+        ms = np.zeros(max(cnt, 1))
+        cls = np.zeros(max(cnt, 1), dtype=np.int32)
+        lib().b200_trace_launches(self.h, _p(ms), _p(cls), cnt)
+        return cls[:cnt], ms[:cnt]
 
     def solve(self, b: np.ndarray) -> np.ndarray:
         x = np.asfortranarray(np.array(b, dtype=np.float64).reshape(self.n, -1))

@@ -59,7 +59,7 @@ def test_noalloc_refuses_sizes_beyond_its_scratch():
     A = M.laplacian(16, 16, 16, 7, 6.0)
     s = factored("potrf", A)
     n = A.n
-    nrhs = SCRATCH_DOUBLES // n + 1
+    nrhs = SCRATCH_DOUBLES // (2 * n) + 1  # a call needs 2 * n * nrhs doubles of scratch
     d = torch.ones((nrhs, n), dtype=torch.float64, device="cuda")
     torch.cuda.synchronize()
     rc = native.lib().b200_solve_device_noalloc(s.h, nrhs, ctypes.c_void_p(d.data_ptr()), n, None)
