@@ -531,116 +531,122 @@ __device__ void invert_lower_ld(const T *t, int ldt, T *w, int ldw, int pb, int 
     }
 }
 
-// 64x64 diagonal tile of a sub-panel, blocked 2 x 32:
-//   L11 = fact(A11); W11 = L11^{-1};  X21 = A21 L11^{-T}  (LDL^T: L21 = X21 D1^{-1});
-//   A22 -= L21 X21^T;  L22 = fact(A22); W22 = L22^{-1};  W21 = -W22 L21 W11.
-// The tile and its inverse W (64x64, lower) are written back.
+// 64x64 diagonal tile of a sub-panel, held in registers: thread t owns row
+// i = t & 63, columns q*16 .. q*16+15 (q = t >> 6).  Right-looking factorization
+// (core_zpotf2sp / core_zsytf2sp), one barrier per column: the threads owning
+// column c publish it to a double-buffered shared vector and every thread
+// updates its own elements.  Then W = L^{-1} by the same scheme (row c of W is
+// final once divided by L[c][c]; rows below subtract L[i][c] W[c][:]).
 template <typename T, int FACTO>
 __global__ void __launch_bounds__(256) subpanel_diag_kernel(DevSym s, const SubTask *__restrict__ tasks, T *L,
                                                             T *winv, const double *__restrict__ thr_ptr,
                                                             unsigned long long *npiv, int *err) {
-    extern __shared__ __align__(16) unsigned char sp_smem[];
-    T *a = reinterpret_cast<T *>(sp_smem);   // 64 x 64 tile (ld SPP)
-    T *w = a + SP * SPP;                     // 64 x 64 inverse (ld SPP)
-    __shared__ T x21[32 * 33];               // X21 (LDL^T: L21 D1), then L21 W11
+    __shared__ T col[2][SP];
+    __shared__ T roww[2][SP];
+    __shared__ T dg[SP];
     __shared__ int s_piv, s_err;
     const SubTask tk = tasks[blockIdx.x];
     const int k = tk.k, c0 = tk.c0, ld = s.ld[k];
     const int n = s.ncols[k], wd = min(SP, n - c0);
-    const int w1 = min(32, wd), w2 = wd - w1;
     const double thr = *thr_ptr;
     T *A = L + s.off[k] + c0 + (size_t)c0 * ld;
-    const int tid = threadIdx.x, nth = blockDim.x, lane = tid & 31, warp = tid >> 5;
+    const int tid = threadIdx.x;
+    const int i = tid & 63, q = tid >> 6, j0 = q * 16;
     if (tid == 0) { s_piv = 0; s_err = 0; }
-    for (int idx = tid; idx < SP * SP; idx += nth) {
-        const int i = idx & 63, j = idx >> 6;
-        a[i + j * SPP] = (i < wd && j < wd && i >= j) ? A[i + (size_t)j * ld] : (T)0;
-        w[i + j * SPP] = 0;
+    T r[16];
+#pragma unroll
+    for (int u = 0; u < 16; u++) {
+        const int j = j0 + u;
+        r[u] = (i < wd && j < wd && i >= j) ? A[i + (size_t)j * ld] : (T)0;
     }
     __syncthreads();
-    if (warp == 0) {
-        factor_tile_ld<T, FACTO>(a, SPP, w1, lane, thr, &s_piv, &s_err);
-        invert_lower_ld<T>(a, SPP, w, SPP, w1, lane, FACTO != FACTO_POTRF);
+    // ---- factorization
+    for (int c = 0; c < wd; c++) {
+        const int b = c & 1;
+        if (q == (c >> 4)) {  // column c (rows < c hold zeros); select without runtime indexing
+            T v = 0;
+#pragma unroll
+            for (int u = 0; u < 16; u++)
+                if (u == (c & 15)) v = r[u];
+            col[b][i] = v;
+        }
+        __syncthreads();
+        T d = col[b][c];
+        bool replaced = false;
+        if (fabs((double)d) < thr) {
+            d = (FACTO == FACTO_POTRF) ? (T)thr : ((d < (T)0) ? (T)(-thr) : (T)thr);
+            replaced = true;
+        }
+        bool negative = false;
+        if (FACTO == FACTO_POTRF) {
+            if (d < (T)0) { negative = true; d = -d; }
+            d = sqrt(d);
+        }
+        if (tid == 0) {
+            if (replaced) s_piv++;
+            if (negative) s_err = 1;
+        }
+        const T inv = (T)1 / d;
+        const T li = (i > c && i < wd) ? col[b][i] * inv : (T)0;
+        if (q == (c >> 4) && i >= c) {
+            const T nv = (i == c) ? d : li;
+#pragma unroll
+            for (int u = 0; u < 16; u++)
+                if (u == (c & 15)) r[u] = nv;
+        }
+#pragma unroll
+        for (int u = 0; u < 16; u++) {
+            const int j = j0 + u;
+            if (j > c && j <= i && i < wd) {
+                const T lj = col[b][j] * inv;  // l_j (POTRF) ; LDL^T: d l_i l_j = l_i * col[j]
+                r[u] -= (FACTO == FACTO_POTRF) ? li * lj : li * col[b][j];
+            }
+        }
     }
+    // ---- inverse W = L^{-1} (unit diagonal for LDL^T)
+    if (q == (i >> 4) && i < wd) {
+        T v = 0;
+#pragma unroll
+        for (int u = 0; u < 16; u++)
+            if (u == (i & 15)) v = r[u];
+        dg[i] = (FACTO == FACTO_POTRF) ? v : (T)1;
+    }
+    T w[16];
+#pragma unroll
+    for (int u = 0; u < 16; u++) w[u] = (j0 + u == i && i < wd) ? (T)1 : (T)0;
     __syncthreads();
-    if (w2 > 0) {
-        // X21 = A21 W11^T (32 x 32): thread -> (row i, 4 columns)
-        {
-            const int i = tid & 31, cq = (tid >> 5) * 4;
-            T v[4];
+    for (int c = 0; c < wd; c++) {
+        const int b = c & 1;
+        const T invd = (T)1 / dg[c];
+        if (i == c) {
 #pragma unroll
-            for (int q = 0; q < 4; q++) {
-                const int c = cq + q;
-                T acc = 0;
-                if (i < w2 && c < w1)
-                    for (int l = 0; l <= c; l++) acc += a[(32 + i) + l * SPP] * w[c + l * SPP];
-                v[q] = acc;
-            }
-            __syncthreads();
-#pragma unroll
-            for (int q = 0; q < 4; q++) {
-                const int c = cq + q;
-                x21[i + c * 33] = v[q];
-                if (i < w2 && c < w1)
-                    a[(32 + i) + c * SPP] = (FACTO == FACTO_SYTRF) ? v[q] / a[c * (SPP + 1)] : v[q];
+            for (int u = 0; u < 16; u++) {
+                w[u] *= invd;
+                roww[b][j0 + u] = w[u];
             }
         }
-        __syncthreads();
-        // A22 -= L21 X21^T (lower): thread -> (row i, 4 columns)
-        {
-            const int i = tid & 31, jq = (tid >> 5) * 4;
+        if (q == (c >> 4)) {
+            T v = 0;
 #pragma unroll
-            for (int q = 0; q < 4; q++) {
-                const int j = jq + q;
-                if (i < w2 && j <= i) {
-                    T acc = 0;
-                    for (int c = 0; c < w1; c++) acc += a[(32 + i) + c * SPP] * x21[j + c * 33];
-                    a[(32 + i) + (32 + j) * SPP] -= acc;
-                }
-            }
+            for (int u = 0; u < 16; u++)
+                if (u == (c & 15)) v = r[u];
+            col[b][i] = (i > c && i < wd) ? v : (T)0;
         }
         __syncthreads();
-        if (warp == 0) {
-            factor_tile_ld<T, FACTO>(a + 32 * (SPP + 1), SPP, w2, lane, thr, &s_piv, &s_err);
-            invert_lower_ld<T>(a + 32 * (SPP + 1), SPP, w + 32 * (SPP + 1), SPP, w2, lane, FACTO != FACTO_POTRF);
+        if (i > c && i < wd) {
+            const T lic = col[b][i];
+#pragma unroll
+            for (int u = 0; u < 16; u++) w[u] -= lic * roww[b][j0 + u];
         }
-        __syncthreads();
-        // T21 = L21 W11 -> x21 ; W21 = -W22 T21
-        {
-            const int i = tid & 31, cq = (tid >> 5) * 4;
-            T v[4];
-#pragma unroll
-            for (int q = 0; q < 4; q++) {
-                const int c = cq + q;
-                T acc = 0;
-                if (i < w2 && c < w1)
-                    for (int l = c; l < w1; l++) acc += a[(32 + i) + l * SPP] * w[l + c * SPP];
-                v[q] = acc;
-            }
-            __syncthreads();
-#pragma unroll
-            for (int q = 0; q < 4; q++) x21[i + (cq + q) * 33] = v[q];
-            __syncthreads();
-#pragma unroll
-            for (int q = 0; q < 4; q++) {
-                const int c = cq + q;
-                T acc = 0;
-                if (i < w2 && c < w1)
-                    for (int m = 0; m <= i; m++) acc += w[(32 + i) + (32 + m) * SPP] * x21[m + c * 33];
-                v[q] = -acc;
-            }
-#pragma unroll
-            for (int q = 0; q < 4; q++)
-                if (i < w2 && cq + q < w1) w[(32 + i) + (cq + q) * SPP] = v[q];
-        }
-        __syncthreads();
     }
     T *W = winv + (size_t)tk.pos * SP * SP;
-    for (int idx = tid; idx < SP * SP; idx += nth) {
-        const int i = idx & 63, j = idx >> 6;
-        if (i < wd && j < wd && i >= j) A[i + (size_t)j * ld] = a[i + j * SPP];
-        W[idx] = w[i + j * SPP];
+#pragma unroll
+    for (int u = 0; u < 16; u++) {
+        const int j = j0 + u;
+        if (i < wd && j < wd && i >= j) A[i + (size_t)j * ld] = r[u];
+        W[i + j * SP] = (i < wd && j < wd && i >= j) ? w[u] : (T)0;
     }
+    __syncthreads();
     if (tid == 0) {
         if (s_piv) atomicAdd(npiv, (unsigned long long)s_piv);
         if (s_err) atomicExch(err, 1);
@@ -694,11 +700,10 @@ template <typename T>
 void launch_subpanel_diag(int facto, const DevSym &s, const SubTask *tasks, int ntasks, T *L, T *winv,
                           const double *thr, unsigned long long *npiv, int *err, cudaStream_t st) {
     if (ntasks <= 0) return;
-    const size_t smem = 2 * SP * SPP * sizeof(T);
     if (facto == FACTO_POTRF)
-        subpanel_diag_kernel<T, FACTO_POTRF><<<ntasks, 256, smem, st>>>(s, tasks, L, winv, thr, npiv, err);
+        subpanel_diag_kernel<T, FACTO_POTRF><<<ntasks, 256, 0, st>>>(s, tasks, L, winv, thr, npiv, err);
     else
-        subpanel_diag_kernel<T, FACTO_SYTRF><<<ntasks, 256, smem, st>>>(s, tasks, L, winv, thr, npiv, err);
+        subpanel_diag_kernel<T, FACTO_SYTRF><<<ntasks, 256, 0, st>>>(s, tasks, L, winv, thr, npiv, err);
 }
 
 template <typename T>
@@ -997,9 +1002,7 @@ static int raise_smem(K kernel) {
 int configure_factor_kernels() {
     int lim = 1 << 30;
     int v;
-    if (raise_smem(subpanel_diag_kernel<double, FACTO_POTRF>) < 0 || raise_smem(subpanel_diag_kernel<double, FACTO_SYTRF>) < 0 ||
-        raise_smem(subpanel_diag_kernel<float, FACTO_POTRF>) < 0 || raise_smem(subpanel_diag_kernel<float, FACTO_SYTRF>) < 0 ||
-        raise_smem(subpanel_trsm_kernel<double, FACTO_POTRF>) < 0 || raise_smem(subpanel_trsm_kernel<double, FACTO_SYTRF>) < 0 ||
+    if (raise_smem(subpanel_trsm_kernel<double, FACTO_POTRF>) < 0 || raise_smem(subpanel_trsm_kernel<double, FACTO_SYTRF>) < 0 ||
         raise_smem(subpanel_trsm_kernel<float, FACTO_POTRF>) < 0 || raise_smem(subpanel_trsm_kernel<float, FACTO_SYTRF>) < 0)
         return -1;
     if ((v = raise_smem(update_f64_kernel)) < UPD_F64_SMEM) return -1;
