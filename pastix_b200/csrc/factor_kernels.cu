@@ -361,7 +361,7 @@ __global__ void __launch_bounds__(256) diag_factor_kernel(DevSym s, const int *_
     }
     if (tid == 0) {
         if (s_piv) atomicAdd(npiv, (unsigned long long)s_piv);
-        if (s_err) atomicExch(err, 1);
+        if (s_err) atomicOr(err, 1);
     }
 }
 
@@ -649,7 +649,7 @@ __global__ void __launch_bounds__(256) subpanel_diag_kernel(DevSym s, const SubT
     __syncthreads();
     if (tid == 0) {
         if (s_piv) atomicAdd(npiv, (unsigned long long)s_piv);
-        if (s_err) atomicExch(err, 1);
+        if (s_err) atomicOr(err, 1);
     }
 }
 

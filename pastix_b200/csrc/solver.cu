@@ -5,6 +5,7 @@
 #include <chrono>
 #include <cmath>
 #include <cstdio>
+#include <cstdlib>
 #include <cstring>
 #include <map>
 #include <mutex>
@@ -102,12 +103,22 @@ struct b200_solver_s {
         int t0, t1;   // subpanel TRSM tasks
         int u0, u1;   // internal updates
         int ntiles;
+        int tu0, tu1;  // internal updates on the tensor cores
+        int tntiles;
     };
     std::vector<std::vector<SubStep>> lvl_steps;
     SubTask *d_subtask = nullptr;
     Upd *d_subupd = nullptr;
     void *d_subwinv = nullptr;
     int64_t subwinv_slots = 0;
+    // FP32 updates on the tensor cores (precision TF32 / TF32X3); updates below the
+    // size thresholds stay on the SIMT kernel
+    bool use_tc = false;
+    int tc_min_k = 32, tc_min_m = 64;
+    Upd *d_tcupd = nullptr;
+    std::vector<int> lvl_tc_u0, lvl_tc_u1, lvl_tc_tiles;
+    std::vector<char> tc_wanted;          // cblks whose panels the tensor-core updates read
+    void *d_mapL = nullptr, *d_mapU = nullptr;
     std::vector<int> lvl_tr;            // TRSM rows per task of each level
     std::vector<int> lvl_s0, lvl_s1;    // solve row tasks of each level
     int nmax_all = 0;
@@ -188,6 +199,24 @@ int build_schedule(b200_solver_t *s) {
     std::vector<int> diag_list;
     std::vector<SubTask> subtasks;
     std::vector<Upd> subupds;
+    std::vector<Upd> tcupds;
+    s->tc_wanted.assign(N, 0);
+    s->lvl_tc_u0.assign(nlev, 0);
+    s->lvl_tc_u1.assign(nlev, 0);
+    s->lvl_tc_tiles.assign(nlev, 0);
+    auto tc_ok = [&](const Upd &u) {
+        return s->use_tc && !(u.flags & UPD_SCALE_D) && u.K >= s->tc_min_k && u.M >= s->tc_min_m &&
+               (u.colK0 == 0 || u.K % 32 == 0);
+    };
+    // tensor-core tiles: 128 x 64 from the rows rounded down to a multiple of 4
+    auto push_tc = [&](Upd u, int &t0) {
+        u.tiles_m = (u.M + (u.rowA0 & 3) + 127) / 128;
+        u.tiles_n = (u.N + (u.rowB0 & 3) + 63) / 64;
+        u.tile0 = t0;
+        t0 += u.tiles_m * u.tiles_n;
+        s->tc_wanted[u.k] = 1;
+        tcupds.push_back(u);
+    };
     s->lvl_ds0.assign(nlev, 0);
     s->lvl_ds1.assign(nlev, 0);
     s->lvl_steps.assign(nlev, {});
@@ -253,7 +282,8 @@ int build_schedule(b200_solver_t *s) {
                 }
                 ss.t1 = (int)subtasks.size();
                 ss.u0 = (int)subupds.size();
-                int t0 = 0;
+                ss.tu0 = (int)tcupds.size();
+                int t0 = 0, tt0 = 0;
                 for (auto &m : members) {
                     const int k = m.first, n = s->ncols[k];
                     if (c0 + 64 >= n) continue;
@@ -269,6 +299,10 @@ int build_schedule(b200_solver_t *s) {
                     u.K = 64;
                     u.colbase = c0 + 64;
                     u.flags = UPD_SYM | (s->facto == FACTO_SYTRF ? UPD_SCALE_D : 0);
+                    if (tc_ok(u)) {
+                        push_tc(u, tt0);
+                        continue;
+                    }
                     u.tiles_m = (u.M + 63) / 64;
                     u.tiles_n = (u.N + 63) / 64;
                     u.tile0 = t0;
@@ -277,6 +311,8 @@ int build_schedule(b200_solver_t *s) {
                 }
                 ss.u1 = (int)subupds.size();
                 ss.ntiles = t0;
+                ss.tu1 = (int)tcupds.size();
+                ss.tntiles = tt0;
                 s->lvl_steps[l].push_back(ss);
             }
         }
@@ -305,7 +341,8 @@ int build_schedule(b200_solver_t *s) {
             }
         }
         L.u0 = (int)upds.size();
-        int tile0 = 0;
+        s->lvl_tc_u0[l] = (int)tcupds.size();
+        int tile0 = 0, tc_tile0 = 0;
         int64_t flops = 0;
         for (int i = L.c0; i < L.c1; i++) {
             const int k = lvl_cblk[i];
@@ -339,23 +376,29 @@ int build_schedule(b200_solver_t *s) {
                     u.N = nj;
                     u.K = nc;
                     u.colbase = s->frow[j] - s->fcol[f];
+                    // useful work: the lower triangle of the diagonal square for symmetric updates
+                    const double mn = (u.flags & UPD_SYM) ? (double)u.N * (u.M - u.N) + 0.5 * u.N * (u.N + 1.0)
+                                                          : (double)u.M * u.N;
+                    flops += (int64_t)(2.0 * mn * u.K);
+                    s->flops_class[3] += 2.0 * mn * u.K;
+                    if (tc_ok(u)) {
+                        push_tc(u, tc_tile0);
+                        continue;
+                    }
                     u.tiles_m = (u.M + 63) / 64;
                     u.tiles_n = (u.N + 63) / 64;
                     const int nt = (u.flags & UPD_SYM) ? u.tiles_n * u.tiles_m - u.tiles_n * (u.tiles_n - 1) / 2
                                                        : u.tiles_n * u.tiles_m;
                     u.tile0 = tile0;
                     tile0 += nt;
-                    // useful work: the lower triangle of the diagonal square for symmetric updates
-                    const double mn = (u.flags & UPD_SYM) ? (double)u.N * (u.M - u.N) + 0.5 * u.N * (u.N + 1.0)
-                                                          : (double)u.M * u.N;
-                    flops += (int64_t)(2.0 * mn * u.K);
-                    s->flops_class[3] += 2.0 * mn * u.K;
                     upds.push_back(u);
                 }
             }
         }
         L.u1 = (int)upds.size();
         L.ntiles = tile0;
+        s->lvl_tc_u1[l] = (int)tcupds.size();
+        s->lvl_tc_tiles[l] = tc_tile0;
         L.flops = flops;
         s->total_tiles += tile0;
         // reset the per-level source counters
@@ -404,6 +447,7 @@ int build_schedule(b200_solver_t *s) {
     s->tinv_elems = tpos;
     RET(s->dupload(&s->d_toff, toff));
     RET(s->dupload(&s->d_upd, upds));
+    RET(s->dupload(&s->d_tcupd, tcupds));
     return ERR_SUCCESS;
 }
 
@@ -435,10 +479,11 @@ int ensure_scal(b200_solver_t *s, int count) {
 // blocks, 2 panel TRSM, 3 GEMM-scatter updates.
 // Fine kernel kinds recorded in the per-launch detail; ids 0-3 are the classes
 // above, 4 subpanel diagonal, 5 subpanel TRSM, 6 subpanel internal update,
-// 7 diagonal-block inverses (summed into classes 1, 2, 2, 1).
+// 7 diagonal-block inverses, 8 updates on the tensor cores (summed into classes
+// 1, 2, 2, 1, 3).
 struct Trace {
-    static constexpr int NK = 8;
-    static int coarse(int c) { return c < 4 ? c : (c == 4 || c == 7) ? 1 : 2; }
+    static constexpr int NK = 9;
+    static int coarse(int c) { return c < 4 ? c : (c == 4 || c == 7) ? 1 : c == 8 ? 3 : 2; }
     std::vector<std::pair<cudaEvent_t, cudaEvent_t>> ev[NK];
     cudaEvent_t open = nullptr;
     void begin(cudaStream_t st) {
@@ -529,6 +574,13 @@ int enqueue_numfact(b200_solver_t *s, cudaStream_t st, Trace *tr = nullptr) {
                 launches++;
                 if (tr) tr->end(6, st);
             }
+            if (ss.tntiles > 0) {
+                if (tr) tr->begin(st);
+                launch_update_tc(s->ds, s->d_tcupd + ss.tu0, ss.tu1 - ss.tu0, ss.tntiles, s->d_mapL, s->d_mapU,
+                                 (float *)L, (float *)U, s->prec == B200_PREC_TF32X3, s->d_err, st);
+                launches++;
+                if (tr) tr->end(8, st);
+            }
         }
         if (tr) tr->begin(st);
         if (Lv.ntiles > 0) {
@@ -539,6 +591,14 @@ int enqueue_numfact(b200_solver_t *s, cudaStream_t st, Trace *tr = nullptr) {
             launches++;
         }
         if (tr) tr->end(3, st);
+        if (s->lvl_tc_tiles[l] > 0) {
+            if (tr) tr->begin(st);
+            launch_update_tc(s->ds, s->d_tcupd + s->lvl_tc_u0[l], s->lvl_tc_u1[l] - s->lvl_tc_u0[l],
+                             s->lvl_tc_tiles[l], s->d_mapL, s->d_mapU, (float *)L, (float *)U,
+                             s->prec == B200_PREC_TF32X3, s->d_err, st);
+            launches++;
+            if (tr) tr->end(8, st);
+        }
     }
     // inverses of the diagonal blocks for the solves (W_L of L; for LU also W_U of the stored U^T)
     if (tr) tr->begin(st);
@@ -973,6 +1033,9 @@ int b200_solver_create(const b200_symbol_t *sym, int facto, int precision, void 
     s->prec = precision;
     s->f32 = precision != B200_PREC_FP64;
     s->esz = s->f32 ? 4 : 8;
+    s->use_tc = precision == B200_PREC_TF32 || precision == B200_PREC_TF32X3;
+    if (const char *e = getenv("B200_TC_MIN_K")) s->tc_min_k = std::max(1, atoi(e));
+    if (const char *e = getenv("B200_TC_MIN_M")) s->tc_min_m = std::max(1, atoi(e));
     if (stream) {
         s->st = (cudaStream_t)stream;
     } else {
@@ -1033,7 +1096,8 @@ int b200_solver_create(const b200_symbol_t *sym, int facto, int precision, void 
     s->coefnbr = coef;
     int rc = ERR_SUCCESS;
     s->trsm_smem = configure_factor_kernels();
-    if (s->trsm_smem < 0 || configure_solve_kernels() < 0 || configure_inverse_kernels() < 0) {
+    if (s->trsm_smem < 0 || configure_solve_kernels() < 0 || configure_inverse_kernels() < 0 ||
+        (s->use_tc && configure_tc_kernels() < 0)) {
         fprintf(stderr, "pastix_b200: cannot configure the shared memory of the kernels\n");
         rc = ERR_INTERNAL;
     }
@@ -1060,6 +1124,21 @@ int b200_solver_create(const b200_symbol_t *sym, int facto, int precision, void 
     if (!rc) rc = dalloc((char **)&s->dTinv, (size_t)s->tinv_elems * s->esz);
     if (!rc) rc = dalloc((char **)&s->d_subwinv, (size_t)std::max<int64_t>(s->subwinv_slots, 1) * 64 * 64 * s->esz);
     if (!rc && facto == FACTO_GETRF) rc = dalloc((char **)&s->dWU, (size_t)s->winv_elems * s->esz);
+    if (!rc && s->use_tc) {
+        for (int side = 0; side < (facto == FACTO_GETRF ? 2 : 1) && !rc; side++) {
+            std::vector<CUtensorMap> maps;
+            if (encode_panel_maps(s->off, s->ld, s->ncols, s->tc_wanted, (float *)(side ? s->dU : s->dL), maps)) {
+                fprintf(stderr, "pastix_b200: cannot encode the tensor maps of the factor panels\n");
+                rc = ERR_INTERNAL;
+                break;
+            }
+            CUtensorMap *d = nullptr;
+            rc = s->dmalloc(&d, maps.size());
+            if (!rc && cudaMemcpy(d, maps.data(), maps.size() * sizeof(CUtensorMap), cudaMemcpyHostToDevice) != cudaSuccess)
+                rc = ERR_INTERNAL;
+            (side ? s->d_mapU : s->d_mapL) = d;
+        }
+    }
     if (!rc) rc = s->dmalloc(&s->d_thr, 1);
     if (!rc) rc = s->dmalloc(&s->d_npiv, 1);
     if (!rc) rc = s->dmalloc(&s->d_err, 1);
@@ -1198,10 +1277,9 @@ int b200_numfact(b200_solver_t *s, double epsilon_magn_ctrl, int64_t *nbpivots) 
     s->t_fact = ms;
     s->last_npiv = (int64_t)piv;
     if (nbpivots) *nbpivots = (int64_t)piv;
-    if (err) {
-        fprintf(stderr, "pastix_b200: negative diagonal term in the Cholesky factorization\n");
-        return ERR_INTERNAL;
-    }
+    if (err & 2) fprintf(stderr, "pastix_b200: a tensor-core update timed out waiting for its operands\n");
+    if (err & 1) fprintf(stderr, "pastix_b200: negative diagonal term in the Cholesky factorization\n");
+    if (err) return ERR_INTERNAL;
     s->factored = true;
     return ERR_SUCCESS;
 }
