@@ -84,6 +84,14 @@ struct SubTask {
     int pos;
 };
 
+// 32 x 32 tile of a panel copied to the row-major operand arena of the tensor-core
+// updates.
+struct SplitTask {
+    int k;
+    int row0;
+    int col0;
+};
+
 struct Level {
     int c0, c1;          // cblks (indices into lvl_cblk)
     int t0, t1;          // row tasks of the off-diagonal panels

@@ -33,15 +33,20 @@ void launch_update_f32(const DevSym &s, const Upd *upds, int nupd, int ntiles, f
                        cudaStream_t st);
 // returns the dynamic shared memory (bytes) the panel TRSM may use, or -1
 int configure_factor_kernels();
-// FP32 updates on the tensor cores (update_tc.cu): tiles of 128 rows x 64 columns,
-// tile index space of each update sized for rows rounded down to a multiple of 4;
-// mapL / mapU: device arrays of one tensor map per cblk panel; split: 3xTF32
-void launch_update_tc(const DevSym &s, const Upd *upds, int nupd, int ntiles, const void *mapL, const void *mapU,
-                      float *L, float *U, int split, int *err, cudaStream_t st);
+// FP32 updates on the tensor cores (update_tc.cu).  Tiles of 128 rows x 64
+// columns (tiles_m / tiles_n of each update counted that way); maps: 4 x cblknbr
+// tensor maps of the operand arenas, [(side * 2 + part) * cblknbr + k] with side
+// 0 L / 1 U and part 0 hi / 1 lo; split: 3xTF32.
+void launch_update_tc(const DevSym &s, const Upd *upds, int nupd, int ntiles, const void *maps, float *L, float *U,
+                      int split, int *err, cudaStream_t st);
 int configure_tc_kernels();
-// tensor maps (FP32, ld x ncols, boxes of 32 x 32, 128-byte swizzle) of the cblks with wanted[k] != 0
-int encode_panel_maps(const std::vector<int64_t> &off, const std::vector<int> &ld, const std::vector<int> &ncols,
-                      const std::vector<char> &wanted, float *arena, std::vector<CUtensorMap> &maps);
+// copy panel tiles row-major into the operand arena (hi, and lo = x - hi when lo is given)
+void launch_panel_split(const DevSym &s, const SplitTask *tasks, int ntasks, const float *P, const int64_t *toff,
+                        float *hi, float *lo, cudaStream_t st);
+// tensor maps of the operand copies of the cblks with wanted[k] != 0 (maps: cblknbr entries)
+int encode_operand_maps(const std::vector<int64_t> &toff, const std::vector<int> &stride,
+                        const std::vector<int> &ncols, const std::vector<char> &wanted, float *arena,
+                        CUtensorMap *maps);
 
 // solve (solve_kernels.cu); x is the permuted right-hand side block, n x nrhs, leading dimension ldx
 template <typename T>

@@ -105,6 +105,7 @@ struct b200_solver_s {
         int ntiles;
         int tu0, tu1;  // internal updates on the tensor cores
         int tntiles;
+        int sp0, sp1;  // operand copies for them
     };
     std::vector<std::vector<SubStep>> lvl_steps;
     SubTask *d_subtask = nullptr;
@@ -118,7 +119,13 @@ struct b200_solver_s {
     Upd *d_tcupd = nullptr;
     std::vector<int> lvl_tc_u0, lvl_tc_u1, lvl_tc_tiles;
     std::vector<char> tc_wanted;          // cblks whose panels the tensor-core updates read
-    void *d_mapL = nullptr, *d_mapU = nullptr;
+    std::vector<int64_t> toff;            // operand copy of cblk k: row-major, pitch ncols rounded up to 4
+    int64_t tsize = 0;                    // floats of one operand arena
+    void *d_tarena = nullptr;             // [L hi][L lo][U hi][U lo] (lo only for TF32X3, U only for LU)
+    int64_t *d_toffT = nullptr;
+    void *d_maps = nullptr;               // 4 x cblknbr tensor maps
+    SplitTask *d_split = nullptr;
+    std::vector<int> lvl_sp0, lvl_sp1;    // operand copies of each level (before its external updates)
     std::vector<int> lvl_tr;            // TRSM rows per task of each level
     std::vector<int> lvl_s0, lvl_s1;    // solve row tasks of each level
     int nmax_all = 0;
@@ -200,6 +207,10 @@ int build_schedule(b200_solver_t *s) {
     std::vector<SubTask> subtasks;
     std::vector<Upd> subupds;
     std::vector<Upd> tcupds;
+    std::vector<SplitTask> splits;
+    std::vector<char> ext_wanted(N, 0);   // cblks with external tensor-core updates
+    s->lvl_sp0.assign(nlev, 0);
+    s->lvl_sp1.assign(nlev, 0);
     s->tc_wanted.assign(N, 0);
     s->lvl_tc_u0.assign(nlev, 0);
     s->lvl_tc_u1.assign(nlev, 0);
@@ -208,10 +219,10 @@ int build_schedule(b200_solver_t *s) {
         return s->use_tc && !(u.flags & UPD_SCALE_D) && u.K >= s->tc_min_k && u.M >= s->tc_min_m &&
                (u.colK0 == 0 || u.K % 32 == 0);
     };
-    // tensor-core tiles: 128 x 64 from the rows rounded down to a multiple of 4
+    // tensor-core tiles: 128 x 64
     auto push_tc = [&](Upd u, int &t0) {
-        u.tiles_m = (u.M + (u.rowA0 & 3) + 127) / 128;
-        u.tiles_n = (u.N + (u.rowB0 & 3) + 63) / 64;
+        u.tiles_m = (u.M + 127) / 128;
+        u.tiles_n = (u.N + 63) / 64;
         u.tile0 = t0;
         t0 += u.tiles_m * u.tiles_n;
         s->tc_wanted[u.k] = 1;
@@ -283,6 +294,7 @@ int build_schedule(b200_solver_t *s) {
                 ss.t1 = (int)subtasks.size();
                 ss.u0 = (int)subupds.size();
                 ss.tu0 = (int)tcupds.size();
+                ss.sp0 = (int)splits.size();
                 int t0 = 0, tt0 = 0;
                 for (auto &m : members) {
                     const int k = m.first, n = s->ncols[k];
@@ -301,6 +313,8 @@ int build_schedule(b200_solver_t *s) {
                     u.flags = UPD_SYM | (s->facto == FACTO_SYTRF ? UPD_SCALE_D : 0);
                     if (tc_ok(u)) {
                         push_tc(u, tt0);
+                        for (int r0 = c0 + 64; r0 < s->stride[k]; r0 += 32)
+                            for (int cc = c0; cc < c0 + 64; cc += 32) splits.push_back({k, r0, cc});
                         continue;
                     }
                     u.tiles_m = (u.M + 63) / 64;
@@ -313,6 +327,7 @@ int build_schedule(b200_solver_t *s) {
                 ss.ntiles = t0;
                 ss.tu1 = (int)tcupds.size();
                 ss.tntiles = tt0;
+                ss.sp1 = (int)splits.size();
                 s->lvl_steps[l].push_back(ss);
             }
         }
@@ -383,6 +398,7 @@ int build_schedule(b200_solver_t *s) {
                     s->flops_class[3] += 2.0 * mn * u.K;
                     if (tc_ok(u)) {
                         push_tc(u, tc_tile0);
+                        ext_wanted[k] = 1;
                         continue;
                     }
                     u.tiles_m = (u.M + 63) / 64;
@@ -399,6 +415,15 @@ int build_schedule(b200_solver_t *s) {
         L.ntiles = tile0;
         s->lvl_tc_u1[l] = (int)tcupds.size();
         s->lvl_tc_tiles[l] = tc_tile0;
+        // operand copies of the off-diagonal rows of the level's panels read by them
+        s->lvl_sp0[l] = (int)splits.size();
+        for (int i = L.c0; i < L.c1; i++) {
+            const int k = lvl_cblk[i];
+            if (!ext_wanted[k]) continue;
+            for (int r0 = s->ncols[k]; r0 < s->stride[k]; r0 += 32)
+                for (int c0 = 0; c0 < s->ncols[k]; c0 += 32) splits.push_back({k, r0, c0});
+        }
+        s->lvl_sp1[l] = (int)splits.size();
         L.flops = flops;
         s->total_tiles += tile0;
         // reset the per-level source counters
@@ -448,6 +473,17 @@ int build_schedule(b200_solver_t *s) {
     RET(s->dupload(&s->d_toff, toff));
     RET(s->dupload(&s->d_upd, upds));
     RET(s->dupload(&s->d_tcupd, tcupds));
+    RET(s->dupload(&s->d_split, splits));
+    s->toff.assign(N, 0);
+    int64_t tp = 0;
+    for (int k = 0; k < N; k++) {
+        if (!s->tc_wanted[k]) continue;
+        s->toff[k] = tp;
+        tp += (int64_t)s->stride[k] * ((s->ncols[k] + 3) & ~3);
+        tp = (tp + 63) / 64 * 64;  // 256-byte starts
+    }
+    s->tsize = tp;
+    RET(s->dupload(&s->d_toffT, s->toff));
     return ERR_SUCCESS;
 }
 
@@ -479,11 +515,11 @@ int ensure_scal(b200_solver_t *s, int count) {
 // blocks, 2 panel TRSM, 3 GEMM-scatter updates.
 // Fine kernel kinds recorded in the per-launch detail; ids 0-3 are the classes
 // above, 4 subpanel diagonal, 5 subpanel TRSM, 6 subpanel internal update,
-// 7 diagonal-block inverses, 8 updates on the tensor cores (summed into classes
-// 1, 2, 2, 1, 3).
+// 7 diagonal-block inverses, 8 updates on the tensor cores, 9 operand copies for
+// them (summed into classes 1, 2, 2, 1, 3, 3).
 struct Trace {
-    static constexpr int NK = 9;
-    static int coarse(int c) { return c < 4 ? c : (c == 4 || c == 7) ? 1 : c == 8 ? 3 : 2; }
+    static constexpr int NK = 10;
+    static int coarse(int c) { return c < 4 ? c : (c == 4 || c == 7) ? 1 : c >= 8 ? 3 : 2; }
     std::vector<std::pair<cudaEvent_t, cudaEvent_t>> ev[NK];
     cudaEvent_t open = nullptr;
     void begin(cudaStream_t st) {
@@ -514,6 +550,19 @@ struct Trace {
         }
     }
 };
+
+// Row-major (split) copies of the panel tiles sp0..sp1 for the tensor-core updates.
+void enqueue_split(b200_solver_t *s, int sp0, int sp1, cudaStream_t st) {
+    const bool split = s->prec == B200_PREC_TF32X3;
+    float *a = (float *)s->d_tarena;
+    const int parts = split ? 2 : 1;
+    for (int side = 0; side < (s->facto == FACTO_GETRF ? 2 : 1); side++) {
+        float *hi = a + (size_t)(side * parts) * s->tsize;
+        float *lo = split ? hi + s->tsize : nullptr;
+        launch_panel_split(s->ds, s->d_split + sp0, sp1 - sp0, (const float *)(side ? s->dU : s->dL), s->d_toffT, hi,
+                           lo, st);
+    }
+}
 
 template <typename T>
 int enqueue_numfact(b200_solver_t *s, cudaStream_t st, Trace *tr = nullptr) {
@@ -576,8 +625,12 @@ int enqueue_numfact(b200_solver_t *s, cudaStream_t st, Trace *tr = nullptr) {
             }
             if (ss.tntiles > 0) {
                 if (tr) tr->begin(st);
-                launch_update_tc(s->ds, s->d_tcupd + ss.tu0, ss.tu1 - ss.tu0, ss.tntiles, s->d_mapL, s->d_mapU,
-                                 (float *)L, (float *)U, s->prec == B200_PREC_TF32X3, s->d_err, st);
+                enqueue_split(s, ss.sp0, ss.sp1, st);
+                launches += 1 + (s->facto == FACTO_GETRF);
+                if (tr) tr->end(9, st);
+                if (tr) tr->begin(st);
+                launch_update_tc(s->ds, s->d_tcupd + ss.tu0, ss.tu1 - ss.tu0, ss.tntiles, s->d_maps, (float *)L,
+                                 (float *)U, s->prec == B200_PREC_TF32X3, s->d_err, st);
                 launches++;
                 if (tr) tr->end(8, st);
             }
@@ -593,9 +646,13 @@ int enqueue_numfact(b200_solver_t *s, cudaStream_t st, Trace *tr = nullptr) {
         if (tr) tr->end(3, st);
         if (s->lvl_tc_tiles[l] > 0) {
             if (tr) tr->begin(st);
+            enqueue_split(s, s->lvl_sp0[l], s->lvl_sp1[l], st);
+            launches += 1 + (s->facto == FACTO_GETRF);
+            if (tr) tr->end(9, st);
+            if (tr) tr->begin(st);
             launch_update_tc(s->ds, s->d_tcupd + s->lvl_tc_u0[l], s->lvl_tc_u1[l] - s->lvl_tc_u0[l],
-                             s->lvl_tc_tiles[l], s->d_mapL, s->d_mapU, (float *)L, (float *)U,
-                             s->prec == B200_PREC_TF32X3, s->d_err, st);
+                             s->lvl_tc_tiles[l], s->d_maps, (float *)L, (float *)U, s->prec == B200_PREC_TF32X3,
+                             s->d_err, st);
             launches++;
             if (tr) tr->end(8, st);
         }
@@ -1125,19 +1182,24 @@ int b200_solver_create(const b200_symbol_t *sym, int facto, int precision, void 
     if (!rc) rc = dalloc((char **)&s->d_subwinv, (size_t)std::max<int64_t>(s->subwinv_slots, 1) * 64 * 64 * s->esz);
     if (!rc && facto == FACTO_GETRF) rc = dalloc((char **)&s->dWU, (size_t)s->winv_elems * s->esz);
     if (!rc && s->use_tc) {
-        for (int side = 0; side < (facto == FACTO_GETRF ? 2 : 1) && !rc; side++) {
-            std::vector<CUtensorMap> maps;
-            if (encode_panel_maps(s->off, s->ld, s->ncols, s->tc_wanted, (float *)(side ? s->dU : s->dL), maps)) {
-                fprintf(stderr, "pastix_b200: cannot encode the tensor maps of the factor panels\n");
-                rc = ERR_INTERNAL;
-                break;
+        // operand arenas and their tensor maps
+        const int parts = precision == B200_PREC_TF32X3 ? 2 : 1, sides = facto == FACTO_GETRF ? 2 : 1;
+        rc = dalloc((char **)&s->d_tarena, (size_t)std::max<int64_t>(s->tsize, 64) * parts * sides * sizeof(float));
+        std::vector<CUtensorMap> maps((size_t)4 * N);
+        for (int side = 0; side < sides && !rc; side++)
+            for (int part = 0; part < parts && !rc; part++) {
+                float *arena = (float *)s->d_tarena + (size_t)(side * parts + part) * s->tsize;
+                if (encode_operand_maps(s->toff, s->stride, s->ncols, s->tc_wanted, arena,
+                                        maps.data() + (size_t)(side * 2 + part) * N)) {
+                    fprintf(stderr, "pastix_b200: cannot encode the tensor maps of the operand copies\n");
+                    rc = ERR_INTERNAL;
+                }
             }
-            CUtensorMap *d = nullptr;
-            rc = s->dmalloc(&d, maps.size());
-            if (!rc && cudaMemcpy(d, maps.data(), maps.size() * sizeof(CUtensorMap), cudaMemcpyHostToDevice) != cudaSuccess)
-                rc = ERR_INTERNAL;
-            (side ? s->d_mapU : s->d_mapL) = d;
-        }
+        CUtensorMap *d = nullptr;
+        if (!rc) rc = s->dmalloc(&d, maps.size());
+        if (!rc && cudaMemcpy(d, maps.data(), maps.size() * sizeof(CUtensorMap), cudaMemcpyHostToDevice) != cudaSuccess)
+            rc = ERR_INTERNAL;
+        s->d_maps = d;
     }
     if (!rc) rc = s->dmalloc(&s->d_thr, 1);
     if (!rc) rc = s->dmalloc(&s->d_npiv, 1);
@@ -1164,6 +1226,7 @@ int b200_solver_destroy(b200_solver_t *s) {
     if (s->dWL) cudaFree(s->dWL);
     if (s->dTinv) cudaFree(s->dTinv);
     if (s->d_subwinv) cudaFree(s->d_subwinv);
+    if (s->d_tarena) cudaFree(s->d_tarena);
     if (s->dWU) cudaFree(s->dWU);
     if (s->d_colptr) cudaFree(s->d_colptr);
     if (s->d_rowtab) cudaFree(s->d_rowtab);

@@ -1,29 +1,34 @@
 // GEMM + scatter-add update of FP32 factors on the 5th-generation tensor cores
-// (sm_100a: TMA, tcgen05.mma kind::tf32, accumulator in tensor memory).
+// (sm_100a: TMA, tcgen05.mma kind::tf32, accumulators in tensor memory).
 //
 // Same operation as update_simt_f32_kernel (core_zgemmsp_2d2d,
 // kernels/core_zgemmsp.c:396-465): C_f[rows, cols of block j] -= A_k[rows] B_k[j]^T
 // with K = ncols_k, scattered into the facing cblk f through the block index map.
 //
-//  * Operands are read from the factor panels by TMA through one 2D tensor map per
-//    cblk panel (rows x columns, leading dimension ld_k), boxes of 32 rows x 32
-//    columns with 128-byte swizzle (rows of the panel contiguous).  A TMA row
-//    coordinate must be a multiple of 4 FP32 elements, so a tile starts at the row
-//    rounded down to 4 and the rows above the update's range are masked in the
-//    epilogue.  3-stage TMA ring over K in chunks of 32.
-//  * kind::tf32 reads its operands K-major (the MN-major form leaves the
-//    accumulator untouched on sm_100a), so all threads transpose each chunk into
-//    the K-major 128-byte-swizzled layout (one 128-byte line of 32 K values per
-//    row) of a double-buffered operand area, splitting on the way for TF32X3:
-//    x = hi + lo with hi = x with its 13 low mantissa bits cleared (exact in TF32)
-//    and lo = x - hi (exact); D += hi_A hi_B + hi_A lo_B + lo_A hi_B keeps close
-//    to FP32 accuracy.  TF32 stores x once and D += A B.
-//  * One thread issues tcgen05.mma (M = 128, N = 64, K = 8 per instruction) into
-//    a 128 x 64 FP32 accumulator in TMEM and commits each operand buffer to an
-//    mbarrier; the transposition of chunk c + 1 overlaps the MMAs of chunk c.
-//  * Epilogue: tcgen05.ld rows of TMEM (one row per thread), scatter-add into f.
-//  * Every mbarrier wait is bounded; on expiry the kernel records an error
-//    (bit 2 of err), skips its writes, frees its TMEM and returns.
+// Operand copies.  kind::tf32 reads its operands K-major (the MN-major form leaves
+// the accumulator untouched on sm_100a) while the factor panels are column-major,
+// so once a panel is final (after its TRSM) panel_split_kernel writes it row-major
+// (row r of cblk k at toff[k] + r * kp_k, kp_k = ncols_k rounded up to 4) into an
+// operand arena, split for TF32X3: x = hi + lo with hi = x with its 13 low mantissa
+// bits cleared (exact in TF32) and lo = x - hi (exact); D += hi_A hi_B + hi_A lo_B +
+// lo_A hi_B keeps close to FP32 accuracy.  TF32 keeps x once and D += A B.
+//
+// update_tc_kernel is persistent (one CTA per SM, tiles of 128 rows x 64 columns
+// striding over the launch's tile list) and warp-specialised:
+//  * warp 0 (one lane): TMA producer.  One 2D tensor map per panel copy (K
+//    innermost, boxes of 32 K x 64 rows, 128-byte swizzle: exactly the canonical
+//    K-major UMMA layout), NST-stage ring of [A hi][B hi]([A lo][B lo]) in shared
+//    memory, K in chunks of 32.
+//  * warp 1 (one lane): allocates 128 TMEM columns (two 128 x 64 FP32
+//    accumulators) and issues tcgen05.mma (M = 128, N = 64, K = 8); each stage is
+//    released to the producer and each accumulator to the epilogue by
+//    tcgen05.commit on an mbarrier.
+//  * warps 2-5: epilogue.  Thread = accumulator row (TMEM lane quarter = warp % 4);
+//    tcgen05.ld the 64 columns, release the accumulator, scatter-add into f (atomic
+//    when another source of the level updates f), overlapping the next tile's MMAs.
+//  * Every mbarrier wait is bounded and also gives up once another role has given
+//    up; the kernel then records bit 2 of err, waits (bounded) for its TMA loads and
+//    MMAs in flight, frees its TMEM and returns.
 #include <cuda.h>
 
 #include "b200_internal.h"
@@ -31,14 +36,19 @@
 
 namespace b200 {
 
-constexpr int TC_BM = 128, TC_BN = 64, TC_BK = 32, TC_ST = 3;
-constexpr int TC_A_BYTES = TC_BM * TC_BK * 4;           // 16 KB
-constexpr int TC_B_BYTES = TC_BN * TC_BK * 4;           // 8 KB
-constexpr int TC_RAW_BYTES = TC_A_BYTES + TC_B_BYTES;   // one TMA stage: [A][B], MN-major
-constexpr int TC_OP_BYTES = 2 * TC_RAW_BYTES;           // one operand buffer: [A hi][A lo][B hi][B lo], K-major
-constexpr int TC_SMEM = TC_ST * TC_RAW_BYTES + 2 * TC_OP_BYTES + 1024;  // + alignment slack
-constexpr uint32_t TC_TMEM_COLS = 64;
+constexpr int TC_BM = 128, TC_BN = 64, TC_BK = 32;
+constexpr int TC_A_BYTES = TC_BM * TC_BK * 4;  // 16 KB
+constexpr int TC_B_BYTES = TC_BN * TC_BK * 4;  // 8 KB
+constexpr uint32_t TC_TMEM_COLS = 128;          // two accumulators of 64 columns
 constexpr long long TC_WAIT_CYCLES = 1000000000LL;  // about 0.5 s at the maximum SM clock
+constexpr int TC_THREADS = 192;
+
+template <int SPLIT>
+struct TcCfg {
+    static constexpr int STAGE = SPLIT ? 2 * (TC_A_BYTES + TC_B_BYTES) : (TC_A_BYTES + TC_B_BYTES);
+    static constexpr int NST = SPLIT ? 4 : 8;
+    static constexpr int SMEM = NST * STAGE + 1024;  // + alignment slack
+};
 
 __device__ __forceinline__ uint32_t smem_addr(const void *p) {
     return static_cast<uint32_t>(__cvta_generic_to_shared(p));
@@ -52,21 +62,33 @@ __device__ __forceinline__ void mbar_expect_tx(uint32_t bar, uint32_t bytes) {
     asm volatile("mbarrier.arrive.expect_tx.shared::cta.b64 _, [%0], %1;\n" ::"r"(bar), "r"(bytes) : "memory");
 }
 
-// Bounded wait for the given phase parity; returns false if the limit expired.
-__device__ __forceinline__ bool mbar_wait(uint32_t bar, uint32_t parity) {
+__device__ __forceinline__ void mbar_arrive(uint32_t bar) {
+    asm volatile("mbarrier.arrive.shared::cta.b64 _, [%0];\n" ::"r"(bar) : "memory");
+}
+
+__device__ __forceinline__ bool mbar_test(uint32_t bar, uint32_t parity) {
+    uint32_t done;
+    asm volatile(
+        "{\n\t.reg .pred p;\n\t"
+        "mbarrier.try_wait.parity.shared::cta.b64 p, [%1], %2;\n\t"
+        "selp.u32 %0, 1, 0, p;\n\t}\n"
+        : "=r"(done)
+        : "r"(bar), "r"(parity)
+        : "memory");
+    return done != 0;
+}
+
+// Bounded wait for the given phase parity.  Returns false if the limit expired or,
+// when abort is given, once *abort is set by another role.
+__device__ __forceinline__ bool mbar_wait(uint32_t bar, uint32_t parity, volatile int *abort) {
     const long long t0 = clock64();
-    while (clock64() - t0 < TC_WAIT_CYCLES) {
-        uint32_t done;
-        asm volatile(
-            "{\n\t.reg .pred p;\n\t"
-            "mbarrier.try_wait.parity.shared::cta.b64 p, [%1], %2;\n\t"
-            "selp.u32 %0, 1, 0, p;\n\t}\n"
-            : "=r"(done)
-            : "r"(bar), "r"(parity)
-            : "memory");
-        if (done) return true;
+    for (int it = 0;; it++) {
+        if (mbar_test(bar, parity)) return true;
+        if ((it & 63) == 63) {
+            if (abort && *abort) return false;
+            if (clock64() - t0 > TC_WAIT_CYCLES) return false;
+        }
     }
-    return false;
 }
 
 __device__ __forceinline__ void tma_load_2d(uint32_t dst, const CUtensorMap *map, int x, int y, uint32_t bar) {
@@ -77,14 +99,14 @@ __device__ __forceinline__ void tma_load_2d(uint32_t dst, const CUtensorMap *map
 }
 
 // UMMA shared-memory descriptor, 128-byte swizzle: K-major operand with one
-// 128-byte line per row, SBO = stride between 8-row groups (bytes); LBO unused.
-__device__ __forceinline__ uint64_t umma_desc(uint32_t addr, uint32_t lbo, uint32_t sbo) {
+// 128-byte line per row, SBO = 1024 bytes between 8-row groups; LBO unused.
+__device__ __forceinline__ uint64_t umma_desc(uint32_t addr) {
     uint64_t d = 0;
     d |= (uint64_t)((addr >> 4) & 0x3FFF);
-    d |= (uint64_t)((lbo >> 4) & 0x3FFF) << 16;
-    d |= (uint64_t)((sbo >> 4) & 0x3FFF) << 32;
-    d |= (uint64_t)1 << 46;  // descriptor version (sm100)
-    d |= (uint64_t)2 << 61;  // SWIZZLE_128B
+    d |= (uint64_t)1 << 16;                  // LBO (ignored for swizzled K-major)
+    d |= (uint64_t)(1024 >> 4) << 32;        // SBO
+    d |= (uint64_t)1 << 46;                  // descriptor version (sm100)
+    d |= (uint64_t)2 << 61;                  // SWIZZLE_128B
     return d;
 }
 
@@ -131,240 +153,305 @@ __device__ __forceinline__ int tc_dest_row(const DevSym &s, int k, int f, int pr
     return s.rowoff[flo] + (grow - s.frow[flo]);
 }
 
-// One 4-row x 4-K block: MN-major TMA tile (32-row boxes of 4 KB: K line of 128
-// bytes, 16-byte chunk (r/4) ^ (K % 8)) -> K-major tile (row line of 128 bytes,
-// 8-row groups of 1 KB, chunk (K/4) ^ (r % 8)).  Thread p of each group of 8 takes
-// row group 8x + p and K group (p + c) % 8, which keeps both the 16-byte loads and
-// the 16-byte stores of a group free of bank conflicts.
-template <int SPLIT>
-__device__ __forceinline__ void tc_transpose_block(const unsigned char *src, unsigned char *hi, unsigned char *lo,
-                                                   int rg, int kg) {
-    const int r0 = 4 * rg, kk0 = 4 * kg;
-    float4 v[4];
-#pragma unroll
-    for (int j = 0; j < 4; j++) {
-        const int kk = kk0 + j;
-        v[j] = *reinterpret_cast<const float4 *>(src + (r0 >> 5) * 4096 + kk * 128 +
-                                                  ((((r0 & 31) >> 2) ^ (kk & 7)) << 4));
-    }
+// Tile t of the launch: its update, row tile and column tile; false for a tile
+// entirely above the diagonal of a symmetric update (nothing to compute).
+struct TcTile {
+    Upd u;
+    int mt, nt;
+};
+
+__device__ __forceinline__ bool tc_decode(const Upd *__restrict__ upds, int nupd, int t, TcTile &tt) {
+    tt.u = upds[tc_find_update(upds, nupd, t)];
+    const int lt = t - tt.u.tile0;
+    tt.mt = lt % tt.u.tiles_m;
+    tt.nt = lt / tt.u.tiles_m;
+    return !((tt.u.flags & UPD_SYM) && tt.mt * TC_BM + TC_BM - 1 < tt.nt * TC_BN);
+}
+
+// ---------------------------------------------------------------- operand copies
+
+// One 32 x 32 tile of a panel to the row-major operand arena(s).
+__global__ void __launch_bounds__(256) panel_split_kernel(DevSym s, const SplitTask *__restrict__ tasks,
+                                                          const float *__restrict__ P,
+                                                          const int64_t *__restrict__ toff, float *hi, float *lo) {
+    __shared__ float t[32][33];
+    const SplitTask tk = tasks[blockIdx.x];
+    const int k = tk.k, tx = threadIdx.x & 31, ty = threadIdx.x >> 5;
+    const int stride = s.stride[k], nc = s.ncols[k], ld = s.ld[k], kp = (nc + 3) & ~3;
+    const float *src = P + s.off[k];
 #pragma unroll
     for (int i = 0; i < 4; i++) {
-        const int r = r0 + i;
-        const float4 w = i == 0 ? make_float4(v[0].x, v[1].x, v[2].x, v[3].x)
-                       : i == 1 ? make_float4(v[0].y, v[1].y, v[2].y, v[3].y)
-                       : i == 2 ? make_float4(v[0].z, v[1].z, v[2].z, v[3].z)
-                                : make_float4(v[0].w, v[1].w, v[2].w, v[3].w);
-        const int off = (r >> 3) * 1024 + (r & 7) * 128 + ((kg ^ (r & 7)) << 4);
-        if (SPLIT) {
-            const float4 wh = make_float4(__uint_as_float(__float_as_uint(w.x) & 0xFFFFE000u),
-                                          __uint_as_float(__float_as_uint(w.y) & 0xFFFFE000u),
-                                          __uint_as_float(__float_as_uint(w.z) & 0xFFFFE000u),
-                                          __uint_as_float(__float_as_uint(w.w) & 0xFFFFE000u));
-            *reinterpret_cast<float4 *>(hi + off) = wh;
-            *reinterpret_cast<float4 *>(lo + off) = make_float4(w.x - wh.x, w.y - wh.y, w.z - wh.z, w.w - wh.w);
-        } else {
-            *reinterpret_cast<float4 *>(hi + off) = w;
+        const int r = tk.row0 + tx, c = tk.col0 + ty + 8 * i;
+        t[ty + 8 * i][tx] = (r < stride && c < nc) ? src[r + (size_t)c * ld] : 0.f;
+    }
+    __syncthreads();
+    float *dh = hi + toff[k];
+    float *dl = lo ? lo + toff[k] : nullptr;
+#pragma unroll
+    for (int i = 0; i < 4; i++) {
+        const int r = tk.row0 + ty + 8 * i, c = tk.col0 + tx;
+        if (r < stride && c < kp) {
+            const float x = t[tx][ty + 8 * i];
+            if (dl) {
+                const float h = __uint_as_float(__float_as_uint(x) & 0xFFFFE000u);
+                dh[(size_t)r * kp + c] = h;
+                dl[(size_t)r * kp + c] = x - h;
+            } else {
+                dh[(size_t)r * kp + c] = x;
+            }
         }
     }
 }
 
+void launch_panel_split(const DevSym &s, const SplitTask *tasks, int ntasks, const float *P, const int64_t *toff,
+                        float *hi, float *lo, cudaStream_t st) {
+    if (ntasks > 0) panel_split_kernel<<<ntasks, 256, 0, st>>>(s, tasks, P, toff, hi, lo);
+}
+
+// ---------------------------------------------------------------- GEMM-scatter
+
+// maps[(side * 2 + part) * cblknbr + k]: side 0 L / 1 U, part 0 hi / 1 lo
 template <int SPLIT>
-__global__ void __launch_bounds__(128, 1) update_tc_kernel(DevSym s, const Upd *__restrict__ upds, int nupd,
-                                                           const CUtensorMap *__restrict__ mapL,
-                                                           const CUtensorMap *__restrict__ mapU, float *L, float *U,
-                                                           int *err) {
+__global__ void __launch_bounds__(TC_THREADS, 1) update_tc_kernel(DevSym s, const Upd *__restrict__ upds, int nupd,
+                                                                  int ntiles, const CUtensorMap *__restrict__ maps,
+                                                                  float *L, float *U, int *err) {
+    using Cfg = TcCfg<SPLIT>;
+    constexpr int NST = Cfg::NST;
     extern __shared__ __align__(1024) unsigned char tc_smem_raw[];
-    __shared__ __align__(8) uint64_t full_bar[TC_ST];
-    __shared__ __align__(8) uint64_t mma_bar[2];
-    __shared__ __align__(8) uint64_t done_bar;
+    __shared__ __align__(8) uint64_t full_bar[NST];
+    __shared__ __align__(8) uint64_t empty_bar[NST];
+    __shared__ __align__(8) uint64_t tfull_bar[2];
+    __shared__ __align__(8) uint64_t tempty_bar[2];
+    __shared__ __align__(8) uint64_t fin_bar;
     __shared__ uint32_t tmem_base_sh;
-    __shared__ int drow[TC_BM];
     __shared__ volatile int abort_sh;
 
     unsigned char *smem = reinterpret_cast<unsigned char *>(
         (reinterpret_cast<uintptr_t>(tc_smem_raw) + 1023) & ~(uintptr_t)1023);
-    unsigned char *raw = smem;                          // TC_ST TMA stages
-    unsigned char *opnd = smem + TC_ST * TC_RAW_BYTES;  // 2 operand buffers
-    const int tid = threadIdx.x, warp = tid >> 5;
-
-    const Upd u = upds[tc_find_update(upds, nupd, blockIdx.x)];
-    const int lt = blockIdx.x - u.tile0;
-    const int mt = lt % u.tiles_m, nt = lt / u.tiles_m;
-    const int rA = u.rowA0 & 3, rB = u.rowB0 & 3;
-    const int lm0 = mt * TC_BM - rA;  // first local row of the tile (may be negative)
-    const int ln0 = nt * TC_BN - rB;
-    const bool sym = (u.flags & UPD_SYM) != 0;
-    // a tile entirely above the diagonal of a symmetric update has nothing to do
-    if (sym && lm0 + TC_BM - 1 < ln0) return;
-    // once a tile has timed out, the remaining tiles of the factorization do nothing
-    if (*reinterpret_cast<volatile int *>(err) & 2) return;
-
-    const int k = u.k;
-    const CUtensorMap *ma = ((u.flags & UPD_A_U) ? mapU : mapL) + k;
-    const CUtensorMap *mb = ((u.flags & UPD_B_U) ? mapU : mapL) + k;
-    const int xa = u.rowA0 + lm0;  // multiple of 4
-    const int xb = u.rowB0 + ln0;
-    const int nk = (u.K + TC_BK - 1) / TC_BK;
+    const int tid = threadIdx.x, warp = tid >> 5, lane = tid & 31;
+    const int N = s.cblknbr;
 
     if (tid == 0) {
-        for (int st = 0; st < TC_ST; st++) mbar_init(smem_addr(&full_bar[st]), 1);
-        mbar_init(smem_addr(&mma_bar[0]), 1);
-        mbar_init(smem_addr(&mma_bar[1]), 1);
-        mbar_init(smem_addr(&done_bar), 1);
+        for (int i = 0; i < NST; i++) {
+            mbar_init(smem_addr(&full_bar[i]), 1);
+            mbar_init(smem_addr(&empty_bar[i]), 1);
+        }
+        for (int i = 0; i < 2; i++) {
+            mbar_init(smem_addr(&tfull_bar[i]), 1);
+            mbar_init(smem_addr(&tempty_bar[i]), 4);  // one arrival per epilogue warp
+        }
+        mbar_init(smem_addr(&fin_bar), 1);
         asm volatile("fence.mbarrier_init.release.cluster;\n" ::: "memory");
         abort_sh = 0;
     }
-    if (warp == 0) {
+    if (warp == 1) {
         asm volatile("tcgen05.alloc.cta_group::1.sync.aligned.shared::cta.b32 [%0], %1;\n" ::"r"(
                          smem_addr(&tmem_base_sh)),
                      "r"(TC_TMEM_COLS));
         asm volatile("tcgen05.relinquish_alloc_permit.cta_group::1.sync.aligned;\n" ::);
-    }
-    {
-        const int lr = lm0 + tid;
-        drow[tid] = (lr >= 0 && lr < u.M) ? tc_dest_row(s, k, u.f, u.rowA0 + lr) : -1;
     }
     asm volatile("tcgen05.fence::before_thread_sync;\n" ::: "memory");
     __syncthreads();
     asm volatile("tcgen05.fence::after_thread_sync;\n" ::: "memory");
     const uint32_t tmem = tmem_base_sh;
 
-    auto issue_loads = [&](int st, int kc) {
-        const uint32_t bar = smem_addr(&full_bar[st]);
-        mbar_expect_tx(bar, TC_RAW_BYTES);
-        unsigned char *base = raw + (size_t)st * TC_RAW_BYTES;
-        const int y = kc * TC_BK + u.colK0;
+    if (warp == 0) {
+        // ------------------------------------------------ TMA producer
+        if (lane == 0) {
+            int it = 0;
+            int last_ph[NST];
 #pragma unroll
-        for (int g = 0; g < TC_BM / 32; g++) tma_load_2d(smem_addr(base + g * 4096), ma, xa + 32 * g, y, bar);
-#pragma unroll
-        for (int g = 0; g < TC_BN / 32; g++)
-            tma_load_2d(smem_addr(base + TC_A_BYTES + g * 4096), mb, xb + 32 * g, y, bar);
-    };
-
-    bool ok = true;
-    if (tid == 0) {
-        for (int st = 0; st < TC_ST && st < nk; st++) issue_loads(st, st);
-    }
-    const int p8 = tid & 7, w8 = tid >> 3;
-    for (int kc = 0; kc < nk; kc++) {
-        const int st = kc % TC_ST;
-        const int b = kc & 1;
-        // operands of chunk kc arrived; the MMAs of chunk kc - 2 released operand
-        // buffer b.  A failed wait is published before the barrier, so every thread
-        // leaves the loop together.
-        if (ok && !mbar_wait(smem_addr(&full_bar[st]), (kc / TC_ST) & 1)) ok = false;
-        if (ok && kc >= 2 && !mbar_wait(smem_addr(&mma_bar[b]), ((kc >> 1) - 1) & 1)) ok = false;
-        if (!ok) abort_sh = 1;
-        if (ok) {
-            const unsigned char *src = raw + (size_t)st * TC_RAW_BYTES;
-            unsigned char *ob = opnd + (size_t)b * TC_OP_BYTES;
-#pragma unroll
-            for (int it = 0; it < 2; it++) {
-                const int combo = w8 + 16 * it;
-                tc_transpose_block<SPLIT>(src, ob, ob + TC_A_BYTES, 8 * (combo & 3) + p8, (p8 + (combo >> 2)) & 7);
-            }
-            tc_transpose_block<SPLIT>(src + TC_A_BYTES, ob + 2 * TC_A_BYTES, ob + 2 * TC_A_BYTES + TC_B_BYTES,
-                                      8 * (w8 & 1) + p8, (p8 + (w8 >> 1)) & 7);
-            asm volatile("fence.proxy.async.shared::cta;\n" ::: "memory");
-        }
-        asm volatile("tcgen05.fence::before_thread_sync;\n" ::: "memory");
-        __syncthreads();
-        asm volatile("tcgen05.fence::after_thread_sync;\n" ::: "memory");
-        if (abort_sh) break;
-        if (tid == 0) {
-            // stage st has been read by every thread: refill it with chunk kc + TC_ST
-            if (kc + TC_ST < nk) issue_loads(st, kc + TC_ST);
-            const uint32_t ob = smem_addr(opnd + (size_t)b * TC_OP_BYTES);
-            const uint32_t a_hi = ob, a_lo = ob + TC_A_BYTES, b_hi = ob + 2 * TC_A_BYTES,
-                           b_lo = ob + 2 * TC_A_BYTES + TC_B_BYTES;
-#pragma unroll
-            for (int t = 0; t < TC_BK / 8; t++) {
-                // K step t: 8 values = 32 bytes into each row line
-                const uint64_t dah = umma_desc(a_hi + 32 * t, 16, 1024);
-                const uint64_t dbh = umma_desc(b_hi + 32 * t, 16, 1024);
-                umma_tf32(tmem, dah, dbh, (kc > 0 || t > 0) ? 1u : 0u);
-                if (SPLIT) {
-                    umma_tf32(tmem, dah, umma_desc(b_lo + 32 * t, 16, 1024), 1u);
-                    umma_tf32(tmem, umma_desc(a_lo + 32 * t, 16, 1024), dbh, 1u);
+            for (int i = 0; i < NST; i++) last_ph[i] = -1;
+            bool ok = true;
+            for (int t = blockIdx.x; t < ntiles && ok; t += gridDim.x) {
+                TcTile tt;
+                if (!tc_decode(upds, nupd, t, tt)) continue;
+                const Upd &u = tt.u;
+                const int side_a = (u.flags & UPD_A_U) ? 1 : 0, side_b = (u.flags & UPD_B_U) ? 1 : 0;
+                const CUtensorMap *ma = maps + (size_t)(side_a * 2) * N + u.k;
+                const CUtensorMap *mb = maps + (size_t)(side_b * 2) * N + u.k;
+                const int ya = u.rowA0 + tt.mt * TC_BM, yb = u.rowB0 + tt.nt * TC_BN;
+                const int nk = (u.K + TC_BK - 1) / TC_BK;
+                for (int kc = 0; kc < nk; kc++, it++) {
+                    const int st = it % NST;
+                    if (it >= NST && !mbar_wait(smem_addr(&empty_bar[st]), ((it / NST) - 1) & 1, &abort_sh)) {
+                        ok = false;
+                        break;
+                    }
+                    const uint32_t bar = smem_addr(&full_bar[st]);
+                    mbar_expect_tx(bar, Cfg::STAGE);
+                    last_ph[st] = (it / NST) & 1;
+                    const uint32_t base = smem_addr(smem + (size_t)st * Cfg::STAGE);
+                    const int x = kc * TC_BK + u.colK0;
+                    tma_load_2d(base, ma, x, ya, bar);
+                    tma_load_2d(base + TC_A_BYTES / 2, ma, x, ya + 64, bar);
+                    tma_load_2d(base + TC_A_BYTES, mb, x, yb, bar);
+                    if (SPLIT) {
+                        const uint32_t lb = base + TC_A_BYTES + TC_B_BYTES;
+                        tma_load_2d(lb, ma + N, x, ya, bar);
+                        tma_load_2d(lb + TC_A_BYTES / 2, ma + N, x, ya + 64, bar);
+                        tma_load_2d(lb + TC_A_BYTES, mb + N, x, yb, bar);
+                    }
                 }
             }
-            umma_commit(smem_addr(&mma_bar[b]));
+            if (!ok) abort_sh = 1;
+            // the loads still in flight land before the CTA exits
+            for (int i = 0; i < NST; i++)
+                if (last_ph[i] >= 0) mbar_wait(smem_addr(&full_bar[i]), (uint32_t)last_ph[i], nullptr);
         }
-    }
-    if (tid == 0) umma_commit(smem_addr(&done_bar));
-    if (!mbar_wait(smem_addr(&done_bar), 0)) abort_sh = 1;
-    asm volatile("tcgen05.fence::after_thread_sync;\n" ::: "memory");
-    __syncthreads();
-    const bool aborted = abort_sh != 0;
-    if (!aborted) {
-        // epilogue: thread = row (TMEM lane), 4 x 16 columns
-        const int r = tid;
-        const int d = drow[r];
-        const int lr = lm0 + r;
-        float *C = ((u.flags & UPD_C_U) ? U : L) + s.off[u.f];
-        const int ldf = s.ld[u.f];
-        const bool atomic = (u.flags & UPD_ATOMIC) != 0;
+    } else if (warp == 1) {
+        // ------------------------------------------------ MMA issuer
+        if (lane == 0) {
+            int it = 0, tl = 0;
+            bool ok = true;
+            for (int t = blockIdx.x; t < ntiles && ok; t += gridDim.x) {
+                TcTile tt;
+                if (!tc_decode(upds, nupd, t, tt)) continue;
+                const int a = tl & 1;
+                if (tl >= 2 && !mbar_wait(smem_addr(&tempty_bar[a]), ((tl >> 1) - 1) & 1, &abort_sh)) {
+                    ok = false;
+                    break;
+                }
+                asm volatile("tcgen05.fence::after_thread_sync;\n" ::: "memory");
+                const uint32_t acc = tmem + (uint32_t)(a * TC_BN);
+                const int nk = (tt.u.K + TC_BK - 1) / TC_BK;
+                for (int kc = 0; kc < nk; kc++, it++) {
+                    const int st = it % NST;
+                    if (!mbar_wait(smem_addr(&full_bar[st]), (it / NST) & 1, &abort_sh)) {
+                        ok = false;
+                        break;
+                    }
+                    asm volatile("tcgen05.fence::after_thread_sync;\n" ::: "memory");
+                    const uint32_t base = smem_addr(smem + (size_t)st * Cfg::STAGE);
+                    const uint32_t a_hi = base, b_hi = base + TC_A_BYTES;
+                    const uint32_t a_lo = base + TC_A_BYTES + TC_B_BYTES, b_lo = a_lo + TC_A_BYTES;
 #pragma unroll
-        for (int cb = 0; cb < TC_BN; cb += 16) {
-            uint32_t v[16];
-            const uint32_t taddr = tmem + ((uint32_t)(warp * 32) << 16) + (uint32_t)cb;
-            asm volatile(
-                "tcgen05.ld.sync.aligned.32x32b.x16.b32 {%0,%1,%2,%3,%4,%5,%6,%7,%8,%9,%10,%11,%12,%13,%14,%15}, [%16];\n"
-                "tcgen05.wait::ld.sync.aligned;\n"
-                : "=r"(v[0]), "=r"(v[1]), "=r"(v[2]), "=r"(v[3]), "=r"(v[4]), "=r"(v[5]), "=r"(v[6]), "=r"(v[7]),
-                  "=r"(v[8]), "=r"(v[9]), "=r"(v[10]), "=r"(v[11]), "=r"(v[12]), "=r"(v[13]), "=r"(v[14]), "=r"(v[15])
-                : "r"(taddr)
-                : "memory");
+                    for (int k8 = 0; k8 < TC_BK / 8; k8++) {
+                        // K step: 8 values = 32 bytes into each row line
+                        const uint64_t dah = umma_desc(a_hi + 32 * k8), dbh = umma_desc(b_hi + 32 * k8);
+                        umma_tf32(acc, dah, dbh, (kc > 0 || k8 > 0) ? 1u : 0u);
+                        if (SPLIT) {
+                            umma_tf32(acc, dah, umma_desc(b_lo + 32 * k8), 1u);
+                            umma_tf32(acc, umma_desc(a_lo + 32 * k8), dbh, 1u);
+                        }
+                    }
+                    umma_commit(smem_addr(&empty_bar[st]));
+                }
+                if (!ok) break;
+                umma_commit(smem_addr(&tfull_bar[a]));
+                tl++;
+            }
+            if (!ok) abort_sh = 1;
+            // every MMA issued has completed before the TMEM is freed
+            umma_commit(smem_addr(&fin_bar));
+            mbar_wait(smem_addr(&fin_bar), 0, nullptr);
+        }
+    } else {
+        // ------------------------------------------------ epilogue (warps 2-5)
+        const int q = warp & 3;  // TMEM lane quarter this warp may access
+        const int row = q * 32 + lane;
+        int tl = 0;
+        for (int t = blockIdx.x; t < ntiles; t += gridDim.x) {
+            TcTile tt;
+            if (!tc_decode(upds, nupd, t, tt)) continue;
+            const Upd &u = tt.u;
+            const int a = tl & 1;
+            const int lr = tt.mt * TC_BM + row;
+            const int d = lr < u.M ? tc_dest_row(s, u.k, u.f, u.rowA0 + lr) : -1;
+            if (!mbar_wait(smem_addr(&tfull_bar[a]), (tl >> 1) & 1, &abort_sh)) {
+                abort_sh = 1;
+                break;
+            }
+            asm volatile("tcgen05.fence::after_thread_sync;\n" ::: "memory");
+            uint32_t v[TC_BN];
+            const uint32_t taddr = tmem + ((uint32_t)(q * 32) << 16) + (uint32_t)(a * TC_BN);
+#pragma unroll
+            for (int cb = 0; cb < TC_BN; cb += 16) {
+                asm volatile(
+                    "tcgen05.ld.sync.aligned.32x32b.x16.b32 {%0,%1,%2,%3,%4,%5,%6,%7,%8,%9,%10,%11,%12,%13,%14,%15}, "
+                    "[%16];\n"
+                    : "=r"(v[cb + 0]), "=r"(v[cb + 1]), "=r"(v[cb + 2]), "=r"(v[cb + 3]), "=r"(v[cb + 4]),
+                      "=r"(v[cb + 5]), "=r"(v[cb + 6]), "=r"(v[cb + 7]), "=r"(v[cb + 8]), "=r"(v[cb + 9]),
+                      "=r"(v[cb + 10]), "=r"(v[cb + 11]), "=r"(v[cb + 12]), "=r"(v[cb + 13]), "=r"(v[cb + 14]),
+                      "=r"(v[cb + 15])
+                    : "r"(taddr + (uint32_t)cb)
+                    : "memory");
+            }
+            asm volatile("tcgen05.wait::ld.sync.aligned;\n" ::: "memory");
+            // the accumulator may be overwritten by the next tile's MMAs
+            asm volatile("tcgen05.fence::before_thread_sync;\n" ::: "memory");
+            __syncwarp();
+            if (lane == 0) mbar_arrive(smem_addr(&tempty_bar[a]));
             if (d >= 0) {
+                float *C = ((u.flags & UPD_C_U) ? U : L) + s.off[u.f];
+                const size_t ldf = (size_t)s.ld[u.f];
+                const bool atomic = (u.flags & UPD_ATOMIC) != 0;
+                const int cmax = min(TC_BN, u.N - tt.nt * TC_BN);
+                const int csym = (u.flags & UPD_SYM) ? lr - tt.nt * TC_BN : TC_BN - 1;  // last column kept
+                const int cend = min(cmax, csym + 1);
+                float *p = C + d + (size_t)(u.colbase + tt.nt * TC_BN) * ldf;
+                if (atomic) {
 #pragma unroll
-                for (int q = 0; q < 16; q++) {
-                    const int lc = ln0 + cb + q;
-                    if (lc < 0 || lc >= u.N) continue;
-                    if (sym && lr < lc) continue;
-                    float *p = C + d + (size_t)(u.colbase + lc) * ldf;
-                    const float val = __uint_as_float(v[q]);
-                    if (atomic) atomicAdd(p, -val);
-                    else *p -= val;
+                    for (int c = 0; c < TC_BN; c++)
+                        if (c < cend) atomicAdd(p + (size_t)c * ldf, -__uint_as_float(v[c]));
+                } else {
+                    // all loads of a 32-column half first, then the stores: one memory
+                    // latency per half instead of one per column
+#pragma unroll
+                    for (int h = 0; h < TC_BN; h += 32) {
+                        float old[32];
+#pragma unroll
+                        for (int c = 0; c < 32; c++) old[c] = (h + c < cend) ? p[(size_t)(h + c) * ldf] : 0.f;
+#pragma unroll
+                        for (int c = 0; c < 32; c++)
+                            if (h + c < cend) p[(size_t)(h + c) * ldf] = old[c] - __uint_as_float(v[h + c]);
+                    }
                 }
             }
+            tl++;
         }
-    } else if (tid == 0) {
-        atomicOr(err, 2);
     }
     asm volatile("tcgen05.fence::before_thread_sync;\n" ::: "memory");
     __syncthreads();
-    if (warp == 0) {
+    if (tid == 0 && abort_sh) atomicOr(err, 2);
+    if (warp == 1) {
         asm volatile("tcgen05.fence::after_thread_sync;\n" ::: "memory");
         asm volatile("tcgen05.dealloc.cta_group::1.sync.aligned.b32 %0, %1;\n" ::"r"(tmem), "r"(TC_TMEM_COLS));
     }
 }
 
-void launch_update_tc(const DevSym &s, const Upd *upds, int nupd, int ntiles, const void *mapL, const void *mapU,
-                      float *L, float *U, int split, int *err, cudaStream_t st) {
+static int g_num_sms = 0;
+
+void launch_update_tc(const DevSym &s, const Upd *upds, int nupd, int ntiles, const void *maps, float *L, float *U,
+                      int split, int *err, cudaStream_t st) {
     if (ntiles <= 0) return;
-    const CUtensorMap *ml = static_cast<const CUtensorMap *>(mapL);
-    const CUtensorMap *mu = static_cast<const CUtensorMap *>(mapU);
+    const CUtensorMap *m = static_cast<const CUtensorMap *>(maps);
+    const int grid = ntiles < g_num_sms ? ntiles : g_num_sms;
     if (split)
-        update_tc_kernel<1><<<ntiles, 128, TC_SMEM, st>>>(s, upds, nupd, ml, mu ? mu : ml, L, U, err);
+        update_tc_kernel<1><<<grid, TC_THREADS, TcCfg<1>::SMEM, st>>>(s, upds, nupd, ntiles, m, L, U, err);
     else
-        update_tc_kernel<0><<<ntiles, 128, TC_SMEM, st>>>(s, upds, nupd, ml, mu ? mu : ml, L, U, err);
+        update_tc_kernel<0><<<grid, TC_THREADS, TcCfg<0>::SMEM, st>>>(s, upds, nupd, ntiles, m, L, U, err);
 }
 
 int configure_tc_kernels() {
-    int rc = 0;
-    rc |= (int)cudaFuncSetAttribute(update_tc_kernel<0>, cudaFuncAttributeMaxDynamicSharedMemorySize, TC_SMEM);
-    rc |= (int)cudaFuncSetAttribute(update_tc_kernel<1>, cudaFuncAttributeMaxDynamicSharedMemorySize, TC_SMEM);
-    return rc == 0 ? 0 : -1;
+    int dev = 0, rc = 0;
+    rc |= (int)cudaGetDevice(&dev);
+    rc |= (int)cudaDeviceGetAttribute(&g_num_sms, cudaDevAttrMultiProcessorCount, dev);
+    rc |= (int)cudaFuncSetAttribute(update_tc_kernel<0>, cudaFuncAttributeMaxDynamicSharedMemorySize, TcCfg<0>::SMEM);
+    rc |= (int)cudaFuncSetAttribute(update_tc_kernel<1>, cudaFuncAttributeMaxDynamicSharedMemorySize, TcCfg<1>::SMEM);
+    return rc == 0 && g_num_sms > 0 ? 0 : -1;
 }
 
-// One 2D tensor map per cblk panel (FP32, rows x columns, leading dimension ld),
-// boxes of 32 x 32 with 128-byte swizzle, out-of-range elements read as zero.
+// One 2D tensor map per operand copy (FP32, K innermost: ncols x stride with row
+// pitch kp = ncols rounded up to 4), boxes of 32 K x 64 rows with 128-byte swizzle;
+// elements past ncols or stride read as zero.
 typedef CUresult (*EncodeTiledFn)(CUtensorMap *, CUtensorMapDataType, cuuint32_t, void *, const cuuint64_t *,
                                   const cuuint64_t *, const cuuint32_t *, const cuuint32_t *, CUtensorMapInterleave,
                                   CUtensorMapSwizzle, CUtensorMapL2promotion, CUtensorMapFloatOOBfill);
 
-int encode_panel_maps(const std::vector<int64_t> &off, const std::vector<int> &ld, const std::vector<int> &ncols,
-                      const std::vector<char> &wanted, float *arena, std::vector<CUtensorMap> &maps) {
+int encode_operand_maps(const std::vector<int64_t> &toff, const std::vector<int> &stride,
+                        const std::vector<int> &ncols, const std::vector<char> &wanted, float *arena,
+                        CUtensorMap *maps) {
     static EncodeTiledFn encode = nullptr;
     if (!encode) {
         void *fn = nullptr;
@@ -374,15 +461,16 @@ int encode_panel_maps(const std::vector<int64_t> &off, const std::vector<int> &l
             return -1;
         encode = reinterpret_cast<EncodeTiledFn>(fn);
     }
-    const size_t n = off.size();
-    maps.assign(n, CUtensorMap{});
+    const size_t n = toff.size();
     for (size_t k = 0; k < n; k++) {
-        if (!wanted[k]) continue;
-        cuuint64_t dims[2] = {(cuuint64_t)ld[k], (cuuint64_t)ncols[k]};
-        cuuint64_t strides[1] = {(cuuint64_t)ld[k] * sizeof(float)};
-        cuuint32_t box[2] = {32, 32};
+        maps[k] = CUtensorMap{};
+        if (!wanted[k] || !arena) continue;
+        const int kp = (ncols[k] + 3) & ~3;
+        cuuint64_t dims[2] = {(cuuint64_t)ncols[k], (cuuint64_t)stride[k]};
+        cuuint64_t strides[1] = {(cuuint64_t)kp * sizeof(float)};
+        cuuint32_t box[2] = {32, 64};
         cuuint32_t estr[2] = {1, 1};
-        CUresult r = encode(&maps[k], CU_TENSOR_MAP_DATA_TYPE_FLOAT32, 2, arena + off[k], dims, strides, box, estr,
+        CUresult r = encode(&maps[k], CU_TENSOR_MAP_DATA_TYPE_FLOAT32, 2, arena + toff[k], dims, strides, box, estr,
                             CU_TENSOR_MAP_INTERLEAVE_NONE, CU_TENSOR_MAP_SWIZZLE_128B,
                             CU_TENSOR_MAP_L2_PROMOTION_L2_256B, CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE);
         if (r != CUDA_SUCCESS) return -2;
