@@ -72,12 +72,13 @@ __global__ void scatter_kernel(int64_t nnz, const int64_t *__restrict__ dest, co
 
 constexpr int TP = 33;  // padded leading dimension of 32x32 shared tiles
 
-// Unblocked factorization of a pb x pb tile by one warp (lane = row).
+// Unblocked factorization of a pb x pb tile by one warp, in shared memory (lane =
+// row); low register use for the many-CTA diagonal kernel.
 // POTRF: core_zpotf2sp (kernels/core_zpotrfsp.c:66-100)
 // GETRF: core_zgetf2sp (kernels/core_zgetrfsp.c:64-110)
 // SYTRF: core_zsytf2sp (kernels/core_zsytrfsp.c:63-103)
 template <typename T, int FACTO>
-__device__ void factor_tile(T *t, int pb, int lane, double thr, int *piv, int *err) {
+__device__ void factor_tile_smem(T *t, int pb, int lane, double thr, int *piv, int *err) {
     for (int c = 0; c < pb; c++) {
         if (lane == 0) {
             T d = t[c * (TP + 1)];
@@ -121,7 +122,7 @@ __device__ void factor_tile(T *t, int pb, int lane, double thr, int *piv, int *e
 // -(1/T[i][i]) sum_{j<=m<i} T[i][m] W[m][j], rows in order.  trans = 1 reads the
 // tile transposed (the lower triangle of T^T is the upper triangle of T).
 template <typename T>
-__device__ void invert_lower_tile(const T *t, T *w, int pb, int lane, int unit, int trans) {
+__device__ void invert_lower_tile_smem(const T *t, T *w, int pb, int lane, int unit, int trans) {
     for (int i = 0; i < 32; i++) {
         if (lane <= i) {
             const int j = lane;
@@ -142,6 +143,101 @@ __device__ void invert_lower_tile(const T *t, T *w, int pb, int lane, int unit, 
         }
         __syncwarp();
     }
+}
+
+// Unblocked factorization of a pb x pb tile by one warp, held in registers: lane
+// i owns row i (r[j] = t[i][j]), columns are broadcast with warp shuffles.  Same
+// algorithm and pivot rule as factor_tile_smem; the reciprocal of each pivot comes
+// from rsqrt (POTRF) or one division computed beside the pivot, off the critical
+// path of the trailing updates.
+template <typename T, int FACTO>
+__device__ void factor_tile(T *t, int pb, int lane, double thr, int *piv, int *err) {
+    T r[32];
+#pragma unroll
+    for (int j = 0; j < 32; j++) r[j] = t[lane + j * TP];
+    const bool row_in = lane < pb;
+    // Columns >= pb run too (no branch, so the compiler can overlap consecutive
+    // columns): they only touch padding rows (lane >= pb) and count nothing.
+#pragma unroll
+    for (int c = 0; c < 32; c++) {
+        {
+            const bool col_in = c < pb;
+            T a = __shfl_sync(0xffffffffu, r[c], c);
+            const bool rep = fabs((double)a) < thr;
+            if (rep) a = (FACTO == FACTO_POTRF) ? (T)thr : ((a < (T)0) ? (T)(-thr) : (T)thr);
+            bool neg = false;
+            T d, inv;
+            if (FACTO == FACTO_POTRF) {
+                if (a < (T)0) { neg = true; a = -a; }
+                d = sqrt(a);
+                inv = rsqrt(a);
+            } else {
+                d = a;
+                inv = (T)1 / a;
+            }
+            if (lane == 0 && col_in) {
+                if (rep) (*piv)++;
+                if (neg) *err = 1;
+            }
+            const bool below = lane > c && row_in;
+            if (lane == c) r[c] = d;
+            if (below) {
+                if (FACTO == FACTO_SYTRF) t[c + lane * TP] = r[c];  // D L^T copy in the upper part
+                r[c] *= inv;
+            }
+            const T li = r[c];
+            if (FACTO == FACTO_GETRF) {
+#pragma unroll
+                for (int j = c + 1; j < 32; j++) {
+                    const T ucj = __shfl_sync(0xffffffffu, r[j], c);  // row c of U
+                    if (below && j < pb) r[j] -= li * ucj;
+                }
+            } else {
+                const T m = (FACTO == FACTO_SYTRF) ? -d * li : li;
+#pragma unroll
+                for (int j = c + 1; j < 32; j++) {
+                    const T lj = __shfl_sync(0xffffffffu, r[c], j);  // l_j
+                    if (below && j <= lane) {
+                        if (FACTO == FACTO_SYTRF) r[j] += m * lj;
+                        else r[j] -= m * lj;
+                    }
+                }
+            }
+        }
+    }
+    __syncwarp();
+#pragma unroll
+    for (int j = 0; j < 32; j++) {
+        // LDL^T keeps the D L^T copies of the upper part written above
+        if (FACTO != FACTO_SYTRF || j <= lane) t[lane + j * TP] = r[j];
+    }
+    __syncwarp();
+}
+
+// Inverse of the lower triangle of a pb x pb tile by one warp: lane j forms column
+// j of W by forward substitution, W[m][j] = (delta_mj - sum_{p<m} T[m][p] W[p][j])
+// / T[m][m] (T[m][m] = 1 if unit), with row m of T broadcast by warp shuffles and
+// the reciprocals of the diagonal formed first.  trans = 1 inverts the lower
+// triangle of T^T (the upper triangle of T read transposed).  Rows and columns
+// >= pb of W are zero.  Called by a whole warp.
+template <typename T>
+__device__ void invert_lower_tile(const T *t, T *w, int pb, int lane, int unit, int trans) {
+    T r[32];  // row `lane` of the triangle to invert
+#pragma unroll
+    for (int p = 0; p < 32; p++) r[p] = trans ? t[p + lane * TP] : t[lane + p * TP];
+    const T rd = unit ? (T)1 : (T)1 / r[lane];  // reciprocal of this lane's diagonal entry
+    T x[32];
+#pragma unroll
+    for (int m = 0; m < 32; m++) {
+        T acc = (lane == m) ? (T)1 : (T)0;
+#pragma unroll
+        for (int p = 0; p < m; p++) acc -= __shfl_sync(0xffffffffu, r[p], m) * x[p];
+        const T rm = __shfl_sync(0xffffffffu, rd, m);
+        x[m] = (m < pb && lane < pb) ? acc * rm : (T)0;
+    }
+#pragma unroll
+    for (int m = 0; m < 32; m++) w[m + lane * TP] = x[m];
+    __syncwarp();
 }
 
 // 32x32 output tile of a trailing update, computed by one warp:
@@ -267,10 +363,10 @@ __global__ void __launch_bounds__(256) diag_factor_kernel(DevSym s, const int *_
             tile[i + j * TP] = (i < pb && j < pb) ? Ap[i + (size_t)j * ld] : (T)0;
         }
         __syncthreads();
-        if (warp == 0) factor_tile<T, FACTO>(tile, pb, lane, thr, &s_piv, &s_err);
+        if (warp == 0) factor_tile_smem<T, FACTO>(tile, pb, lane, thr, &s_piv, &s_err);
         __syncthreads();
-        if (warp == 0) invert_lower_tile<T>(tile, wl, pb, lane, FACTO != FACTO_POTRF, 0);
-        if (FACTO == FACTO_GETRF && warp == 1) invert_lower_tile<T>(tile, wu, pb, lane, 0, 1);  // inv(U^T)
+        if (warp == 0) invert_lower_tile_smem<T>(tile, wl, pb, lane, FACTO != FACTO_POTRF, 0);
+        if (FACTO == FACTO_GETRF && warp == 1) invert_lower_tile_smem<T>(tile, wu, pb, lane, 0, 1);  // inv(U^T)
         __syncthreads();
         // store the factored tile and its inverse(s)
         for (int idx = tid; idx < 32 * 32; idx += nth) {
@@ -472,179 +568,144 @@ __global__ void __launch_bounds__(256) panel_trsm_kernel(DevSym s, const RowTask
 
 constexpr int SP = 64, SPP = 65;
 
-// factor_tile / invert_lower_tile on a tile with leading dimension ldt (shared memory)
-template <typename T, int FACTO>
-__device__ void factor_tile_ld(T *t, int ldt, int pb, int lane, double thr, int *piv, int *err) {
-    for (int c = 0; c < pb; c++) {
-        if (lane == 0) {
-            T d = t[c * (ldt + 1)];
-            if (fabs((double)d) < thr) {
-                if (FACTO == FACTO_POTRF) d = (T)thr;
-                else d = (d < (T)0) ? (T)(-thr) : (T)thr;
-                (*piv)++;
-            }
-            if (FACTO == FACTO_POTRF) {
-                if (d < (T)0) { *err = 1; d = -d; }
-                d = sqrt(d);
-            }
-            t[c * (ldt + 1)] = d;
-        }
-        __syncwarp();
-        const T d = t[c * (ldt + 1)];
-        const T inv = (T)1 / d;
-        T lic = 0;
-        if (lane > c && lane < pb) {
-            const T v = t[lane + c * ldt];
-            lic = v * inv;
-            t[lane + c * ldt] = lic;
-        }
-        __syncwarp();
-        if (lane > c && lane < pb) {
-            const T f = (FACTO == FACTO_POTRF) ? lic : d * lic;
-            for (int j = c + 1; j <= lane; j++) t[lane + j * ldt] -= f * t[j + c * ldt];
-        }
-        __syncwarp();
-    }
-}
-
-template <typename T>
-__device__ void invert_lower_ld(const T *t, int ldt, T *w, int ldw, int pb, int lane, int unit) {
-    for (int i = 0; i < 32; i++) {
-        if (lane <= i) {
-            const int j = lane;
-            T v = 0;
-            if (i < pb) {
-                const T dii = unit ? (T)1 : t[i + i * ldt];
-                if (j == i) {
-                    v = (T)1 / dii;
-                } else {
-                    T acc = 0;
-                    for (int m = j; m < i; m++) acc += t[i + m * ldt] * w[m + j * ldw];
-                    v = -acc / dii;
-                }
-            }
-            w[i + j * ldw] = v;
-        } else {
-            w[i + lane * ldw] = 0;
-        }
-        __syncwarp();
-    }
-}
-
-// 64x64 diagonal tile of a sub-panel, held in registers: thread t owns row
-// i = t & 63, columns q*16 .. q*16+15 (q = t >> 6).  Right-looking factorization
-// (core_zpotf2sp / core_zsytf2sp), one barrier per column: the threads owning
-// column c publish it to a double-buffered shared vector and every thread
-// updates its own elements.  Then W = L^{-1} by the same scheme (row c of W is
-// final once divided by L[c][c]; rows below subtract L[i][c] W[c][:]).
+// 64x64 diagonal tile of a sub-panel as a 2x2 block factorization
+// (core_zpotrfsp / core_zsytrfsp, kernels/core_zpotrfsp.c:66-100 and
+// kernels/core_zsytrfsp.c:63-103, in 32-column blocks):
+//   L11 = factor(A11) and W11 = L11^{-1} by one warp (factor_tile / invert_lower_tile),
+//   L21 = A21 L11^{-T} by substitution (LDL^T: V = A21 L11^{-T} = L21 D1, L21 = V D1^{-1}),
+//   A22 -= L21 L21^T (LDL^T: V L21^T), L22 = factor(A22), W22 = L22^{-1},
+//   W21 = -W22 L21 W11,
+// so that W = L^{-1} of the 64x64 tile (unit diagonal for LDL^T) is ready for the
+// sub-panel TRSM.  The serial column recurrences stay inside one warp (two 32-column
+// factorizations and inverses, the substitution); the rest is 32x32x32 products
+// over 256 threads.  L21 and A22 follow the column order of the right-looking
+// factorization, so the factor matches the unblocked one to rounding.
 template <typename T, int FACTO>
 __global__ void __launch_bounds__(256) subpanel_diag_kernel(DevSym s, const SubTask *__restrict__ tasks, T *L,
                                                             T *winv, const double *__restrict__ thr_ptr,
                                                             unsigned long long *npiv, int *err) {
-    __shared__ T col[2][SP];
-    __shared__ T roww[2][SP];
-    __shared__ T dg[SP];
+    __shared__ T t11[32 * TP];  // L11, then V (LDL^T) / L21 W11
+    __shared__ T t21[32 * TP];
+    __shared__ T t22[32 * TP];
+    __shared__ T w11[32 * TP];
+    __shared__ T w22[32 * TP];
+    __shared__ T dd[32];
+    __shared__ T rdg[32];  // reciprocals of the diagonal of L11
     __shared__ int s_piv, s_err;
     const SubTask tk = tasks[blockIdx.x];
     const int k = tk.k, c0 = tk.c0, ld = s.ld[k];
-    const int n = s.ncols[k], wd = min(SP, n - c0);
+    const int wd = min(SP, s.ncols[k] - c0);
+    const int pb1 = min(32, wd), pb2 = wd - pb1;
     const double thr = *thr_ptr;
     T *A = L + s.off[k] + c0 + (size_t)c0 * ld;
-    const int tid = threadIdx.x;
-    const int i = tid & 63, q = tid >> 6, j0 = q * 16;
-    if (tid == 0) { s_piv = 0; s_err = 0; }
-    T r[16];
-#pragma unroll
-    for (int u = 0; u < 16; u++) {
-        const int j = j0 + u;
-        r[u] = (i < wd && j < wd && i >= j) ? A[i + (size_t)j * ld] : (T)0;
-    }
-    __syncthreads();
-    // ---- factorization
-    for (int c = 0; c < wd; c++) {
-        const int b = c & 1;
-        if (q == (c >> 4)) {  // column c (rows < c hold zeros); select without runtime indexing
-            T v = 0;
-#pragma unroll
-            for (int u = 0; u < 16; u++)
-                if (u == (c & 15)) v = r[u];
-            col[b][i] = v;
-        }
-        __syncthreads();
-        T d = col[b][c];
-        bool replaced = false;
-        if (fabs((double)d) < thr) {
-            d = (FACTO == FACTO_POTRF) ? (T)thr : ((d < (T)0) ? (T)(-thr) : (T)thr);
-            replaced = true;
-        }
-        bool negative = false;
-        if (FACTO == FACTO_POTRF) {
-            if (d < (T)0) { negative = true; d = -d; }
-            d = sqrt(d);
-        }
-        if (tid == 0) {
-            if (replaced) s_piv++;
-            if (negative) s_err = 1;
-        }
-        const T inv = (T)1 / d;
-        const T li = (i > c && i < wd) ? col[b][i] * inv : (T)0;
-        if (q == (c >> 4) && i >= c) {
-            const T nv = (i == c) ? d : li;
-#pragma unroll
-            for (int u = 0; u < 16; u++)
-                if (u == (c & 15)) r[u] = nv;
-        }
-#pragma unroll
-        for (int u = 0; u < 16; u++) {
-            const int j = j0 + u;
-            if (j > c && j <= i && i < wd) {
-                const T lj = col[b][j] * inv;  // l_j (POTRF) ; LDL^T: d l_i l_j = l_i * col[j]
-                r[u] -= (FACTO == FACTO_POTRF) ? li * lj : li * col[b][j];
-            }
-        }
-    }
-    // ---- inverse W = L^{-1} (unit diagonal for LDL^T)
-    if (q == (i >> 4) && i < wd) {
-        T v = 0;
-#pragma unroll
-        for (int u = 0; u < 16; u++)
-            if (u == (i & 15)) v = r[u];
-        dg[i] = (FACTO == FACTO_POTRF) ? v : (T)1;
-    }
-    T w[16];
-#pragma unroll
-    for (int u = 0; u < 16; u++) w[u] = (j0 + u == i && i < wd) ? (T)1 : (T)0;
-    __syncthreads();
-    for (int c = 0; c < wd; c++) {
-        const int b = c & 1;
-        const T invd = (T)1 / dg[c];
-        if (i == c) {
-#pragma unroll
-            for (int u = 0; u < 16; u++) {
-                w[u] *= invd;
-                roww[b][j0 + u] = w[u];
-            }
-        }
-        if (q == (c >> 4)) {
-            T v = 0;
-#pragma unroll
-            for (int u = 0; u < 16; u++)
-                if (u == (c & 15)) v = r[u];
-            col[b][i] = (i > c && i < wd) ? v : (T)0;
-        }
-        __syncthreads();
-        if (i > c && i < wd) {
-            const T lic = col[b][i];
-#pragma unroll
-            for (int u = 0; u < 16; u++) w[u] -= lic * roww[b][j0 + u];
-        }
-    }
     T *W = winv + (size_t)tk.pos * SP * SP;
+    const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
+    if (tid == 0) { s_piv = 0; s_err = 0; }
+    for (int idx = tid; idx < 1024; idx += 256) {
+        const int i = idx & 31, j = idx >> 5;
+        t11[i + j * TP] = (i < pb1 && j < pb1 && i >= j) ? A[i + (size_t)j * ld] : (T)0;
+        t21[i + j * TP] = (i < pb2 && j < pb1) ? A[(32 + i) + (size_t)j * ld] : (T)0;
+        t22[i + j * TP] = (i < pb2 && j < pb2 && i >= j) ? A[(32 + i) + (size_t)(32 + j) * ld] : (T)0;
+    }
+    __syncthreads();
+    if (warp == 0) factor_tile<T, FACTO>(t11, pb1, lane, thr, &s_piv, &s_err);
+    __syncthreads();
+    if (warp == 0) invert_lower_tile<T>(t11, w11, pb1, lane, FACTO != FACTO_POTRF, 0);
+    if (tid < 32) {
+        dd[tid] = (tid < pb1) ? t11[tid * (TP + 1)] : (T)1;
+        rdg[tid] = (T)1 / dd[tid];
+    }
+    __syncthreads();
+    // L11 and W11 are final
+    for (int idx = tid; idx < 1024; idx += 256) {
+        const int i = idx & 31, j = idx >> 5;
+        if (i < pb1 && j < pb1 && i >= j) A[i + (size_t)j * ld] = t11[i + j * TP];
+        W[i + j * SP] = (i < pb1 && j < pb1 && i >= j) ? w11[i + j * TP] : (T)0;
+        W[i + (32 + j) * SP] = 0;
+    }
+    if (pb2 > 0) {
+        T v[4];
+        __syncthreads();
+        // L21 by substitution against L11^T, one row per thread of warp 0, in the
+        // column order of the right-looking factorization:
+        // POTRF  L21[i][c] = (A21[i][c] - sum_{l<c} L21[i][l] L11[c][l]) / L11[c][c]
+        // LDL^T  V[i][c]   =  A21[i][c] - sum_{l<c} V[i][l] L11[c][l],  L21 = V D1^{-1}
+        if (tid < 32) {
+            const int i = tid;
+            T x[32];
 #pragma unroll
-    for (int u = 0; u < 16; u++) {
-        const int j = j0 + u;
-        if (i < wd && j < wd && i >= j) A[i + (size_t)j * ld] = r[u];
-        W[i + j * SP] = (i < wd && j < wd && i >= j) ? w[u] : (T)0;
+            for (int c = 0; c < 32; c++) x[c] = t21[i + c * TP];
+#pragma unroll
+            for (int c = 0; c < 32; c++) {
+                if (c < pb1) {
+#pragma unroll
+                    for (int l = 0; l < c; l++) x[c] -= x[l] * t11[c + l * TP];
+                    if (FACTO == FACTO_POTRF) x[c] *= rdg[c];
+                }
+            }
+#pragma unroll
+            for (int c = 0; c < 32; c++) t21[i + c * TP] = x[c];
+        }
+        __syncthreads();
+        if (FACTO == FACTO_SYTRF) {
+            // V to t11 (L11 is stored already), L21 = V D1^{-1} in t21
+#pragma unroll
+            for (int e = 0; e < 4; e++) {
+                const int idx = tid + 256 * e, i = idx & 31, c = idx >> 5;
+                const T x = t21[i + c * TP];
+                t11[i + c * TP] = x;
+                t21[i + c * TP] = (c < pb1) ? x / dd[c] : (T)0;
+            }
+            __syncthreads();
+        }
+        // A22 -= L21 X^T on the lower triangle, X = L21 (POTRF) or V (LDL^T), one
+        // subtraction per column of L21 in order
+        const T *X = (FACTO == FACTO_SYTRF) ? t11 : t21;
+#pragma unroll
+        for (int e = 0; e < 4; e++) {
+            const int idx = tid + 256 * e, i = idx & 31, j = idx >> 5;
+            if (i >= j) {
+                T acc = t22[i + j * TP];
+                for (int l = 0; l < pb1; l++) acc -= t21[i + l * TP] * X[j + l * TP];
+                t22[i + j * TP] = acc;
+            }
+        }
+        __syncthreads();
+        if (warp == 0) factor_tile<T, FACTO>(t22, pb2, lane, thr, &s_piv, &s_err);
+        __syncthreads();
+        if (warp == 0) invert_lower_tile<T>(t22, w22, pb2, lane, FACTO != FACTO_POTRF, 0);
+        // M = L21 W11: M[i][j] = sum_{l >= j} L21[i][l] W11[l][j]
+#pragma unroll
+        for (int e = 0; e < 4; e++) {
+            const int idx = tid + 256 * e, i = idx & 31, j = idx >> 5;
+            T acc = 0;
+            for (int l = j; l < pb1; l++) acc += t21[i + l * TP] * w11[l + j * TP];
+            v[e] = acc;
+        }
+        __syncthreads();
+#pragma unroll
+        for (int e = 0; e < 4; e++) {
+            const int idx = tid + 256 * e, i = idx & 31, j = idx >> 5;
+            t11[i + j * TP] = v[e];
+        }
+        __syncthreads();
+        // W21 = -W22 M: W21[i][j] = -sum_{l <= i} W22[i][l] M[l][j]
+        for (int idx = tid; idx < 1024; idx += 256) {
+            const int i = idx & 31, j = idx >> 5;
+            T acc = 0;
+            for (int l = 0; l <= i; l++) acc += w22[i + l * TP] * t11[l + j * TP];
+            const bool in = i < pb2 && j < pb1;
+            W[(32 + i) + j * SP] = in ? -acc : (T)0;
+            W[(32 + i) + (32 + j) * SP] = (i < pb2 && j < pb2 && i >= j) ? w22[i + j * TP] : (T)0;
+            if (i < pb2 && j < pb1) A[(32 + i) + (size_t)j * ld] = t21[i + j * TP];
+            if (i < pb2 && j < pb2 && i >= j) A[(32 + i) + (size_t)(32 + j) * ld] = t22[i + j * TP];
+        }
+    } else {
+        for (int idx = tid; idx < 1024; idx += 256) {
+            const int i = idx & 31, j = idx >> 5;
+            W[(32 + i) + j * SP] = 0;
+            W[(32 + i) + (32 + j) * SP] = 0;
+        }
     }
     __syncthreads();
     if (tid == 0) {
