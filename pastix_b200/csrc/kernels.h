@@ -59,6 +59,11 @@ void launch_solve_offdiag(const DevSym &s, const RowTask *tasks, int ntasks, con
 template <typename T>
 void launch_solve_tiles(const DevSym &s, const SolveTile *tasks, int ntasks, const T *L, const double *x, double *b,
                         int64_t ldx, int nrhs, int backward, cudaStream_t st);
+// both sweeps' work of cblks with at most 32 columns, one warp per cblk: forward
+// aux_k = W_k x_k and x[rows below] -= P aux_k; backward x_k = W_k^T (aux_k - P^T x[rows below])
+template <typename T>
+void launch_solve_leaf(const DevSym &s, const int *cblks, int ncblk, const T *P, const T *W, const int64_t *woff,
+                       double *x, double *aux, int64_t ldx, int nrhs, int backward, cudaStream_t st);
 // W_k = inverse of the lower-triangular diagonal block of every listed cblk (W: n x n per cblk)
 template <typename T>
 void launch_diag_inverse(const DevSym &s, const int *cblks, int ncblk, const T *L, T *W, const int64_t *woff,
@@ -67,9 +72,10 @@ void launch_diag_inverse(const DevSym &s, const int *cblks, int ncblk, const T *
 template <typename T>
 void launch_copy_tile_inverse(const DevSym &s, const int *cblks, int ncblk, const T *tinv, const int64_t *toff, T *W,
                               const int64_t *woff, int which, cudaStream_t st);
-// xout[k] = W_k xin[k] (forward) or W_k^T xin[k] (backward) on 64-row tiles (task row0 < ncols)
+// xout[k] += W_k xin[k] (forward) or W_k^T xin[k] (backward), one 64 x 64 tile of W_k per task
+// {k, output row0, K chunk col0}; xout zeroed by the caller before the sweep
 template <typename T>
-void launch_solve_diag_inv(const DevSym &s, const RowTask *tasks, int ntasks, const T *W, const int64_t *woff,
+void launch_solve_diag_inv(const DevSym &s, const SolveTile *tasks, int ntasks, const T *W, const int64_t *woff,
                            const double *xin, double *xout, int64_t ldx, int nrhs, int backward, cudaStream_t st);
 template <typename T>
 void launch_solve_scale_diag(const DevSym &s, const int *cblks, int ncblk, const T *L, double *x, int64_t ldx,

@@ -297,20 +297,28 @@ template void launch_solve_scale_diag<float>(const DevSym &, const int *, int, c
 
 // ====================================================================== tensor-core solve tiles
 //
-// The off-diagonal part of the supernodal solves as small GEMMs on FP64 tensor
-// cores (DMMA m16n8k4).  One CTA (4 warps) takes a 64-row x 64-column tile of a
-// cblk's off-diagonal panel:
-//   forward : b[grow(r)] -= sum_c P[r][c] x_k[c]        (warp = 16 rows)
-//   backward: b_k[c]     -= sum_r P[r][c] x[grow(r)]    (warp = 16 columns)
-// The panel is read straight into the MMA A fragments (for every lane group the
-// 8 consecutive rows of one column, i.e. whole 32-byte sectors); the x operand is
-// staged in shared memory; partial sums from the tiles of one cblk meet in
-// global memory through atomics.  Up to 32 right-hand sides per pass.
+// The off-diagonal and diagonal-inverse products of the supernodal solves as
+// small GEMMs on FP64 tensor cores (DMMA m16n8k4), one CTA (4 warps) per 64 x 64
+// tile of the factor (or of a diagonal-block inverse W) times up to 32 right-hand
+// sides per pass:
+//   OFF_FWD : b[grow(r)] -= sum_c P[r][c] x_k[c]     (solve_blok_zgemm forward,
+//             kernels/solve_ztrsmsp.c:275-280; warp = 16 rows)
+//   OFF_BWD : b_k[c]     -= sum_r P[r][c] x[grow(r)] (backward; warp = 16 columns)
+//   DIAG_FWD: out_k[r]    = sum_c W[r][c] in_k[c]     (W = L_kk^{-1}, lower)
+//   DIAG_BWD: out_k[c]    = sum_r W[r][c] in_k[r]     (W^T, upper)
+// The factor tile is staged in shared memory with cp.async (every load of the tile
+// in flight at once, zero fill outside the panel) and the diagonal products run a
+// double-buffered pipeline over 64-column chunks, so a tile costs about one memory
+// latency; partial sums of the off-diagonal tiles of one cblk meet in global
+// memory through atomics.
 namespace b200 {
 
 constexpr int STT = 64;          // tile rows / columns
 constexpr int SRHS = 32;         // right-hand sides per pass
 constexpr int SXP = SRHS + 4;    // padded row of the staged x tile (conflict-free fragment reads)
+constexpr int SM_FWD = 72;       // pitch of a staged tile read row-wise by the fragments
+constexpr int SM_BWD = 68;       // pitch of a staged tile read column-wise
+enum { OFF_FWD = 0, OFF_BWD = 1, DIAG_FWD = 2, DIAG_BWD = 3 };
 
 __device__ __forceinline__ void dmma16x8x4(double (&c)[4], double a0, double a1, double b) {
     asm volatile(
@@ -319,122 +327,294 @@ __device__ __forceinline__ void dmma16x8x4(double (&c)[4], double a0, double a1,
         : "d"(a0), "d"(a1), "d"(b));
 }
 
+__device__ __forceinline__ unsigned sm_addr(const void *p) { return (unsigned)__cvta_generic_to_shared(p); }
 template <typename T>
-__global__ void __launch_bounds__(128) solve_tile_fwd_kernel(DevSym s, const SolveTile *__restrict__ tasks,
-                                                             const T *__restrict__ L, const double *x,
-                                                             double *b, int64_t ldx, int nrhs) {
-    __shared__ double xs[STT * SXP];
-    __shared__ int grows[STT];
+__device__ __forceinline__ void cp_async_el(T *dst, const T *src, bool ok) {
+    asm volatile("cp.async.ca.shared.global [%0], [%1], %2, %3;\n" ::"r"(sm_addr(dst)), "l"(src), "n"(sizeof(T)),
+                 "r"(ok ? (int)sizeof(T) : 0));
+}
+__device__ __forceinline__ void cp_commit() { asm volatile("cp.async.commit_group;\n" ::); }
+template <int N>
+__device__ __forceinline__ void cp_wait() { asm volatile("cp.async.wait_group %0;\n" ::"n"(N)); }
+
+// Stage M[gr0 + r][gc0 + c] (column-major, leading dimension ldm, nr x nc valid) as
+// ms[c * PM + r] for r, c < 64; zeros outside.  Warp w takes columns w, w + 4, ...
+// and its lanes rows lane and lane + 32: consecutive lanes read consecutive rows.
+template <typename T, int PM>
+__device__ __forceinline__ void stage_tile(T *ms, const T *M, int64_t ldm, int gr0, int gc0, int nr, int nc) {
+    const int lane = threadIdx.x & 31, w = threadIdx.x >> 5, nw = blockDim.x >> 5;
+    const bool r0ok = gr0 + lane < nr, r1ok = gr0 + lane + 32 < nr;
+    const T *col = M + gr0 + lane + (size_t)(gc0 + w) * ldm;
+    for (int c = w; c < STT; c += nw, col += (size_t)nw * ldm) {
+        const bool cok = gc0 + c < nc;
+        cp_async_el(ms + c * PM + lane, (cok && r0ok) ? col : M, cok && r0ok);
+        cp_async_el(ms + c * PM + lane + 32, (cok && r1ok) ? col + 32 : M, cok && r1ok);
+    }
+}
+
+// x tile: xs[i * SXP + j] = xv[i][q0 + j] for i < ni, j < R (zeros elsewhere); rows
+// either contiguous from xv (rowmap null) or gathered through rowmap.
+__device__ __forceinline__ void stage_x(double *xs, const double *xv, const int *rowmap, int ni, int64_t ldx, int q0,
+                                        int R) {
+    const int lane = threadIdx.x & 31, w = threadIdx.x >> 5, nw = blockDim.x >> 5;
+    const int i0 = lane, i1 = lane + 32;
+    const bool ok0 = i0 < ni, ok1 = i1 < ni;
+    const double *x0 = xv + (ok0 ? (rowmap ? rowmap[i0] : i0) : 0);
+    const double *x1 = xv + (ok1 ? (rowmap ? rowmap[i1] : i1) : 0);
+    for (int j = w; j < SRHS; j += nw) {
+        const bool jok = j < R;
+        cp_async_el(xs + i0 * SXP + j, x0 + (size_t)(q0 + j) * ldx, jok && ok0);
+        cp_async_el(xs + i1 * SXP + j, x1 + (size_t)(q0 + j) * ldx, jok && ok1);
+    }
+}
+
+// acc += M_tile(op) x_tile over 64 K values; ROW = 1: output index = tile row
+// (a fragment reads ms[k * PM + out]), ROW = 0: output index = tile column
+// (ms[out * PM + k]).
+template <typename T, int PM, int ROW>
+__device__ __forceinline__ void tile_mma(double (&acc)[4][4], const T *ms, const double *xs, int o0w, int ntn) {
+    const int lane = threadIdx.x & 31, g = lane >> 2, tg = lane & 3;
+#pragma unroll 4
+    for (int kk = 0; kk < STT; kk += 4) {
+        const int kq = kk + tg;
+        const double a0 = ROW ? (double)ms[kq * PM + o0w + g] : (double)ms[(o0w + g) * PM + kq];
+        const double a1 = ROW ? (double)ms[kq * PM + o0w + g + 8] : (double)ms[(o0w + g + 8) * PM + kq];
+#pragma unroll
+        for (int nt = 0; nt < 4; nt++)
+            if (nt < ntn) dmma16x8x4(acc[nt], a0, a1, xs[kq * SXP + nt * 8 + g]);
+    }
+}
+
+template <typename T, int MODE>
+struct SolveSmem {
+    static constexpr int PM = (MODE == OFF_FWD || MODE == DIAG_FWD) ? SM_FWD : SM_BWD;
+    static constexpr int BYTES = STT * PM * (int)sizeof(T) + STT * SXP * 8;
+};
+
+// One 64 x 64 tile times up to 32 right-hand sides per pass.  Task {k, row0, col0}:
+//   OFF_*  : panel rows [row0, row0 + 64) x columns [col0, col0 + 64) of cblk k
+//   DIAG_* : output tile [row0, row0 + 64) of cblk k, K chunk [col0, col0 + 64) of
+//            W_k (forward) or W_k^T (backward); the output (zeroed before the sweep)
+//            accumulates the chunks through atomics.
+template <typename T, int MODE>
+__global__ void __launch_bounds__(128) solve_mm_kernel(DevSym s, const SolveTile *__restrict__ tasks,
+                                                       const T *__restrict__ M, const int64_t *__restrict__ woff,
+                                                       const double *xin, double *out, int64_t ldx, int nrhs) {
+    using SS = SolveSmem<T, MODE>;
+    constexpr int PM = SS::PM;
+    constexpr bool ROW = (MODE == OFF_FWD || MODE == DIAG_FWD);
+    extern __shared__ __align__(16) unsigned char sv_smem[];
+    T *ms = reinterpret_cast<T *>(sv_smem);
+    double *xs = reinterpret_cast<double *>(sv_smem + STT * PM * sizeof(T));
+    __shared__ int rmap[STT];
     const SolveTile t = tasks[blockIdx.x];
-    const int k = t.k, n = s.ncols[k], ld = s.ld[k];
-    const int rows = min(STT, s.stride[k] - t.row0), cols = min(STT, n - t.col0);
-    const T *P = L + s.off[k] + t.row0 + (size_t)t.col0 * ld;
-    const double *xk = x + s.fcol[k] + t.col0;
+    const int k = t.k, n = s.ncols[k];
     const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
     const int g = lane >> 2, tg = lane & 3;
-    if (tid < STT) grows[tid] = (tid < rows) ? panel_row_to_global(s, k, t.row0 + tid) : -1;
-    const int r0w = warp * 16;
-    const bool okA0 = (r0w + g) < rows, okA1 = (r0w + g + 8) < rows;
+    const int o0w = warp * 16;  // this warp's 16 outputs of the tile
+    int nout;
+    const double *xsrc;
+    const int *xmap = nullptr;
+    int nk;
+    if (MODE == OFF_FWD || MODE == OFF_BWD) {
+        const int rows = min(STT, s.stride[k] - t.row0), cols = min(STT, n - t.col0);
+        if (tid < STT) rmap[tid] = (tid < rows) ? panel_row_to_global(s, k, t.row0 + tid) : 0;
+        __syncthreads();
+        stage_tile<T, PM>(ms, M + s.off[k], s.ld[k], t.row0, t.col0, s.stride[k], n);
+        nout = ROW ? rows : cols;
+        nk = ROW ? cols : rows;
+        if (MODE == OFF_FWD) xsrc = xin + s.fcol[k] + t.col0;
+        else { xsrc = xin; xmap = rmap; }
+    } else {
+        const T *Wk = M + woff[k];
+        nout = min(STT, n - t.row0);
+        nk = min(STT, n - t.col0);
+        if (MODE == DIAG_FWD) stage_tile<T, PM>(ms, Wk, n, t.row0, t.col0, n, n);  // W[o][k]
+        else stage_tile<T, PM>(ms, Wk, n, t.col0, t.row0, n, n);                   // W[k][o]
+        xsrc = xin + s.fcol[k] + t.col0;
+    }
     for (int q0 = 0; q0 < nrhs; q0 += SRHS) {
-        const int R = min(SRHS, nrhs - q0);
+        const int R = min(SRHS, nrhs - q0), ntn = (R + 7) >> 3;
+        if (q0 > 0) __syncthreads();
+        stage_x(xs, xsrc, xmap, nk, ldx, q0, R);
+        cp_commit();
+        cp_wait<0>();
         __syncthreads();
-        for (int idx = tid; idx < STT * SRHS; idx += blockDim.x) {
-            const int c = idx % STT, j = idx / STT;
-            xs[c * SXP + j] = (c < cols && j < R) ? xk[c + (size_t)(q0 + j) * ldx] : 0.0;
-        }
-        __syncthreads();
-        const int ntn = (R + 7) >> 3;
-        double acc[4][4];
-#pragma unroll
-        for (int a = 0; a < 4; a++)
-#pragma unroll
-            for (int e = 0; e < 4; e++) acc[a][e] = 0.0;
-        if (r0w < rows) {
-#pragma unroll 4
-            for (int kk = 0; kk < cols; kk += 4) {
-                const int c = kk + tg;
-                const bool okc = c < cols;
-                const double a0 = (okA0 && okc) ? (double)P[(r0w + g) + (size_t)c * ld] : 0.0;
-                const double a1 = (okA1 && okc) ? (double)P[(r0w + g + 8) + (size_t)c * ld] : 0.0;
-#pragma unroll
-                for (int nt = 0; nt < 4; nt++)
-                    if (nt < ntn) dmma16x8x4(acc[nt], a0, a1, xs[c * SXP + nt * 8 + g]);
-            }
+        if (o0w < nout) {
+            double acc[4][4] = {};
+            tile_mma<T, PM, ROW>(acc, ms, xs, o0w, ntn);
+            const double sg = (MODE == OFF_FWD || MODE == OFF_BWD) ? -1.0 : 1.0;
 #pragma unroll
             for (int nt = 0; nt < 4; nt++) {
                 if (nt >= ntn) continue;
 #pragma unroll
                 for (int e = 0; e < 4; e++) {
-                    const int r = r0w + g + (e >> 1) * 8;
+                    const int o = o0w + g + (e >> 1) * 8;
                     const int j = nt * 8 + 2 * tg + (e & 1);
-                    if (r < rows && j < R) atomicAdd(&b[grows[r] + (size_t)(q0 + j) * ldx], -acc[nt][e]);
+                    if (o < nout && j < R) {
+                        double *dst = (MODE == OFF_FWD)   ? out + rmap[o]
+                                      : (MODE == OFF_BWD) ? out + s.fcol[k] + t.col0 + o
+                                                          : out + s.fcol[k] + t.row0 + o;
+                        atomicAdd(dst + (size_t)(q0 + j) * ldx, sg * acc[nt][e]);
+                    }
                 }
             }
         }
     }
 }
 
+// Cblks of at most 32 columns, one warp each: the diagonal-block product and the
+// off-diagonal rows of one sweep in a single pass (the bottom levels of the tree
+// hold thousands of such cblks, far smaller than a 64 x 64 tile).
+//   forward : aux_k = W_k x_k; x[grow(r)] -= P[r][:] aux_k  (lane = row)
+//   backward: t = aux_k - P^T x[grow(rows)] (lane = column); x_k = W_k^T t
+// W_k is the inverse of the diagonal block (n x n, column-major), P the cblk panel.
+constexpr int LEAF_R = 16;  // right-hand sides per pass
+
 template <typename T>
-__global__ void __launch_bounds__(128) solve_tile_bwd_kernel(DevSym s, const SolveTile *__restrict__ tasks,
-                                                             const T *__restrict__ L, const double *x,
-                                                             double *b, int64_t ldx, int nrhs) {
-    __shared__ double xg[STT * SXP];
-    __shared__ int grows[STT];
-    const SolveTile t = tasks[blockIdx.x];
-    const int k = t.k, n = s.ncols[k], ld = s.ld[k];
-    const int rows = min(STT, s.stride[k] - t.row0), cols = min(STT, n - t.col0);
-    const T *P = L + s.off[k] + t.row0 + (size_t)t.col0 * ld;
-    double *bk = b + s.fcol[k] + t.col0;
-    const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
-    const int g = lane >> 2, tg = lane & 3;
-    if (tid < STT) grows[tid] = (tid < rows) ? panel_row_to_global(s, k, t.row0 + tid) : -1;
-    const int c0w = warp * 16;
-    const bool okA0 = (c0w + g) < cols, okA1 = (c0w + g + 8) < cols;
-    for (int q0 = 0; q0 < nrhs; q0 += SRHS) {
-        const int R = min(SRHS, nrhs - q0);
-        __syncthreads();
-        for (int idx = tid; idx < STT * SRHS; idx += blockDim.x) {
-            const int r = idx % STT, j = idx / STT;
-            xg[r * SXP + j] = (r < rows && j < R) ? x[grows[r] + (size_t)(q0 + j) * ldx] : 0.0;
-        }
-        __syncthreads();
-        const int ntn = (R + 7) >> 3;
-        double acc[4][4];
+__global__ void __launch_bounds__(128) solve_leaf_kernel(DevSym s, const int *__restrict__ cblks, int ncblk,
+                                                         const T *__restrict__ P, const T *__restrict__ W,
+                                                         const int64_t *__restrict__ woff, double *x, double *aux,
+                                                         int64_t ldx, int nrhs, int backward) {
+    __shared__ double ys[4][32][LEAF_R + 1];
+    __shared__ double xr[4][32][LEAF_R + 1];
+    __shared__ int gr[4][32];
+    const int w = threadIdx.x >> 5, lane = threadIdx.x & 31;
+    const int ci = blockIdx.x * 4 + w;
+    if (ci >= ncblk) return;
+    const int k = cblks[ci];
+    const int n = s.ncols[k], ld = s.ld[k], stride = s.stride[k], f0 = s.fcol[k];
+    const T *Pk = P + s.off[k];
+    const T *Wk = W + woff[k];
+    for (int q0 = 0; q0 < nrhs; q0 += LEAF_R) {
+        const int R = min(LEAF_R, nrhs - q0);
+        if (!backward) {
 #pragma unroll
-        for (int a = 0; a < 4; a++)
+            for (int j = 0; j < LEAF_R; j++)
+                ys[w][lane][j] = (lane < n && j < R) ? x[f0 + lane + (size_t)(q0 + j) * ldx] : 0.0;
+            __syncwarp();
+            double y[LEAF_R];
 #pragma unroll
-            for (int e = 0; e < 4; e++) acc[a][e] = 0.0;
-        if (c0w < cols) {
-#pragma unroll 4
-            for (int kk = 0; kk < rows; kk += 4) {
-                const int r = kk + tg;
-                const bool okr = r < rows;
-                const double a0 = (okA0 && okr) ? (double)P[r + (size_t)(c0w + g) * ld] : 0.0;
-                const double a1 = (okA1 && okr) ? (double)P[r + (size_t)(c0w + g + 8) * ld] : 0.0;
+            for (int j = 0; j < LEAF_R; j++) y[j] = 0.0;
+            if (lane < n) {
+                for (int c = 0; c <= lane; c++) {
+                    const double wv = (double)Wk[lane + (size_t)c * n];
 #pragma unroll
-                for (int nt = 0; nt < 4; nt++)
-                    if (nt < ntn) dmma16x8x4(acc[nt], a0, a1, xg[r * SXP + nt * 8 + g]);
-            }
-#pragma unroll
-            for (int nt = 0; nt < 4; nt++) {
-                if (nt >= ntn) continue;
-#pragma unroll
-                for (int e = 0; e < 4; e++) {
-                    const int c = c0w + g + (e >> 1) * 8;
-                    const int j = nt * 8 + 2 * tg + (e & 1);
-                    if (c < cols && j < R) atomicAdd(&bk[c + (size_t)(q0 + j) * ldx], -acc[nt][e]);
+                    for (int j = 0; j < LEAF_R; j++) y[j] += wv * ys[w][c][j];
                 }
             }
+            __syncwarp();
+            if (lane < n) {
+#pragma unroll
+                for (int j = 0; j < LEAF_R; j++) {
+                    ys[w][lane][j] = y[j];
+                    if (j < R) aux[f0 + lane + (size_t)(q0 + j) * ldx] = y[j];
+                }
+            }
+            __syncwarp();
+            for (int r = n + lane; r < stride; r += 32) {
+                const int g = panel_row_to_global(s, k, r);
+                double acc[LEAF_R];
+#pragma unroll
+                for (int j = 0; j < LEAF_R; j++) acc[j] = 0.0;
+                for (int c = 0; c < n; c++) {
+                    const double pv = (double)Pk[r + (size_t)c * ld];
+#pragma unroll
+                    for (int j = 0; j < LEAF_R; j++) acc[j] += pv * ys[w][c][j];
+                }
+#pragma unroll
+                for (int j = 0; j < LEAF_R; j++)
+                    if (j < R) atomicAdd(&x[g + (size_t)(q0 + j) * ldx], -acc[j]);
+            }
+            __syncwarp();
+        } else {
+            double t[LEAF_R];
+#pragma unroll
+            for (int j = 0; j < LEAF_R; j++) t[j] = (lane < n && j < R) ? aux[f0 + lane + (size_t)(q0 + j) * ldx] : 0.0;
+            for (int r0 = n; r0 < stride; r0 += 32) {
+                const int nr = min(32, stride - r0);
+                gr[w][lane] = (lane < nr) ? panel_row_to_global(s, k, r0 + lane) : 0;
+                __syncwarp();
+                // stage x of the 32 rows: xr[i][j] = x[grow(r0 + i)][q0 + j]
+                for (int idx = lane; idx < 32 * LEAF_R; idx += 32) {
+                    const int i = idx / LEAF_R, j = idx % LEAF_R;
+                    xr[w][i][j] = (i < nr && j < R) ? x[gr[w][i] + (size_t)(q0 + j) * ldx] : 0.0;
+                }
+                __syncwarp();
+                if (lane < n) {
+                    for (int i = 0; i < nr; i++) {
+                        const double pv = (double)Pk[r0 + i + (size_t)lane * ld];
+#pragma unroll
+                        for (int j = 0; j < LEAF_R; j++) t[j] -= pv * xr[w][i][j];
+                    }
+                }
+                __syncwarp();
+            }
+            if (lane < n) {
+#pragma unroll
+                for (int j = 0; j < LEAF_R; j++) ys[w][lane][j] = t[j];
+            }
+            __syncwarp();
+            if (lane < n) {
+                double o[LEAF_R];
+#pragma unroll
+                for (int j = 0; j < LEAF_R; j++) o[j] = 0.0;
+                for (int r = lane; r < n; r++) {
+                    const double wv = (double)Wk[r + (size_t)lane * n];
+#pragma unroll
+                    for (int j = 0; j < LEAF_R; j++) o[j] += wv * ys[w][r][j];
+                }
+#pragma unroll
+                for (int j = 0; j < LEAF_R; j++)
+                    if (j < R) x[f0 + lane + (size_t)(q0 + j) * ldx] = o[j];
+            }
+            __syncwarp();
         }
     }
 }
+
+template <typename T>
+void launch_solve_leaf(const DevSym &s, const int *cblks, int ncblk, const T *P, const T *W, const int64_t *woff,
+                       double *x, double *aux, int64_t ldx, int nrhs, int backward, cudaStream_t st) {
+    if (ncblk <= 0) return;
+    solve_leaf_kernel<T><<<(ncblk + 3) / 4, 128, 0, st>>>(s, cblks, ncblk, P, W, woff, x, aux, ldx, nrhs, backward);
+}
+template void launch_solve_leaf<double>(const DevSym &, const int *, int, const double *, const double *,
+                                        const int64_t *, double *, double *, int64_t, int, int, cudaStream_t);
+template void launch_solve_leaf<float>(const DevSym &, const int *, int, const float *, const float *,
+                                       const int64_t *, double *, double *, int64_t, int, int, cudaStream_t);
 
 template <typename T>
 void launch_solve_tiles(const DevSym &s, const SolveTile *tasks, int ntasks, const T *L, const double *x, double *b,
                         int64_t ldx, int nrhs, int backward, cudaStream_t st) {
     if (ntasks <= 0) return;
-    if (!backward) solve_tile_fwd_kernel<T><<<ntasks, 128, 0, st>>>(s, tasks, L, x, b, ldx, nrhs);
-    else solve_tile_bwd_kernel<T><<<ntasks, 128, 0, st>>>(s, tasks, L, x, b, ldx, nrhs);
+    if (!backward)
+        solve_mm_kernel<T, OFF_FWD><<<ntasks, 128, SolveSmem<T, OFF_FWD>::BYTES, st>>>(s, tasks, L, nullptr, x, b, ldx,
+                                                                                     nrhs);
+    else
+        solve_mm_kernel<T, OFF_BWD><<<ntasks, 128, SolveSmem<T, OFF_BWD>::BYTES, st>>>(s, tasks, L, nullptr, x, b, ldx,
+                                                                                     nrhs);
+}
+
+template <typename T, int MODE>
+void solve_diag_mm(const DevSym &s, const SolveTile *tasks, int ntasks, const T *W, const int64_t *woff,
+                   const double *xin, double *xout, int64_t ldx, int nrhs, cudaStream_t st) {
+    solve_mm_kernel<T, MODE><<<ntasks, 128, SolveSmem<T, MODE>::BYTES, st>>>(s, tasks, W, woff, xin, xout, ldx, nrhs);
+}
+
+// dynamic shared memory of the staged solve kernels (above the 48 KB default)
+template <typename T>
+int configure_solve_mm() {
+    int rc = 0;
+    rc |= (int)cudaFuncSetAttribute(solve_mm_kernel<T, OFF_FWD>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                    SolveSmem<T, OFF_FWD>::BYTES);
+    rc |= (int)cudaFuncSetAttribute(solve_mm_kernel<T, OFF_BWD>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                    SolveSmem<T, OFF_BWD>::BYTES);
+    rc |= (int)cudaFuncSetAttribute(solve_mm_kernel<T, DIAG_FWD>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                    SolveSmem<T, DIAG_FWD>::BYTES);
+    rc |= (int)cudaFuncSetAttribute(solve_mm_kernel<T, DIAG_BWD>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                    SolveSmem<T, DIAG_BWD>::BYTES);
+    return rc;
 }
 
 template void launch_solve_tiles<double>(const DevSym &, const SolveTile *, int, const double *, const double *,
@@ -567,81 +747,6 @@ __global__ void __launch_bounds__(256) diag_inverse_kernel(DevSym s, const int *
     }
 }
 
-// x_out[k] = W_k x_in[k] (forward) or W_k^T x_in[k] (backward) for a 64-row tile
-// of one cblk, on tensor cores; W is n x n column-major (ld = n), lower triangular.
-template <typename T>
-__global__ void __launch_bounds__(128) solve_diag_inv_kernel(DevSym s, const RowTask *__restrict__ tasks,
-                                                             const T *__restrict__ W,
-                                                             const int64_t *__restrict__ woff,
-                                                             const double *__restrict__ xin, double *__restrict__ xout,
-                                                             int64_t ldx, int nrhs, int backward) {
-    __shared__ double xs[STT * SXP];
-    const RowTask t = tasks[blockIdx.x];
-    const int k = t.k, n = s.ncols[k];
-    const int row0 = t.row0, rows = min(STT, n - row0);
-    const T *Wk = W + woff[k];
-    const double *in = xin + s.fcol[k];
-    double *out = xout + s.fcol[k];
-    const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
-    const int g = lane >> 2, tg = lane & 3;
-    const int r0w = warp * 16;
-    const int ra = row0 + r0w + g, rb = ra + 8;
-    const bool okA0 = (r0w + g) < rows, okA1 = (r0w + g + 8) < rows;
-    // nonzero range of the product: forward columns [0, row0 + rows), backward [row0, n)
-    const int cbeg = backward ? (row0 / STT) * STT : 0;
-    const int cend = backward ? n : row0 + rows;
-    for (int q0 = 0; q0 < nrhs; q0 += SRHS) {
-        const int R = min(SRHS, nrhs - q0);
-        const int ntn = (R + 7) >> 3;
-        double acc[4][4];
-#pragma unroll
-        for (int a = 0; a < 4; a++)
-#pragma unroll
-            for (int e = 0; e < 4; e++) acc[a][e] = 0.0;
-        for (int c0 = cbeg; c0 < cend; c0 += STT) {
-            const int cw = min(STT, cend - c0);
-            __syncthreads();
-            for (int idx = tid; idx < STT * SRHS; idx += blockDim.x) {
-                const int c = idx % STT, j = idx / STT;
-                xs[c * SXP + j] = (c < cw && j < R) ? in[c0 + c + (size_t)(q0 + j) * ldx] : 0.0;
-            }
-            __syncthreads();
-            if (r0w < rows) {
-#pragma unroll 4
-                for (int kk = 0; kk < cw; kk += 4) {
-                    const int c = c0 + kk + tg;
-                    const bool okc = (kk + tg) < cw;
-                    double a0 = 0.0, a1 = 0.0;
-                    if (okc) {
-                        if (!backward) {
-                            if (okA0) a0 = (double)Wk[ra + (size_t)c * n];
-                            if (okA1) a1 = (double)Wk[rb + (size_t)c * n];
-                        } else {
-                            if (okA0) a0 = (double)Wk[c + (size_t)ra * n];
-                            if (okA1) a1 = (double)Wk[c + (size_t)rb * n];
-                        }
-                    }
-#pragma unroll
-                    for (int nt = 0; nt < 4; nt++)
-                        if (nt < ntn) dmma16x8x4(acc[nt], a0, a1, xs[(kk + tg) * SXP + nt * 8 + g]);
-                }
-            }
-        }
-        if (r0w < rows) {
-#pragma unroll
-            for (int nt = 0; nt < 4; nt++) {
-                if (nt >= ntn) continue;
-#pragma unroll
-                for (int e = 0; e < 4; e++) {
-                    const int r = r0w + g + (e >> 1) * 8;
-                    const int j = nt * 8 + 2 * tg + (e & 1);
-                    if (r < rows && j < R) out[row0 + r + (size_t)(q0 + j) * ldx] = acc[nt][e];
-                }
-            }
-        }
-    }
-}
-
 template <typename T>
 void launch_diag_inverse(const DevSym &s, const int *cblks, int ncblk, const T *L, T *W, const int64_t *woff,
                          int unit, cudaStream_t st) {
@@ -650,14 +755,15 @@ void launch_diag_inverse(const DevSym &s, const int *cblks, int ncblk, const T *
 }
 
 template <typename T>
-void launch_solve_diag_inv(const DevSym &s, const RowTask *tasks, int ntasks, const T *W, const int64_t *woff,
+void launch_solve_diag_inv(const DevSym &s, const SolveTile *tasks, int ntasks, const T *W, const int64_t *woff,
                            const double *xin, double *xout, int64_t ldx, int nrhs, int backward, cudaStream_t st) {
     if (ntasks <= 0) return;
-    solve_diag_inv_kernel<T><<<ntasks, 128, 0, st>>>(s, tasks, W, woff, xin, xout, ldx, nrhs, backward);
+    if (!backward) solve_diag_mm<T, DIAG_FWD>(s, tasks, ntasks, W, woff, xin, xout, ldx, nrhs, st);
+    else solve_diag_mm<T, DIAG_BWD>(s, tasks, ntasks, W, woff, xin, xout, ldx, nrhs, st);
 }
 
 int configure_inverse_kernels() {
-    int rc = 0;
+    int rc = configure_solve_mm<double>() | configure_solve_mm<float>();
     rc |= (int)cudaFuncSetAttribute(diag_inverse_kernel<double>, cudaFuncAttributeMaxDynamicSharedMemorySize,
                                     DIAG_INV_SMEM);
     rc |= (int)cudaFuncSetAttribute(diag_inverse_kernel<float>, cudaFuncAttributeMaxDynamicSharedMemorySize,
@@ -669,9 +775,9 @@ template void launch_diag_inverse<double>(const DevSym &, const int *, int, cons
                                           int, cudaStream_t);
 template void launch_diag_inverse<float>(const DevSym &, const int *, int, const float *, float *, const int64_t *,
                                          int, cudaStream_t);
-template void launch_solve_diag_inv<double>(const DevSym &, const RowTask *, int, const double *, const int64_t *,
+template void launch_solve_diag_inv<double>(const DevSym &, const SolveTile *, int, const double *, const int64_t *,
                                             const double *, double *, int64_t, int, int, cudaStream_t);
-template void launch_solve_diag_inv<float>(const DevSym &, const RowTask *, int, const float *, const int64_t *,
+template void launch_solve_diag_inv<float>(const DevSym &, const SolveTile *, int, const float *, const int64_t *,
                                            const double *, double *, int64_t, int, int, cudaStream_t);
 
 }  // namespace b200

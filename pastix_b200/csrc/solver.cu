@@ -81,8 +81,12 @@ struct b200_solver_s {
     RowTask *d_trsm = nullptr, *d_stask = nullptr;
     SolveTile *d_stile = nullptr;
     std::vector<int> lvl_st0, lvl_st1;  // solve tiles of each level
-    RowTask *d_dtask = nullptr;         // 64-row tiles of the diagonal blocks (solves)
+    SolveTile *d_dtask = nullptr;       // 64 x 64 tiles of the diagonal-block inverses, forward (lower)
     std::vector<int> lvl_dt0, lvl_dt1;
+    SolveTile *d_dtaskb = nullptr;      // and backward (upper triangle of the transpose)
+    std::vector<int> lvl_db0, lvl_db1;
+    int *d_leaf = nullptr;              // cblks of <= 32 columns, solved by the one-warp kernel
+    std::vector<int> lvl_lf0, lvl_lf1;
     // inverses of the diagonal blocks: W_L (forward sweep) and, for LU, W_U (backward)
     int64_t *d_woff = nullptr;
     int64_t winv_elems = 0;
@@ -237,7 +241,12 @@ int build_schedule(b200_solver_t *s) {
     s->lvl_st1.assign(nlev, 0);
     s->lvl_dt0.assign(nlev, 0);
     s->lvl_dt1.assign(nlev, 0);
-    std::vector<RowTask> dtask;
+    std::vector<SolveTile> dtask, dtaskb;
+    std::vector<int> leaf;
+    s->lvl_db0.assign(nlev, 0);
+    s->lvl_db1.assign(nlev, 0);
+    s->lvl_lf0.assign(nlev, 0);
+    s->lvl_lf1.assign(nlev, 0);
     s->levels.assign(nlev, Level{});
     s->lvl_tr.assign(nlev, 64);
     s->lvl_s0.assign(nlev, 0);
@@ -262,6 +271,7 @@ int build_schedule(b200_solver_t *s) {
         s->lvl_s0[l] = (int)stask.size();
         s->lvl_st0[l] = (int)stile.size();
         s->lvl_dt0[l] = (int)dtask.size();
+        s->lvl_db0[l] = (int)dtaskb.size();
         s->lvl_ds0[l] = (int)diag_list.size();
         for (int i = L.c0; i < L.c1; i++)
             if (!is_big(lvl_cblk[i])) diag_list.push_back(lvl_cblk[i]);
@@ -331,17 +341,31 @@ int build_schedule(b200_solver_t *s) {
                 s->lvl_steps[l].push_back(ss);
             }
         }
+        s->lvl_lf0[l] = (int)leaf.size();
         for (int i = L.c0; i < L.c1; i++) {
             const int k = lvl_cblk[i];
-            for (int r0 = 0; r0 < s->ncols[k]; r0 += 64) dtask.push_back({k, r0});
             if (!is_big(k))
                 for (int r0 = s->ncols[k]; r0 < s->stride[k]; r0 += TR) trsm.push_back({k, r0});
             for (int r0 = s->ncols[k]; r0 < s->stride[k]; r0 += 128) stask.push_back({k, r0});
+            if (s->ncols[k] <= 32) {
+                // small cblk: both parts of each sweep in the one-warp kernel
+                leaf.push_back(k);
+                continue;
+            }
+            // tiles of W_k: forward the lower triangle (K chunk <= row tile), backward
+            // the upper triangle of W_k^T (K chunk >= output tile)
+            for (int r0 = 0; r0 < s->ncols[k]; r0 += 64)
+                for (int c0 = 0; c0 < s->ncols[k]; c0 += 64) {
+                    if (c0 <= r0) dtask.push_back({k, r0, c0});
+                    if (c0 >= r0) dtaskb.push_back({k, r0, c0});
+                }
             for (int r0 = s->ncols[k]; r0 < s->stride[k]; r0 += 64)
                 for (int c0 = 0; c0 < s->ncols[k]; c0 += 64) stile.push_back({k, r0, c0});
         }
+        s->lvl_lf1[l] = (int)leaf.size();
         s->lvl_st1[l] = (int)stile.size();
         s->lvl_dt1[l] = (int)dtask.size();
+        s->lvl_db1[l] = (int)dtaskb.size();
         L.t1 = (int)trsm.size();
         s->lvl_s1[l] = (int)stask.size();
         // number of sources of this level facing each cblk
@@ -441,6 +465,8 @@ int build_schedule(b200_solver_t *s) {
     RET(s->dupload(&s->d_stask, stask));
     RET(s->dupload(&s->d_stile, stile));
     RET(s->dupload(&s->d_dtask, dtask));
+    RET(s->dupload(&s->d_dtaskb, dtaskb));
+    RET(s->dupload(&s->d_leaf, leaf));
     RET(s->dupload(&s->d_diag_list, diag_list));
     {
         std::vector<int> small, big;
@@ -689,7 +715,16 @@ int enqueue_sweeps(b200_solver_t *s, double *x, double *aux, int64_t ldx, int nr
     const T *WL = (const T *)s->dWL;
     const T *WB = (s->facto == FACTO_GETRF) ? (const T *)s->dWU : WL;
     const int nlev = (int)s->levels.size();
+    // the diagonal-block products accumulate their K chunks: zero their outputs
+    CU(cudaMemset2DAsync(aux, (size_t)ldx * sizeof(double), 0, (size_t)s->n * sizeof(double), nrhs, st));
     for (int l = 0; l < nlev; l++) {
+        const int nlf = s->lvl_lf1[l] - s->lvl_lf0[l];
+        if (nlf > 0) {
+            if (tr) tr->begin(st);
+            launch_solve_leaf<T>(s->ds, s->d_leaf + s->lvl_lf0[l], nlf, L, WL, s->d_woff, x, aux, ldx, nrhs, 0, st);
+            if (tr) tr->end(3, st);
+            *launches += 1;
+        }
         const int nd = s->lvl_dt1[l] - s->lvl_dt0[l];
         if (tr) tr->begin(st);
         launch_solve_diag_inv<T>(s->ds, s->d_dtask + s->lvl_dt0[l], nd, WL, s->d_woff, x, aux, ldx, nrhs, 0, st);
@@ -698,22 +733,30 @@ int enqueue_sweeps(b200_solver_t *s, double *x, double *aux, int64_t ldx, int nr
         if (tr) tr->begin(st);
         launch_solve_tiles<T>(s->ds, s->d_stile + s->lvl_st0[l], ns, L, aux, x, ldx, nrhs, 0, st);
         if (tr) tr->end(2, st);
-        *launches += 1 + (ns > 0);
+        *launches += (nd > 0) + (ns > 0);
     }
     if (s->facto == FACTO_SYTRF) {
         launch_solve_scale_diag<T>(s->ds, s->d_lvl_cblk, s->cblknbr, L, aux, ldx, nrhs, st);
         *launches += 1;
     }
+    CU(cudaMemset2DAsync(x, (size_t)ldx * sizeof(double), 0, (size_t)s->n * sizeof(double), nrhs, st));
     for (int l = nlev - 1; l >= 0; l--) {
+        const int nlf = s->lvl_lf1[l] - s->lvl_lf0[l];
+        if (nlf > 0) {
+            if (tr) tr->begin(st);
+            launch_solve_leaf<T>(s->ds, s->d_leaf + s->lvl_lf0[l], nlf, Ub, WB, s->d_woff, x, aux, ldx, nrhs, 1, st);
+            if (tr) tr->end(3, st);
+            *launches += 1;
+        }
         const int ns = s->lvl_st1[l] - s->lvl_st0[l];
         if (tr) tr->begin(st);
         launch_solve_tiles<T>(s->ds, s->d_stile + s->lvl_st0[l], ns, Ub, x, aux, ldx, nrhs, 1, st);
         if (tr) tr->end(2, st);
-        const int nd = s->lvl_dt1[l] - s->lvl_dt0[l];
+        const int nd = s->lvl_db1[l] - s->lvl_db0[l];
         if (tr) tr->begin(st);
-        launch_solve_diag_inv<T>(s->ds, s->d_dtask + s->lvl_dt0[l], nd, WB, s->d_woff, aux, x, ldx, nrhs, 1, st);
+        launch_solve_diag_inv<T>(s->ds, s->d_dtaskb + s->lvl_db0[l], nd, WB, s->d_woff, aux, x, ldx, nrhs, 1, st);
         if (tr) tr->end(1, st);
-        *launches += 1 + (ns > 0);
+        *launches += (nd > 0) + (ns > 0);
     }
     CU(cudaGetLastError());
     return ERR_SUCCESS;
@@ -1383,17 +1426,20 @@ int b200_solve_trace(b200_solver_t *s, int64_t nrhs, double *ms, double *bytes) 
     s->kernel_launches += launches;
     tr.finish(ms);
     if (bytes) {
-        // algorithmic traffic: every factor entry once per sweep (LU: L then U) + vectors
-        double fb = 0, db = 0;
+        // algorithmic traffic: every factor entry (diagonal blocks: their inverses'
+        // triangles) once per sweep, x_k read and written per sweep, the rows below
+        // read and written per sweep; class 3 holds the cblks of <= 32 columns
+        for (int c = 0; c < 4; c++) bytes[c] = 0;
         for (int k = 0; k < s->cblknbr; k++) {
-            const double nc = s->ncols[k];
-            db += nc * nc * 0.5;
-            fb += (s->stride[k] - nc) * nc;
+            const double nc = s->ncols[k], m = s->stride[k] - nc, v = (double)nrhs * 8.0;
+            const double dbk = 2.0 * nc * nc * 0.5 * s->esz + 4.0 * nc * v;
+            const double obk = 2.0 * m * nc * s->esz + 4.0 * m * v;
+            if (s->ncols[k] <= 32) bytes[3] += dbk + obk;
+            else {
+                bytes[1] += dbk;
+                bytes[2] += obk;
+            }
         }
-        bytes[0] = 0;
-        bytes[1] = 2.0 * db * s->esz + 4.0 * n * nrhs * 8.0;
-        bytes[2] = 2.0 * fb * s->esz + 4.0 * (double)n * nrhs * 8.0;
-        bytes[3] = 0;
     }
     return ERR_SUCCESS;
 }
