@@ -381,36 +381,50 @@ __global__ void __launch_bounds__(256) diag_factor_kernel(DevSym s, const int *_
         }
         const int rest = n - p - pb;
         if (rest > 0) {
-            // rows below the tile: X = A op(T)^{-1} with the tile inverse
+            // rows below the tile: X = A op(T)^{-1}; Cholesky with the tile inverse,
+            // LU / LDL^T by substitution in the reference's order (indefinite or
+            // badly scaled tiles)
             for (int r = tid; r < rest; r += nth) {
                 T *row = A + (p + pb + r) + (size_t)p * ld;
                 T a[32];
 #pragma unroll
                 for (int c = 0; c < 32; c++) a[c] = (c < pb) ? row[(size_t)c * ld] : (T)0;
+                if (FACTO == FACTO_POTRF) {
 #pragma unroll
-                for (int c = 0; c < 32; c++) {
-                    if (c < pb) {
-                        T v = 0;
-                        if (FACTO == FACTO_GETRF) {
-                            // X = A U^{-1}: (U^{-1})[l][c] = inv(U^T)[c][l]
-#pragma unroll
-                            for (int l = 0; l <= c; l++) v += a[l] * wu[c + l * TP];
-                        } else {
+                    for (int c = 0; c < 32; c++) {
+                        if (c < pb) {
                             // X = A L^{-T}: (L^{-T})[l][c] = inv(L)[c][l]
+                            T v = 0;
 #pragma unroll
                             for (int l = 0; l <= c; l++) v += a[l] * wl[c + l * TP];
-                        }
-                        if (FACTO == FACTO_SYTRF) {
-                            A[(p + c) + (size_t)(p + pb + r) * ld] = v;          // (L D)^T in the upper part
-                            row[(size_t)c * ld] = v * ((T)1 / tile[c * (TP + 1)]);  // L
-                        } else {
                             row[(size_t)c * ld] = v;
+                        }
+                    }
+                } else {
+#pragma unroll
+                    for (int c = 0; c < 32; c++) {
+                        if (c < pb) {
+                            T v = a[c];
+#pragma unroll
+                            for (int l = 0; l < c; l++) {
+                                // GETRF: X U = A with U = the upper part; LDL^T: V L^T = A, unit L
+                                const T u = (FACTO == FACTO_GETRF) ? tile[l + c * TP] : tile[c + l * TP];
+                                v -= a[l] * u;
+                            }
+                            if (FACTO == FACTO_GETRF) v /= tile[c * (TP + 1)];
+                            a[c] = v;
+                            if (FACTO == FACTO_SYTRF) {
+                                A[(p + c) + (size_t)(p + pb + r) * ld] = v;          // (L D)^T in the upper part
+                                row[(size_t)c * ld] = v * ((T)1 / tile[c * (TP + 1)]);  // L
+                            } else {
+                                row[(size_t)c * ld] = v;
+                            }
                         }
                     }
                 }
             }
             if (FACTO == FACTO_GETRF) {
-                // columns right of the tile: Y = L_tile^{-1} A (unit lower)
+                // columns right of the tile: Y = L_tile^{-1} A (unit lower), by substitution
                 for (int cc = tid; cc < rest; cc += nth) {
                     T *col = A + p + (size_t)(p + pb + cc) * ld;
                     T a[32];
@@ -419,9 +433,10 @@ __global__ void __launch_bounds__(256) diag_factor_kernel(DevSym s, const int *_
 #pragma unroll
                     for (int l = 0; l < 32; l++) {
                         if (l < pb) {
-                            T v = 0;
+                            T v = a[l];
 #pragma unroll
-                            for (int m = 0; m <= l; m++) v += wl[l + m * TP] * a[m];
+                            for (int m = 0; m < l; m++) v -= tile[l + m * TP] * a[m];
+                            a[l] = v;
                             col[l] = v;
                         }
                     }
@@ -517,8 +532,9 @@ __global__ void __launch_bounds__(256) panel_trsm_kernel(DevSym s, const RowTask
             const int c = cg * CPG + q;
             if (q < CPG && c < w) xs[r + (cb + c) * TR] -= acc[q];
         }
+        if (!getrf && !scale_d) {
         // multiplier of this column block: M(l, c) = W[c][l] (W = the stored tile
-        // inverse, inv(L) or inv(U^T)), divided by D[c] for LDL^T
+        // inverse of the Cholesky factor)
         {
             const T *W = tinv + tinv_off[k] + (size_t)(cb >> 5) * 1024 * (getrf ? 2 : 1) + (which ? 32 * w : 0);
             for (int idx = tid; idx < 32 * 32; idx += nth) {
@@ -546,6 +562,28 @@ __global__ void __launch_bounds__(256) panel_trsm_kernel(DevSym s, const RowTask
             for (int q = 0; q < 8; q++) {
                 const int c = cg * CPG + q;
                 if (q < CPG && c < w) xs[r + (cb + c) * TR] = out[q];
+            }
+        }
+        } else {
+            // LU and LDL^T: substitution against the upper triangular block
+            // U(l, c) = op(T)[cb + l][cb + c] (LDL^T: D L^T; the U-side LU panel has a
+            // unit diagonal), the order of PaStiX's TRSM, which keeps indefinite or
+            // badly scaled diagonal blocks as accurate as the reference
+            for (int idx = tid; idx < 32 * 32; idx += nth) {
+                const int l = idx >> 5, c = idx & 31;
+                T v = 0;
+                if (l < w && c < w && c >= l)
+                    v = mode == 0 ? D[(cb + l) + (size_t)(cb + c) * ld] : D[(cb + c) + (size_t)(cb + l) * ld];
+                tt[l * TP + c] = v;
+            }
+            __syncthreads();
+            const bool unit = getrf && which == 0;
+            if (tid < TR) {
+                for (int c = 0; c < w; c++) {
+                    T x = xs[tid + (cb + c) * TR];
+                    for (int l = 0; l < c; l++) x -= xs[tid + (cb + l) * TR] * tt[l * TP + c];
+                    xs[tid + (cb + c) * TR] = unit ? x : x / tt[c * TP + c];
+                }
             }
         }
         __syncthreads();

@@ -368,20 +368,41 @@ __device__ __forceinline__ void stage_x(double *xs, const double *xv, const int 
     }
 }
 
+// D += A B with A 16 x 16 (a[2j], a[2j+1] = rows g, g + 8 of column 4j + tg), B 16 x 8
+// (b[j] = row 4j + tg, column g), the fragment layout of four m16n8k4 steps.
+__device__ __forceinline__ void dmma16x8x16(double (&c)[4], const double (&a)[8], const double (&b)[4]) {
+    asm volatile(
+        "mma.sync.aligned.m16n8k16.row.col.f64.f64.f64.f64 {%0,%1,%2,%3}, {%4,%5,%6,%7,%8,%9,%10,%11}, "
+        "{%12,%13,%14,%15}, {%0,%1,%2,%3};\n"
+        : "+d"(c[0]), "+d"(c[1]), "+d"(c[2]), "+d"(c[3])
+        : "d"(a[0]), "d"(a[1]), "d"(a[2]), "d"(a[3]), "d"(a[4]), "d"(a[5]), "d"(a[6]), "d"(a[7]), "d"(b[0]),
+          "d"(b[1]), "d"(b[2]), "d"(b[3]));
+}
+
 // acc += M_tile(op) x_tile over 64 K values; ROW = 1: output index = tile row
 // (a fragment reads ms[k * PM + out]), ROW = 0: output index = tile column
 // (ms[out * PM + k]).
 template <typename T, int PM, int ROW>
 __device__ __forceinline__ void tile_mma(double (&acc)[4][4], const T *ms, const double *xs, int o0w, int ntn) {
     const int lane = threadIdx.x & 31, g = lane >> 2, tg = lane & 3;
-#pragma unroll 4
-    for (int kk = 0; kk < STT; kk += 4) {
-        const int kq = kk + tg;
-        const double a0 = ROW ? (double)ms[kq * PM + o0w + g] : (double)ms[(o0w + g) * PM + kq];
-        const double a1 = ROW ? (double)ms[kq * PM + o0w + g + 8] : (double)ms[(o0w + g + 8) * PM + kq];
+#pragma unroll 2
+    for (int kk = 0; kk < STT; kk += 16) {
+        double a[8];
 #pragma unroll
-        for (int nt = 0; nt < 4; nt++)
-            if (nt < ntn) dmma16x8x4(acc[nt], a0, a1, xs[kq * SXP + nt * 8 + g]);
+        for (int j = 0; j < 4; j++) {
+            const int kq = kk + 4 * j + tg;
+            a[2 * j] = ROW ? (double)ms[kq * PM + o0w + g] : (double)ms[(o0w + g) * PM + kq];
+            a[2 * j + 1] = ROW ? (double)ms[kq * PM + o0w + g + 8] : (double)ms[(o0w + g + 8) * PM + kq];
+        }
+#pragma unroll
+        for (int nt = 0; nt < 4; nt++) {
+            if (nt < ntn) {
+                double b[4];
+#pragma unroll
+                for (int j = 0; j < 4; j++) b[j] = xs[(kk + 4 * j + tg) * SXP + nt * 8 + g];
+                dmma16x8x16(acc[nt], a, b);
+            }
+        }
     }
 }
 
