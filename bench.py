@@ -9,7 +9,7 @@ One step = the hot path from the matrix values resident in HBM to x at backward
 error <= 1e-12: numerical factorization + 16-RHS solve (+ FP64 iterative
 refinement for the mixed-precision path).  Both paths are measured:
   fp64  : FP64 factor (DMMA updates) + solve          -- the drop-in path
-  mixed : FP32 factor (tensor-core updates) + solve + FP64 CG refinement
+  mixed : FP32 factor (3xTF32 tcgen05 updates) + solve + FP64 CG refinement
 ``value`` is the numfact-equivalent throughput of the faster path that meets the
 accuracy target: PaStiX's theoretical flop count (DPARM_FACT_THFLOPS, SI) divided
 by that path's device time per step.
@@ -46,8 +46,13 @@ def parse():
     ap.add_argument("--nx", type=int, default=80)
     ap.add_argument("--points", type=int, default=27)
     ap.add_argument("--nrhs", type=int, default=16)
-    ap.add_argument("--mixed", default="auto", help="precision of the mixed path (fp32, tf32, tf32x3; auto = best built)")
+    ap.add_argument("--mixed", default="auto",
+                    help="precision of the mixed path (fp32, tf32, tf32x3; auto = tf32x3: FP32 factor with 3xTF32 "
+                         "tensor-core updates)")
     ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--numfact-once", default=None, metavar="PREC",
+                    help="profiling aid: one factorization of the workload in precision PREC (fp64, fp32, tf32, "
+                         "tf32x3) through the library, then exit")
     ap.add_argument("--cpu-budget", type=float, default=150.0, help="seconds of CPU time for the reference arm")
     return ap.parse_args()
 
@@ -301,6 +306,17 @@ def main():
     from pastix_b200.refhost import Analysis
 
     torch.cuda.set_device(local_rank)
+    if args.numfact_once:
+        A, xt, b, name = workload(args)
+        an = Analysis(A, "potrf")
+        s = native.Solver(an.structure(), "potrf", args.numfact_once)
+        s.bcsc_load(an.bcsc())
+        s.numfact(0.0)
+        st_ = s.stats()
+        print(json.dumps({"workload": name, "precision": args.numfact_once, "numfact_ms": st_["numfact_ms"],
+                          "launches": st_["launches_numfact"]}), flush=True)
+        s.close()
+        return 0
     dist = None
     if world > 1:
         import datetime
@@ -326,7 +342,7 @@ def main():
 
     mixed_prec = args.mixed
     if mixed_prec == "auto":
-        mixed_prec = os.environ.get("B200_MIXED", "fp32")
+        mixed_prec = os.environ.get("B200_MIXED", "tf32x3")
 
     stream = torch.cuda.Stream()
     nrhs, n = args.nrhs, A.n
@@ -335,11 +351,15 @@ def main():
     results = {}
     traces = {}
     solvers = {}
+    kinds_trace, kinds_launches = {}, {}
     for prec, refine in (("fp64", False), (mixed_prec, True)):
         s = native.Solver(st, "potrf", prec, stream=stream.cuda_stream)
         s.bcsc_load(bc)
         solvers[prec] = (s, refine)
         traces[prec] = s.numfact_trace(0.0)
+        kinds_trace[prec] = s.trace_kinds()
+        cls, _ = s.trace_launches()
+        kinds_launches[prec] = {n: int(np.sum(cls == i)) for i, n in enumerate(native.Solver.KIND_NAMES)}
 
     clk = ClockSampler(torch.cuda.current_device())
     if dist is not None:
@@ -370,21 +390,33 @@ def main():
     e2e_s, h2d, d2h = e2e_path(hs, bc, A, b, head["prec"], head["prec"] != "fp64", nrhs)
     e2e_value = world * st.thflops / e2e_s / 1e9
 
-    # roofline of the dominant kernel (the GEMM-scatter update) of the headline path
-    tr = traces[head["prec"]]
-    upd = tr["update"]
+    # roofline of the dominant kernel of the headline path: the update kind with
+    # the largest device time in the per-launch trace (CUDA events around every
+    # launch of one factorization), its algorithmic flops (useful products, PaStiX's
+    # counting) over that time, against the measured cuBLAS GEMM of the same type
+    kinds = kinds_trace[head["prec"]]
+    dom = max((k for k, v in kinds.items() if v["flops"] > 0), key=lambda k: kinds[k]["ms"])
+    dk = kinds[dom]
     peak_dtype = "fp64" if head["prec"] == "fp64" else ("tf32" if head["prec"].startswith("tf32") else "fp32")
     try:
         peak = gemm_peak_tflops(peak_dtype)
     except Exception:
         peak = None
-    achieved = upd["flops"] / (upd["ms"] * 1e-3) / 1e12 if upd["ms"] > 0 else 0.0
-    kname = "update_f64_kernel" if head["prec"] == "fp64" else "update_kernel_" + head["prec"]
+    achieved = dk["flops"] / (dk["ms"] * 1e-3) / 1e12 if dk["ms"] > 0 else 0.0
+    kname = {"update": "update_f64_kernel" if head["prec"] == "fp64" else "update_simt_f32_kernel",
+             "sub_update": "update_f64_kernel" if head["prec"] == "fp64" else "update_simt_f32_kernel",
+             "tc_update": "update_tc_kernel<%d>" % (1 if head["prec"] == "tf32x3" else 0)}[dom]
+    traffic = ncu_traffic(kname)
     roofline = {"bound": "tensor", "achieved": achieved, "peak": peak, "unit": "TFLOP/s",
-                "frac": (achieved / peak) if peak else None, "traffic": ncu_traffic(kname),
-                "kernel": kname,
-                "peak_source": f"measured cuBLAS {peak_dtype.upper()} GEMM on this GPU (bench.py)",
-                "share_of_numfact": upd["ms"] / max(sum(v["ms"] for v in tr.values()), 1e-9)}
+                "frac": (achieved / peak) if peak else None,
+                "traffic": traffic.get("bytes_per_launch") if traffic else None,
+                "kernel": kname, "trace_kind": dom, "launches": kinds_launches[head["prec"]].get(dom),
+                "mma_per_product": 3 if head["prec"] == "tf32x3" else 1,
+                "peak_source": f"measured cuBLAS {peak_dtype.upper()} GEMM on this GPU, in bench.py",
+                "share_of_numfact": dk["ms"] / max(sum(v["ms"] for v in kinds.values()), 1e-9),
+                "measured_peaks_json": {k: measured_peaks().get(k) for k in ("hbm_gbs", "bf16_tflops")}}
+    if traffic:
+        roofline["traffic_source"] = traffic.get("source")
 
     if rank == 0:
         line = {
@@ -401,6 +433,7 @@ def main():
             "speedup_mixed_vs_fp64": (results["fp64"]["step_ms"] / results[mixed_prec]["step_ms"]),
             "solve_latency_ms": {"p50": p50, "p99": p99, "nrhs": nrhs, "path": head["prec"]},
             "numfact_trace": traces,
+            "numfact_kinds": kinds_trace,
             "roofline": roofline,
             "cpu_baseline": cpu,
             "e2e": {"value": e2e_value, "unit": "GFLOP/s", "h2d_bytes_per_step": h2d, "d2h_bytes_per_step": d2h,

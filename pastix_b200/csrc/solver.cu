@@ -110,6 +110,7 @@ struct b200_solver_s {
         int tu0, tu1;  // internal updates on the tensor cores
         int tntiles;
         int sp0, sp1;  // operand copies for them
+        int tm0;       // their tile map
     };
     std::vector<std::vector<SubStep>> lvl_steps;
     SubTask *d_subtask = nullptr;
@@ -121,7 +122,8 @@ struct b200_solver_s {
     bool use_tc = false;
     int tc_min_k = 32, tc_min_m = 64;
     Upd *d_tcupd = nullptr;
-    std::vector<int> lvl_tc_u0, lvl_tc_u1, lvl_tc_tiles;
+    std::vector<int> lvl_tc_u0, lvl_tc_u1, lvl_tc_tiles, lvl_tc_m0;
+    int2 *d_tcmap = nullptr;              // tiles of each tensor-core launch: {update, row | col << 16}
     std::vector<char> tc_wanted;          // cblks whose panels the tensor-core updates read
     std::vector<int64_t> toff;            // operand copy of cblk k: row-major, pitch ncols rounded up to 4
     int64_t tsize = 0;                    // floats of one operand arena
@@ -136,6 +138,7 @@ struct b200_solver_s {
     int64_t total_tiles = 0;
     int trsm_smem = 0;                  // dynamic shared memory available to the panel TRSM
     double flops_class[4] = {0, 0, 0, 0};  // algorithmic flops per kernel class (see Trace)
+    double flops_kind[10] = {};            // algorithmic flops of the update kinds 3, 6, 8
     double bytes_scatter = 0;
 
     // bcsc
@@ -211,6 +214,7 @@ int build_schedule(b200_solver_t *s) {
     std::vector<SubTask> subtasks;
     std::vector<Upd> subupds;
     std::vector<Upd> tcupds;
+    std::vector<int2> tcmap;
     std::vector<SplitTask> splits;
     std::vector<char> ext_wanted(N, 0);   // cblks with external tensor-core updates
     s->lvl_sp0.assign(nlev, 0);
@@ -219,16 +223,31 @@ int build_schedule(b200_solver_t *s) {
     s->lvl_tc_u0.assign(nlev, 0);
     s->lvl_tc_u1.assign(nlev, 0);
     s->lvl_tc_tiles.assign(nlev, 0);
+    s->lvl_tc_m0.assign(nlev, 0);
     auto tc_ok = [&](const Upd &u) {
         return s->use_tc && !(u.flags & UPD_SCALE_D) && u.K >= s->tc_min_k && u.M >= s->tc_min_m &&
                (u.colK0 == 0 || u.K % 32 == 0);
     };
     // tensor-core tiles: 128 x 64
-    auto push_tc = [&](Upd u, int &t0) {
+    // useful flops of an update: the lower triangle of the diagonal square when symmetric
+    auto upd_flops = [](const Upd &u) {
+        const double mn = (u.flags & UPD_SYM) ? (double)u.N * (u.M - u.N) + 0.5 * u.N * (u.N + 1.0)
+                                              : (double)u.M * u.N;
+        return 2.0 * mn * u.K;
+    };
+    // base: first update of the launch the update belongs to (map entries are relative)
+    auto push_tc = [&](Upd u, int &t0, int base) {
+        s->flops_kind[8] += upd_flops(u);
         u.tiles_m = (u.M + 127) / 128;
         u.tiles_n = (u.N + 63) / 64;
         u.tile0 = t0;
-        t0 += u.tiles_m * u.tiles_n;
+        const int ui = (int)tcupds.size() - base;
+        for (int nt = 0; nt < u.tiles_n; nt++)
+            for (int mt = 0; mt < u.tiles_m; mt++) {
+                if ((u.flags & UPD_SYM) && mt * 128 + 127 < nt * 64) continue;  // above the diagonal
+                tcmap.push_back(make_int2(ui, mt | (nt << 16)));
+                t0++;
+            }
         s->tc_wanted[u.k] = 1;
         tcupds.push_back(u);
     };
@@ -304,6 +323,7 @@ int build_schedule(b200_solver_t *s) {
                 ss.t1 = (int)subtasks.size();
                 ss.u0 = (int)subupds.size();
                 ss.tu0 = (int)tcupds.size();
+                ss.tm0 = (int)tcmap.size();
                 ss.sp0 = (int)splits.size();
                 int t0 = 0, tt0 = 0;
                 for (auto &m : members) {
@@ -322,11 +342,12 @@ int build_schedule(b200_solver_t *s) {
                     u.colbase = c0 + 64;
                     u.flags = UPD_SYM | (s->facto == FACTO_SYTRF ? UPD_SCALE_D : 0);
                     if (tc_ok(u)) {
-                        push_tc(u, tt0);
+                        push_tc(u, tt0, ss.tu0);
                         for (int r0 = c0 + 64; r0 < s->stride[k]; r0 += 32)
                             for (int cc = c0; cc < c0 + 64; cc += 32) splits.push_back({k, r0, cc});
                         continue;
                     }
+                    s->flops_kind[6] += upd_flops(u);
                     u.tiles_m = (u.M + 63) / 64;
                     u.tiles_n = (u.N + 63) / 64;
                     u.tile0 = t0;
@@ -381,6 +402,7 @@ int build_schedule(b200_solver_t *s) {
         }
         L.u0 = (int)upds.size();
         s->lvl_tc_u0[l] = (int)tcupds.size();
+        s->lvl_tc_m0[l] = (int)tcmap.size();
         int tile0 = 0, tc_tile0 = 0;
         int64_t flops = 0;
         for (int i = L.c0; i < L.c1; i++) {
@@ -421,7 +443,7 @@ int build_schedule(b200_solver_t *s) {
                     flops += (int64_t)(2.0 * mn * u.K);
                     s->flops_class[3] += 2.0 * mn * u.K;
                     if (tc_ok(u)) {
-                        push_tc(u, tc_tile0);
+                        push_tc(u, tc_tile0, s->lvl_tc_u0[l]);
                         ext_wanted[k] = 1;
                         continue;
                     }
@@ -431,6 +453,7 @@ int build_schedule(b200_solver_t *s) {
                                                        : u.tiles_n * u.tiles_m;
                     u.tile0 = tile0;
                     tile0 += nt;
+                    s->flops_kind[3] += upd_flops(u);
                     upds.push_back(u);
                 }
             }
@@ -499,6 +522,7 @@ int build_schedule(b200_solver_t *s) {
     RET(s->dupload(&s->d_toff, toff));
     RET(s->dupload(&s->d_upd, upds));
     RET(s->dupload(&s->d_tcupd, tcupds));
+    RET(s->dupload(&s->d_tcmap, tcmap));
     RET(s->dupload(&s->d_split, splits));
     s->toff.assign(N, 0);
     int64_t tp = 0;
@@ -655,7 +679,7 @@ int enqueue_numfact(b200_solver_t *s, cudaStream_t st, Trace *tr = nullptr) {
                 launches += 1 + (s->facto == FACTO_GETRF);
                 if (tr) tr->end(9, st);
                 if (tr) tr->begin(st);
-                launch_update_tc(s->ds, s->d_tcupd + ss.tu0, ss.tu1 - ss.tu0, ss.tntiles, s->d_maps, (float *)L,
+                launch_update_tc(s->ds, s->d_tcupd + ss.tu0, s->d_tcmap + ss.tm0, ss.tntiles, s->d_maps, (float *)L,
                                  (float *)U, s->prec == B200_PREC_TF32X3, s->d_err, st);
                 launches++;
                 if (tr) tr->end(8, st);
@@ -676,9 +700,8 @@ int enqueue_numfact(b200_solver_t *s, cudaStream_t st, Trace *tr = nullptr) {
             launches += 1 + (s->facto == FACTO_GETRF);
             if (tr) tr->end(9, st);
             if (tr) tr->begin(st);
-            launch_update_tc(s->ds, s->d_tcupd + s->lvl_tc_u0[l], s->lvl_tc_u1[l] - s->lvl_tc_u0[l],
-                             s->lvl_tc_tiles[l], s->d_maps, (float *)L, (float *)U, s->prec == B200_PREC_TF32X3,
-                             s->d_err, st);
+            launch_update_tc(s->ds, s->d_tcupd + s->lvl_tc_u0[l], s->d_tcmap + s->lvl_tc_m0[l], s->lvl_tc_tiles[l],
+                             s->d_maps, (float *)L, (float *)U, s->prec == B200_PREC_TF32X3, s->d_err, st);
             launches++;
             if (tr) tr->end(8, st);
         }
@@ -903,6 +926,16 @@ int refine_cg(RefineCtx &c, const double *b, double *x, int itermax, double eps,
         c.count();
         launch_axpys(n, R, c.scal(0), -1.0, g2, n, gr, n, c.st);
         c.count();
+        // convergence test on the updated residual before the next preconditioner
+        // application, which the last iteration does not need
+        RET(c.dots(gr, gr, nr));
+        any = false;
+        for (int j = 0; j < R; j++) {
+            if (active[j] == 0.0) continue;
+            resid[j] = std::sqrt(nr[j]) / (nb[j] > 0 ? nb[j] : 1.0);
+            if (resid[j] > eps) any = true; else active[j] = 0.0;
+        }
+        if (!any || iter >= itermax) break;
         launch_copy(n, R, gr, n, gz, n, c.st);
         c.count();
         RET(c.spsv(gz));
@@ -911,13 +944,6 @@ int refine_cg(RefineCtx &c, const double *b, double *x, int itermax, double eps,
         RET(c.set_scal(tmp, 1));
         launch_xpbys(n, R, gz, n, c.scal(1), gp, n, c.st);
         c.count();
-        RET(c.dots(gr, gr, nr));
-        any = false;
-        for (int j = 0; j < R; j++) {
-            if (active[j] == 0.0) continue;
-            resid[j] = std::sqrt(nr[j]) / (nb[j] > 0 ? nb[j] : 1.0);
-            if (resid[j] > eps) any = true; else active[j] = 0.0;
-        }
     }
     berr = resid;
     *niter = iter;
@@ -1442,6 +1468,19 @@ int b200_solve_trace(b200_solver_t *s, int64_t nrhs, double *ms, double *bytes) 
         }
     }
     return ERR_SUCCESS;
+}
+
+int b200_trace_kinds(b200_solver_t *s, double *ms, double *flops, int nkinds) {
+    if (!s || nkinds < 0) return -ERR_BADPARAM;
+    const int nk = std::min(nkinds, 10);
+    for (int i = 0; i < nk; i++) {
+        if (ms) ms[i] = 0.0;
+        if (flops) flops[i] = s->flops_kind[i];
+    }
+    if (ms)
+        for (auto &pr : s->trace_detail)
+            if (pr.first < nk) ms[pr.first] += pr.second;
+    return nk;
 }
 
 int64_t b200_trace_launches(b200_solver_t *s, double *ms, int32_t *cls, int64_t cap) {

@@ -23,9 +23,10 @@
 //    accumulators) and issues tcgen05.mma (M = 128, N = 64, K = 8); each stage is
 //    released to the producer and each accumulator to the epilogue by
 //    tcgen05.commit on an mbarrier.
-//  * warps 2-5: epilogue.  Thread = accumulator row (TMEM lane quarter = warp % 4);
-//    tcgen05.ld the 64 columns, release the accumulator, scatter-add into f (atomic
-//    when another source of the level updates f), overlapping the next tile's MMAs.
+//  * warps 2-9: epilogue.  Thread = accumulator row (TMEM lane quarter = warp % 4),
+//    two warps per quarter with 32 columns each; tcgen05.ld, release the
+//    accumulator, scatter-add into f with reductions (red.global.add), overlapping
+//    the next tile's MMAs.
 //  * Every mbarrier wait is bounded and also gives up once another role has given
 //    up; the kernel then records bit 2 of err, waits (bounded) for its TMA loads and
 //    MMAs in flight, frees its TMEM and returns.
@@ -41,7 +42,8 @@ constexpr int TC_A_BYTES = TC_BM * TC_BK * 4;  // 16 KB
 constexpr int TC_B_BYTES = TC_BN * TC_BK * 4;  // 8 KB
 constexpr uint32_t TC_TMEM_COLS = 128;          // two accumulators of 64 columns
 constexpr long long TC_WAIT_CYCLES = 1000000000LL;  // about 0.5 s at the maximum SM clock
-constexpr int TC_THREADS = 192;
+constexpr int TC_THREADS = 320;  // producer, MMA, 8 epilogue warps
+constexpr int TC_EPI_WARPS = 8;
 
 template <int SPLIT>
 struct TcCfg {
@@ -128,15 +130,6 @@ __device__ __forceinline__ void umma_commit(uint32_t bar) {
                  : "memory");
 }
 
-__device__ __forceinline__ int tc_find_update(const Upd *__restrict__ upds, int nupd, int tile) {
-    int lo = 0, hi = nupd - 1;
-    while (lo < hi) {
-        const int mid = (lo + hi + 1) >> 1;
-        if (upds[mid].tile0 <= tile) lo = mid; else hi = mid - 1;
-    }
-    return lo;
-}
-
 __device__ __forceinline__ int tc_dest_row(const DevSym &s, int k, int f, int prow) {
     int lo = s.fblok[k], hi = s.fblok[k + 1] - 1;
     while (lo < hi) {
@@ -153,19 +146,20 @@ __device__ __forceinline__ int tc_dest_row(const DevSym &s, int k, int f, int pr
     return s.rowoff[flo] + (grow - s.frow[flo]);
 }
 
-// Tile t of the launch: its update, row tile and column tile; false for a tile
-// entirely above the diagonal of a symmetric update (nothing to compute).
+// Tile t of the launch from the host-built tile map {update, row tile | column
+// tile << 16} (tiles entirely above the diagonal of a symmetric update are not
+// listed): two loads instead of a search.
 struct TcTile {
     Upd u;
     int mt, nt;
 };
 
-__device__ __forceinline__ bool tc_decode(const Upd *__restrict__ upds, int nupd, int t, TcTile &tt) {
-    tt.u = upds[tc_find_update(upds, nupd, t)];
-    const int lt = t - tt.u.tile0;
-    tt.mt = lt % tt.u.tiles_m;
-    tt.nt = lt / tt.u.tiles_m;
-    return !((tt.u.flags & UPD_SYM) && tt.mt * TC_BM + TC_BM - 1 < tt.nt * TC_BN);
+__device__ __forceinline__ void tc_decode(const Upd *__restrict__ upds, const int2 *__restrict__ tmap, int t,
+                                          TcTile &tt) {
+    const int2 e = tmap[t];
+    tt.u = upds[e.x];
+    tt.mt = e.y & 0xffff;
+    tt.nt = e.y >> 16;
 }
 
 // ---------------------------------------------------------------- operand copies
@@ -212,8 +206,9 @@ void launch_panel_split(const DevSym &s, const SplitTask *tasks, int ntasks, con
 
 // maps[(side * 2 + part) * cblknbr + k]: side 0 L / 1 U, part 0 hi / 1 lo
 template <int SPLIT>
-__global__ void __launch_bounds__(TC_THREADS, 1) update_tc_kernel(DevSym s, const Upd *__restrict__ upds, int nupd,
-                                                                  int ntiles, const CUtensorMap *__restrict__ maps,
+__global__ void __launch_bounds__(TC_THREADS, 1) update_tc_kernel(DevSym s, const Upd *__restrict__ upds,
+                                                                  const int2 *__restrict__ tmap, int ntiles,
+                                                                  const CUtensorMap *__restrict__ maps,
                                                                   float *L, float *U, int *err) {
     using Cfg = TcCfg<SPLIT>;
     constexpr int NST = Cfg::NST;
@@ -238,7 +233,7 @@ __global__ void __launch_bounds__(TC_THREADS, 1) update_tc_kernel(DevSym s, cons
         }
         for (int i = 0; i < 2; i++) {
             mbar_init(smem_addr(&tfull_bar[i]), 1);
-            mbar_init(smem_addr(&tempty_bar[i]), 4);  // one arrival per epilogue warp
+            mbar_init(smem_addr(&tempty_bar[i]), TC_EPI_WARPS);  // one arrival per epilogue warp
         }
         mbar_init(smem_addr(&fin_bar), 1);
         asm volatile("fence.mbarrier_init.release.cluster;\n" ::: "memory");
@@ -265,7 +260,7 @@ __global__ void __launch_bounds__(TC_THREADS, 1) update_tc_kernel(DevSym s, cons
             bool ok = true;
             for (int t = blockIdx.x; t < ntiles && ok; t += gridDim.x) {
                 TcTile tt;
-                if (!tc_decode(upds, nupd, t, tt)) continue;
+                tc_decode(upds, tmap, t, tt);
                 const Upd &u = tt.u;
                 const int side_a = (u.flags & UPD_A_U) ? 1 : 0, side_b = (u.flags & UPD_B_U) ? 1 : 0;
                 const CUtensorMap *ma = maps + (size_t)(side_a * 2) * N + u.k;
@@ -306,7 +301,7 @@ __global__ void __launch_bounds__(TC_THREADS, 1) update_tc_kernel(DevSym s, cons
             bool ok = true;
             for (int t = blockIdx.x; t < ntiles && ok; t += gridDim.x) {
                 TcTile tt;
-                if (!tc_decode(upds, nupd, t, tt)) continue;
+                tc_decode(upds, tmap, t, tt);
                 const int a = tl & 1;
                 if (tl >= 2 && !mbar_wait(smem_addr(&tempty_bar[a]), ((tl >> 1) - 1) & 1, &abort_sh)) {
                     ok = false;
@@ -347,13 +342,14 @@ __global__ void __launch_bounds__(TC_THREADS, 1) update_tc_kernel(DevSym s, cons
             mbar_wait(smem_addr(&fin_bar), 0, nullptr);
         }
     } else {
-        // ------------------------------------------------ epilogue (warps 2-5)
-        const int q = warp & 3;  // TMEM lane quarter this warp may access
+        // ------------------------------------------------ epilogue (warps 2-9)
+        const int q = warp & 3;                 // TMEM lane quarter this warp may access
+        const int c0 = ((warp - 2) >> 2) * 32;  // its half of the 64 columns
         const int row = q * 32 + lane;
         int tl = 0;
         for (int t = blockIdx.x; t < ntiles; t += gridDim.x) {
             TcTile tt;
-            if (!tc_decode(upds, nupd, t, tt)) continue;
+            tc_decode(upds, tmap, t, tt);
             const Upd &u = tt.u;
             const int a = tl & 1;
             const int lr = tt.mt * TC_BM + row;
@@ -363,10 +359,10 @@ __global__ void __launch_bounds__(TC_THREADS, 1) update_tc_kernel(DevSym s, cons
                 break;
             }
             asm volatile("tcgen05.fence::after_thread_sync;\n" ::: "memory");
-            uint32_t v[TC_BN];
-            const uint32_t taddr = tmem + ((uint32_t)(q * 32) << 16) + (uint32_t)(a * TC_BN);
+            uint32_t v[32];
+            const uint32_t taddr = tmem + ((uint32_t)(q * 32) << 16) + (uint32_t)(a * TC_BN + c0);
 #pragma unroll
-            for (int cb = 0; cb < TC_BN; cb += 16) {
+            for (int cb = 0; cb < 32; cb += 16) {
                 asm volatile(
                     "tcgen05.ld.sync.aligned.32x32b.x16.b32 {%0,%1,%2,%3,%4,%5,%6,%7,%8,%9,%10,%11,%12,%13,%14,%15}, "
                     "[%16];\n"
@@ -383,30 +379,17 @@ __global__ void __launch_bounds__(TC_THREADS, 1) update_tc_kernel(DevSym s, cons
             __syncwarp();
             if (lane == 0) mbar_arrive(smem_addr(&tempty_bar[a]));
             if (d >= 0) {
+                // reductions without a returned value: no load latency on the SM, and
+                // consecutive rows of a warp merge into one L2 transaction per column
                 float *C = ((u.flags & UPD_C_U) ? U : L) + s.off[u.f];
                 const size_t ldf = (size_t)s.ld[u.f];
-                const bool atomic = (u.flags & UPD_ATOMIC) != 0;
-                const int cmax = min(TC_BN, u.N - tt.nt * TC_BN);
-                const int csym = (u.flags & UPD_SYM) ? lr - tt.nt * TC_BN : TC_BN - 1;  // last column kept
+                const int cmax = min(TC_BN, u.N - tt.nt * TC_BN) - c0;
+                const int csym = (u.flags & UPD_SYM) ? lr - tt.nt * TC_BN - c0 : 31;  // last column kept
                 const int cend = min(cmax, csym + 1);
-                float *p = C + d + (size_t)(u.colbase + tt.nt * TC_BN) * ldf;
-                if (atomic) {
+                float *p = C + d + (size_t)(u.colbase + tt.nt * TC_BN + c0) * ldf;
 #pragma unroll
-                    for (int c = 0; c < TC_BN; c++)
-                        if (c < cend) atomicAdd(p + (size_t)c * ldf, -__uint_as_float(v[c]));
-                } else {
-                    // all loads of a 32-column half first, then the stores: one memory
-                    // latency per half instead of one per column
-#pragma unroll
-                    for (int h = 0; h < TC_BN; h += 32) {
-                        float old[32];
-#pragma unroll
-                        for (int c = 0; c < 32; c++) old[c] = (h + c < cend) ? p[(size_t)(h + c) * ldf] : 0.f;
-#pragma unroll
-                        for (int c = 0; c < 32; c++)
-                            if (h + c < cend) p[(size_t)(h + c) * ldf] = old[c] - __uint_as_float(v[h + c]);
-                    }
-                }
+                for (int c = 0; c < 32; c++)
+                    if (c < cend) atomicAdd(p + (size_t)c * ldf, -__uint_as_float(v[c]));
             }
             tl++;
         }
@@ -422,15 +405,15 @@ __global__ void __launch_bounds__(TC_THREADS, 1) update_tc_kernel(DevSym s, cons
 
 static int g_num_sms = 0;
 
-void launch_update_tc(const DevSym &s, const Upd *upds, int nupd, int ntiles, const void *maps, float *L, float *U,
-                      int split, int *err, cudaStream_t st) {
+void launch_update_tc(const DevSym &s, const Upd *upds, const int2 *tmap, int ntiles, const void *maps, float *L,
+                      float *U, int split, int *err, cudaStream_t st) {
     if (ntiles <= 0) return;
     const CUtensorMap *m = static_cast<const CUtensorMap *>(maps);
     const int grid = ntiles < g_num_sms ? ntiles : g_num_sms;
     if (split)
-        update_tc_kernel<1><<<grid, TC_THREADS, TcCfg<1>::SMEM, st>>>(s, upds, nupd, ntiles, m, L, U, err);
+        update_tc_kernel<1><<<grid, TC_THREADS, TcCfg<1>::SMEM, st>>>(s, upds, tmap, ntiles, m, L, U, err);
     else
-        update_tc_kernel<0><<<grid, TC_THREADS, TcCfg<0>::SMEM, st>>>(s, upds, nupd, ntiles, m, L, U, err);
+        update_tc_kernel<0><<<grid, TC_THREADS, TcCfg<0>::SMEM, st>>>(s, upds, tmap, ntiles, m, L, U, err);
 }
 
 int configure_tc_kernels() {

@@ -24,7 +24,7 @@ _lib = None
 
 # exported symbols, in the order of include/pastix_b200.h
 SYMBOLS = ["b200_solver_create", "b200_solver_destroy", "b200_bcsc_load", "b200_numfact", "b200_numfact_trace",
-           "b200_solve_trace", "b200_trace_launches", "b200_solve",
+           "b200_solve_trace", "b200_trace_launches", "b200_trace_kinds", "b200_solve",
            "b200_solve_device", "b200_solve_device_noalloc", "b200_refine", "b200_refine_device", "b200_spmv", "b200_factor_download",
            "b200_stats", "b200_strerror"]
 
@@ -55,6 +55,7 @@ def lib():
         L.b200_solve_trace.argtypes = [_P, _I64, _P, _P]
         L.b200_trace_launches.argtypes = [_P, _P, _P, _I64]
         L.b200_trace_launches.restype = _I64
+        L.b200_trace_kinds.argtypes = [_P, _P, _P, C.c_int]
         L.b200_solve_device.argtypes = [_P, _I64, _P, _I64, _P]
         L.b200_solve_device_noalloc.argtypes = [_P, _I64, _P, _I64, _P]
         L.b200_refine.argtypes = [_P, _I64, _P, _I64, _P, _I64, C.c_int, C.c_double, _I64, _I64,
@@ -146,6 +147,16 @@ class Solver:
         cls = np.zeros(max(cnt, 1), dtype=np.int32)
         lib().b200_trace_launches(self.h, _p(ms), _p(cls), cnt)
         return cls[:cnt], ms[:cnt]
+
+    KIND_NAMES = ["scatter", "diag", "trsm", "update", "sub_diag", "sub_trsm", "sub_update", "inverse",
+                  "tc_update", "tc_split"]
+
+    def trace_kinds(self) -> dict:
+        """Per-kind device time and algorithmic flops of the last numfact trace."""
+        ms = np.zeros(10)
+        fl = np.zeros(10)
+        lib().b200_trace_kinds(self.h, _p(ms), _p(fl), 10)
+        return {n: dict(ms=float(ms[i]), flops=float(fl[i])) for i, n in enumerate(self.KIND_NAMES)}
 
     def solve(self, b: np.ndarray) -> np.ndarray:
         x = np.asfortranarray(np.array(b, dtype=np.float64).reshape(self.n, -1))
