@@ -9,6 +9,7 @@
 //  update_simt_kernel  the same update for FP32 factors on CUDA cores
 #include "b200_internal.h"
 #include "kernels.h"
+#include "tile_ops.cuh"
 
 #include <algorithm>
 
@@ -70,7 +71,6 @@ __global__ void scatter_kernel(int64_t nnz, const int64_t *__restrict__ dest, co
 
 // ------------------------------------------------------------------ diagonal blocks
 
-constexpr int TP = 33;  // padded leading dimension of 32x32 shared tiles
 
 // Unblocked factorization of a pb x pb tile by one warp, in shared memory (lane =
 // row); low register use for the many-CTA diagonal kernel.
@@ -211,32 +211,6 @@ __device__ void factor_tile(T *t, int pb, int lane, double thr, int *piv, int *e
         // LDL^T keeps the D L^T copies of the upper part written above
         if (FACTO != FACTO_SYTRF || j <= lane) t[lane + j * TP] = r[j];
     }
-    __syncwarp();
-}
-
-// Inverse of the lower triangle of a pb x pb tile by one warp: lane j forms column
-// j of W by forward substitution, W[m][j] = (delta_mj - sum_{p<m} T[m][p] W[p][j])
-// / T[m][m] (T[m][m] = 1 if unit), with row m of T broadcast by warp shuffles and
-// the reciprocals of the diagonal formed first.  trans = 1 inverts the lower
-// triangle of T^T (the upper triangle of T read transposed).  Rows and columns
-// >= pb of W are zero.  Called by a whole warp.
-template <typename T>
-__device__ void invert_lower_tile(const T *t, T *w, int pb, int lane, int unit, int trans) {
-    T r[32];  // row `lane` of the triangle to invert
-#pragma unroll
-    for (int p = 0; p < 32; p++) r[p] = trans ? t[p + lane * TP] : t[lane + p * TP];
-    const T rd = unit ? (T)1 : (T)1 / r[lane];  // reciprocal of this lane's diagonal entry
-    T x[32];
-#pragma unroll
-    for (int m = 0; m < 32; m++) {
-        T acc = (lane == m) ? (T)1 : (T)0;
-#pragma unroll
-        for (int p = 0; p < m; p++) acc -= __shfl_sync(0xffffffffu, r[p], m) * x[p];
-        const T rm = __shfl_sync(0xffffffffu, rd, m);
-        x[m] = (m < pb && lane < pb) ? acc * rm : (T)0;
-    }
-#pragma unroll
-    for (int m = 0; m < 32; m++) w[m + lane * TP] = x[m];
     __syncwarp();
 }
 

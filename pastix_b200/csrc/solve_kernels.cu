@@ -12,6 +12,7 @@
 //  permute_kernel           bvec_zlapmr with peritab (bcsc/bvec_zcompute.c:875)
 #include "b200_internal.h"
 #include "kernels.h"
+#include "tile_ops.cuh"
 
 namespace b200 {
 
@@ -656,115 +657,98 @@ template void launch_solve_tiles<float>(const DevSym &, const SolveTile *, int, 
 //   phase 2: block column j of W by one warp: W_ij = -W_ii sum_{j<=m<i} T_im W_mj.
 namespace b200 {
 
-constexpr int IVP = 33;
-constexpr int DIAG_INV_SMEM = 2 * 8 * 32 * IVP * sizeof(double);
+constexpr int INV_WARPS = 4;
+constexpr int DIAG_INV_SMEM = INV_WARPS * 2 * 32 * TP * sizeof(double);
 
+// W_k = T_k^{-1} for the lower-triangular diagonal block T_k of every listed cblk
+// (L_kk, unit for LDL^T and LU; for the backward sweep of LU the stored U_kk^T).
+// With W the diagonal solves of both sweeps are plain products on tensor cores.
+// One CTA of 4 warps per cblk, 32 x 32 blocks:
+//   phase 1: every diagonal block inverted by one warp (invert_lower_tile);
+//   phase 2: block rows in order, the blocks of a row in parallel over the warps:
+//            W_ij = -W_ii sum_{j <= m < i} T_im W_mj, each product from shared-memory
+//            copies of T_im and W_mj staged with all loads in flight.
 template <typename T>
-__global__ void __launch_bounds__(256) diag_inverse_kernel(DevSym s, const int *__restrict__ cblks,
+__global__ void __launch_bounds__(128) diag_inverse_kernel(DevSym s, const int *__restrict__ cblks,
                                                            const T *__restrict__ Lsrc, T *W,
                                                            const int64_t *__restrict__ woff, int unit) {
     extern __shared__ __align__(16) double inv_smem[];
-    double *tl_all = inv_smem;                 // per warp: T tile, then W_mj tile
-    double *wi_all = inv_smem + 8 * 32 * IVP;  // per warp: W_ii
+    const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
+    double *ta = inv_smem + warp * 2 * 32 * TP;
+    double *tb = ta + 32 * TP;
     const int k = cblks[blockIdx.x];
     const int n = s.ncols[k], ld = s.ld[k];
     const T *Tk = Lsrc + s.off[k];
     T *Wk = W + woff[k];
-    const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
     const int nb = (n + 31) / 32;
-    double *t = tl_all + warp * 32 * IVP;
-    double *w = wi_all + warp * 32 * IVP;
-    // phase 1: inverse of every diagonal 32x32 tile
-    for (int b = warp; b < nb; b += 8) {
+    // phase 1: diagonal blocks; the blocks above them are zero
+    for (int b = warp; b < nb; b += INV_WARPS) {
         const int b0 = b * 32, bw = min(32, n - b0);
         for (int idx = lane; idx < 32 * 32; idx += 32) {
             const int i = idx & 31, j = idx >> 5;
-            t[i + j * IVP] = (i < bw && j < bw && i >= j) ? (double)Tk[(b0 + i) + (size_t)(b0 + j) * ld] : 0.0;
+            ta[i + j * TP] = (i < bw && j < bw && i >= j) ? (double)Tk[(b0 + i) + (size_t)(b0 + j) * ld] : 0.0;
         }
         __syncwarp();
-        // lane i computes row i of the inverse: W[i][i] = 1/T[i][i];
-        // W[i][j] = -(1/T[i][i]) sum_{m=j}^{i-1} T[i][m] W[m][j]  (rows in order)
-        for (int i = 0; i < bw; i++) {
-            if (lane <= i) {
-                const int j = lane;
-                const double dii = unit ? 1.0 : t[i + i * IVP];
-                double v;
-                if (j == i) {
-                    v = 1.0 / dii;
-                } else {
-                    double acc = 0.0;
-                    for (int m = j; m < i; m++) acc += t[i + m * IVP] * w[m + j * IVP];
-                    v = -acc / dii;
-                }
-                w[i + j * IVP] = v;
-            }
-            __syncwarp();
-        }
-        for (int idx = lane; idx < 32 * 32; idx += 32) {
+        invert_lower_tile<double>(ta, tb, bw, lane, unit, 0);
+        for (int idx = lane; idx < 32 * bw; idx += 32) {
             const int i = idx & 31, j = idx >> 5;
-            if (i < bw && j < bw) Wk[(b0 + i) + (size_t)(b0 + j) * n] = (T)((i >= j) ? w[i + j * IVP] : 0.0);
+            if (i < bw) Wk[(b0 + i) + (size_t)(b0 + j) * n] = (T)tb[i + j * TP];
+        }
+        for (int idx = lane; idx < b0 * bw; idx += 32) {
+            const int i = idx % b0, j = idx / b0;
+            Wk[i + (size_t)(b0 + j) * n] = (T)0;
         }
         __syncwarp();
     }
     __syncthreads();
-    // phase 2: the blocks below the diagonal, one block column per warp
-    for (int bj = warp; bj < nb; bj += 8) {
-        const int j0 = bj * 32, jw = min(32, n - j0);
-        // zero the strict upper blocks of this block column (W is lower triangular)
-        for (int bi = 0; bi < bj; bi++) {
-            const int i0 = bi * 32;
-            for (int idx = lane; idx < 32 * jw; idx += 32) {
-                const int i = idx & 31, j = idx >> 5;
-                if (i0 + i < n) Wk[(i0 + i) + (size_t)(j0 + j) * n] = (T)0;
-            }
-        }
-        for (int bi = bj + 1; bi < nb; bi++) {
-            const int i0 = bi * 32, iw = min(32, n - i0);
-            // acc (row = lane) = sum_{m = bj}^{bi-1} T[i0.., m0..] * W[m0.., j0..]
+    // phase 2
+    for (int bi = 1; bi < nb; bi++) {
+        const int i0 = bi * 32, iw = min(32, n - i0);
+        for (int bj = warp; bj < bi; bj += INV_WARPS) {
+            const int j0 = bj * 32, jw = min(32, n - j0);
             double acc[32];
 #pragma unroll
             for (int j = 0; j < 32; j++) acc[j] = 0.0;
             for (int bm = bj; bm < bi; bm++) {
                 const int m0 = bm * 32, mw = min(32, n - m0);
-                __syncwarp();
                 for (int idx = lane; idx < 32 * 32; idx += 32) {
                     const int i = idx & 31, j = idx >> 5;
-                    t[i + j * IVP] = (i < mw && j < jw) ? (double)Wk[(m0 + i) + (size_t)(j0 + j) * n] : 0.0;
+                    ta[i + j * TP] = (i < iw && j < mw) ? (double)Tk[(i0 + i) + (size_t)(m0 + j) * ld] : 0.0;
+                    tb[i + j * TP] = (i < mw && j < jw) ? (double)Wk[(m0 + i) + (size_t)(j0 + j) * n] : 0.0;
                 }
                 __syncwarp();
-                if (lane < iw) {
-                    for (int m = 0; m < mw; m++) {
-                        const double tv = (double)Tk[(i0 + lane) + (size_t)(m0 + m) * ld];
+#pragma unroll 4
+                for (int m = 0; m < 32; m++) {
+                    const double tv = ta[lane + m * TP];
 #pragma unroll
-                        for (int j = 0; j < 32; j++) acc[j] += tv * t[m + j * IVP];
-                    }
+                    for (int j = 0; j < 32; j++) acc[j] += tv * tb[m + j * TP];
                 }
+                __syncwarp();
             }
-            __syncwarp();
-            // W_ij = -W_ii acc : W_ii read back from the output (written in phase 1)
+            // W_ij = -W_ii acc (W_ii written in phase 1)
             for (int idx = lane; idx < 32 * 32; idx += 32) {
                 const int i = idx & 31, j = idx >> 5;
-                w[i + j * IVP] = (i < iw && j < iw) ? (double)Wk[(i0 + i) + (size_t)(i0 + j) * n] : 0.0;
+                tb[i + j * TP] = (i < iw && j < iw && i >= j) ? (double)Wk[(i0 + i) + (size_t)(i0 + j) * n] : 0.0;
             }
-            // stage acc in t (row lane)
-            __syncwarp();
 #pragma unroll
-            for (int j = 0; j < 32; j++) t[lane + j * IVP] = acc[j];
+            for (int j = 0; j < 32; j++) ta[lane + j * TP] = acc[j];
             __syncwarp();
             if (lane < iw) {
                 double out[32];
 #pragma unroll
                 for (int j = 0; j < 32; j++) out[j] = 0.0;
-                for (int m = 0; m <= lane; m++) {
-                    const double wv = w[lane + m * IVP];
+                for (int l = 0; l <= lane; l++) {
+                    const double wv = tb[lane + l * TP];
 #pragma unroll
-                    for (int j = 0; j < 32; j++) out[j] += wv * t[m + j * IVP];
+                    for (int j = 0; j < 32; j++) out[j] -= wv * ta[l + j * TP];
                 }
 #pragma unroll
                 for (int j = 0; j < 32; j++)
-                    if (j < jw) Wk[(i0 + lane) + (size_t)(j0 + j) * n] = (T)(-out[j]);
+                    if (j < jw) Wk[(i0 + lane) + (size_t)(j0 + j) * n] = (T)out[j];
             }
+            __syncwarp();
         }
+        __syncthreads();
     }
 }
 
@@ -772,7 +756,7 @@ template <typename T>
 void launch_diag_inverse(const DevSym &s, const int *cblks, int ncblk, const T *L, T *W, const int64_t *woff,
                          int unit, cudaStream_t st) {
     if (ncblk <= 0) return;
-    diag_inverse_kernel<T><<<ncblk, 256, DIAG_INV_SMEM, st>>>(s, cblks, L, W, woff, unit);
+    diag_inverse_kernel<T><<<ncblk, 32 * INV_WARPS, DIAG_INV_SMEM, st>>>(s, cblks, L, W, woff, unit);
 }
 
 template <typename T>
