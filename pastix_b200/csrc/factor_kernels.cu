@@ -1025,6 +1025,86 @@ void launch_scatter(int64_t nnz, const int64_t *dest, const double *Lv, const do
     scatter_kernel<T><<<(unsigned)((nnz + bs - 1) / bs), bs, 0, st>>>(nnz, dest, Lv, Uv, L, U);
 }
 
+// Diagonal blocks of cblks with at most 32 columns, one warp per cblk (the bottom
+// levels of the tree hold tens of thousands): the single-panel case of
+// diag_factor_kernel -- geadd of U^T for LU, factor_tile, the tile inverse(s) for
+// the panel TRSM, write-back (and U^T for LU).
+constexpr int DS_WARPS = 4;
+
+template <typename T, int FACTO>
+__global__ void __launch_bounds__(32 * DS_WARPS) diag_small_kernel(DevSym s, const int *__restrict__ cblks, int ncblk,
+                                                                   T *L, T *U, T *tinv,
+                                                                   const int64_t *__restrict__ tinv_off,
+                                                                   const double *__restrict__ thr_ptr,
+                                                                   unsigned long long *npiv, int *err) {
+    extern __shared__ __align__(16) unsigned char ds_smem[];
+    const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+    constexpr int NT = (FACTO == FACTO_GETRF) ? 3 : 2;
+    T *tile = reinterpret_cast<T *>(ds_smem) + (size_t)warp * NT * 32 * TP;
+    T *wl = tile + 32 * TP;
+    T *wu = wl + 32 * TP;
+    __shared__ int s_piv[DS_WARPS], s_err[DS_WARPS];
+    const int ci = blockIdx.x * DS_WARPS + warp;
+    if (ci >= ncblk) return;
+    const int k = cblks[ci];
+    const int n = s.ncols[k], ld = s.ld[k];
+    const double thr = *thr_ptr;
+    T *A = L + s.off[k];
+    if (lane == 0) { s_piv[warp] = 0; s_err[warp] = 0; }
+    for (int idx = lane; idx < 32 * 32; idx += 32) {
+        const int i = idx & 31, j = idx >> 5;
+        T v = 0;
+        if (i < n && j < n) {
+            v = A[i + (size_t)j * ld];
+            if (FACTO == FACTO_GETRF) v += U[s.off[k] + j + (size_t)i * ld];
+        }
+        tile[i + j * TP] = v;
+    }
+    __syncwarp();
+    factor_tile<T, FACTO>(tile, n, lane, thr, &s_piv[warp], &s_err[warp]);
+    invert_lower_tile<T>(tile, wl, n, lane, FACTO != FACTO_POTRF, 0);
+    if (FACTO == FACTO_GETRF) invert_lower_tile<T>(tile, wu, n, lane, 0, 1);  // inv(U^T)
+    T *tp = tinv + tinv_off[k];
+    for (int idx = lane; idx < 32 * 32; idx += 32) {
+        const int i = idx & 31, j = idx >> 5;
+        if (i < n && j < n && (FACTO != FACTO_POTRF || i >= j)) {
+            A[i + (size_t)j * ld] = tile[i + j * TP];
+            if (FACTO == FACTO_GETRF) U[s.off[k] + j + (size_t)i * ld] = tile[i + j * TP];
+        }
+        if (j < n) {
+            tp[i + j * 32] = wl[i + j * TP];
+            if (FACTO == FACTO_GETRF) tp[32 * n + i + j * 32] = wu[i + j * TP];
+        }
+    }
+    __syncwarp();
+    if (lane == 0) {
+        if (s_piv[warp]) atomicAdd(npiv, (unsigned long long)s_piv[warp]);
+        if (s_err[warp]) atomicOr(err, 1);
+    }
+}
+
+template <typename T>
+void launch_diag_small(int facto, const DevSym &s, const int *cblks, int ncblk, T *L, T *U, T *tinv,
+                       const int64_t *tinv_off, const double *thr, unsigned long long *npiv, int *err,
+                       cudaStream_t st) {
+    if (ncblk <= 0) return;
+    const int grid = (ncblk + DS_WARPS - 1) / DS_WARPS;
+    const size_t smem = (size_t)DS_WARPS * (facto == FACTO_GETRF ? 3 : 2) * 32 * TP * sizeof(T);
+    if (facto == FACTO_POTRF)
+        diag_small_kernel<T, FACTO_POTRF><<<grid, 32 * DS_WARPS, smem, st>>>(s, cblks, ncblk, L, U, tinv, tinv_off, thr,
+                                                                           npiv, err);
+    else if (facto == FACTO_GETRF)
+        diag_small_kernel<T, FACTO_GETRF><<<grid, 32 * DS_WARPS, smem, st>>>(s, cblks, ncblk, L, U, tinv, tinv_off, thr,
+                                                                           npiv, err);
+    else
+        diag_small_kernel<T, FACTO_SYTRF><<<grid, 32 * DS_WARPS, smem, st>>>(s, cblks, ncblk, L, U, tinv, tinv_off, thr,
+                                                                           npiv, err);
+}
+template void launch_diag_small<double>(int, const DevSym &, const int *, int, double *, double *, double *,
+                                        const int64_t *, const double *, unsigned long long *, int *, cudaStream_t);
+template void launch_diag_small<float>(int, const DevSym &, const int *, int, float *, float *, float *,
+                                       const int64_t *, const double *, unsigned long long *, int *, cudaStream_t);
+
 template <typename T>
 void launch_diag(int facto, const DevSym &s, const int *cblks, int ncblk, T *L, T *U, T *tinv,
                  const int64_t *tinv_off, const double *thr, unsigned long long *npiv, int *err, cudaStream_t st) {
@@ -1079,6 +1159,10 @@ int configure_factor_kernels() {
         raise_smem(subpanel_trsm_kernel<float, FACTO_POTRF>) < 0 || raise_smem(subpanel_trsm_kernel<float, FACTO_SYTRF>) < 0)
         return -1;
     if ((v = raise_smem(update_f64_kernel)) < UPD_F64_SMEM) return -1;
+    if (raise_smem(diag_small_kernel<double, FACTO_POTRF>) < 0 || raise_smem(diag_small_kernel<double, FACTO_SYTRF>) < 0 ||
+        raise_smem(diag_small_kernel<double, FACTO_GETRF>) < 0 || raise_smem(diag_small_kernel<float, FACTO_POTRF>) < 0 ||
+        raise_smem(diag_small_kernel<float, FACTO_SYTRF>) < 0 || raise_smem(diag_small_kernel<float, FACTO_GETRF>) < 0)
+        return -1;
     if ((v = raise_smem(panel_trsm_kernel<double>)) < 0) return -1;
     lim = std::min(lim, v);
     if ((v = raise_smem(panel_trsm_kernel<float>)) < 0) return -1;

@@ -15,6 +15,11 @@ void launch_scatter(int64_t nnz, const int64_t *dest, const double *Lv, const do
 template <typename T>
 void launch_diag(int facto, const DevSym &s, const int *cblks, int ncblk, T *L, T *U, T *tinv,
                  const int64_t *tinv_off, const double *thr, unsigned long long *npiv, int *err, cudaStream_t st);
+// the same for cblks of at most 32 columns, one warp per cblk
+template <typename T>
+void launch_diag_small(int facto, const DevSym &s, const int *cblks, int ncblk, T *L, T *U, T *tinv,
+                       const int64_t *tinv_off, const double *thr, unsigned long long *npiv, int *err,
+                       cudaStream_t st);
 // X op(T) = B: mode 0 upper / 1 lower-transposed for the left-looking part; which = 0 (inv L) or 1 (inv U^T)
 // selects the tile inverse; scale_d divides by D (LDL^T)
 template <typename T>

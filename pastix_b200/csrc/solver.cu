@@ -101,6 +101,7 @@ struct b200_solver_s {
     int *d_inv_small = nullptr, *d_inv_big = nullptr;  // cblks of <= 32 / > 32 columns
     int n_inv_small = 0, n_inv_big = 0;
     std::vector<int> lvl_ds0, lvl_ds1;
+    std::vector<int> lvl_dsm0, lvl_dsm1;  // cblks of <= 32 columns (one warp each)
     // sub-panel steps of wide POTRF / LDL^T cblks
     struct SubStep {
         int d0, d1;   // subpanel diagonal tasks
@@ -253,6 +254,8 @@ int build_schedule(b200_solver_t *s) {
     };
     s->lvl_ds0.assign(nlev, 0);
     s->lvl_ds1.assign(nlev, 0);
+    s->lvl_dsm0.assign(nlev, 0);
+    s->lvl_dsm1.assign(nlev, 0);
     s->lvl_steps.assign(nlev, {});
     const int split_min = 96;  // wider POTRF / LDL^T cblks take the sub-panel path
     auto is_big = [&](int k) { return s->facto != FACTO_GETRF && s->ncols[k] > split_min; };
@@ -291,10 +294,16 @@ int build_schedule(b200_solver_t *s) {
         s->lvl_st0[l] = (int)stile.size();
         s->lvl_dt0[l] = (int)dtask.size();
         s->lvl_db0[l] = (int)dtaskb.size();
+        // diagonal blocks: <= 32 columns by the one-warp kernel, up to the sub-panel
+        // width by the one-CTA kernel
         s->lvl_ds0[l] = (int)diag_list.size();
         for (int i = L.c0; i < L.c1; i++)
-            if (!is_big(lvl_cblk[i])) diag_list.push_back(lvl_cblk[i]);
+            if (!is_big(lvl_cblk[i]) && s->ncols[lvl_cblk[i]] > 32) diag_list.push_back(lvl_cblk[i]);
         s->lvl_ds1[l] = (int)diag_list.size();
+        s->lvl_dsm0[l] = (int)diag_list.size();
+        for (int i = L.c0; i < L.c1; i++)
+            if (s->ncols[lvl_cblk[i]] <= 32) diag_list.push_back(lvl_cblk[i]);
+        s->lvl_dsm1[l] = (int)diag_list.size();
         {
             // sub-panel steps: 64 columns each, for every wide cblk of the level
             int nsteps = 0;
@@ -631,6 +640,9 @@ int enqueue_numfact(b200_solver_t *s, cudaStream_t st, Trace *tr = nullptr) {
         if (tr) tr->begin(st);
         launch_diag<T>(s->facto, s->ds, s->d_diag_list + s->lvl_ds0[l], s->lvl_ds1[l] - s->lvl_ds0[l], L, U,
                        (T *)s->dTinv, s->d_toff, s->d_thr, s->d_npiv, s->d_err, st);
+        launch_diag_small<T>(s->facto, s->ds, s->d_diag_list + s->lvl_dsm0[l], s->lvl_dsm1[l] - s->lvl_dsm0[l], L, U,
+                             (T *)s->dTinv, s->d_toff, s->d_thr, s->d_npiv, s->d_err, st);
+        launches += (s->lvl_dsm1[l] > s->lvl_dsm0[l]);
         if (tr) tr->end(1, st);
         launches++;
         const int nt = Lv.t1 - Lv.t0;
