@@ -1083,6 +1083,65 @@ __global__ void __launch_bounds__(32 * DS_WARPS) diag_small_kernel(DevSym s, con
     }
 }
 
+// Small GEMM-scatter updates (K <= 16, N <= 32: the bottom levels of the tree,
+// far below a 64 x 64 tile), one warp each: lane = row of the M-range (32 rows per
+// pass), C[d(i)][colbase + c] -= sum_k A[i][k] (D[k]) B[c][k] for c < N (c <= i when
+// symmetric).  Same operation as the tile kernels (core_zgemmsp_2d2d,
+// kernels/core_zgemmsp.c:396-465).
+constexpr int US_WARPS = 8;
+
+template <typename T>
+__global__ void __launch_bounds__(32 * US_WARPS) update_small_kernel(DevSym s, const Upd *__restrict__ upds, int nupd,
+                                                                     T *L, T *U) {
+    const int lane = threadIdx.x & 31;
+    const int ui = blockIdx.x * US_WARPS + (threadIdx.x >> 5);
+    if (ui >= nupd) return;
+    const Upd u = upds[ui];
+    const int k = u.k, ldk = s.ld[k];
+    const T *Ap = ((u.flags & UPD_A_U) ? U : L) + s.off[k] + u.rowA0 + (size_t)u.colK0 * ldk;
+    const T *Bp = ((u.flags & UPD_B_U) ? U : L) + s.off[k] + u.rowB0 + (size_t)u.colK0 * ldk;
+    const T *Dp = L + s.off[k] + (size_t)u.colK0 * (ldk + 1);
+    const bool scale = (u.flags & UPD_SCALE_D) != 0;
+    const bool atomic = (u.flags & UPD_ATOMIC) != 0;
+    const bool sym = (u.flags & UPD_SYM) != 0;
+    T *C = ((u.flags & UPD_C_U) ? U : L) + s.off[u.f];
+    const int ldf = s.ld[u.f];
+    // B (N x K, N <= 32) and D in registers of the lanes, broadcast by shuffles
+    T bk[16];
+#pragma unroll
+    for (int q = 0; q < 16; q++) bk[q] = (lane < u.N && q < u.K) ? Bp[lane + (size_t)q * ldk] : (T)0;
+    T dk = (scale && lane < u.K) ? Dp[(size_t)lane * (ldk + 1)] : (T)1;
+    for (int r0 = 0; r0 < u.M; r0 += 32) {
+        const int i = r0 + lane;
+        const bool in = i < u.M;
+        T a[16];
+#pragma unroll
+        for (int q = 0; q < 16; q++) {
+            const T dq = __shfl_sync(0xffffffffu, dk, q);
+            a[q] = (in && q < u.K) ? Ap[i + (size_t)q * ldk] * dq : (T)0;
+        }
+        const int d = in ? dest_row(s, k, u.f, u.rowA0 + i) : -1;
+        T *crow = C + d + (size_t)u.colbase * ldf;
+        for (int c = 0; c < u.N; c++) {
+            T acc = 0;
+#pragma unroll
+            for (int q = 0; q < 16; q++) acc += a[q] * __shfl_sync(0xffffffffu, bk[q], c);
+            if (d >= 0 && !(sym && i < c)) {
+                if (atomic) atomicAdd(crow + (size_t)c * ldf, -acc);
+                else crow[(size_t)c * ldf] -= acc;
+            }
+        }
+    }
+}
+
+template <typename T>
+void launch_update_small(const DevSym &s, const Upd *upds, int nupd, T *L, T *U, cudaStream_t st) {
+    if (nupd <= 0) return;
+    update_small_kernel<T><<<(nupd + US_WARPS - 1) / US_WARPS, 32 * US_WARPS, 0, st>>>(s, upds, nupd, L, U);
+}
+template void launch_update_small<double>(const DevSym &, const Upd *, int, double *, double *, cudaStream_t);
+template void launch_update_small<float>(const DevSym &, const Upd *, int, float *, float *, cudaStream_t);
+
 template <typename T>
 void launch_diag_small(int facto, const DevSym &s, const int *cblks, int ncblk, T *L, T *U, T *tinv,
                        const int64_t *tinv_off, const double *thr, unsigned long long *npiv, int *err,

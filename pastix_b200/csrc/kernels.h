@@ -32,6 +32,9 @@ void launch_subpanel_diag(int facto, const DevSym &s, const SubTask *tasks, int 
 template <typename T>
 void launch_subpanel_trsm(int facto, const DevSym &s, const SubTask *tasks, int ntasks, T *L, const T *winv,
                           cudaStream_t st);
+// updates with K <= 16 and N <= 32, one warp each
+template <typename T>
+void launch_update_small(const DevSym &s, const Upd *upds, int nupd, T *L, T *U, cudaStream_t st);
 void launch_update_f64(const DevSym &s, const Upd *upds, int nupd, int ntiles, double *L, double *U,
                        cudaStream_t st);
 void launch_update_f32(const DevSym &s, const Upd *upds, int nupd, int ntiles, float *L, float *U,

@@ -125,6 +125,8 @@ struct b200_solver_s {
     Upd *d_tcupd = nullptr;
     std::vector<int> lvl_tc_u0, lvl_tc_u1, lvl_tc_tiles, lvl_tc_m0;
     int2 *d_tcmap = nullptr;              // tiles of each tensor-core launch: {update, row | col << 16}
+    Upd *d_smallupd = nullptr;            // updates with K <= 16, N <= 32 (one warp each)
+    std::vector<int> lvl_us0, lvl_us1;
     std::vector<char> tc_wanted;          // cblks whose panels the tensor-core updates read
     std::vector<int64_t> toff;            // operand copy of cblk k: row-major, pitch ncols rounded up to 4
     int64_t tsize = 0;                    // floats of one operand arena
@@ -216,6 +218,9 @@ int build_schedule(b200_solver_t *s) {
     std::vector<Upd> subupds;
     std::vector<Upd> tcupds;
     std::vector<int2> tcmap;
+    std::vector<Upd> smallupds;
+    s->lvl_us0.assign(nlev, 0);
+    s->lvl_us1.assign(nlev, 0);
     std::vector<SplitTask> splits;
     std::vector<char> ext_wanted(N, 0);   // cblks with external tensor-core updates
     s->lvl_sp0.assign(nlev, 0);
@@ -410,6 +415,7 @@ int build_schedule(b200_solver_t *s) {
             }
         }
         L.u0 = (int)upds.size();
+        s->lvl_us0[l] = (int)smallupds.size();
         s->lvl_tc_u0[l] = (int)tcupds.size();
         s->lvl_tc_m0[l] = (int)tcmap.size();
         int tile0 = 0, tc_tile0 = 0;
@@ -456,6 +462,11 @@ int build_schedule(b200_solver_t *s) {
                         ext_wanted[k] = 1;
                         continue;
                     }
+                    if (u.K <= 16 && u.N <= 32) {
+                        s->flops_kind[3] += upd_flops(u);
+                        smallupds.push_back(u);
+                        continue;
+                    }
                     u.tiles_m = (u.M + 63) / 64;
                     u.tiles_n = (u.N + 63) / 64;
                     const int nt = (u.flags & UPD_SYM) ? u.tiles_n * u.tiles_m - u.tiles_n * (u.tiles_n - 1) / 2
@@ -469,6 +480,7 @@ int build_schedule(b200_solver_t *s) {
         }
         L.u1 = (int)upds.size();
         L.ntiles = tile0;
+        s->lvl_us1[l] = (int)smallupds.size();
         s->lvl_tc_u1[l] = (int)tcupds.size();
         s->lvl_tc_tiles[l] = tc_tile0;
         // operand copies of the off-diagonal rows of the level's panels read by them
@@ -532,6 +544,7 @@ int build_schedule(b200_solver_t *s) {
     RET(s->dupload(&s->d_upd, upds));
     RET(s->dupload(&s->d_tcupd, tcupds));
     RET(s->dupload(&s->d_tcmap, tcmap));
+    RET(s->dupload(&s->d_smallupd, smallupds));
     RET(s->dupload(&s->d_split, splits));
     s->toff.assign(N, 0);
     int64_t tp = 0;
@@ -698,6 +711,10 @@ int enqueue_numfact(b200_solver_t *s, cudaStream_t st, Trace *tr = nullptr) {
             }
         }
         if (tr) tr->begin(st);
+        if (s->lvl_us1[l] > s->lvl_us0[l]) {
+            launch_update_small<T>(s->ds, s->d_smallupd + s->lvl_us0[l], s->lvl_us1[l] - s->lvl_us0[l], L, U, st);
+            launches++;
+        }
         if (Lv.ntiles > 0) {
             if (sizeof(T) == 8)
                 launch_update_f64(s->ds, s->d_upd + Lv.u0, Lv.u1 - Lv.u0, Lv.ntiles, (double *)L, (double *)U, st);
