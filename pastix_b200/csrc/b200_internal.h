@@ -82,6 +82,7 @@ struct SubTask {
     int row0;
     int c0;
     int pos;
+    int split;  // TRSM task: also write the rows row-major (hi / lo) for the tensor-core update
 };
 
 // 32 x 32 tile of a panel copied to the row-major operand arena of the tensor-core

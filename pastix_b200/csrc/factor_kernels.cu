@@ -727,10 +727,14 @@ __global__ void __launch_bounds__(256) subpanel_diag_kernel(DevSym s, const SubT
 }
 
 // X = A W^T (POTRF) or A W^T D^{-1} (LDL^T) for 64 rows of the panel below the
-// sub-panel's diagonal tile, in place.
+// sub-panel's diagonal tile, in place.  Tasks with `split` also write the rows into
+// the row-major operand arena of the tensor-core updates (hi = x with 13 low mantissa
+// bits cleared, lo = x - hi when lo is given), which panel_split_kernel would
+// otherwise copy in a launch of its own.
 template <typename T, int FACTO>
 __global__ void __launch_bounds__(256) subpanel_trsm_kernel(DevSym s, const SubTask *__restrict__ tasks, T *L,
-                                                            const T *__restrict__ winv) {
+                                                            const T *__restrict__ winv,
+                                                            const int64_t *__restrict__ toff, float *hi, float *lo) {
     extern __shared__ __align__(16) unsigned char sp_smem[];
     T *xa = reinterpret_cast<T *>(sp_smem);
     T *wt = xa + SP * SPP;
@@ -760,11 +764,31 @@ __global__ void __launch_bounds__(256) subpanel_trsm_kernel(DevSym s, const SubT
 #pragma unroll
         for (int q = 0; q < 16; q++) acc[q] += x * wt[(cg * 16 + q) + l * SPP];  // W[c][l]
     }
+#pragma unroll
+    for (int q = 0; q < 16; q++) acc[q] *= dinv[cg * 16 + q];
     if (r < rows) {
 #pragma unroll
         for (int q = 0; q < 16; q++) {
             const int c = cg * 16 + q;
-            if (c < wd) X[r + (size_t)c * ld] = acc[q] * dinv[c];
+            if (c < wd) X[r + (size_t)c * ld] = acc[q];
+        }
+    }
+    if (tk.split && hi) {
+        // row-major copy through shared memory: consecutive threads, consecutive columns
+        __syncthreads();
+#pragma unroll
+        for (int q = 0; q < 16; q++) xa[r + (cg * 16 + q) * SPP] = acc[q];
+        __syncthreads();
+        const int kp = (s.ncols[k] + 3) & ~3;
+        for (int idx = tid; idx < rows * SP; idx += nth) {
+            const int rr = idx >> 6, c = idx & 63;
+            if (c < wd) {
+                const float x = (float)xa[rr + c * SPP];
+                const float h = lo ? __uint_as_float(__float_as_uint(x) & 0xFFFFE000u) : x;
+                const size_t o = toff[k] + (size_t)(tk.row0 + rr) * kp + c0 + c;
+                hi[o] = h;
+                if (lo) lo[o] = x - h;
+            }
         }
     }
 }
@@ -781,11 +805,13 @@ void launch_subpanel_diag(int facto, const DevSym &s, const SubTask *tasks, int 
 
 template <typename T>
 void launch_subpanel_trsm(int facto, const DevSym &s, const SubTask *tasks, int ntasks, T *L, const T *winv,
-                          cudaStream_t st) {
+                          const int64_t *toff, float *hi, float *lo, cudaStream_t st) {
     if (ntasks <= 0) return;
     const size_t smem = 2 * SP * SPP * sizeof(T);
-    if (facto == FACTO_POTRF) subpanel_trsm_kernel<T, FACTO_POTRF><<<ntasks, 256, smem, st>>>(s, tasks, L, winv);
-    else subpanel_trsm_kernel<T, FACTO_SYTRF><<<ntasks, 256, smem, st>>>(s, tasks, L, winv);
+    if (facto == FACTO_POTRF)
+        subpanel_trsm_kernel<T, FACTO_POTRF><<<ntasks, 256, smem, st>>>(s, tasks, L, winv, toff, hi, lo);
+    else
+        subpanel_trsm_kernel<T, FACTO_SYTRF><<<ntasks, 256, smem, st>>>(s, tasks, L, winv, toff, hi, lo);
 }
 
 template void launch_subpanel_diag<double>(int, const DevSym &, const SubTask *, int, double *, double *,
@@ -793,9 +819,9 @@ template void launch_subpanel_diag<double>(int, const DevSym &, const SubTask *,
 template void launch_subpanel_diag<float>(int, const DevSym &, const SubTask *, int, float *, float *, const double *,
                                           unsigned long long *, int *, cudaStream_t);
 template void launch_subpanel_trsm<double>(int, const DevSym &, const SubTask *, int, double *, const double *,
-                                           cudaStream_t);
+                                           const int64_t *, float *, float *, cudaStream_t);
 template void launch_subpanel_trsm<float>(int, const DevSym &, const SubTask *, int, float *, const float *,
-                                          cudaStream_t);
+                                          const int64_t *, float *, float *, cudaStream_t);
 
 // ------------------------------------------------------------------ updates
 

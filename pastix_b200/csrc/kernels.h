@@ -29,9 +29,10 @@ void launch_trsm(const DevSym &s, const RowTask *tasks, int ntasks, int TR, int 
 template <typename T>
 void launch_subpanel_diag(int facto, const DevSym &s, const SubTask *tasks, int ntasks, T *L, T *winv,
                           const double *thr, unsigned long long *npiv, int *err, cudaStream_t st);
+// (tasks with split also write their rows into the tensor-core operand arenas hi / lo)
 template <typename T>
 void launch_subpanel_trsm(int facto, const DevSym &s, const SubTask *tasks, int ntasks, T *L, const T *winv,
-                          cudaStream_t st);
+                          const int64_t *toff, float *hi, float *lo, cudaStream_t st);
 // updates with K <= 16 and N <= 32, one warp each
 template <typename T>
 void launch_update_small(const DevSym &s, const Upd *upds, int nupd, T *L, T *U, cudaStream_t st);

@@ -324,25 +324,14 @@ int build_schedule(b200_solver_t *s) {
                     const int k = lvl_cblk[i];
                     if (!is_big(k) || c0 >= s->ncols[k]) continue;
                     members.push_back({k, pos});
-                    subtasks.push_back({k, c0, c0, pos});
+                    subtasks.push_back({k, c0, c0, pos, 0});
                     pos++;
                 }
                 ss.d1 = (int)subtasks.size();
                 s->subwinv_slots = std::max<int64_t>(s->subwinv_slots, pos);
-                ss.t0 = (int)subtasks.size();
-                for (auto &m : members) {
-                    const int wd = std::min(64, s->ncols[m.first] - c0);  // rows below the sub-panel's tile
-                    for (int r0 = c0 + wd; r0 < s->stride[m.first]; r0 += 64) subtasks.push_back({m.first, r0, c0, m.second});
-                }
-                ss.t1 = (int)subtasks.size();
-                ss.u0 = (int)subupds.size();
-                ss.tu0 = (int)tcupds.size();
-                ss.tm0 = (int)tcmap.size();
-                ss.sp0 = (int)splits.size();
-                int t0 = 0, tt0 = 0;
-                for (auto &m : members) {
-                    const int k = m.first, n = s->ncols[k];
-                    if (c0 + 64 >= n) continue;
+                // internal update of a member: the columns right of the sub-panel
+                auto internal = [&](int k) {
+                    const int n = s->ncols[k];
                     Upd u{};
                     u.k = k;
                     u.j = -1;
@@ -355,10 +344,28 @@ int build_schedule(b200_solver_t *s) {
                     u.K = 64;
                     u.colbase = c0 + 64;
                     u.flags = UPD_SYM | (s->facto == FACTO_SYTRF ? UPD_SCALE_D : 0);
+                    return u;
+                };
+                ss.t0 = (int)subtasks.size();
+                for (auto &m : members) {
+                    const int k = m.first;
+                    const int wd = std::min(64, s->ncols[k] - c0);  // rows below the sub-panel's tile
+                    // the TRSM also writes the tensor-core operand copies of its rows
+                    const int split = (c0 + 64 < s->ncols[k] && tc_ok(internal(k))) ? 1 : 0;
+                    for (int r0 = c0 + wd; r0 < s->stride[k]; r0 += 64) subtasks.push_back({k, r0, c0, m.second, split});
+                }
+                ss.t1 = (int)subtasks.size();
+                ss.u0 = (int)subupds.size();
+                ss.tu0 = (int)tcupds.size();
+                ss.tm0 = (int)tcmap.size();
+                ss.sp0 = (int)splits.size();
+                int t0 = 0, tt0 = 0;
+                for (auto &m : members) {
+                    const int k = m.first, n = s->ncols[k];
+                    if (c0 + 64 >= n) continue;
+                    Upd u = internal(k);
                     if (tc_ok(u)) {
-                        push_tc(u, tt0, ss.tu0);
-                        for (int r0 = c0 + 64; r0 < s->stride[k]; r0 += 32)
-                            for (int cc = c0; cc < c0 + 64; cc += 32) splits.push_back({k, r0, cc});
+                        push_tc(u, tt0, ss.tu0);  // operands copied by the step's TRSM
                         continue;
                     }
                     s->flops_kind[6] += upd_flops(u);
@@ -684,8 +691,13 @@ int enqueue_numfact(b200_solver_t *s, cudaStream_t st, Trace *tr = nullptr) {
             if (tr) tr->end(4, st);
             if (ss.t1 > ss.t0) {
                 if (tr) tr->begin(st);
+                float *hi = nullptr, *lo = nullptr;
+                if (s->use_tc) {
+                    hi = (float *)s->d_tarena;
+                    lo = s->prec == B200_PREC_TF32X3 ? hi + s->tsize : nullptr;
+                }
                 launch_subpanel_trsm<T>(s->facto, s->ds, s->d_subtask + ss.t0, ss.t1 - ss.t0, L,
-                                        (const T *)s->d_subwinv, st);
+                                        (const T *)s->d_subwinv, s->d_toffT, hi, lo, st);
                 launches++;
                 if (tr) tr->end(5, st);
             }
@@ -699,10 +711,12 @@ int enqueue_numfact(b200_solver_t *s, cudaStream_t st, Trace *tr = nullptr) {
                 if (tr) tr->end(6, st);
             }
             if (ss.tntiles > 0) {
-                if (tr) tr->begin(st);
-                enqueue_split(s, ss.sp0, ss.sp1, st);
-                launches += 1 + (s->facto == FACTO_GETRF);
-                if (tr) tr->end(9, st);
+                if (ss.sp1 > ss.sp0) {
+                    if (tr) tr->begin(st);
+                    enqueue_split(s, ss.sp0, ss.sp1, st);
+                    launches += 1 + (s->facto == FACTO_GETRF);
+                    if (tr) tr->end(9, st);
+                }
                 if (tr) tr->begin(st);
                 launch_update_tc(s->ds, s->d_tcupd + ss.tu0, s->d_tcmap + ss.tm0, ss.tntiles, s->d_maps, (float *)L,
                                  (float *)U, s->prec == B200_PREC_TF32X3, s->d_err, st);
