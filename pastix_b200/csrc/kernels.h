@@ -42,12 +42,12 @@ void launch_update_f32(const DevSym &s, const Upd *upds, int nupd, int ntiles, f
                        cudaStream_t st);
 // returns the dynamic shared memory (bytes) the panel TRSM may use, or -1
 int configure_factor_kernels();
-// FP32 updates on the tensor cores (update_tc.cu).  Tiles of 128 rows x 64
+// FP32 updates on the tensor cores (update_tc.cu).  Tiles of 128 rows x bn (64 or 128)
 // columns listed by tmap ({update index, row tile | column tile << 16}); maps: 4 x cblknbr
 // tensor maps of the operand arenas, [(side * 2 + part) * cblknbr + k] with side
 // 0 L / 1 U and part 0 hi / 1 lo; split: 3xTF32.
 void launch_update_tc(const DevSym &s, const Upd *upds, const int2 *tmap, int ntiles, const void *maps, float *L,
-                      float *U, int split, int *err, cudaStream_t st);
+                      float *U, int split, int bn, int *err, cudaStream_t st);
 int configure_tc_kernels();
 // copy panel tiles row-major into the operand arena (hi, and lo = x - hi when lo is given)
 void launch_panel_split(const DevSym &s, const SplitTask *tasks, int ntasks, const float *P, const int64_t *toff,

@@ -111,7 +111,8 @@ struct b200_solver_s {
         int tu0, tu1;  // internal updates on the tensor cores
         int tntiles;
         int sp0, sp1;  // operand copies for them
-        int tm0;       // their tile map
+        int tm0;       // their tile map (64-column tiles)
+        int tmw0, twtiles;  // and the 128-column tiles
     };
     std::vector<std::vector<SubStep>> lvl_steps;
     SubTask *d_subtask = nullptr;
@@ -123,7 +124,8 @@ struct b200_solver_s {
     bool use_tc = false;
     int tc_min_k = 32, tc_min_m = 64;
     Upd *d_tcupd = nullptr;
-    std::vector<int> lvl_tc_u0, lvl_tc_u1, lvl_tc_tiles, lvl_tc_m0;
+    std::vector<int> lvl_tc_u0, lvl_tc_u1, lvl_tc_tiles, lvl_tc_m0, lvl_tc_wtiles, lvl_tc_mw0;
+    int2 *d_tcmapw = nullptr;             // 128-column tiles
     int2 *d_tcmap = nullptr;              // tiles of each tensor-core launch: {update, row | col << 16}
     Upd *d_smallupd = nullptr;            // updates with K <= 16, N <= 32 (one warp each)
     std::vector<int> lvl_us0, lvl_us1;
@@ -217,7 +219,7 @@ int build_schedule(b200_solver_t *s) {
     std::vector<SubTask> subtasks;
     std::vector<Upd> subupds;
     std::vector<Upd> tcupds;
-    std::vector<int2> tcmap;
+    std::vector<int2> tcmap, tcmapw;  // tile maps of the 64- and 128-column tensor-core launches
     std::vector<Upd> smallupds;
     s->lvl_us0.assign(nlev, 0);
     s->lvl_us1.assign(nlev, 0);
@@ -230,6 +232,8 @@ int build_schedule(b200_solver_t *s) {
     s->lvl_tc_u1.assign(nlev, 0);
     s->lvl_tc_tiles.assign(nlev, 0);
     s->lvl_tc_m0.assign(nlev, 0);
+    s->lvl_tc_mw0.assign(nlev, 0);
+    s->lvl_tc_wtiles.assign(nlev, 0);
     auto tc_ok = [&](const Upd &u) {
         return s->use_tc && !(u.flags & UPD_SCALE_D) && u.K >= s->tc_min_k && u.M >= s->tc_min_m &&
                (u.colK0 == 0 || u.K % 32 == 0);
@@ -242,17 +246,19 @@ int build_schedule(b200_solver_t *s) {
         return 2.0 * mn * u.K;
     };
     // base: first update of the launch the update belongs to (map entries are relative)
-    auto push_tc = [&](Upd u, int &t0, int base) {
+    // updates more than 64 columns wide take 128-column tiles (half the operand
+    // traffic per flop of the 64-column tiles)
+    auto push_tc = [&](Upd u, int &t0, int &t0w, int base) {
         s->flops_kind[8] += upd_flops(u);
+        const int bn = u.N > 64 ? 128 : 64;
         u.tiles_m = (u.M + 127) / 128;
-        u.tiles_n = (u.N + 63) / 64;
-        u.tile0 = t0;
+        u.tiles_n = (u.N + bn - 1) / bn;
         const int ui = (int)tcupds.size() - base;
         for (int nt = 0; nt < u.tiles_n; nt++)
             for (int mt = 0; mt < u.tiles_m; mt++) {
-                if ((u.flags & UPD_SYM) && mt * 128 + 127 < nt * 64) continue;  // above the diagonal
-                tcmap.push_back(make_int2(ui, mt | (nt << 16)));
-                t0++;
+                if ((u.flags & UPD_SYM) && mt * 128 + 127 < nt * bn) continue;  // above the diagonal
+                (bn == 128 ? tcmapw : tcmap).push_back(make_int2(ui, mt | (nt << 16)));
+                (bn == 128 ? t0w : t0)++;
             }
         s->tc_wanted[u.k] = 1;
         tcupds.push_back(u);
@@ -358,14 +364,15 @@ int build_schedule(b200_solver_t *s) {
                 ss.u0 = (int)subupds.size();
                 ss.tu0 = (int)tcupds.size();
                 ss.tm0 = (int)tcmap.size();
+                ss.tmw0 = (int)tcmapw.size();
                 ss.sp0 = (int)splits.size();
-                int t0 = 0, tt0 = 0;
+                int t0 = 0, tt0 = 0, ttw = 0;
                 for (auto &m : members) {
                     const int k = m.first, n = s->ncols[k];
                     if (c0 + 64 >= n) continue;
                     Upd u = internal(k);
                     if (tc_ok(u)) {
-                        push_tc(u, tt0, ss.tu0);  // operands copied by the step's TRSM
+                        push_tc(u, tt0, ttw, ss.tu0);  // operands copied by the step's TRSM
                         continue;
                     }
                     s->flops_kind[6] += upd_flops(u);
@@ -379,6 +386,7 @@ int build_schedule(b200_solver_t *s) {
                 ss.ntiles = t0;
                 ss.tu1 = (int)tcupds.size();
                 ss.tntiles = tt0;
+                ss.twtiles = ttw;
                 ss.sp1 = (int)splits.size();
                 s->lvl_steps[l].push_back(ss);
             }
@@ -425,7 +433,8 @@ int build_schedule(b200_solver_t *s) {
         s->lvl_us0[l] = (int)smallupds.size();
         s->lvl_tc_u0[l] = (int)tcupds.size();
         s->lvl_tc_m0[l] = (int)tcmap.size();
-        int tile0 = 0, tc_tile0 = 0;
+        s->lvl_tc_mw0[l] = (int)tcmapw.size();
+        int tile0 = 0, tc_tile0 = 0, tc_tilew = 0;
         int64_t flops = 0;
         for (int i = L.c0; i < L.c1; i++) {
             const int k = lvl_cblk[i];
@@ -465,7 +474,7 @@ int build_schedule(b200_solver_t *s) {
                     flops += (int64_t)(2.0 * mn * u.K);
                     s->flops_class[3] += 2.0 * mn * u.K;
                     if (tc_ok(u)) {
-                        push_tc(u, tc_tile0, s->lvl_tc_u0[l]);
+                        push_tc(u, tc_tile0, tc_tilew, s->lvl_tc_u0[l]);
                         ext_wanted[k] = 1;
                         continue;
                     }
@@ -490,6 +499,7 @@ int build_schedule(b200_solver_t *s) {
         s->lvl_us1[l] = (int)smallupds.size();
         s->lvl_tc_u1[l] = (int)tcupds.size();
         s->lvl_tc_tiles[l] = tc_tile0;
+        s->lvl_tc_wtiles[l] = tc_tilew;
         // operand copies of the off-diagonal rows of the level's panels read by them
         s->lvl_sp0[l] = (int)splits.size();
         for (int i = L.c0; i < L.c1; i++) {
@@ -551,6 +561,7 @@ int build_schedule(b200_solver_t *s) {
     RET(s->dupload(&s->d_upd, upds));
     RET(s->dupload(&s->d_tcupd, tcupds));
     RET(s->dupload(&s->d_tcmap, tcmap));
+    RET(s->dupload(&s->d_tcmapw, tcmapw));
     RET(s->dupload(&s->d_smallupd, smallupds));
     RET(s->dupload(&s->d_split, splits));
     s->toff.assign(N, 0);
@@ -710,7 +721,7 @@ int enqueue_numfact(b200_solver_t *s, cudaStream_t st, Trace *tr = nullptr) {
                 launches++;
                 if (tr) tr->end(6, st);
             }
-            if (ss.tntiles > 0) {
+            if (ss.tntiles + ss.twtiles > 0) {
                 if (ss.sp1 > ss.sp0) {
                     if (tr) tr->begin(st);
                     enqueue_split(s, ss.sp0, ss.sp1, st);
@@ -718,9 +729,12 @@ int enqueue_numfact(b200_solver_t *s, cudaStream_t st, Trace *tr = nullptr) {
                     if (tr) tr->end(9, st);
                 }
                 if (tr) tr->begin(st);
+                const int split = s->prec == B200_PREC_TF32X3;
                 launch_update_tc(s->ds, s->d_tcupd + ss.tu0, s->d_tcmap + ss.tm0, ss.tntiles, s->d_maps, (float *)L,
-                                 (float *)U, s->prec == B200_PREC_TF32X3, s->d_err, st);
-                launches++;
+                                 (float *)U, split, 64, s->d_err, st);
+                launch_update_tc(s->ds, s->d_tcupd + ss.tu0, s->d_tcmapw + ss.tmw0, ss.twtiles, s->d_maps, (float *)L,
+                                 (float *)U, split, 128, s->d_err, st);
+                launches += (ss.tntiles > 0) + (ss.twtiles > 0);
                 if (tr) tr->end(8, st);
             }
         }
@@ -737,15 +751,18 @@ int enqueue_numfact(b200_solver_t *s, cudaStream_t st, Trace *tr = nullptr) {
             launches++;
         }
         if (tr) tr->end(3, st);
-        if (s->lvl_tc_tiles[l] > 0) {
+        if (s->lvl_tc_tiles[l] + s->lvl_tc_wtiles[l] > 0) {
             if (tr) tr->begin(st);
             enqueue_split(s, s->lvl_sp0[l], s->lvl_sp1[l], st);
             launches += 1 + (s->facto == FACTO_GETRF);
             if (tr) tr->end(9, st);
             if (tr) tr->begin(st);
+            const int split = s->prec == B200_PREC_TF32X3;
             launch_update_tc(s->ds, s->d_tcupd + s->lvl_tc_u0[l], s->d_tcmap + s->lvl_tc_m0[l], s->lvl_tc_tiles[l],
-                             s->d_maps, (float *)L, (float *)U, s->prec == B200_PREC_TF32X3, s->d_err, st);
-            launches++;
+                             s->d_maps, (float *)L, (float *)U, split, 64, s->d_err, st);
+            launch_update_tc(s->ds, s->d_tcupd + s->lvl_tc_u0[l], s->d_tcmapw + s->lvl_tc_mw0[l],
+                             s->lvl_tc_wtiles[l], s->d_maps, (float *)L, (float *)U, split, 128, s->d_err, st);
+            launches += (s->lvl_tc_tiles[l] > 0) + (s->lvl_tc_wtiles[l] > 0);
             if (tr) tr->end(8, st);
         }
     }

@@ -13,18 +13,18 @@
 // bits cleared (exact in TF32) and lo = x - hi (exact); D += hi_A hi_B + hi_A lo_B +
 // lo_A hi_B keeps close to FP32 accuracy.  TF32 keeps x once and D += A B.
 //
-// update_tc_kernel is persistent (one CTA per SM, tiles of 128 rows x 64 columns
-// striding over the launch's tile list) and warp-specialised:
+// update_tc_kernel is persistent (one CTA per SM, tiles of 128 rows x BN = 64 or
+// 128 columns striding over the launch's tile list) and warp-specialised:
 //  * warp 0 (one lane): TMA producer.  One 2D tensor map per panel copy (K
 //    innermost, boxes of 32 K x 64 rows, 128-byte swizzle: exactly the canonical
-//    K-major UMMA layout), NST-stage ring of [A hi][B hi]([A lo][B lo]) in shared
+//    K-major UMMA layout), a ring of [A hi][B hi]([A lo][B lo]) stages in shared
 //    memory, K in chunks of 32.
-//  * warp 1 (one lane): allocates 128 TMEM columns (two 128 x 64 FP32
-//    accumulators) and issues tcgen05.mma (M = 128, N = 64, K = 8); each stage is
+//  * warp 1 (one lane): allocates 2 BN TMEM columns (two 128 x BN FP32
+//    accumulators) and issues tcgen05.mma (M = 128, N = BN, K = 8); each stage is
 //    released to the producer and each accumulator to the epilogue by
 //    tcgen05.commit on an mbarrier.
 //  * warps 2-9: epilogue.  Thread = accumulator row (TMEM lane quarter = warp % 4),
-//    two warps per quarter with 32 columns each; tcgen05.ld, release the
+//    two warps per quarter with BN / 2 columns each; tcgen05.ld, release the
 //    accumulator, scatter-add into f with reductions (red.global.add), overlapping
 //    the next tile's MMAs.
 //  * Every mbarrier wait is bounded and also gives up once another role has given
@@ -37,19 +37,24 @@
 
 namespace b200 {
 
-constexpr int TC_BM = 128, TC_BN = 64, TC_BK = 32;
+constexpr int TC_BM = 128, TC_BK = 32;
 constexpr int TC_A_BYTES = TC_BM * TC_BK * 4;  // 16 KB
-constexpr int TC_B_BYTES = TC_BN * TC_BK * 4;  // 8 KB
-constexpr uint32_t TC_TMEM_COLS = 128;          // two accumulators of 64 columns
 constexpr long long TC_WAIT_CYCLES = 1000000000LL;  // about 0.5 s at the maximum SM clock
 constexpr int TC_THREADS = 320;  // producer, MMA, 8 epilogue warps
 constexpr int TC_EPI_WARPS = 8;
 
-template <int SPLIT>
+// BN = tile columns (64 or 128); a stage holds [A hi][B hi]([A lo][B lo]), as many
+// stages as fit in about 192 KB
+template <int SPLIT, int BN>
 struct TcCfg {
-    static constexpr int STAGE = SPLIT ? 2 * (TC_A_BYTES + TC_B_BYTES) : (TC_A_BYTES + TC_B_BYTES);
-    static constexpr int NST = SPLIT ? 4 : 8;
+    static constexpr int B_BYTES = BN * TC_BK * 4;
+    static constexpr int STAGE = SPLIT ? 2 * (TC_A_BYTES + B_BYTES) : (TC_A_BYTES + B_BYTES);
+    static constexpr int NST = (192 * 1024) / STAGE;
     static constexpr int SMEM = NST * STAGE + 1024;  // + alignment slack
+    static constexpr uint32_t TMEM_COLS = 2 * BN;    // two accumulators
+    // instruction descriptor: D F32, A/B TF32, both K-major, M = 128, N = BN
+    static constexpr uint32_t IDESC = (1u << 4) | (2u << 7) | (2u << 10) | ((uint32_t)(BN >> 3) << 17) |
+                                      ((uint32_t)(TC_BM >> 4) << 24);
 };
 
 __device__ __forceinline__ uint32_t smem_addr(const void *p) {
@@ -112,16 +117,13 @@ __device__ __forceinline__ uint64_t umma_desc(uint32_t addr) {
     return d;
 }
 
-// Instruction descriptor: D F32, A/B TF32, both K-major, M = 128, N = 64.
-constexpr uint32_t TC_IDESC = (1u << 4) | (2u << 7) | (2u << 10) | ((uint32_t)(TC_BN >> 3) << 17) |
-                              ((uint32_t)(TC_BM >> 4) << 24);
-
+template <uint32_t IDESC>
 __device__ __forceinline__ void umma_tf32(uint32_t tmem, uint64_t da, uint64_t db, uint32_t accumulate) {
     asm volatile(
         "{\n\t.reg .pred p;\n\t"
         "setp.ne.b32 p, %4, 0;\n\t"
         "tcgen05.mma.cta_group::1.kind::tf32 [%0], %1, %2, %3, {%5, %6, %7, %8}, p;\n\t}\n" ::"r"(tmem),
-        "l"(da), "l"(db), "r"(TC_IDESC), "r"(accumulate), "r"(0), "r"(0), "r"(0), "r"(0)
+        "l"(da), "l"(db), "r"(IDESC), "r"(accumulate), "r"(0), "r"(0), "r"(0), "r"(0)
         : "memory");
 }
 
@@ -205,12 +207,16 @@ void launch_panel_split(const DevSym &s, const SplitTask *tasks, int ntasks, con
 // ---------------------------------------------------------------- GEMM-scatter
 
 // maps[(side * 2 + part) * cblknbr + k]: side 0 L / 1 U, part 0 hi / 1 lo
-template <int SPLIT>
+template <int SPLIT, int BN>
 __global__ void __launch_bounds__(TC_THREADS, 1) update_tc_kernel(DevSym s, const Upd *__restrict__ upds,
                                                                   const int2 *__restrict__ tmap, int ntiles,
                                                                   const CUtensorMap *__restrict__ maps,
                                                                   float *L, float *U, int *err) {
-    using Cfg = TcCfg<SPLIT>;
+    using Cfg = TcCfg<SPLIT, BN>;
+    constexpr int TC_B_BYTES = Cfg::B_BYTES;
+    constexpr int TC_BN = BN;
+    constexpr uint32_t TC_TMEM_COLS = Cfg::TMEM_COLS;
+    constexpr int ECOLS = BN / 2;  // columns per epilogue warp
     constexpr int NST = Cfg::NST;
     extern __shared__ __align__(1024) unsigned char tc_smem_raw[];
     __shared__ __align__(8) uint64_t full_bar[NST];
@@ -280,12 +286,15 @@ __global__ void __launch_bounds__(TC_THREADS, 1) update_tc_kernel(DevSym s, cons
                     const int x = kc * TC_BK + u.colK0;
                     tma_load_2d(base, ma, x, ya, bar);
                     tma_load_2d(base + TC_A_BYTES / 2, ma, x, ya + 64, bar);
-                    tma_load_2d(base + TC_A_BYTES, mb, x, yb, bar);
+#pragma unroll
+                    for (int g = 0; g < BN / 64; g++) tma_load_2d(base + TC_A_BYTES + g * 8192, mb, x, yb + 64 * g, bar);
                     if (SPLIT) {
                         const uint32_t lb = base + TC_A_BYTES + TC_B_BYTES;
                         tma_load_2d(lb, ma + N, x, ya, bar);
                         tma_load_2d(lb + TC_A_BYTES / 2, ma + N, x, ya + 64, bar);
-                        tma_load_2d(lb + TC_A_BYTES, mb + N, x, yb, bar);
+#pragma unroll
+                        for (int g = 0; g < BN / 64; g++)
+                            tma_load_2d(lb + TC_A_BYTES + g * 8192, mb + N, x, yb + 64 * g, bar);
                     }
                 }
             }
@@ -324,10 +333,10 @@ __global__ void __launch_bounds__(TC_THREADS, 1) update_tc_kernel(DevSym s, cons
                     for (int k8 = 0; k8 < TC_BK / 8; k8++) {
                         // K step: 8 values = 32 bytes into each row line
                         const uint64_t dah = umma_desc(a_hi + 32 * k8), dbh = umma_desc(b_hi + 32 * k8);
-                        umma_tf32(acc, dah, dbh, (kc > 0 || k8 > 0) ? 1u : 0u);
+                        umma_tf32<Cfg::IDESC>(acc, dah, dbh, (kc > 0 || k8 > 0) ? 1u : 0u);
                         if (SPLIT) {
-                            umma_tf32(acc, dah, umma_desc(b_lo + 32 * k8), 1u);
-                            umma_tf32(acc, umma_desc(a_lo + 32 * k8), dbh, 1u);
+                            umma_tf32<Cfg::IDESC>(acc, dah, umma_desc(b_lo + 32 * k8), 1u);
+                            umma_tf32<Cfg::IDESC>(acc, umma_desc(a_lo + 32 * k8), dbh, 1u);
                         }
                     }
                     umma_commit(smem_addr(&empty_bar[st]));
@@ -344,7 +353,7 @@ __global__ void __launch_bounds__(TC_THREADS, 1) update_tc_kernel(DevSym s, cons
     } else {
         // ------------------------------------------------ epilogue (warps 2-9)
         const int q = warp & 3;                 // TMEM lane quarter this warp may access
-        const int c0 = ((warp - 2) >> 2) * 32;  // its half of the 64 columns
+        const int c0 = ((warp - 2) >> 2) * ECOLS;  // its half of the BN columns
         const int row = q * 32 + lane;
         int tl = 0;
         for (int t = blockIdx.x; t < ntiles; t += gridDim.x) {
@@ -359,10 +368,10 @@ __global__ void __launch_bounds__(TC_THREADS, 1) update_tc_kernel(DevSym s, cons
                 break;
             }
             asm volatile("tcgen05.fence::after_thread_sync;\n" ::: "memory");
-            uint32_t v[32];
+            uint32_t v[ECOLS];
             const uint32_t taddr = tmem + ((uint32_t)(q * 32) << 16) + (uint32_t)(a * TC_BN + c0);
 #pragma unroll
-            for (int cb = 0; cb < 32; cb += 16) {
+            for (int cb = 0; cb < ECOLS; cb += 16) {
                 asm volatile(
                     "tcgen05.ld.sync.aligned.32x32b.x16.b32 {%0,%1,%2,%3,%4,%5,%6,%7,%8,%9,%10,%11,%12,%13,%14,%15}, "
                     "[%16];\n"
@@ -384,11 +393,11 @@ __global__ void __launch_bounds__(TC_THREADS, 1) update_tc_kernel(DevSym s, cons
                 float *C = ((u.flags & UPD_C_U) ? U : L) + s.off[u.f];
                 const size_t ldf = (size_t)s.ld[u.f];
                 const int cmax = min(TC_BN, u.N - tt.nt * TC_BN) - c0;
-                const int csym = (u.flags & UPD_SYM) ? lr - tt.nt * TC_BN - c0 : 31;  // last column kept
+                const int csym = (u.flags & UPD_SYM) ? lr - tt.nt * TC_BN - c0 : ECOLS - 1;  // last column kept
                 const int cend = min(cmax, csym + 1);
                 float *p = C + d + (size_t)(u.colbase + tt.nt * TC_BN + c0) * ldf;
 #pragma unroll
-                for (int c = 0; c < 32; c++)
+                for (int c = 0; c < ECOLS; c++)
                     if (c < cend) atomicAdd(p + (size_t)c * ldf, -__uint_as_float(v[c]));
             }
             tl++;
@@ -406,22 +415,34 @@ __global__ void __launch_bounds__(TC_THREADS, 1) update_tc_kernel(DevSym s, cons
 static int g_num_sms = 0;
 
 void launch_update_tc(const DevSym &s, const Upd *upds, const int2 *tmap, int ntiles, const void *maps, float *L,
-                      float *U, int split, int *err, cudaStream_t st) {
+                      float *U, int split, int bn, int *err, cudaStream_t st) {
     if (ntiles <= 0) return;
     const CUtensorMap *m = static_cast<const CUtensorMap *>(maps);
     const int grid = ntiles < g_num_sms ? ntiles : g_num_sms;
-    if (split)
-        update_tc_kernel<1><<<grid, TC_THREADS, TcCfg<1>::SMEM, st>>>(s, upds, tmap, ntiles, m, L, U, err);
-    else
-        update_tc_kernel<0><<<grid, TC_THREADS, TcCfg<0>::SMEM, st>>>(s, upds, tmap, ntiles, m, L, U, err);
+    if (bn == 128) {
+        if (split)
+            update_tc_kernel<1, 128><<<grid, TC_THREADS, TcCfg<1, 128>::SMEM, st>>>(s, upds, tmap, ntiles, m, L, U, err);
+        else
+            update_tc_kernel<0, 128><<<grid, TC_THREADS, TcCfg<0, 128>::SMEM, st>>>(s, upds, tmap, ntiles, m, L, U, err);
+    } else {
+        if (split)
+            update_tc_kernel<1, 64><<<grid, TC_THREADS, TcCfg<1, 64>::SMEM, st>>>(s, upds, tmap, ntiles, m, L, U, err);
+        else
+            update_tc_kernel<0, 64><<<grid, TC_THREADS, TcCfg<0, 64>::SMEM, st>>>(s, upds, tmap, ntiles, m, L, U, err);
+    }
+}
+
+template <int SPLIT, int BN>
+static int tc_set_smem() {
+    return (int)cudaFuncSetAttribute(update_tc_kernel<SPLIT, BN>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                     TcCfg<SPLIT, BN>::SMEM);
 }
 
 int configure_tc_kernels() {
     int dev = 0, rc = 0;
     rc |= (int)cudaGetDevice(&dev);
     rc |= (int)cudaDeviceGetAttribute(&g_num_sms, cudaDevAttrMultiProcessorCount, dev);
-    rc |= (int)cudaFuncSetAttribute(update_tc_kernel<0>, cudaFuncAttributeMaxDynamicSharedMemorySize, TcCfg<0>::SMEM);
-    rc |= (int)cudaFuncSetAttribute(update_tc_kernel<1>, cudaFuncAttributeMaxDynamicSharedMemorySize, TcCfg<1>::SMEM);
+    rc |= tc_set_smem<0, 64>() | tc_set_smem<1, 64>() | tc_set_smem<0, 128>() | tc_set_smem<1, 128>();
     return rc == 0 && g_num_sms > 0 ? 0 : -1;
 }
 
