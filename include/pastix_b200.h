@@ -78,6 +78,15 @@ int b200_bcsc_load( b200_solver_t *solver, int64_t nnz, const int64_t *colptr,
                     const int64_t *rowtab, const double *Lvalues, const double *Uvalues,
                     double anorm );
 
+/* New values on the pattern of the last b200_bcsc_load (same colptr/rowtab, in the
+ * same order), without re-checking or re-deriving the structure: the
+ * refactorization path of PaStiX, where pastix_subtask_bcsc2ctab refills the
+ * coeftab from the bcsc of an spm whose values changed
+ * (sopalin/pastix_task_sopalin.c:196).  Host arrays of nnz doubles; pinned host
+ * memory makes the copy a DMA at full PCIe / C2C speed.  PASTIX_ERR_BADPARAMETER
+ * before a first b200_bcsc_load. */
+int b200_bcsc_values( b200_solver_t *solver, const double *Lvalues, const double *Uvalues, double anorm );
+
 /* Numerical factorization: bcsc -> coeftab scatter (cpucblk_zfillin,
  * kernels/cpucblk_zinit.c:229) and the supernodal factorization
  * (sopalin/sequential_z{potrf,sytrf,getrf}.c).  epsilon_magn_ctrl has the

@@ -1371,6 +1371,17 @@ int b200_solver_destroy(b200_solver_t *s) {
     return ERR_SUCCESS;
 }
 
+int b200_bcsc_values(b200_solver_t *s, const double *Lvalues, const double *Uvalues, double anorm) {
+    if (!s || s->nnz < 0 || !Lvalues) return ERR_BADPARAM;
+    if (s->facto == FACTO_GETRF && (!Uvalues || !s->d_Uv)) return ERR_BADPARAM;
+    CU(cudaMemcpyAsync(s->d_Lv, Lvalues, s->nnz * sizeof(double), cudaMemcpyHostToDevice, s->st));
+    if (Uvalues && s->d_Uv) CU(cudaMemcpyAsync(s->d_Uv, Uvalues, s->nnz * sizeof(double), cudaMemcpyHostToDevice, s->st));
+    CU(cudaStreamSynchronize(s->st));
+    s->anorm = anorm;
+    s->factored = false;
+    return ERR_SUCCESS;
+}
+
 int b200_bcsc_load(b200_solver_t *s, int64_t nnz, const int64_t *colptr, const int64_t *rowtab, const double *Lvalues,
                    const double *Uvalues, double anorm) {
     if (!s || nnz < 0 || !colptr || !rowtab || !Lvalues) return ERR_BADPARAM;

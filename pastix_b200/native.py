@@ -23,7 +23,7 @@ _I64 = C.c_int64
 _lib = None
 
 # exported symbols, in the order of include/pastix_b200.h
-SYMBOLS = ["b200_solver_create", "b200_solver_destroy", "b200_bcsc_load", "b200_numfact", "b200_numfact_trace",
+SYMBOLS = ["b200_solver_create", "b200_solver_destroy", "b200_bcsc_load", "b200_bcsc_values", "b200_numfact", "b200_numfact_trace",
            "b200_solve_trace", "b200_trace_launches", "b200_trace_kinds", "b200_solve",
            "b200_solve_device", "b200_solve_device_noalloc", "b200_refine", "b200_refine_device", "b200_spmv", "b200_factor_download",
            "b200_stats", "b200_strerror"]
@@ -55,6 +55,7 @@ def lib():
         L.b200_solve_trace.argtypes = [_P, _I64, _P, _P]
         L.b200_trace_launches.argtypes = [_P, _P, _P, _I64]
         L.b200_trace_launches.restype = _I64
+        L.b200_bcsc_values.argtypes = [_P, _P, _P, C.c_double]
         L.b200_trace_kinds.argtypes = [_P, _P, _P, C.c_int]
         L.b200_solve_device.argtypes = [_P, _I64, _P, _I64, _P]
         L.b200_solve_device_noalloc.argtypes = [_P, _I64, _P, _I64, _P]
@@ -118,6 +119,12 @@ class Solver:
         check(lib().b200_bcsc_load(self.h, int(colptr[-1]), _p(colptr), _p(rowtab), _p(Lv), _p(Uv), bcsc.anorm),
               "b200_bcsc_load")
 
+    def bcsc_values(self, Lvalues, Uvalues=None, anorm: float = 0.0):
+        """New values on the pattern of the last bcsc_load (refactorization)."""
+        Lv = np.ascontiguousarray(Lvalues, dtype=np.float64)
+        Uv = np.ascontiguousarray(Uvalues, dtype=np.float64) if Uvalues is not None else None
+        check(lib().b200_bcsc_values(self.h, _p(Lv), _p(Uv), anorm), "b200_bcsc_values")
+
     def numfact(self, epsilon_magn_ctrl: float = 0.0) -> int:
         piv = _I64(0)
         check(lib().b200_numfact(self.h, epsilon_magn_ctrl, C.byref(piv)), "b200_numfact")
@@ -158,24 +165,41 @@ class Solver:
         lib().b200_trace_kinds(self.h, _p(ms), _p(fl), 10)
         return {n: dict(ms=float(ms[i]), flops=float(fl[i])) for i, n in enumerate(self.KIND_NAMES)}
 
-    def solve(self, b: np.ndarray) -> np.ndarray:
-        x = np.asfortranarray(np.array(b, dtype=np.float64).reshape(self.n, -1))
+    def solve(self, b: np.ndarray, inplace: bool = False) -> np.ndarray:
+        """x = A^{-1} b.  inplace: b (float64, column-major n x nrhs) is overwritten
+        with x and returned, as pastix_task_solve does; otherwise a copy is solved."""
+        if inplace:
+            x = b if b.ndim == 2 else b.reshape(self.n, 1)
+            if x.dtype != np.float64 or not x.flags.f_contiguous or x.shape[0] != self.n:
+                raise ValueError("inplace solve needs a column-major float64 (n, nrhs) array")
+        else:
+            x = np.array(b, dtype=np.float64, order="F", copy=True).reshape(self.n, -1, order="F")
         check(lib().b200_solve(self.h, x.shape[1], _p(x), self.n), "b200_solve")
-        return x.reshape(np.shape(b))
+        return x.reshape(np.shape(b), order="F")
 
     def solve_device(self, d_ptr: int, nrhs: int, ld: int, stream: int | None = None):
         check(lib().b200_solve_device(self.h, nrhs, _P(d_ptr), ld, _P(stream) if stream else None),
               "b200_solve_device")
 
-    def refine(self, b, x, method="gmres", eps=1e-12, itermax=250, gmres_im=25):
-        b2 = np.asfortranarray(np.array(b, dtype=np.float64).reshape(self.n, -1))
-        x2 = np.asfortranarray(np.array(x, dtype=np.float64).reshape(self.n, -1))
+    def refine(self, b, x, method="gmres", eps=1e-12, itermax=250, gmres_im=25, inplace=False):
+        """Refine x for A x = b (pastix_task_refine).  inplace: x (float64,
+        column-major n x nrhs) is updated and returned; otherwise a copy is refined.
+        b is read only."""
+        b2 = np.asarray(b, dtype=np.float64).reshape(self.n, -1, order="F")
+        if not b2.flags.f_contiguous:
+            b2 = np.asfortranarray(b2)
+        if inplace:
+            x2 = x if x.ndim == 2 else x.reshape(self.n, 1)
+            if x2.dtype != np.float64 or not x2.flags.f_contiguous or x2.shape[0] != self.n:
+                raise ValueError("inplace refine needs a column-major float64 (n, nrhs) array")
+        else:
+            x2 = np.array(x, dtype=np.float64, order="F", copy=True).reshape(self.n, -1, order="F")
         nit = _I64(0)
         berr = np.zeros(b2.shape[1])
         m = REFINE[method] if isinstance(method, str) else int(method)
         check(lib().b200_refine(self.h, b2.shape[1], _p(b2), self.n, _p(x2), self.n, m, eps, itermax, gmres_im,
                                 C.byref(nit), _p(berr)), "b200_refine")
-        return x2.reshape(np.shape(x)), int(nit.value), berr
+        return x2.reshape(np.shape(x), order="F"), int(nit.value), berr
 
     def refine_device(self, d_b: int, d_x: int, nrhs: int, method="gmres", eps=1e-12, itermax=250, gmres_im=25,
                       stream: int | None = None):

@@ -158,6 +158,46 @@ def test_refactorization_same_pattern():
     s.close()
 
 
+def test_values_only_reload_and_inplace_host_calls():
+    """b200_bcsc_values (new values on the loaded pattern) gives the factor of a full
+    b200_bcsc_load of the same values; in-place solve / refine on column-major host
+    arrays agree with the copying calls."""
+    A = M.laplacian(14, 14, 14, 27, 26.0, shift=1e-3)
+    an = Analysis(A, "potrf")
+    st = an.structure()
+    rng = np.random.default_rng(3)
+    vals = A.values.copy()
+    cols = np.repeat(np.arange(A.n), np.diff(A.colptr))
+    diag = A.rowind == cols
+    vals[diag] *= rng.uniform(1.0, 1.2, A.n)[cols[diag]]
+    bc1, bc2 = an.bcsc(), an.bcsc(vals)
+    s = native.Solver(st, "potrf", "fp64")
+    s.bcsc_load(bc1)
+    s.numfact(0.0)
+    s.bcsc_values(bc2.Lvalues, None, bc2.anorm)
+    s.numfact(0.0)
+    Lv, _ = s.factor()
+    t = native.Solver(st, "potrf", "fp64")
+    t.bcsc_load(bc2)
+    t.numfact(0.0)
+    Lf, _ = t.factor()
+    orc = oracle.Oracle(st)
+    mask = orc.factor_mask(an.facto)
+    assert np.linalg.norm((Lv - Lf)[mask]) / np.linalg.norm(Lf[mask]) <= 1e-14
+    A2 = M.CSC(A.n, A.colptr, A.rowind, vals, True, A.grid)
+    xt, b = M.rhs_from_xtrue(A2, 3, seed=4)
+    x_copy = s.solve(b)
+    xb = np.asfortranarray(b.copy())
+    s.solve(xb, inplace=True)
+    assert np.linalg.norm(xb - x_copy) <= 1e-14 * np.linalg.norm(x_copy)
+    xr, _, _ = s.refine(b, x_copy, "cg", 1e-14, 20, 25)
+    s.refine(b, xb, "cg", 1e-14, 20, 25, inplace=True)
+    assert np.linalg.norm(xb - xr) <= 1e-13 * np.linalg.norm(xr)
+    assert backward_error(A2, xb, b).max() <= BERR_FP64
+    s.close()
+    t.close()
+
+
 def test_multi_rhs_columns_match_single_solves():
     """Each column of a multi-RHS solve equals the one-column solve (within tolerance)."""
     A = M.laplacian(16, 16, 16, 27, 26.0, shift=1e-3)
