@@ -580,248 +580,256 @@ __global__ void __launch_bounds__(256) panel_trsm_kernel(DevSym s, const RowTask
 
 constexpr int SP = 64, SPP = 65;
 
-// 64x64 diagonal tile of a sub-panel as a 2x2 block factorization
-// (core_zpotrfsp / core_zsytrfsp, kernels/core_zpotrfsp.c:66-100 and
-// kernels/core_zsytrfsp.c:63-103, in 32-column blocks):
-//   L11 = factor(A11) and W11 = L11^{-1} by one warp (factor_tile / invert_lower_tile),
-//   L21 = A21 L11^{-T} by substitution (LDL^T: V = A21 L11^{-T} = L21 D1, L21 = V D1^{-1}),
-//   A22 -= L21 L21^T (LDL^T: V L21^T), L22 = factor(A22), W22 = L22^{-1},
-//   W21 = -W22 L21 W11,
-// so that W = L^{-1} of the 64x64 tile (unit diagonal for LDL^T) is ready for the
-// sub-panel TRSM.  The serial column recurrences stay inside one warp (two 32-column
-// factorizations and inverses, the substitution); the rest is 32x32x32 products
-// over 256 threads.  L21 and A22 follow the column order of the right-looking
-// factorization, so the factor matches the unblocked one to rounding.
+// 64x64 diagonal tile of a sub-panel (core_zpotrfsp / core_zsytrfsp,
+// kernels/core_zpotrfsp.c:66-100 and kernels/core_zsytrfsp.c:63-103), blocked
+// right-looking with 8-column leaves, in shared memory:
+//   leaf  (one warp, registers): the 8 columns factored column by column over all
+//         rows of the tile (lane = rows b + lane and b + lane + 32), pivots and
+//         leaf-internal updates broadcast by warp shuffles;
+//   update (256 threads): the columns right of the leaf, a_ij -= sum_c l_ic (d_c) l_jc
+//         in column order.
+// Two CTA barriers per leaf instead of three per column; the summation order per
+// entry is the right-looking factorization's, so the result matches it to rounding.
+// LDL^T keeps D on the diagonal and unit L below (no D L^T copy is needed by the
+// sub-panel TRSM, which solves against L and D).
 template <typename T, int FACTO>
 __global__ void __launch_bounds__(256) subpanel_diag_kernel(DevSym s, const SubTask *__restrict__ tasks, T *L,
-                                                            T *winv, const double *__restrict__ thr_ptr,
+                                                            const double *__restrict__ thr_ptr,
                                                             unsigned long long *npiv, int *err) {
-    __shared__ T t11[32 * TP];  // L11, then V (LDL^T) / L21 W11
-    __shared__ T t21[32 * TP];
-    __shared__ T t22[32 * TP];
-    __shared__ T w11[32 * TP];
-    __shared__ T w22[32 * TP];
-    __shared__ T dd[32];
-    __shared__ T rdg[32];  // reciprocals of the diagonal of L11
+    __shared__ T a[SP * SPP];
     __shared__ int s_piv, s_err;
     const SubTask tk = tasks[blockIdx.x];
     const int k = tk.k, c0 = tk.c0, ld = s.ld[k];
     const int wd = min(SP, s.ncols[k] - c0);
-    const int pb1 = min(32, wd), pb2 = wd - pb1;
     const double thr = *thr_ptr;
     T *A = L + s.off[k] + c0 + (size_t)c0 * ld;
-    T *W = winv + (size_t)tk.pos * SP * SP;
     const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
     if (tid == 0) { s_piv = 0; s_err = 0; }
-    for (int idx = tid; idx < 1024; idx += 256) {
-        const int i = idx & 31, j = idx >> 5;
-        t11[i + j * TP] = (i < pb1 && j < pb1 && i >= j) ? A[i + (size_t)j * ld] : (T)0;
-        t21[i + j * TP] = (i < pb2 && j < pb1) ? A[(32 + i) + (size_t)j * ld] : (T)0;
-        t22[i + j * TP] = (i < pb2 && j < pb2 && i >= j) ? A[(32 + i) + (size_t)(32 + j) * ld] : (T)0;
-    }
+    stage_n<SP * SP / 256, T>(
+        [&](int u) {
+            const int idx = tid + 256 * u, i = idx & 63, j = idx >> 6;
+            return (i < wd && j < wd && i >= j) ? A[i + (size_t)j * ld] : (T)0;
+        },
+        [&](int u, T v) {
+            const int idx = tid + 256 * u;
+            a[(idx & 63) + (idx >> 6) * SPP] = v;
+        });
     __syncthreads();
-    if (warp == 0) factor_tile<T, FACTO>(t11, pb1, lane, thr, &s_piv, &s_err);
-    __syncthreads();
-    if (warp == 0) invert_lower_tile<T>(t11, w11, pb1, lane, FACTO != FACTO_POTRF, 0);
-    if (tid < 32) {
-        dd[tid] = (tid < pb1) ? t11[tid * (TP + 1)] : (T)1;
-        rdg[tid] = (T)1 / dd[tid];
-    }
-    __syncthreads();
-    // L11 and W11 are final
-    for (int idx = tid; idx < 1024; idx += 256) {
-        const int i = idx & 31, j = idx >> 5;
-        if (i < pb1 && j < pb1 && i >= j) A[i + (size_t)j * ld] = t11[i + j * TP];
-        W[i + j * SP] = (i < pb1 && j < pb1 && i >= j) ? w11[i + j * TP] : (T)0;
-        W[i + (32 + j) * SP] = 0;
-    }
-    if (pb2 > 0) {
-        T v[4];
-        __syncthreads();
-        // L21 by substitution against L11^T, one row per thread of warp 0, in the
-        // column order of the right-looking factorization:
-        // POTRF  L21[i][c] = (A21[i][c] - sum_{l<c} L21[i][l] L11[c][l]) / L11[c][c]
-        // LDL^T  V[i][c]   =  A21[i][c] - sum_{l<c} V[i][l] L11[c][l],  L21 = V D1^{-1}
-        if (tid < 32) {
-            const int i = tid;
-            T x[32];
+    for (int b = 0; b < wd; b += 8) {
+        const int bw = min(8, wd - b);
+        if (warp == 0) {
+            const int i0 = b + lane, i1 = b + lane + 32;
+            const bool in0 = i0 < wd, in1 = i1 < wd;
+            T r0[8], r1[8];
 #pragma unroll
-            for (int c = 0; c < 32; c++) x[c] = t21[i + c * TP];
+            for (int j = 0; j < 8; j++) {
+                r0[j] = (in0 && j < bw) ? a[i0 + (b + j) * SPP] : (T)0;
+                r1[j] = (in1 && j < bw) ? a[i1 + (b + j) * SPP] : (T)0;
+            }
+            int piv = 0, neg = 0;
 #pragma unroll
-            for (int c = 0; c < 32; c++) {
-                if (c < pb1) {
+            for (int c = 0; c < 8; c++) {
+                if (c < bw) {
+                    T p = __shfl_sync(0xffffffffu, r0[c], c);
+                    const bool rep = fabs((double)p) < thr;
+                    if (rep) p = (FACTO == FACTO_POTRF) ? (T)thr : ((p < (T)0) ? (T)(-thr) : (T)thr);
+                    T d, inv;
+                    if (FACTO == FACTO_POTRF) {
+                        if (p < (T)0) { neg = 1; p = -p; }
+                        d = sqrt(p);
+                        inv = rsqrt(p);
+                    } else {
+                        d = p;
+                        inv = (T)1 / p;
+                    }
+                    piv += rep;
+                    const bool b0 = in0 && i0 > b + c;
+                    if (lane == c) r0[c] = d;
+                    if (b0) r0[c] *= inv;
+                    if (in1) r1[c] *= inv;
+                    const T m0 = (FACTO == FACTO_SYTRF) ? -d * r0[c] : r0[c];
+                    const T m1 = (FACTO == FACTO_SYTRF) ? -d * r1[c] : r1[c];
 #pragma unroll
-                    for (int l = 0; l < c; l++) x[c] -= x[l] * t11[c + l * TP];
-                    if (FACTO == FACTO_POTRF) x[c] *= rdg[c];
+                    for (int j = c + 1; j < 8; j++) {
+                        const T lj = __shfl_sync(0xffffffffu, r0[c], j);
+                        if (j < bw) {
+                            if (b0 && i0 >= b + j) {
+                                if (FACTO == FACTO_SYTRF) r0[j] += m0 * lj;
+                                else r0[j] -= m0 * lj;
+                            }
+                            if (in1) {
+                                if (FACTO == FACTO_SYTRF) r1[j] += m1 * lj;
+                                else r1[j] -= m1 * lj;
+                            }
+                        }
+                    }
                 }
             }
 #pragma unroll
-            for (int c = 0; c < 32; c++) t21[i + c * TP] = x[c];
-        }
-        __syncthreads();
-        if (FACTO == FACTO_SYTRF) {
-            // V to t11 (L11 is stored already), L21 = V D1^{-1} in t21
-#pragma unroll
-            for (int e = 0; e < 4; e++) {
-                const int idx = tid + 256 * e, i = idx & 31, c = idx >> 5;
-                const T x = t21[i + c * TP];
-                t11[i + c * TP] = x;
-                t21[i + c * TP] = (c < pb1) ? x / dd[c] : (T)0;
+            for (int j = 0; j < 8; j++) {
+                if (j < bw) {
+                    if (in0 && i0 >= b + j) a[i0 + (b + j) * SPP] = r0[j];
+                    if (in1) a[i1 + (b + j) * SPP] = r1[j];
+                }
             }
-            __syncthreads();
-        }
-        // A22 -= L21 X^T on the lower triangle, X = L21 (POTRF) or V (LDL^T), one
-        // subtraction per column of L21 in order
-        const T *X = (FACTO == FACTO_SYTRF) ? t11 : t21;
-#pragma unroll
-        for (int e = 0; e < 4; e++) {
-            const int idx = tid + 256 * e, i = idx & 31, j = idx >> 5;
-            if (i >= j) {
-                T acc = t22[i + j * TP];
-                for (int l = 0; l < pb1; l++) acc -= t21[i + l * TP] * X[j + l * TP];
-                t22[i + j * TP] = acc;
+            if (lane == 0) {
+                s_piv += piv;
+                if (neg) s_err = 1;
             }
         }
         __syncthreads();
-        if (warp == 0) factor_tile<T, FACTO>(t22, pb2, lane, thr, &s_piv, &s_err);
-        __syncthreads();
-        if (warp == 0) invert_lower_tile<T>(t22, w22, pb2, lane, FACTO != FACTO_POTRF, 0);
-        // M = L21 W11: M[i][j] = sum_{l >= j} L21[i][l] W11[l][j]
+        // columns right of the leaf
+        const int j0 = b + bw, rem = wd - j0;
+        for (int idx = tid; idx < rem * rem; idx += 256) {
+            const int i = j0 + idx % rem, j = j0 + idx / rem;
+            if (i < j) continue;
+            T acc = a[i + j * SPP];
 #pragma unroll
-        for (int e = 0; e < 4; e++) {
-            const int idx = tid + 256 * e, i = idx & 31, j = idx >> 5;
-            T acc = 0;
-            for (int l = j; l < pb1; l++) acc += t21[i + l * TP] * w11[l + j * TP];
-            v[e] = acc;
+            for (int c = 0; c < 8; c++) {
+                if (c < bw) {
+                    const T lic = a[i + (b + c) * SPP], ljc = a[j + (b + c) * SPP];
+                    if (FACTO == FACTO_SYTRF) acc -= (lic * a[(b + c) * (SPP + 1)]) * ljc;
+                    else acc -= lic * ljc;
+                }
+            }
+            a[i + j * SPP] = acc;
         }
         __syncthreads();
-#pragma unroll
-        for (int e = 0; e < 4; e++) {
-            const int idx = tid + 256 * e, i = idx & 31, j = idx >> 5;
-            t11[i + j * TP] = v[e];
-        }
-        __syncthreads();
-        // W21 = -W22 M: W21[i][j] = -sum_{l <= i} W22[i][l] M[l][j]
-        for (int idx = tid; idx < 1024; idx += 256) {
-            const int i = idx & 31, j = idx >> 5;
-            T acc = 0;
-            for (int l = 0; l <= i; l++) acc += w22[i + l * TP] * t11[l + j * TP];
-            const bool in = i < pb2 && j < pb1;
-            W[(32 + i) + j * SP] = in ? -acc : (T)0;
-            W[(32 + i) + (32 + j) * SP] = (i < pb2 && j < pb2 && i >= j) ? w22[i + j * TP] : (T)0;
-            if (i < pb2 && j < pb1) A[(32 + i) + (size_t)j * ld] = t21[i + j * TP];
-            if (i < pb2 && j < pb2 && i >= j) A[(32 + i) + (size_t)(32 + j) * ld] = t22[i + j * TP];
-        }
-    } else {
-        for (int idx = tid; idx < 1024; idx += 256) {
-            const int i = idx & 31, j = idx >> 5;
-            W[(32 + i) + j * SP] = 0;
-            W[(32 + i) + (32 + j) * SP] = 0;
-        }
     }
-    __syncthreads();
+    for (int idx = tid; idx < SP * SP; idx += 256) {
+        const int i = idx & 63, j = idx >> 6;
+        if (i < wd && j < wd && i >= j) A[i + (size_t)j * ld] = a[i + j * SPP];
+    }
     if (tid == 0) {
         if (s_piv) atomicAdd(npiv, (unsigned long long)s_piv);
         if (s_err) atomicOr(err, 1);
     }
 }
 
-// X = A W^T (POTRF) or A W^T D^{-1} (LDL^T) for 64 rows of the panel below the
-// sub-panel's diagonal tile, in place.  Tasks with `split` also write the rows into
-// the row-major operand arena of the tensor-core updates (hi = x with 13 low mantissa
-// bits cleared, lo = x - hi when lo is given), which panel_split_kernel would
-// otherwise copy in a launch of its own.
+// The rows of the panel below the sub-panel's diagonal tile, 128 rows per CTA
+// (thread = row): POTRF X L^T = A, LDL^T X D L^T = A, by substitution against the
+// factored 64x64 tile in the reference's order (x_c = (a_c - sum_{l<c} x_l L_cl) /
+// L_cc; for LDL^T unit L, then division by D).  Tasks with `split` also write the
+// rows into the row-major operand arena of the tensor-core updates (hi = x with 13
+// low mantissa bits cleared, lo = x - hi when lo is given).
+constexpr int ST_ROWS = 128;
+
 template <typename T, int FACTO>
-__global__ void __launch_bounds__(256) subpanel_trsm_kernel(DevSym s, const SubTask *__restrict__ tasks, T *L,
-                                                            const T *__restrict__ winv,
-                                                            const int64_t *__restrict__ toff, float *hi, float *lo) {
+__global__ void __launch_bounds__(ST_ROWS) subpanel_trsm_kernel(DevSym s, const SubTask *__restrict__ tasks, T *L,
+                                                                const int64_t *__restrict__ toff, float *hi,
+                                                                float *lo) {
     extern __shared__ __align__(16) unsigned char sp_smem[];
-    T *xa = reinterpret_cast<T *>(sp_smem);
-    T *wt = xa + SP * SPP;
-    __shared__ T dinv[SP];
+    T *lt = reinterpret_cast<T *>(sp_smem);  // lt[c + l * SPP] = L[c][l], l <= c (identity past wd)
+    T *xs = lt + SP * SPP;                   // the rows, ST_ROWS x 64 with pitch ST_ROWS + 1
+    __shared__ T rdiag[SP], dinv[SP];
     const SubTask tk = tasks[blockIdx.x];
     const int k = tk.k, c0 = tk.c0, ld = s.ld[k];
     const int wd = min(SP, s.ncols[k] - c0);
-    const int rows = min(SP, s.stride[k] - tk.row0);
+    const int rows = min(ST_ROWS, s.stride[k] - tk.row0);
     T *X = L + s.off[k] + tk.row0 + (size_t)c0 * ld;
-    const T *W = winv + (size_t)tk.pos * SP * SP;
     const T *Dg = L + s.off[k] + c0 + (size_t)c0 * ld;
-    const int tid = threadIdx.x, nth = blockDim.x;
-    for (int idx = tid; idx < SP * SP; idx += nth) {
-        const int i = idx & 63, j = idx >> 6;
-        xa[i + j * SPP] = (i < rows && j < wd) ? X[i + (size_t)j * ld] : (T)0;
-        wt[i + j * SPP] = (i < wd && j < wd) ? W[idx] : (T)0;
+    const int tid = threadIdx.x;
+    stage_n<SP * SP / ST_ROWS, T>(
+        [&](int u) {
+            const int idx = tid + ST_ROWS * u, c = idx & 63, l = idx >> 6;
+            T v = 0;
+            if (c < wd && l < wd) v = (c > l) ? Dg[c + (size_t)l * ld] : (c == l ? (T)1 : (T)0);
+            else if (c == l) v = 1;
+            return v;
+        },
+        [&](int u, T v) {
+            const int idx = tid + ST_ROWS * u;
+            lt[(idx & 63) + (idx >> 6) * SPP] = v;
+        });
+    if (tid < SP) {
+        const T dgv = tid < wd ? Dg[(size_t)tid * (ld + 1)] : (T)1;
+        rdiag[tid] = (FACTO == FACTO_POTRF) ? (T)1 / dgv : (T)1;
+        dinv[tid] = (FACTO == FACTO_SYTRF) ? (T)1 / dgv : (T)1;
     }
-    if (tid < SP) dinv[tid] = (FACTO == FACTO_SYTRF && tid < wd) ? (T)1 / Dg[(size_t)tid * (ld + 1)] : (T)1;
+    // the rows, staged column-major: xs[r + c * (ST_ROWS + 1)]
+#pragma unroll 1
+    for (int c0s = 0; c0s < SP; c0s += 16)
+        stage_n<16, T>([&](int u) { const int c = c0s + u; return (tid < rows && c < wd) ? X[tid + (size_t)c * ld] : (T)0; },
+                       [&](int u, T v) { xs[tid + (c0s + u) * (ST_ROWS + 1)] = v; });
     __syncthreads();
-    // thread: row r = tid & 63, columns cg*16 .. cg*16+15
-    const int r = tid & 63, cg = tid >> 6;
-    T acc[16];
+    const int r = tid;
+    T *xr = xs + r;
+    // 16-column blocks: the block's right-hand sides minus the solved columns to its
+    // left (one x per 16 updates), then substitution inside the block in registers
+#pragma unroll 1
+    for (int cb = 0; cb < SP; cb += 16) {
+        T acc[16];
 #pragma unroll
-    for (int q = 0; q < 16; q++) acc[q] = 0;
-    for (int l = 0; l < wd; l++) {
-        const T x = xa[r + l * SPP];
+        for (int q = 0; q < 16; q++) acc[q] = xr[(cb + q) * (ST_ROWS + 1)];
+        for (int l = 0; l < cb; l++) {
+            const T xl = xr[l * (ST_ROWS + 1)];
+            const T *lc = lt + cb + l * SPP;
 #pragma unroll
-        for (int q = 0; q < 16; q++) acc[q] += x * wt[(cg * 16 + q) + l * SPP];  // W[c][l]
-    }
-#pragma unroll
-    for (int q = 0; q < 16; q++) acc[q] *= dinv[cg * 16 + q];
-    if (r < rows) {
+            for (int q = 0; q < 16; q++) acc[q] -= xl * lc[q];
+        }
 #pragma unroll
         for (int q = 0; q < 16; q++) {
-            const int c = cg * 16 + q;
-            if (c < wd) X[r + (size_t)c * ld] = acc[q];
+#pragma unroll
+            for (int p2 = 0; p2 < q; p2++) acc[q] -= acc[p2] * lt[(cb + q) + (cb + p2) * SPP];
+            acc[q] *= rdiag[cb + q];
         }
+#pragma unroll
+        for (int q = 0; q < 16; q++) xr[(cb + q) * (ST_ROWS + 1)] = acc[q];
+    }
+    if (FACTO == FACTO_SYTRF) {
+        for (int c = 0; c < SP; c++) xr[c * (ST_ROWS + 1)] *= dinv[c];
+    }
+    if (r < rows) {
+        for (int c = 0; c < wd; c++) X[r + (size_t)c * ld] = xr[c * (ST_ROWS + 1)];
     }
     if (tk.split && hi) {
-        // row-major copy through shared memory: consecutive threads, consecutive columns
-        __syncthreads();
-#pragma unroll
-        for (int q = 0; q < 16; q++) xa[r + (cg * 16 + q) * SPP] = acc[q];
+        // row-major copy: consecutive threads, consecutive columns
         __syncthreads();
         const int kp = (s.ncols[k] + 3) & ~3;
-        for (int idx = tid; idx < rows * SP; idx += nth) {
+        for (int idx = tid; idx < rows * SP; idx += ST_ROWS) {
             const int rr = idx >> 6, c = idx & 63;
             if (c < wd) {
-                const float x = (float)xa[rr + c * SPP];
-                const float h = lo ? __uint_as_float(__float_as_uint(x) & 0xFFFFE000u) : x;
+                const float xv = (float)xs[rr + c * (ST_ROWS + 1)];
+                const float h = lo ? __uint_as_float(__float_as_uint(xv) & 0xFFFFE000u) : xv;
                 const size_t o = toff[k] + (size_t)(tk.row0 + rr) * kp + c0 + c;
                 hi[o] = h;
-                if (lo) lo[o] = x - h;
+                if (lo) lo[o] = xv - h;
             }
         }
     }
 }
 
 template <typename T>
-void launch_subpanel_diag(int facto, const DevSym &s, const SubTask *tasks, int ntasks, T *L, T *winv,
-                          const double *thr, unsigned long long *npiv, int *err, cudaStream_t st) {
+void launch_subpanel_diag(int facto, const DevSym &s, const SubTask *tasks, int ntasks, T *L, const double *thr,
+                          unsigned long long *npiv, int *err, cudaStream_t st) {
     if (ntasks <= 0) return;
     if (facto == FACTO_POTRF)
-        subpanel_diag_kernel<T, FACTO_POTRF><<<ntasks, 256, 0, st>>>(s, tasks, L, winv, thr, npiv, err);
+        subpanel_diag_kernel<T, FACTO_POTRF><<<ntasks, 256, 0, st>>>(s, tasks, L, thr, npiv, err);
     else
-        subpanel_diag_kernel<T, FACTO_SYTRF><<<ntasks, 256, 0, st>>>(s, tasks, L, winv, thr, npiv, err);
+        subpanel_diag_kernel<T, FACTO_SYTRF><<<ntasks, 256, 0, st>>>(s, tasks, L, thr, npiv, err);
 }
 
 template <typename T>
-void launch_subpanel_trsm(int facto, const DevSym &s, const SubTask *tasks, int ntasks, T *L, const T *winv,
-                          const int64_t *toff, float *hi, float *lo, cudaStream_t st) {
+void launch_subpanel_trsm(int facto, const DevSym &s, const SubTask *tasks, int ntasks, T *L, const int64_t *toff,
+                          float *hi, float *lo, cudaStream_t st) {
     if (ntasks <= 0) return;
-    const size_t smem = 2 * SP * SPP * sizeof(T);
+    const size_t smem = (SP * SPP + (ST_ROWS + 1) * SP) * sizeof(T);
     if (facto == FACTO_POTRF)
-        subpanel_trsm_kernel<T, FACTO_POTRF><<<ntasks, 256, smem, st>>>(s, tasks, L, winv, toff, hi, lo);
+        subpanel_trsm_kernel<T, FACTO_POTRF><<<ntasks, ST_ROWS, smem, st>>>(s, tasks, L, toff, hi, lo);
     else
-        subpanel_trsm_kernel<T, FACTO_SYTRF><<<ntasks, 256, smem, st>>>(s, tasks, L, winv, toff, hi, lo);
+        subpanel_trsm_kernel<T, FACTO_SYTRF><<<ntasks, ST_ROWS, smem, st>>>(s, tasks, L, toff, hi, lo);
 }
 
-template void launch_subpanel_diag<double>(int, const DevSym &, const SubTask *, int, double *, double *,
-                                           const double *, unsigned long long *, int *, cudaStream_t);
-template void launch_subpanel_diag<float>(int, const DevSym &, const SubTask *, int, float *, float *, const double *,
+template void launch_subpanel_diag<double>(int, const DevSym &, const SubTask *, int, double *, const double *,
+                                           unsigned long long *, int *, cudaStream_t);
+template void launch_subpanel_diag<float>(int, const DevSym &, const SubTask *, int, float *, const double *,
                                           unsigned long long *, int *, cudaStream_t);
-template void launch_subpanel_trsm<double>(int, const DevSym &, const SubTask *, int, double *, const double *,
-                                           const int64_t *, float *, float *, cudaStream_t);
-template void launch_subpanel_trsm<float>(int, const DevSym &, const SubTask *, int, float *, const float *,
-                                          const int64_t *, float *, float *, cudaStream_t);
+template void launch_subpanel_trsm<double>(int, const DevSym &, const SubTask *, int, double *, const int64_t *,
+                                           float *, float *, cudaStream_t);
+template void launch_subpanel_trsm<float>(int, const DevSym &, const SubTask *, int, float *, const int64_t *, float *,
+                                          float *, cudaStream_t);
+
+
 
 // ------------------------------------------------------------------ updates
 
@@ -1077,15 +1085,16 @@ __global__ void __launch_bounds__(32 * DS_WARPS) diag_small_kernel(DevSym s, con
     const double thr = *thr_ptr;
     T *A = L + s.off[k];
     if (lane == 0) { s_piv[warp] = 0; s_err[warp] = 0; }
-    for (int idx = lane; idx < 32 * 32; idx += 32) {
-        const int i = idx & 31, j = idx >> 5;
-        T v = 0;
-        if (i < n && j < n) {
-            v = A[i + (size_t)j * ld];
-            if (FACTO == FACTO_GETRF) v += U[s.off[k] + j + (size_t)i * ld];
-        }
-        tile[i + j * TP] = v;
-    }
+    stage_n<32, T>(
+        [&](int j) {
+            T v = 0;
+            if (lane < n && j < n) {
+                v = A[lane + (size_t)j * ld];
+                if (FACTO == FACTO_GETRF) v += U[s.off[k] + j + (size_t)lane * ld];
+            }
+            return v;
+        },
+        [&](int j, T v) { tile[lane + j * TP] = v; });
     __syncwarp();
     factor_tile<T, FACTO>(tile, n, lane, thr, &s_piv[warp], &s_err[warp]);
     invert_lower_tile<T>(tile, wl, n, lane, FACTO != FACTO_POTRF, 0);

@@ -25,14 +25,15 @@ void launch_diag_small(int facto, const DevSym &s, const int *cblks, int ncblk, 
 template <typename T>
 void launch_trsm(const DevSym &s, const RowTask *tasks, int ntasks, int TR, int nmax, T *P, const T *D, int mode,
                  const T *tinv, const int64_t *tinv_off, int which, int getrf, int scale_d, cudaStream_t st);
-// sub-panel path of wide POTRF / LDL^T cblks (64-column steps)
+// sub-panel path of wide POTRF / LDL^T cblks (64-column steps): the 64x64 diagonal
+// tile, then the rows below it by substitution (tasks with split also write their
+// rows into the tensor-core operand arenas hi / lo)
 template <typename T>
-void launch_subpanel_diag(int facto, const DevSym &s, const SubTask *tasks, int ntasks, T *L, T *winv,
-                          const double *thr, unsigned long long *npiv, int *err, cudaStream_t st);
-// (tasks with split also write their rows into the tensor-core operand arenas hi / lo)
+void launch_subpanel_diag(int facto, const DevSym &s, const SubTask *tasks, int ntasks, T *L, const double *thr,
+                          unsigned long long *npiv, int *err, cudaStream_t st);
 template <typename T>
-void launch_subpanel_trsm(int facto, const DevSym &s, const SubTask *tasks, int ntasks, T *L, const T *winv,
-                          const int64_t *toff, float *hi, float *lo, cudaStream_t st);
+void launch_subpanel_trsm(int facto, const DevSym &s, const SubTask *tasks, int ntasks, T *L, const int64_t *toff,
+                          float *hi, float *lo, cudaStream_t st);
 // updates with K <= 16 and N <= 32, one warp each
 template <typename T>
 void launch_update_small(const DevSym &s, const Upd *upds, int nupd, T *L, T *U, cudaStream_t st);
@@ -57,22 +58,17 @@ int encode_operand_maps(const std::vector<int64_t> &toff, const std::vector<int>
                         const std::vector<int> &ncols, const std::vector<char> &wanted, float *arena,
                         CUtensorMap *maps);
 
-// solve (solve_kernels.cu); x is the permuted right-hand side block, n x nrhs, leading dimension ldx
-template <typename T>
-void launch_solve_diag(const DevSym &s, const int *cblks, int ncblk, int nmax, const T *L, double *x, int64_t ldx,
-                       int nrhs, int backward, int unit, cudaStream_t st);
-template <typename T>
-void launch_solve_offdiag(const DevSym &s, const RowTask *tasks, int ntasks, const T *L, double *x, int64_t ldx,
-                          int nrhs, int backward, cudaStream_t st);
-// off-diagonal solve on 64x64 tiles with FP64 tensor cores; x and b may be the same buffer
-template <typename T>
-void launch_solve_tiles(const DevSym &s, const SolveTile *tasks, int ntasks, const T *L, const double *x, double *b,
+// solve (solve_kernels.cu); x is the permuted right-hand side block, n x nrhs, leading
+// dimension ldx, in the vector precision V (double with an FP64 factor, float with FP32)
+// off-diagonal solve on 64x64 tiles with tensor cores (atomic accumulation into b)
+template <typename T, typename V>
+void launch_solve_tiles(const DevSym &s, const SolveTile *tasks, int ntasks, const T *L, const V *x, V *b,
                         int64_t ldx, int nrhs, int backward, cudaStream_t st);
 // both sweeps' work of cblks with at most 32 columns, one warp per cblk: forward
 // aux_k = W_k x_k and x[rows below] -= P aux_k; backward x_k = W_k^T (aux_k - P^T x[rows below])
-template <typename T>
+template <typename T, typename V>
 void launch_solve_leaf(const DevSym &s, const int *cblks, int ncblk, const T *P, const T *W, const int64_t *woff,
-                       double *x, double *aux, int64_t ldx, int nrhs, int backward, cudaStream_t st);
+                       V *x, V *aux, int64_t ldx, int nrhs, int backward, cudaStream_t st);
 // W_k = inverse of the lower-triangular diagonal block of every listed cblk (W: n x n per cblk)
 template <typename T>
 void launch_diag_inverse(const DevSym &s, const int *cblks, int ncblk, const T *L, T *W, const int64_t *woff,
@@ -82,13 +78,16 @@ template <typename T>
 void launch_copy_tile_inverse(const DevSym &s, const int *cblks, int ncblk, const T *tinv, const int64_t *toff, T *W,
                               const int64_t *woff, int which, cudaStream_t st);
 // xout[k] += W_k xin[k] (forward) or W_k^T xin[k] (backward), one 64 x 64 tile of W_k per task
-// {k, output row0, K chunk col0}; xout zeroed by the caller before the sweep
-template <typename T>
+// {k, output row0, K chunk col0}, xout zeroed by the caller before the sweep
+template <typename T, typename V>
 void launch_solve_diag_inv(const DevSym &s, const SolveTile *tasks, int ntasks, const T *W, const int64_t *woff,
-                           const double *xin, double *xout, int64_t ldx, int nrhs, int backward, cudaStream_t st);
-template <typename T>
-void launch_solve_scale_diag(const DevSym &s, const int *cblks, int ncblk, const T *L, double *x, int64_t ldx,
-                             int nrhs, cudaStream_t st);
+                           const V *xin, V *xout, int64_t ldx, int nrhs, int backward, cudaStream_t st);
+template <typename T, typename V>
+void launch_solve_scale_diag(const DevSym &s, const int *cblks, int ncblk, const T *L, V *x, int64_t ldx, int nrhs,
+                             cudaStream_t st);
+// dst = (D) src on an n x nrhs block
+template <typename S, typename D>
+void launch_convert(int n, int nrhs, const S *src, int64_t lds, D *dst, int64_t ldd, cudaStream_t st);
 void launch_permute(int n, int nrhs, const int *peri, const double *src, int64_t lds, double *dst, int64_t ldd,
                     int forward, cudaStream_t st);
 int configure_solve_kernels();

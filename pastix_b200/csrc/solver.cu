@@ -117,8 +117,6 @@ struct b200_solver_s {
     std::vector<std::vector<SubStep>> lvl_steps;
     SubTask *d_subtask = nullptr;
     Upd *d_subupd = nullptr;
-    void *d_subwinv = nullptr;
-    int64_t subwinv_slots = 0;
     // FP32 updates on the tensor cores (precision TF32 / TF32X3); updates below the
     // size thresholds stay on the SIMT kernel
     bool use_tc = false;
@@ -334,7 +332,6 @@ int build_schedule(b200_solver_t *s) {
                     pos++;
                 }
                 ss.d1 = (int)subtasks.size();
-                s->subwinv_slots = std::max<int64_t>(s->subwinv_slots, pos);
                 // internal update of a member: the columns right of the sub-panel
                 auto internal = [&](int k) {
                     const int n = s->ncols[k];
@@ -358,7 +355,7 @@ int build_schedule(b200_solver_t *s) {
                     const int wd = std::min(64, s->ncols[k] - c0);  // rows below the sub-panel's tile
                     // the TRSM also writes the tensor-core operand copies of its rows
                     const int split = (c0 + 64 < s->ncols[k] && tc_ok(internal(k))) ? 1 : 0;
-                    for (int r0 = c0 + wd; r0 < s->stride[k]; r0 += 64) subtasks.push_back({k, r0, c0, m.second, split});
+                    for (int r0 = c0 + wd; r0 < s->stride[k]; r0 += 128) subtasks.push_back({k, r0, c0, m.second, split});
                 }
                 ss.t1 = (int)subtasks.size();
                 ss.u0 = (int)subupds.size();
@@ -696,7 +693,7 @@ int enqueue_numfact(b200_solver_t *s, cudaStream_t st, Trace *tr = nullptr) {
         // sub-panel steps of the wide cblks
         for (const auto &ss : s->lvl_steps[l]) {
             if (tr) tr->begin(st);
-            launch_subpanel_diag<T>(s->facto, s->ds, s->d_subtask + ss.d0, ss.d1 - ss.d0, L, (T *)s->d_subwinv,
+            launch_subpanel_diag<T>(s->facto, s->ds, s->d_subtask + ss.d0, ss.d1 - ss.d0, L,
                                     s->d_thr, s->d_npiv, s->d_err, st);
             launches++;
             if (tr) tr->end(4, st);
@@ -707,8 +704,8 @@ int enqueue_numfact(b200_solver_t *s, cudaStream_t st, Trace *tr = nullptr) {
                     hi = (float *)s->d_tarena;
                     lo = s->prec == B200_PREC_TF32X3 ? hi + s->tsize : nullptr;
                 }
-                launch_subpanel_trsm<T>(s->facto, s->ds, s->d_subtask + ss.t0, ss.t1 - ss.t0, L,
-                                        (const T *)s->d_subwinv, s->d_toffT, hi, lo, st);
+                launch_subpanel_trsm<T>(s->facto, s->ds, s->d_subtask + ss.t0, ss.t1 - ss.t0, L, s->d_toffT, hi, lo,
+                                        st);
                 launches++;
                 if (tr) tr->end(5, st);
             }
@@ -791,7 +788,7 @@ int enqueue_numfact(b200_solver_t *s, cudaStream_t st, Trace *tr = nullptr) {
 // aux_k = W_L,k x_k, then x[ancestor rows] -= P_k aux_k; backward (levels in
 // reverse): aux_k -= P_k^T x[ancestor rows], then x_k = W_B,k^T aux_k.
 template <typename T>
-int enqueue_sweeps(b200_solver_t *s, double *x, double *aux, int64_t ldx, int nrhs, cudaStream_t st, int *launches,
+int enqueue_sweeps(b200_solver_t *s, T *x, T *aux, int64_t ldx, int nrhs, cudaStream_t st, int *launches,
                    Trace *tr = nullptr) {
     const T *L = (const T *)s->dL;
     const T *Ub = (s->facto == FACTO_GETRF) ? (const T *)s->dU : L;
@@ -799,7 +796,7 @@ int enqueue_sweeps(b200_solver_t *s, double *x, double *aux, int64_t ldx, int nr
     const T *WB = (s->facto == FACTO_GETRF) ? (const T *)s->dWU : WL;
     const int nlev = (int)s->levels.size();
     // the diagonal-block products accumulate their K chunks: zero their outputs
-    CU(cudaMemset2DAsync(aux, (size_t)ldx * sizeof(double), 0, (size_t)s->n * sizeof(double), nrhs, st));
+    CU(cudaMemset2DAsync(aux, (size_t)ldx * sizeof(T), 0, (size_t)s->n * sizeof(T), nrhs, st));
     for (int l = 0; l < nlev; l++) {
         const int nlf = s->lvl_lf1[l] - s->lvl_lf0[l];
         if (nlf > 0) {
@@ -822,7 +819,7 @@ int enqueue_sweeps(b200_solver_t *s, double *x, double *aux, int64_t ldx, int nr
         launch_solve_scale_diag<T>(s->ds, s->d_lvl_cblk, s->cblknbr, L, aux, ldx, nrhs, st);
         *launches += 1;
     }
-    CU(cudaMemset2DAsync(x, (size_t)ldx * sizeof(double), 0, (size_t)s->n * sizeof(double), nrhs, st));
+    CU(cudaMemset2DAsync(x, (size_t)ldx * sizeof(T), 0, (size_t)s->n * sizeof(T), nrhs, st));
     for (int l = nlev - 1; l >= 0; l--) {
         const int nlf = s->lvl_lf1[l] - s->lvl_lf0[l];
         if (nlf > 0) {
@@ -845,9 +842,19 @@ int enqueue_sweeps(b200_solver_t *s, double *x, double *aux, int64_t ldx, int nr
     return ERR_SUCCESS;
 }
 
-int sweeps(b200_solver_t *s, double *x, double *aux, int64_t ldx, int nrhs, cudaStream_t st, int *launches) {
-    return s->f32 ? enqueue_sweeps<float>(s, x, aux, ldx, nrhs, st, launches)
-                  : enqueue_sweeps<double>(s, x, aux, ldx, nrhs, st, launches);
+// Sweeps on the permuted block x (double, leading dimension ldx) with the scratch
+// aux (n x nrhs doubles).  An FP32 factor runs the sweeps in FP32 -- they apply the
+// preconditioner of an FP64 refinement -- on two n x nrhs float blocks held in aux,
+// converted from and back to x.
+int sweeps(b200_solver_t *s, double *x, double *aux, int64_t ldx, int nrhs, cudaStream_t st, int *launches,
+           Trace *tr = nullptr) {
+    if (!s->f32) return enqueue_sweeps<double>(s, x, aux, ldx, nrhs, st, launches, tr);
+    float *xf = reinterpret_cast<float *>(aux), *af = xf + (size_t)s->n * nrhs;
+    launch_convert<double, float>(s->n, nrhs, x, ldx, xf, s->n, st);
+    RET(enqueue_sweeps<float>(s, xf, af, s->n, nrhs, st, launches, tr));
+    launch_convert<float, double>(s->n, nrhs, xf, s->n, x, ldx, st);
+    *launches += 2;
+    return ERR_SUCCESS;
 }
 
 // Full solve of device b (original ordering): permute, sweeps, permute back.
@@ -1308,7 +1315,6 @@ int b200_solver_create(const b200_symbol_t *sym, int facto, int precision, void 
     if (!rc && facto == FACTO_GETRF) rc = dalloc((char **)&s->dU, (size_t)s->arena * s->esz);
     if (!rc) rc = dalloc((char **)&s->dWL, (size_t)s->winv_elems * s->esz);
     if (!rc) rc = dalloc((char **)&s->dTinv, (size_t)s->tinv_elems * s->esz);
-    if (!rc) rc = dalloc((char **)&s->d_subwinv, (size_t)std::max<int64_t>(s->subwinv_slots, 1) * 64 * 64 * s->esz);
     if (!rc && facto == FACTO_GETRF) rc = dalloc((char **)&s->dWU, (size_t)s->winv_elems * s->esz);
     if (!rc && s->use_tc) {
         // operand arenas and their tensor maps
@@ -1354,7 +1360,6 @@ int b200_solver_destroy(b200_solver_t *s) {
     if (s->dU) cudaFree(s->dU);
     if (s->dWL) cudaFree(s->dWL);
     if (s->dTinv) cudaFree(s->dTinv);
-    if (s->d_subwinv) cudaFree(s->d_subwinv);
     if (s->d_tarena) cudaFree(s->d_tarena);
     if (s->dWU) cudaFree(s->dWU);
     if (s->d_colptr) cudaFree(s->d_colptr);
@@ -1516,8 +1521,7 @@ int b200_solve_trace(b200_solver_t *s, int64_t nrhs, double *ms, double *bytes) 
     int launches = 0;
     tr.begin(s->st);
     tr.end(0, s->st);
-    int rc = s->f32 ? enqueue_sweeps<float>(s, xp, aux, n, (int)nrhs, s->st, &launches, &tr)
-                    : enqueue_sweeps<double>(s, xp, aux, n, (int)nrhs, s->st, &launches, &tr);
+    int rc = sweeps(s, xp, aux, n, (int)nrhs, s->st, &launches, &tr);
     if (rc) return rc;
     CU(cudaStreamSynchronize(s->st));
     s->kernel_launches += launches;

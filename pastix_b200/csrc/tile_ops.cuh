@@ -6,6 +6,18 @@ namespace b200 {
 
 constexpr int TP = 33;  // padded leading dimension of 32x32 shared tiles
 
+// Staging copy of N elements per thread: every load issued before the first store,
+// so a thread waits for one memory latency instead of N (a loop that stores each
+// loaded value into shared memory before the next load serialises the latencies).
+template <int N, typename V, typename Load, typename Store>
+__device__ __forceinline__ void stage_n(Load load, Store store) {
+    V tmp[N];
+#pragma unroll
+    for (int u = 0; u < N; u++) tmp[u] = load(u);
+#pragma unroll
+    for (int u = 0; u < N; u++) store(u, tmp[u]);
+}
+
 // Inverse of the lower triangle of a pb x pb tile by one warp: lane j forms column
 // j of W by forward substitution, W[m][j] = (delta_mj - sum_{p<m} T[m][p] W[p][j])
 // / T[m][m] (T[m][m] = 1 if unit), with row m of T broadcast by warp shuffles and
