@@ -41,7 +41,7 @@ def olib():
             from .build_oracle import build_oracle
             build_oracle()
         L = C.CDLL(_ORACLE)
-        for p in ("or_d_", "or_s_"):
+        for p in ("or_d_", "or_s_", "or_q_"):
             getattr(L, p + "fillin").argtypes = [_P] * 7
             getattr(L, p + "numfact").argtypes = [_P, C.c_int, _P, _P, _P, C.c_double, _P]
             getattr(L, p + "numfact").restype = C.c_int
@@ -81,7 +81,8 @@ class Oracle:
         self.cs = _Struct(st.cblknbr, st.bloknbr, *[a.ctypes.data for a in self._keep])
 
     def _fn(self, dtype, name):
-        return getattr(olib(), ("or_s_" if dtype == np.float32 else "or_d_") + name)
+        pre = {np.dtype(np.float32): "or_s_", np.dtype(np.longdouble): "or_q_"}.get(np.dtype(dtype), "or_d_")
+        return getattr(olib(), pre + name)
 
     def fillin(self, bcsc, dtype=np.float64):
         L = np.zeros(self.st.coefnbr, dtype=dtype)

@@ -1,7 +1,7 @@
 """Build the oracle (TEST INFRASTRUCTURE).
 
-* ``oracle/_lib/liboracle.so``: the plain-C restatement ``oracle.c`` (double and
-  float instantiations).  Needs only gcc.
+* ``oracle/_lib/liboracle.so``: the plain-C restatement ``oracle.c`` (double,
+  float and long double instantiations).  Needs only gcc.
 * ``oracle/_ref/libpastix_refdriver.so``: ``ref_driver.c``, which runs PaStiX's own
   CPU numerical factorization/solve/refinement; it links the PaStiX library built
   by ``pastix_b200/refhost/build_ref.py`` and needs that build's generated headers,
@@ -25,7 +25,7 @@ def build_oracle() -> str:
     if os.path.exists(so) and os.path.getmtime(so) >= os.path.getmtime(src):
         return so
     objs = []
-    for tag, defs in (("d", []), ("s", ["-DREAL=float"])):
+    for tag, defs in (("d", []), ("s", ["-DREAL=float"]), ("q", ["-DREAL=long double", "-DORACLE_LONG"])):
         o = os.path.join(out, f"oracle_{tag}.o")
         subprocess.run(["gcc", "-O2", "-fPIC", "-std=gnu99", *defs, "-c", src, "-o", o], check=True)
         objs.append(o)

@@ -13,8 +13,10 @@
  *
  * Arithmetic follows the reference kernels step by step (same blocking of 64
  * in the diagonal factorizations, same static-pivot rule, same update
- * ordering), restated with plain loops instead of BLAS calls.  Compiled twice,
- * for double (or_d_*) and float (or_s_*).
+ * ordering), restated with plain loops instead of BLAS calls.  Compiled for
+ * double (or_d_*) and float (or_s_*), and for x87 long double (or_q_*, 64-bit
+ * mantissa), whose factor stands in for the exact one when the tests rate how far
+ * two FP64 factorizations of an ill-conditioned matrix sit from it.
  */
 #include <math.h>
 #include <stdint.h>
@@ -24,8 +26,13 @@
 #ifndef REAL
 #define REAL double
 #define FN(x) or_d_##x
+#define SQRT(x) sqrt(x)
+#elif defined(ORACLE_LONG)
+#define FN(x) or_q_##x
+#define SQRT(x) sqrtl(x)
 #else
 #define FN(x) or_s_##x
+#define SQRT(x) sqrt((double)(x))
 #endif
 
 #define MAXSIZEOFBLOCKS 64 /* kernels/core_zpotrfsp.c:25 */
@@ -137,7 +144,7 @@ potf2( int64_t n, REAL *A, int64_t lda, int64_t *nbpivots, double criterion )
             (*nbpivots)++;
         }
         if ( *akk < 0 ) return -1;
-        *akk = (REAL)sqrt( (double)*akk );
+        *akk = (REAL)SQRT( *akk );
         REAL alpha = (REAL)1.0 / *akk;
         for ( int64_t i = k + 1; i < n; i++ ) A[i + k * lda] *= alpha;
         /* zher lower: A[k+1:,k+1:] -= a a^T */

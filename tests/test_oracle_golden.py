@@ -58,3 +58,22 @@ def test_oracle_detects_negative_pivot():
     L, U = orc.fillin(bc2)
     with pytest.raises(RuntimeError):
         orc.numfact(0, L, U, float(d["threshold"]))
+
+
+@pytest.mark.parametrize("name", names())
+def test_long_double_oracle_matches_pastix(name):
+    """The x87 long double instantiation (the exact-factor stand-in of the parity
+    tests) computes the same factor: PaStiX's FP64 factor lies within FP64
+    rounding of it, and it carries the same static pivots."""
+    A, st, bc, d = load(name)
+    orc = oracle.Oracle(st)
+    facto = int(d["facto"])
+    Lq, Uq = orc.fillin(bc, np.longdouble)
+    piv = orc.numfact(facto, Lq, Uq, float(d["threshold"]))
+    assert Lq.dtype == np.longdouble and piv == int(d["nbpivots"])
+    mask = orc.factor_mask(facto)
+    Lx = Lq.astype(np.float64)
+    assert np.linalg.norm((Lx - d["L"])[mask]) / np.linalg.norm(Lx[mask]) <= 1e-12
+    if Uq is not None:
+        Ux = Uq.astype(np.float64)
+        assert np.linalg.norm(Ux - d["U"]) / np.linalg.norm(Ux) <= 1e-12
