@@ -10,7 +10,7 @@ REPO = os.path.dirname(HERE)
 CSRC = os.path.join(HERE, "csrc")
 OUT = os.path.join(HERE, "lib")
 LIB = os.path.join(OUT, "libpastix_b200.so")
-SOURCES = ["solver.cu", "factor_kernels.cu", "solve_kernels.cu", "refine_kernels.cu", "update_tc.cu"]
+SOURCES = ["solver.cu", "factor_kernels.cu", "panel_kernels.cu", "solve_kernels.cu", "refine_kernels.cu", "update_tc.cu"]
 NVCC = os.environ.get("NVCC", "/usr/local/cuda/bin/nvcc")
 FLAGS = ["-gencode", "arch=compute_100a,code=sm_100a", "-lineinfo", "-O3", "-std=c++17",
          "-Xcompiler", "-fPIC", f"-I{os.path.join(REPO, 'include')}", f"-I{CSRC}"]

@@ -74,15 +74,17 @@ struct SolveTile {
     int col0;  // first column of the cblk
 };
 
-// Task of the sub-panel path for wide cblks: a 64-row tile of cblk k below the
-// 64-column sub-panel starting at column c0; pos is the cblk's slot in the step's
-// scratch of 64x64 inverses.
-struct SubTask {
-    int k;
-    int row0;
-    int c0;
-    int pos;
-    int split;  // TRSM task: also write the rows row-major (hi / lo) for the tensor-core update
+// Wide cblk of a panel launch (POTRF / LDL^T cblks wider than the one-CTA diagonal
+// kernel): ns steps of 64 columns, nrb row blocks of 64 rows (the first ns cover the
+// diagonal block, the others the rows below it), flag0 its first slot in the
+// per-row-block dependency counters.
+struct PanelCblk {
+    int k, ns, nrb, flag0;
+};
+
+// Item of a panel launch: step j of wide cblk p on row block b (b >= j).
+struct PanelItem {
+    int p, j, b;
 };
 
 // 32 x 32 tile of a panel copied to the row-major operand arena of the tensor-core

@@ -568,266 +568,6 @@ __global__ void __launch_bounds__(256) panel_trsm_kernel(DevSym s, const RowTask
     }
 }
 
-// ------------------------------------------------------------------ sub-panels of wide cblks
-//
-// POTRF / LDL^T of a wide cblk as a sequence of 64-column sub-panels (PaStiX
-// factors the diagonal block with its blocked core_zpotrfsp / core_zsytrfsp and
-// then solves the whole panel; here the same blocked right-looking algorithm is
-// spread over many CTAs): factor the 64x64 diagonal tile of the sub-panel and
-// invert it (one CTA, in shared memory), solve every row below it in the panel
-// as a product with that inverse (one CTA per 64 rows), then update the
-// remaining columns of the panel with the GEMM-scatter kernel (f = k).
-
-constexpr int SP = 64, SPP = 65;
-
-// 64x64 diagonal tile of a sub-panel (core_zpotrfsp / core_zsytrfsp,
-// kernels/core_zpotrfsp.c:66-100 and kernels/core_zsytrfsp.c:63-103), blocked
-// right-looking with 8-column leaves, in shared memory:
-//   leaf  (one warp, registers): the 8 columns factored column by column over all
-//         rows of the tile (lane = rows b + lane and b + lane + 32), pivots and
-//         leaf-internal updates broadcast by warp shuffles;
-//   update (256 threads): the columns right of the leaf, a_ij -= sum_c l_ic (d_c) l_jc
-//         in column order.
-// Two CTA barriers per leaf instead of three per column; the summation order per
-// entry is the right-looking factorization's, so the result matches it to rounding.
-// LDL^T keeps D on the diagonal and unit L below (no D L^T copy is needed by the
-// sub-panel TRSM, which solves against L and D).
-template <typename T, int FACTO>
-__global__ void __launch_bounds__(256) subpanel_diag_kernel(DevSym s, const SubTask *__restrict__ tasks, T *L,
-                                                            const double *__restrict__ thr_ptr,
-                                                            unsigned long long *npiv, int *err) {
-    __shared__ T a[SP * SPP];
-    __shared__ int s_piv, s_err;
-    const SubTask tk = tasks[blockIdx.x];
-    const int k = tk.k, c0 = tk.c0, ld = s.ld[k];
-    const int wd = min(SP, s.ncols[k] - c0);
-    const double thr = *thr_ptr;
-    T *A = L + s.off[k] + c0 + (size_t)c0 * ld;
-    const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
-    if (tid == 0) { s_piv = 0; s_err = 0; }
-    stage_n<SP * SP / 256, T>(
-        [&](int u) {
-            const int idx = tid + 256 * u, i = idx & 63, j = idx >> 6;
-            return (i < wd && j < wd && i >= j) ? A[i + (size_t)j * ld] : (T)0;
-        },
-        [&](int u, T v) {
-            const int idx = tid + 256 * u;
-            a[(idx & 63) + (idx >> 6) * SPP] = v;
-        });
-    __syncthreads();
-    for (int b = 0; b < wd; b += 8) {
-        const int bw = min(8, wd - b);
-        if (warp == 0) {
-            const int i0 = b + lane, i1 = b + lane + 32;
-            const bool in0 = i0 < wd, in1 = i1 < wd;
-            T r0[8], r1[8];
-#pragma unroll
-            for (int j = 0; j < 8; j++) {
-                r0[j] = (in0 && j < bw) ? a[i0 + (b + j) * SPP] : (T)0;
-                r1[j] = (in1 && j < bw) ? a[i1 + (b + j) * SPP] : (T)0;
-            }
-            int piv = 0, neg = 0;
-#pragma unroll
-            for (int c = 0; c < 8; c++) {
-                if (c < bw) {
-                    T p = __shfl_sync(0xffffffffu, r0[c], c);
-                    const bool rep = fabs((double)p) < thr;
-                    if (rep) p = (FACTO == FACTO_POTRF) ? (T)thr : ((p < (T)0) ? (T)(-thr) : (T)thr);
-                    T d, inv;
-                    if (FACTO == FACTO_POTRF) {
-                        if (p < (T)0) { neg = 1; p = -p; }
-                        d = sqrt(p);
-                        inv = rsqrt(p);
-                    } else {
-                        d = p;
-                        inv = (T)1 / p;
-                    }
-                    piv += rep;
-                    const bool b0 = in0 && i0 > b + c;
-                    if (lane == c) r0[c] = d;
-                    if (b0) r0[c] *= inv;
-                    if (in1) r1[c] *= inv;
-                    const T m0 = (FACTO == FACTO_SYTRF) ? -d * r0[c] : r0[c];
-                    const T m1 = (FACTO == FACTO_SYTRF) ? -d * r1[c] : r1[c];
-#pragma unroll
-                    for (int j = c + 1; j < 8; j++) {
-                        const T lj = __shfl_sync(0xffffffffu, r0[c], j);
-                        if (j < bw) {
-                            if (b0 && i0 >= b + j) {
-                                if (FACTO == FACTO_SYTRF) r0[j] += m0 * lj;
-                                else r0[j] -= m0 * lj;
-                            }
-                            if (in1) {
-                                if (FACTO == FACTO_SYTRF) r1[j] += m1 * lj;
-                                else r1[j] -= m1 * lj;
-                            }
-                        }
-                    }
-                }
-            }
-#pragma unroll
-            for (int j = 0; j < 8; j++) {
-                if (j < bw) {
-                    if (in0 && i0 >= b + j) a[i0 + (b + j) * SPP] = r0[j];
-                    if (in1) a[i1 + (b + j) * SPP] = r1[j];
-                }
-            }
-            if (lane == 0) {
-                s_piv += piv;
-                if (neg) s_err = 1;
-            }
-        }
-        __syncthreads();
-        // columns right of the leaf
-        const int j0 = b + bw, rem = wd - j0;
-        for (int idx = tid; idx < rem * rem; idx += 256) {
-            const int i = j0 + idx % rem, j = j0 + idx / rem;
-            if (i < j) continue;
-            T acc = a[i + j * SPP];
-#pragma unroll
-            for (int c = 0; c < 8; c++) {
-                if (c < bw) {
-                    const T lic = a[i + (b + c) * SPP], ljc = a[j + (b + c) * SPP];
-                    if (FACTO == FACTO_SYTRF) acc -= (lic * a[(b + c) * (SPP + 1)]) * ljc;
-                    else acc -= lic * ljc;
-                }
-            }
-            a[i + j * SPP] = acc;
-        }
-        __syncthreads();
-    }
-    for (int idx = tid; idx < SP * SP; idx += 256) {
-        const int i = idx & 63, j = idx >> 6;
-        if (i < wd && j < wd && i >= j) A[i + (size_t)j * ld] = a[i + j * SPP];
-    }
-    if (tid == 0) {
-        if (s_piv) atomicAdd(npiv, (unsigned long long)s_piv);
-        if (s_err) atomicOr(err, 1);
-    }
-}
-
-// The rows of the panel below the sub-panel's diagonal tile, 128 rows per CTA
-// (thread = row): POTRF X L^T = A, LDL^T X D L^T = A, by substitution against the
-// factored 64x64 tile in the reference's order (x_c = (a_c - sum_{l<c} x_l L_cl) /
-// L_cc; for LDL^T unit L, then division by D).  Tasks with `split` also write the
-// rows into the row-major operand arena of the tensor-core updates (hi = x with 13
-// low mantissa bits cleared, lo = x - hi when lo is given).
-constexpr int ST_ROWS = 128;
-
-template <typename T, int FACTO>
-__global__ void __launch_bounds__(ST_ROWS) subpanel_trsm_kernel(DevSym s, const SubTask *__restrict__ tasks, T *L,
-                                                                const int64_t *__restrict__ toff, float *hi,
-                                                                float *lo) {
-    extern __shared__ __align__(16) unsigned char sp_smem[];
-    T *lt = reinterpret_cast<T *>(sp_smem);  // lt[c + l * SPP] = L[c][l], l <= c (identity past wd)
-    T *xs = lt + SP * SPP;                   // the rows, ST_ROWS x 64 with pitch ST_ROWS + 1
-    __shared__ T rdiag[SP], dinv[SP];
-    const SubTask tk = tasks[blockIdx.x];
-    const int k = tk.k, c0 = tk.c0, ld = s.ld[k];
-    const int wd = min(SP, s.ncols[k] - c0);
-    const int rows = min(ST_ROWS, s.stride[k] - tk.row0);
-    T *X = L + s.off[k] + tk.row0 + (size_t)c0 * ld;
-    const T *Dg = L + s.off[k] + c0 + (size_t)c0 * ld;
-    const int tid = threadIdx.x;
-    stage_n<SP * SP / ST_ROWS, T>(
-        [&](int u) {
-            const int idx = tid + ST_ROWS * u, c = idx & 63, l = idx >> 6;
-            T v = 0;
-            if (c < wd && l < wd) v = (c > l) ? Dg[c + (size_t)l * ld] : (c == l ? (T)1 : (T)0);
-            else if (c == l) v = 1;
-            return v;
-        },
-        [&](int u, T v) {
-            const int idx = tid + ST_ROWS * u;
-            lt[(idx & 63) + (idx >> 6) * SPP] = v;
-        });
-    if (tid < SP) {
-        const T dgv = tid < wd ? Dg[(size_t)tid * (ld + 1)] : (T)1;
-        rdiag[tid] = (FACTO == FACTO_POTRF) ? (T)1 / dgv : (T)1;
-        dinv[tid] = (FACTO == FACTO_SYTRF) ? (T)1 / dgv : (T)1;
-    }
-    // the rows, staged column-major: xs[r + c * (ST_ROWS + 1)]
-#pragma unroll 1
-    for (int c0s = 0; c0s < SP; c0s += 16)
-        stage_n<16, T>([&](int u) { const int c = c0s + u; return (tid < rows && c < wd) ? X[tid + (size_t)c * ld] : (T)0; },
-                       [&](int u, T v) { xs[tid + (c0s + u) * (ST_ROWS + 1)] = v; });
-    __syncthreads();
-    const int r = tid;
-    T *xr = xs + r;
-    // 16-column blocks: the block's right-hand sides minus the solved columns to its
-    // left (one x per 16 updates), then substitution inside the block in registers
-#pragma unroll 1
-    for (int cb = 0; cb < SP; cb += 16) {
-        T acc[16];
-#pragma unroll
-        for (int q = 0; q < 16; q++) acc[q] = xr[(cb + q) * (ST_ROWS + 1)];
-        for (int l = 0; l < cb; l++) {
-            const T xl = xr[l * (ST_ROWS + 1)];
-            const T *lc = lt + cb + l * SPP;
-#pragma unroll
-            for (int q = 0; q < 16; q++) acc[q] -= xl * lc[q];
-        }
-#pragma unroll
-        for (int q = 0; q < 16; q++) {
-#pragma unroll
-            for (int p2 = 0; p2 < q; p2++) acc[q] -= acc[p2] * lt[(cb + q) + (cb + p2) * SPP];
-            acc[q] *= rdiag[cb + q];
-        }
-#pragma unroll
-        for (int q = 0; q < 16; q++) xr[(cb + q) * (ST_ROWS + 1)] = acc[q];
-    }
-    if (FACTO == FACTO_SYTRF) {
-        for (int c = 0; c < SP; c++) xr[c * (ST_ROWS + 1)] *= dinv[c];
-    }
-    if (r < rows) {
-        for (int c = 0; c < wd; c++) X[r + (size_t)c * ld] = xr[c * (ST_ROWS + 1)];
-    }
-    if (tk.split && hi) {
-        // row-major copy: consecutive threads, consecutive columns
-        __syncthreads();
-        const int kp = (s.ncols[k] + 3) & ~3;
-        for (int idx = tid; idx < rows * SP; idx += ST_ROWS) {
-            const int rr = idx >> 6, c = idx & 63;
-            if (c < wd) {
-                const float xv = (float)xs[rr + c * (ST_ROWS + 1)];
-                const float h = lo ? __uint_as_float(__float_as_uint(xv) & 0xFFFFE000u) : xv;
-                const size_t o = toff[k] + (size_t)(tk.row0 + rr) * kp + c0 + c;
-                hi[o] = h;
-                if (lo) lo[o] = xv - h;
-            }
-        }
-    }
-}
-
-template <typename T>
-void launch_subpanel_diag(int facto, const DevSym &s, const SubTask *tasks, int ntasks, T *L, const double *thr,
-                          unsigned long long *npiv, int *err, cudaStream_t st) {
-    if (ntasks <= 0) return;
-    if (facto == FACTO_POTRF)
-        subpanel_diag_kernel<T, FACTO_POTRF><<<ntasks, 256, 0, st>>>(s, tasks, L, thr, npiv, err);
-    else
-        subpanel_diag_kernel<T, FACTO_SYTRF><<<ntasks, 256, 0, st>>>(s, tasks, L, thr, npiv, err);
-}
-
-template <typename T>
-void launch_subpanel_trsm(int facto, const DevSym &s, const SubTask *tasks, int ntasks, T *L, const int64_t *toff,
-                          float *hi, float *lo, cudaStream_t st) {
-    if (ntasks <= 0) return;
-    const size_t smem = (SP * SPP + (ST_ROWS + 1) * SP) * sizeof(T);
-    if (facto == FACTO_POTRF)
-        subpanel_trsm_kernel<T, FACTO_POTRF><<<ntasks, ST_ROWS, smem, st>>>(s, tasks, L, toff, hi, lo);
-    else
-        subpanel_trsm_kernel<T, FACTO_SYTRF><<<ntasks, ST_ROWS, smem, st>>>(s, tasks, L, toff, hi, lo);
-}
-
-template void launch_subpanel_diag<double>(int, const DevSym &, const SubTask *, int, double *, const double *,
-                                           unsigned long long *, int *, cudaStream_t);
-template void launch_subpanel_diag<float>(int, const DevSym &, const SubTask *, int, float *, const double *,
-                                          unsigned long long *, int *, cudaStream_t);
-template void launch_subpanel_trsm<double>(int, const DevSym &, const SubTask *, int, double *, const int64_t *,
-                                           float *, float *, cudaStream_t);
-template void launch_subpanel_trsm<float>(int, const DevSym &, const SubTask *, int, float *, const int64_t *, float *,
-                                          float *, cudaStream_t);
 
 
 
@@ -1249,9 +989,6 @@ static int raise_smem(K kernel) {
 int configure_factor_kernels() {
     int lim = 1 << 30;
     int v;
-    if (raise_smem(subpanel_trsm_kernel<double, FACTO_POTRF>) < 0 || raise_smem(subpanel_trsm_kernel<double, FACTO_SYTRF>) < 0 ||
-        raise_smem(subpanel_trsm_kernel<float, FACTO_POTRF>) < 0 || raise_smem(subpanel_trsm_kernel<float, FACTO_SYTRF>) < 0)
-        return -1;
     if ((v = raise_smem(update_f64_kernel)) < UPD_F64_SMEM) return -1;
     if (raise_smem(diag_small_kernel<double, FACTO_POTRF>) < 0 || raise_smem(diag_small_kernel<double, FACTO_SYTRF>) < 0 ||
         raise_smem(diag_small_kernel<double, FACTO_GETRF>) < 0 || raise_smem(diag_small_kernel<float, FACTO_POTRF>) < 0 ||

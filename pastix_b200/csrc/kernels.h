@@ -25,15 +25,23 @@ void launch_diag_small(int facto, const DevSym &s, const int *cblks, int ncblk, 
 template <typename T>
 void launch_trsm(const DevSym &s, const RowTask *tasks, int ntasks, int TR, int nmax, T *P, const T *D, int mode,
                  const T *tinv, const int64_t *tinv_off, int which, int getrf, int scale_d, cudaStream_t st);
-// sub-panel path of wide POTRF / LDL^T cblks (64-column steps): the 64x64 diagonal
-// tile, then the rows below it by substitution (tasks with split also write their
-// rows into the tensor-core operand arenas hi / lo)
+// every wide POTRF / LDL^T cblk of a level in one launch (panel_kernels.cu): items
+// taken in order from *ticket, dependencies through the solved / updated counters
+// (zeroed before the factorization, like *ticket and *abort_word)
 template <typename T>
-void launch_subpanel_diag(int facto, const DevSym &s, const SubTask *tasks, int ntasks, T *L, const double *thr,
-                          unsigned long long *npiv, int *err, cudaStream_t st);
+void launch_panel(int facto, const DevSym &s, const PanelCblk *pcb, const PanelItem *items, int nitems, int *ticket,
+                  int *solved, int *updated, int *abort_word, T *L, const double *thr, unsigned long long *npiv,
+                  int *err, cudaStream_t st);
+// the row-block form (one item per 64-row block, resident in shared memory for all
+// steps): items = the diagonal blocks' row blocks first, then the rows below;
+// nsmax = the most 64-column steps of a cblk of the launch; panel_rows_fit says
+// whether 64 rows of such a cblk fit in shared memory
 template <typename T>
-void launch_subpanel_trsm(int facto, const DevSym &s, const SubTask *tasks, int ntasks, T *L, const int64_t *toff,
-                          float *hi, float *lo, cudaStream_t st);
+void launch_panel_rows(int facto, const DevSym &s, const PanelCblk *pcb, const PanelItem *items, int nitems,
+                       int nsmax, int *ticket, int *solved, int *abort_word, T *L, const double *thr,
+                       unsigned long long *npiv, int *err, cudaStream_t st);
+bool panel_rows_fit(int nsmax, size_t esz);
+int configure_panel_kernels();
 // updates with K <= 16 and N <= 32, one warp each
 template <typename T>
 void launch_update_small(const DevSym &s, const Upd *upds, int nupd, T *L, T *U, cudaStream_t st);

@@ -102,21 +102,16 @@ struct b200_solver_s {
     int n_inv_small = 0, n_inv_big = 0;
     std::vector<int> lvl_ds0, lvl_ds1;
     std::vector<int> lvl_dsm0, lvl_dsm1;  // cblks of <= 32 columns (one warp each)
-    // sub-panel steps of wide POTRF / LDL^T cblks
-    struct SubStep {
-        int d0, d1;   // subpanel diagonal tasks
-        int t0, t1;   // subpanel TRSM tasks
-        int u0, u1;   // internal updates
-        int ntiles;
-        int tu0, tu1;  // internal updates on the tensor cores
-        int tntiles;
-        int sp0, sp1;  // operand copies for them
-        int tm0;       // their tile map (64-column tiles)
-        int tmw0, twtiles;  // and the 128-column tiles
-    };
-    std::vector<std::vector<SubStep>> lvl_steps;
-    SubTask *d_subtask = nullptr;
-    Upd *d_subupd = nullptr;
+    // wide POTRF / LDL^T cblks: one panel launch per level over their 64 x 64 tiles
+    std::vector<int> lvl_pi0, lvl_pi1;  // items of each level's launch
+    std::vector<int> lvl_prows;         // 1: row-block form (64 rows resident), 0: 64 x 64 tile items
+    std::vector<int> lvl_pns;           // most 64-column steps of a cblk of the level
+    bool panel_steps_only = false;      // environment B200_PANEL_TILES=1: always the tile-item form
+    PanelCblk *d_pcb = nullptr;
+    PanelItem *d_pitem = nullptr;
+    // [nlev tickets][solved counters][updated counters][abort word], zeroed per factorization
+    int *d_pflags = nullptr;
+    int n_pflags = 0, n_prb = 0;
     // FP32 updates on the tensor cores (precision TF32 / TF32X3); updates below the
     // size thresholds stay on the SIMT kernel
     bool use_tc = false;
@@ -141,7 +136,7 @@ struct b200_solver_s {
     int64_t total_tiles = 0;
     int trsm_smem = 0;                  // dynamic shared memory available to the panel TRSM
     double flops_class[4] = {0, 0, 0, 0};  // algorithmic flops per kernel class (see Trace)
-    double flops_kind[10] = {};            // algorithmic flops of the update kinds 3, 6, 8
+    double flops_kind[8] = {};             // algorithmic flops of the kinds 3 (updates), 4 (panels), 6 (TC updates)
     double bytes_scatter = 0;
 
     // bcsc
@@ -214,8 +209,8 @@ int build_schedule(b200_solver_t *s) {
     std::vector<SolveTile> stile;
     std::vector<Upd> upds;
     std::vector<int> diag_list;
-    std::vector<SubTask> subtasks;
-    std::vector<Upd> subupds;
+    std::vector<PanelCblk> pcbs;
+    std::vector<PanelItem> pitems;
     std::vector<Upd> tcupds;
     std::vector<int2> tcmap, tcmapw;  // tile maps of the 64- and 128-column tensor-core launches
     std::vector<Upd> smallupds;
@@ -247,7 +242,7 @@ int build_schedule(b200_solver_t *s) {
     // updates more than 64 columns wide take 128-column tiles (half the operand
     // traffic per flop of the 64-column tiles)
     auto push_tc = [&](Upd u, int &t0, int &t0w, int base) {
-        s->flops_kind[8] += upd_flops(u);
+        s->flops_kind[6] += upd_flops(u);
         const int bn = u.N > 64 ? 128 : 64;
         u.tiles_m = (u.M + 127) / 128;
         u.tiles_n = (u.N + bn - 1) / bn;
@@ -265,7 +260,10 @@ int build_schedule(b200_solver_t *s) {
     s->lvl_ds1.assign(nlev, 0);
     s->lvl_dsm0.assign(nlev, 0);
     s->lvl_dsm1.assign(nlev, 0);
-    s->lvl_steps.assign(nlev, {});
+    s->lvl_pi0.assign(nlev, 0);
+    s->lvl_pi1.assign(nlev, 0);
+    s->lvl_prows.assign(nlev, 0);
+    s->lvl_pns.assign(nlev, 0);
     const int split_min = 96;  // wider POTRF / LDL^T cblks take the sub-panel path
     auto is_big = [&](int k) { return s->facto != FACTO_GETRF && s->ncols[k] > split_min; };
     s->lvl_st0.assign(nlev, 0);
@@ -314,79 +312,45 @@ int build_schedule(b200_solver_t *s) {
             if (s->ncols[lvl_cblk[i]] <= 32) diag_list.push_back(lvl_cblk[i]);
         s->lvl_dsm1[l] = (int)diag_list.size();
         {
-            // sub-panel steps: 64 columns each, for every wide cblk of the level
-            int nsteps = 0;
-            for (int i = L.c0; i < L.c1; i++)
-                if (is_big(lvl_cblk[i])) nsteps = std::max(nsteps, (s->ncols[lvl_cblk[i]] + 63) / 64);
-            for (int st = 0; st < nsteps; st++) {
-                b200_solver_s::SubStep ss{};
-                const int c0 = st * 64;
-                int pos = 0;
-                ss.d0 = (int)subtasks.size();
-                std::vector<std::pair<int, int>> members;  // (k, pos)
-                for (int i = L.c0; i < L.c1; i++) {
-                    const int k = lvl_cblk[i];
-                    if (!is_big(k) || c0 >= s->ncols[k]) continue;
-                    members.push_back({k, pos});
-                    subtasks.push_back({k, c0, c0, pos, 0});
-                    pos++;
-                }
-                ss.d1 = (int)subtasks.size();
-                // internal update of a member: the columns right of the sub-panel
-                auto internal = [&](int k) {
-                    const int n = s->ncols[k];
-                    Upd u{};
-                    u.k = k;
-                    u.j = -1;
-                    u.f = k;
-                    u.colK0 = c0;
-                    u.rowA0 = c0 + 64;
-                    u.rowB0 = c0 + 64;
-                    u.M = s->stride[k] - (c0 + 64);
-                    u.N = n - (c0 + 64);
-                    u.K = 64;
-                    u.colbase = c0 + 64;
-                    u.flags = UPD_SYM | (s->facto == FACTO_SYTRF ? UPD_SCALE_D : 0);
-                    return u;
-                };
-                ss.t0 = (int)subtasks.size();
-                for (auto &m : members) {
-                    const int k = m.first;
-                    const int wd = std::min(64, s->ncols[k] - c0);  // rows below the sub-panel's tile
-                    // the TRSM also writes the tensor-core operand copies of its rows
-                    const int split = (c0 + 64 < s->ncols[k] && tc_ok(internal(k))) ? 1 : 0;
-                    for (int r0 = c0 + wd; r0 < s->stride[k]; r0 += 128) subtasks.push_back({k, r0, c0, m.second, split});
-                }
-                ss.t1 = (int)subtasks.size();
-                ss.u0 = (int)subupds.size();
-                ss.tu0 = (int)tcupds.size();
-                ss.tm0 = (int)tcmap.size();
-                ss.tmw0 = (int)tcmapw.size();
-                ss.sp0 = (int)splits.size();
-                int t0 = 0, tt0 = 0, ttw = 0;
-                for (auto &m : members) {
-                    const int k = m.first, n = s->ncols[k];
-                    if (c0 + 64 >= n) continue;
-                    Upd u = internal(k);
-                    if (tc_ok(u)) {
-                        push_tc(u, tt0, ttw, ss.tu0);  // operands copied by the step's TRSM
-                        continue;
-                    }
-                    s->flops_kind[6] += upd_flops(u);
-                    u.tiles_m = (u.M + 63) / 64;
-                    u.tiles_n = (u.N + 63) / 64;
-                    u.tile0 = t0;
-                    t0 += u.tiles_n * u.tiles_m - u.tiles_n * (u.tiles_n - 1) / 2;
-                    subupds.push_back(u);
-                }
-                ss.u1 = (int)subupds.size();
-                ss.ntiles = t0;
-                ss.tu1 = (int)tcupds.size();
-                ss.tntiles = tt0;
-                ss.twtiles = ttw;
-                ss.sp1 = (int)splits.size();
-                s->lvl_steps[l].push_back(ss);
+            // wide cblks: items (step j, row block b >= j) of the level's panel launch,
+            // step by step, then by the row block's distance from the step's diagonal
+            // tile, then by cblk (every item depends only on items before it)
+            s->lvl_pi0[l] = (int)pitems.size();
+            const int p0 = (int)pcbs.size();
+            int nsmax = 0, nrbmax = 0;
+            for (int i = L.c0; i < L.c1; i++) {
+                const int k = lvl_cblk[i];
+                if (!is_big(k)) continue;
+                PanelCblk pc;
+                pc.k = k;
+                pc.ns = (s->ncols[k] + 63) / 64;
+                pc.nrb = pc.ns + (s->stride[k] - s->ncols[k] + 63) / 64;
+                pc.flag0 = s->n_prb;
+                s->n_prb += pc.nrb;
+                pcbs.push_back(pc);
+                nsmax = std::max(nsmax, pc.ns);
+                nrbmax = std::max(nrbmax, pc.nrb);
+                // diagonal factorization, panel solve and the updates inside the panel
+                const double nc = s->ncols[k], m = s->stride[k] - s->ncols[k];
+                s->flops_kind[4] += nc * nc * nc / 3.0 + m * nc * nc;
             }
+            s->lvl_pns[l] = nsmax;
+            s->lvl_prows[l] = !s->panel_steps_only && panel_rows_fit(nsmax, s->esz);
+            if (s->lvl_prows[l]) {
+                // row blocks: the diagonal blocks' first (by row block, then cblk), then the rest
+                for (int b = 0; b < nsmax; b++)
+                    for (int p = p0; p < (int)pcbs.size(); p++)
+                        if (b < pcbs[p].ns) pitems.push_back({p, 0, b});
+                for (int b = 0; b < nrbmax; b++)
+                    for (int p = p0; p < (int)pcbs.size(); p++)
+                        if (pcbs[p].ns + b < pcbs[p].nrb) pitems.push_back({p, 0, pcbs[p].ns + b});
+            } else {
+                for (int j = 0; j < nsmax; j++)
+                    for (int d = 0; d < nrbmax - j; d++)
+                        for (int p = p0; p < (int)pcbs.size(); p++)
+                            if (j < pcbs[p].ns && j + d < pcbs[p].nrb) pitems.push_back({p, j, j + d});
+            }
+            s->lvl_pi1[l] = (int)pitems.size();
         }
         s->lvl_lf0[l] = (int)leaf.size();
         for (int i = L.c0; i < L.c1; i++) {
@@ -534,8 +498,10 @@ int build_schedule(b200_solver_t *s) {
         RET(s->dupload(&s->d_inv_small, small));
         RET(s->dupload(&s->d_inv_big, big));
     }
-    RET(s->dupload(&s->d_subtask, subtasks));
-    RET(s->dupload(&s->d_subupd, subupds));
+    RET(s->dupload(&s->d_pcb, pcbs));
+    RET(s->dupload(&s->d_pitem, pitems));
+    s->n_pflags = nlev + 2 * s->n_prb + 1;
+    RET(s->dmalloc(&s->d_pflags, (size_t)s->n_pflags));
     // inverse arena: n_k x n_k per cblk, 256-byte aligned
     std::vector<int64_t> woff(N);
     int64_t wpos = 0;
@@ -601,12 +567,11 @@ int ensure_scal(b200_solver_t *s, int count) {
 // kernels/kernels_trace.h:206-300): class 0 arena clear + bcsc scatter, 1 diagonal
 // blocks, 2 panel TRSM, 3 GEMM-scatter updates.
 // Fine kernel kinds recorded in the per-launch detail; ids 0-3 are the classes
-// above, 4 subpanel diagonal, 5 subpanel TRSM, 6 subpanel internal update,
-// 7 diagonal-block inverses, 8 updates on the tensor cores, 9 operand copies for
-// them (summed into classes 1, 2, 2, 1, 3, 3).
+// above, 4 panel factorizations of wide cblks, 5 diagonal-block inverses, 6 updates
+// on the tensor cores, 7 operand copies for them (summed into classes 1, 1, 3, 3).
 struct Trace {
-    static constexpr int NK = 10;
-    static int coarse(int c) { return c < 4 ? c : (c == 4 || c == 7) ? 1 : c >= 8 ? 3 : 2; }
+    static constexpr int NK = 8;
+    static int coarse(int c) { return c < 4 ? c : c < 6 ? 1 : 3; }
     std::vector<std::pair<cudaEvent_t, cudaEvent_t>> ev[NK];
     cudaEvent_t open = nullptr;
     void begin(cudaStream_t st) {
@@ -660,6 +625,7 @@ int enqueue_numfact(b200_solver_t *s, cudaStream_t st, Trace *tr = nullptr) {
     if (U) CU(cudaMemsetAsync(U, 0, s->arena * sizeof(T), st));
     CU(cudaMemsetAsync(s->d_npiv, 0, sizeof(unsigned long long), st));
     CU(cudaMemsetAsync(s->d_err, 0, sizeof(int), st));
+    CU(cudaMemsetAsync(s->d_pflags, 0, (size_t)s->n_pflags * sizeof(int), st));
     launch_scatter<T>(s->nnz, s->d_dest, s->d_Lv, s->d_Uv, L, U, st);
     if (tr) tr->end(0, st);
     launches++;
@@ -690,50 +656,20 @@ int enqueue_numfact(b200_solver_t *s, cudaStream_t st, Trace *tr = nullptr) {
             launches++;
         }
         if (tr) tr->end(2, st);
-        // sub-panel steps of the wide cblks
-        for (const auto &ss : s->lvl_steps[l]) {
+        // wide cblks: the whole panel factorization in one launch
+        if (s->lvl_pi1[l] > s->lvl_pi0[l]) {
             if (tr) tr->begin(st);
-            launch_subpanel_diag<T>(s->facto, s->ds, s->d_subtask + ss.d0, ss.d1 - ss.d0, L,
-                                    s->d_thr, s->d_npiv, s->d_err, st);
+            int *tickets = s->d_pflags, *solved = tickets + s->levels.size(), *updated = solved + s->n_prb;
+            int *abort_word = updated + s->n_prb;
+            if (s->lvl_prows[l])
+                launch_panel_rows<T>(s->facto, s->ds, s->d_pcb, s->d_pitem + s->lvl_pi0[l],
+                                     s->lvl_pi1[l] - s->lvl_pi0[l], s->lvl_pns[l], tickets + l, solved, abort_word, L,
+                                     s->d_thr, s->d_npiv, s->d_err, st);
+            else
+                launch_panel<T>(s->facto, s->ds, s->d_pcb, s->d_pitem + s->lvl_pi0[l], s->lvl_pi1[l] - s->lvl_pi0[l],
+                                tickets + l, solved, updated, abort_word, L, s->d_thr, s->d_npiv, s->d_err, st);
             launches++;
             if (tr) tr->end(4, st);
-            if (ss.t1 > ss.t0) {
-                if (tr) tr->begin(st);
-                float *hi = nullptr, *lo = nullptr;
-                if (s->use_tc) {
-                    hi = (float *)s->d_tarena;
-                    lo = s->prec == B200_PREC_TF32X3 ? hi + s->tsize : nullptr;
-                }
-                launch_subpanel_trsm<T>(s->facto, s->ds, s->d_subtask + ss.t0, ss.t1 - ss.t0, L, s->d_toffT, hi, lo,
-                                        st);
-                launches++;
-                if (tr) tr->end(5, st);
-            }
-            if (ss.ntiles > 0) {
-                if (tr) tr->begin(st);
-                if (sizeof(T) == 8)
-                    launch_update_f64(s->ds, s->d_subupd + ss.u0, ss.u1 - ss.u0, ss.ntiles, (double *)L, (double *)U, st);
-                else
-                    launch_update_f32(s->ds, s->d_subupd + ss.u0, ss.u1 - ss.u0, ss.ntiles, (float *)L, (float *)U, st);
-                launches++;
-                if (tr) tr->end(6, st);
-            }
-            if (ss.tntiles + ss.twtiles > 0) {
-                if (ss.sp1 > ss.sp0) {
-                    if (tr) tr->begin(st);
-                    enqueue_split(s, ss.sp0, ss.sp1, st);
-                    launches += 1 + (s->facto == FACTO_GETRF);
-                    if (tr) tr->end(9, st);
-                }
-                if (tr) tr->begin(st);
-                const int split = s->prec == B200_PREC_TF32X3;
-                launch_update_tc(s->ds, s->d_tcupd + ss.tu0, s->d_tcmap + ss.tm0, ss.tntiles, s->d_maps, (float *)L,
-                                 (float *)U, split, 64, s->d_err, st);
-                launch_update_tc(s->ds, s->d_tcupd + ss.tu0, s->d_tcmapw + ss.tmw0, ss.twtiles, s->d_maps, (float *)L,
-                                 (float *)U, split, 128, s->d_err, st);
-                launches += (ss.tntiles > 0) + (ss.twtiles > 0);
-                if (tr) tr->end(8, st);
-            }
         }
         if (tr) tr->begin(st);
         if (s->lvl_us1[l] > s->lvl_us0[l]) {
@@ -752,7 +688,7 @@ int enqueue_numfact(b200_solver_t *s, cudaStream_t st, Trace *tr = nullptr) {
             if (tr) tr->begin(st);
             enqueue_split(s, s->lvl_sp0[l], s->lvl_sp1[l], st);
             launches += 1 + (s->facto == FACTO_GETRF);
-            if (tr) tr->end(9, st);
+            if (tr) tr->end(7, st);
             if (tr) tr->begin(st);
             const int split = s->prec == B200_PREC_TF32X3;
             launch_update_tc(s->ds, s->d_tcupd + s->lvl_tc_u0[l], s->d_tcmap + s->lvl_tc_m0[l], s->lvl_tc_tiles[l],
@@ -760,7 +696,7 @@ int enqueue_numfact(b200_solver_t *s, cudaStream_t st, Trace *tr = nullptr) {
             launch_update_tc(s->ds, s->d_tcupd + s->lvl_tc_u0[l], s->d_tcmapw + s->lvl_tc_mw0[l],
                              s->lvl_tc_wtiles[l], s->d_maps, (float *)L, (float *)U, split, 128, s->d_err, st);
             launches += (s->lvl_tc_tiles[l] > 0) + (s->lvl_tc_wtiles[l] > 0);
-            if (tr) tr->end(8, st);
+            if (tr) tr->end(6, st);
         }
     }
     // inverses of the diagonal blocks for the solves (W_L of L; for LU also W_U of the stored U^T)
@@ -775,7 +711,7 @@ int enqueue_numfact(b200_solver_t *s, cudaStream_t st, Trace *tr = nullptr) {
         launch_diag_inverse<T>(s->ds, s->d_inv_big, s->n_inv_big, U, (T *)s->dWU, s->d_woff, 0, st);
         launches += 2;
     }
-    if (tr) tr->end(7, st);
+    if (tr) tr->end(5, st);
     CU(cudaGetLastError());
     s->launches_fact = launches;
     return ERR_SUCCESS;
@@ -1229,6 +1165,7 @@ int b200_solver_create(const b200_symbol_t *sym, int facto, int precision, void 
     s->use_tc = precision == B200_PREC_TF32 || precision == B200_PREC_TF32X3;
     if (const char *e = getenv("B200_TC_MIN_K")) s->tc_min_k = std::max(1, atoi(e));
     if (const char *e = getenv("B200_TC_MIN_M")) s->tc_min_m = std::max(1, atoi(e));
+    if (const char *e = getenv("B200_PANEL_TILES")) s->panel_steps_only = atoi(e) != 0;
     if (stream) {
         s->st = (cudaStream_t)stream;
     } else {
@@ -1290,7 +1227,7 @@ int b200_solver_create(const b200_symbol_t *sym, int facto, int precision, void 
     int rc = ERR_SUCCESS;
     s->trsm_smem = configure_factor_kernels();
     if (s->trsm_smem < 0 || configure_solve_kernels() < 0 || configure_inverse_kernels() < 0 ||
-        (s->use_tc && configure_tc_kernels() < 0)) {
+        configure_panel_kernels() < 0 || (s->use_tc && configure_tc_kernels() < 0)) {
         fprintf(stderr, "pastix_b200: cannot configure the shared memory of the kernels\n");
         rc = ERR_INTERNAL;
     }
@@ -1486,6 +1423,7 @@ int b200_numfact(b200_solver_t *s, double epsilon_magn_ctrl, int64_t *nbpivots) 
     s->last_npiv = (int64_t)piv;
     if (nbpivots) *nbpivots = (int64_t)piv;
     if (err & 2) fprintf(stderr, "pastix_b200: a tensor-core update timed out waiting for its operands\n");
+    if (err & 8) fprintf(stderr, "pastix_b200: a panel factorization timed out waiting for a tile\n");
     if (err & 1) fprintf(stderr, "pastix_b200: negative diagonal term in the Cholesky factorization\n");
     if (err) return ERR_INTERNAL;
     s->factored = true;
@@ -1547,7 +1485,7 @@ int b200_solve_trace(b200_solver_t *s, int64_t nrhs, double *ms, double *bytes) 
 
 int b200_trace_kinds(b200_solver_t *s, double *ms, double *flops, int nkinds) {
     if (!s || nkinds < 0) return -ERR_BADPARAM;
-    const int nk = std::min(nkinds, 10);
+    const int nk = std::min(nkinds, 8);
     for (int i = 0; i < nk; i++) {
         if (ms) ms[i] = 0.0;
         if (flops) flops[i] = s->flops_kind[i];

@@ -155,14 +155,14 @@ class Solver:
         lib().b200_trace_launches(self.h, _p(ms), _p(cls), cnt)
         return cls[:cnt], ms[:cnt]
 
-    KIND_NAMES = ["scatter", "diag", "trsm", "update", "sub_diag", "sub_trsm", "sub_update", "inverse",
-                  "tc_update", "tc_split"]
+    KIND_NAMES = ["scatter", "diag", "trsm", "update", "panel", "inverse", "tc_update", "tc_split"]
 
     def trace_kinds(self) -> dict:
         """Per-kind device time and algorithmic flops of the last numfact trace."""
-        ms = np.zeros(10)
-        fl = np.zeros(10)
-        lib().b200_trace_kinds(self.h, _p(ms), _p(fl), 10)
+        nk = len(self.KIND_NAMES)
+        ms = np.zeros(nk)
+        fl = np.zeros(nk)
+        lib().b200_trace_kinds(self.h, _p(ms), _p(fl), nk)
         return {n: dict(ms=float(ms[i]), flops=float(fl[i])) for i, n in enumerate(self.KIND_NAMES)}
 
     def solve(self, b: np.ndarray, inplace: bool = False) -> np.ndarray:

@@ -64,6 +64,7 @@ CASES = [
     ("sytrf", lambda: M.shifted_laplacian_2d(40, 0.5)),
     ("sytrf", lambda: M.shifted_laplacian_2d(40, 0.8)),           # indefinite, pivot growth ~70
     ("potrf", lambda: M.laplacian(30, 7, 5, 7, 6.0)),             # ragged grid
+    ("sytrf", lambda: M.laplacian(14, 14, 14, 7, 6.0, shift=-0.7)),  # indefinite 3D, cblks of 98 and 196 columns
     ("getrf", lambda: M.convection_diffusion(3, 2, 2, seed=1)),   # tiny: 12 unknowns
 ]
 
@@ -93,6 +94,19 @@ def test_fp64_factor_matches_oracle(facto, make):
     from the exact factor (PaStiX's and the oracle's alike) and two summation
     orders land ~1e-12 apart; there the bar is also met if the GPU factor is
     within 4x of the reference's own FP64 error from the exact factor."""
+    check_fp64_case(facto, make)
+
+
+@pytest.mark.parametrize("facto,make", [CASES[0], CASES[1], CASES[-2]])
+def test_panel_tile_item_form(monkeypatch, facto, make):
+    """The 64 x 64 tile-item form of the wide-cblk panel launch (the form taken
+    when 64 rows of a level's widest cblk do not fit in shared memory) gives the
+    same factor and solve."""
+    monkeypatch.setenv("B200_PANEL_TILES", "1")
+    check_fp64_case(facto, make)
+
+
+def check_fp64_case(facto, make):
     A = make()
     an = Analysis(A, facto)
     st = an.structure()

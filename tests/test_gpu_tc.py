@@ -22,7 +22,7 @@ from pastix_b200.refhost import Analysis
 pytestmark = pytest.mark.gpu
 
 BERR_TARGET = 1e-12
-TC_KIND = 8  # per-launch trace kind of the tensor-core update kernel
+TC_KIND = native.Solver.KIND_NAMES.index("tc_update")
 
 
 def factor_rel_diff(st, facto, bc, thr, s):
