@@ -32,15 +32,16 @@ template <typename T>
 void launch_panel(int facto, const DevSym &s, const PanelCblk *pcb, const PanelItem *items, int nitems, int *ticket,
                   int *solved, int *updated, int *abort_word, T *L, const double *thr, unsigned long long *npiv,
                   int *err, cudaStream_t st);
-// the row-block form (one item per 64-row block, resident in shared memory for all
-// steps): items = the diagonal blocks' row blocks first, then the rows below;
-// nsmax = the most 64-column steps of a cblk of the launch; panel_rows_fit says
-// whether 64 rows of such a cblk fit in shared memory
+// the row-block form (one item per row block, resident in shared memory for all
+// steps): items = the diagonal blocks' 64-row blocks first, then the rb-row blocks
+// below; nsmax = the most 64-column steps of a cblk of the launch;
+// panel_rows_block gives the rb (128 or 64) whose blocks of such a cblk fit in
+// shared memory, 0 if none does
 template <typename T>
 void launch_panel_rows(int facto, const DevSym &s, const PanelCblk *pcb, const PanelItem *items, int nitems,
-                       int nsmax, int *ticket, int *solved, int *abort_word, T *L, const double *thr,
+                       int nsmax, int rb, int *ticket, int *solved, int *abort_word, T *L, const double *thr,
                        unsigned long long *npiv, int *err, cudaStream_t st);
-bool panel_rows_fit(int nsmax, size_t esz);
+int panel_rows_block(int nsmax, size_t esz);
 int configure_panel_kernels();
 // updates with K <= 16 and N <= 32, one warp each
 template <typename T>

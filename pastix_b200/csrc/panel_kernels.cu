@@ -412,26 +412,169 @@ __global__ void __launch_bounds__(PT, sizeof(T) == 4 ? 2 : 1) panel_kernel(DevSy
     }
 }
 
-// Row-block form (when 64 rows x the level's widest cblk fit in shared memory):
-// one item per row block b, which keeps its 64 rows resident in shared memory for
-// all the steps -- solve of step j's columns, update of its columns right of the
-// step, for every j before the row block's own diagonal tile (all ns steps for
-// the rows below the diagonal block) -- and, for b < ns, finally factors its
-// diagonal tile (b, b).  Each solved step is written back and announced at once
-// (solved[b] = j + 1; b + 1 after the factorization), the only cross-item reads
-// being the factored tiles L[j, j] and the diagonal block's solved tiles L[c, j].
-// Items: the diagonal blocks' row blocks of every cblk first (b ascending), then
-// the rows below.
-template <typename T, int FACTO>
-__global__ void __launch_bounds__(PT, sizeof(T) == 4 ? 2 : 1) panel_rows_kernel(DevSym s, const PanelCblk *__restrict__ pcb,
-                                                        const PanelItem *__restrict__ items, int nitems, int *ticket,
-                                                        int *solved, int *abort_word, T *L,
-                                                        const double *__restrict__ thr_ptr, unsigned long long *npiv,
-                                                        int *err) {
+// Row-block form (when a row block x the level's widest cblk fits in shared
+// memory): one item per row block b, which keeps its rows resident in shared
+// memory for all the steps -- solve of step j's columns, update of its columns
+// right of the step, for every j before the row block's own diagonal tile (all ns
+// steps for the rows below the diagonal block) -- and, for b < ns, finally
+// factors its diagonal tile (b, b).  Each solved step of the diagonal block's
+// rows is written back and announced at once (solved[b] = j + 1; b + 1 after the
+// factorization), the only cross-item reads being the factored tiles L[j, j] and
+// the diagonal block's solved tiles L[c, j].  Row blocks: 64 rows in the diagonal
+// block, R rows (64 or 128) below it.  Items: the diagonal blocks' row blocks of
+// every cblk first (b ascending), then the rows below.
+template <typename T, int FACTO, int R>
+__device__ void rows_item(const DevSym &s, const PanelCblk &pc, int b, T *L, T *lt, T *rdiag, T *dinv, T *dd, T *xs,
+                          int *sol, const int *abort_word, double thr, int *s_ok, int *s_piv, int *s_err) {
+    constexpr int MR = R / 16;  // rows of a thread's update tile
+    const int tid = threadIdx.x;
+    const int k = pc.k, W = s.ncols[k], S = s.stride[k], ld = s.ld[k];
+    T *P = L + s.off[k];
+    const bool drows = b < pc.ns;
+    const int r0 = drows ? PB * b : W + R * (b - pc.ns);
+    const int nr = min(R, (drows ? W : S) - r0);
+    const int ncol = drows ? min(W, PB * (b + 1)) : W;  // columns held (lower part for the diagonal block)
+    const int nstep = drows ? b : pc.ns;                 // steps solved in this row block
+    // the row block: rows past nr, the diagonal tile's upper triangle and (below
+    // the diagonal block) the last step's columns past W as zeros
+    const int nzero = drows ? ncol : PB * pc.ns;
+    constexpr int CG = PT / R;  // column groups of a load pass
+    for (int c0s = 0; c0s < nzero; c0s += 4 * CG) {
+        stage_n<4, T>(
+            [&](int u) {
+                const int r = tid % R, c = c0s + tid / R + CG * u;
+                const bool keep = r < nr && c < ncol && (!drows || c < PB * b || r >= c - PB * b);
+                return keep ? __ldcg(P + r0 + r + (size_t)c * ld) : (T)0;
+            },
+            [&](int u, T v) {
+                const int r = tid % R, c = c0s + tid / R + CG * u;
+                if (c < nzero) xs[r + c * R] = v;
+            });
+    }
+    __syncthreads();
+    const int tx = tid & 15, ty = tid >> 4;
+    for (int j = 0; j < nstep && *s_ok; j++) {
+        const int c0 = PB * j, wd = min(PB, W - c0);
+        if (tid == 0 && !panel_wait(sol + j, j + 1, abort_word)) *s_ok = 0;
+        __syncthreads();
+        if (!*s_ok) break;
+        // ---------------------------------------------- solve of step j's columns
+        const T *Dg = P + c0 + (size_t)c0 * ld;
+        stage_n<PB * PB / PT, T>(
+            [&](int u) {
+                const int idx = tid + PT * u, c = idx & 63, l = idx >> 6;
+                T v = 0;
+                if (c < wd && l < wd) v = (c > l) ? __ldcg(Dg + c + (size_t)l * ld) : (c == l ? (T)1 : (T)0);
+                else if (c == l) v = 1;
+                return v;
+            },
+            [&](int u, T v) {
+                const int idx = tid + PT * u;
+                lt[(idx & 63) + (idx >> 6) * LP] = v;
+            });
+        if (tid < PB) {
+            const T dgv = tid < wd ? __ldcg(Dg + (size_t)tid * (ld + 1)) : (T)1;
+            rdiag[tid] = (FACTO == FACTO_POTRF) ? (T)1 / dgv : (T)1;
+            dinv[tid] = (FACTO == FACTO_SYTRF) ? (T)1 / dgv : (T)1;
+            dd[tid] = (FACTO == FACTO_SYTRF) ? dgv : (T)1;
+        }
+        __syncthreads();
+        if (tid < R) trsm_row64<T, FACTO, R>(xs + c0 * R, lt, rdiag, dinv, tid);
+        __syncthreads();
+        for (int idx = tid; idx < R * wd; idx += PT) {
+            const int r = idx % R, c = idx / R;
+            if (r < nr) P[r0 + r + (size_t)(c0 + c) * ld] = xs[r + (c0 + c) * R];
+        }
+        __syncthreads();
+        if (tid == 0 && drows) {
+            __threadfence();
+            st_release(sol + b, j + 1);
+        }
+        // ---------------------------------------------- update of the columns right of the step
+        const int cmax = drows ? b : pc.ns - 1;
+        for (int c = j + 1; c <= cmax; c++) {
+            if (tid == 0 && c != b && !panel_wait(sol + c, j + 1, abort_word)) *s_ok = 0;
+            __syncthreads();
+            if (!*s_ok) break;
+            const int wc = min(PB, W - PB * c);
+            T *bs = lt;  // bs[l * PB + row]
+            if (drows && c == b) {
+                // this row block's own tile: its solved columns are in shared memory
+                for (int idx = tid; idx < PB * PB; idx += PT) {
+                    const int rr = idx & 63, l = idx >> 6;
+                    const T v = (rr < wc && l < wd) ? xs[rr + (c0 + l) * R] : (T)0;
+                    bs[idx] = (FACTO == FACTO_SYTRF) ? v * dd[l] : v;
+                }
+            } else {
+                const T *B = P + PB * c + (size_t)c0 * ld;
+                stage_n<PB * PB / PT, T>(
+                    [&](int u) {
+                        const int idx = tid + PT * u, rr = idx & 63, l = idx >> 6;
+                        return (rr < wc && l < wd) ? __ldcg(B + rr + (size_t)l * ld) : (T)0;
+                    },
+                    [&](int u, T v) {
+                        const int idx = tid + PT * u;
+                        bs[idx] = (FACTO == FACTO_SYTRF) ? v * dd[idx >> 6] : v;
+                    });
+            }
+            __syncthreads();
+            T acc[MR][4];
+#pragma unroll
+            for (int i = 0; i < MR; i++)
+#pragma unroll
+                for (int q = 0; q < 4; q++) acc[i][q] = 0;
+            const T *xa = xs + c0 * R + MR * tx;
+            for (int l = 0; l < wd; l++) {
+                T av[MR], bv[4];
+#pragma unroll
+                for (int h = 0; h < MR / 4; h++) load4(xa + l * R + 4 * h, av + 4 * h);
+                load4(bs + l * PB + 4 * ty, bv);
+#pragma unroll
+                for (int i = 0; i < MR; i++)
+#pragma unroll
+                    for (int q = 0; q < 4; q++) acc[i][q] += av[i] * bv[q];
+            }
+            T *xc = xs + (PB * c) * R;
+#pragma unroll
+            for (int q = 0; q < 4; q++) {
+                const int cc = 4 * ty + q;
+                if (cc < wc) {
+#pragma unroll
+                    for (int i = 0; i < MR; i++) {
+                        const int r = MR * tx + i;
+                        if (!(drows && c == b) || r >= cc) xc[r + cc * R] -= acc[i][q];
+                    }
+                }
+            }
+            __syncthreads();
+        }
+    }
+    if (!*s_ok) return;
+    if (drows) {
+        // ---------------------------------------------- the row block's diagonal tile
+        const int c0 = PB * b, wd = min(PB, W - c0);
+        factor_tile64<T, FACTO, R>(xs + c0 * R, wd, thr, s_piv, s_err);
+        for (int idx = tid; idx < PB * PB; idx += PT) {
+            const int i = idx & 63, jj = idx >> 6;
+            if (i < wd && jj < wd && i >= jj) P[c0 + i + (size_t)(c0 + jj) * ld] = xs[i + (c0 + jj) * R];
+        }
+        __syncthreads();
+        if (tid == 0) {
+            __threadfence();
+            st_release(sol + b, b + 1);
+        }
+    }
+}
+
+template <typename T, int FACTO, int RB>
+__global__ void __launch_bounds__(PT, 1)
+    panel_rows_kernel(DevSym s, const PanelCblk *__restrict__ pcb, const PanelItem *__restrict__ items, int nitems,
+                      int *ticket, int *solved, int *abort_word, T *L, const double *__restrict__ thr_ptr,
+                      unsigned long long *npiv, int *err) {
     extern __shared__ __align__(16) unsigned char pn_smem[];
     T *lt = reinterpret_cast<T *>(pn_smem);  // L[j, j] (pitch LP) for the solve; L[c, j] (D_j) for the update
     T *rdiag = lt + PB * LP, *dinv = rdiag + PB, *dd = dinv + PB;
-    T *xs = dd + PB;                         // the row block: 64 rows x ncols, pitch RP
+    T *xs = dd + PB;                         // the row block, column-major (pitch = its rows)
     __shared__ int s_item, s_ok, s_piv, s_err;
     const int tid = threadIdx.x;
     const double thr = *thr_ptr;
@@ -448,146 +591,21 @@ __global__ void __launch_bounds__(PT, sizeof(T) == 4 ? 2 : 1) panel_rows_kernel(
         if (t >= nitems) break;
         const PanelItem it = items[t];
         const PanelCblk pc = pcb[it.p];
-        const int k = pc.k, b = it.b;
-        const int W = s.ncols[k], S = s.stride[k], ld = s.ld[k];
-        T *P = L + s.off[k];
         int *sol = solved + pc.flag0;
-        const bool drows = b < pc.ns;
-        const int r0 = drows ? PB * b : W + PB * (b - pc.ns);
-        const int nr = min(PB, (drows ? W : S) - r0);
-        const int ncol = drows ? min(W, PB * (b + 1)) : W;  // columns held (lower part for the diagonal block)
-        const int nstep = drows ? b : pc.ns;                 // steps solved in this row block
-        // the row block: rows past nr, the diagonal tile's upper triangle and (below
-        // the diagonal block) the last step's columns past W as zeros
-        const int nzero = drows ? ncol : PB * pc.ns;
-        for (int c0s = 0; c0s < nzero; c0s += PT / PB * 4) {
-            stage_n<4, T>(
-                [&](int u) {
-                    const int r = tid & 63, c = c0s + (tid >> 6) + 4 * u;
-                    const bool keep = r < nr && c < ncol && (!drows || c < PB * b || r >= c - PB * b);
-                    return keep ? __ldcg(P + r0 + r + (size_t)c * ld) : (T)0;
-                },
-                [&](int u, T v) {
-                    const int r = tid & 63, c = c0s + (tid >> 6) + 4 * u;
-                    if (c < nzero) xs[r + c * RP] = v;
-                });
-        }
+        if (it.b < pc.ns)
+            rows_item<T, FACTO, PB>(s, pc, it.b, L, lt, rdiag, dinv, dd, xs, sol, abort_word, thr, &s_ok, &s_piv,
+                                    &s_err);
+        else
+            rows_item<T, FACTO, RB>(s, pc, it.b, L, lt, rdiag, dinv, dd, xs, sol, abort_word, thr, &s_ok, &s_piv,
+                                    &s_err);
         __syncthreads();
-        const int tx = tid & 15, ty = tid >> 4;
-        for (int j = 0; j < nstep && s_ok; j++) {
-            const int c0 = PB * j, wd = min(PB, W - c0);
-            if (tid == 0 && !panel_wait(sol + j, j + 1, abort_word)) s_ok = 0;
-            __syncthreads();
-            if (!s_ok) break;
-            // ---------------------------------------------- solve of step j's columns
-            const T *Dg = P + c0 + (size_t)c0 * ld;
-            stage_n<PB * PB / PT, T>(
-                [&](int u) {
-                    const int idx = tid + PT * u, c = idx & 63, l = idx >> 6;
-                    T v = 0;
-                    if (c < wd && l < wd) v = (c > l) ? __ldcg(Dg + c + (size_t)l * ld) : (c == l ? (T)1 : (T)0);
-                    else if (c == l) v = 1;
-                    return v;
-                },
-                [&](int u, T v) {
-                    const int idx = tid + PT * u;
-                    lt[(idx & 63) + (idx >> 6) * LP] = v;
-                });
-            if (tid < PB) {
-                const T dgv = tid < wd ? __ldcg(Dg + (size_t)tid * (ld + 1)) : (T)1;
-                rdiag[tid] = (FACTO == FACTO_POTRF) ? (T)1 / dgv : (T)1;
-                dinv[tid] = (FACTO == FACTO_SYTRF) ? (T)1 / dgv : (T)1;
-                dd[tid] = (FACTO == FACTO_SYTRF) ? dgv : (T)1;
-            }
-            __syncthreads();
-            if (tid < PB) trsm_row64<T, FACTO, RP>(xs + c0 * RP, lt, rdiag, dinv, tid);
-            __syncthreads();
-            for (int idx = tid; idx < PB * wd; idx += PT) {
-                const int r = idx & 63, c = idx >> 6;
-                if (r < nr) P[r0 + r + (size_t)(c0 + c) * ld] = xs[r + (c0 + c) * RP];
-            }
-            __syncthreads();
-            if (tid == 0 && drows) {
-                __threadfence();
-                st_release(sol + b, j + 1);
-            }
-            // ---------------------------------------------- update of the columns right of the step
-            const int cmax = drows ? b : pc.ns - 1;
-            for (int c = j + 1; c <= cmax; c++) {
-                if (tid == 0 && c != b && !panel_wait(sol + c, j + 1, abort_word)) s_ok = 0;
-                __syncthreads();
-                if (!s_ok) break;
-                const int wc = min(PB, W - PB * c);
-                T *bs = lt;  // bs[l * PB + row]
-                if (c == b) {
-                    // this row block's own tile: its solved columns are in shared memory
-                    for (int idx = tid; idx < PB * PB; idx += PT) {
-                        const int rr = idx & 63, l = idx >> 6;
-                        const T v = (rr < wc && l < wd) ? xs[rr + (c0 + l) * RP] : (T)0;
-                        bs[idx] = (FACTO == FACTO_SYTRF) ? v * dd[l] : v;
-                    }
-                } else {
-                    const T *B = P + PB * c + (size_t)c0 * ld;
-                    stage_n<PB * PB / PT, T>(
-                        [&](int u) {
-                            const int idx = tid + PT * u, rr = idx & 63, l = idx >> 6;
-                            return (rr < wc && l < wd) ? __ldcg(B + rr + (size_t)l * ld) : (T)0;
-                        },
-                        [&](int u, T v) {
-                            const int idx = tid + PT * u;
-                            bs[idx] = (FACTO == FACTO_SYTRF) ? v * dd[idx >> 6] : v;
-                        });
-                }
-                __syncthreads();
-                T acc[4][4];
-#pragma unroll
-                for (int i = 0; i < 4; i++)
-#pragma unroll
-                    for (int q = 0; q < 4; q++) acc[i][q] = 0;
-                const T *xa = xs + c0 * RP + 4 * tx;
-                for (int l = 0; l < wd; l++) {
-                    T av[4], bv[4];
-                    load4(xa + l * RP, av);
-                    load4(bs + l * PB + 4 * ty, bv);
-#pragma unroll
-                    for (int i = 0; i < 4; i++)
-#pragma unroll
-                        for (int q = 0; q < 4; q++) acc[i][q] += av[i] * bv[q];
-                }
-                T *xc = xs + (PB * c) * RP;
-#pragma unroll
-                for (int q = 0; q < 4; q++) {
-                    const int cc = 4 * ty + q;
-                    if (cc < wc) {
-#pragma unroll
-                        for (int i = 0; i < 4; i++) {
-                            const int r = 4 * tx + i;
-                            if (c != b || r >= cc) xc[r + cc * RP] -= acc[i][q];
-                        }
-                    }
-                }
-                __syncthreads();
-            }
-        }
         if (!s_ok) {
             aborted = true;
             break;
         }
-        if (drows) {
-            // ---------------------------------------------- the row block's diagonal tile
-            const int c0 = PB * b, wd = min(PB, W - c0);
-            factor_tile64<T, FACTO, RP>(xs + c0 * RP, wd, thr, &s_piv, &s_err);
-            for (int idx = tid; idx < PB * PB; idx += PT) {
-                const int i = idx & 63, jj = idx >> 6;
-                if (i < wd && jj < wd && i >= jj) P[c0 + i + (size_t)(c0 + jj) * ld] = xs[i + (c0 + jj) * RP];
-            }
-            __syncthreads();
-            if (tid == 0) {
-                if (s_piv) atomicAdd(npiv, (unsigned long long)s_piv);
-                if (s_err) atomicOr(err, 1);
-                __threadfence();
-                st_release(sol + b, b + 1);
-            }
+        if (tid == 0) {
+            if (s_piv) atomicAdd(npiv, (unsigned long long)s_piv);
+            if (s_err) atomicOr(err, 1);
         }
         __syncthreads();
     }
@@ -600,7 +618,7 @@ __global__ void __launch_bounds__(PT, sizeof(T) == 4 ? 2 : 1) panel_rows_kernel(
 int g_panel_ctas = 0;  // resident CTAs of the panel kernel on the device (all SMs)
 int g_sms = 0, g_smem_optin = 0;
 
-constexpr size_t rows_smem_elems(int nsmax) { return (size_t)PB * LP + 3 * PB + (size_t)PB * PB * nsmax; }
+constexpr size_t rows_smem_elems(int nsmax, int rb) { return (size_t)PB * LP + 3 * PB + (size_t)rb * PB * nsmax; }
 
 template <typename T, int FACTO>
 int panel_occupancy() {
@@ -622,10 +640,12 @@ int configure_panel_kernels() {
     if (cudaDeviceGetAttribute(&g_smem_optin, cudaDevAttrMaxSharedMemoryPerBlockOptin, dev) != cudaSuccess) return -1;
     g_sms = sms;
     const int dyn = g_smem_optin - 64;  // room for the kernels' static shared variables
-    if (cudaFuncSetAttribute(panel_rows_kernel<double, FACTO_POTRF>, cudaFuncAttributeMaxDynamicSharedMemorySize, dyn) ||
-        cudaFuncSetAttribute(panel_rows_kernel<double, FACTO_SYTRF>, cudaFuncAttributeMaxDynamicSharedMemorySize, dyn) ||
-        cudaFuncSetAttribute(panel_rows_kernel<float, FACTO_POTRF>, cudaFuncAttributeMaxDynamicSharedMemorySize, dyn) ||
-        cudaFuncSetAttribute(panel_rows_kernel<float, FACTO_SYTRF>, cudaFuncAttributeMaxDynamicSharedMemorySize, dyn))
+    if (cudaFuncSetAttribute(panel_rows_kernel<double, FACTO_POTRF, PB>, cudaFuncAttributeMaxDynamicSharedMemorySize, dyn) ||
+        cudaFuncSetAttribute(panel_rows_kernel<double, FACTO_SYTRF, PB>, cudaFuncAttributeMaxDynamicSharedMemorySize, dyn) ||
+        cudaFuncSetAttribute(panel_rows_kernel<float, FACTO_POTRF, PB>, cudaFuncAttributeMaxDynamicSharedMemorySize, dyn) ||
+        cudaFuncSetAttribute(panel_rows_kernel<float, FACTO_SYTRF, PB>, cudaFuncAttributeMaxDynamicSharedMemorySize, dyn) ||
+        cudaFuncSetAttribute(panel_rows_kernel<float, FACTO_POTRF, 2 * PB>, cudaFuncAttributeMaxDynamicSharedMemorySize, dyn) ||
+        cudaFuncSetAttribute(panel_rows_kernel<float, FACTO_SYTRF, 2 * PB>, cudaFuncAttributeMaxDynamicSharedMemorySize, dyn))
         return -1;
     int occ = panel_occupancy<double, FACTO_POTRF>();
     occ = std::min(occ, panel_occupancy<double, FACTO_SYTRF>());
@@ -651,32 +671,50 @@ void launch_panel(int facto, const DevSym &s, const PanelCblk *pcb, const PanelI
                                                             abort_word, L, thr, npiv, err);
 }
 
-bool panel_rows_fit(int nsmax, size_t esz) { return rows_smem_elems(nsmax) * esz <= (size_t)g_smem_optin - 64; }
+int panel_rows_block(int nsmax, size_t esz) {
+    const size_t lim = (size_t)g_smem_optin - 64;
+    if (esz == 4 && rows_smem_elems(nsmax, 2 * PB) * esz <= lim) return 2 * PB;
+    return rows_smem_elems(nsmax, PB) * esz <= lim ? PB : 0;
+}
+
+template <typename T, int RB>
+static void launch_rows(int facto, const DevSym &s, const PanelCblk *pcb, const PanelItem *items, int nitems,
+                        int nsmax, int *ticket, int *solved, int *abort_word, T *L, const double *thr,
+                        unsigned long long *npiv, int *err, cudaStream_t st) {
+    const size_t smem = rows_smem_elems(nsmax, RB) * sizeof(T);
+    int occ = 0;
+    if (facto == FACTO_POTRF)
+        cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ, panel_rows_kernel<T, FACTO_POTRF, RB>, PT, smem);
+    else
+        cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ, panel_rows_kernel<T, FACTO_SYTRF, RB>, PT, smem);
+    const int grid = std::min(nitems, std::max(occ, 1) * g_sms);
+    if (facto == FACTO_POTRF)
+        panel_rows_kernel<T, FACTO_POTRF, RB><<<grid, PT, smem, st>>>(s, pcb, items, nitems, ticket, solved,
+                                                                     abort_word, L, thr, npiv, err);
+    else
+        panel_rows_kernel<T, FACTO_SYTRF, RB><<<grid, PT, smem, st>>>(s, pcb, items, nitems, ticket, solved,
+                                                                     abort_word, L, thr, npiv, err);
+}
 
 template <typename T>
 void launch_panel_rows(int facto, const DevSym &s, const PanelCblk *pcb, const PanelItem *items, int nitems,
-                       int nsmax, int *ticket, int *solved, int *abort_word, T *L, const double *thr,
+                       int nsmax, int rb, int *ticket, int *solved, int *abort_word, T *L, const double *thr,
                        unsigned long long *npiv, int *err, cudaStream_t st) {
     if (nitems <= 0) return;
-    const size_t smem = rows_smem_elems(nsmax) * sizeof(T);
-    int occ = 0;
-    if (facto == FACTO_POTRF)
-        cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ, panel_rows_kernel<T, FACTO_POTRF>, PT, smem);
-    else
-        cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ, panel_rows_kernel<T, FACTO_SYTRF>, PT, smem);
-    const int grid = std::min(nitems, std::max(occ, 1) * g_sms);
-    if (facto == FACTO_POTRF)
-        panel_rows_kernel<T, FACTO_POTRF><<<grid, PT, smem, st>>>(s, pcb, items, nitems, ticket, solved, abort_word, L,
-                                                                 thr, npiv, err);
-    else
-        panel_rows_kernel<T, FACTO_SYTRF><<<grid, PT, smem, st>>>(s, pcb, items, nitems, ticket, solved, abort_word, L,
-                                                                 thr, npiv, err);
+    if constexpr (sizeof(T) == 4) {
+        if (rb == 2 * PB) {
+            launch_rows<T, 2 * PB>(facto, s, pcb, items, nitems, nsmax, ticket, solved, abort_word, L, thr, npiv, err,
+                                   st);
+            return;
+        }
+    }
+    launch_rows<T, PB>(facto, s, pcb, items, nitems, nsmax, ticket, solved, abort_word, L, thr, npiv, err, st);
 }
 
-template void launch_panel_rows<double>(int, const DevSym &, const PanelCblk *, const PanelItem *, int, int, int *,
+template void launch_panel_rows<double>(int, const DevSym &, const PanelCblk *, const PanelItem *, int, int, int, int *,
                                         int *, int *, double *, const double *, unsigned long long *, int *,
                                         cudaStream_t);
-template void launch_panel_rows<float>(int, const DevSym &, const PanelCblk *, const PanelItem *, int, int, int *,
+template void launch_panel_rows<float>(int, const DevSym &, const PanelCblk *, const PanelItem *, int, int, int, int *,
                                        int *, int *, float *, const double *, unsigned long long *, int *,
                                        cudaStream_t);
 

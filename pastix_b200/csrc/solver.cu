@@ -104,7 +104,7 @@ struct b200_solver_s {
     std::vector<int> lvl_dsm0, lvl_dsm1;  // cblks of <= 32 columns (one warp each)
     // wide POTRF / LDL^T cblks: one panel launch per level over their 64 x 64 tiles
     std::vector<int> lvl_pi0, lvl_pi1;  // items of each level's launch
-    std::vector<int> lvl_prows;         // 1: row-block form (64 rows resident), 0: 64 x 64 tile items
+    std::vector<int> lvl_prows;         // row-block form: rows of the blocks below the diagonal (0: tile items)
     std::vector<int> lvl_pns;           // most 64-column steps of a cblk of the level
     bool panel_steps_only = false;      // environment B200_PANEL_TILES=1: always the tile-item form
     PanelCblk *d_pcb = nullptr;
@@ -335,15 +335,19 @@ int build_schedule(b200_solver_t *s) {
                 s->flops_kind[4] += nc * nc * nc / 3.0 + m * nc * nc;
             }
             s->lvl_pns[l] = nsmax;
-            s->lvl_prows[l] = !s->panel_steps_only && panel_rows_fit(nsmax, s->esz);
-            if (s->lvl_prows[l]) {
-                // row blocks: the diagonal blocks' first (by row block, then cblk), then the rest
+            const int rb = s->panel_steps_only ? 0 : panel_rows_block(nsmax, s->esz);
+            s->lvl_prows[l] = rb;
+            if (rb) {
+                // row blocks: the diagonal blocks' first (by row block, then cblk), then the
+                // rb-row blocks below them
                 for (int b = 0; b < nsmax; b++)
                     for (int p = p0; p < (int)pcbs.size(); p++)
                         if (b < pcbs[p].ns) pitems.push_back({p, 0, b});
                 for (int b = 0; b < nrbmax; b++)
-                    for (int p = p0; p < (int)pcbs.size(); p++)
-                        if (pcbs[p].ns + b < pcbs[p].nrb) pitems.push_back({p, 0, pcbs[p].ns + b});
+                    for (int p = p0; p < (int)pcbs.size(); p++) {
+                        const int k = pcbs[p].k, nbelow = (s->stride[k] - s->ncols[k] + rb - 1) / rb;
+                        if (b < nbelow) pitems.push_back({p, 0, pcbs[p].ns + b});
+                    }
             } else {
                 for (int j = 0; j < nsmax; j++)
                     for (int d = 0; d < nrbmax - j; d++)
@@ -663,8 +667,8 @@ int enqueue_numfact(b200_solver_t *s, cudaStream_t st, Trace *tr = nullptr) {
             int *abort_word = updated + s->n_prb;
             if (s->lvl_prows[l])
                 launch_panel_rows<T>(s->facto, s->ds, s->d_pcb, s->d_pitem + s->lvl_pi0[l],
-                                     s->lvl_pi1[l] - s->lvl_pi0[l], s->lvl_pns[l], tickets + l, solved, abort_word, L,
-                                     s->d_thr, s->d_npiv, s->d_err, st);
+                                     s->lvl_pi1[l] - s->lvl_pi0[l], s->lvl_pns[l], s->lvl_prows[l], tickets + l,
+                                     solved, abort_word, L, s->d_thr, s->d_npiv, s->d_err, st);
             else
                 launch_panel<T>(s->facto, s->ds, s->d_pcb, s->d_pitem + s->lvl_pi0[l], s->lvl_pi1[l] - s->lvl_pi0[l],
                                 tickets + l, solved, updated, abort_word, L, s->d_thr, s->d_npiv, s->d_err, st);
@@ -1405,6 +1409,8 @@ int b200_numfact(b200_solver_t *s, double epsilon_magn_ctrl, int64_t *nbpivots) 
         cudaError_t ec = cudaStreamEndCapture(s->st, &g);
         if (rc) return rc;
         CU(ec);
+        // B200_GRAPH_DOT=<file>: the captured graph in Graphviz form (debugging aid)
+        if (const char *dot = getenv("B200_GRAPH_DOT")) cudaGraphDebugDotPrint(g, dot, 0);
         CU(cudaGraphInstantiate(&s->fact_graph, g, 0));
         cudaGraphDestroy(g);
     }
