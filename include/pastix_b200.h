@@ -110,12 +110,12 @@ int b200_numfact_trace( b200_solver_t *solver, double epsilon_magn_ctrl, double 
  * with x. */
 int b200_solve( b200_solver_t *solver, int64_t nrhs, double *b, int64_t ldb );
 
-/* Per-kernel timing of the triangular sweeps of one solve of nrhs zero
- * right-hand sides (in the permuted basis, no permutation): ms[1] diagonal-block
- * products, ms[2] off-diagonal tiles, ms[3] the cblks of at most 32 columns
- * (both parts in one kernel; ms[0] unused), with CUDA events around every launch;
- * bytes[4] (may be NULL) the algorithmic traffic of each class (factor entries
- * read once per sweep, vectors read and written). */
+/* Timing of the triangular sweeps of one solve of nrhs zero right-hand sides (in
+ * the permuted basis, no permutation): ms[1] the forward sweep, ms[2] the
+ * backward sweep (one dataflow launch each), ms[3] the D scaling of LDL^T
+ * (ms[0] unused), with CUDA events around every launch; bytes[4] (may be NULL)
+ * the algorithmic traffic of each sweep (factor entries read once, vectors read
+ * and written once, in the factor's precision). */
 int b200_solve_trace( b200_solver_t *solver, int64_t nrhs, double *ms, double *bytes );
 
 /* Per-launch device times of the last b200_numfact_trace / b200_solve_trace:

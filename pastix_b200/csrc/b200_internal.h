@@ -74,6 +74,17 @@ struct SolveTile {
     int col0;  // first column of the cblk
 };
 
+// Item of a dataflow solve sweep (one launch per sweep): FI_LEAF up to 16 cblks
+// of at most 32 columns of one level (k = first position in the leaf list, n their
+// number); FI_DIAG output rows [r0, r0 + 64) x K chunk [n, n + 64) of the
+// diagonal-block product of cblk k; FI_OFF panel rows [r0, r0 + 64) x columns
+// [n, n + 64) of cblk k.  flist[f0 .. f0 + nf) are the distinct cblks facing the
+// item's off-diagonal rows.
+enum : int { FI_LEAF = 0, FI_DIAG = 1, FI_OFF = 2 };
+struct FlowItem {
+    int type, k, r0, n, f0, nf;
+};
+
 // Wide cblk of a panel launch (POTRF / LDL^T cblks wider than the one-CTA diagonal
 // kernel): ns steps of 64 columns, nrb row blocks of 64 rows (the first ns cover the
 // diagonal block, the others the rows below it), flag0 its first slot in the

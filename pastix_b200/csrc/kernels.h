@@ -94,6 +94,15 @@ void launch_solve_diag_inv(const DevSym &s, const SolveTile *tasks, int ntasks, 
 template <typename T, typename V>
 void launch_solve_scale_diag(const DevSym &s, const int *cblks, int ncblk, const T *L, V *x, int64_t ldx, int nrhs,
                              cudaStream_t st);
+// one sweep as a dataflow launch (solve_kernels.cu): items in order from *ticket;
+// forward: need[f] contributions complete x_f (cnt_a), nprev[k] diagonal items
+// complete aux_k (cnt_b); backward: need[f] items finish x_f (cnt_a), nprev[k]
+// off-diagonal items complete aux_k (cnt_b); counters zeroed before the launch
+template <typename T, typename V>
+void launch_solve_flow(const DevSym &s, const FlowItem *items, int nitems, const int *leaf, const int *flist,
+                       const int *need, const int *nprev, const T *P, const T *W, const int64_t *woff, V *x, V *aux,
+                       int64_t ldx, int nrhs, int backward, int *ticket, int *cnt_a, int *cnt_b, int *abort_word,
+                       int *err, cudaStream_t st);
 // dst = (D) src on an n x nrhs block
 template <typename S, typename D>
 void launch_convert(int n, int nrhs, const S *src, int64_t lds, D *dst, int64_t ldd, cudaStream_t st);

@@ -478,6 +478,359 @@ template void launch_solve_tiles<double, double>(const DevSym &, const SolveTile
 template void launch_solve_tiles<float, float>(const DevSym &, const SolveTile *, int, const float *, const float *,
                                                float *, int64_t, int, int, cudaStream_t);
 
+// ---------------------------------------------------------------- dataflow sweeps
+//
+// One sweep in one launch: the products above as items taken in a fixed order
+// (level by level; the forward sweep bottom-up, the backward sweep top-down) from
+// an atomic ticket by persistent CTAs, each item waiting only for the inputs it
+// reads instead of for the whole previous level (solve_cblk_ztrsmsp_forward /
+// _backward, kernels/solve_ztrsmsp.c, scheduled by the cblks' contributions as
+// PaStiX's dynamic solve does).  Counters in global memory, per cblk:
+//   forward : cnt_a[f] items that have subtracted into x_f (complete at need[f]);
+//             cnt_b[k] diagonal items of k done (aux_k complete at ndiag[k]);
+//   backward: cnt_a[f] items that have written x_f (final at need[f]);
+//             cnt_b[k] off-diagonal items of k done (aux_k complete at noff[k]).
+// Items:
+//   FI_LEAF up to 16 cblks of <= 32 columns of one level, a warp at a time (the
+//           leaf products above); forward: raises cnt_a of the facing cblks in its
+//           list; backward: waits for them, then raises cnt_a of its own cblks;
+//   FI_DIAG output rows [r0, r0 + 64), K chunk [c0, c0 + 64) of W_k x_k into aux_k
+//           (forward) / W_k^T aux_k into x_k (backward), both zeroed before the sweep;
+//   FI_OFF  panel rows [r0, r0 + 64), columns [c0, c0 + 64) of cblk k: forward
+//           x[rows] -= P aux_k, raising the facing cblks' cnt_a; backward
+//           aux_k -= P^T x[rows] after the facing cblks are final.
+// Partial products meet through atomics, as in the level-synchronous tiles.
+// Values other items write are read through L2 (ld.cg): an L1 line could hold a
+// neighbouring cblk's entries from before they were final.  Every wait is bounded;
+// on expiry the CTA sets bit 4 of err and an abort word that ends the others'
+// waits.
+constexpr int FLOW_THREADS = 128;
+
+namespace {
+
+constexpr long long FLOW_WAIT_CYCLES = 1000000000LL;  // about 0.5 s at the maximum SM clock
+
+__device__ __forceinline__ int flow_ld_acquire(const int *p) {
+    int v;
+    asm volatile("ld.acquire.gpu.global.b32 %0, [%1];\n" : "=r"(v) : "l"(p) : "memory");
+    return v;
+}
+
+__device__ bool flow_wait(const int *c, int target, const int *abort_word) {
+    const long long t0 = clock64();
+    for (int it = 0;; it++) {
+        if (flow_ld_acquire(c) >= target) return true;
+        if ((it & 15) == 15) {
+            if (flow_ld_acquire(abort_word)) return false;
+            if (clock64() - t0 > FLOW_WAIT_CYCLES) return false;
+        }
+        __nanosleep(64);
+    }
+}
+
+// x tile through L2: xs[i * XP + j] = xv[row(i)][q0 + j], zeros outside
+template <typename V, int NT>
+__device__ __forceinline__ void stage_x_cg(V *xs, const V *xv, const int *rowmap, int ni, int64_t ldx, int q0, int R) {
+    constexpr int XP = XPitch<V>::P;
+    stage_n<STT * SRHS / NT, V>(
+        [&](int u) {
+            const int idx = threadIdx.x + NT * u, i = idx % STT, j = idx / STT;
+            return (i < ni && j < R) ? __ldcg(xv + (rowmap ? rowmap[i] : i) + (size_t)(q0 + j) * ldx) : (V)0;
+        },
+        [&](int u, V v) {
+            const int idx = threadIdx.x + NT * u;
+            xs[(idx % STT) * XP + idx / STT] = v;
+        });
+}
+
+}  // namespace
+
+template <typename T, typename V>
+struct FlowSmem {
+    static constexpr int TILE = STT * SM_FWD * (int)sizeof(T) + STT * XPitch<V>::P * (int)sizeof(V);
+    static constexpr int LEAF = 2 * 4 * 32 * (LEAF_R + 1) * (int)sizeof(V);
+    static constexpr int BYTES = TILE > LEAF ? TILE : LEAF;
+};
+
+template <typename T, typename V, int BWD>
+__global__ void __launch_bounds__(FLOW_THREADS) solve_flow_kernel(DevSym s, const FlowItem *__restrict__ items,
+                                                                  int nitems, const int *__restrict__ leaf,
+                                                                  const int *__restrict__ flist,
+                                                                  const int *__restrict__ need,
+                                                                  const int *__restrict__ nprev, const T *P,
+                                                                  const T *W, const int64_t *__restrict__ woff, V *x,
+                                                                  V *aux, int64_t ldx, int nrhs, int *ticket,
+                                                                  int *cnt_a, int *cnt_b, int *abort_word, int *err) {
+    extern __shared__ __align__(16) unsigned char fl_smem[];
+    __shared__ int rmap[STT];
+    __shared__ int s_item, s_ok;
+    const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
+    const int g = lane >> 2, tg = lane & 3;
+    const int o0w = warp * 16;
+    bool aborted = false;
+    for (;;) {
+        if (tid == 0) {
+            s_item = atomicAdd(ticket, 1);
+            s_ok = 1;
+        }
+        __syncthreads();
+        const int t = s_item;
+        if (t >= nitems) break;
+        const FlowItem it = items[t];
+        // ------------------------------------------------------------ inputs complete
+        if (tid == 0) {
+            if (it.type == FI_LEAF) {
+                if (!BWD) {
+                    for (int i = 0; i < it.n && s_ok; i++) {
+                        const int kk = leaf[it.k + i];
+                        if (!flow_wait(cnt_a + kk, need[kk], abort_word)) s_ok = 0;
+                    }
+                } else {
+                    for (int i = 0; i < it.nf && s_ok; i++) {
+                        const int f = flist[it.f0 + i];
+                        if (!flow_wait(cnt_a + f, need[f], abort_word)) s_ok = 0;
+                    }
+                }
+            } else if (it.type == FI_DIAG) {
+                if (!flow_wait(BWD ? cnt_b + it.k : cnt_a + it.k, BWD ? nprev[it.k] : need[it.k], abort_word)) s_ok = 0;
+            } else {
+                if (!BWD) {
+                    if (!flow_wait(cnt_b + it.k, nprev[it.k], abort_word)) s_ok = 0;
+                } else {
+                    for (int i = 0; i < it.nf && s_ok; i++) {
+                        const int f = flist[it.f0 + i];
+                        if (!flow_wait(cnt_a + f, need[f], abort_word)) s_ok = 0;
+                    }
+                }
+            }
+        }
+        __syncthreads();
+        if (!s_ok) {
+            aborted = true;
+            break;
+        }
+        if (it.type == FI_LEAF) {
+            // ------------------------------------------------------------ leaf cblks
+            V (*ys)[LEAF_R + 1] = reinterpret_cast<V (*)[LEAF_R + 1]>(fl_smem) + warp * 32;
+            V (*xr)[LEAF_R + 1] = reinterpret_cast<V (*)[LEAF_R + 1]>(fl_smem) + 4 * 32 + warp * 32;
+            for (int wi = warp; wi < it.n; wi += 4) {
+                const int k = leaf[it.k + wi];
+                const int n = s.ncols[k], ld = s.ld[k], stride = s.stride[k], f0 = s.fcol[k];
+                const T *Pk = P + s.off[k];
+                const T *Wk = W + woff[k];
+                for (int q0 = 0; q0 < nrhs; q0 += LEAF_R) {
+                    const int R = min(LEAF_R, nrhs - q0);
+                    if (!BWD) {
+#pragma unroll
+                        for (int j = 0; j < LEAF_R; j++)
+                            ys[lane][j] = (lane < n && j < R) ? __ldcg(x + f0 + lane + (size_t)(q0 + j) * ldx) : (V)0;
+                        __syncwarp();
+                        V y[LEAF_R];
+#pragma unroll
+                        for (int j = 0; j < LEAF_R; j++) y[j] = 0;
+                        if (lane < n) {
+                            for (int c = 0; c <= lane; c++) {
+                                const V wv = (V)Wk[lane + (size_t)c * n];
+#pragma unroll
+                                for (int j = 0; j < LEAF_R; j++) y[j] += wv * ys[c][j];
+                            }
+                        }
+                        __syncwarp();
+                        if (lane < n) {
+#pragma unroll
+                            for (int j = 0; j < LEAF_R; j++) {
+                                ys[lane][j] = y[j];
+                                if (j < R) aux[f0 + lane + (size_t)(q0 + j) * ldx] = y[j];
+                            }
+                        }
+                        __syncwarp();
+                        for (int r = n + lane; r < stride; r += 32) {
+                            const int gg = panel_row_to_global(s, k, r);
+                            V acc[LEAF_R];
+#pragma unroll
+                            for (int j = 0; j < LEAF_R; j++) acc[j] = 0;
+                            for (int c = 0; c < n; c++) {
+                                const V pv = (V)Pk[r + (size_t)c * ld];
+#pragma unroll
+                                for (int j = 0; j < LEAF_R; j++) acc[j] += pv * ys[c][j];
+                            }
+#pragma unroll
+                            for (int j = 0; j < LEAF_R; j++)
+                                if (j < R) atomicAdd(&x[gg + (size_t)(q0 + j) * ldx], -acc[j]);
+                        }
+                        __syncwarp();
+                    } else {
+                        V tt[LEAF_R];
+#pragma unroll
+                        for (int j = 0; j < LEAF_R; j++)
+                            tt[j] = (lane < n && j < R) ? __ldcg(aux + f0 + lane + (size_t)(q0 + j) * ldx) : (V)0;
+                        for (int r0 = n; r0 < stride; r0 += 32) {
+                            const int nr = min(32, stride - r0);
+                            const int myg = (lane < nr) ? panel_row_to_global(s, k, r0 + lane) : 0;
+                            for (int idx = lane; idx < 32 * LEAF_R; idx += 32) {
+                                const int i = idx / LEAF_R, j = idx % LEAF_R;
+                                const int gi = __shfl_sync(0xffffffffu, myg, i);
+                                xr[i][j] = (i < nr && j < R) ? __ldcg(x + gi + (size_t)(q0 + j) * ldx) : (V)0;
+                            }
+                            __syncwarp();
+                            if (lane < n) {
+                                for (int i = 0; i < nr; i++) {
+                                    const V pv = (V)Pk[r0 + i + (size_t)lane * ld];
+#pragma unroll
+                                    for (int j = 0; j < LEAF_R; j++) tt[j] -= pv * xr[i][j];
+                                }
+                            }
+                            __syncwarp();
+                        }
+                        if (lane < n) {
+#pragma unroll
+                            for (int j = 0; j < LEAF_R; j++) ys[lane][j] = tt[j];
+                        }
+                        __syncwarp();
+                        if (lane < n) {
+                            V o[LEAF_R];
+#pragma unroll
+                            for (int j = 0; j < LEAF_R; j++) o[j] = 0;
+                            for (int r = lane; r < n; r++) {
+                                const V wv = (V)Wk[r + (size_t)lane * n];
+#pragma unroll
+                                for (int j = 0; j < LEAF_R; j++) o[j] += wv * ys[r][j];
+                            }
+#pragma unroll
+                            for (int j = 0; j < LEAF_R; j++)
+                                if (j < R) x[f0 + lane + (size_t)(q0 + j) * ldx] = o[j];
+                        }
+                        __syncwarp();
+                    }
+                }
+            }
+        } else {
+            // ------------------------------------------------------------ one 64 x 64 tile
+            T *ms = reinterpret_cast<T *>(fl_smem);
+            V *xs = reinterpret_cast<V *>(fl_smem + STT * SM_FWD * sizeof(T));
+            const int k = it.k, n = s.ncols[k], c0 = it.n;
+            int nout, nk;
+            const V *xsrc;
+            const int *xmap = nullptr;
+            if (it.type == FI_DIAG) {
+                const T *Wk = W + woff[k];
+                nout = min(STT, n - it.r0);
+                nk = min(STT, n - c0);
+                // forward W[o][kk] (row form); backward W[kk][o] (W^T, column form)
+                if (!BWD) stage_tile<T, SM_FWD>(ms, Wk, n, it.r0, c0, n, n);
+                else stage_tile<T, SM_BWD>(ms, Wk, n, c0, it.r0, n, n);
+                xsrc = (BWD ? aux : x) + s.fcol[k] + c0;
+            } else {
+                const int rows = min(STT, s.stride[k] - it.r0), cols = min(STT, n - c0);
+                if (tid < STT) rmap[tid] = (tid < rows) ? panel_row_to_global(s, k, it.r0 + tid) : 0;
+                if (!BWD) stage_tile<T, SM_FWD>(ms, P + s.off[k], s.ld[k], it.r0, c0, s.stride[k], n);
+                else stage_tile<T, SM_BWD>(ms, P + s.off[k], s.ld[k], it.r0, c0, s.stride[k], n);
+                nout = BWD ? cols : rows;
+                nk = BWD ? rows : cols;
+                if (!BWD) xsrc = aux + s.fcol[k] + c0;
+                else { xsrc = x; xmap = rmap; }
+                __syncthreads();
+            }
+            cp_commit();
+            for (int q0 = 0; q0 < nrhs; q0 += SRHS) {
+                const int R = min(SRHS, nrhs - q0), ntn = (R + 7) >> 3;
+                if (q0 > 0) __syncthreads();
+                stage_x_cg<V, FLOW_THREADS>(xs, xsrc, xmap, nk, ldx, q0, R);
+                cp_wait<0>();
+                __syncthreads();
+                if (o0w < nout) {
+                    V acc[4][4] = {};
+                    const bool row = !BWD;  // forward: outputs are tile rows; backward: tile columns
+                    if (row) tile_mma<T, SM_FWD, 1>(acc, ms, xs, o0w, ntn);
+                    else tile_mma<T, SM_BWD, 0>(acc, ms, xs, o0w, ntn);
+                    // DIAG: + into aux_k (forward) / x_k (backward); OFF: - into x[rows] / aux_k
+                    const V sg = it.type == FI_DIAG ? (V)1 : (V)-1;
+                    V *dst;
+                    if (it.type == FI_DIAG) dst = (BWD ? x : aux) + s.fcol[k] + it.r0;
+                    else dst = BWD ? aux + s.fcol[k] + c0 : x;
+#pragma unroll
+                    for (int nt = 0; nt < 4; nt++) {
+                        if (nt >= ntn) continue;
+#pragma unroll
+                        for (int e = 0; e < 4; e++) {
+                            const int o = o0w + g + (e >> 1) * 8;
+                            const int j = nt * 8 + 2 * tg + (e & 1);
+                            if (o < nout && j < R) {
+                                const int row_o = (it.type == FI_OFF && !BWD) ? rmap[o] : o;
+                                atomicAdd(dst + row_o + (size_t)(q0 + j) * ldx, sg * acc[nt][e]);
+                            }
+                        }
+                    }
+                }
+            }
+        }
+        // ------------------------------------------------------------ announce
+        __syncthreads();
+        if (tid == 0) {
+            __threadfence();
+            if (it.type == FI_LEAF) {
+                if (!BWD)
+                    for (int i = 0; i < it.nf; i++) atomicAdd(cnt_a + flist[it.f0 + i], 1);
+                else
+                    for (int i = 0; i < it.n; i++) atomicAdd(cnt_a + leaf[it.k + i], 1);
+            } else if (it.type == FI_DIAG) {
+                atomicAdd(BWD ? cnt_a + it.k : cnt_b + it.k, 1);
+            } else {
+                if (!BWD)
+                    for (int i = 0; i < it.nf; i++) atomicAdd(cnt_a + flist[it.f0 + i], 1);
+                else
+                    atomicAdd(cnt_b + it.k, 1);
+            }
+        }
+    }
+    if (aborted && tid == 0) {
+        atomicOr(err, 16);
+        atomicExch(abort_word, 1);
+    }
+}
+
+template <typename T, typename V>
+void launch_solve_flow(const DevSym &s, const FlowItem *items, int nitems, const int *leaf, const int *flist,
+                       const int *need, const int *nprev, const T *P, const T *W, const int64_t *woff, V *x, V *aux,
+                       int64_t ldx, int nrhs, int backward, int *ticket, int *cnt_a, int *cnt_b, int *abort_word,
+                       int *err, cudaStream_t st) {
+    if (nitems <= 0) return;
+    static int ctas[2] = {0, 0};
+    const int bi = backward ? 1 : 0;
+    const int smem = FlowSmem<T, V>::BYTES;
+    if (!ctas[bi]) {
+        int dev = 0, sms = 0, occ = 0;
+        cudaGetDevice(&dev);
+        cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
+        if (backward) {
+            cudaFuncSetAttribute(solve_flow_kernel<T, V, 1>, cudaFuncAttributeMaxDynamicSharedMemorySize, smem);
+            cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ, solve_flow_kernel<T, V, 1>, FLOW_THREADS, smem);
+        } else {
+            cudaFuncSetAttribute(solve_flow_kernel<T, V, 0>, cudaFuncAttributeMaxDynamicSharedMemorySize, smem);
+            cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ, solve_flow_kernel<T, V, 0>, FLOW_THREADS, smem);
+        }
+        ctas[bi] = std::max(occ, 1) * std::max(sms, 1);
+    }
+    const int grid = std::min(nitems, ctas[bi]);
+    if (backward)
+        solve_flow_kernel<T, V, 1><<<grid, FLOW_THREADS, smem, st>>>(s, items, nitems, leaf, flist, need, nprev, P, W,
+                                                                    woff, x, aux, ldx, nrhs, ticket, cnt_a, cnt_b,
+                                                                    abort_word, err);
+    else
+        solve_flow_kernel<T, V, 0><<<grid, FLOW_THREADS, smem, st>>>(s, items, nitems, leaf, flist, need, nprev, P, W,
+                                                                    woff, x, aux, ldx, nrhs, ticket, cnt_a, cnt_b,
+                                                                    abort_word, err);
+}
+
+template void launch_solve_flow<double, double>(const DevSym &, const FlowItem *, int, const int *, const int *,
+                                                const int *, const int *, const double *, const double *,
+                                                const int64_t *, double *, double *, int64_t, int, int, int *, int *,
+                                                int *, int *, int *, cudaStream_t);
+template void launch_solve_flow<float, float>(const DevSym &, const FlowItem *, int, const int *, const int *,
+                                              const int *, const int *, const float *, const float *, const int64_t *,
+                                              float *, float *, int64_t, int, int, int *, int *, int *, int *, int *,
+                                              cudaStream_t);
+
 }  // namespace b200
 
 // ====================================================================== diagonal-block inverses

@@ -102,6 +102,17 @@ struct b200_solver_s {
     int n_inv_small = 0, n_inv_big = 0;
     std::vector<int> lvl_ds0, lvl_ds1;
     std::vector<int> lvl_dsm0, lvl_dsm1;  // cblks of <= 32 columns (one warp each)
+    // dataflow solve sweeps: items of the forward and backward launches, the facing
+    // lists, and per cblk the counts that complete x (need_f / need_b) and aux
+    // (nprev_f: diagonal items, nprev_b: off-diagonal items)
+    // the levels from flow_level up take the dataflow sweeps (few cblks per level:
+    // launch-bound level by level); the levels below, the level-synchronous kernels
+    int flow_level = 0;
+    FlowItem *d_fitem_f = nullptr, *d_fitem_b = nullptr;
+    int n_fitem_f = 0, n_fitem_b = 0;
+    int *d_flist = nullptr, *d_need_f = nullptr, *d_need_b = nullptr, *d_nprev_f = nullptr, *d_nprev_b = nullptr;
+    // [ticket f, ticket b, abort, pad][cnt_a f][cnt_b f][cnt_a b][cnt_b b], zeroed per solve
+    int *d_sflags = nullptr;
     // wide POTRF / LDL^T cblks: one panel launch per level over their 64 x 64 tiles
     std::vector<int> lvl_pi0, lvl_pi1;  // items of each level's launch
     std::vector<int> lvl_prows;         // row-block form: rows of the blocks below the diagonal (0: tile items)
@@ -493,6 +504,89 @@ int build_schedule(b200_solver_t *s) {
     RET(s->dupload(&s->d_dtask, dtask));
     RET(s->dupload(&s->d_dtaskb, dtaskb));
     RET(s->dupload(&s->d_leaf, leaf));
+    {
+        // dataflow sweep items, level by level (forward bottom-up, backward top-down)
+        std::vector<FlowItem> fwd, bwd;
+        std::vector<int> flist, need_f(N, 0), need_b(N, 0), nprev_f(N, 0), nprev_b(N, 0);
+        std::vector<int> mark(N, -1);
+        int stamp = 0;
+        auto facing = [&](int k, int r0, int r1, FlowItem &it) {  // distinct cblks facing panel rows [r0, r1)
+            for (int b = s->fblok[k] + 1; b < s->fblok[k + 1]; b++) {
+                const int b0 = s->rowoff[b], b1 = b0 + s->lrow[b] - s->frow[b] + 1;
+                if (b1 <= r0 || b0 >= r1) continue;
+                const int f = s->fcblk[b];
+                if (mark[f] == stamp) continue;
+                mark[f] = stamp;
+                flist.push_back(f);
+                it.nf++;
+            }
+        };
+        std::vector<std::vector<FlowItem>> lvl_bwd(nlev);
+        // first level with fewer than flow_min cblks (environment B200_FLOW_MIN)
+        int flow_min = 8;
+        if (const char *e = getenv("B200_FLOW_MIN")) flow_min = atoi(e);
+        s->flow_level = nlev;
+        for (int l = 0; l < nlev; l++)
+            if (s->levels[l].c1 - s->levels[l].c0 < flow_min) {
+                s->flow_level = l;
+                break;
+            }
+        for (int l = s->flow_level; l < nlev; l++) {
+            const Level &L = s->levels[l];
+            for (int p = s->lvl_lf0[l]; p < s->lvl_lf1[l]; p += 16) {
+                FlowItem it{FI_LEAF, p, 0, std::min(16, s->lvl_lf1[l] - p), (int)flist.size(), 0};
+                stamp++;
+                for (int q = 0; q < it.n; q++) {
+                    const int k = leaf[p + q];
+                    facing(k, s->ncols[k], s->stride[k], it);
+                    need_b[k] = 1;
+                }
+                for (int q = 0; q < it.nf; q++) need_f[flist[it.f0 + q]]++;
+                fwd.push_back(it);
+                lvl_bwd[l].push_back(it);
+            }
+            for (int i = L.c0; i < L.c1; i++) {
+                const int k = lvl_cblk[i], nc = s->ncols[k];
+                if (nc <= 32) continue;
+                // W_k lower triangular: forward chunks c0 <= r0, backward (W_k^T) c0 >= r0
+                std::vector<FlowItem> diagf, diagb, off;
+                for (int r0 = 0; r0 < nc; r0 += 64)
+                    for (int c0 = 0; c0 < nc; c0 += 64) {
+                        if (c0 <= r0) diagf.push_back({FI_DIAG, k, r0, c0, 0, 0});
+                        if (c0 >= r0) diagb.push_back({FI_DIAG, k, r0, c0, 0, 0});
+                    }
+                for (int r0 = nc; r0 < s->stride[k]; r0 += 64) {
+                    FlowItem it{FI_OFF, k, r0, 0, (int)flist.size(), 0};
+                    stamp++;
+                    facing(k, r0, std::min(r0 + 64, s->stride[k]), it);
+                    for (int c0 = 0; c0 < nc; c0 += 64) {
+                        it.n = c0;
+                        for (int q = 0; q < it.nf; q++) need_f[flist[it.f0 + q]]++;
+                        off.push_back(it);
+                    }
+                }
+                nprev_f[k] = (int)diagf.size();
+                nprev_b[k] = (int)off.size();
+                need_b[k] = (int)diagb.size();
+                fwd.insert(fwd.end(), diagf.begin(), diagf.end());
+                fwd.insert(fwd.end(), off.begin(), off.end());
+                lvl_bwd[l].insert(lvl_bwd[l].end(), off.begin(), off.end());
+                lvl_bwd[l].insert(lvl_bwd[l].end(), diagb.begin(), diagb.end());
+            }
+        }
+        for (int l = nlev - 1; l >= s->flow_level; l--) bwd.insert(bwd.end(), lvl_bwd[l].begin(), lvl_bwd[l].end());
+        s->n_fitem_f = (int)fwd.size();
+        s->n_fitem_b = (int)bwd.size();
+        if (flist.empty()) flist.push_back(0);
+        RET(s->dupload(&s->d_fitem_f, fwd));
+        RET(s->dupload(&s->d_fitem_b, bwd));
+        RET(s->dupload(&s->d_flist, flist));
+        RET(s->dupload(&s->d_need_f, need_f));
+        RET(s->dupload(&s->d_need_b, need_b));
+        RET(s->dupload(&s->d_nprev_f, nprev_f));
+        RET(s->dupload(&s->d_nprev_b, nprev_b));
+        RET(s->dmalloc(&s->d_sflags, (size_t)4 * N + 4));
+    }
     RET(s->dupload(&s->d_diag_list, diag_list));
     {
         std::vector<int> small, big;
@@ -734,48 +828,65 @@ int enqueue_sweeps(b200_solver_t *s, T *x, T *aux, int64_t ldx, int nrhs, cudaSt
     const T *Ub = (s->facto == FACTO_GETRF) ? (const T *)s->dU : L;
     const T *WL = (const T *)s->dWL;
     const T *WB = (s->facto == FACTO_GETRF) ? (const T *)s->dWU : WL;
-    const int nlev = (int)s->levels.size();
-    // the diagonal-block products accumulate their K chunks: zero their outputs
+    const int N = s->cblknbr, nlev = (int)s->levels.size(), fl0 = s->flow_level;
+    int *fl = s->d_sflags, *abort_word = fl + 2;
+    CU(cudaMemsetAsync(fl, 0, ((size_t)4 * N + 4) * sizeof(int), st));
+    // the diagonal products accumulate their K chunks: zero their outputs (aux now, x
+    // before the backward sweep)
     CU(cudaMemset2DAsync(aux, (size_t)ldx * sizeof(T), 0, (size_t)s->n * sizeof(T), nrhs, st));
-    for (int l = 0; l < nlev; l++) {
+    for (int l = 0; l < fl0; l++) {
         const int nlf = s->lvl_lf1[l] - s->lvl_lf0[l];
         if (nlf > 0) {
             if (tr) tr->begin(st);
             launch_solve_leaf<T>(s->ds, s->d_leaf + s->lvl_lf0[l], nlf, L, WL, s->d_woff, x, aux, ldx, nrhs, 0, st);
-            if (tr) tr->end(3, st);
+            if (tr) tr->end(1, st);
             *launches += 1;
         }
         const int nd = s->lvl_dt1[l] - s->lvl_dt0[l];
         if (tr) tr->begin(st);
         launch_solve_diag_inv<T>(s->ds, s->d_dtask + s->lvl_dt0[l], nd, WL, s->d_woff, x, aux, ldx, nrhs, 0, st);
-        if (tr) tr->end(1, st);
         const int ns = s->lvl_st1[l] - s->lvl_st0[l];
-        if (tr) tr->begin(st);
         launch_solve_tiles<T>(s->ds, s->d_stile + s->lvl_st0[l], ns, L, aux, x, ldx, nrhs, 0, st);
-        if (tr) tr->end(2, st);
+        if (tr) tr->end(1, st);
         *launches += (nd > 0) + (ns > 0);
     }
+    if (fl0 < nlev) {
+        if (tr) tr->begin(st);
+        launch_solve_flow<T, T>(s->ds, s->d_fitem_f, s->n_fitem_f, s->d_leaf, s->d_flist, s->d_need_f, s->d_nprev_f,
+                                L, WL, s->d_woff, x, aux, ldx, nrhs, 0, fl, fl + 4, fl + 4 + N, abort_word, s->d_err,
+                                st);
+        if (tr) tr->end(1, st);
+        *launches += 1;
+    }
     if (s->facto == FACTO_SYTRF) {
+        if (tr) tr->begin(st);
         launch_solve_scale_diag<T>(s->ds, s->d_lvl_cblk, s->cblknbr, L, aux, ldx, nrhs, st);
+        if (tr) tr->end(3, st);
         *launches += 1;
     }
     CU(cudaMemset2DAsync(x, (size_t)ldx * sizeof(T), 0, (size_t)s->n * sizeof(T), nrhs, st));
-    for (int l = nlev - 1; l >= 0; l--) {
+    if (fl0 < nlev) {
+        if (tr) tr->begin(st);
+        launch_solve_flow<T, T>(s->ds, s->d_fitem_b, s->n_fitem_b, s->d_leaf, s->d_flist, s->d_need_b, s->d_nprev_b,
+                                Ub, WB, s->d_woff, x, aux, ldx, nrhs, 1, fl + 1, fl + 4 + 2 * N, fl + 4 + 3 * N,
+                                abort_word, s->d_err, st);
+        if (tr) tr->end(2, st);
+        *launches += 1;
+    }
+    for (int l = fl0 - 1; l >= 0; l--) {
         const int nlf = s->lvl_lf1[l] - s->lvl_lf0[l];
         if (nlf > 0) {
             if (tr) tr->begin(st);
             launch_solve_leaf<T>(s->ds, s->d_leaf + s->lvl_lf0[l], nlf, Ub, WB, s->d_woff, x, aux, ldx, nrhs, 1, st);
-            if (tr) tr->end(3, st);
+            if (tr) tr->end(2, st);
             *launches += 1;
         }
         const int ns = s->lvl_st1[l] - s->lvl_st0[l];
         if (tr) tr->begin(st);
         launch_solve_tiles<T>(s->ds, s->d_stile + s->lvl_st0[l], ns, Ub, x, aux, ldx, nrhs, 1, st);
-        if (tr) tr->end(2, st);
         const int nd = s->lvl_db1[l] - s->lvl_db0[l];
-        if (tr) tr->begin(st);
         launch_solve_diag_inv<T>(s->ds, s->d_dtaskb + s->lvl_db0[l], nd, WB, s->d_woff, aux, x, ldx, nrhs, 1, st);
-        if (tr) tr->end(1, st);
+        if (tr) tr->end(2, st);
         *launches += (nd > 0) + (ns > 0);
     }
     CU(cudaGetLastError());
@@ -1471,19 +1582,15 @@ int b200_solve_trace(b200_solver_t *s, int64_t nrhs, double *ms, double *bytes) 
     s->kernel_launches += launches;
     tr.finish(ms);
     if (bytes) {
-        // algorithmic traffic: every factor entry (diagonal blocks: their inverses'
-        // triangles) once per sweep, x_k read and written per sweep, the rows below
-        // read and written per sweep; class 3 holds the cblks of <= 32 columns
+        // algorithmic traffic of each sweep: every factor entry once (diagonal blocks:
+        // their inverses' triangles), x_k and aux_k read or written once, the rows
+        // below read and written once
         for (int c = 0; c < 4; c++) bytes[c] = 0;
         for (int k = 0; k < s->cblknbr; k++) {
-            const double nc = s->ncols[k], m = s->stride[k] - nc, v = (double)nrhs * 8.0;
-            const double dbk = 2.0 * nc * nc * 0.5 * s->esz + 4.0 * nc * v;
-            const double obk = 2.0 * m * nc * s->esz + 4.0 * m * v;
-            if (s->ncols[k] <= 32) bytes[3] += dbk + obk;
-            else {
-                bytes[1] += dbk;
-                bytes[2] += obk;
-            }
+            const double nc = s->ncols[k], m = s->stride[k] - nc, v = (double)nrhs * s->esz;
+            const double per_sweep = (nc * nc * 0.5 + m * nc) * s->esz + 2.0 * nc * v + 2.0 * m * v;
+            bytes[1] += per_sweep;
+            bytes[2] += per_sweep;
         }
     }
     return ERR_SUCCESS;
@@ -1544,6 +1651,18 @@ int b200_solve_device_noalloc(b200_solver_t *s, int64_t nrhs, double *d_b, int64
     return ERR_SUCCESS;
 }
 
+// Bit 4 of the device error word: a dataflow sweep gave up waiting for its inputs
+// (its result is not to be used).  Read after the stream has been synchronized.
+static int sweep_status(b200_solver_t *s) {
+    int err = 0;
+    if (cudaMemcpy(&err, s->d_err, sizeof(int), cudaMemcpyDeviceToHost) != cudaSuccess) return ERR_INTERNAL;
+    if (err & 16) {
+        fprintf(stderr, "pastix_b200: a solve sweep timed out waiting for its inputs\n");
+        return ERR_INTERNAL;
+    }
+    return ERR_SUCCESS;
+}
+
 int b200_solve(b200_solver_t *s, int64_t nrhs, double *b, int64_t ldb) {
     if (!s || !s->factored || nrhs < 0 || ldb < s->n || (!b && nrhs)) return ERR_BADPARAM;
     if (nrhs == 0) return ERR_SUCCESS;
@@ -1561,6 +1680,7 @@ int b200_solve(b200_solver_t *s, int64_t nrhs, double *b, int64_t ldb) {
     if (!rc && cudaMemcpy2DAsync(b, ldb * sizeof(double), db, n * sizeof(double), n * sizeof(double), nrhs,
                                  cudaMemcpyDeviceToHost, s->st) != cudaSuccess) rc = ERR_INTERNAL;
     if (cudaStreamSynchronize(s->st) != cudaSuccess) rc = ERR_INTERNAL;
+    if (!rc) rc = sweep_status(s);
     float ms = 0;
     if (!rc) cudaEventElapsedTime(&ms, s->ev0, s->ev1);
     s->t_solve = ms;
@@ -1577,6 +1697,7 @@ int b200_refine_device(b200_solver_t *s, int64_t nrhs, const double *d_b, int64_
     auto t0 = std::chrono::steady_clock::now();
     int rc = refine_device(s, (int)nrhs, d_b, ldb, d_x, ldx, method, eps, itermax, gmres_im, niter, berr, st);
     if (!rc && cudaStreamSynchronize(st) != cudaSuccess) rc = ERR_INTERNAL;
+    if (!rc) rc = sweep_status(s);
     s->t_refine = std::chrono::duration<double, std::milli>(std::chrono::steady_clock::now() - t0).count();
     return rc;
 }

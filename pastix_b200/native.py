@@ -143,9 +143,9 @@ class Solver:
         ms = np.zeros(4)
         by = np.zeros(4)
         check(lib().b200_solve_trace(self.h, nrhs, _p(ms), _p(by)), "b200_solve_trace")
-        return {"diag": dict(ms=float(ms[1]), bytes=float(by[1])),
-                "offdiag": dict(ms=float(ms[2]), bytes=float(by[2])),
-                "small": dict(ms=float(ms[3]), bytes=float(by[3]))}
+        return {"forward": dict(ms=float(ms[1]), bytes=float(by[1])),
+                "backward": dict(ms=float(ms[2]), bytes=float(by[2])),
+                "scale": dict(ms=float(ms[3]), bytes=float(by[3]))}
 
     def trace_launches(self):
         """(class, ms) of every launch of the last trace, grouped by class."""

@@ -106,6 +106,29 @@ def test_panel_tile_item_form(monkeypatch, facto, make):
     check_fp64_case(facto, make)
 
 
+@pytest.mark.parametrize("flow_min", ["0", "100000"])
+@pytest.mark.parametrize("facto,make", [CASES[1], CASES[2], CASES[-2]])
+def test_solve_sweep_forms(monkeypatch, flow_min, facto, make):
+    """Both forms of the sweeps give the oracle's solution: level by level only
+    (B200_FLOW_MIN=0) and one dataflow launch per sweep for every level."""
+    monkeypatch.setenv("B200_FLOW_MIN", flow_min)
+    A = make()
+    an = Analysis(A, facto)
+    st = an.structure()
+    bc = an.bcsc()
+    s = native.Solver(st, facto, "fp64")
+    s.bcsc_load(bc)
+    s.numfact(0.0)
+    thr = s.stats()["threshold"]
+    orc, L, U, _ = oracle_factor(st, bc, an.facto, thr)
+    xt, b = M.rhs_from_xtrue(A, 20, seed=3)
+    x = s.solve(b)
+    xo = orc.solve(an.facto, L, U, b)
+    assert np.linalg.norm(x - xo) / np.linalg.norm(xo) <= 1e-12
+    assert backward_error(A, x, b).max() <= BERR_FP64
+    s.close()
+
+
 def check_fp64_case(facto, make):
     A = make()
     an = Analysis(A, facto)
