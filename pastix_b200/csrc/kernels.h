@@ -112,8 +112,10 @@ int configure_solve_kernels();
 int configure_inverse_kernels();
 
 // refinement vectors (refine_kernels.cu)
+// xt (n x 16 doubles, may be null): row-major staging of 16 columns of x at a time
 void launch_spmv(int n, int nrhs, const int64_t *colptr, const int *rowtab, const double *vals, const double *x,
-                 int64_t ldx, double *y, int64_t ldy, double alpha, double beta, cudaStream_t st);
+                 int64_t ldx, double *y, int64_t ldy, double alpha, double beta, cudaStream_t st,
+                 double *xt = nullptr);
 // out[r] = sum_i x[i,r] * y[i,r]  (nrhs columns), accumulated in double
 void launch_dots(int n, int nrhs, const double *x, int64_t ldx, const double *y, int64_t ldy, double *out,
                  cudaStream_t st);

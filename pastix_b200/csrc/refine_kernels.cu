@@ -86,11 +86,73 @@ __global__ void scal_cols_kernel(int n, int nrhs, const double *__restrict__ s, 
 
 static inline unsigned nblk(int64_t tot, int bs) { return (unsigned)((tot + bs - 1) / bs); }
 
+// Several right-hand sides: the columns r0 .. r0 + 15 of x first gathered
+// row-major (16 doubles = 128 contiguous bytes per row), so that every matrix entry
+// gathers one line instead of 16 scattered ones; then warp per row, every entry read
+// once and applied to the 16 columns in registers, one butterfly per column.
+constexpr int SPMV_R = 16;
+
+__global__ void gather_rows_kernel(int n, int R, const double *__restrict__ x, int64_t ldx, double *__restrict__ xt) {
+    const int i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= n) return;
+    double v[SPMV_R];
+#pragma unroll
+    for (int r = 0; r < SPMV_R; r++) v[r] = r < R ? x[i + (int64_t)r * ldx] : 0.0;
+    double2 *o = reinterpret_cast<double2 *>(xt + (int64_t)i * SPMV_R);
+#pragma unroll
+    for (int h = 0; h < SPMV_R / 2; h++) o[h] = make_double2(v[2 * h], v[2 * h + 1]);
+}
+
+__global__ void __launch_bounds__(256) spmv_rows_kernel(int n, int R, const int64_t *__restrict__ colptr,
+                                                        const int *__restrict__ rowtab,
+                                                        const double *__restrict__ vals,
+                                                        const double *__restrict__ xt, double *y, int64_t ldy,
+                                                        double alpha, double beta) {
+    const int warp = (blockIdx.x * blockDim.x + threadIdx.x) >> 5;
+    const int lane = threadIdx.x & 31;
+    if (warp >= n) return;
+    const int64_t e0 = colptr[warp], e1 = colptr[warp + 1];
+    double acc[SPMV_R];
+#pragma unroll
+    for (int r = 0; r < SPMV_R; r++) acc[r] = 0.0;
+    for (int64_t e = e0 + lane; e < e1; e += 32) {
+        const double v = vals[e];
+        const double2 *xr = reinterpret_cast<const double2 *>(xt + (int64_t)rowtab[e] * SPMV_R);
+#pragma unroll
+        for (int h = 0; h < SPMV_R / 2; h++) {
+            const double2 q = xr[h];
+            acc[2 * h] += v * q.x;
+            acc[2 * h + 1] += v * q.y;
+        }
+    }
+    double mine = 0.0;
+#pragma unroll
+    for (int r = 0; r < SPMV_R; r++) {
+        double a = acc[r];
+#pragma unroll
+        for (int o = 16; o > 0; o >>= 1) a += __shfl_xor_sync(0xffffffffu, a, o);
+        if (lane == r) mine = a;
+    }
+    if (lane < R) {
+        double *yp = y + warp + (int64_t)lane * ldy;
+        *yp = (beta == 0.0) ? alpha * mine : alpha * mine + beta * *yp;
+    }
+}
+
 void launch_spmv(int n, int nrhs, const int64_t *colptr, const int *rowtab, const double *vals, const double *x,
-                 int64_t ldx, double *y, int64_t ldy, double alpha, double beta, cudaStream_t st) {
+                 int64_t ldx, double *y, int64_t ldy, double alpha, double beta, cudaStream_t st, double *xt) {
     if (n <= 0) return;
-    spmv_kernel<<<nblk((int64_t)n * 32, 256), 256, 0, st>>>(n, nrhs, colptr, rowtab, vals, x, ldx, y, ldy, alpha,
-                                                             beta);
+    if (nrhs > 1 && xt) {
+        for (int r0 = 0; r0 < nrhs; r0 += SPMV_R) {
+            const int R = nrhs - r0 < SPMV_R ? nrhs - r0 : SPMV_R;
+            gather_rows_kernel<<<nblk(n, 256), 256, 0, st>>>(n, R, x + (int64_t)r0 * ldx, ldx, xt);
+            spmv_rows_kernel<<<nblk((int64_t)n * 32, 256), 256, 0, st>>>(n, R, colptr, rowtab, vals, xt,
+                                                                          y + (int64_t)r0 * ldy, ldy, alpha, beta);
+        }
+    } else {
+        spmv_kernel<<<nblk((int64_t)n * 32, 256), 256, 0, st>>>(n, nrhs, colptr, rowtab, vals, x, ldx, y, ldy, alpha,
+                                                                 beta);
+    }
 }
 
 void launch_dots(int n, int nrhs, const double *x, int64_t ldx, const double *y, int64_t ldy, double *out,

@@ -113,6 +113,7 @@ struct b200_solver_s {
     int *d_flist = nullptr, *d_need_f = nullptr, *d_need_b = nullptr, *d_nprev_f = nullptr, *d_nprev_b = nullptr;
     // [ticket f, ticket b, abort, pad][cnt_a f][cnt_b f][cnt_a b][cnt_b b], zeroed per solve
     int *d_sflags = nullptr;
+    double *d_xt = nullptr;  // n x 16 row-major staging of the multi-column SpMV (allocated on first use)
     // wide POTRF / LDL^T cblks: one panel launch per level over their 64 x 64 tiles
     std::vector<int> lvl_pi0, lvl_pi1;  // items of each level's launch
     std::vector<int> lvl_prows;         // row-block form: rows of the blocks below the diagonal (0: tile items)
@@ -934,8 +935,9 @@ struct RefineCtx {
     // A x in the permuted basis with the bcsc
     int spmv(const double *x, double *y, double alpha, double beta) {
         const double *vals = (s->facto == FACTO_GETRF) ? s->d_Uv : s->d_Lv;
-        launch_spmv(n, nrhs, s->d_colptr, s->d_rowtab, vals, x, n, y, n, alpha, beta, st);
-        s->kernel_launches++;
+        if (nrhs > 1 && !s->d_xt) RET(dalloc(&s->d_xt, (size_t)n * 16));
+        launch_spmv(n, nrhs, s->d_colptr, s->d_rowtab, vals, x, n, y, n, alpha, beta, st, s->d_xt);
+        s->kernel_launches += nrhs > 1 ? 2 * ((nrhs + 15) / 16) : 1;
         return ERR_SUCCESS;
     }
     // z <- M^{-1} z with the factor (sweeps only, already permuted)
@@ -1421,6 +1423,7 @@ int b200_solver_destroy(b200_solver_t *s) {
     if (s->d_dest) cudaFree(s->d_dest);
     if (s->d_ws) cudaFree(s->d_ws);
     if (s->d_scal) cudaFree(s->d_scal);
+    if (s->d_xt) cudaFree(s->d_xt);
     if (s->ev0) cudaEventDestroy(s->ev0);
     if (s->ev1) cudaEventDestroy(s->ev1);
     if (s->own_stream && s->st) cudaStreamDestroy(s->st);
@@ -1741,7 +1744,8 @@ int b200_spmv(b200_solver_t *s, int64_t nrhs, double alpha, const double *x, int
         launch_permute(n, (int)nrhs, s->d_peri, dx, n, px, n, 1, s->st);
         launch_permute(n, (int)nrhs, s->d_peri, dy, n, py, n, 1, s->st);
         const double *vals = (s->facto == FACTO_GETRF) ? s->d_Uv : s->d_Lv;
-        launch_spmv(n, (int)nrhs, s->d_colptr, s->d_rowtab, vals, px, n, py, n, alpha, beta, s->st);
+        if (nrhs > 1 && !s->d_xt && dalloc(&s->d_xt, (size_t)n * 16)) rc = ERR_OOM;
+        if (!rc) launch_spmv(n, (int)nrhs, s->d_colptr, s->d_rowtab, vals, px, n, py, n, alpha, beta, s->st, s->d_xt);
         launch_permute(n, (int)nrhs, s->d_peri, py, n, dy, n, 0, s->st);
         if (cudaMemcpy2DAsync(y, ldy * sizeof(double), dy, n * sizeof(double), n * sizeof(double), nrhs,
                               cudaMemcpyDeviceToHost, s->st) != cudaSuccess) rc = ERR_INTERNAL;
