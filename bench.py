@@ -53,6 +53,8 @@ def parse():
     ap.add_argument("--numfact-once", default=None, metavar="PREC",
                     help="profiling aid: one factorization of the workload in precision PREC (fp64, fp32, tf32, "
                          "tf32x3) through the library, then exit")
+    ap.add_argument("--solve-once", action="store_true",
+                    help="with --numfact-once: also one solve of the right-hand sides (profiling aid)")
     ap.add_argument("--cpu-budget", type=float, default=150.0, help="seconds of CPU time for the reference arm")
     return ap.parse_args()
 
@@ -327,8 +329,14 @@ def main():
         s.bcsc_load(an.bcsc())
         s.numfact(0.0)
         st_ = s.stats()
-        print(json.dumps({"workload": name, "precision": args.numfact_once, "numfact_ms": st_["numfact_ms"],
-                          "launches": st_["launches_numfact"]}), flush=True)
+        out = {"workload": name, "precision": args.numfact_once, "numfact_ms": st_["numfact_ms"],
+               "launches": st_["launches_numfact"]}
+        if args.solve_once:
+            # one solve of the workload's right-hand sides after the factorization
+            x = s.solve(b)
+            out["solve_ms"] = s.stats()["solve_ms"]
+            out["berr"] = float(np.max(np.linalg.norm(b - A.matvec(x), axis=0) / np.linalg.norm(b, axis=0)))
+        print(json.dumps(out), flush=True)
         s.close()
         return 0
     dist = None

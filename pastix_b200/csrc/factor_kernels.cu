@@ -881,11 +881,14 @@ __global__ void __launch_bounds__(32 * US_WARPS) update_small_kernel(DevSym s, c
     const bool sym = (u.flags & UPD_SYM) != 0;
     T *C = ((u.flags & UPD_C_U) ? U : L) + s.off[u.f];
     const int ldf = s.ld[u.f];
-    // B (N x K, N <= 32) and D in registers of the lanes, broadcast by shuffles
-    T bk[16];
+    // B (N x K, N <= 32, K <= 16) with D folded into A: bs[c][q] = B[c][q] in shared
+    // memory, read by every lane as 128-bit broadcasts
+    __shared__ __align__(16) T bsm[US_WARPS][32][16];
+    T(*bs)[16] = bsm[threadIdx.x >> 5];
 #pragma unroll
-    for (int q = 0; q < 16; q++) bk[q] = (lane < u.N && q < u.K) ? Bp[lane + (size_t)q * ldk] : (T)0;
+    for (int q = 0; q < 16; q++) bs[lane][q] = (lane < u.N && q < u.K) ? Bp[lane + (size_t)q * ldk] : (T)0;
     T dk = (scale && lane < u.K) ? Dp[(size_t)lane * (ldk + 1)] : (T)1;
+    __syncwarp();
     for (int r0 = 0; r0 < u.M; r0 += 32) {
         const int i = r0 + lane;
         const bool in = i < u.M;
@@ -899,8 +902,25 @@ __global__ void __launch_bounds__(32 * US_WARPS) update_small_kernel(DevSym s, c
         T *crow = C + d + (size_t)u.colbase * ldf;
         for (int c = 0; c < u.N; c++) {
             T acc = 0;
+            if constexpr (sizeof(T) == 4) {
+                const float4 *b4 = reinterpret_cast<const float4 *>(bs[c]);
 #pragma unroll
-            for (int q = 0; q < 16; q++) acc += a[q] * __shfl_sync(0xffffffffu, bk[q], c);
+                for (int h = 0; h < 4; h++) {
+                    const float4 bq = b4[h];
+                    acc += a[4 * h] * bq.x;
+                    acc += a[4 * h + 1] * bq.y;
+                    acc += a[4 * h + 2] * bq.z;
+                    acc += a[4 * h + 3] * bq.w;
+                }
+            } else {
+                const double2 *b2 = reinterpret_cast<const double2 *>(bs[c]);
+#pragma unroll
+                for (int h = 0; h < 8; h++) {
+                    const double2 bq = b2[h];
+                    acc += a[2 * h] * bq.x;
+                    acc += a[2 * h + 1] * bq.y;
+                }
+            }
             if (d >= 0 && !(sym && i < c)) {
                 if (atomic) atomicAdd(crow + (size_t)c * ldf, -acc);
                 else crow[(size_t)c * ldf] -= acc;
