@@ -87,6 +87,20 @@ int b200_bcsc_load( b200_solver_t *solver, int64_t nnz, const int64_t *colptr,
  * before a first b200_bcsc_load. */
 int b200_bcsc_values( b200_solver_t *solver, const double *Lvalues, const double *Uvalues, double anorm );
 
+/* The bcsc construction of a same-pattern refactorization on the device
+ * (bcsc_zinit_centralized, bcsc/bcsc_zinit.c:52-541, after pastix_subtask_spm2bcsc,
+ * sopalin/pastix_task_sopalin.c:82): b200_spm_map records, for every entry e of the
+ * bcsc of the last b200_bcsc_load, the index lmap[e] (umap[e] for the A^T values of
+ * LU) of the input matrix value it holds, in the matrix's own CSC order (nnz_spm
+ * values; for symmetric matrices the stored triangle, both bcsc entries of an
+ * off-diagonal value mapping to it).  b200_spm_values / b200_spm_values_device then
+ * take new values in that order (host / device memory), permute and expand them on
+ * the GPU, and set ||A||_F for the threshold (computed on the device when anorm < 0,
+ * as spmNorm(SpmFrobeniusNorm)).  A new pattern in b200_bcsc_load drops the map. */
+int b200_spm_map( b200_solver_t *solver, int64_t nnz_spm, const int64_t *lmap, const int64_t *umap );
+int b200_spm_values( b200_solver_t *solver, const double *values, double anorm );
+int b200_spm_values_device( b200_solver_t *solver, const double *d_values, double anorm, void *stream );
+
 /* Numerical factorization: bcsc -> coeftab scatter (cpucblk_zfillin,
  * kernels/cpucblk_zinit.c:229) and the supernodal factorization
  * (sopalin/sequential_z{potrf,sytrf,getrf}.c).  epsilon_magn_ctrl has the

@@ -116,6 +116,8 @@ int configure_inverse_kernels();
 void launch_spmv(int n, int nrhs, const int64_t *colptr, const int *rowtab, const double *vals, const double *x,
                  int64_t ldx, double *y, int64_t ldy, double alpha, double beta, cudaStream_t st,
                  double *xt = nullptr);
+// dst[e] = src[map[e]], e < nnz
+void launch_gather_values(int64_t nnz, const int64_t *map, const double *src, double *dst, cudaStream_t st);
 // out[r] = sum_i x[i,r] * y[i,r]  (nrhs columns), accumulated in double
 void launch_dots(int n, int nrhs, const double *x, int64_t ldx, const double *y, int64_t ldy, double *out,
                  cudaStream_t st);

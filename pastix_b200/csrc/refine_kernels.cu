@@ -155,6 +155,18 @@ void launch_spmv(int n, int nrhs, const int64_t *colptr, const int *rowtab, cons
     }
 }
 
+// dst[e] = src[map[e]] (values of the input matrix -> bcsc entries)
+__global__ void gather_values_kernel(int64_t nnz, const int64_t *__restrict__ map, const double *__restrict__ src,
+                                     double *__restrict__ dst) {
+    const int64_t e = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
+    if (e < nnz) dst[e] = src[map[e]];
+}
+
+void launch_gather_values(int64_t nnz, const int64_t *map, const double *src, double *dst, cudaStream_t st) {
+    if (nnz <= 0) return;
+    gather_values_kernel<<<nblk(nnz, 256), 256, 0, st>>>(nnz, map, src, dst);
+}
+
 void launch_dots(int n, int nrhs, const double *x, int64_t ldx, const double *y, int64_t ldy, double *out,
                  cudaStream_t st) {
     if (nrhs <= 0) return;

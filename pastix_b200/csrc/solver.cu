@@ -156,6 +156,11 @@ struct b200_solver_s {
     int64_t *d_colptr = nullptr;
     int *d_rowtab = nullptr;
     double *d_Lv = nullptr, *d_Uv = nullptr;
+    // the input matrix's own values -> bcsc entries (b200_spm_map): d_Lv[e] =
+    // spm[lmap[e]], d_Uv[e] = spm[umap[e]]; d_spmv holds the uploaded spm values
+    int64_t nnz_spm = 0;
+    int64_t *d_lmap = nullptr, *d_umap = nullptr;
+    double *d_spmv = nullptr;
     int64_t *d_dest = nullptr;
     std::vector<int64_t> h_colptr, h_rowtab;
     double anorm = 0.0;
@@ -1420,6 +1425,9 @@ int b200_solver_destroy(b200_solver_t *s) {
     if (s->d_rowtab) cudaFree(s->d_rowtab);
     if (s->d_Lv) cudaFree(s->d_Lv);
     if (s->d_Uv) cudaFree(s->d_Uv);
+    if (s->d_lmap) cudaFree(s->d_lmap);
+    if (s->d_umap) cudaFree(s->d_umap);
+    if (s->d_spmv) cudaFree(s->d_spmv);
     if (s->d_dest) cudaFree(s->d_dest);
     if (s->d_ws) cudaFree(s->d_ws);
     if (s->d_scal) cudaFree(s->d_scal);
@@ -1442,6 +1450,67 @@ int b200_bcsc_values(b200_solver_t *s, const double *Lvalues, const double *Uval
     return ERR_SUCCESS;
 }
 
+// bcsc_zinit_centralized (bcsc/bcsc_zinit.c:52-541) on the device for a matrix whose
+// pattern is the one of the last b200_bcsc_load: the permutation and symmetric
+// expansion of the input values is a gather through maps built once on the host
+// (by running PaStiX's own bcsc construction on the entry indices).
+int b200_spm_map(b200_solver_t *s, int64_t nnz_spm, const int64_t *lmap, const int64_t *umap) {
+    if (!s || s->nnz < 0 || nnz_spm <= 0 || !lmap) return ERR_BADPARAM;
+    if (s->facto == FACTO_GETRF && !umap) return ERR_BADPARAM;
+    for (int64_t e = 0; e < s->nnz; e++) {
+        if (lmap[e] < 0 || lmap[e] >= nnz_spm) return ERR_BADPARAM;
+        if (s->facto == FACTO_GETRF && (umap[e] < 0 || umap[e] >= nnz_spm)) return ERR_BADPARAM;
+    }
+    if (s->d_lmap) cudaFree(s->d_lmap);
+    if (s->d_umap) cudaFree(s->d_umap);
+    if (s->d_spmv) cudaFree(s->d_spmv);
+    s->d_lmap = s->d_umap = nullptr;
+    s->d_spmv = nullptr;
+    s->nnz_spm = 0;
+    RET(dalloc(&s->d_lmap, (size_t)s->nnz));
+    RET(dalloc(&s->d_spmv, (size_t)nnz_spm));
+    CU(cudaMemcpy(s->d_lmap, lmap, s->nnz * sizeof(int64_t), cudaMemcpyHostToDevice));
+    if (s->facto == FACTO_GETRF) {
+        RET(dalloc(&s->d_umap, (size_t)s->nnz));
+        CU(cudaMemcpy(s->d_umap, umap, s->nnz * sizeof(int64_t), cudaMemcpyHostToDevice));
+    }
+    s->nnz_spm = nnz_spm;
+    return ERR_SUCCESS;
+}
+
+int b200_spm_values_device(b200_solver_t *s, const double *d_values, double anorm, void *stream) {
+    if (!s || s->nnz < 0 || !s->nnz_spm || !d_values) return ERR_BADPARAM;
+    cudaStream_t st = stream ? (cudaStream_t)stream : s->st;
+    launch_gather_values(s->nnz, s->d_lmap, d_values, s->d_Lv, st);
+    if (s->facto == FACTO_GETRF) launch_gather_values(s->nnz, s->d_umap, d_values, s->d_Uv, st);
+    if (anorm < 0.0) {
+        // ||A||_F over the expanded bcsc (both triangles), as spmNorm(SpmFrobeniusNorm)
+        RET(ensure_scal(s, 4));
+        CU(cudaMemsetAsync(s->d_scal, 0, sizeof(double), st));
+        launch_dots((int)s->nnz, 1, s->d_Lv, s->nnz, s->d_Lv, s->nnz, s->d_scal, st);
+        double ss = 0.0;
+        CU(cudaMemcpyAsync(&ss, s->d_scal, sizeof(double), cudaMemcpyDeviceToHost, st));
+        CU(cudaStreamSynchronize(st));
+        anorm = std::sqrt(ss);
+    }
+    if (st != s->st) {
+        // the factorization runs on the solver's stream
+        CU(cudaEventRecord(s->ev1, st));
+        CU(cudaStreamWaitEvent(s->st, s->ev1, 0));
+    }
+    s->anorm = anorm;
+    s->factored = false;
+    return ERR_SUCCESS;
+}
+
+int b200_spm_values(b200_solver_t *s, const double *values, double anorm) {
+    if (!s || s->nnz < 0 || !s->nnz_spm || !values) return ERR_BADPARAM;
+    CU(cudaMemcpyAsync(s->d_spmv, values, s->nnz_spm * sizeof(double), cudaMemcpyHostToDevice, s->st));
+    RET(b200_spm_values_device(s, s->d_spmv, anorm, s->st));
+    CU(cudaStreamSynchronize(s->st));
+    return ERR_SUCCESS;
+}
+
 int b200_bcsc_load(b200_solver_t *s, int64_t nnz, const int64_t *colptr, const int64_t *rowtab, const double *Lvalues,
                    const double *Uvalues, double anorm) {
     if (!s || nnz < 0 || !colptr || !rowtab || !Lvalues) return ERR_BADPARAM;
@@ -1457,6 +1526,8 @@ int b200_bcsc_load(b200_solver_t *s, int64_t nnz, const int64_t *colptr, const i
         if (s->d_Uv) cudaFree(s->d_Uv);
         if (s->d_dest) cudaFree(s->d_dest);
         s->d_colptr = nullptr; s->d_rowtab = nullptr; s->d_Lv = nullptr; s->d_Uv = nullptr; s->d_dest = nullptr;
+        s->d_lmap = nullptr; s->d_umap = nullptr; s->d_spmv = nullptr;  // a new pattern invalidates the spm map
+        s->nnz_spm = 0;
         if (s->fact_graph) cudaGraphExecDestroy(s->fact_graph);
         s->fact_graph = nullptr;
         s->h_colptr.assign(colptr, colptr + n + 1);

@@ -23,7 +23,8 @@ _I64 = C.c_int64
 _lib = None
 
 # exported symbols, in the order of include/pastix_b200.h
-SYMBOLS = ["b200_solver_create", "b200_solver_destroy", "b200_bcsc_load", "b200_bcsc_values", "b200_numfact", "b200_numfact_trace",
+SYMBOLS = ["b200_solver_create", "b200_solver_destroy", "b200_bcsc_load", "b200_bcsc_values", "b200_spm_map",
+           "b200_spm_values", "b200_spm_values_device", "b200_numfact", "b200_numfact_trace",
            "b200_solve_trace", "b200_trace_launches", "b200_trace_kinds", "b200_solve",
            "b200_solve_device", "b200_solve_device_noalloc", "b200_refine", "b200_refine_device", "b200_spmv", "b200_factor_download",
            "b200_stats", "b200_strerror"]
@@ -56,6 +57,9 @@ def lib():
         L.b200_trace_launches.argtypes = [_P, _P, _P, _I64]
         L.b200_trace_launches.restype = _I64
         L.b200_bcsc_values.argtypes = [_P, _P, _P, C.c_double]
+        L.b200_spm_map.argtypes = [_P, _I64, _P, _P]
+        L.b200_spm_values.argtypes = [_P, _P, C.c_double]
+        L.b200_spm_values_device.argtypes = [_P, _P, C.c_double, _P]
         L.b200_trace_kinds.argtypes = [_P, _P, _P, C.c_int]
         L.b200_solve_device.argtypes = [_P, _I64, _P, _I64, _P]
         L.b200_solve_device_noalloc.argtypes = [_P, _I64, _P, _I64, _P]
@@ -124,6 +128,21 @@ class Solver:
         Lv = np.ascontiguousarray(Lvalues, dtype=np.float64)
         Uv = np.ascontiguousarray(Uvalues, dtype=np.float64) if Uvalues is not None else None
         check(lib().b200_bcsc_values(self.h, _p(Lv), _p(Uv), anorm), "b200_bcsc_values")
+
+    def spm_map(self, nnz_spm: int, lmap, umap=None):
+        """Map of the input matrix's values onto the bcsc entries (b200_spm_map)."""
+        lm = np.ascontiguousarray(lmap, dtype=np.int64)
+        um = np.ascontiguousarray(umap, dtype=np.int64) if umap is not None else None
+        check(lib().b200_spm_map(self.h, int(nnz_spm), _p(lm), _p(um)), "b200_spm_map")
+
+    def spm_values(self, values, anorm: float = -1.0):
+        """New values in the input matrix's own CSC order; bcsc built on the GPU."""
+        v = np.ascontiguousarray(values, dtype=np.float64)
+        check(lib().b200_spm_values(self.h, _p(v), anorm), "b200_spm_values")
+
+    def spm_values_device(self, d_values: int, anorm: float = -1.0, stream: int | None = None):
+        check(lib().b200_spm_values_device(self.h, _P(d_values), anorm, _P(stream) if stream else None),
+              "b200_spm_values_device")
 
     def numfact(self, epsilon_magn_ctrl: float = 0.0) -> int:
         piv = _I64(0)

@@ -202,6 +202,20 @@ class Analysis:
                          Uv.ctypes.data_as(C.c_void_p) if Uv is not None else None)
         return BCSC(n, colptr, rowtab, Lv, Uv, float(L.rh_anorm(self.h)))
 
+    def spm_maps(self):
+        """For every bcsc entry, the index of the input matrix value it holds (and, for
+        LU, of the A^T value): PaStiX's own bcsc construction run on the entry
+        indices (exact in double), the instance's values restored afterwards."""
+        if self._vals.dtype != np.float64:
+            raise ValueError("spm_maps needs a double-precision matrix")
+        orig = self._vals
+        nnz_spm = orig.size
+        idx = self.bcsc(values=np.arange(nnz_spm, dtype=np.float64))
+        lmap = idx.Lvalues.astype(np.int64)
+        umap = idx.Uvalues.astype(np.int64) if idx.Uvalues is not None else None
+        self.bcsc(values=orig)
+        return nnz_spm, lmap, umap
+
     def iparm(self, name):
         ip, _ = param_ids()
         return int(lib().rh_iparm(self.h)[ip[name]])

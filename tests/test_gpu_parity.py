@@ -347,3 +347,43 @@ def test_full_size_config2_backward_error():
     assert backward_error(A, x, b).max() <= BERR_TARGET
     assert forward_error(x, xt).max() <= 1e-9
     s.close()
+
+
+@pytest.mark.parametrize("facto,make", [CASES[1], CASES[2], CASES[-2]])
+def test_device_bcsc_from_matrix_values(facto, make):
+    """Same-pattern refactorization from the matrix's own values (bcsc built on the
+    device through the maps): the same factor as the host bcsc path, the norm as
+    PaStiX computes it, and new values (the matrix scaled by 3, diagonal shifted)
+    factor and solve to the oracle's results."""
+    A = make()
+    an = Analysis(A, facto)
+    st = an.structure()
+    bc = an.bcsc()
+    s = native.Solver(st, facto, "fp64")
+    s.bcsc_load(bc)
+    nnz, lmap, umap = an.spm_maps()
+    s.spm_map(nnz, lmap, umap)
+    s.spm_values(A.values)
+    piv = s.numfact(0.0)
+    thr = s.stats()["threshold"]
+    assert abs(thr - np.sqrt(np.finfo(np.float64).eps / 2) * bc.anorm) <= 1e-12 * thr
+    orc, L, U, opiv = oracle_factor(st, bc, an.facto, thr)
+    assert piv == opiv
+    Lg, Ug = s.factor()
+    d = factor_diff(orc, an.facto, Lg, Ug, L, U)
+    assert d <= 1e-12 or facto == "sytrf", d
+    # new values on the same pattern
+    B = type(A)(A.n, A.colptr, A.rowind, 3.0 * A.values, A.symmetric, A.grid)
+    cols = np.repeat(np.arange(A.n), np.diff(A.colptr))
+    B.values[A.rowind == cols] += 0.5
+    s.spm_values(B.values)
+    s.numfact(0.0)
+    an2 = Analysis(B, facto)
+    bc2 = an2.bcsc()
+    orc2, L2, U2, _ = oracle_factor(an2.structure(), bc2, an2.facto, s.stats()["threshold"])
+    xt, b = M.rhs_from_xtrue(B, 2, seed=5)
+    x = s.solve(b)
+    xo = orc2.solve(an2.facto, L2, U2, b)
+    assert np.linalg.norm(x - xo) / np.linalg.norm(xo) <= 1e-11
+    assert backward_error(B, x, b).max() <= BERR_FP64
+    s.close()

@@ -8,6 +8,7 @@ import pytest
 from golden_util import FIELDS, load, names
 from pastix_b200 import matrices as M
 from pastix_b200 import refhost
+from pastix_b200.refhost import Analysis
 
 pytestmark = pytest.mark.skipif(not os.path.exists(refhost.LIBPATH), reason="PaStiX host library not built")
 
@@ -49,3 +50,26 @@ def test_structure_invariants():
         assert np.array_equal(st.blok_coefind[b0:b1], np.concatenate([[0], np.cumsum(rows[b0:b1])[:-1]]) * nc[k])
     assert np.array_equal(np.sort(st.permtab), np.arange(st.n))
     assert np.array_equal(st.peritab[st.permtab], np.arange(st.n))
+
+
+@pytest.mark.parametrize("facto,make", [
+    ("potrf", lambda: M.laplacian(8, 8, 8, 27, 26.0, shift=1e-3)),
+    ("getrf", lambda: M.convection_diffusion(6, 6, 6, seed=2)),
+    ("sytrf", lambda: M.laplacian(6, 6, 6, 7, 6.0, shift=-0.7)),
+])
+def test_spm_maps_reproduce_pastix_bcsc(facto, make):
+    """The input-value maps behind the device bcsc construction: gathering the
+    matrix's own values through them gives PaStiX's bcsc exactly, and the
+    instance's values are left as they were."""
+    A = make()
+    an = Analysis(A, facto)
+    bc = an.bcsc()
+    nnz, lmap, umap = an.spm_maps()
+    assert nnz == A.values.size and lmap.size == bc.Lvalues.size
+    assert np.array_equal(A.values[lmap], bc.Lvalues)
+    if facto == "getrf":
+        assert np.array_equal(A.values[umap], bc.Uvalues)
+    else:
+        assert umap is None
+    assert np.array_equal(an.bcsc().Lvalues, bc.Lvalues)
+    assert abs(np.sqrt(np.sum(bc.Lvalues ** 2)) - bc.anorm) <= 1e-13 * bc.anorm
