@@ -262,26 +262,28 @@ def pinned_like(a, order="C"):
     return out, t
 
 
-def e2e_path(solver, bc, A, b, prec, refine, nrhs, reps=3):
+def e2e_path(solver, an, A, b, prec, refine, nrhs, reps=3):
     """The same step through the C ABI with host buffers in pinned memory: the
-    matrix values uploaded (b200_bcsc_values, the refactorization entry point),
-    factorization, x = b copied on the host and solved in place (b200_solve),
-    refinement of x against b with host vectors (b200_refine)."""
-    Lv, _tl = pinned_like(bc.Lvalues)
-    Uv, _tu = pinned_like(bc.Uvalues) if bc.Uvalues is not None else (None, None)
+    matrix's own values uploaded and turned into the bcsc on the GPU
+    (b200_spm_values, the same-pattern refactorization entry point; ||A||_F computed
+    on the device), factorization, x = b copied on the host and solved in place
+    (b200_solve), refinement of x against b with host vectors (b200_refine)."""
+    nnz_spm, lmap, umap = an.spm_maps()
+    solver.spm_map(nnz_spm, lmap, umap)
+    vp, _tv = pinned_like(np.ascontiguousarray(A.values, dtype=np.float64))
     bp, _tb = pinned_like(np.asfortranarray(b), order="F")
     xp, _tx = pinned_like(np.asfortranarray(b), order="F")
     ts = []
     for _ in range(reps):
         t0 = time.perf_counter()
-        solver.bcsc_values(Lv, Uv, bc.anorm)
+        solver.spm_values(vp, -1.0)
         solver.numfact(0.0)
         np.copyto(xp, bp)
         solver.solve(xp, inplace=True)
         if refine:
             solver.refine(bp, xp, "cg", BERR_TARGET, 50, 25, inplace=True)
         ts.append(time.perf_counter() - t0)
-    h2d = bc.Lvalues.nbytes + (bc.Uvalues.nbytes if bc.Uvalues is not None else 0) + b.nbytes * (3 if refine else 1)
+    h2d = vp.nbytes + b.nbytes * (3 if refine else 1)
     d2h = b.nbytes * (2 if refine else 1)
     return float(np.median(ts)), int(h2d), int(d2h)
 
@@ -409,7 +411,7 @@ def main():
 
     hs, _ = solvers[head["prec"]]
     p50, p99 = solve_latency(hs, A, b, stream, device_b, device_x, nrhs)
-    e2e_s, h2d, d2h = e2e_path(hs, bc, A, b, head["prec"], head["prec"] != "fp64", nrhs)
+    e2e_s, h2d, d2h = e2e_path(hs, an, A, b, head["prec"], head["prec"] != "fp64", nrhs)
     e2e_value = world * st.thflops / e2e_s / 1e9
 
     # roofline of the dominant kernel of the headline path: the update kind with
@@ -460,7 +462,7 @@ def main():
             "cpu_baseline": cpu,
             "e2e": {"value": e2e_value, "unit": "GFLOP/s", "h2d_bytes_per_step": h2d, "d2h_bytes_per_step": d2h,
                     "seconds_per_step": e2e_s, "host_buffers": "pinned",
-                    "step": "b200_bcsc_values + b200_numfact + host copy x=b + b200_solve + b200_refine"},
+                    "step": "b200_spm_values (bcsc built on the GPU) + b200_numfact + host copy x=b + b200_solve + b200_refine"},
             "gpu_launches": int(sum(r["launches"] for r in results.values())),
             "clocks": clocks,
             "wall_s_timed_region": wall,
