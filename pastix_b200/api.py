@@ -12,8 +12,10 @@ from __future__ import annotations
 
 import numpy as np
 
+import dataclasses
+
 from . import native
-from .refhost import Analysis
+from .refhost import BCSC, Analysis, SolverStructure
 
 DEFAULT_IPARM = {
     "FACTORIZATION": "potrf",   # IPARM_FACTORIZATION: potrf / sytrf / getrf
@@ -54,6 +56,32 @@ class PastixB200:
                                     self.stream)
         return self
 
+    # pastixOrderSave / pastixSymbolSave / solverSave under IPARM_IO_STRATEGY
+    # (order/order_io.c:294, symbol/symbol_io.c:146, blend/solver_io.c:45)
+    def save_analysis(self, path):
+        if self.analysis is None:
+            raise RuntimeError("save_analysis needs task_analyze first")
+        save_analysis(path, self.analysis, self.iparm["FACTORIZATION"])
+
+    # pastixOrderLoad / pastixSymbolLoad / solverLoad (order/order_io.c:141,
+    # symbol/symbol_io.c:76, blend/solver_io.c:260): task_analyze from a file
+    def load_analysis(self, path):
+        saved = load_analysis(path)
+        if saved.facto != self.iparm["FACTORIZATION"]:
+            raise ValueError(f"saved analysis is for {saved.facto}, not {self.iparm['FACTORIZATION']}")
+        st = saved.structure
+        self.analysis = None
+        self.structure = st
+        self.out["FACT_THFLOPS"] = st.thflops
+        if self.solver is not None:
+            self.solver.close()
+        self.solver = native.Solver(st, saved.facto, self.iparm["PRECISION"], self.stream)
+        zeros = np.zeros(saved.bcsc_rowtab.size)
+        self.solver.bcsc_load(BCSC(st.n, saved.bcsc_colptr, saved.bcsc_rowtab, zeros,
+                                   zeros if saved.facto == "getrf" else None, 0.0))
+        self.solver.spm_map(saved.nnz_spm, saved.lmap, saved.umap)
+        return self
+
     # pastix_subtask_spm2bcsc (sopalin/pastix_task_sopalin.c:82)
     def subtask_spm2bcsc(self, values=None):
         bc = self.analysis.bcsc(values)
@@ -63,7 +91,13 @@ class PastixB200:
 
     # pastix_task_numfact (sopalin/pastix_task_sopalin.c:563)
     def task_numfact(self, values=None):
-        self.subtask_spm2bcsc(values)
+        if self.analysis is None:
+            # loaded analysis: the matrix's own values, bcsc built on the GPU
+            if values is None:
+                raise ValueError("a loaded analysis needs the matrix values")
+            self.solver.spm_values(np.ascontiguousarray(values, dtype=np.float64), -1.0)
+        else:
+            self.subtask_spm2bcsc(values)
         piv = self.solver.numfact(self.dparm["EPSILON_MAGN_CTRL"])
         st = self.solver.stats()
         self.out["STATIC_PIVOTING"] = piv
@@ -90,6 +124,49 @@ class PastixB200:
         if self.solver is not None:
             self.solver.close()
             self.solver = None
+
+
+@dataclasses.dataclass
+class SavedAnalysis:
+    """What a serving process needs to factor and solve without PaStiX's analysis:
+    the SolverMatrix tables with the ordering, the bcsc pattern, the map of the
+    matrix's own values onto the bcsc entries, and the matrix pattern they refer to."""
+    facto: str
+    structure: SolverStructure
+    bcsc_colptr: np.ndarray
+    bcsc_rowtab: np.ndarray
+    nnz_spm: int
+    lmap: np.ndarray
+    umap: np.ndarray | None
+    a_colptr: np.ndarray
+    a_rowind: np.ndarray
+    a_symmetric: bool
+
+
+def save_analysis(path, analysis: Analysis, facto: str):
+    """The analysis of ``analysis`` in one .npz file (plain arrays, no pickling)."""
+    st = analysis.structure()
+    bc = analysis.bcsc()
+    nnz_spm, lmap, umap = analysis.spm_maps()
+    A = analysis.A
+    arrays = {"st_" + f.name: getattr(st, f.name) for f in dataclasses.fields(st) if f.name != "extra"}
+    np.savez(path, **arrays, bcsc_colptr=bc.colptr, bcsc_rowtab=bc.rowtab, nnz_spm=nnz_spm, lmap=lmap,
+             umap=umap if umap is not None else np.zeros(0, np.int64), a_colptr=A.colptr, a_rowind=A.rowind,
+             a_symmetric=bool(A.symmetric), facto=facto)
+
+
+def load_analysis(path) -> SavedAnalysis:
+    with np.load(path, allow_pickle=False) as z:
+        kw = {}
+        for f in dataclasses.fields(SolverStructure):
+            if f.name == "extra":
+                continue
+            v = z["st_" + f.name]
+            kw[f.name] = v if v.ndim else v.item()
+        umap = z["umap"]
+        return SavedAnalysis(str(z["facto"]), SolverStructure(**kw), z["bcsc_colptr"], z["bcsc_rowtab"],
+                             int(z["nnz_spm"]), z["lmap"], umap if umap.size else None, z["a_colptr"],
+                             z["a_rowind"], bool(z["a_symmetric"]))
 
 
 def backward_error(A, x, b) -> np.ndarray:

@@ -387,3 +387,31 @@ def test_device_bcsc_from_matrix_values(facto, make):
     assert np.linalg.norm(x - xo) / np.linalg.norm(xo) <= 1e-11
     assert backward_error(B, x, b).max() <= BERR_FP64
     s.close()
+
+
+def test_serving_from_saved_analysis(tmp_path):
+    """A second instance that only loads the saved analysis (no PaStiX host analysis,
+    bcsc built on the GPU from the matrix's own values) factors and solves like the
+    analysed one, also after new values on the same pattern."""
+    A = M.laplacian(12, 12, 12, 27, 26.0, shift=1e-3)
+    p1 = PastixB200({"FACTORIZATION": "potrf"})
+    p1.task_analyze(A)
+    p1.save_analysis(tmp_path / "an.npz")
+    p1.task_numfact()
+    xt, b = M.rhs_from_xtrue(A, 3, seed=2)
+    x1 = p1.task_solve(b)
+    p2 = PastixB200({"FACTORIZATION": "potrf"})
+    p2.load_analysis(tmp_path / "an.npz")
+    assert p2.analysis is None
+    p2.task_numfact(A.values)
+    assert p2.out["STATIC_PIVOTING"] == p1.out["STATIC_PIVOTING"]
+    x2 = p2.task_solve(b)
+    assert np.linalg.norm(x2 - x1) / np.linalg.norm(x1) <= 1e-12
+    assert backward_error(A, x2, b).max() <= BERR_FP64
+    B = type(A)(A.n, A.colptr, A.rowind, 2.0 * A.values, A.symmetric, A.grid)
+    p2.task_numfact(B.values)
+    x3 = p2.task_solve(b)
+    assert backward_error(B, x3, b).max() <= BERR_FP64
+    assert np.linalg.norm(2.0 * x3 - x1) / np.linalg.norm(x1) <= 1e-11
+    p1.close()
+    p2.close()

@@ -73,3 +73,25 @@ def test_spm_maps_reproduce_pastix_bcsc(facto, make):
         assert umap is None
     assert np.array_equal(an.bcsc().Lvalues, bc.Lvalues)
     assert abs(np.sqrt(np.sum(bc.Lvalues ** 2)) - bc.anorm) <= 1e-13 * bc.anorm
+
+
+def test_saved_analysis_round_trip(tmp_path):
+    """save_analysis / load_analysis (pastixOrderSave, pastixSymbolSave, solverSave
+    counterparts): every table, the bcsc pattern and the value maps come back
+    unchanged, and the maps still rebuild PaStiX's bcsc from the matrix values."""
+    from pastix_b200.api import load_analysis, save_analysis
+    A = M.laplacian(7, 6, 5, 27, 26.0, shift=1e-3)
+    an = Analysis(A, "potrf")
+    path = tmp_path / "analysis.npz"
+    save_analysis(path, an, "potrf")
+    sv = load_analysis(path)
+    st = an.structure()
+    for f in ("n", "cblknbr", "bloknbr", "brownbr", "coefnbr", "thflops"):
+        assert getattr(sv.structure, f) == getattr(st, f)
+    for f in ("cblk_fcolnum", "cblk_fblok", "cblk_stride", "blok_frownum", "blok_fcblknm", "browtab", "peritab"):
+        assert np.array_equal(getattr(sv.structure, f), getattr(st, f))
+    bc = an.bcsc()
+    assert np.array_equal(sv.bcsc_colptr, bc.colptr) and np.array_equal(sv.bcsc_rowtab, bc.rowtab)
+    assert sv.facto == "potrf" and sv.umap is None and sv.nnz_spm == A.values.size
+    assert np.array_equal(A.values[sv.lmap], bc.Lvalues)
+    assert np.array_equal(sv.a_colptr, A.colptr) and sv.a_symmetric == A.symmetric
