@@ -97,6 +97,12 @@ int b200_bcsc_values( b200_solver_t *solver, const double *Lvalues, const double
  * take new values in that order (host / device memory), permute and expand them on
  * the GPU, and set ||A||_F for the threshold (computed on the device when anorm < 0,
  * as spmNorm(SpmFrobeniusNorm)).  A new pattern in b200_bcsc_load drops the map. */
+/* pastixGetDiag (sopalin/diag.c:55, coeftab_zgetdiag, sopalin/coeftab_z.c:462): the
+ * diagonal of the factor's diagonal blocks in the permuted numbering (Cholesky: the
+ * diagonal of L; LDL^T: D; LU: the diagonal of U), n values D[i * incD] as double.
+ * Requires a completed b200_numfact. */
+int b200_get_diag( b200_solver_t *solver, double *D, int64_t incD );
+
 int b200_spm_map( b200_solver_t *solver, int64_t nnz_spm, const int64_t *lmap, const int64_t *umap );
 int b200_spm_values( b200_solver_t *solver, const double *values, double anorm );
 int b200_spm_values_device( b200_solver_t *solver, const double *d_values, double anorm, void *stream );

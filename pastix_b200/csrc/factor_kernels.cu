@@ -929,6 +929,24 @@ __global__ void __launch_bounds__(32 * US_WARPS) update_small_kernel(DevSym s, c
     }
 }
 
+// pastixGetDiag / coeftab_zgetdiag (sopalin/diag.c:55, sopalin/coeftab_z.c:462-492):
+// the diagonal of every cblk's diagonal block in cblk order (the permuted
+// numbering): L_kk's diagonal for Cholesky, D for LDL^T, U_kk's for LU.
+template <typename T>
+__global__ void get_diag_kernel(DevSym s, const T *__restrict__ L, double *out) {
+    const int k = blockIdx.x;
+    const int nc = s.ncols[k], ld = s.ld[k];
+    const T *Lk = L + s.off[k];
+    for (int i = threadIdx.x; i < nc; i += blockDim.x) out[s.fcol[k] + i] = (double)Lk[(size_t)i * (ld + 1)];
+}
+
+template <typename T>
+void launch_get_diag(const DevSym &s, const T *L, double *out, cudaStream_t st) {
+    if (s.cblknbr > 0) get_diag_kernel<T><<<s.cblknbr, 64, 0, st>>>(s, L, out);
+}
+template void launch_get_diag<double>(const DevSym &, const double *, double *, cudaStream_t);
+template void launch_get_diag<float>(const DevSym &, const float *, double *, cudaStream_t);
+
 template <typename T>
 void launch_update_small(const DevSym &s, const Upd *upds, int nupd, T *L, T *U, cudaStream_t st) {
     if (nupd <= 0) return;

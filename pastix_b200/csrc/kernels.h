@@ -43,6 +43,9 @@ void launch_panel_rows(int facto, const DevSym &s, const PanelCblk *pcb, const P
                        unsigned long long *npiv, int *err, cudaStream_t st);
 int panel_rows_block(int nsmax, size_t esz);
 int configure_panel_kernels();
+// the diagonal of the factor's diagonal blocks, in the permuted numbering (n doubles)
+template <typename T>
+void launch_get_diag(const DevSym &s, const T *L, double *out, cudaStream_t st);
 // updates with K <= 16 and N <= 32, one warp each
 template <typename T>
 void launch_update_small(const DevSym &s, const Upd *upds, int nupd, T *L, T *U, cudaStream_t st);

@@ -856,7 +856,7 @@ constexpr int DIAG_INV_SMEM = INV_WARPS * 2 * 32 * TP * sizeof(double);
 //            W_ij = -W_ii sum_{j <= m < i} T_im W_mj, each product from shared-memory
 //            copies of T_im and W_mj staged with all loads in flight.
 template <typename T>
-__global__ void __launch_bounds__(128) diag_inverse_kernel(DevSym s, const int *__restrict__ cblks,
+__global__ void __launch_bounds__(128, 3) diag_inverse_kernel(DevSym s, const int *__restrict__ cblks,
                                                            const T *__restrict__ Lsrc, T *W,
                                                            const int64_t *__restrict__ woff, int unit) {
     extern __shared__ __align__(16) double inv_smem[];

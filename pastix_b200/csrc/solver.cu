@@ -1503,6 +1503,19 @@ int b200_spm_values_device(b200_solver_t *s, const double *d_values, double anor
     return ERR_SUCCESS;
 }
 
+int b200_get_diag(b200_solver_t *s, double *D, int64_t incD) {
+    if (!s || !D || incD <= 0) return ERR_BADPARAM;
+    if (!s->factored) return ERR_BADPARAM;  // pastixGetDiag requires the numerical factorization
+    const int n = s->n;
+    RET(ensure_ws(s, (size_t)n));
+    if (s->f32) launch_get_diag<float>(s->ds, (const float *)s->dL, s->d_ws, s->st);
+    else launch_get_diag<double>(s->ds, (const double *)s->dL, s->d_ws, s->st);
+    CU(cudaMemcpy2DAsync(D, incD * sizeof(double), s->d_ws, sizeof(double), sizeof(double), n, cudaMemcpyDeviceToHost,
+                         s->st));
+    CU(cudaStreamSynchronize(s->st));
+    return ERR_SUCCESS;
+}
+
 int b200_spm_values(b200_solver_t *s, const double *values, double anorm) {
     if (!s || s->nnz < 0 || !s->nnz_spm || !values) return ERR_BADPARAM;
     CU(cudaMemcpyAsync(s->d_spmv, values, s->nnz_spm * sizeof(double), cudaMemcpyHostToDevice, s->st));

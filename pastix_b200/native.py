@@ -24,7 +24,7 @@ _lib = None
 
 # exported symbols, in the order of include/pastix_b200.h
 SYMBOLS = ["b200_solver_create", "b200_solver_destroy", "b200_bcsc_load", "b200_bcsc_values", "b200_spm_map",
-           "b200_spm_values", "b200_spm_values_device", "b200_numfact", "b200_numfact_trace",
+           "b200_spm_values", "b200_spm_values_device", "b200_get_diag", "b200_numfact", "b200_numfact_trace",
            "b200_solve_trace", "b200_trace_launches", "b200_trace_kinds", "b200_solve",
            "b200_solve_device", "b200_solve_device_noalloc", "b200_refine", "b200_refine_device", "b200_spmv", "b200_factor_download",
            "b200_stats", "b200_strerror"]
@@ -58,6 +58,7 @@ def lib():
         L.b200_trace_launches.restype = _I64
         L.b200_bcsc_values.argtypes = [_P, _P, _P, C.c_double]
         L.b200_spm_map.argtypes = [_P, _I64, _P, _P]
+        L.b200_get_diag.argtypes = [_P, _P, _I64]
         L.b200_spm_values.argtypes = [_P, _P, C.c_double]
         L.b200_spm_values_device.argtypes = [_P, _P, C.c_double, _P]
         L.b200_trace_kinds.argtypes = [_P, _P, _P, C.c_int]
@@ -143,6 +144,12 @@ class Solver:
     def spm_values_device(self, d_values: int, anorm: float = -1.0, stream: int | None = None):
         check(lib().b200_spm_values_device(self.h, _P(d_values), anorm, _P(stream) if stream else None),
               "b200_spm_values_device")
+
+    def get_diag(self) -> np.ndarray:
+        """pastixGetDiag: the factor's diagonal in the permuted numbering."""
+        d = np.zeros(self.n)
+        check(lib().b200_get_diag(self.h, _p(d), 1), "b200_get_diag")
+        return d
 
     def numfact(self, epsilon_magn_ctrl: float = 0.0) -> int:
         piv = _I64(0)

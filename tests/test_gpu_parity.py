@@ -415,3 +415,22 @@ def test_serving_from_saved_analysis(tmp_path):
     assert np.linalg.norm(2.0 * x3 - x1) / np.linalg.norm(x1) <= 1e-11
     p1.close()
     p2.close()
+
+
+@pytest.mark.parametrize("facto,make", [CASES[1], CASES[2], CASES[3]])
+def test_get_diag_matches_oracle_factor(facto, make):
+    """pastixGetDiag: the diagonal of the factor's diagonal blocks (L's for
+    Cholesky, D for LDL^T, U's for LU) in the permuted numbering."""
+    A = make()
+    an = Analysis(A, facto)
+    st = an.structure()
+    bc = an.bcsc()
+    s = native.Solver(st, facto, "fp64")
+    s.bcsc_load(bc)
+    s.numfact(0.0)
+    d = s.get_diag()
+    orc, L, U, _ = oracle_factor(st, bc, an.facto, s.stats()["threshold"])
+    nc = st.cblk_lcolnum[:-1] - st.cblk_fcolnum[:-1] + 1
+    ref = np.concatenate([L[orc.cblkoff[k] + np.arange(nc[k]) * (nc[k] + 1)] for k in range(st.cblknbr)])
+    assert np.max(np.abs(d - ref) / np.abs(ref)) <= 1e-12
+    s.close()
