@@ -68,6 +68,15 @@ int b200_solver_create( const b200_symbol_t *symbol, int facto, int precision, v
                         b200_solver_t **solver );
 int b200_solver_destroy( b200_solver_t *solver );
 
+/* The same with a Schur complement (pastixSetSchurUnknownList, IPARM_SCHUR_SOLV_MODE =
+ * PastixSolvModeInterface): the cblks from cblkschur on (PaStiX's
+ * solvmtx->cblkschur, the CBLK_IN_SCHUR cblks) receive the updates of the others but
+ * are not factored (sopalin/sequential_zpotrf.c:51); b200_get_schur returns that
+ * block, b200_trsm solves around it.  b200_solve, b200_solve_device* and
+ * b200_refine* refuse such an instance (PASTIX_ERR_BADPARAMETER). */
+int b200_solver_create_schur( const b200_symbol_t *symbol, int facto, int precision, void *stream,
+                              int64_t cblkschur, b200_solver_t **solver );
+
 /* Load the permuted blocked CSC (bcsc/bcsc.h:28-53; pastix_subtask_spm2bcsc,
  * sopalin/pastix_task_sopalin.c:82).  colptr has n+1 entries in the permuted
  * column numbering; Lvalues holds A (both triangles for a symmetric matrix),
@@ -97,6 +106,25 @@ int b200_bcsc_values( b200_solver_t *solver, const double *Lvalues, const double
  * take new values in that order (host / device memory), permute and expand them on
  * the GPU, and set ||A||_F for the threshold (computed on the device when anorm < 0,
  * as spmNorm(SpmFrobeniusNorm)).  A new pattern in b200_bcsc_load drops the map. */
+/* pastixGetSchur (sopalin/schur.c, coeftab_zgetschur, sopalin/coeftab_z.c:413-437):
+ * the Schur complement after b200_numfact, nschur x nschur column-major in S
+ * (lds >= nschur = n - first column of the Schur part), in the permuted order of
+ * the Schur unknowns: the lower triangle for Cholesky and LDL^T, the full block for
+ * LU. */
+int b200_get_schur( b200_solver_t *solver, double *S, int64_t lds );
+
+/* pastix_subtask_applyorder (sopalin/pastix_task_solve.c:118-170): b <- P b (dir 0,
+ * to the permuted basis) or P^T b (dir 1, back). */
+int b200_applyorder( b200_solver_t *solver, int dir, int64_t nrhs, double *b, int64_t ldb );
+
+/* pastix_subtask_trsm / pastix_subtask_diag (sopalin/pastix_task_solve.c:194-407)
+ * on a permuted b (host memory): step 0 the forward sweep (L y = b, unit L for LU and
+ * LDL^T), 1 the backward sweep (L^T, U, or L^T for LDL^T with unit diagonal),
+ * 2 b <- D^{-1} b (LDL^T; no-op otherwise).  With a Schur complement the sweeps cover
+ * the unknowns before it: the forward sweep leaves b_S - A_S1 y_1 in the Schur rows,
+ * the backward sweep reads the Schur rows as the caller's solution. */
+int b200_trsm( b200_solver_t *solver, int step, int64_t nrhs, double *b, int64_t ldb );
+
 /* pastixGetDiag (sopalin/diag.c:55, coeftab_zgetdiag, sopalin/coeftab_z.c:462): the
  * diagonal of the factor's diagonal blocks in the permuted numbering (Cholesky: the
  * diagonal of L; LDL^T: D; LU: the diagonal of U), n values D[i * incD] as double.

@@ -78,6 +78,10 @@ struct b200_solver_s {
     void *dL = nullptr, *dU = nullptr;
     int *d_peri = nullptr;
     int *d_lvl_cblk = nullptr;
+    // cblks from cblkschur on form a Schur complement (CBLK_IN_SCHUR): they receive
+    // the updates of the others but are neither factored nor swept; n_active cblks
+    // and n1 unknowns (columns before the Schur part) remain
+    int cblkschur = 0, n_active = 0, n1 = 0;
     RowTask *d_trsm = nullptr, *d_stask = nullptr;
     SolveTile *d_stile = nullptr;
     std::vector<int> lvl_st0, lvl_st1;  // solve tiles of each level
@@ -201,6 +205,10 @@ struct b200_solver_s {
     }
 };
 
+extern "C" {
+static int sweep_status(b200_solver_t *s);
+}
+
 namespace {
 
 int build_schedule(b200_solver_t *s) {
@@ -214,13 +222,17 @@ int build_schedule(b200_solver_t *s) {
             level[f] = std::max(level[f], level[k] + 1);
         }
     const int nlev = N ? *std::max_element(level.begin(), level.end()) + 1 : 0;
+    // the level lists hold the cblks before the Schur complement only
+    const int cs = s->cblkschur;
+    s->n_active = cs;
+    s->n1 = cs < N ? s->fcol[cs] : s->n;
     std::vector<int> cnt(nlev + 1, 0);
-    for (int k = 0; k < N; k++) cnt[level[k] + 1]++;
+    for (int k = 0; k < cs; k++) cnt[level[k] + 1]++;
     for (int l = 0; l < nlev; l++) cnt[l + 1] += cnt[l];
-    std::vector<int> lvl_cblk(N);
+    std::vector<int> lvl_cblk(std::max(cs, 1));
     {
         std::vector<int> pos(cnt.begin(), cnt.end() - 1);
-        for (int k = 0; k < N; k++) lvl_cblk[pos[level[k]]++] = k;
+        for (int k = 0; k < cs; k++) lvl_cblk[pos[level[k]]++] = k;
     }
     std::vector<RowTask> trsm, stask;
     std::vector<SolveTile> stile;
@@ -596,7 +608,7 @@ int build_schedule(b200_solver_t *s) {
     RET(s->dupload(&s->d_diag_list, diag_list));
     {
         std::vector<int> small, big;
-        for (int k = 0; k < N; k++) (s->ncols[k] <= 32 && !is_big(k) ? small : big).push_back(k);
+        for (int k = 0; k < cs; k++) (s->ncols[k] <= 32 && !is_big(k) ? small : big).push_back(k);
         s->n_inv_small = (int)small.size();
         s->n_inv_big = (int)big.size();
         RET(s->dupload(&s->d_inv_small, small));
@@ -827,9 +839,13 @@ int enqueue_numfact(b200_solver_t *s, cudaStream_t st, Trace *tr = nullptr) {
 // exit; aux (same shape) receives the forward solution.  Per level, forward:
 // aux_k = W_L,k x_k, then x[ancestor rows] -= P_k aux_k; backward (levels in
 // reverse): aux_k -= P_k^T x[ancestor rows], then x_k = W_B,k^T aux_k.
+// parts of the sweeps: the forward sweep leaves L^{-1} b in aux (the Schur rows of
+// x updated), the backward sweep reads its input from aux
+enum { SWEEP_FORWARD = 1, SWEEP_BACKWARD = 2, SWEEP_BOTH = 3 };
+
 template <typename T>
 int enqueue_sweeps(b200_solver_t *s, T *x, T *aux, int64_t ldx, int nrhs, cudaStream_t st, int *launches,
-                   Trace *tr = nullptr) {
+                   Trace *tr = nullptr, int parts = SWEEP_BOTH) {
     const T *L = (const T *)s->dL;
     const T *Ub = (s->facto == FACTO_GETRF) ? (const T *)s->dU : L;
     const T *WL = (const T *)s->dWL;
@@ -838,7 +854,8 @@ int enqueue_sweeps(b200_solver_t *s, T *x, T *aux, int64_t ldx, int nrhs, cudaSt
     int *fl = s->d_sflags, *abort_word = fl + 2;
     CU(cudaMemsetAsync(fl, 0, ((size_t)4 * N + 4) * sizeof(int), st));
     // the diagonal products accumulate their K chunks: zero their outputs (aux now, x
-    // before the backward sweep)
+    // before the backward sweep; the Schur rows of x stay, they are the caller's)
+    if (parts & SWEEP_FORWARD) {
     CU(cudaMemset2DAsync(aux, (size_t)ldx * sizeof(T), 0, (size_t)s->n * sizeof(T), nrhs, st));
     for (int l = 0; l < fl0; l++) {
         const int nlf = s->lvl_lf1[l] - s->lvl_lf0[l];
@@ -864,13 +881,15 @@ int enqueue_sweeps(b200_solver_t *s, T *x, T *aux, int64_t ldx, int nrhs, cudaSt
         if (tr) tr->end(1, st);
         *launches += 1;
     }
-    if (s->facto == FACTO_SYTRF) {
+    }
+    if (s->facto == FACTO_SYTRF && parts == SWEEP_BOTH) {
         if (tr) tr->begin(st);
-        launch_solve_scale_diag<T>(s->ds, s->d_lvl_cblk, s->cblknbr, L, aux, ldx, nrhs, st);
+        launch_solve_scale_diag<T>(s->ds, s->d_lvl_cblk, s->n_active, L, aux, ldx, nrhs, st);
         if (tr) tr->end(3, st);
         *launches += 1;
     }
-    CU(cudaMemset2DAsync(x, (size_t)ldx * sizeof(T), 0, (size_t)s->n * sizeof(T), nrhs, st));
+    if (!(parts & SWEEP_BACKWARD)) return ERR_SUCCESS;
+    if (s->n1 > 0) CU(cudaMemset2DAsync(x, (size_t)ldx * sizeof(T), 0, (size_t)s->n1 * sizeof(T), nrhs, st));
     if (fl0 < nlev) {
         if (tr) tr->begin(st);
         launch_solve_flow<T, T>(s->ds, s->d_fitem_b, s->n_fitem_b, s->d_leaf, s->d_flist, s->d_need_b, s->d_nprev_b,
@@ -909,6 +928,38 @@ int sweeps(b200_solver_t *s, double *x, double *aux, int64_t ldx, int nrhs, cuda
     float *xf = reinterpret_cast<float *>(aux), *af = xf + (size_t)s->n * nrhs;
     launch_convert<double, float>(s->n, nrhs, x, ldx, xf, s->n, st);
     RET(enqueue_sweeps<float>(s, xf, af, s->n, nrhs, st, launches, tr));
+    launch_convert<float, double>(s->n, nrhs, xf, s->n, x, ldx, st);
+    *launches += 2;
+    return ERR_SUCCESS;
+}
+
+// One step of the solve on the permuted block x (pastix_subtask_trsm /
+// pastix_subtask_diag, sopalin/pastix_task_solve.c:194-407): 0 the forward sweep
+// (x <- L^{-1} x on the unknowns before the Schur part; the Schur rows receive the
+// contributions of the others), 1 the backward sweep (L^T or U, reading the Schur
+// rows of x as given), 2 x <- D^{-1} x (LDL^T).  aux: n x nrhs doubles of scratch.
+template <typename T>
+int sweep_step_t(b200_solver_t *s, T *x, T *aux, int64_t ldx, int nrhs, int step, cudaStream_t st, int *launches) {
+    const size_t pitch = (size_t)ldx * sizeof(T);
+    if (step == 0) {
+        RET(enqueue_sweeps<T>(s, x, aux, ldx, nrhs, st, launches, nullptr, SWEEP_FORWARD));
+        if (s->n1 > 0) CU(cudaMemcpy2DAsync(x, pitch, aux, pitch, (size_t)s->n1 * sizeof(T), nrhs, cudaMemcpyDeviceToDevice, st));
+    } else if (step == 1) {
+        if (s->n1 > 0) CU(cudaMemcpy2DAsync(aux, pitch, x, pitch, (size_t)s->n1 * sizeof(T), nrhs, cudaMemcpyDeviceToDevice, st));
+        RET(enqueue_sweeps<T>(s, x, aux, ldx, nrhs, st, launches, nullptr, SWEEP_BACKWARD));
+    } else if (s->facto == FACTO_SYTRF) {
+        launch_solve_scale_diag<T>(s->ds, s->d_lvl_cblk, s->n_active, (const T *)s->dL, x, ldx, nrhs, st);
+        *launches += 1;
+    }
+    return ERR_SUCCESS;
+}
+
+int sweep_step(b200_solver_t *s, double *x, double *aux, int64_t ldx, int nrhs, int step, cudaStream_t st,
+               int *launches) {
+    if (!s->f32) return sweep_step_t<double>(s, x, aux, ldx, nrhs, step, st, launches);
+    float *xf = reinterpret_cast<float *>(aux), *af = xf + (size_t)s->n * nrhs;
+    launch_convert<double, float>(s->n, nrhs, x, ldx, xf, s->n, st);
+    RET(sweep_step_t<float>(s, xf, af, s->n, nrhs, step, st, launches));
     launch_convert<float, double>(s->n, nrhs, xf, s->n, x, ldx, st);
     *launches += 2;
     return ERR_SUCCESS;
@@ -1274,8 +1325,14 @@ const char *b200_strerror(int code) {
 }
 
 int b200_solver_create(const b200_symbol_t *sym, int facto, int precision, void *stream, b200_solver_t **out) {
+    return sym ? b200_solver_create_schur(sym, facto, precision, stream, sym->cblknbr, out) : ERR_BADPARAM;
+}
+
+int b200_solver_create_schur(const b200_symbol_t *sym, int facto, int precision, void *stream, int64_t cblkschur,
+                             b200_solver_t **out) {
     if (!sym || !out || facto < 0 || facto > 2 || precision < 0 || precision > 3) return ERR_BADPARAM;
     if (sym->n <= 0 || sym->cblknbr <= 0 || sym->n >= (1LL << 31) || sym->bloknbr >= (1LL << 31)) return ERR_BADPARAM;
+    if (cblkschur < 1 || cblkschur > sym->cblknbr) return ERR_BADPARAM;
     int dev = 0;
     CU(cudaGetDevice(&dev));
     b200_solver_t *s = new b200_solver_t();
@@ -1300,6 +1357,7 @@ int b200_solver_create(const b200_symbol_t *sym, int facto, int precision, void 
     const int N = (int)sym->cblknbr, B = (int)sym->bloknbr;
     s->n = (int)sym->n;
     s->cblknbr = N;
+    s->cblkschur = (int)cblkschur;
     s->bloknbr = B;
     s->fcol.resize(N + 1);
     s->ncols.resize(N);
@@ -1516,6 +1574,78 @@ int b200_get_diag(b200_solver_t *s, double *D, int64_t incD) {
     return ERR_SUCCESS;
 }
 
+int b200_get_schur(b200_solver_t *s, double *S, int64_t lds) {
+    if (!s || !S || !s->factored) return ERR_BADPARAM;
+    const int cs = s->cblkschur, N = s->cblknbr;
+    const int64_t ns = s->n - s->n1;
+    if (cs >= N || lds < ns) return ERR_BADPARAM;
+    // the Schur cblks' panels sit at the end of the arena(s)
+    const int64_t off0 = s->off[cs], len = s->arena - off0;
+    std::vector<double> pl((size_t)len), pu(s->facto == FACTO_GETRF ? (size_t)len : 0);
+    auto fetch = [&](const void *arena, std::vector<double> &dst) -> int {
+        if (s->f32) {
+            std::vector<float> tmp((size_t)len);
+            CU(cudaMemcpy(tmp.data(), (const float *)arena + off0, len * sizeof(float), cudaMemcpyDeviceToHost));
+            for (int64_t i = 0; i < len; i++) dst[i] = tmp[i];
+        } else {
+            CU(cudaMemcpy(dst.data(), (const double *)arena + off0, len * sizeof(double), cudaMemcpyDeviceToHost));
+        }
+        return ERR_SUCCESS;
+    };
+    CU(cudaStreamSynchronize(s->st));
+    RET(fetch(s->dL, pl));
+    if (s->facto == FACTO_GETRF) RET(fetch(s->dU, pu));
+    // coeftab_zgetschur / cpucblk_zgetschur_fr (sopalin/coeftab_z.c:413-437,
+    // kernels/cpucblk_zschur.c:114-150): S zeroed, every block of every Schur cblk
+    // copied at (its rows, the cblk's columns); for LU the U part added transposed
+    for (int64_t j = 0; j < ns; j++) std::fill(S + j * lds, S + j * lds + ns, 0.0);
+    for (int k = cs; k < N; k++) {
+        const int64_t c0 = s->fcol[k] - s->n1, ld = s->ld[k], po = s->off[k] - off0;
+        for (int b = s->fblok[k]; b < s->fblok[k + 1]; b++) {
+            const int64_t r0 = s->frow[b] - s->n1, nr = s->lrow[b] - s->frow[b] + 1, ro = s->rowoff[b];
+            for (int64_t j = 0; j < s->ncols[k]; j++)
+                for (int64_t i = 0; i < nr; i++) {
+                    const int64_t src = po + ro + i + j * ld;
+                    S[(r0 + i) + (c0 + j) * lds] += pl[(size_t)src];
+                    if (s->facto == FACTO_GETRF) S[(c0 + j) + (r0 + i) * lds] += pu[(size_t)src];
+                }
+        }
+    }
+    return ERR_SUCCESS;
+}
+
+int b200_applyorder(b200_solver_t *s, int dir, int64_t nrhs, double *b, int64_t ldb) {
+    if (!s || (dir != 0 && dir != 1) || nrhs < 0 || ldb < s->n || (!b && nrhs)) return ERR_BADPARAM;
+    if (nrhs == 0) return ERR_SUCCESS;
+    const int n = s->n;
+    RET(ensure_ws(s, (size_t)2 * n * nrhs));
+    double *d = s->d_ws, *p = s->d_ws + (size_t)n * nrhs;
+    CU(cudaMemcpy2DAsync(d, n * sizeof(double), b, ldb * sizeof(double), n * sizeof(double), nrhs,
+                         cudaMemcpyHostToDevice, s->st));
+    launch_permute(n, (int)nrhs, s->d_peri, d, n, p, n, dir == 0 ? 1 : 0, s->st);
+    CU(cudaMemcpy2DAsync(b, ldb * sizeof(double), p, n * sizeof(double), n * sizeof(double), nrhs,
+                         cudaMemcpyDeviceToHost, s->st));
+    CU(cudaStreamSynchronize(s->st));
+    return ERR_SUCCESS;
+}
+
+int b200_trsm(b200_solver_t *s, int step, int64_t nrhs, double *b, int64_t ldb) {
+    if (!s || !s->factored || step < 0 || step > 2 || nrhs < 0 || ldb < s->n || (!b && nrhs)) return ERR_BADPARAM;
+    if (nrhs == 0) return ERR_SUCCESS;
+    const int n = s->n;
+    RET(ensure_ws(s, (size_t)2 * n * nrhs));
+    double *x = s->d_ws, *aux = s->d_ws + (size_t)n * nrhs;
+    CU(cudaMemcpy2DAsync(x, n * sizeof(double), b, ldb * sizeof(double), n * sizeof(double), nrhs,
+                         cudaMemcpyHostToDevice, s->st));
+    int launches = 0;
+    RET(sweep_step(s, x, aux, n, (int)nrhs, step, s->st, &launches));
+    s->kernel_launches += launches;
+    CU(cudaMemcpy2DAsync(b, ldb * sizeof(double), x, n * sizeof(double), n * sizeof(double), nrhs,
+                         cudaMemcpyDeviceToHost, s->st));
+    CU(cudaStreamSynchronize(s->st));
+    return sweep_status(s);
+}
+
 int b200_spm_values(b200_solver_t *s, const double *values, double anorm) {
     if (!s || s->nnz < 0 || !s->nnz_spm || !values) return ERR_BADPARAM;
     CU(cudaMemcpyAsync(s->d_spmv, values, s->nnz_spm * sizeof(double), cudaMemcpyHostToDevice, s->st));
@@ -1707,6 +1837,7 @@ int64_t b200_trace_launches(b200_solver_t *s, double *ms, int32_t *cls, int64_t 
 }
 
 int b200_solve_device(b200_solver_t *s, int64_t nrhs, double *d_b, int64_t ldb, void *stream) {
+    if (s && s->cblkschur < s->cblknbr) return ERR_BADPARAM;
     if (!s || !s->factored || nrhs < 0 || ldb < s->n) return ERR_BADPARAM;
     if (nrhs == 0) return ERR_SUCCESS;
     cudaStream_t st = stream ? (cudaStream_t)stream : s->st;
@@ -1714,6 +1845,7 @@ int b200_solve_device(b200_solver_t *s, int64_t nrhs, double *d_b, int64_t ldb, 
 }
 
 int b200_solve_device_noalloc(b200_solver_t *s, int64_t nrhs, double *d_b, int64_t ldb, void *stream) {
+    if (s && s->cblkschur < s->cblknbr) return ERR_BADPARAM;
     if (!s || !s->factored || nrhs < 0 || ldb < s->n || (!d_b && nrhs)) return ERR_BADPARAM;
     if (nrhs == 0) return ERR_SUCCESS;
     const int n = s->n;
@@ -1751,6 +1883,7 @@ static int sweep_status(b200_solver_t *s) {
 }
 
 int b200_solve(b200_solver_t *s, int64_t nrhs, double *b, int64_t ldb) {
+    if (s && s->cblkschur < s->cblknbr) return ERR_BADPARAM;  // the Schur part is the caller's: b200_trsm
     if (!s || !s->factored || nrhs < 0 || ldb < s->n || (!b && nrhs)) return ERR_BADPARAM;
     if (nrhs == 0) return ERR_SUCCESS;
     const int n = s->n;
@@ -1778,6 +1911,7 @@ int b200_solve(b200_solver_t *s, int64_t nrhs, double *b, int64_t ldb) {
 int b200_refine_device(b200_solver_t *s, int64_t nrhs, const double *d_b, int64_t ldb, double *d_x, int64_t ldx,
                        int method, double eps, int64_t itermax, int64_t gmres_im, int64_t *niter, double *berr,
                        void *stream) {
+    if (s && s->cblkschur < s->cblknbr) return ERR_BADPARAM;
     if (!s || !s->factored || nrhs < 0 || ldb < s->n || ldx < s->n || method < 0 || method > 2) return ERR_BADPARAM;
     if (nrhs == 0) return ERR_SUCCESS;
     cudaStream_t st = stream ? (cudaStream_t)stream : s->st;

@@ -23,7 +23,8 @@ _I64 = C.c_int64
 _lib = None
 
 # exported symbols, in the order of include/pastix_b200.h
-SYMBOLS = ["b200_solver_create", "b200_solver_destroy", "b200_bcsc_load", "b200_bcsc_values", "b200_spm_map",
+SYMBOLS = ["b200_solver_create", "b200_solver_destroy", "b200_solver_create_schur", "b200_get_schur",
+           "b200_applyorder", "b200_trsm", "b200_bcsc_load", "b200_bcsc_values", "b200_spm_map",
            "b200_spm_values", "b200_spm_values_device", "b200_get_diag", "b200_numfact", "b200_numfact_trace",
            "b200_solve_trace", "b200_trace_launches", "b200_trace_kinds", "b200_solve",
            "b200_solve_device", "b200_solve_device_noalloc", "b200_refine", "b200_refine_device", "b200_spmv", "b200_factor_download",
@@ -58,6 +59,10 @@ def lib():
         L.b200_trace_launches.restype = _I64
         L.b200_bcsc_values.argtypes = [_P, _P, _P, C.c_double]
         L.b200_spm_map.argtypes = [_P, _I64, _P, _P]
+        L.b200_solver_create_schur.argtypes = [_P, C.c_int, C.c_int, _P, _I64, _P]
+        L.b200_get_schur.argtypes = [_P, _P, _I64]
+        L.b200_applyorder.argtypes = [_P, C.c_int, _I64, _P, _I64]
+        L.b200_trsm.argtypes = [_P, C.c_int, _I64, _P, _I64]
         L.b200_get_diag.argtypes = [_P, _P, _I64]
         L.b200_spm_values.argtypes = [_P, _P, C.c_double]
         L.b200_spm_values_device.argtypes = [_P, _P, C.c_double, _P]
@@ -101,8 +106,15 @@ class Solver:
             st.browtab if st.browtab.size else np.zeros(1, np.int64), st.peritab)]
         sym = Symbol(st.n, st.cblknbr, st.bloknbr, st.brownbr, *[a.ctypes.data for a in self._keep])
         h = _P()
-        check(lib().b200_solver_create(C.byref(sym), self.facto, self.precision, stream, C.byref(h)),
-              "b200_solver_create")
+        cs = int(getattr(st, "cblkschur", -1))
+        self.nschur = 0
+        if 0 <= cs < st.cblknbr:
+            self.nschur = int(st.n - st.cblk_fcolnum[cs])
+            check(lib().b200_solver_create_schur(C.byref(sym), self.facto, self.precision, stream, cs, C.byref(h)),
+                  "b200_solver_create_schur")
+        else:
+            check(lib().b200_solver_create(C.byref(sym), self.facto, self.precision, stream, C.byref(h)),
+                  "b200_solver_create")
         self.h = h
 
     def close(self):
@@ -144,6 +156,25 @@ class Solver:
     def spm_values_device(self, d_values: int, anorm: float = -1.0, stream: int | None = None):
         check(lib().b200_spm_values_device(self.h, _P(d_values), anorm, _P(stream) if stream else None),
               "b200_spm_values_device")
+
+    def get_schur(self) -> np.ndarray:
+        """pastixGetSchur: the nschur x nschur Schur complement (lower triangle for
+        symmetric factorizations, full for LU), permuted order of its unknowns."""
+        S = np.zeros((self.nschur, self.nschur), order="F")
+        check(lib().b200_get_schur(self.h, _p(S), max(self.nschur, 1)), "b200_get_schur")
+        return S
+
+    def applyorder(self, b, forward: bool = True) -> np.ndarray:
+        """pastix_subtask_applyorder: P b (forward) or P^T b, on a copy."""
+        x = np.asfortranarray(np.array(b, dtype=np.float64).reshape(self.n, -1))
+        check(lib().b200_applyorder(self.h, 0 if forward else 1, x.shape[1], _p(x), self.n), "b200_applyorder")
+        return x.reshape(np.shape(b))
+
+    def trsm(self, b, step: int) -> np.ndarray:
+        """pastix_subtask_trsm / _diag on a permuted block (copy): 0 forward, 1 backward, 2 D^-1."""
+        x = np.asfortranarray(np.array(b, dtype=np.float64).reshape(self.n, -1))
+        check(lib().b200_trsm(self.h, int(step), x.shape[1], _p(x), self.n), "b200_trsm")
+        return x.reshape(np.shape(b))
 
     def get_diag(self) -> np.ndarray:
         """pastixGetDiag: the factor's diagonal in the permuted numbering."""

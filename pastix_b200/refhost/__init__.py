@@ -46,6 +46,10 @@ def lib():
         L.rh_analyze.argtypes = [C.c_int64, _I64P, _I64P, _P, C.c_int, C.c_int, C.c_int, C.c_int64,
                                  C.c_int64, C.c_int64, C.c_int, C.c_int, C.c_int, _P,
                                  C.POINTER(C.c_int)]
+        L.rh_analyze_schur.restype = _P
+        L.rh_analyze_schur.argtypes = [C.c_int64, _I64P, _I64P, _P, C.c_int, C.c_int, C.c_int, C.c_int64,
+                                       C.c_int64, C.c_int64, C.c_int, C.c_int, C.c_int, _P, C.c_int64, _P,
+                                       C.POINTER(C.c_int)]
         L.rh_sizes.argtypes = [_P, _I64P]
         L.rh_export_solver.argtypes = [_P] + [_I64P] * 7 + [_I32P] + [_I64P] * 7
         L.rh_export_perm.argtypes = [_P, _I64P, _I64P]
@@ -109,6 +113,7 @@ class SolverStructure:
     permtab: np.ndarray
     peritab: np.ndarray
     thflops: float
+    cblkschur: int = -1  # first cblk of the Schur complement (cblknbr: none)
     extra: dict = field(default_factory=dict)
 
     @property
@@ -131,7 +136,10 @@ class Analysis:
     """One PaStiX instance after ``pastix_task_analyze`` (grid ND ordering)."""
 
     def __init__(self, A, facto: str = "potrf", nthreads: int = 1, verbose: bool = False,
-                 iparm: dict | None = None, flttype: int = 3):
+                 iparm: dict | None = None, flttype: int = 3, schur=None):
+        """schur: unknowns (0-based, original numbering) of a Schur complement
+        (pastixSetSchurUnknownList); they must be the last ones of the grid ordering
+        (``schur_candidates`` gives them)."""
         L = lib()
         self.A = A
         self.facto_name = facto
@@ -146,11 +154,13 @@ class Analysis:
         vals = np.ascontiguousarray(A.values, dtype=np.float32 if flttype == 2 else np.float64)
         self._vals = vals
         nx, ny, nz = A.grid
-        self.h = L.rh_analyze(A.n, np.ascontiguousarray(A.colptr, dtype=np.int64),
-                              np.ascontiguousarray(A.rowind, dtype=np.int64),
-                              vals.ctypes.data_as(C.c_void_p), 0 if not A.symmetric else 1,
-                              flttype, self.facto, nx, ny, nz, nthreads, 1 if verbose else 0,
-                              len(kv) // 2, kva.ctypes.data_as(C.c_void_p), C.byref(info))
+        sl = np.ascontiguousarray(schur if schur is not None else np.zeros(0), dtype=np.int64)
+        self.h = L.rh_analyze_schur(A.n, np.ascontiguousarray(A.colptr, dtype=np.int64),
+                                    np.ascontiguousarray(A.rowind, dtype=np.int64),
+                                    vals.ctypes.data_as(C.c_void_p), 0 if not A.symmetric else 1,
+                                    flttype, self.facto, nx, ny, nz, nthreads, 1 if verbose else 0,
+                                    len(kv) // 2, kva.ctypes.data_as(C.c_void_p), sl.size,
+                                    sl.ctypes.data_as(C.c_void_p) if sl.size else None, C.byref(info))
         if info.value != 0:
             raise RuntimeError(f"PaStiX analysis failed: {info.value}")
         self._bcsc_done = False
@@ -164,7 +174,7 @@ class Analysis:
             pass
 
     def sizes(self):
-        s = np.zeros(10, dtype=np.int64)
+        s = np.zeros(11, dtype=np.int64)
         lib().rh_sizes(self.h, s)
         return s
 
@@ -180,7 +190,16 @@ class Analysis:
         peri = np.zeros(n, dtype=np.int64)
         lib().rh_export_perm(self.h, perm, peri)
         return SolverStructure(n, cblknbr, bloknbr, brownbr, coefnbr, self.facto, *c, ctype, *b,
-                               brow[:brownbr], perm, peri, float(lib().rh_thflops(self.h)))
+                               brow[:brownbr], perm, peri, float(lib().rh_thflops(self.h)), int(s[10]))
+
+    def schur_candidates(self, nschur: int):
+        """The last nschur unknowns of the grid ordering (original numbering), a valid
+        Schur list when a cblk boundary of this analysis falls at n - nschur."""
+        st = self.structure()
+        bounds = set(int(x) for x in st.cblk_fcolnum[:st.cblknbr])
+        if st.n - nschur not in bounds:
+            raise ValueError("n - nschur is not a cblk boundary of the ordering")
+        return np.sort(st.peritab[st.n - nschur:])
 
     def bcsc(self, values=None) -> BCSC:
         """pastix_subtask_spm2bcsc with the given values (same pattern), exported."""

@@ -37,10 +37,31 @@ typedef struct rh_s {
  * flttype: 2 float, 3 double.  facto: PastixFactPOTRF=0, SYTRF=1, GETRF=2.
  * kv is a list of nkv (index,value) pairs applied to iparm before pastixInit;
  * the indices come from rh_param_ids(). */
+/* Same with a Schur complement (pastixSetSchurUnknownList, sopalin/schur.c): the
+ * nschur unknowns of schur_list (0-based, original numbering) must be the last ones
+ * of the grid ordering, as PaStiX requires of a personal ordering
+ * (order/pastix_subtask_order.c:145-153); the symbolic factorization then starts the
+ * Schur part at column n - nschur and blend marks those cblks CBLK_IN_SCHUR. */
+void *
+rh_analyze_schur( int64_t n, const int64_t *colptr, const int64_t *rowind, const void *values,
+                  int mtxtype, int flttype, int facto, int64_t nx, int64_t ny, int64_t nz,
+                  int nthreads, int verbose, int nkv, const int64_t *kv, int64_t nschur,
+                  const int64_t *schur_list, int *info );
+
 void *
 rh_analyze( int64_t n, const int64_t *colptr, const int64_t *rowind, const void *values,
             int mtxtype, int flttype, int facto, int64_t nx, int64_t ny, int64_t nz,
             int nthreads, int verbose, int nkv, const int64_t *kv, int *info )
+{
+    return rh_analyze_schur( n, colptr, rowind, values, mtxtype, flttype, facto, nx, ny, nz, nthreads,
+                             verbose, nkv, kv, 0, NULL, info );
+}
+
+void *
+rh_analyze_schur( int64_t n, const int64_t *colptr, const int64_t *rowind, const void *values,
+                  int mtxtype, int flttype, int facto, int64_t nx, int64_t ny, int64_t nz,
+                  int nthreads, int verbose, int nkv, const int64_t *kv, int64_t nschur,
+                  const int64_t *schur_list, int *info )
 {
     rh_t *h = calloc( 1, sizeof(rh_t) );
     pastix_order_t *ord = NULL;
@@ -77,6 +98,10 @@ rh_analyze( int64_t n, const int64_t *colptr, const int64_t *rowind, const void 
         h->iparm[kv[2 * i]] = kv[2 * i + 1];
     }
     pastixInit( &h->pastix_data, MPI_COMM_WORLD, h->iparm, h->dparm );
+    if ( nschur > 0 ) {
+        pastixSetSchurUnknownList( h->pastix_data, nschur, schur_list );
+        h->iparm[IPARM_SCHUR_SOLV_MODE] = PastixSolvModeInterface;
+    }
 
     /* pastixOrderGrid fills a caller-allocated order (order/order_grids.c:306);
      * grid vertex (i,j,k) is numbered i + nx*j + nx*ny*k. */
@@ -126,7 +151,8 @@ rh_dparm( void *vh )
     return ((rh_t *)vh)->dparm;
 }
 
-/* sizes[0..9] = n, cblknbr, bloknbr, brownbr, coefnbr, bcsc nnz, facto, flttype, gN, cblkmaxblk */
+/* sizes[0..10] = n, cblknbr, bloknbr, brownbr, coefnbr, bcsc nnz, facto, flttype, gN, cblkmaxblk,
+ * cblkschur (first cblk of the Schur complement; cblknbr without one) */
 void
 rh_sizes( void *vh, int64_t *sizes )
 {
@@ -145,6 +171,7 @@ rh_sizes( void *vh, int64_t *sizes )
     sizes[7] = h->spm.flttype;
     sizes[8] = h->spm.gN;
     sizes[9] = s->cblkmaxblk;
+    sizes[10] = s->cblkschur;
 }
 
 /* cblk arrays have cblknbr+1 entries (the sentinel cblk is exported too);

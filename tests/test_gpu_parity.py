@@ -434,3 +434,48 @@ def test_get_diag_matches_oracle_factor(facto, make):
     ref = np.concatenate([L[orc.cblkoff[k] + np.arange(nc[k]) * (nc[k] + 1)] for k in range(st.cblknbr)])
     assert np.max(np.abs(d - ref) / np.abs(ref)) <= 1e-12
     s.close()
+
+
+@pytest.mark.parametrize("facto,make", [
+    ("potrf", lambda: M.laplacian(8, 8, 8, 7, 6.0)),
+    ("getrf", lambda: M.convection_diffusion(8, 8, 8, seed=3)),
+    ("sytrf", lambda: M.laplacian(8, 8, 8, 7, 6.0, shift=-0.7)),
+])
+def test_schur_complement_and_solve_around_it(facto, make):
+    """Schur complement (pastixSetSchurUnknownList / pastixGetSchur, example/schur.c):
+    the Schur block equals A22 - A21 A11^-1 A12 of the permuted matrix, and the solve
+    forward sweep -> (D^-1) -> caller's dense Schur solve -> backward sweep gives
+    A^-1 b."""
+    A = make()
+    st0 = Analysis(A, facto).structure()
+    ns = int(st0.cblk_lcolnum[st0.cblknbr - 1] - st0.cblk_fcolnum[st0.cblknbr - 1] + 1)
+    an = Analysis(A, facto, schur=Analysis(A, facto).schur_candidates(ns))
+    st = an.structure()
+    assert st.cblkschur == st.cblknbr - 1
+    s = native.Solver(st, facto, "fp64")
+    s.bcsc_load(an.bcsc())
+    s.numfact(0.0)
+    S = s.get_schur()
+    Ad = A.to_dense()
+    P = st.peritab
+    Ap = Ad[np.ix_(P, P)]
+    n1 = A.n - ns
+    Sref = Ap[n1:, n1:] - Ap[n1:, :n1] @ np.linalg.solve(Ap[:n1, :n1], Ap[:n1, n1:])
+    if facto == "getrf":
+        assert np.linalg.norm(S - Sref) <= 1e-12 * np.linalg.norm(Sref)
+        Sfull = S
+    else:
+        assert np.linalg.norm(np.tril(S) - np.tril(Sref)) <= 1e-12 * np.linalg.norm(np.tril(Sref))
+        assert np.all(np.triu(S, 1) == 0.0)
+        Sfull = np.tril(S) + np.tril(S, -1).T
+    xt, b = M.rhs_from_xtrue(A, 2, seed=8)
+    y = s.trsm(s.applyorder(b, True), 0)
+    if facto == "sytrf":
+        y = s.trsm(y, 2)
+    y[n1:] = np.linalg.solve(Sfull, y[n1:])
+    x = s.applyorder(s.trsm(y, 1), False)
+    assert np.linalg.norm(x - xt) / np.linalg.norm(xt) <= 1e-10
+    assert backward_error(A, x, b).max() <= 1e-13
+    with pytest.raises(Exception):
+        s.solve(b)  # the full solve does not apply with a Schur complement
+    s.close()

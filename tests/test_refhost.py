@@ -95,3 +95,23 @@ def test_saved_analysis_round_trip(tmp_path):
     assert sv.facto == "potrf" and sv.umap is None and sv.nnz_spm == A.values.size
     assert np.array_equal(A.values[sv.lmap], bc.Lvalues)
     assert np.array_equal(sv.a_colptr, A.colptr) and sv.a_symmetric == A.symmetric
+
+
+def test_schur_analysis_puts_the_schur_unknowns_last():
+    """pastixSetSchurUnknownList with the grid ordering's last cblk: blend marks it
+    CBLK_IN_SCHUR (blend/solver.h:46), cblkschur points at it, and the Schur unknowns
+    are the last ones of the permutation."""
+    A = M.laplacian(8, 8, 8, 7, 6.0)
+    st0 = Analysis(A, "potrf").structure()
+    ns = int(st0.cblk_lcolnum[st0.cblknbr - 1] - st0.cblk_fcolnum[st0.cblknbr - 1] + 1)
+    an = Analysis(A, "potrf")
+    sl = an.schur_candidates(ns)
+    st = Analysis(A, "potrf", schur=sl).structure()
+    assert st0.cblkschur == st0.cblknbr
+    assert st.cblkschur == st.cblknbr - 1
+    assert st.cblk_fcolnum[st.cblkschur] == A.n - ns
+    assert all(int(t) & 16 for t in st.cblk_type[st.cblkschur:st.cblknbr])
+    assert not any(int(t) & 16 for t in st.cblk_type[:st.cblkschur])
+    assert set(st.peritab[A.n - ns:].tolist()) == set(sl.tolist())
+    with pytest.raises(ValueError):
+        an.schur_candidates(ns + 1)
