@@ -43,11 +43,17 @@ class PastixB200:
         self.structure = None
         self.solver = None
         self.out = {}
+        self.schur_list = None
+
+    # pastixSetSchurUnknownList (sopalin/schur.c): before task_analyze; with the grid
+    # ordering the list must be its last unknowns (Analysis.schur_candidates)
+    def set_schur_unknown_list(self, unknowns):
+        self.schur_list = np.ascontiguousarray(unknowns, dtype=np.int64)
 
     # pastix_task_analyze (blend/pastix_task_analyze.c:52)
     def task_analyze(self, A):
         ip = {"MIN_BLOCKSIZE": self.iparm["MIN_BLOCKSIZE"], "MAX_BLOCKSIZE": self.iparm["MAX_BLOCKSIZE"]}
-        self.analysis = Analysis(A, self.iparm["FACTORIZATION"], iparm=ip)
+        self.analysis = Analysis(A, self.iparm["FACTORIZATION"], iparm=ip, schur=self.schur_list)
         self.structure = self.analysis.structure()
         self.out["FACT_THFLOPS"] = self.structure.thflops
         if self.solver is not None:
@@ -119,6 +125,24 @@ class PastixB200:
         self.out["RELATIVE_ERROR"] = float(np.max(berr)) if berr.size else 0.0
         self.out["REFINE_TIME"] = self.solver.stats()["refine_ms"] / 1e3
         return x
+
+    # pastixGetSchur (sopalin/schur.c) and pastixGetDiag (sopalin/diag.c:55)
+    def get_schur(self):
+        return self.solver.get_schur()
+
+    def get_diag(self):
+        return self.solver.get_diag()
+
+    # pastix_subtask_applyorder / pastix_subtask_trsm / pastix_subtask_diag
+    # (sopalin/pastix_task_solve.c:118-407) for solves around a Schur complement
+    def subtask_applyorder(self, b, forward: bool = True):
+        return self.solver.applyorder(b, forward)
+
+    def subtask_trsm(self, b, backward: bool = False):
+        return self.solver.trsm(b, 1 if backward else 0)
+
+    def subtask_diag(self, b):
+        return self.solver.trsm(b, 2)
 
     def close(self):
         if self.solver is not None:
