@@ -142,6 +142,28 @@ __device__ __forceinline__ void stage_tile(T *ms, const T *M, int64_t ldm, int g
     }
 }
 
+// The same tile in 16-byte chunks when every column of M starts on a 16-byte
+// boundary (ldm a multiple of 16 / sizeof(T) and M aligned): the rows from gr0
+// rounded down to a chunk boundary are copied as they are (chunks past nr zero
+// filled), so the tile starts at ms + shift with shift = gr0 % (16 / sizeof(T)) < 4;
+// a column takes at most 68 entries of its PM >= 68.  Returns shift.
+template <typename T, int PM>
+__device__ __forceinline__ int stage_tile16(T *ms, const T *M, int64_t ldm, int gr0, int gc0, int nr, int nc) {
+    constexpr int EPV = 16 / sizeof(T);
+    const int shift = gr0 % EPV, gr0a = gr0 - shift;
+    const int cpc = (STT + shift + EPV - 1) / EPV;  // chunks per column
+    for (int idx = threadIdx.x; idx < STT * cpc; idx += blockDim.x) {
+        const int c = idx / cpc, i = idx % cpc;
+        const int row = gr0a + i * EPV;
+        int bytes = 0;
+        if (gc0 + c < nc && row < nr) bytes = (nr - row >= EPV ? EPV : nr - row) * (int)sizeof(T);
+        const T *src = bytes ? M + row + (size_t)(gc0 + c) * ldm : M;
+        asm volatile("cp.async.cg.shared.global [%0], [%1], 16, %2;\n" ::"r"(sm_addr(ms + c * PM + i * EPV)), "l"(src),
+                     "r"(bytes));
+    }
+    return shift;
+}
+
 // x tile: xs[i * XP + j] = xv[i][q0 + j] for i < ni, j < R (zeros elsewhere); rows
 // either contiguous from xv (rowmap null) or gathered through rowmap.
 template <typename V>
@@ -271,11 +293,12 @@ __global__ void __launch_bounds__(128) solve_mm_kernel(DevSym s, const SolveTile
     const V *xsrc;
     const int *xmap = nullptr;
     int nk;
+    int shift = 0;  // the staged tile starts at ms + shift
     if (MODE == OFF_FWD || MODE == OFF_BWD) {
         const int rows = min(STT, s.stride[k] - t.row0), cols = min(STT, n - t.col0);
         if (tid < STT) rmap[tid] = (tid < rows) ? panel_row_to_global(s, k, t.row0 + tid) : 0;
         __syncthreads();
-        stage_tile<T, PM>(ms, M + s.off[k], s.ld[k], t.row0, t.col0, s.stride[k], n);
+        shift = stage_tile16<T, PM>(ms, M + s.off[k], s.ld[k], t.row0, t.col0, s.stride[k], n);
         nout = ROW ? rows : cols;
         nk = ROW ? cols : rows;
         if (MODE == OFF_FWD) xsrc = xin + s.fcol[k] + t.col0;
@@ -284,8 +307,13 @@ __global__ void __launch_bounds__(128) solve_mm_kernel(DevSym s, const SolveTile
         const T *Wk = M + woff[k];
         nout = min(STT, n - t.row0);
         nk = min(STT, n - t.col0);
-        if (MODE == DIAG_FWD) stage_tile<T, PM>(ms, Wk, n, t.row0, t.col0, n, n);  // W[o][k]
-        else stage_tile<T, PM>(ms, Wk, n, t.col0, t.row0, n, n);                   // W[k][o]
+        if (n % (16 / (int)sizeof(T)) == 0) {
+            if (MODE == DIAG_FWD) shift = stage_tile16<T, PM>(ms, Wk, n, t.row0, t.col0, n, n);  // W[o][k]
+            else shift = stage_tile16<T, PM>(ms, Wk, n, t.col0, t.row0, n, n);                   // W[k][o]
+        } else {
+            if (MODE == DIAG_FWD) stage_tile<T, PM>(ms, Wk, n, t.row0, t.col0, n, n);
+            else stage_tile<T, PM>(ms, Wk, n, t.col0, t.row0, n, n);
+        }
         xsrc = xin + s.fcol[k] + t.col0;
     }
     for (int q0 = 0; q0 < nrhs; q0 += SRHS) {
@@ -297,7 +325,7 @@ __global__ void __launch_bounds__(128) solve_mm_kernel(DevSym s, const SolveTile
         __syncthreads();
         if (o0w < nout) {
             V acc[4][4] = {};
-            tile_mma<T, PM, ROW>(acc, ms, xs, o0w, ntn);
+            tile_mma<T, PM, ROW>(acc, ms + shift, xs, o0w, ntn);
             const V sg = (MODE == OFF_FWD || MODE == OFF_BWD) ? (V)-1 : (V)1;
 #pragma unroll
             for (int nt = 0; nt < 4; nt++) {
@@ -709,7 +737,7 @@ __global__ void __launch_bounds__(FLOW_THREADS) solve_flow_kernel(DevSym s, cons
             T *ms = reinterpret_cast<T *>(fl_smem);
             V *xs = reinterpret_cast<V *>(fl_smem + STT * SM_FWD * sizeof(T));
             const int k = it.k, n = s.ncols[k], c0 = it.n;
-            int nout, nk;
+            int nout, nk, shift = 0;
             const V *xsrc;
             const int *xmap = nullptr;
             if (it.type == FI_DIAG) {
@@ -717,14 +745,19 @@ __global__ void __launch_bounds__(FLOW_THREADS) solve_flow_kernel(DevSym s, cons
                 nout = min(STT, n - it.r0);
                 nk = min(STT, n - c0);
                 // forward W[o][kk] (row form); backward W[kk][o] (W^T, column form)
-                if (!BWD) stage_tile<T, SM_FWD>(ms, Wk, n, it.r0, c0, n, n);
-                else stage_tile<T, SM_BWD>(ms, Wk, n, c0, it.r0, n, n);
+                if (n % (16 / (int)sizeof(T)) == 0) {
+                    if (!BWD) shift = stage_tile16<T, SM_FWD>(ms, Wk, n, it.r0, c0, n, n);
+                    else shift = stage_tile16<T, SM_BWD>(ms, Wk, n, c0, it.r0, n, n);
+                } else {
+                    if (!BWD) stage_tile<T, SM_FWD>(ms, Wk, n, it.r0, c0, n, n);
+                    else stage_tile<T, SM_BWD>(ms, Wk, n, c0, it.r0, n, n);
+                }
                 xsrc = (BWD ? aux : x) + s.fcol[k] + c0;
             } else {
                 const int rows = min(STT, s.stride[k] - it.r0), cols = min(STT, n - c0);
                 if (tid < STT) rmap[tid] = (tid < rows) ? panel_row_to_global(s, k, it.r0 + tid) : 0;
-                if (!BWD) stage_tile<T, SM_FWD>(ms, P + s.off[k], s.ld[k], it.r0, c0, s.stride[k], n);
-                else stage_tile<T, SM_BWD>(ms, P + s.off[k], s.ld[k], it.r0, c0, s.stride[k], n);
+                if (!BWD) shift = stage_tile16<T, SM_FWD>(ms, P + s.off[k], s.ld[k], it.r0, c0, s.stride[k], n);
+                else shift = stage_tile16<T, SM_BWD>(ms, P + s.off[k], s.ld[k], it.r0, c0, s.stride[k], n);
                 nout = BWD ? cols : rows;
                 nk = BWD ? rows : cols;
                 if (!BWD) xsrc = aux + s.fcol[k] + c0;
@@ -741,8 +774,8 @@ __global__ void __launch_bounds__(FLOW_THREADS) solve_flow_kernel(DevSym s, cons
                 if (o0w < nout) {
                     V acc[4][4] = {};
                     const bool row = !BWD;  // forward: outputs are tile rows; backward: tile columns
-                    if (row) tile_mma<T, SM_FWD, 1>(acc, ms, xs, o0w, ntn);
-                    else tile_mma<T, SM_BWD, 0>(acc, ms, xs, o0w, ntn);
+                    if (row) tile_mma<T, SM_FWD, 1>(acc, ms + shift, xs, o0w, ntn);
+                    else tile_mma<T, SM_BWD, 0>(acc, ms + shift, xs, o0w, ntn);
                     // DIAG: + into aux_k (forward) / x_k (backward); OFF: - into x[rows] / aux_k
                     const V sg = it.type == FI_DIAG ? (V)1 : (V)-1;
                     V *dst;
