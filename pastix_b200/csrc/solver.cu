@@ -123,6 +123,10 @@ struct b200_solver_s {
     std::vector<int> lvl_prows;         // row-block form: rows of the blocks below the diagonal (0: tile items)
     std::vector<int> lvl_pns;           // most 64-column steps of a cblk of the level
     bool panel_steps_only = false;      // environment B200_PANEL_TILES=1: always the tile-item form
+    // failure-path tests (environment B200_TEST_WITHHOLD=panel|flow): the first item of
+    // every panel launch / of the forward dataflow sweep is never taken, so the waits
+    // that depend on it run out and the error path is exercised
+    int test_withhold = 0;
     PanelCblk *d_pcb = nullptr;
     PanelItem *d_pitem = nullptr;
     // [nlev tickets][solved counters][updated counters][abort word], zeroed per factorization
@@ -742,6 +746,9 @@ int enqueue_numfact(b200_solver_t *s, cudaStream_t st, Trace *tr = nullptr) {
     CU(cudaMemsetAsync(s->d_npiv, 0, sizeof(unsigned long long), st));
     CU(cudaMemsetAsync(s->d_err, 0, sizeof(int), st));
     CU(cudaMemsetAsync(s->d_pflags, 0, (size_t)s->n_pflags * sizeof(int), st));
+    if (s->test_withhold & 1)
+        for (size_t l = 0; l < s->levels.size(); l++)
+            if (s->lvl_pi1[l] > s->lvl_pi0[l]) CU(cudaMemsetAsync(s->d_pflags + l, 1, 1, st));  // ticket = 1
     launch_scatter<T>(s->nnz, s->d_dest, s->d_Lv, s->d_Uv, L, U, st);
     if (tr) tr->end(0, st);
     launches++;
@@ -853,6 +860,7 @@ int enqueue_sweeps(b200_solver_t *s, T *x, T *aux, int64_t ldx, int nrhs, cudaSt
     const int N = s->cblknbr, nlev = (int)s->levels.size(), fl0 = s->flow_level;
     int *fl = s->d_sflags, *abort_word = fl + 2;
     CU(cudaMemsetAsync(fl, 0, ((size_t)4 * N + 4) * sizeof(int), st));
+    if (s->test_withhold & 2) CU(cudaMemsetAsync(fl, 1, 1, st));  // forward ticket = 1
     // the diagonal products accumulate their K chunks: zero their outputs (aux now, x
     // before the backward sweep; the Schur rows of x stay, they are the caller's)
     if (parts & SWEEP_FORWARD) {
@@ -1345,6 +1353,8 @@ int b200_solver_create_schur(const b200_symbol_t *sym, int facto, int precision,
     if (const char *e = getenv("B200_TC_MIN_K")) s->tc_min_k = std::max(1, atoi(e));
     if (const char *e = getenv("B200_TC_MIN_M")) s->tc_min_m = std::max(1, atoi(e));
     if (const char *e = getenv("B200_PANEL_TILES")) s->panel_steps_only = atoi(e) != 0;
+    if (const char *e = getenv("B200_TEST_WITHHOLD"))
+        s->test_withhold = !strcmp(e, "panel") ? 1 : !strcmp(e, "flow") ? 2 : 0;
     if (stream) {
         s->st = (cudaStream_t)stream;
     } else {

@@ -479,3 +479,41 @@ def test_schur_complement_and_solve_around_it(facto, make):
     with pytest.raises(Exception):
         s.solve(b)  # the full solve does not apply with a Schur complement
     s.close()
+
+
+def test_bounded_waits_report_errors(monkeypatch):
+    """The dependency-counter waits of the panel launches and of the dataflow sweeps
+    are bounded: with the first item withheld (a counter nothing raises), the launch
+    gives up within about a second, b200_numfact / b200_solve report the error, and a
+    fresh instance works."""
+    import time
+    A = M.laplacian(20, 20, 20, 7, 6.0)
+    an = Analysis(A, "potrf")
+    st = an.structure()
+    bc = an.bcsc()
+    assert np.max(st.cblk_lcolnum[:-1] - st.cblk_fcolnum[:-1] + 1) > 96  # wide cblks: panel launches
+    xt, b = M.rhs_from_xtrue(A, 2, seed=4)
+    monkeypatch.setenv("B200_TEST_WITHHOLD", "panel")
+    s = native.Solver(st, "potrf", "fp64")
+    s.bcsc_load(bc)
+    t0 = time.perf_counter()
+    with pytest.raises(native.B200Error):
+        s.numfact(0.0)
+    assert time.perf_counter() - t0 < 30.0
+    s.close()
+    monkeypatch.setenv("B200_TEST_WITHHOLD", "flow")
+    s = native.Solver(st, "potrf", "fp64")
+    s.bcsc_load(bc)
+    s.numfact(0.0)
+    t0 = time.perf_counter()
+    with pytest.raises(native.B200Error):
+        s.solve(b)
+    assert time.perf_counter() - t0 < 30.0
+    s.close()
+    monkeypatch.delenv("B200_TEST_WITHHOLD")
+    s = native.Solver(st, "potrf", "fp64")
+    s.bcsc_load(bc)
+    s.numfact(0.0)
+    x = s.solve(b)
+    assert backward_error(A, x, b).max() <= BERR_FP64
+    s.close()
