@@ -82,7 +82,7 @@ struct b200_solver_s {
     // the updates of the others but are neither factored nor swept; n_active cblks
     // and n1 unknowns (columns before the Schur part) remain
     int cblkschur = 0, n_active = 0, n1 = 0;
-    RowTask *d_trsm = nullptr, *d_stask = nullptr;
+    RowTask *d_trsm = nullptr;
     SolveTile *d_stile = nullptr;
     std::vector<int> lvl_st0, lvl_st1;  // solve tiles of each level
     SolveTile *d_dtask = nullptr;       // 64 x 64 tiles of the diagonal-block inverses, forward (lower)
@@ -151,7 +151,6 @@ struct b200_solver_s {
     SplitTask *d_split = nullptr;
     std::vector<int> lvl_sp0, lvl_sp1;    // operand copies of each level (before its external updates)
     std::vector<int> lvl_tr;            // TRSM rows per task of each level
-    std::vector<int> lvl_s0, lvl_s1;    // solve row tasks of each level
     int nmax_all = 0;
     int64_t total_tiles = 0;
     int trsm_smem = 0;                  // dynamic shared memory available to the panel TRSM
@@ -238,7 +237,7 @@ int build_schedule(b200_solver_t *s) {
         std::vector<int> pos(cnt.begin(), cnt.end() - 1);
         for (int k = 0; k < cs; k++) lvl_cblk[pos[level[k]]++] = k;
     }
-    std::vector<RowTask> trsm, stask;
+    std::vector<RowTask> trsm;
     std::vector<SolveTile> stile;
     std::vector<Upd> upds;
     std::vector<int> diag_list;
@@ -311,8 +310,6 @@ int build_schedule(b200_solver_t *s) {
     s->lvl_lf1.assign(nlev, 0);
     s->levels.assign(nlev, Level{});
     s->lvl_tr.assign(nlev, 64);
-    s->lvl_s0.assign(nlev, 0);
-    s->lvl_s1.assign(nlev, 0);
     std::vector<int> src_count(N, 0), src_last(N, -1);
     const size_t trsm_smem = (size_t)s->trsm_smem;
     for (int l = 0; l < nlev; l++) {
@@ -330,7 +327,6 @@ int build_schedule(b200_solver_t *s) {
         if ((size_t)TR * L.nmax * s->esz > trsm_smem) return ERR_NOTIMPL;
         s->lvl_tr[l] = TR;
         L.t0 = (int)trsm.size();
-        s->lvl_s0[l] = (int)stask.size();
         s->lvl_st0[l] = (int)stile.size();
         s->lvl_dt0[l] = (int)dtask.size();
         s->lvl_db0[l] = (int)dtaskb.size();
@@ -394,7 +390,6 @@ int build_schedule(b200_solver_t *s) {
             const int k = lvl_cblk[i];
             if (!is_big(k))
                 for (int r0 = s->ncols[k]; r0 < s->stride[k]; r0 += TR) trsm.push_back({k, r0});
-            for (int r0 = s->ncols[k]; r0 < s->stride[k]; r0 += 128) stask.push_back({k, r0});
             if (s->ncols[k] <= 32) {
                 // small cblk: both parts of each sweep in the one-warp kernel
                 leaf.push_back(k);
@@ -415,7 +410,6 @@ int build_schedule(b200_solver_t *s) {
         s->lvl_dt1[l] = (int)dtask.size();
         s->lvl_db1[l] = (int)dtaskb.size();
         L.t1 = (int)trsm.size();
-        s->lvl_s1[l] = (int)stask.size();
         // number of sources of this level facing each cblk
         for (int i = L.c0; i < L.c1; i++) {
             const int k = lvl_cblk[i];
@@ -521,7 +515,6 @@ int build_schedule(b200_solver_t *s) {
     }
     RET(s->dupload(&s->d_lvl_cblk, lvl_cblk));
     RET(s->dupload(&s->d_trsm, trsm));
-    RET(s->dupload(&s->d_stask, stask));
     RET(s->dupload(&s->d_stile, stile));
     RET(s->dupload(&s->d_dtask, dtask));
     RET(s->dupload(&s->d_dtaskb, dtaskb));
