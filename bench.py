@@ -273,19 +273,28 @@ def e2e_path(solver, an, A, b, prec, refine, nrhs, reps=3):
     vp, _tv = pinned_like(np.ascontiguousarray(A.values, dtype=np.float64))
     bp, _tb = pinned_like(np.asfortranarray(b), order="F")
     xp, _tx = pinned_like(np.asfortranarray(b), order="F")
-    ts = []
+    ts, ph = [], []
     for _ in range(reps):
-        t0 = time.perf_counter()
+        t = [time.perf_counter()]
         solver.spm_values(vp, -1.0)
+        t.append(time.perf_counter())
         solver.numfact(0.0)
+        t.append(time.perf_counter())
         np.copyto(xp, bp)
+        t.append(time.perf_counter())
         solver.solve(xp, inplace=True)
+        t.append(time.perf_counter())
         if refine:
             solver.refine(bp, xp, "cg", BERR_TARGET, 50, 25, inplace=True)
-        ts.append(time.perf_counter() - t0)
+        t.append(time.perf_counter())
+        ts.append(t[-1] - t[0])
+        ph.append(np.diff(t))
     h2d = vp.nbytes + b.nbytes * (3 if refine else 1)
     d2h = b.nbytes * (2 if refine else 1)
-    return float(np.median(ts)), int(h2d), int(d2h)
+    # host wall time of each call of the median step (every call returns synchronised)
+    med = ph[int(np.argsort(ts)[len(ts) // 2])] * 1e3
+    phases = dict(zip(["spm_values", "numfact", "copy_b", "solve", "refine"], [round(float(v), 3) for v in med]))
+    return float(np.median(ts)), int(h2d), int(d2h), phases
 
 
 def main():
@@ -411,7 +420,7 @@ def main():
 
     hs, _ = solvers[head["prec"]]
     p50, p99 = solve_latency(hs, A, b, stream, device_b, device_x, nrhs)
-    e2e_s, h2d, d2h = e2e_path(hs, an, A, b, head["prec"], head["prec"] != "fp64", nrhs)
+    e2e_s, h2d, d2h, e2e_phases = e2e_path(hs, an, A, b, head["prec"], head["prec"] != "fp64", nrhs, reps=5)
     e2e_value = world * st.thflops / e2e_s / 1e9
 
     # roofline of the dominant kernel of the headline path: the update kind with
@@ -461,7 +470,7 @@ def main():
             "roofline": roofline,
             "cpu_baseline": cpu,
             "e2e": {"value": e2e_value, "unit": "GFLOP/s", "h2d_bytes_per_step": h2d, "d2h_bytes_per_step": d2h,
-                    "seconds_per_step": e2e_s, "host_buffers": "pinned",
+                    "seconds_per_step": e2e_s, "host_buffers": "pinned", "phases_ms": e2e_phases,
                     "step": "b200_spm_values (bcsc built on the GPU) + b200_numfact + host copy x=b + b200_solve + b200_refine"},
             "gpu_launches": int(sum(r["launches"] for r in results.values())),
             "clocks": clocks,
