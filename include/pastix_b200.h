@@ -131,6 +131,30 @@ int b200_trsm( b200_solver_t *solver, int step, int64_t nrhs, double *b, int64_t
  * Requires a completed b200_numfact. */
 int b200_get_diag( b200_solver_t *solver, double *D, int64_t incD );
 
+/* Batch of independent systems.  The reference factors each system through its own
+ * pastix_task_numfact / pastix_task_solve / pastix_task_refine
+ * (sopalin/pastix_task_sopalin.c:563, sopalin/pastix_task_solve.c:550,
+ * refinement/pastix_task_refine.c:226); here the systems' SolverMatrix structures
+ * are concatenated into one elimination forest (cblks, blocks, columns and browtab
+ * offset system by system) so that every level of all trees runs in the same
+ * launches.  sys_cblk[0..nsys]: first cblk of each system (sys_cblk[0] = 0,
+ * sys_cblk[nsys] = cblknbr); every block of a system's cblks must face a cblk of
+ * the same system.  Call once, after b200_solver_create and before b200_numfact.
+ * Then each system keeps its own static-pivoting threshold (the threshold rule with
+ * its own ||A_i||_F, computed from its bcsc columns on the device; b200_stats
+ * reports -1 as the threshold) and its own pivot count (b200_numfact returns their
+ * sum), and b200_refine /
+ * b200_refine_device run one refinement per (column, system), each with its own
+ * stopping rule; their berr then holds per column the largest error of its systems. */
+int b200_batch_set( b200_solver_t *solver, int64_t nsys, const int64_t *sys_cblk );
+/* the nsys thresholds of the last b200_numfact of a batch */
+int b200_batch_thresholds( b200_solver_t *solver, double *thr, int64_t nsys );
+/* the pivots each system's last factorization replaced (its IPARM_STATIC_PIVOTING) */
+int b200_batch_pivots( b200_solver_t *solver, int64_t *npiv, int64_t nsys );
+/* the backward errors of the last refinement per problem, column-major
+ * (problem r * nsys + system; count = nrhs * nsys, or nrhs outside a batch) */
+int b200_batch_berr( b200_solver_t *solver, double *berr, int64_t count );
+
 int b200_spm_map( b200_solver_t *solver, int64_t nnz_spm, const int64_t *lmap, const int64_t *umap );
 int b200_spm_values( b200_solver_t *solver, const double *values, double anorm );
 int b200_spm_values_device( b200_solver_t *solver, const double *d_values, double anorm, void *stream );

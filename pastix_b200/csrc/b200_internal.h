@@ -33,7 +33,21 @@ struct DevSym {
     const int *lrow;      // [bloknbr]
     const int *rowoff;    // [bloknbr] first panel row of the block inside its cblk
     const int *fcblk;     // [bloknbr] facing cblk
+    const int *csys;      // [cblknbr] system of each cblk of a batch; nullptr: one system
 };
+
+#ifdef __CUDACC__
+// Static-pivoting threshold of cblk k: thr[0], or in a batch of independent
+// systems the threshold of k's own system (each system keeps the rule of its own
+// factorization, sopalin/pastix_task_sopalin.c:401-425, with its own norm).
+__device__ __forceinline__ double cblk_threshold(const DevSym &s, const double *thr, int k) {
+    return thr[s.csys ? s.csys[k] : 0];
+}
+// Counter of the pivots replaced in cblk k: npiv[0], or its system's in a batch.
+__device__ __forceinline__ unsigned long long *cblk_pivot_counter(const DevSym &s, unsigned long long *npiv, int k) {
+    return npiv + (s.csys ? s.csys[k] : 0);
+}
+#endif
 
 // One update of the right-looking supernodal factorization: the contribution of
 // cblk k's block j (and the blocks below it) to the facing cblk f

@@ -316,7 +316,7 @@ __global__ void __launch_bounds__(256) diag_factor_kernel(DevSym s, const int *_
     __shared__ int s_piv, s_err;
     const int k = cblks[blockIdx.x];
     const int n = s.ncols[k], ld = s.ld[k];
-    const double thr = *thr_ptr;
+    const double thr = cblk_threshold(s, thr_ptr, k);
     T *A = L + s.off[k];
     T *ti = tinv + tinv_off[k];
     const int tid = threadIdx.x, nth = blockDim.x, lane = tid & 31, warp = tid >> 5;
@@ -445,7 +445,7 @@ __global__ void __launch_bounds__(256) diag_factor_kernel(DevSym s, const int *_
         }
     }
     if (tid == 0) {
-        if (s_piv) atomicAdd(npiv, (unsigned long long)s_piv);
+        if (s_piv) atomicAdd(cblk_pivot_counter(s, npiv, k), (unsigned long long)s_piv);
         if (s_err) atomicOr(err, 1);
     }
 }
@@ -822,7 +822,7 @@ __global__ void __launch_bounds__(32 * DS_WARPS) diag_small_kernel(DevSym s, con
     if (ci >= ncblk) return;
     const int k = cblks[ci];
     const int n = s.ncols[k], ld = s.ld[k];
-    const double thr = *thr_ptr;
+    const double thr = cblk_threshold(s, thr_ptr, k);
     T *A = L + s.off[k];
     if (lane == 0) { s_piv[warp] = 0; s_err[warp] = 0; }
     stage_n<32, T>(
@@ -853,7 +853,7 @@ __global__ void __launch_bounds__(32 * DS_WARPS) diag_small_kernel(DevSym s, con
     }
     __syncwarp();
     if (lane == 0) {
-        if (s_piv[warp]) atomicAdd(npiv, (unsigned long long)s_piv[warp]);
+        if (s_piv[warp]) atomicAdd(cblk_pivot_counter(s, npiv, k), (unsigned long long)s_piv[warp]);
         if (s_err[warp]) atomicOr(err, 1);
     }
 }

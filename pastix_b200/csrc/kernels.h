@@ -124,18 +124,26 @@ void launch_gather_values(int64_t nnz, const int64_t *map, const double *src, do
 // out[r] = sum_i x[i,r] * y[i,r]  (nrhs columns), accumulated in double
 void launch_dots(int n, int nrhs, const double *x, int64_t ldx, const double *y, int64_t ldy, double *out,
                  cudaStream_t st);
-// y[:,r] += a[r] * x[:,r]  (a on the device); sign: +1 or -1 applied to a
+// Per-problem scalars: problem p(i, r) = r * nseg + segid[i] in a batch of nseg
+// independent systems (segid: system of each row), r without one (nseg = 1).
+// y[:,r] += a[p] * x[:,r]  (a on the device); sign: +1 or -1 applied to a
 void launch_axpys(int n, int nrhs, const double *a, double sign, const double *x, int64_t ldx, double *y,
-                  int64_t ldy, cudaStream_t st);
-// y[:,r] = x[:,r] + b[r] * y[:,r]
+                  int64_t ldy, cudaStream_t st, int nseg = 1, const int *segid = nullptr);
+// y[:,r] = x[:,r] + b[p] * y[:,r]
 void launch_xpbys(int n, int nrhs, const double *x, int64_t ldx, const double *b, double *y, int64_t ldy,
-                  cudaStream_t st);
+                  cudaStream_t st, int nseg = 1, const int *segid = nullptr);
 void launch_copy(int n, int nrhs, const double *x, int64_t ldx, double *y, int64_t ldy, cudaStream_t st);
 // y[:,r] = alpha * x[:,r] + beta * y[:,r]
 void launch_axpby(int n, int nrhs, double alpha, const double *x, int64_t ldx, double beta, double *y, int64_t ldy,
                   cudaStream_t st);
-// y[:,r] = s[r] * x[:,r]
+// y[:,r] = s[p] * x[:,r]
 void launch_scal_cols(int n, int nrhs, const double *s, const double *x, int64_t ldx, double *y, int64_t ldy,
-                      cudaStream_t st);
+                      cudaStream_t st, int nseg = 1, const int *segid = nullptr);
+// out[r * nseg + p] = sum over the rows [seg[p], seg[p+1]) of x[i,r] * y[i,r]
+void launch_seg_dots(int nseg, const int *seg, int nrhs, const double *x, int64_t ldx, const double *y, int64_t ldy,
+                     double *out, cudaStream_t st);
+// thr[i] = use_norm ? c * ||columns [sys_col[i], sys_col[i+1]) of the bcsc||_F : c
+void launch_batch_threshold(int nsys, const int *sys_col, const int64_t *colptr, const double *vals, double c,
+                            int use_norm, double *thr, cudaStream_t st);
 
 }  // namespace b200

@@ -243,7 +243,6 @@ __global__ void __launch_bounds__(PT, sizeof(T) == 4 ? 2 : 1) panel_kernel(DevSy
     T *rdiag = bs + PB * PB, *dinv = rdiag + PB, *dd = dinv + PB;
     __shared__ int s_item, s_ok, s_piv, s_err;
     const int tid = threadIdx.x;
-    const double thr = *thr_ptr;
     bool aborted = false;
     for (;;) {
         if (tid == 0) {
@@ -259,6 +258,7 @@ __global__ void __launch_bounds__(PT, sizeof(T) == 4 ? 2 : 1) panel_kernel(DevSy
         const PanelCblk pc = pcb[it.p];
         const int k = pc.k, j = it.j, b = it.b;
         const int W = s.ncols[k], S = s.stride[k], ld = s.ld[k];
+        const double thr = cblk_threshold(s, thr_ptr, k);
         T *P = L + s.off[k];
         const int c0 = PB * j, wd = min(PB, W - c0);
         int *sol = solved + pc.flag0, *upd = updated + pc.flag0;
@@ -292,7 +292,7 @@ __global__ void __launch_bounds__(PT, sizeof(T) == 4 ? 2 : 1) panel_kernel(DevSy
             }
             __syncthreads();
             if (tid == 0) {
-                if (s_piv) atomicAdd(npiv, (unsigned long long)s_piv);
+                if (s_piv) atomicAdd(cblk_pivot_counter(s, npiv, k), (unsigned long long)s_piv);
                 if (s_err) atomicOr(err, 1);
                 __threadfence();
                 st_release(sol + b, j + 1);
@@ -577,7 +577,6 @@ __global__ void __launch_bounds__(PT, 1)
     T *xs = dd + PB;                         // the row block, column-major (pitch = its rows)
     __shared__ int s_item, s_ok, s_piv, s_err;
     const int tid = threadIdx.x;
-    const double thr = *thr_ptr;
     bool aborted = false;
     for (;;) {
         if (tid == 0) {
@@ -592,6 +591,7 @@ __global__ void __launch_bounds__(PT, 1)
         const PanelItem it = items[t];
         const PanelCblk pc = pcb[it.p];
         int *sol = solved + pc.flag0;
+        const double thr = cblk_threshold(s, thr_ptr, pc.k);
         if (it.b < pc.ns)
             rows_item<T, FACTO, PB>(s, pc, it.b, L, lt, rdiag, dinv, dd, xs, sol, abort_word, thr, &s_ok, &s_piv,
                                     &s_err);
@@ -604,7 +604,7 @@ __global__ void __launch_bounds__(PT, 1)
             break;
         }
         if (tid == 0) {
-            if (s_piv) atomicAdd(npiv, (unsigned long long)s_piv);
+            if (s_piv) atomicAdd(cblk_pivot_counter(s, npiv, pc.k), (unsigned long long)s_piv);
             if (s_err) atomicOr(err, 1);
         }
         __syncthreads();

@@ -51,20 +51,71 @@ __global__ void dots_kernel(int n, const double *__restrict__ x, int64_t ldx, co
     }
 }
 
+// Refinement runs one independent problem per right-hand side column, or in a
+// batch of independent systems one per (column, system): the problem of row i of
+// column r is r * nseg + segid[i] (segid null: nseg = 1, the column).
+__device__ __forceinline__ int problem_of(int i, int r, int nseg, const int *__restrict__ segid) {
+    return r * nseg + (segid ? segid[i] : 0);
+}
+
 __global__ void axpys_kernel(int n, int nrhs, const double *__restrict__ a, double sign,
-                             const double *__restrict__ x, int64_t ldx, double *y, int64_t ldy) {
+                             const double *__restrict__ x, int64_t ldx, double *y, int64_t ldy, int nseg,
+                             const int *__restrict__ segid) {
     const int64_t idx = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
     if (idx >= (int64_t)n * nrhs) return;
     const int i = (int)(idx % n), r = (int)(idx / n);
-    y[i + r * ldy] += sign * a[r] * x[i + r * ldx];
+    y[i + r * ldy] += sign * a[problem_of(i, r, nseg, segid)] * x[i + r * ldx];
 }
 
 __global__ void xpbys_kernel(int n, int nrhs, const double *__restrict__ x, int64_t ldx, const double *__restrict__ b,
-                             double *y, int64_t ldy) {
+                             double *y, int64_t ldy, int nseg, const int *__restrict__ segid) {
     const int64_t idx = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
     if (idx >= (int64_t)n * nrhs) return;
     const int i = (int)(idx % n), r = (int)(idx / n);
-    y[i + r * ldy] = x[i + r * ldx] + b[r] * y[i + r * ldy];
+    y[i + r * ldy] = x[i + r * ldx] + b[problem_of(i, r, nseg, segid)] * y[i + r * ldy];
+}
+
+// Dot products of every (column, system) problem of a batch: one block per
+// problem over its system's rows [seg[p], seg[p + 1]), in a fixed order.
+__global__ void seg_dots_kernel(int nseg, const int *__restrict__ seg, const double *__restrict__ x, int64_t ldx,
+                                const double *__restrict__ y, int64_t ldy, double *out) {
+    const int p = blockIdx.x, r = blockIdx.y;
+    __shared__ double red[32];
+    double acc = 0.0;
+    for (int i = seg[p] + threadIdx.x; i < seg[p + 1]; i += blockDim.x) acc += x[i + r * ldx] * y[i + r * ldy];
+#pragma unroll
+    for (int o = 16; o > 0; o >>= 1) acc += __shfl_xor_sync(0xffffffffu, acc, o);
+    if ((threadIdx.x & 31) == 0) red[threadIdx.x >> 5] = acc;
+    __syncthreads();
+    if (threadIdx.x < 32) {
+        acc = (threadIdx.x < (blockDim.x >> 5)) ? red[threadIdx.x] : 0.0;
+#pragma unroll
+        for (int o = 16; o > 0; o >>= 1) acc += __shfl_xor_sync(0xffffffffu, acc, o);
+        if (threadIdx.x == 0) out[r * nseg + p] = acc;
+    }
+}
+
+// Static-pivoting threshold of every system of a batch from its own Frobenius
+// norm, summed over its columns [sys_col[i], sys_col[i + 1]) of the bcsc (full
+// pattern: both triangles of a symmetric matrix):
+// thr_i = use_norm ? c * ||A_i||_F : c.
+__global__ void batch_threshold_kernel(const int *__restrict__ sys_col, const int64_t *__restrict__ colptr,
+                                       const double *__restrict__ vals, double c, int use_norm, double *thr) {
+    const int p = blockIdx.x;
+    __shared__ double red[32];
+    double acc = 0.0;
+    for (int64_t e = colptr[sys_col[p]] + threadIdx.x; e < colptr[sys_col[p + 1]]; e += blockDim.x)
+        acc += vals[e] * vals[e];
+#pragma unroll
+    for (int o = 16; o > 0; o >>= 1) acc += __shfl_xor_sync(0xffffffffu, acc, o);
+    if ((threadIdx.x & 31) == 0) red[threadIdx.x >> 5] = acc;
+    __syncthreads();
+    if (threadIdx.x < 32) {
+        acc = (threadIdx.x < (blockDim.x >> 5)) ? red[threadIdx.x] : 0.0;
+#pragma unroll
+        for (int o = 16; o > 0; o >>= 1) acc += __shfl_xor_sync(0xffffffffu, acc, o);
+        if (threadIdx.x == 0) thr[p] = use_norm ? c * sqrt(acc) : c;
+    }
 }
 
 __global__ void axpby_kernel(int n, int nrhs, double alpha, const double *__restrict__ x, int64_t ldx, double beta,
@@ -77,11 +128,11 @@ __global__ void axpby_kernel(int n, int nrhs, double alpha, const double *__rest
 }
 
 __global__ void scal_cols_kernel(int n, int nrhs, const double *__restrict__ s, const double *__restrict__ x,
-                                 int64_t ldx, double *y, int64_t ldy) {
+                                 int64_t ldx, double *y, int64_t ldy, int nseg, const int *__restrict__ segid) {
     const int64_t idx = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
     if (idx >= (int64_t)n * nrhs) return;
     const int i = (int)(idx % n), r = (int)(idx / n);
-    y[i + r * ldy] = s[r] * x[i + r * ldx];
+    y[i + r * ldy] = s[problem_of(i, r, nseg, segid)] * x[i + r * ldx];
 }
 
 static inline unsigned nblk(int64_t tot, int bs) { return (unsigned)((tot + bs - 1) / bs); }
@@ -178,17 +229,29 @@ void launch_dots(int n, int nrhs, const double *x, int64_t ldx, const double *y,
 }
 
 void launch_axpys(int n, int nrhs, const double *a, double sign, const double *x, int64_t ldx, double *y,
-                  int64_t ldy, cudaStream_t st) {
+                  int64_t ldy, cudaStream_t st, int nseg, const int *segid) {
     const int64_t tot = (int64_t)n * nrhs;
     if (tot <= 0) return;
-    axpys_kernel<<<nblk(tot, 256), 256, 0, st>>>(n, nrhs, a, sign, x, ldx, y, ldy);
+    axpys_kernel<<<nblk(tot, 256), 256, 0, st>>>(n, nrhs, a, sign, x, ldx, y, ldy, nseg, segid);
 }
 
 void launch_xpbys(int n, int nrhs, const double *x, int64_t ldx, const double *b, double *y, int64_t ldy,
-                  cudaStream_t st) {
+                  cudaStream_t st, int nseg, const int *segid) {
     const int64_t tot = (int64_t)n * nrhs;
     if (tot <= 0) return;
-    xpbys_kernel<<<nblk(tot, 256), 256, 0, st>>>(n, nrhs, x, ldx, b, y, ldy);
+    xpbys_kernel<<<nblk(tot, 256), 256, 0, st>>>(n, nrhs, x, ldx, b, y, ldy, nseg, segid);
+}
+
+void launch_seg_dots(int nseg, const int *seg, int nrhs, const double *x, int64_t ldx, const double *y, int64_t ldy,
+                     double *out, cudaStream_t st) {
+    if (nseg <= 0 || nrhs <= 0) return;
+    seg_dots_kernel<<<dim3(nseg, nrhs), 256, 0, st>>>(nseg, seg, x, ldx, y, ldy, out);
+}
+
+void launch_batch_threshold(int nsys, const int *sys_col, const int64_t *colptr, const double *vals, double c,
+                            int use_norm, double *thr, cudaStream_t st) {
+    if (nsys <= 0) return;
+    batch_threshold_kernel<<<nsys, 256, 0, st>>>(sys_col, colptr, vals, c, use_norm, thr);
 }
 
 void launch_copy(int n, int nrhs, const double *x, int64_t ldx, double *y, int64_t ldy, cudaStream_t st) {
@@ -203,10 +266,10 @@ void launch_axpby(int n, int nrhs, double alpha, const double *x, int64_t ldx, d
 }
 
 void launch_scal_cols(int n, int nrhs, const double *s, const double *x, int64_t ldx, double *y, int64_t ldy,
-                      cudaStream_t st) {
+                      cudaStream_t st, int nseg, const int *segid) {
     const int64_t tot = (int64_t)n * nrhs;
     if (tot <= 0) return;
-    scal_cols_kernel<<<nblk(tot, 256), 256, 0, st>>>(n, nrhs, s, x, ldx, y, ldy);
+    scal_cols_kernel<<<nblk(tot, 256), 256, 0, st>>>(n, nrhs, s, x, ldx, y, ldy, nseg, segid);
 }
 
 }  // namespace b200

@@ -181,6 +181,15 @@ struct b200_solver_s {
     double thr_used = 0.0;
     int64_t last_npiv = 0;
 
+    // batch of independent systems (b200_batch_set): one elimination forest whose
+    // trees are the systems, each with its own pivot threshold and refinement
+    int nsys = 0;
+    int *d_csys = nullptr;     // [cblknbr] system of each cblk
+    int *d_sys_col = nullptr;  // [nsys+1] first (permuted) column of each system
+    int *d_segid = nullptr;    // [n] system of each permuted row
+    std::vector<double> last_berr;  // per-problem backward errors of the last refinement
+    std::vector<unsigned long long> last_piv_sys;  // pivots replaced per system by the last numfact
+
     // solve / refine workspaces
     double *d_ws = nullptr;
     size_t ws_cap = 0;
@@ -736,7 +745,7 @@ int enqueue_numfact(b200_solver_t *s, cudaStream_t st, Trace *tr = nullptr) {
     if (tr) tr->begin(st);
     CU(cudaMemsetAsync(L, 0, s->arena * sizeof(T), st));
     if (U) CU(cudaMemsetAsync(U, 0, s->arena * sizeof(T), st));
-    CU(cudaMemsetAsync(s->d_npiv, 0, sizeof(unsigned long long), st));
+    CU(cudaMemsetAsync(s->d_npiv, 0, (size_t)std::max(s->nsys, 1) * sizeof(unsigned long long), st));
     CU(cudaMemsetAsync(s->d_err, 0, sizeof(int), st));
     CU(cudaMemsetAsync(s->d_pflags, 0, (size_t)s->n_pflags * sizeof(int), st));
     if (s->test_withhold & 1)
@@ -989,6 +998,12 @@ struct RefineCtx {
     b200_solver_t *s;
     cudaStream_t st;
     int n, nrhs;
+    // independent problems: one per right-hand side column, or in a batch one per
+    // (column, system), problem r * nseg + system
+    int nseg = 1;
+    const int *seg = nullptr;    // [nseg+1] first permuted row of each system
+    const int *segid = nullptr;  // [n] system of each permuted row
+    int np() const { return nrhs * nseg; }
     // A x in the permuted basis with the bcsc
     int spmv(const double *x, double *y, double alpha, double beta) {
         const double *vals = (s->facto == FACTO_GETRF) ? s->d_Uv : s->d_Lv;
@@ -1008,27 +1023,45 @@ struct RefineCtx {
     // one BLAS-1 kernel launched by the caller
     void count(int k = 1) { s->kernel_launches += k; }
     int dots(const double *x, const double *y, std::vector<double> &out) {
-        launch_dots(n, nrhs, x, n, y, n, s->d_scal, st);
+        if (segid) launch_seg_dots(nseg, seg, nrhs, x, n, y, n, s->d_scal, st);
+        else launch_dots(n, nrhs, x, n, y, n, s->d_scal, st);
         s->kernel_launches++;
-        out.resize(nrhs);
-        CU(cudaMemcpyAsync(out.data(), s->d_scal, nrhs * sizeof(double), cudaMemcpyDeviceToHost, st));
+        out.resize(np());
+        CU(cudaMemcpyAsync(out.data(), s->d_scal, np() * sizeof(double), cudaMemcpyDeviceToHost, st));
         CU(cudaStreamSynchronize(st));
         return ERR_SUCCESS;
     }
     int set_scal(const std::vector<double> &v, int slot) {
-        CU(cudaMemcpyAsync(s->d_scal + (size_t)slot * nrhs, v.data(), nrhs * sizeof(double), cudaMemcpyHostToDevice,
+        CU(cudaMemcpyAsync(s->d_scal + (size_t)slot * np(), v.data(), np() * sizeof(double), cudaMemcpyHostToDevice,
                            st));
         return ERR_SUCCESS;
     }
-    double *scal(int slot) { return s->d_scal + (size_t)slot * nrhs; }
+    double *scal(int slot) { return s->d_scal + (size_t)slot * np(); }
+    // vector operations over n x nrhs blocks with per-problem scalars from slot
+    void copy(const double *x, double *y) {
+        launch_copy(n, nrhs, x, n, y, n, st);
+        count();
+    }
+    void axpys(int slot, double sign, const double *x, double *y) {
+        launch_axpys(n, nrhs, scal(slot), sign, x, n, y, n, st, nseg, segid);
+        count();
+    }
+    void xpbys(const double *x, int slot, double *y) {
+        launch_xpbys(n, nrhs, x, n, scal(slot), y, n, st, nseg, segid);
+        count();
+    }
+    void scal_cols(int slot, const double *x, double *y) {
+        launch_scal_cols(n, nrhs, scal(slot), x, n, y, n, st, nseg, segid);
+        count();
+    }
 };
 
 // z_pivot_smp (refinement/z_refine_pivot.c:45-140), all right-hand sides together,
 // each column with its own stopping rule.
 int refine_sr(RefineCtx &c, const double *b, double *x, int itermax, double eps, int64_t *niter,
               std::vector<double> &berr) {
-    const int n = c.n, R = c.nrhs;
-    double *r = c.s->d_ws + (size_t)2 * n * R, *dx = r + (size_t)n * R;
+    const int n = c.n, R = c.np();
+    double *r = c.s->d_ws + (size_t)2 * n * c.nrhs, *dx = r + (size_t)n * c.nrhs;
     std::vector<double> nb, nr, last(R, 0.0), mask(R, 1.0);
     RET(c.dots(b, b, nb));
     for (auto &v : nb) v = std::sqrt(v);
@@ -1036,8 +1069,7 @@ int refine_sr(RefineCtx &c, const double *b, double *x, int itermax, double eps,
     bool any = true;
     berr.assign(R, 0.0);
     while (any) {
-        launch_copy(n, R, b, n, r, n, c.st);
-        c.count();
+        c.copy(b, r);
         RET(c.spmv(x, r, -1.0, 1.0));
         RET(c.dots(r, r, nr));
         any = false;
@@ -1054,12 +1086,10 @@ int refine_sr(RefineCtx &c, const double *b, double *x, int itermax, double eps,
             }
         }
         if (!any) break;
-        launch_copy(n, R, r, n, dx, n, c.st);
-        c.count();
+        c.copy(r, dx);
         RET(c.spsv(dx));
         RET(c.set_scal(mask, 0));
-        launch_axpys(n, R, c.scal(0), 1.0, dx, n, x, n, c.st);
-        c.count();
+        c.axpys(0, 1.0, dx, x);
         iter++;
     }
     *niter = iter;
@@ -1069,15 +1099,14 @@ int refine_sr(RefineCtx &c, const double *b, double *x, int itermax, double eps,
 // z_grad_smp (refinement/z_refine_grad.c:46-156): preconditioned CG.
 int refine_cg(RefineCtx &c, const double *b, double *x, int itermax, double eps, int64_t *niter,
               std::vector<double> &berr) {
-    const int n = c.n, R = c.nrhs;
-    const size_t blk = (size_t)n * R;
+    const int n = c.n, R = c.np();
+    const size_t blk = (size_t)n * c.nrhs;
     double *gr = c.s->d_ws + 2 * blk, *gp = gr + blk, *gz = gp + blk, *g2 = gz + blk;
     std::vector<double> nb, nx, nr, beta, alpha, tmp;
     RET(c.dots(b, b, nb));
     RET(c.dots(x, x, nx));
     for (auto &v : nb) v = std::sqrt(v);
-    launch_copy(n, R, b, n, gr, n, c.st);
-    c.count();
+    c.copy(b, gr);
     RET(c.spmv(x, gr, -1.0, 1.0));
     RET(c.dots(gr, gr, nr));
     std::vector<double> resid(R), active(R, 1.0);
@@ -1086,11 +1115,9 @@ int refine_cg(RefineCtx &c, const double *b, double *x, int itermax, double eps,
         resid[j] = std::sqrt(nr[j]) / (nb[j] > 0 ? nb[j] : 1.0);
         if (resid[j] > eps) any = true; else active[j] = 0.0;
     }
-    launch_copy(n, R, gr, n, gz, n, c.st);
-    c.count();
+    c.copy(gr, gz);
     RET(c.spsv(gz));
-    launch_copy(n, R, gz, n, gp, n, c.st);
-    c.count();
+    c.copy(gz, gp);
     int iter = 0;
     while (any && iter < itermax) {
         iter++;
@@ -1099,10 +1126,8 @@ int refine_cg(RefineCtx &c, const double *b, double *x, int itermax, double eps,
         RET(c.dots(g2, gp, alpha));
         for (int j = 0; j < R; j++) alpha[j] = (active[j] != 0.0 && alpha[j] != 0.0) ? beta[j] / alpha[j] : 0.0;
         RET(c.set_scal(alpha, 0));
-        launch_axpys(n, R, c.scal(0), 1.0, gp, n, x, n, c.st);
-        c.count();
-        launch_axpys(n, R, c.scal(0), -1.0, g2, n, gr, n, c.st);
-        c.count();
+        c.axpys(0, 1.0, gp, x);
+        c.axpys(0, -1.0, g2, gr);
         // convergence test on the updated residual before the next preconditioner
         // application, which the last iteration does not need
         RET(c.dots(gr, gr, nr));
@@ -1113,14 +1138,12 @@ int refine_cg(RefineCtx &c, const double *b, double *x, int itermax, double eps,
             if (resid[j] > eps) any = true; else active[j] = 0.0;
         }
         if (!any || iter >= itermax) break;
-        launch_copy(n, R, gr, n, gz, n, c.st);
-        c.count();
+        c.copy(gr, gz);
         RET(c.spsv(gz));
         RET(c.dots(gr, gz, tmp));
         for (int j = 0; j < R; j++) tmp[j] = (beta[j] != 0.0) ? tmp[j] / beta[j] : 0.0;
         RET(c.set_scal(tmp, 1));
-        launch_xpbys(n, R, gz, n, c.scal(1), gp, n, c.st);
-        c.count();
+        c.xpbys(gz, 1, gp);
     }
     berr = resid;
     *niter = iter;
@@ -1132,8 +1155,8 @@ int refine_cg(RefineCtx &c, const double *b, double *x, int itermax, double eps,
 // right-hand sides are computed together.
 int refine_gmres(RefineCtx &c, const double *b, double *x, int itermax, int im, double eps, int64_t *niter,
                  std::vector<double> &berr) {
-    const int n = c.n, R = c.nrhs;
-    const size_t blk = (size_t)n * R;
+    const int n = c.n, R = c.np();
+    const size_t blk = (size_t)n * c.nrhs;
     double *V = c.s->d_ws + 2 * blk;               // (im+1) blocks
     double *W = V + (size_t)(im + 1) * blk;         // im blocks
     const int im1 = im + 1;
@@ -1148,8 +1171,7 @@ int refine_gmres(RefineCtx &c, const double *b, double *x, int itermax, int im, 
     int iters = 0;
     bool outer = true;
     while (outer) {
-        launch_copy(n, R, b, n, V, n, c.st);
-        c.count();
+        c.copy(b, V);
         RET(c.spmv(x, V, -1.0, 1.0));
         RET(c.dots(V, V, nr));
         bool any = false;
@@ -1166,23 +1188,20 @@ int refine_gmres(RefineCtx &c, const double *b, double *x, int itermax, int im, 
         }
         if (!any) break;
         RET(c.set_scal(inv, 0));
-        launch_scal_cols(n, R, c.scal(0), V, n, V, n, c.st);
-        c.count();
+        c.scal_cols(0, V, V);
         int i = -1;
         bool inner = true;
         while (inner) {
             i++;
             double *Vi = V + (size_t)i * blk, *Wi = W + (size_t)i * blk, *Vn = V + (size_t)(i + 1) * blk;
-            launch_copy(n, R, Vi, n, Wi, n, c.st);
-            c.count();
+            c.copy(Vi, Wi);
             RET(c.spsv(Wi));
             RET(c.spmv(Wi, Vn, 1.0, 0.0));
             for (int jj = 0; jj <= i; jj++) {
                 RET(c.dots(Vn, V + (size_t)jj * blk, h));
                 for (int j = 0; j < R; j++) H[j][(size_t)i * im1 + jj] = h[j];
                 RET(c.set_scal(h, 0));
-                launch_axpys(n, R, c.scal(0), -1.0, V + (size_t)jj * blk, n, Vn, n, c.st);
-                c.count();
+                c.axpys(0, -1.0, V + (size_t)jj * blk, Vn);
             }
             RET(c.dots(Vn, Vn, nr));
             std::vector<double> sc(R, 1.0);
@@ -1206,8 +1225,7 @@ int refine_gmres(RefineCtx &c, const double *b, double *x, int itermax, int im, 
                 if (!done[j]) resid_b[j] = std::fabs(G[j][i + 1]) / (nb[j] > 0 ? nb[j] : 1.0);
             }
             RET(c.set_scal(sc, 0));
-            launch_scal_cols(n, R, c.scal(0), Vn, n, Vn, n, c.st);
-            c.count();
+            c.scal_cols(0, Vn, Vn);
             iters++;
             bool all_conv = true;
             for (int j = 0; j < R; j++)
@@ -1228,8 +1246,7 @@ int refine_gmres(RefineCtx &c, const double *b, double *x, int itermax, int im, 
             std::vector<double> y(R);
             for (int j = 0; j < R; j++) y[j] = G[j][q];
             RET(c.set_scal(y, 0));
-            launch_axpys(n, R, c.scal(0), 1.0, W + (size_t)q * blk, n, x, n, c.st);
-            c.count();
+            c.axpys(0, 1.0, W + (size_t)q * blk, x);
         }
         if (iters >= itermax) outer = false;
     }
@@ -1250,12 +1267,18 @@ int refine_device(b200_solver_t *s, int nrhs, const double *b, int64_t ldb, doub
     const size_t aux_at = need;
     need += blk;  // scratch of the sweeps
     RET(ensure_ws(s, need));
-    RET(ensure_scal(s, 2 * nrhs));
+    const int nseg = s->nsys > 0 ? s->nsys : 1;
+    RET(ensure_scal(s, 2 * nrhs * nseg));
     double *bp = s->d_ws, *xp = s->d_ws + blk;
     launch_permute(n, nrhs, s->d_peri, b, ldb, bp, n, 1, st);
     launch_permute(n, nrhs, s->d_peri, x, ldx, xp, n, 1, st);
     s->kernel_launches += 3;
     RefineCtx c{s, st, n, nrhs};
+    if (s->nsys > 0) {
+        c.nseg = s->nsys;
+        c.seg = s->d_sys_col;
+        c.segid = s->d_segid;
+    }
     c.aux = s->d_ws + aux_at;
     std::vector<double> be;
     int64_t it = 0;
@@ -1267,8 +1290,13 @@ int refine_device(b200_solver_t *s, int nrhs, const double *b, int64_t ldb, doub
     launch_permute(n, nrhs, s->d_peri, xp, n, x, ldx, 0, st);
     CU(cudaGetLastError());
     if (niter) *niter = it;
+    s->last_berr = be;
+    // per column: the largest backward error of its problems (its systems in a batch)
     if (berr)
-        for (int j = 0; j < nrhs; j++) berr[j] = be[j];
+        for (int j = 0; j < nrhs; j++) {
+            berr[j] = 0.0;
+            for (int q = 0; q < nseg; q++) berr[j] = std::max(berr[j], be[(size_t)j * nseg + q]);
+        }
     return ERR_SUCCESS;
 }
 
@@ -1577,6 +1605,63 @@ int b200_get_diag(b200_solver_t *s, double *D, int64_t incD) {
     return ERR_SUCCESS;
 }
 
+int b200_batch_set(b200_solver_t *s, int64_t nsys, const int64_t *sys_cblk) {
+    if (!s || !sys_cblk || nsys < 1 || nsys > s->cblknbr || s->nsys != 0) return ERR_BADPARAM;
+    if (s->cblkschur < s->cblknbr) return ERR_BADPARAM;  // a batch has no Schur complement
+    if (sys_cblk[0] != 0 || sys_cblk[nsys] != s->cblknbr) return ERR_BADPARAM;
+    std::vector<int> csys(s->cblknbr), col(nsys + 1), segid(s->n);
+    for (int64_t i = 0; i < nsys; i++) {
+        if (sys_cblk[i + 1] <= sys_cblk[i]) return ERR_BADPARAM;
+        for (int64_t k = sys_cblk[i]; k < sys_cblk[i + 1]; k++) {
+            csys[k] = (int)i;
+            // the systems are independent: every block of a system's cblk faces a cblk of it
+            for (int b = s->fblok[k]; b < s->fblok[k + 1]; b++)
+                if (s->fcblk[b] < sys_cblk[i] || s->fcblk[b] >= sys_cblk[i + 1]) return ERR_BADPARAM;
+        }
+        col[i] = s->fcol[sys_cblk[i]];
+        for (int r = col[i]; r < s->fcol[sys_cblk[i + 1]]; r++) segid[r] = (int)i;
+    }
+    col[nsys] = s->n;
+    double *thr = nullptr;
+    unsigned long long *npiv = nullptr;
+    RET(s->dmalloc(&npiv, (size_t)nsys));
+    RET(s->dupload(&s->d_csys, csys));
+    RET(s->dupload(&s->d_sys_col, col));
+    RET(s->dupload(&s->d_segid, segid));
+    RET(s->dmalloc(&thr, (size_t)nsys));
+    CU(cudaStreamSynchronize(s->st));
+    s->d_thr = thr;
+    s->d_npiv = npiv;
+    s->ds.csys = s->d_csys;
+    s->nsys = (int)nsys;
+    // the captured factorization holds the structure tables by value: capture again
+    if (s->fact_graph) {
+        cudaGraphExecDestroy(s->fact_graph);
+        s->fact_graph = nullptr;
+    }
+    s->factored = false;
+    return ERR_SUCCESS;
+}
+
+int b200_batch_thresholds(b200_solver_t *s, double *thr, int64_t nsys) {
+    if (!s || !thr || s->nsys == 0 || nsys != s->nsys || !s->factored) return ERR_BADPARAM;
+    CU(cudaMemcpyAsync(thr, s->d_thr, (size_t)nsys * sizeof(double), cudaMemcpyDeviceToHost, s->st));
+    CU(cudaStreamSynchronize(s->st));
+    return ERR_SUCCESS;
+}
+
+int b200_batch_pivots(b200_solver_t *s, int64_t *npiv, int64_t nsys) {
+    if (!s || !npiv || s->nsys == 0 || nsys != s->nsys || !s->factored) return ERR_BADPARAM;
+    for (int64_t i = 0; i < nsys; i++) npiv[i] = (int64_t)s->last_piv_sys[i];
+    return ERR_SUCCESS;
+}
+
+int b200_batch_berr(b200_solver_t *s, double *berr, int64_t count) {
+    if (!s || !berr || count != (int64_t)s->last_berr.size() || count == 0) return ERR_BADPARAM;
+    std::copy(s->last_berr.begin(), s->last_berr.end(), berr);
+    return ERR_SUCCESS;
+}
+
 int b200_get_schur(b200_solver_t *s, double *S, int64_t lds) {
     if (!s || !S || !s->factored) return ERR_BADPARAM;
     const int cs = s->cblkschur, N = s->cblknbr;
@@ -1731,8 +1816,20 @@ int b200_numfact(b200_solver_t *s, double epsilon_magn_ctrl, int64_t *nbpivots) 
         const double eps = s->f32 ? std::ldexp(1.0, -24) : std::ldexp(1.0, -53);  // LAPACK xlamch('e')
         thr = std::sqrt(eps) * s->anorm;
     } else thr = epsilon_magn_ctrl * s->anorm;
-    s->thr_used = thr;
-    CU(cudaMemcpyAsync(s->d_thr, &thr, sizeof(double), cudaMemcpyHostToDevice, s->st));
+    if (s->nsys > 0) {
+        // one threshold per system, from its own norm (computed from the bcsc on the device)
+        const double eps = s->f32 ? std::ldexp(1.0, -24) : std::ldexp(1.0, -53);
+        const double c = epsilon_magn_ctrl < 0.0 ? -epsilon_magn_ctrl
+                                                 : (epsilon_magn_ctrl == 0.0 ? std::sqrt(eps) : epsilon_magn_ctrl);
+        launch_batch_threshold(s->nsys, s->d_sys_col, s->d_colptr, s->d_Lv, c, epsilon_magn_ctrl >= 0.0, s->d_thr,
+                               s->st);
+        CU(cudaGetLastError());
+        s->kernel_launches++;
+        s->thr_used = -1.0;
+    } else {
+        s->thr_used = thr;
+        CU(cudaMemcpyAsync(s->d_thr, &thr, sizeof(double), cudaMemcpyHostToDevice, s->st));
+    }
     if (!s->fact_graph) {
         cudaGraph_t g;
         CU(cudaStreamBeginCapture(s->st, cudaStreamCaptureModeThreadLocal));
@@ -1751,9 +1848,12 @@ int b200_numfact(b200_solver_t *s, double epsilon_magn_ctrl, int64_t *nbpivots) 
     CU(cudaEventRecord(s->ev1, s->st));
     unsigned long long piv = 0;
     int err = 0;
-    CU(cudaMemcpyAsync(&piv, s->d_npiv, sizeof(piv), cudaMemcpyDeviceToHost, s->st));
+    s->last_piv_sys.assign(std::max(s->nsys, 1), 0ull);
+    CU(cudaMemcpyAsync(s->last_piv_sys.data(), s->d_npiv, s->last_piv_sys.size() * sizeof(unsigned long long),
+                       cudaMemcpyDeviceToHost, s->st));
     CU(cudaMemcpyAsync(&err, s->d_err, sizeof(err), cudaMemcpyDeviceToHost, s->st));
     CU(cudaStreamSynchronize(s->st));
+    for (unsigned long long v : s->last_piv_sys) piv += v;
     float ms = 0;
     cudaEventElapsedTime(&ms, s->ev0, s->ev1);
     s->t_fact = ms;

@@ -25,7 +25,8 @@ _lib = None
 # exported symbols, in the order of include/pastix_b200.h
 SYMBOLS = ["b200_solver_create", "b200_solver_destroy", "b200_solver_create_schur", "b200_get_schur",
            "b200_applyorder", "b200_trsm", "b200_bcsc_load", "b200_bcsc_values", "b200_spm_map",
-           "b200_spm_values", "b200_spm_values_device", "b200_get_diag", "b200_numfact", "b200_numfact_trace",
+           "b200_spm_values", "b200_spm_values_device", "b200_get_diag", "b200_batch_set", "b200_batch_thresholds",
+           "b200_batch_pivots", "b200_batch_berr", "b200_numfact", "b200_numfact_trace",
            "b200_solve_trace", "b200_trace_launches", "b200_trace_kinds", "b200_solve",
            "b200_solve_device", "b200_solve_device_noalloc", "b200_refine", "b200_refine_device", "b200_spmv", "b200_factor_download",
            "b200_stats", "b200_strerror"]
@@ -64,6 +65,10 @@ def lib():
         L.b200_applyorder.argtypes = [_P, C.c_int, _I64, _P, _I64]
         L.b200_trsm.argtypes = [_P, C.c_int, _I64, _P, _I64]
         L.b200_get_diag.argtypes = [_P, _P, _I64]
+        L.b200_batch_set.argtypes = [_P, _I64, _P]
+        L.b200_batch_thresholds.argtypes = [_P, _P, _I64]
+        L.b200_batch_berr.argtypes = [_P, _P, _I64]
+        L.b200_batch_pivots.argtypes = [_P, _P, _I64]
         L.b200_spm_values.argtypes = [_P, _P, C.c_double]
         L.b200_spm_values_device.argtypes = [_P, _P, C.c_double, _P]
         L.b200_trace_kinds.argtypes = [_P, _P, _P, C.c_int]
@@ -181,6 +186,31 @@ class Solver:
         d = np.zeros(self.n)
         check(lib().b200_get_diag(self.h, _p(d), 1), "b200_get_diag")
         return d
+
+    def batch_set(self, sys_cblk):
+        """Independent systems (b200_batch_set): sys_cblk[i] is the first cblk of
+        system i, sys_cblk[-1] = cblknbr."""
+        sc = np.ascontiguousarray(sys_cblk, dtype=np.int64)
+        check(lib().b200_batch_set(self.h, sc.size - 1, _p(sc)), "b200_batch_set")
+        self.nsys = sc.size - 1
+
+    def batch_thresholds(self) -> np.ndarray:
+        thr = np.zeros(self.nsys)
+        check(lib().b200_batch_thresholds(self.h, _p(thr), self.nsys), "b200_batch_thresholds")
+        return thr
+
+    def batch_pivots(self) -> np.ndarray:
+        """Pivots replaced in every system by the last numfact."""
+        piv = np.zeros(self.nsys, dtype=np.int64)
+        check(lib().b200_batch_pivots(self.h, _p(piv), self.nsys), "b200_batch_pivots")
+        return piv
+
+    def batch_berr(self, nrhs: int = 1) -> np.ndarray:
+        """Backward errors of the last refinement, shape (nsys, nrhs)."""
+        ns = getattr(self, "nsys", 1)
+        be = np.zeros(ns * nrhs)
+        check(lib().b200_batch_berr(self.h, _p(be), be.size), "b200_batch_berr")
+        return be.reshape(nrhs, ns).T
 
     def numfact(self, epsilon_magn_ctrl: float = 0.0) -> int:
         piv = _I64(0)
