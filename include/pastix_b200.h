@@ -254,6 +254,11 @@ int b200_refine_device( b200_solver_t *solver, int64_t nrhs, const double *d_b, 
 int b200_spmv( b200_solver_t *solver, int64_t nrhs, double alpha, const double *x, int64_t ldx,
                double beta, double *y, int64_t ldy );
 
+/* The same product on device pointers, enqueued on stream (NULL: the solver's
+ * stream) without a synchronization; its scratch is the solve workspace. */
+int b200_spmv_device( b200_solver_t *solver, int64_t nrhs, double alpha, const double *d_x, int64_t ldx,
+                      double beta, double *d_y, int64_t ldy, void *stream );
+
 /* Copy the factor back in PaStiX's coeftab layout: every cblk's 2D block layout
  * (blend/solver_matrix_gen_utils.h:137-165), cblks concatenated in order, as
  * double.  U (LU only, else NULL) receives the transposed U factor.  Each array

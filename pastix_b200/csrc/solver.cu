@@ -2076,6 +2076,27 @@ int b200_spmv(b200_solver_t *s, int64_t nrhs, double alpha, const double *x, int
     return rc;
 }
 
+int b200_spmv_device(b200_solver_t *s, int64_t nrhs, double alpha, const double *d_x, int64_t ldx, double beta,
+                     double *d_y, int64_t ldy, void *stream) {
+    if (!s || s->nnz < 0 || nrhs < 0 || ldx < s->n || ldy < s->n || nrhs > (1 << 20)) return ERR_BADPARAM;
+    if (nrhs == 0) return ERR_SUCCESS;
+    if (!d_x || !d_y) return ERR_BADPARAM;
+    const int n = s->n;
+    const size_t blk = (size_t)n * nrhs;
+    cudaStream_t st = stream ? (cudaStream_t)stream : s->st;
+    RET(ensure_ws(s, 2 * blk));
+    double *px = s->d_ws, *py = s->d_ws + blk;
+    if (nrhs > 1 && !s->d_xt) RET(dalloc(&s->d_xt, (size_t)n * 16));
+    const double *vals = (s->facto == FACTO_GETRF) ? s->d_Uv : s->d_Lv;
+    launch_permute(n, (int)nrhs, s->d_peri, d_x, ldx, px, n, 1, st);
+    launch_permute(n, (int)nrhs, s->d_peri, d_y, ldy, py, n, 1, st);
+    launch_spmv(n, (int)nrhs, s->d_colptr, s->d_rowtab, vals, px, n, py, n, alpha, beta, st, s->d_xt);
+    launch_permute(n, (int)nrhs, s->d_peri, py, n, d_y, ldy, 0, st);
+    CU(cudaGetLastError());
+    s->kernel_launches += 3 + (nrhs > 1 ? 2 * ((nrhs + 15) / 16) : 1);
+    return ERR_SUCCESS;
+}
+
 int b200_factor_download(b200_solver_t *s, double *L, double *U) {
     if (!s || !L || !s->factored) return ERR_BADPARAM;
     std::vector<char> host((size_t)s->arena * s->esz);

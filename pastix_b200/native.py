@@ -28,7 +28,7 @@ SYMBOLS = ["b200_solver_create", "b200_solver_destroy", "b200_solver_create_schu
            "b200_spm_values", "b200_spm_values_device", "b200_get_diag", "b200_batch_set", "b200_batch_thresholds",
            "b200_batch_pivots", "b200_batch_berr", "b200_numfact", "b200_numfact_trace",
            "b200_solve_trace", "b200_trace_launches", "b200_trace_kinds", "b200_solve",
-           "b200_solve_device", "b200_solve_device_noalloc", "b200_refine", "b200_refine_device", "b200_spmv", "b200_factor_download",
+           "b200_solve_device", "b200_solve_device_noalloc", "b200_refine", "b200_refine_device", "b200_spmv", "b200_spmv_device", "b200_factor_download",
            "b200_stats", "b200_strerror"]
 
 
@@ -69,6 +69,7 @@ def lib():
         L.b200_batch_thresholds.argtypes = [_P, _P, _I64]
         L.b200_batch_berr.argtypes = [_P, _P, _I64]
         L.b200_batch_pivots.argtypes = [_P, _P, _I64]
+        L.b200_spmv_device.argtypes = [_P, _I64, C.c_double, _P, _I64, C.c_double, _P, _I64, _P]
         L.b200_spm_values.argtypes = [_P, _P, C.c_double]
         L.b200_spm_values_device.argtypes = [_P, _P, C.c_double, _P]
         L.b200_trace_kinds.argtypes = [_P, _P, _P, C.c_int]
@@ -303,6 +304,13 @@ class Solver:
         y2 = np.zeros_like(x2) if y is None else np.asfortranarray(np.array(y, dtype=np.float64).reshape(self.n, -1))
         check(lib().b200_spmv(self.h, x2.shape[1], alpha, _p(x2), self.n, beta, _p(y2), self.n), "b200_spmv")
         return y2.reshape(np.shape(x))
+
+    def spmv_device(self, d_x: int, d_y: int, nrhs: int, alpha=1.0, beta=0.0, ld: int | None = None,
+                    stream: int | None = None):
+        """y = alpha A x + beta y on device column-major n x nrhs blocks (asynchronous)."""
+        ld = self.n if ld is None else ld
+        check(lib().b200_spmv_device(self.h, nrhs, alpha, _P(d_x), ld, beta, _P(d_y), ld,
+                                     _P(stream) if stream else None), "b200_spmv_device")
 
     def factor(self):
         """The factor in PaStiX's coeftab layout (2D blocks), as float64 arrays."""

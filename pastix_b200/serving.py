@@ -1,0 +1,138 @@
+"""Serving solve requests from a resident factor.
+
+The reference serves a stream of right-hand sides from one instance:
+``pastix_task_solve`` then ``pastix_task_refine`` per request
+(sopalin/pastix_task_solve.c:550, refinement/pastix_task_refine.c:226), and
+``pastix_task_numfact`` again when the values change on the same pattern (the
+analysis is kept, sopalin/pastix_task_sopalin.c:563).  ``SolveServer`` is that loop
+on one B200: the factor and the bcsc stay in device memory, requests arrive as
+device blocks, and a refactorization takes the new values on the device
+(``b200_spm_values_device``: the bcsc gathered from the input matrix's values, its
+norm computed there) before ``b200_numfact``.
+
+Every request is solved and then refined to the backward-error target (the FP64
+path too: its refinement checks the residual and usually stops at once).  Requests
+are padded with zero columns to a few column counts (powers of two up to 16, then
+multiples of 16) so that the workspaces, sized once for the largest count at
+warm-up, are never reallocated while serving; the padded columns converge at once
+(zero right-hand side).
+"""
+from __future__ import annotations
+
+import time
+
+import numpy as np
+
+from . import native
+
+
+def bucket(nrhs: int) -> int:
+    """Column count a request of nrhs columns is padded to."""
+    if nrhs < 1:
+        raise ValueError("a request has at least one column")
+    if nrhs <= 16:
+        return 1 << (nrhs - 1).bit_length()
+    return -(-nrhs // 16) * 16
+
+
+def buckets(max_nrhs: int) -> list[int]:
+    out = sorted({bucket(k) for k in range(1, max_nrhs + 1)})
+    return out
+
+
+def fifo_latencies(arrivals, service) -> np.ndarray:
+    """Latency (completion - arrival) of requests served one at a time in arrival
+    order: completion_i = max(arrival_i, completion_{i-1}) + service_i."""
+    arrivals = np.asarray(arrivals, dtype=np.float64)
+    service = np.asarray(service, dtype=np.float64)
+    done = np.empty_like(arrivals)
+    t = -np.inf
+    for i in range(arrivals.size):
+        t = max(arrivals[i], t) + service[i]
+        done[i] = t
+    return done - arrivals
+
+
+class SolveServer:
+    """One resident factorization answering solve requests on device buffers
+    (column-major n x nrhs blocks; as torch tensors of shape (nrhs, n))."""
+
+    def __init__(self, analysis, precision: str = "tf32x3", method: str = "cg", eps: float = 1e-12,
+                 itermax: int = 250, gmres_im: int = 25, max_nrhs: int = 256, device: int = 0):
+        import torch
+        self.torch = torch
+        self.dev = torch.device("cuda", device)
+        st = analysis.structure()
+        self.n = st.n
+        self.precision = precision
+        self.method, self.eps, self.itermax, self.im = method, eps, itermax, gmres_im
+        self.solver = native.Solver(st, analysis.facto_name, precision)
+        self.solver.bcsc_load(analysis.bcsc())
+        nnz, lmap, umap = analysis.spm_maps()
+        self.solver.spm_map(nnz, lmap, umap)
+        self.max_nrhs = bucket(max_nrhs)
+        self.d_b = torch.zeros((self.max_nrhs, self.n), dtype=torch.float64, device=self.dev)
+        self.d_x = torch.zeros_like(self.d_b)
+        self.d_vals = torch.empty(nnz, dtype=torch.float64, device=self.dev)
+        self.factored = False
+
+    def _stream(self) -> int:
+        # torch's current stream (0, the legacy default stream, selects the solver's
+        # own); every call below is bracketed by device synchronizations
+        return self.torch.cuda.current_stream(self.dev).cuda_stream
+
+    def refactor(self, values) -> dict:
+        """New values of the input matrix (host array or CUDA tensor, in the
+        analysis's entry order): device bcsc, then the factorization."""
+        t = self.torch
+        v = values if isinstance(values, t.Tensor) else t.from_numpy(np.ascontiguousarray(values, dtype=np.float64))
+        self.d_vals.copy_(v)
+        t.cuda.synchronize(self.dev)
+        t0 = time.perf_counter()
+        self.solver.spm_values_device(self.d_vals.data_ptr(), -1.0, self._stream())
+        t.cuda.synchronize(self.dev)
+        npiv = self.solver.numfact(0.0)
+        self.factored = True
+        return dict(ms=(time.perf_counter() - t0) * 1e3, nbpivots=npiv, numfact_ms=self.solver.stats()["numfact_ms"])
+
+    def matvec(self, x):
+        """A x for a device block x of shape (nrhs, n), with the current values."""
+        y = self.torch.empty_like(x)
+        self.torch.cuda.synchronize(self.dev)
+        self.solver.spmv_device(x.data_ptr(), y.data_ptr(), x.shape[0], 1.0, 0.0, stream=self._stream())
+        self.torch.cuda.synchronize(self.dev)
+        return y
+
+    def warm_up(self):
+        """Workspaces for the largest request first, then one pass of every column
+        count, so that serving allocates nothing."""
+        for nb in sorted(buckets(self.max_nrhs), reverse=True):
+            self.solve(self.torch.zeros((nb, self.n), dtype=self.torch.float64, device=self.dev))
+
+    def solve(self, b):
+        """x with A x = b for a device block b of shape (nrhs, n): solve, then
+        refinement to the target.  Returns (x view, info)."""
+        if not self.factored:
+            raise RuntimeError("refactor() first")
+        t = self.torch
+        nrhs = b.shape[0]
+        nb = bucket(nrhs)
+        if nb > self.max_nrhs:
+            raise ValueError(f"request of {nrhs} columns above the server's {self.max_nrhs}")
+        self.d_b[:nrhs].copy_(b)
+        if nb > nrhs:
+            self.d_b[nrhs:nb].zero_()
+        self.d_x[:nb].copy_(self.d_b[:nb])
+        t.cuda.synchronize(self.dev)
+        t0 = time.perf_counter()
+        st = self._stream()
+        self.solver.solve_device(self.d_x.data_ptr(), nb, self.n, stream=st)
+        it, berr = self.solver.refine_device(self.d_b.data_ptr(), self.d_x.data_ptr(), nb, self.method, self.eps,
+                                             self.itermax, self.im, stream=st)
+        t.cuda.synchronize(self.dev)
+        ms = (time.perf_counter() - t0) * 1e3
+        return self.d_x[:nrhs], dict(ms=ms, iters=it, berr=berr[:nrhs], nrhs=nrhs, padded=nb)
+
+    def close(self):
+        self.solver.close()
+        del self.d_b, self.d_x, self.d_vals
