@@ -34,6 +34,8 @@ struct DevSym {
     const int *rowoff;    // [bloknbr] first panel row of the block inside its cblk
     const int *fcblk;     // [bloknbr] facing cblk
     const int *csys;      // [cblknbr] system of each cblk of a batch; nullptr: one system
+    const int64_t *rbase; // [cblknbr] first entry of cblk k in prow
+    const int *prow;      // [sum of strides] global row of every panel row, cblk after cblk
 };
 
 #ifdef __CUDACC__

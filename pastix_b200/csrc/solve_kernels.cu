@@ -17,12 +17,7 @@
 namespace b200 {
 
 __device__ __forceinline__ int panel_row_to_global(const DevSym &s, int k, int prow) {
-    int lo = s.fblok[k], hi = s.fblok[k + 1] - 1;
-    while (lo < hi) {
-        const int mid = (lo + hi + 1) >> 1;
-        if (s.rowoff[mid] <= prow) lo = mid; else hi = mid - 1;
-    }
-    return s.frow[lo] + (prow - s.rowoff[lo]);
+    return s.prow[s.rbase[k] + prow];
 }
 
 template <typename T, typename V>
@@ -296,9 +291,10 @@ __global__ void __launch_bounds__(128) solve_mm_kernel(DevSym s, const SolveTile
     int shift = 0;  // the staged tile starts at ms + shift
     if (MODE == OFF_FWD || MODE == OFF_BWD) {
         const int rows = min(STT, s.stride[k] - t.row0), cols = min(STT, n - t.col0);
+        // the tile's copies first: the row map's loads then overlap them
+        shift = stage_tile16<T, PM>(ms, M + s.off[k], s.ld[k], t.row0, t.col0, s.stride[k], n);
         if (tid < STT) rmap[tid] = (tid < rows) ? panel_row_to_global(s, k, t.row0 + tid) : 0;
         __syncthreads();
-        shift = stage_tile16<T, PM>(ms, M + s.off[k], s.ld[k], t.row0, t.col0, s.stride[k], n);
         nout = ROW ? rows : cols;
         nk = ROW ? cols : rows;
         if (MODE == OFF_FWD) xsrc = xin + s.fcol[k] + t.col0;

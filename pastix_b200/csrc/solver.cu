@@ -1456,8 +1456,28 @@ int b200_solver_create_schur(const b200_symbol_t *sym, int facto, int precision,
     if (!rc) rc = s->dupload(&d_fcblk, s->fcblk);
     if (!rc) rc = s->dupload(&s->d_peri, s->peri);
     if (!rc) {
-        s->ds = DevSym{s->n, N, B, d_fcol, d_ncols, d_stride, d_ld, d_off, d_fblok, d_frow, d_lrow, d_rowoff, d_fcblk};
-        rc = build_schedule(s);
+        // global row of every panel row (blocks stacked in block order in the panel)
+        std::vector<int64_t> rbase(N);
+        std::vector<int> prow;
+        int64_t pos = 0;
+        for (int k = 0; k < N && !rc; k++) {
+            rbase[k] = pos;
+            for (int b = s->fblok[k]; b < s->fblok[k + 1]; b++)
+                for (int r = s->frow[b]; r <= s->lrow[b]; r++) prow.push_back(r);
+            pos = (int64_t)prow.size();
+            if (pos - rbase[k] != s->stride[k]) rc = ERR_BADPARAM;
+        }
+        int64_t *d_rbase = nullptr;
+        int *d_prow = nullptr;
+        if (!rc) rc = s->dupload(&d_rbase, rbase);
+        if (!rc) rc = s->dupload(&d_prow, prow);
+        if (!rc && cudaStreamSynchronize(s->st) != cudaSuccess) rc = ERR_INTERNAL;  // before the vectors go
+        if (!rc) {
+            s->ds = DevSym{s->n, N, B, d_fcol, d_ncols, d_stride, d_ld, d_off, d_fblok, d_frow, d_lrow, d_rowoff, d_fcblk};
+            s->ds.rbase = d_rbase;
+            s->ds.prow = d_prow;
+            rc = build_schedule(s);
+        }
     }
     if (!rc) rc = dalloc((char **)&s->dL, (size_t)s->arena * s->esz);
     if (!rc && facto == FACTO_GETRF) rc = dalloc((char **)&s->dU, (size_t)s->arena * s->esz);
