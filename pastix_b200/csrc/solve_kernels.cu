@@ -87,7 +87,8 @@ template void launch_convert<float, double>(int, int, const float *, int64_t, do
 //
 // The off-diagonal and diagonal-inverse products of the supernodal solves as
 // small GEMMs on tensor cores, one CTA (4 warps) per 64 x 64 tile of the factor
-// (or of a diagonal-block inverse W) times up to 32 right-hand sides per pass:
+// (or of a diagonal-block inverse W) times 16 (FP32) or 32 (FP64) right-hand sides
+// per pass:
 //   OFF_FWD : b[grow(r)] -= sum_c P[r][c] x_k[c]     (solve_blok_zgemm forward,
 //             kernels/solve_ztrsmsp.c:275-280; warp = 16 rows)
 //   OFF_BWD : b_k[c]     -= sum_r P[r][c] x[grow(r)] (backward; warp = 16 columns)
@@ -101,15 +102,17 @@ template void launch_convert<float, double>(int, int, const float *, int64_t, do
 namespace b200 {
 
 constexpr int STT = 64;          // tile rows / columns
-constexpr int SRHS = 32;         // right-hand sides per pass
 constexpr int SM_FWD = 72;       // pitch of a staged tile read row-wise by the fragments
 constexpr int SM_BWD = 68;       // pitch of a staged tile read column-wise
 enum { OFF_FWD = 0, OFF_BWD = 1, DIAG_FWD = 2, DIAG_BWD = 3 };
 
-// padded row of the staged x tile: conflict-free fragment reads
+// Right-hand sides per pass (R) and the padded row of the staged x tile (P,
+// conflict-free fragment reads): 16 for FP32 vectors, so that a CTA's shared
+// memory stays at 24 KB (9 CTAs per SM), 32 for FP64.
 template <typename V>
 struct XPitch {
-    static constexpr int P = sizeof(V) == 8 ? SRHS + 4 : SRHS + 8;
+    static constexpr int R = sizeof(V) == 8 ? 32 : 16;
+    static constexpr int P = sizeof(V) == 8 ? R + 4 : R + 8;
 };
 
 __device__ __forceinline__ unsigned sm_addr(const void *p) { return (unsigned)__cvta_generic_to_shared(p); }
@@ -169,10 +172,11 @@ __device__ __forceinline__ void stage_x(V *xs, const V *xv, const int *rowmap, i
     const bool ok0 = i0 < ni, ok1 = i1 < ni;
     const V *x0 = xv + (ok0 ? (rowmap ? rowmap[i0] : i0) : 0);
     const V *x1 = xv + (ok1 ? (rowmap ? rowmap[i1] : i1) : 0);
-    for (int j = w; j < SRHS; j += nw) {
-        const bool jok = j < R;
-        cp_async_el(xs + i0 * XP + j, x0 + (size_t)(q0 + j) * ldx, jok && ok0);
-        cp_async_el(xs + i1 * XP + j, x1 + (size_t)(q0 + j) * ldx, jok && ok1);
+    // columns j >= R are not staged: an output column of the products reads only its
+    // own x column, and those outputs are discarded
+    for (int j = w; j < R; j += nw) {
+        cp_async_el(xs + i0 * XP + j, x0 + (size_t)(q0 + j) * ldx, ok0);
+        cp_async_el(xs + i1 * XP + j, x1 + (size_t)(q0 + j) * ldx, ok1);
     }
 }
 
@@ -263,7 +267,7 @@ struct SolveSmem {
     static constexpr int BYTES = STT * PM * (int)sizeof(T) + STT * XPitch<V>::P * (int)sizeof(V);
 };
 
-// One 64 x 64 tile times up to 32 right-hand sides per pass.  Task {k, row0, col0}:
+// One 64 x 64 tile times 16 (FP32) or 32 (FP64) right-hand sides per pass.  Task {k, row0, col0}:
 //   OFF_*  : panel rows [row0, row0 + 64) x columns [col0, col0 + 64) of cblk k
 //   DIAG_* : output tile [row0, row0 + 64) of cblk k, K chunk [col0, col0 + 64) of
 //            W_k (forward) or W_k^T (backward); the output (zeroed before the sweep)
@@ -312,8 +316,8 @@ __global__ void __launch_bounds__(128) solve_mm_kernel(DevSym s, const SolveTile
         }
         xsrc = xin + s.fcol[k] + t.col0;
     }
-    for (int q0 = 0; q0 < nrhs; q0 += SRHS) {
-        const int R = min(SRHS, nrhs - q0), ntn = (R + 7) >> 3;
+    for (int q0 = 0; q0 < nrhs; q0 += XPitch<V>::R) {
+        const int R = min(XPitch<V>::R, nrhs - q0), ntn = (R + 7) >> 3;
         if (q0 > 0) __syncthreads();
         stage_x<V>(xs, xsrc, xmap, nk, ldx, q0, R);
         cp_commit();
@@ -556,7 +560,7 @@ __device__ bool flow_wait(const int *c, int target, const int *abort_word) {
 template <typename V, int NT>
 __device__ __forceinline__ void stage_x_cg(V *xs, const V *xv, const int *rowmap, int ni, int64_t ldx, int q0, int R) {
     constexpr int XP = XPitch<V>::P;
-    stage_n<STT * SRHS / NT, V>(
+    stage_n<STT * XPitch<V>::R / NT, V>(
         [&](int u) {
             const int idx = threadIdx.x + NT * u, i = idx % STT, j = idx / STT;
             return (i < ni && j < R) ? __ldcg(xv + (rowmap ? rowmap[i] : i) + (size_t)(q0 + j) * ldx) : (V)0;
@@ -761,8 +765,8 @@ __global__ void __launch_bounds__(FLOW_THREADS) solve_flow_kernel(DevSym s, cons
                 __syncthreads();
             }
             cp_commit();
-            for (int q0 = 0; q0 < nrhs; q0 += SRHS) {
-                const int R = min(SRHS, nrhs - q0), ntn = (R + 7) >> 3;
+            for (int q0 = 0; q0 < nrhs; q0 += XPitch<V>::R) {
+                const int R = min(XPitch<V>::R, nrhs - q0), ntn = (R + 7) >> 3;
                 if (q0 > 0) __syncthreads();
                 stage_x_cg<V, FLOW_THREADS>(xs, xsrc, xmap, nk, ldx, q0, R);
                 cp_wait<0>();
