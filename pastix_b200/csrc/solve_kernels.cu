@@ -239,6 +239,9 @@ template <typename T, int PM, int ROW>
 __device__ __forceinline__ void tile_mma(float (&acc)[4][4], const T *ms, const float *xs, int o0w, int ntn) {
     constexpr int XP = XPitch<float>::P;
     const int lane = threadIdx.x & 31, g = lane >> 2, tg = lane & 3;
+    // the hi*hi products and the two correction terms in separate accumulators: two
+    // shorter dependency chains per output tile instead of one of three MMAs
+    float cor[4][4] = {};
 #pragma unroll 2
     for (int kk = 0; kk < STT; kk += 8) {
         uint32_t ah[4], al[4];
@@ -254,11 +257,15 @@ __device__ __forceinline__ void tile_mma(float (&acc)[4][4], const T *ms, const 
                 tf32_split(xs[(kk + tg) * XP + nt * 8 + g], bh[0], bl[0]);
                 tf32_split(xs[(kk + tg + 4) * XP + nt * 8 + g], bh[1], bl[1]);
                 mma_tf32_16x8x8(acc[nt], ah, bh);
-                mma_tf32_16x8x8(acc[nt], ah, bl);
-                mma_tf32_16x8x8(acc[nt], al, bh);
+                mma_tf32_16x8x8(cor[nt], ah, bl);
+                mma_tf32_16x8x8(cor[nt], al, bh);
             }
         }
     }
+#pragma unroll
+    for (int nt = 0; nt < 4; nt++)
+#pragma unroll
+        for (int e = 0; e < 4; e++) acc[nt][e] += cor[nt][e];
 }
 
 template <typename T, typename V, int MODE>
@@ -380,6 +387,7 @@ __global__ void __launch_bounds__(128) solve_leaf_kernel(DevSym s, const int *__
 #pragma unroll
             for (int j = 0; j < LEAF_R; j++) y[j] = 0;
             if (lane < n) {
+#pragma unroll 4
                 for (int c = 0; c <= lane; c++) {
                     const V wv = (V)Wk[lane + (size_t)c * n];
 #pragma unroll
@@ -400,6 +408,7 @@ __global__ void __launch_bounds__(128) solve_leaf_kernel(DevSym s, const int *__
                 V acc[LEAF_R];
 #pragma unroll
                 for (int j = 0; j < LEAF_R; j++) acc[j] = 0;
+#pragma unroll 4
                 for (int c = 0; c < n; c++) {
                     const V pv = (V)Pk[r + (size_t)c * ld];
 #pragma unroll
@@ -425,6 +434,7 @@ __global__ void __launch_bounds__(128) solve_leaf_kernel(DevSym s, const int *__
                 }
                 __syncwarp();
                 if (lane < n) {
+#pragma unroll 4
                     for (int i = 0; i < nr; i++) {
                         const V pv = (V)Pk[r0 + i + (size_t)lane * ld];
 #pragma unroll
