@@ -23,12 +23,12 @@ _I64 = C.c_int64
 _lib = None
 
 # exported symbols, in the order of include/pastix_b200.h
-SYMBOLS = ["b200_solver_create", "b200_solver_destroy", "b200_solver_create_schur", "b200_get_schur",
-           "b200_applyorder", "b200_trsm", "b200_bcsc_load", "b200_bcsc_values", "b200_spm_map",
-           "b200_spm_values", "b200_spm_values_device", "b200_get_diag", "b200_batch_set", "b200_batch_thresholds",
-           "b200_batch_pivots", "b200_batch_berr", "b200_numfact", "b200_numfact_trace",
-           "b200_solve_trace", "b200_trace_launches", "b200_trace_kinds", "b200_solve",
-           "b200_solve_device", "b200_solve_device_noalloc", "b200_refine", "b200_refine_device", "b200_spmv", "b200_spmv_device", "b200_factor_download",
+SYMBOLS = ["b200_solver_create", "b200_solver_destroy", "b200_solver_create_schur", "b200_bcsc_load",
+           "b200_bcsc_values", "b200_get_schur", "b200_applyorder", "b200_trsm", "b200_get_diag", "b200_batch_set",
+           "b200_batch_thresholds", "b200_batch_pivots", "b200_batch_berr", "b200_spm_map", "b200_spm_values",
+           "b200_spm_values_device", "b200_numfact", "b200_numfact_trace", "b200_solve", "b200_solve_trace",
+           "b200_trace_launches", "b200_trace_kinds", "b200_solve_device", "b200_solve_device_noalloc",
+           "b200_refine", "b200_refine_device", "b200_spmv", "b200_spmv_device", "b200_factor_download",
            "b200_stats", "b200_strerror"]
 
 
