@@ -101,3 +101,20 @@ def test_batch_rejects_mixed_factorizations():
         concat_structures([a, b])
     with pytest.raises(ValueError):
         concat_structures([])
+
+
+@pytest.mark.parametrize("facto", ["potrf", "getrf"])
+def test_batch_of_one_is_the_system(facto):
+    """A batch of a single system is that system's own structure, table by table."""
+    A = _systems(facto)[1]
+    st = Analysis(A, facto).structure()
+    ba = BatchAnalysis([A], facto)
+    bt = ba.structure()
+    for name in ["cblk_fcolnum", "cblk_lcolnum", "cblk_fblok", "cblk_stride", "cblk_lcolidx", "cblk_brownum",
+                 "blok_frownum", "blok_lrownum", "blok_coefind", "blok_browind", "browtab", "permtab", "peritab"]:
+        assert np.array_equal(getattr(bt, name)[:len(getattr(st, name))], getattr(st, name)), name
+    assert np.array_equal(bt.blok_fcblknm[:-1], st.blok_fcblknm[:-1])
+    assert (bt.n, bt.cblknbr, bt.bloknbr, bt.brownbr, bt.coefnbr) == (st.n, st.cblknbr, st.bloknbr, st.brownbr,
+                                                                       st.coefnbr)
+    assert bt.thflops == st.thflops
+    assert list(ba.sys_cblk) == [0, st.cblknbr]
