@@ -55,6 +55,9 @@ def parse():
                          "tf32x3) through the library, then exit")
     ap.add_argument("--solve-once", action="store_true",
                     help="with --numfact-once: also one solve of the right-hand sides (profiling aid)")
+    ap.add_argument("--refine-once", action="store_true",
+                    help="with --numfact-once --solve-once: then one CG refinement of that solution, alone between "
+                         "cudaProfilerStart and cudaProfilerStop (profiling aid, ncu --profile-from-start off)")
     ap.add_argument("--cpu-budget", type=float, default=150.0, help="seconds of CPU time for the reference arm")
     return ap.parse_args()
 
@@ -347,6 +350,15 @@ def main():
             x = s.solve(b)
             out["solve_ms"] = s.stats()["solve_ms"]
             out["berr"] = float(np.max(np.linalg.norm(b - A.matvec(x), axis=0) / np.linalg.norm(b, axis=0)))
+            if args.refine_once:
+                torch.cuda.synchronize()
+                torch.cuda.cudart().cudaProfilerStart()
+                x, it, berr = s.refine(b, x, "cg", BERR_TARGET, 50, 25)
+                torch.cuda.synchronize()
+                torch.cuda.cudart().cudaProfilerStop()
+                out["refine_ms"] = s.stats()["refine_ms"]
+                out["refine_iters"] = it
+                out["berr_refined"] = float(berr.max())
         print(json.dumps(out), flush=True)
         s.close()
         return 0

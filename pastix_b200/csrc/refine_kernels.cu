@@ -139,8 +139,7 @@ static inline unsigned nblk(int64_t tot, int bs) { return (unsigned)((tot + bs -
 
 // Several right-hand sides: the columns r0 .. r0 + 15 of x first gathered
 // row-major (16 doubles = 128 contiguous bytes per row), so that every matrix entry
-// gathers one line instead of 16 scattered ones; then warp per row, every entry read
-// once and applied to the 16 columns in registers, one butterfly per column.
+// gathers one line instead of 16 scattered ones; then half a warp per row.
 constexpr int SPMV_R = 16;
 
 __global__ void gather_rows_kernel(int n, int R, const double *__restrict__ x, int64_t ldx, double *__restrict__ xt) {
@@ -154,39 +153,36 @@ __global__ void gather_rows_kernel(int n, int R, const double *__restrict__ x, i
     for (int h = 0; h < SPMV_R / 2; h++) o[h] = make_double2(v[2 * h], v[2 * h + 1]);
 }
 
+// Half a warp per row, lane c of the half = right-hand side c: every entry is one
+// broadcast load of its value and row index and one contiguous 128-byte load of the
+// staged x row, accumulated in the row's order; no reduction across lanes.
 __global__ void __launch_bounds__(256) spmv_rows_kernel(int n, int R, const int64_t *__restrict__ colptr,
                                                         const int *__restrict__ rowtab,
                                                         const double *__restrict__ vals,
                                                         const double *__restrict__ xt, double *y, int64_t ldy,
                                                         double alpha, double beta) {
-    const int warp = (blockIdx.x * blockDim.x + threadIdx.x) >> 5;
-    const int lane = threadIdx.x & 31;
-    if (warp >= n) return;
-    const int64_t e0 = colptr[warp], e1 = colptr[warp + 1];
-    double acc[SPMV_R];
-#pragma unroll
-    for (int r = 0; r < SPMV_R; r++) acc[r] = 0.0;
-    for (int64_t e = e0 + lane; e < e1; e += 32) {
-        const double v = vals[e];
-        const double2 *xr = reinterpret_cast<const double2 *>(xt + (int64_t)rowtab[e] * SPMV_R);
-#pragma unroll
-        for (int h = 0; h < SPMV_R / 2; h++) {
-            const double2 q = xr[h];
-            acc[2 * h] += v * q.x;
-            acc[2 * h + 1] += v * q.y;
-        }
+    const int64_t t = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
+    const int64_t row = t / SPMV_R;
+    const int c = (int)(t % SPMV_R);
+    if (row >= n) return;
+    const int64_t e0 = colptr[row], e1 = colptr[row + 1];
+    const double *xc = xt + c;
+    double acc = 0.0;
+    int64_t e = e0;
+    for (; e + 4 <= e1; e += 4) {
+        const int j0 = rowtab[e], j1 = rowtab[e + 1], j2 = rowtab[e + 2], j3 = rowtab[e + 3];
+        const double v0 = vals[e], v1 = vals[e + 1], v2 = vals[e + 2], v3 = vals[e + 3];
+        const double x0 = xc[(int64_t)j0 * SPMV_R], x1 = xc[(int64_t)j1 * SPMV_R];
+        const double x2 = xc[(int64_t)j2 * SPMV_R], x3 = xc[(int64_t)j3 * SPMV_R];
+        acc = fma(v0, x0, acc);
+        acc = fma(v1, x1, acc);
+        acc = fma(v2, x2, acc);
+        acc = fma(v3, x3, acc);
     }
-    double mine = 0.0;
-#pragma unroll
-    for (int r = 0; r < SPMV_R; r++) {
-        double a = acc[r];
-#pragma unroll
-        for (int o = 16; o > 0; o >>= 1) a += __shfl_xor_sync(0xffffffffu, a, o);
-        if (lane == r) mine = a;
-    }
-    if (lane < R) {
-        double *yp = y + warp + (int64_t)lane * ldy;
-        *yp = (beta == 0.0) ? alpha * mine : alpha * mine + beta * *yp;
+    for (; e < e1; e++) acc = fma(vals[e], xc[(int64_t)rowtab[e] * SPMV_R], acc);
+    if (c < R) {
+        double *yp = y + row + (int64_t)c * ldy;
+        *yp = (beta == 0.0) ? alpha * acc : alpha * acc + beta * *yp;
     }
 }
 
@@ -197,8 +193,8 @@ void launch_spmv(int n, int nrhs, const int64_t *colptr, const int *rowtab, cons
         for (int r0 = 0; r0 < nrhs; r0 += SPMV_R) {
             const int R = nrhs - r0 < SPMV_R ? nrhs - r0 : SPMV_R;
             gather_rows_kernel<<<nblk(n, 256), 256, 0, st>>>(n, R, x + (int64_t)r0 * ldx, ldx, xt);
-            spmv_rows_kernel<<<nblk((int64_t)n * 32, 256), 256, 0, st>>>(n, R, colptr, rowtab, vals, xt,
-                                                                          y + (int64_t)r0 * ldy, ldy, alpha, beta);
+            spmv_rows_kernel<<<nblk((int64_t)n * SPMV_R, 256), 256, 0, st>>>(n, R, colptr, rowtab, vals, xt,
+                                                                              y + (int64_t)r0 * ldy, ldy, alpha, beta);
         }
     } else {
         spmv_kernel<<<nblk((int64_t)n * 32, 256), 256, 0, st>>>(n, nrhs, colptr, rowtab, vals, x, ldx, y, ldy, alpha,
