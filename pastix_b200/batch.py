@@ -144,11 +144,20 @@ class BatchAnalysis:
     def system_structure(self, i: int) -> SolverStructure:
         return self.patterns[self.keys[i]].structure
 
+    def _check_values(self, values):
+        vals = values if values is not None else [A.values for A in self.mats]
+        if len(vals) != self.nsys:
+            raise ValueError(f"{len(vals)} value arrays for {self.nsys} systems")
+        for i, (v, A) in enumerate(zip(vals, self.mats)):
+            if np.size(v) != A.values.size:
+                raise ValueError(f"system {i}: {np.size(v)} values for {A.values.size} entries")
+        return vals
+
     def bcsc(self, values=None) -> BCSC:
         """The batch's bcsc from every system's values (``values``: one array per
         system, default the matrices' own), gathered through the pattern maps that
         PaStiX's own bcsc construction produced."""
-        vals = values if values is not None else [A.values for A in self.mats]
+        vals = self._check_values(values)
         bcs = []
         for i, key in enumerate(self.keys):
             p = self.patterns[key]
@@ -169,14 +178,22 @@ class BatchAnalysis:
 
     def values(self, values=None) -> np.ndarray:
         """The systems' input values concatenated (the order ``spm_maps`` reads)."""
-        vals = values if values is not None else [A.values for A in self.mats]
-        return np.concatenate([np.asarray(v, dtype=np.float64) for v in vals])
+        vals = self._check_values(values)
+        return np.concatenate([np.asarray(v, dtype=np.float64).ravel() for v in vals])
 
     def split(self, x) -> list[np.ndarray]:
         """Rows of a batch vector (original numbering) split by system."""
+        if np.shape(x)[0] != self.st.n:
+            raise ValueError(f"{np.shape(x)[0]} rows for a batch of {self.st.n} unknowns")
         return [x[self.sys_col[i]:self.sys_col[i + 1]] for i in range(self.nsys)]
 
     def join(self, xs) -> np.ndarray:
+        """The systems' right-hand sides (or solutions) stacked in batch order."""
+        if len(xs) != self.nsys:
+            raise ValueError(f"{len(xs)} blocks for {self.nsys} systems")
+        for i, (x, A) in enumerate(zip(xs, self.mats)):
+            if np.shape(x)[0] != A.n:
+                raise ValueError(f"system {i}: {np.shape(x)[0]} rows for {A.n} unknowns")
         return np.concatenate([np.asarray(x, dtype=np.float64) for x in xs], axis=0)
 
     def coef_ranges(self) -> list[tuple[int, int]]:

@@ -118,3 +118,18 @@ def test_batch_of_one_is_the_system(facto):
                                                                        st.coefnbr)
     assert bt.thflops == st.thflops
     assert list(ba.sys_cblk) == [0, st.cblknbr]
+
+
+def test_batch_rejects_mismatched_inputs():
+    mats = _systems("potrf")
+    ba = BatchAnalysis(mats, "potrf")
+    with pytest.raises(ValueError):
+        ba.bcsc([A.values for A in mats[:-1]])
+    with pytest.raises(ValueError):
+        ba.values([A.values[:-1] for A in mats])
+    with pytest.raises(ValueError):
+        ba.join([np.zeros(A.n + 1) for A in mats])
+    with pytest.raises(ValueError):
+        ba.split(np.zeros(ba.structure().n - 1))
+    x = ba.join([np.full(A.n, float(i)) for i, A in enumerate(mats)])
+    assert [float(v[0]) for v in ba.split(x)] == [0.0, 1.0, 2.0, 3.0]
