@@ -470,6 +470,21 @@ def main():
     if traffic:
         roofline["traffic_source"] = traffic.get("source")
 
+    # the solve against HBM: the algorithmic bytes of both sweeps (every factor entry
+    # once per sweep, diagonal blocks as their inverses' triangles, and the vectors;
+    # b200_solve_trace) over the measured p50 of the whole solve
+    try:
+        tr = hs.solve_trace(nrhs)
+        sbytes = tr["forward"]["bytes"] + tr["backward"]["bytes"]
+        hbm = measured_peaks().get("hbm_gbs")
+        gbs = sbytes / (p50 * 1e-3) / 1e9
+        solve_roofline = {"bound": "hbm", "achieved": gbs, "peak": hbm, "unit": "GB/s",
+                          "frac": (gbs / hbm) if hbm else None, "bytes_per_solve": sbytes, "ms": p50,
+                          "traced_sweeps_ms": tr["forward"]["ms"] + tr["backward"]["ms"],
+                          "peak_source": "MEASURED_PEAKS.json hbm_gbs", "path": head["prec"], "nrhs": nrhs}
+    except Exception as exc:  # an auxiliary figure: the line stands without it
+        solve_roofline = {"unavailable": str(exc)}
+
     if rank == 0:
         line = {
             "metric": METRIC, "value": value, "unit": "GFLOP/s", "n_gpus": world, "steps": args.steps,
@@ -487,6 +502,7 @@ def main():
             "numfact_trace": traces,
             "numfact_kinds": kinds_trace,
             "roofline": roofline,
+            "solve_roofline": solve_roofline,
             "cpu_baseline": cpu,
             "e2e": {"value": e2e_value, "unit": "GFLOP/s", "h2d_bytes_per_step": h2d, "d2h_bytes_per_step": d2h,
                     "seconds_per_step": e2e_s, "host_buffers": "pinned", "phases_ms": e2e_phases,
