@@ -136,3 +136,86 @@ class SolveServer:
     def close(self):
         self.solver.close()
         del self.d_b, self.d_x, self.d_vals
+
+
+class ContinuousBatcher:
+    """Continuous batching of solve requests on one resident factor.
+
+    Requests that arrive while a batch is on the GPU wait for the next batch
+    boundary; there the requests that have arrived are admitted in arrival order as
+    long as their columns fit in the free slots (``max_cols`` columns, the
+    workspace the server was sized for), and one multi-RHS solve + refinement serves
+    them all: their columns share every sweep, SpMV and BLAS-1 launch.  Each column
+    keeps its own refinement (its own stopping rule; a converged column is no longer
+    updated), so a request's result in the mix is its result alone up to the
+    rounding of the products' atomic accumulation.
+
+    ``backend(b)`` solves a block b of shape (ncols, n) and returns (x, info) with
+    info["berr"] per column and info["ms"] the service time; the server's
+    ``SolveServer.solve`` is one.  Time is virtual: a batch starts at the later of
+    the previous batch's end and the first pending arrival, and lasts its measured
+    service time, so latencies under a given arrival process follow from the
+    device's own service times.
+    """
+
+    def __init__(self, backend, max_cols: int, cat, split):
+        self.backend = backend
+        self.max_cols = int(max_cols)
+        self.cat = cat      # list of (k_i, n) blocks -> (sum k_i, n) block
+        self.split = split  # (block, [k_i]) -> list of (k_i, n) copies (the backend reuses its buffers)
+
+    def run(self, requests):
+        """requests: list of (arrival_time_s, b block of shape (k, n)), in any order.
+        Returns, per request in the given order, dict(x, berr, start, done, latency,
+        batch) and the list of batches (each: request indices, columns, service)."""
+        order = sorted(range(len(requests)), key=lambda i: requests[i][0])
+        for i in order:
+            if requests[i][1].shape[0] > self.max_cols:
+                raise ValueError(f"request {i}: {requests[i][1].shape[0]} columns above {self.max_cols} slots")
+        out = [None] * len(requests)
+        batches = []
+        t = 0.0
+        pos = 0
+        pending = []
+        while pos < len(order) or pending:
+            if not pending:
+                t = max(t, requests[order[pos]][0])
+            while pos < len(order) and requests[order[pos]][0] <= t:
+                pending.append(order[pos])
+                pos += 1
+            # admission: arrival order, while the columns fit in the free slots
+            take, cols = [], 0
+            for i in pending:
+                k = requests[i][1].shape[0]
+                if cols + k > self.max_cols:
+                    break
+                take.append(i)
+                cols += k
+            pending = pending[len(take):]
+            ks = [requests[i][1].shape[0] for i in take]
+            x, info = self.backend(self.cat([requests[i][1] for i in take]))
+            service = info["ms"] * 1e-3
+            xs = self.split(x, ks)
+            berr = np.asarray(info["berr"])
+            c0 = 0
+            for i, xi, k in zip(take, xs, ks):
+                out[i] = dict(x=xi, berr=berr[c0:c0 + k], start=t, done=t + service,
+                              latency=t + service - requests[i][0], batch=len(batches))
+                c0 += k
+            batches.append(dict(requests=take, cols=cols, service=service))
+            t += service
+        return out, batches
+
+
+def torch_batcher(server: SolveServer) -> ContinuousBatcher:
+    """A continuous batcher over a SolveServer's device blocks."""
+    import torch
+
+    def split(x, ks):
+        out, c0 = [], 0
+        for k in ks:
+            out.append(x[c0:c0 + k].clone())
+            c0 += k
+        return out
+
+    return ContinuousBatcher(server.solve, server.max_nrhs, lambda bs: torch.cat(bs, dim=0), split)

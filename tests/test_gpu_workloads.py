@@ -100,3 +100,39 @@ def test_serving_resident_factor_100cube():
             latency_p50_ms=round(float(np.percentile(lat, 50)), 2), latency_p99_ms=round(float(np.percentile(lat, 99)), 2),
             iters_mean=round(float(np.mean(iters)), 2))
     print(f"\nserving 100^3, {nreq} requests, nrhs total {nrhs.sum()}: {report}")
+
+
+def test_continuous_batching_same_alone_and_in_the_mix():
+    """Requests arriving faster than they are served share batches (their columns
+    in the same sweeps and refinement launches) and each gets what it gets alone:
+    both refined to <= 1e-12, and the two solutions within 1e-9 of each other (two
+    solutions with backward error <= 1e-12 differ by at most ~cond(A) 2e-12; the
+    24^3 27-point operator has cond ~ 66)."""
+    import torch
+    from pastix_b200.serving import torch_batcher
+    A = M.laplacian(24, 24, 24, 27, 26.0, shift=1e-3)
+    an = Analysis(A, "potrf")
+    srv = SolveServer(an, "tf32x3", "cg", BERR_TARGET, max_nrhs=64)
+    srv.refactor(A.values)
+    srv.warm_up()
+    rng = np.random.default_rng(8)
+    ks = rng.integers(1, 24, 12)
+    arrivals = np.cumsum(rng.exponential(0.0005, 12))
+    g = torch.Generator(device="cuda").manual_seed(5)
+    bs = [srv.matvec(torch.rand((int(k), A.n), generator=g, dtype=torch.float64, device="cuda") * 2 - 1) for k in ks]
+    alone = []
+    for b in bs:
+        x, info = srv.solve(b)
+        alone.append((x.clone(), np.array(info["berr"])))
+    out, batches = torch_batcher(srv).run(list(zip(arrivals, bs)))
+    print(f"\ncontinuous batching: {len(bs)} requests in {len(batches)} batches "
+          f"{[b['cols'] for b in batches]}, latency p50 {np.median([o['latency'] for o in out]) * 1e3:.2f} ms")
+    assert max(len(b["requests"]) for b in batches) > 1
+    for (xa, ba), o, b in zip(alone, out, bs):
+        assert ba.max() <= BERR_TARGET and o["berr"].max() <= BERR_TARGET
+        d = (torch.linalg.vector_norm(o["x"] - xa) / torch.linalg.vector_norm(xa)).item()
+        assert d <= 1e-9, d
+        r = b - srv.matvec(o["x"])
+        be = (torch.linalg.vector_norm(r, dim=1) / torch.linalg.vector_norm(b, dim=1)).max().item()
+        assert be <= 1.01 * BERR_TARGET
+    srv.close()
