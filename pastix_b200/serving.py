@@ -138,6 +138,14 @@ class SolveServer:
         del self.d_b, self.d_x, self.d_vals
 
 
+class Refactor:
+    """A same-pattern refactorization in a request stream: new values of the input
+    matrix (in the analysis's entry order)."""
+
+    def __init__(self, values):
+        self.values = values
+
+
 class ContinuousBatcher:
     """Continuous batching of solve requests on one resident factor.
 
@@ -156,9 +164,15 @@ class ContinuousBatcher:
     the previous batch's end and the first pending arrival, and lasts its measured
     service time, so latencies under a given arrival process follow from the
     device's own service times.
+
+    A ``Refactor`` item in the stream is a same-pattern refactorization
+    (``refactor(values)``, e.g. ``SolveServer.refactor``, returning info["ms"]): the
+    requests that arrived before it are served with the old factor, those after it
+    with the new one; it runs at a batch boundary, in place.
     """
 
-    def __init__(self, backend, max_cols: int, cat, split):
+    def __init__(self, backend, max_cols: int, cat, split, refactor=None):
+        self.refactor = refactor
         self.backend = backend
         self.max_cols = int(max_cols)
         self.cat = cat      # list of (k_i, n) blocks -> (sum k_i, n) block
@@ -169,8 +183,15 @@ class ContinuousBatcher:
         Returns, per request in the given order, dict(x, berr, start, done, latency,
         batch) and the list of batches (each: request indices, columns, service)."""
         order = sorted(range(len(requests)), key=lambda i: requests[i][0])
+
+        def is_ref(i):
+            return isinstance(requests[i][1], Refactor)
+
         for i in order:
-            if requests[i][1].shape[0] > self.max_cols:
+            if is_ref(i):
+                if self.refactor is None:
+                    raise ValueError(f"request {i}: a refactorization, and no refactor callback")
+            elif requests[i][1].shape[0] > self.max_cols:
                 raise ValueError(f"request {i}: {requests[i][1].shape[0]} columns above {self.max_cols} slots")
         out = [None] * len(requests)
         batches = []
@@ -183,9 +204,21 @@ class ContinuousBatcher:
             while pos < len(order) and requests[order[pos]][0] <= t:
                 pending.append(order[pos])
                 pos += 1
-            # admission: arrival order, while the columns fit in the free slots
+            if is_ref(pending[0]):
+                i = pending.pop(0)
+                info = self.refactor(requests[i][1].values)
+                service = info["ms"] * 1e-3
+                out[i] = dict(refactor=info, start=t, done=t + service, latency=t + service - requests[i][0],
+                              batch=len(batches))
+                batches.append(dict(requests=[i], cols=0, service=service, refactor=True))
+                t += service
+                continue
+            # admission: arrival order, while the columns fit in the free slots, up
+            # to the next refactorization
             take, cols = [], 0
             for i in pending:
+                if is_ref(i):
+                    break
                 k = requests[i][1].shape[0]
                 if cols + k > self.max_cols:
                     break
@@ -218,4 +251,5 @@ def torch_batcher(server: SolveServer) -> ContinuousBatcher:
             c0 += k
         return out
 
-    return ContinuousBatcher(server.solve, server.max_nrhs, lambda bs: torch.cat(bs, dim=0), split)
+    return ContinuousBatcher(server.solve, server.max_nrhs, lambda bs: torch.cat(bs, dim=0), split,
+                             refactor=server.refactor)

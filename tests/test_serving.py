@@ -78,3 +78,38 @@ def test_continuous_batching_fifo_admission_and_capacity():
     assert out[3]["start"] == 1.0
     with pytest.raises(ValueError):
         _np_batcher([], 16).run([(0.0, np.ones((17, n)))])
+
+
+def test_continuous_batching_orders_refactorizations():
+    """Requests before a refactorization are served with the old factor, requests
+    after it with the new one, whatever the batching."""
+    from pastix_b200.serving import Refactor
+    state = {"version": 1.0}
+    calls = []
+
+    def backend(b):
+        calls.append(("solve", b.shape[0]))
+        return state["version"] * b, {"berr": np.zeros(b.shape[0]), "ms": 5.0}
+
+    def refactor(values):
+        calls.append(("refactor", float(values[0])))
+        state["version"] = float(values[0])
+        return {"ms": 20.0}
+
+    def split(x, ks):
+        return [x[c0:c0 + k].copy() for c0, k in zip(np.cumsum([0] + ks[:-1]), ks)]
+
+    bat = ContinuousBatcher(backend, 64, lambda bs: np.concatenate(bs, axis=0), split, refactor=refactor)
+    n = 4
+    reqs = [(0.000, np.ones((3, n))), (0.001, np.ones((2, n))), (0.002, Refactor(np.array([2.0]))),
+            (0.003, np.ones((4, n))), (0.004, np.ones((1, n))), (0.050, Refactor(np.array([3.0]))),
+            (0.051, np.ones((2, n)))]
+    out, batches = bat.run(reqs)
+    assert np.all(out[0]["x"] == 1.0) and np.all(out[1]["x"] == 1.0)
+    assert np.all(out[3]["x"] == 2.0) and np.all(out[4]["x"] == 2.0)
+    assert np.all(out[6]["x"] == 3.0)
+    assert out[2]["refactor"]["ms"] == 20.0 and out[2]["done"] <= out[3]["start"] + 1e-12
+    # requests 3 and 4 arrived during the refactorization: served together after it
+    assert [b["requests"] for b in batches][:4] == [[0], [1], [2], [3, 4]]
+    with pytest.raises(ValueError):
+        ContinuousBatcher(backend, 64, None, None).run([(0.0, Refactor(np.array([1.0])))])
