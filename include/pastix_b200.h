@@ -209,8 +209,18 @@ int64_t b200_trace_launches( b200_solver_t *solver, double *ms, int32_t *cls, in
 int b200_trace_kinds( b200_solver_t *solver, double *ms, double *flops, int nkinds );
 
 /* Same on device memory, asynchronously on the solver's stream (or on stream if
- * not NULL). */
+ * not NULL).  Check b200_solve_status once the stream has been synchronized. */
 int b200_solve_device( b200_solver_t *solver, int64_t nrhs, double *d_b, int64_t ldb, void *stream );
+
+/* Status of the last solve or refinement of this instance, for the asynchronous
+ * device entry points (b200_solve_device, b200_solve_device_noalloc,
+ * b200_refine_device with a caller's stream): call it after synchronizing that
+ * stream.  PASTIX_ERR_INTERNAL if a sweep gave up waiting for its inputs (the
+ * result is not to be used), else PASTIX_SUCCESS.  Each solve or refinement call
+ * clears the status when it starts; the host-pointer calls check it themselves.
+ * Counterpart of the return code of pastix_task_solve
+ * (sopalin/pastix_task_solve.c:550). */
+int b200_solve_status( b200_solver_t *solver );
 
 /* Size of the fixed scratch of b200_solve_device_noalloc: 4,194,304 doubles
  * (32 MiB); a call needs 2 * n * nrhs of them. */
@@ -222,14 +232,16 @@ int b200_solve_device( b200_solver_t *solver, int64_t nrhs, double *d_b, int64_t
  * not trigger the implicit device synchronization of cudaMalloc/cudaFree, or a
  * process that must keep a fixed footprint.  Same result as b200_solve_device.
  * The permuted right-hand sides live in one fixed scratch array compiled into
- * this library (B200_NOALLOC_SCRATCH_DOUBLES doubles), which every GPU that
- * loads the library holds until the process exits; calls with
- * 2 * n * nrhs > B200_NOALLOC_SCRATCH_DOUBLES are rejected with
- * PASTIX_ERR_BADPARAMETER.  The first call on a device looks up the array's
- * device address (cudaGetSymbolAddress), so make that first call before any
- * stream capture.  All calls share the array: calls that overlap on the GPU
- * (other streams, other solver instances, other host threads) race and must be
- * serialized by the caller.  stream may be NULL (the solver's own stream). */
+ * this library (B200_NOALLOC_SCRATCH_DOUBLES doubles).  The array is reserved on a
+ * GPU when the first solver instance is created on it (b200_solver_create looks
+ * up its device address with cudaGetSymbolAddress, which loads it there) and is
+ * held until the process exits; this call itself only reads the address stored
+ * in the instance.  Calls with 2 * n * nrhs > B200_NOALLOC_SCRATCH_DOUBLES are
+ * rejected with PASTIX_ERR_BADPARAMETER.  All calls share the array: calls that
+ * overlap on the GPU (other streams, other solver instances, other host threads)
+ * race and must be serialized by the caller; each call writes every entry it
+ * reads first, so what a previous call left there does not matter.  stream may be
+ * NULL (the solver's own stream); check b200_solve_status after synchronizing. */
 int b200_solve_device_noalloc( b200_solver_t *solver, int64_t nrhs, double *d_b, int64_t ldb,
                                void *stream );
 
@@ -267,9 +279,11 @@ int b200_factor_download( b200_solver_t *solver, double *L, double *U );
 
 /* Statistics of the last calls: out[0] numfact ms, out[1] solve ms, out[2]
  * refine ms, out[3] static pivots, out[4] diag threshold used, out[5] device
- * bytes held, out[6] number of etree levels, out[7] kernel launches of the last
- * numfact, out[8] kernel launches of the last solve, out[9] coefnbr, out[10]
- * kernels run by this instance so far.  out holds 11 entries. */
+ * bytes held by the factor, out[6] number of etree levels, out[7] kernel launches
+ * of the last numfact, out[8] kernel launches of the last solve, out[9] coefnbr,
+ * out[10] kernels run by this instance so far, out[11] bytes of the solve /
+ * refinement workspace, out[12] bytes of the device copies of host vectors.
+ * out holds 13 entries. */
 int b200_stats( b200_solver_t *solver, double *out );
 
 /* Short description of a return code. */

@@ -125,7 +125,9 @@ struct b200_solver_s {
     bool panel_steps_only = false;      // environment B200_PANEL_TILES=1: always the tile-item form
     // failure-path tests (environment B200_TEST_WITHHOLD=panel|flow): the first item of
     // every panel launch / of the forward dataflow sweep is never taken, so the waits
-    // that depend on it run out and the error path is exercised
+    // that depend on it run out and the error path is exercised.  "panel" is read when
+    // the instance is created (the factorization graph is captured once); "flow" is
+    // read by every solve, so one instance can fail a solve and then run a good one
     int test_withhold = 0;
     PanelCblk *d_pcb = nullptr;
     PanelItem *d_pitem = nullptr;
@@ -190,9 +192,22 @@ struct b200_solver_s {
     std::vector<double> last_berr;  // per-problem backward errors of the last refinement
     std::vector<unsigned long long> last_piv_sys;  // pivots replaced per system by the last numfact
 
+    // status of the solve sweeps: bit 4 set by a dataflow sweep that gave up waiting;
+    // zeroed at the start of every call that runs sweeps (b200_solve_status reads it)
+    int *d_serr = nullptr;
+
+    // device of the instance and the address of the no-allocation scratch on it
+    // (looked up when the instance is created)
+    int device = 0;
+    double *noalloc_scratch = nullptr;
+
     // solve / refine workspaces
     double *d_ws = nullptr;
     size_t ws_cap = 0;
+    // device copies of the host vectors of b200_solve / b200_refine / b200_spmv,
+    // sized on first use and grown only when a call needs more
+    double *d_stage = nullptr;
+    size_t stage_cap = 0;
     std::map<int, cudaGraphExec_t> solve_graphs;  // keyed by nrhs, on the ws buffer
     double *d_scal = nullptr;                     // per-column scalars
     int scal_cap = 0;
@@ -674,6 +689,22 @@ int ensure_ws(b200_solver_t *s, size_t doubles) {
     return ERR_SUCCESS;
 }
 
+// Device copies of host vectors (the host-pointer entry points): one buffer per
+// instance, grown only when a call needs more, so repeated calls allocate nothing
+// and never pay cudaFree's device synchronization.
+int ensure_stage(b200_solver_t *s, size_t doubles) {
+    if (doubles <= s->stage_cap) return ERR_SUCCESS;
+    if (s->d_stage) {
+        CU(cudaStreamSynchronize(s->st));
+        cudaFree(s->d_stage);
+    }
+    s->d_stage = nullptr;
+    s->stage_cap = 0;
+    RET(dalloc(&s->d_stage, doubles));
+    s->stage_cap = doubles;
+    return ERR_SUCCESS;
+}
+
 int ensure_scal(b200_solver_t *s, int count) {
     if (count <= s->scal_cap) return ERR_SUCCESS;
     if (s->d_scal) cudaFree(s->d_scal);
@@ -852,6 +883,12 @@ int enqueue_numfact(b200_solver_t *s, cudaStream_t st, Trace *tr = nullptr) {
 // x updated), the backward sweep reads its input from aux
 enum { SWEEP_FORWARD = 1, SWEEP_BACKWARD = 2, SWEEP_BOTH = 3 };
 
+// B200_TEST_WITHHOLD=flow: the forward dataflow sweep's first item is withheld
+bool flow_withheld() {
+    const char *e = getenv("B200_TEST_WITHHOLD");
+    return e && !strcmp(e, "flow");
+}
+
 template <typename T>
 int enqueue_sweeps(b200_solver_t *s, T *x, T *aux, int64_t ldx, int nrhs, cudaStream_t st, int *launches,
                    Trace *tr = nullptr, int parts = SWEEP_BOTH) {
@@ -862,7 +899,7 @@ int enqueue_sweeps(b200_solver_t *s, T *x, T *aux, int64_t ldx, int nrhs, cudaSt
     const int N = s->cblknbr, nlev = (int)s->levels.size(), fl0 = s->flow_level;
     int *fl = s->d_sflags, *abort_word = fl + 2;
     CU(cudaMemsetAsync(fl, 0, ((size_t)4 * N + 4) * sizeof(int), st));
-    if (s->test_withhold & 2) CU(cudaMemsetAsync(fl, 1, 1, st));  // forward ticket = 1
+    if (flow_withheld()) CU(cudaMemsetAsync(fl, 1, 1, st));  // forward ticket = 1
     // the diagonal products accumulate their K chunks: zero their outputs (aux now, x
     // before the backward sweep; the Schur rows of x stay, they are the caller's)
     if (parts & SWEEP_FORWARD) {
@@ -886,7 +923,7 @@ int enqueue_sweeps(b200_solver_t *s, T *x, T *aux, int64_t ldx, int nrhs, cudaSt
     if (fl0 < nlev) {
         if (tr) tr->begin(st);
         launch_solve_flow<T, T>(s->ds, s->d_fitem_f, s->n_fitem_f, s->d_leaf, s->d_flist, s->d_need_f, s->d_nprev_f,
-                                L, WL, s->d_woff, x, aux, ldx, nrhs, 0, fl, fl + 4, fl + 4 + N, abort_word, s->d_err,
+                                L, WL, s->d_woff, x, aux, ldx, nrhs, 0, fl, fl + 4, fl + 4 + N, abort_word, s->d_serr,
                                 st);
         if (tr) tr->end(1, st);
         *launches += 1;
@@ -904,7 +941,7 @@ int enqueue_sweeps(b200_solver_t *s, T *x, T *aux, int64_t ldx, int nrhs, cudaSt
         if (tr) tr->begin(st);
         launch_solve_flow<T, T>(s->ds, s->d_fitem_b, s->n_fitem_b, s->d_leaf, s->d_flist, s->d_need_b, s->d_nprev_b,
                                 Ub, WB, s->d_woff, x, aux, ldx, nrhs, 1, fl + 1, fl + 4 + 2 * N, fl + 4 + 3 * N,
-                                abort_word, s->d_err, st);
+                                abort_word, s->d_serr, st);
         if (tr) tr->end(2, st);
         *launches += 1;
     }
@@ -1315,11 +1352,11 @@ constexpr int NOALLOC_MAX_DEVICES = 64;
 std::mutex g_noalloc_mutex;
 double *g_noalloc_addr[NOALLOC_MAX_DEVICES] = {};
 
-// Device address of the scratch array on the current device (looked up on the
-// first call on that device, with that device current).
-int noalloc_scratch(double **out) {
-    int dev = 0;
-    CU(cudaGetDevice(&dev));
+// Device address of the scratch array on device dev, which must be the current
+// device.  Looked up once per device, when the first instance is created on it: the
+// lookup loads this module on the device (under lazy module loading) and so reserves
+// the array there, before any no-allocation solve runs.
+int noalloc_scratch(int dev, double **out) {
     if (dev < 0 || dev >= NOALLOC_MAX_DEVICES) return ERR_INTERNAL;
     std::lock_guard<std::mutex> lock(g_noalloc_mutex);
     if (g_noalloc_addr[dev] == nullptr) {
@@ -1507,6 +1544,10 @@ int b200_solver_create_schur(const b200_symbol_t *sym, int facto, int precision,
     if (!rc) rc = s->dmalloc(&s->d_thr, 1);
     if (!rc) rc = s->dmalloc(&s->d_npiv, 1);
     if (!rc) rc = s->dmalloc(&s->d_err, 1);
+    if (!rc) rc = s->dmalloc(&s->d_serr, 1);
+    if (!rc && cudaMemsetAsync(s->d_serr, 0, sizeof(int), s->st) != cudaSuccess) rc = ERR_INTERNAL;
+    s->device = dev;
+    if (!rc) rc = noalloc_scratch(dev, &s->noalloc_scratch);
     if (!rc && cudaEventCreate(&s->ev0) != cudaSuccess) rc = ERR_INTERNAL;
     if (!rc && cudaEventCreate(&s->ev1) != cudaSuccess) rc = ERR_INTERNAL;
     if (!rc && cudaStreamSynchronize(s->st) != cudaSuccess) rc = ERR_INTERNAL;
@@ -1539,6 +1580,7 @@ int b200_solver_destroy(b200_solver_t *s) {
     if (s->d_spmv) cudaFree(s->d_spmv);
     if (s->d_dest) cudaFree(s->d_dest);
     if (s->d_ws) cudaFree(s->d_ws);
+    if (s->d_stage) cudaFree(s->d_stage);
     if (s->d_scal) cudaFree(s->d_scal);
     if (s->d_xt) cudaFree(s->d_xt);
     if (s->ev0) cudaEventDestroy(s->ev0);
@@ -1743,6 +1785,7 @@ int b200_trsm(b200_solver_t *s, int step, int64_t nrhs, double *b, int64_t ldb) 
     const int n = s->n;
     RET(ensure_ws(s, (size_t)2 * n * nrhs));
     double *x = s->d_ws, *aux = s->d_ws + (size_t)n * nrhs;
+    CU(cudaMemsetAsync(s->d_serr, 0, sizeof(int), s->st));
     CU(cudaMemcpy2DAsync(x, n * sizeof(double), b, ldb * sizeof(double), n * sizeof(double), nrhs,
                          cudaMemcpyHostToDevice, s->st));
     int launches = 0;
@@ -1964,6 +2007,7 @@ int b200_solve_device(b200_solver_t *s, int64_t nrhs, double *d_b, int64_t ldb, 
     if (!s || !s->factored || nrhs < 0 || ldb < s->n) return ERR_BADPARAM;
     if (nrhs == 0) return ERR_SUCCESS;
     cudaStream_t st = stream ? (cudaStream_t)stream : s->st;
+    CU(cudaMemsetAsync(s->d_serr, 0, sizeof(int), st));
     return solve_device(s, (int)nrhs, d_b, ldb, st);
 }
 
@@ -1978,12 +2022,15 @@ int b200_solve_device_noalloc(b200_solver_t *s, int64_t nrhs, double *d_b, int64
                 2LL * n * (long long)nrhs, B200_NOALLOC_SCRATCH_DOUBLES);
         return ERR_BADPARAM;
     }
-    double *xp = nullptr;
-    RET(noalloc_scratch(&xp));
+    // the scratch's address on the instance's device, looked up when it was created
+    double *xp = s->noalloc_scratch;
+    if (!xp) return ERR_INTERNAL;
     double *aux = xp + (size_t)n * nrhs;
     cudaStream_t st = stream ? (cudaStream_t)stream : s->st;
+    CU(cudaMemsetAsync(s->d_serr, 0, sizeof(int), st));
     // every entry of the scratch used here is written before it is read: the first half
-    // by the permutation, the second by the forward diagonal products
+    // by the permutation, the second by the forward diagonal products (for an FP32
+    // factor, the two float blocks of the sweeps by the conversion and the products)
     int launches = 2;
     launch_permute(n, (int)nrhs, s->d_peri, d_b, ldb, xp, n, 1, st);
     RET(sweeps(s, xp, aux, n, (int)nrhs, st, &launches));
@@ -1993,11 +2040,13 @@ int b200_solve_device_noalloc(b200_solver_t *s, int64_t nrhs, double *d_b, int64
     return ERR_SUCCESS;
 }
 
-// Bit 4 of the device error word: a dataflow sweep gave up waiting for its inputs
-// (its result is not to be used).  Read after the stream has been synchronized.
+// Bit 4 of the sweep status word: a dataflow sweep of the last solve / refinement
+// call gave up waiting for its inputs (its result is not to be used).  Every call
+// that runs sweeps clears the word first.  Read after the stream has been
+// synchronized.
 static int sweep_status(b200_solver_t *s) {
     int err = 0;
-    if (cudaMemcpy(&err, s->d_err, sizeof(int), cudaMemcpyDeviceToHost) != cudaSuccess) return ERR_INTERNAL;
+    if (cudaMemcpy(&err, s->d_serr, sizeof(int), cudaMemcpyDeviceToHost) != cudaSuccess) return ERR_INTERNAL;
     if (err & 16) {
         fprintf(stderr, "pastix_b200: a solve sweep timed out waiting for its inputs\n");
         return ERR_INTERNAL;
@@ -2005,16 +2054,22 @@ static int sweep_status(b200_solver_t *s) {
     return ERR_SUCCESS;
 }
 
+int b200_solve_status(b200_solver_t *s) {
+    if (!s) return ERR_BADPARAM;
+    return sweep_status(s);
+}
+
 int b200_solve(b200_solver_t *s, int64_t nrhs, double *b, int64_t ldb) {
     if (s && s->cblkschur < s->cblknbr) return ERR_BADPARAM;  // the Schur part is the caller's: b200_trsm
     if (!s || !s->factored || nrhs < 0 || ldb < s->n || (!b && nrhs)) return ERR_BADPARAM;
     if (nrhs == 0) return ERR_SUCCESS;
     const int n = s->n;
-    double *db = nullptr;
-    RET(dalloc(&db, (size_t)n * nrhs));
+    RET(ensure_stage(s, (size_t)n * nrhs));
+    double *db = s->d_stage;
     int rc = ERR_SUCCESS;
-    if (cudaMemcpy2DAsync(db, n * sizeof(double), b, ldb * sizeof(double), n * sizeof(double), nrhs,
-                          cudaMemcpyHostToDevice, s->st) != cudaSuccess) rc = ERR_INTERNAL;
+    if (cudaMemsetAsync(s->d_serr, 0, sizeof(int), s->st) != cudaSuccess) rc = ERR_INTERNAL;
+    if (!rc && cudaMemcpy2DAsync(db, n * sizeof(double), b, ldb * sizeof(double), n * sizeof(double), nrhs,
+                                 cudaMemcpyHostToDevice, s->st) != cudaSuccess) rc = ERR_INTERNAL;
     if (!rc) {
         cudaEventRecord(s->ev0, s->st);
         rc = solve_device(s, (int)nrhs, db, n, s->st);
@@ -2027,7 +2082,6 @@ int b200_solve(b200_solver_t *s, int64_t nrhs, double *b, int64_t ldb) {
     float ms = 0;
     if (!rc) cudaEventElapsedTime(&ms, s->ev0, s->ev1);
     s->t_solve = ms;
-    cudaFree(db);
     return rc;
 }
 
@@ -2039,6 +2093,7 @@ int b200_refine_device(b200_solver_t *s, int64_t nrhs, const double *d_b, int64_
     if (nrhs == 0) return ERR_SUCCESS;
     cudaStream_t st = stream ? (cudaStream_t)stream : s->st;
     auto t0 = std::chrono::steady_clock::now();
+    CU(cudaMemsetAsync(s->d_serr, 0, sizeof(int), st));
     int rc = refine_device(s, (int)nrhs, d_b, ldb, d_x, ldx, method, eps, itermax, gmres_im, niter, berr, st);
     if (!rc && cudaStreamSynchronize(st) != cudaSuccess) rc = ERR_INTERNAL;
     if (!rc) rc = sweep_status(s);
@@ -2051,19 +2106,17 @@ int b200_refine(b200_solver_t *s, int64_t nrhs, const double *b, int64_t ldb, do
     if (!s || !s->factored || nrhs < 0 || ldb < s->n || ldx < s->n) return ERR_BADPARAM;
     if (nrhs == 0) return ERR_SUCCESS;
     const int n = s->n;
-    double *db = nullptr, *dx = nullptr;
-    RET(dalloc(&db, (size_t)n * nrhs));
-    int rc = dalloc(&dx, (size_t)n * nrhs);
+    RET(ensure_stage(s, (size_t)2 * n * nrhs));
+    double *db = s->d_stage, *dx = s->d_stage + (size_t)n * nrhs;
+    int rc = ERR_SUCCESS;
+    if (cudaMemcpy2DAsync(dx, n * sizeof(double), x, ldx * sizeof(double), n * sizeof(double), nrhs,
+                          cudaMemcpyHostToDevice, s->st) != cudaSuccess) rc = ERR_INTERNAL;
     if (!rc && cudaMemcpy2DAsync(db, n * sizeof(double), b, ldb * sizeof(double), n * sizeof(double), nrhs,
-                                 cudaMemcpyHostToDevice, s->st) != cudaSuccess) rc = ERR_INTERNAL;
-    if (!rc && cudaMemcpy2DAsync(dx, n * sizeof(double), x, ldx * sizeof(double), n * sizeof(double), nrhs,
                                  cudaMemcpyHostToDevice, s->st) != cudaSuccess) rc = ERR_INTERNAL;
     if (!rc) rc = b200_refine_device(s, nrhs, db, n, dx, n, method, eps, itermax, gmres_im, niter, berr, s->st);
     if (!rc && cudaMemcpy2DAsync(x, ldx * sizeof(double), dx, n * sizeof(double), n * sizeof(double), nrhs,
                                  cudaMemcpyDeviceToHost, s->st) != cudaSuccess) rc = ERR_INTERNAL;
     if (cudaStreamSynchronize(s->st) != cudaSuccess) rc = ERR_INTERNAL;
-    cudaFree(db);
-    if (dx) cudaFree(dx);
     return rc;
 }
 
@@ -2073,8 +2126,8 @@ int b200_spmv(b200_solver_t *s, int64_t nrhs, double alpha, const double *x, int
     if (nrhs == 0) return ERR_SUCCESS;
     const int n = s->n;
     const size_t blk = (size_t)n * nrhs;
-    double *d = nullptr;
-    RET(dalloc(&d, 4 * blk));
+    RET(ensure_stage(s, 4 * blk));
+    double *d = s->d_stage;
     double *dx = d, *dy = d + blk, *px = d + 2 * blk, *py = d + 3 * blk;
     int rc = ERR_SUCCESS;
     if (cudaMemcpy2DAsync(dx, n * sizeof(double), x, ldx * sizeof(double), n * sizeof(double), nrhs,
@@ -2092,7 +2145,6 @@ int b200_spmv(b200_solver_t *s, int64_t nrhs, double alpha, const double *x, int
                               cudaMemcpyDeviceToHost, s->st) != cudaSuccess) rc = ERR_INTERNAL;
     }
     if (cudaStreamSynchronize(s->st) != cudaSuccess) rc = ERR_INTERNAL;
-    cudaFree(d);
     return rc;
 }
 
@@ -2158,6 +2210,8 @@ int b200_stats(b200_solver_t *s, double *out) {
     out[8] = s->launches_solve;
     out[9] = (double)s->coefnbr;
     out[10] = (double)s->kernel_launches;
+    out[11] = (double)s->ws_cap * sizeof(double);
+    out[12] = (double)s->stage_cap * sizeof(double);
     return ERR_SUCCESS;
 }
 

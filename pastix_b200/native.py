@@ -27,7 +27,8 @@ SYMBOLS = ["b200_solver_create", "b200_solver_destroy", "b200_solver_create_schu
            "b200_bcsc_values", "b200_get_schur", "b200_applyorder", "b200_trsm", "b200_get_diag", "b200_batch_set",
            "b200_batch_thresholds", "b200_batch_pivots", "b200_batch_berr", "b200_spm_map", "b200_spm_values",
            "b200_spm_values_device", "b200_numfact", "b200_numfact_trace", "b200_solve", "b200_solve_trace",
-           "b200_trace_launches", "b200_trace_kinds", "b200_solve_device", "b200_solve_device_noalloc",
+           "b200_trace_launches", "b200_trace_kinds", "b200_solve_device", "b200_solve_status",
+           "b200_solve_device_noalloc",
            "b200_refine", "b200_refine_device", "b200_spmv", "b200_spmv_device", "b200_factor_download",
            "b200_stats", "b200_strerror"]
 
@@ -75,6 +76,7 @@ def lib():
         L.b200_trace_kinds.argtypes = [_P, _P, _P, C.c_int]
         L.b200_solve_device.argtypes = [_P, _I64, _P, _I64, _P]
         L.b200_solve_device_noalloc.argtypes = [_P, _I64, _P, _I64, _P]
+        L.b200_solve_status.argtypes = [_P]
         L.b200_refine.argtypes = [_P, _I64, _P, _I64, _P, _I64, C.c_int, C.c_double, _I64, _I64,
                                   C.POINTER(_I64), _P]
         L.b200_refine_device.argtypes = [_P, _I64, _P, _I64, _P, _I64, C.c_int, C.c_double, _I64, _I64,
@@ -319,9 +321,15 @@ class Solver:
         check(lib().b200_factor_download(self.h, _p(L), _p(U)), "b200_factor_download")
         return L, U
 
+    def solve_status(self):
+        """Raise if a sweep of the last solve / refinement gave up waiting (call it
+        after synchronizing the stream of a device solve)."""
+        check(lib().b200_solve_status(self.h), "b200_solve_status")
+
     def stats(self) -> dict:
-        out = np.zeros(11)
+        out = np.zeros(13)
         check(lib().b200_stats(self.h, _p(out)), "b200_stats")
         return dict(numfact_ms=out[0], solve_ms=out[1], refine_ms=out[2], nbpivots=int(out[3]), threshold=out[4],
                     device_bytes=int(out[5]), levels=int(out[6]), launches_numfact=int(out[7]),
-                    launches_solve=int(out[8]), coefnbr=int(out[9]), kernel_launches=int(out[10]))
+                    launches_solve=int(out[8]), coefnbr=int(out[9]), kernel_launches=int(out[10]),
+                    workspace_bytes=int(out[11]), staging_bytes=int(out[12]))

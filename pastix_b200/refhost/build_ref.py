@@ -30,7 +30,14 @@ import subprocess
 import sys
 
 REPO = os.path.dirname(os.path.dirname(os.path.dirname(os.path.abspath(__file__))))
-DEFAULT_REF = "/root/reference"
+
+
+def default_reference() -> str:
+    """Where the PaStiX source tree is read from: $PASTIX_REFERENCE_SRC, else a
+    ``reference`` folder beside this repository's folder."""
+    return os.environ.get("PASTIX_REFERENCE_SRC") or os.path.join(os.path.dirname(REPO), "reference")
+
+
 BUILD = os.path.join(REPO, "_build", "refsrc")
 
 _SITE = os.path.join(sys.prefix, "lib", "python3.12", "site-packages")
@@ -142,8 +149,9 @@ def blas_dir() -> str:
     raise RuntimeError("OpenBLAS (opencv_python_headless.libs) not found")
 
 
-def build(outdir: str, extra_sources=(), ref: str = DEFAULT_REF, jobs: int = 8, libname="libpastix_ref.so",
+def build(outdir: str, extra_sources=(), ref: str | None = None, jobs: int = 8, libname="libpastix_ref.so",
           force: bool = False) -> str:
+    ref = ref or default_reference()
     if not os.path.isdir(ref):
         raise RuntimeError(f"reference tree {ref} not present")
     stamp = os.path.join(BUILD, ".generated")
@@ -239,7 +247,8 @@ def include_dirs() -> list[str]:
 if __name__ == "__main__":
     ap = argparse.ArgumentParser()
     ap.add_argument("--out", default=os.path.join(os.path.dirname(os.path.abspath(__file__)), "_lib"))
-    ap.add_argument("--ref", default=DEFAULT_REF)
+    ap.add_argument("--ref", default=None, help="PaStiX source tree (default: $PASTIX_REFERENCE_SRC, else "
+                                                    "../reference beside the repository)")
     ap.add_argument("--force", action="store_true")
     ap.add_argument("extra", nargs="*")
     a = ap.parse_args()

@@ -509,8 +509,26 @@ def test_bounded_waits_report_errors(monkeypatch):
     with pytest.raises(native.B200Error):
         s.solve(b)
     assert time.perf_counter() - t0 < 30.0
-    s.close()
+    # a device solve reports the same failure through b200_solve_status once its
+    # stream is synchronized ...
+    import torch
+    d = torch.from_numpy(np.ascontiguousarray(b.T)).cuda()
+    torch.cuda.synchronize()
+    s.solve_device(d.data_ptr(), 2, A.n)
+    torch.cuda.synchronize()
+    with pytest.raises(native.B200Error):
+        s.solve_status()
+    # ... and the status belongs to one call: the same instance then solves cleanly
     monkeypatch.delenv("B200_TEST_WITHHOLD")
+    d = torch.from_numpy(np.ascontiguousarray(b.T)).cuda()
+    torch.cuda.synchronize()
+    s.solve_device(d.data_ptr(), 2, A.n)
+    torch.cuda.synchronize()
+    s.solve_status()
+    assert backward_error(A, d.cpu().numpy().T, b).max() <= BERR_FP64
+    x = s.solve(b)
+    assert backward_error(A, x, b).max() <= BERR_FP64
+    s.close()
     s = native.Solver(st, "potrf", "fp64")
     s.bcsc_load(bc)
     s.numfact(0.0)
