@@ -117,12 +117,14 @@ class BatchAnalysis:
     bcsc from the systems' own values (on the host here, or on the device through
     ``b200_spm_map`` / ``b200_spm_values``)."""
 
-    def __init__(self, mats, facto: str = "sytrf"):
+    def __init__(self, mats, facto: str = "sytrf", patterns: dict | None = None):
+        """patterns: the per-pattern analyses of another batch of the same
+        factorization, reused for the systems that share them (a sub-batch)."""
         if not len(mats):
             raise ValueError("empty batch")
         self.mats = list(mats)
         self.facto_name = facto
-        self.patterns: dict[str, _Pattern] = {}
+        self.patterns: dict[str, _Pattern] = dict(patterns) if patterns else {}
         self.keys = []
         for A in self.mats:
             key = _pattern_key(A)
@@ -200,3 +202,116 @@ class BatchAnalysis:
         """Each system's slice of the factor in PaStiX's coeftab layout."""
         c = np.concatenate([[0], np.cumsum([self.system_structure(i).coefnbr for i in range(self.nsys)])])
         return [(int(c[i]), int(c[i + 1])) for i in range(self.nsys)]
+
+
+@dataclass
+class BatchResult:
+    x: np.ndarray                 # solutions, batch order (original numbering), n x nrhs
+    berr: np.ndarray              # per (system, column) backward error of the refinement
+    pivots: np.ndarray            # pivots replaced per system by the factorization that solved it
+    fp64_systems: np.ndarray      # systems factored in FP64 (the fallback)
+    iterations: int               # refinement iterations of the forest
+    iterations_fp64: int          # refinement iterations of the FP64 forest (0: none)
+
+
+class BatchSolver:
+    """Factorization, solve and refinement of a batch of independent systems on
+    the GPU, each system to its own backward-error target.
+
+    The whole forest is factored in the requested precision (an FP32 factor for the
+    mixed path) and refined in FP64 with that factor as the preconditioner, one
+    refinement per (column, system).  Static pivoting at sqrt(eps) ||A_i||_F without
+    pivoting can replace a large share of a system's pivots in FP32 (an indefinite
+    system whose shift sits in the middle of its spectrum has near-zero pivots
+    everywhere); every replacement perturbs the factor, and once thousands are
+    replaced no restarted GMRES of a few hundred iterations corrects it -- PaStiX's
+    own FP32 factorization and refinement miss their 1e-6 target on such systems.
+    Those systems are factored again in FP64 on the GPU (a second forest of just
+    them, PaStiX's analyses reused), where the threshold sqrt(eps_64) ||A_i||_F
+    replaces far fewer pivots: a system goes to FP64 when its FP32 factor replaced
+    more than ``fp64_pivot_frac`` of its pivots, or when its refinement with the FP32
+    factor misses the target.  The reference factors each system separately
+    (pastix_task_numfact / _solve / _refine per instance,
+    sopalin/pastix_task_sopalin.c:563, refinement/pastix_task_refine.c:226)."""
+
+    def __init__(self, ba: BatchAnalysis, precision: str = "fp32", fp64_pivot_frac: float = 0.1,
+                 stream=None):
+        from . import native
+        self.ba = ba
+        self.precision = precision
+        self.frac = float(fp64_pivot_frac)
+        self.stream = stream
+        self.s = native.Solver(ba.structure(), ba.facto_name, precision, stream=stream)
+        self.s.batch_set(ba.sys_cblk)
+        self.s.bcsc_load(ba.bcsc())
+        self.sub = None       # (BatchAnalysis, Solver) of the FP64 forest
+        self.sub_idx = np.zeros(0, dtype=np.int64)
+        self.pivots = None
+        self.eps_magn = 0.0
+
+    def close(self):
+        self.s.close()
+        if self.sub is not None:
+            self.sub[1].close()
+            self.sub = None
+
+    def _fp64_forest(self, idx):
+        from . import native
+        if self.sub is not None and np.array_equal(self.sub_idx, idx):
+            return self.sub
+        if self.sub is not None:
+            self.sub[1].close()
+        sba = BatchAnalysis([self.ba.mats[i] for i in idx], self.ba.facto_name, patterns=self.ba.patterns)
+        s64 = native.Solver(sba.structure(), sba.facto_name, "fp64", stream=self.stream)
+        s64.batch_set(sba.sys_cblk)
+        s64.bcsc_load(sba.bcsc())
+        s64.numfact(self.eps_magn)
+        self.sub, self.sub_idx = (sba, s64), np.asarray(idx, dtype=np.int64)
+        return self.sub
+
+    def numfact(self, epsilon_magn_ctrl: float = 0.0) -> np.ndarray:
+        """Factor the forest; returns the pivots replaced per system."""
+        self.eps_magn = epsilon_magn_ctrl
+        self.s.numfact(epsilon_magn_ctrl)
+        self.pivots = self.s.batch_pivots()
+        if self.sub is not None:
+            self.sub[1].close()
+            self.sub, self.sub_idx = None, np.zeros(0, dtype=np.int64)
+        return self.pivots
+
+    def solve(self, b, method: str = "gmres", eps: float = 1e-12, itermax: int = 250,
+              gmres_im: int = 25) -> BatchResult:
+        """Solve and refine every system of the batch to ``eps``."""
+        ba = self.ba
+        b = np.asfortranarray(np.asarray(b, dtype=np.float64).reshape(ba.st.n, -1))
+        nrhs = b.shape[1]
+        sizes = np.diff(ba.sys_col)
+        fp64 = np.zeros(ba.nsys, dtype=bool)
+        if self.precision != "fp64":
+            fp64 = self.pivots > self.frac * sizes
+        rows = np.concatenate([np.arange(ba.sys_col[i], ba.sys_col[i + 1]) for i in np.nonzero(fp64)[0]] +
+                              [np.zeros(0, dtype=np.int64)])
+        # systems bound for FP64 get a zero right-hand side in the forest: their
+        # refinement is done at its first residual
+        bf = b.copy(order="F")
+        bf[rows] = 0.0
+        x = self.s.solve(bf)
+        x, it, _ = self.s.refine(bf, x, method, eps, itermax, gmres_im)
+        berr = self.s.batch_berr(nrhs)
+        late = (berr.max(axis=1) > eps) & ~fp64
+        fp64 |= late
+        piv = self.pivots.copy()
+        it64 = 0
+        if fp64.any():
+            idx = np.nonzero(fp64)[0]
+            sba, s64 = self._fp64_forest(idx)
+            bs = np.concatenate([b[ba.sys_col[i]:ba.sys_col[i + 1]] for i in idx], axis=0)
+            xs = s64.solve(bs)
+            xs, it64, _ = s64.refine(bs, xs, method, eps, itermax, gmres_im)
+            bsub = s64.batch_berr(nrhs)
+            psub = s64.batch_pivots()
+            for j, i in enumerate(idx):
+                x[ba.sys_col[i]:ba.sys_col[i + 1]] = xs[sba.sys_col[j]:sba.sys_col[j + 1]]
+                berr[i] = bsub[j]
+                piv[i] = psub[j]
+        return BatchResult(x, berr, piv, np.nonzero(fp64)[0], int(it), int(it64))

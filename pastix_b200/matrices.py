@@ -180,3 +180,15 @@ def rhs_from_xtrue(A: CSC, nrhs: int, seed: int):
     x = rng.uniform(-1.0, 1.0, size=(A.n, nrhs))
     b = A.matvec(x)
     return np.asfortranarray(x), np.asfortranarray(b)
+
+
+def indefinite_batch(nsys: int = 4096, seed: int = 2024, side_min: int = 16, side_max: int = 128):
+    """The batched indefinite workload: nsys 2D 5-point Laplacians with grid sides
+    log-uniform in [side_min, side_max] (n = 256 .. 16,384 at the defaults), each
+    shifted by -sigma I with sigma uniform in (0, 0.5 lambda_max).  Returns the sides
+    and shifts (the matrices are ``shifted_laplacian_2d(side, sigma)``)."""
+    rng = np.random.default_rng(seed)
+    sides = np.floor(np.exp(rng.uniform(np.log(side_min), np.log(side_max + 1), nsys))).astype(int)
+    sides = sides.clip(side_min, side_max)
+    sig = rng.uniform(0.0, 0.5, nsys) * np.array([lambda_max_5pt(int(s)) for s in sides])
+    return sides, sig

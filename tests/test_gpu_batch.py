@@ -184,55 +184,89 @@ def test_full_size_batched_indefinite_systems():
     """4096 independent 2D 5-point Laplacians, sides log-uniform in [16, 128],
     each shifted by -sigma I with sigma uniform in (0, 0.5 lambda_max): FP32 LDL^T
     of the whole batch (one forest) and FP64 GMRES(25) refinement per system with
-    PaStiX's defaults (250 iterations).
+    PaStiX's defaults (250 iterations).  Every system must reach a backward error
+    <= 1e-12.
 
     With sigma near 0.5 lambda_max (about 4, the diagonal) the first pivots are
     near zero and the FP32 threshold sqrt(eps_32) ||A_i||_F replaces thousands of
-    them; a rank-thousands perturbation of the factor is more than 250 GMRES(25)
-    iterations correct, in the reference's algorithm as here.  The bar: every system
-    converges to <= 1e-12 unless its factor replaced >= 1000 pivots, at least 99 %
-    of the systems converge, and the per-system pivot counts agree with the
-    oracle's FP32 factorization of that system (to the few pivots that FP32
-    rounding moves across the threshold)."""
-    rng = np.random.default_rng(2024)
-    nsys = 4096
-    sides = np.floor(np.exp(rng.uniform(np.log(16), np.log(129), nsys))).astype(int).clip(16, 128)
-    sig = rng.uniform(0.0, 0.5, nsys) * np.array([M.lambda_max_5pt(int(s)) for s in sides])
+    them; PaStiX's own FP32 factorization and refinement miss even their 1e-6
+    target on the worst of these systems, while its FP64 factorization replaces no
+    pivot (tests/golden/batch_hard_pastix.json).  Systems whose FP32 factor replaced
+    more than 10 % of their pivots, or whose refinement misses the target, are
+    factored again in FP64 on the GPU (``BatchSolver``).  The per-system pivot counts
+    of the FP32 forest agree with the oracle's FP32 factorization of that system (to
+    the few pivots that FP32 rounding moves across the threshold)."""
+    from pastix_b200.batch import BatchSolver
+    rng = np.random.default_rng(7)
+    sides, sig = M.indefinite_batch(4096, seed=2024)
+    nsys = sides.size
     mats = [M.shifted_laplacian_2d(int(s), float(g)) for s, g in zip(sides, sig)]
     t0 = time.perf_counter()
     ba = BatchAnalysis(mats, "sytrf")
     t_an = time.perf_counter() - t0
-    s = _solver(ba, "fp32")
-    s.numfact(0.0)
-    s.numfact(0.0)
+    bs_ = BatchSolver(ba, "fp32")
+    bs_.numfact(0.0)
+    pivs = bs_.numfact(0.0)
+    s = bs_.s
     fact_ms = s.stats()["numfact_ms"]
     thr = s.batch_thresholds()
-    pivs = s.batch_pivots()
     bs = [M.rhs_from_xtrue(A, 1, seed=i)[1] for i, A in enumerate(mats)]
     b = ba.join(bs)
-    x0 = s.solve(b)
-    s.solve(b)  # the first call also sizes the workspace: report a second one
-    solve_ms = s.stats()["solve_ms"]
     t1 = time.perf_counter()
-    x, it, berr = s.refine(b, x0, "gmres", BERR_TARGET, 250, 25)
-    t_ref = time.perf_counter() - t1
-    per = s.batch_berr(1)[:, 0]
-    host = _split_errors(ba, x, bs)
-    bad = np.nonzero(per > BERR_TARGET)[0]
+    res = bs_.solve(b, "gmres", BERR_TARGET, 250, 25)
+    t_solve = time.perf_counter() - t1
+    per = res.berr[:, 0]
+    host = _split_errors(ba, res.x, bs)
     s.numfact_trace(0.0)
     kinds = {k: round(v["ms"], 2) for k, v in s.trace_kinds().items() if v["ms"] > 0}
+    fb = res.fp64_systems
     print(f"\nnumfact by kind (ms, traced launch by launch): {kinds}, levels {s.stats()['levels']}, "
           f"launches {s.stats()['launches_numfact']}")
     print(f"batch n={ba.st.n} cblks={ba.st.cblknbr} patterns={len(ba.patterns)} analysis {t_an:.1f}s "
-          f"numfact {fact_ms:.2f} ms, solve {solve_ms:.2f} ms, refine {t_ref * 1e3:.1f} ms ({it} it), "
-          f"thflops {ba.st.thflops:.3e}, pivots {pivs.sum()} (max {pivs.max()}), berr max {per.max():.2e}, "
-          f"not converged {bad.size} with pivots {np.sort(pivs[bad])}, "
-          f"largest pivot count converged {pivs[per <= BERR_TARGET].max()}")
+          f"numfact {fact_ms:.2f} ms, solve + refinement {t_solve * 1e3:.1f} ms ({res.iterations} it, FP64 "
+          f"forest {res.iterations_fp64} it), thflops {ba.st.thflops:.3e}, FP32 pivots {pivs.sum()} "
+          f"(max {pivs.max()}), berr max {per.max():.2e}, {fb.size} systems in FP64 with FP32 pivots "
+          f"{np.sort(pivs[fb])} and FP64 pivots {res.pivots[fb]}")
     assert np.allclose(host, per, rtol=1e-6, atol=1e-15)
-    assert bad.size <= nsys // 100
-    assert np.all(pivs[bad] >= 1000)
-    sample = np.concatenate([bad, rng.choice(nsys, 8, replace=False)])
+    assert per.max() <= BERR_TARGET
+    assert host.max() <= 2 * BERR_TARGET
+    sample = np.concatenate([fb[:4], rng.choice(nsys, 8, replace=False)])
     for i in sample:
         o = _oracle_fp32_pivots(mats[i], thr[i])
         assert abs(int(pivs[i]) - o) <= 2 + o // 100, (i, pivs[i], o)
-    s.close()
+    bs_.close()
+
+
+def test_batch_fp64_fallback_small():
+    """The FP64 fallback on a small batch: two systems whose shift sits at the
+    middle of their spectrum (FP32 replaces a large share of their pivots) among
+    easy ones.  The hard ones are factored again in FP64, every system reaches the
+    target, and the FP64 forest's factor of a hard system equals the oracle's FP64
+    factor of that system alone."""
+    from pastix_b200.batch import BatchSolver
+    sides = [40, 64, 48, 16, 40]
+    fr = [0.2, 0.49948, 0.1, 0.3, 0.4998]
+    mats = [M.shifted_laplacian_2d(s, f * M.lambda_max_5pt(s)) for s, f in zip(sides, fr)]
+    ba = BatchAnalysis(mats, "sytrf")
+    bs_ = BatchSolver(ba, "fp32")
+    pivs = bs_.numfact(0.0)
+    bs = [M.rhs_from_xtrue(A, 2, seed=50 + i)[1] for i, A in enumerate(mats)]
+    res = bs_.solve(ba.join(bs), "gmres", BERR_TARGET, 250, 25)
+    hard = np.nonzero(pivs > 0.1 * np.array([A.n for A in mats]))[0]
+    assert set(hard.tolist()) <= set(res.fp64_systems.tolist())
+    assert res.berr.max() <= BERR_TARGET
+    assert _split_errors(ba, res.x, bs).max() <= 2 * BERR_TARGET
+    sba, s64 = bs_.sub
+    L64, _ = s64.factor()
+    for j, i in enumerate(res.fp64_systems):
+        an = Analysis(mats[i], "sytrf")
+        orc = oracle.Oracle(an.structure())
+        Lo, Uo = orc.fillin(an.bcsc())
+        orc.numfact(an.facto, Lo, Uo, s64.batch_thresholds()[j])
+        c0, c1 = sba.coef_ranges()[j]
+        d = factor_diff(orc, an.facto, L64[c0:c1], None, Lo, Uo)
+        if d > FACTOR_TOL:
+            Lx, Ux = exact_factor(an, orc, an.bcsc(), s64.batch_thresholds()[j])
+            assert factor_diff(orc, an.facto, L64[c0:c1], None, Lx, Ux) <= \
+                4.0 * reference_fp64_error(an, orc, Lo, Uo, Lx, Ux)
+    bs_.close()
