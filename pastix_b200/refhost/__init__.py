@@ -250,3 +250,55 @@ class Analysis:
     def set_dparm(self, name, value):
         _, dp = param_ids()
         lib().rh_dparm(self.h)[dp[name]] = float(value)
+
+
+# ---------------------------------------------------------------- PaStiX with the B200 scheduler
+
+SCHED_LIBPATH = os.path.join(HERE, "_lib", "libpastix_b200sched.so")
+SCHEDULERS = {"sequential": 0, "static": 1, "dynamic": 4, "b200": 5, "b200_mixed": 6}
+REFINEMENTS = {"gmres": 0, "cg": 1, "sr": 2, "bicgstab": 3}
+_slib = None
+
+
+def sched_lib():
+    """PaStiX built with the B200 scheduler ids (build_sched.py): its own task entry
+    points dispatch to libpastix_b200.so for PastixSchedB200 / PastixSchedB200Mixed."""
+    global _slib
+    if _slib is None:
+        if not os.path.exists(SCHED_LIBPATH):
+            raise RuntimeError(f"{SCHED_LIBPATH} missing: run pastix_b200/refhost/build_sched.py")
+        lib()  # OpenBLAS and its runtime, loaded globally
+        L = C.CDLL(SCHED_LIBPATH, mode=C.RTLD_LOCAL)
+        L.pb_simple.restype = C.c_int
+        L.pb_simple.argtypes = [C.c_int64, _I64P, _I64P, _P, C.c_int, C.c_int, C.c_int64, C.c_int64, C.c_int64,
+                                C.c_int, C.c_int, C.c_int, C.c_double, C.c_int64, _P, _P, _P, _P, _P]
+        _slib = L
+    return _slib
+
+
+def pastix_simple(A, facto: str, scheduler: str, b, nthreads: int = 1, refinement: str = "gmres",
+                  epsilon_magn_ctrl: float = 0.0, factor: bool = False) -> dict:
+    """PaStiX's example/simple.c sequence (pastixInit, analysis with the grid
+    ordering, pastix_task_numfact, pastix_task_solve, pastix_task_refine,
+    pastixFinalize) on A under the given scheduler.  Returns the solution, PaStiX's
+    outputs (times, threshold, pivots, iterations, relative error) and, with
+    ``factor``, the factor in PaStiX's coeftab layout."""
+    L = sched_lib()
+    b = np.asfortranarray(np.asarray(b, dtype=np.float64).reshape(A.n, -1))
+    x = np.zeros_like(b, order="F")
+    Lf = Uf = None
+    if factor:
+        coefnbr = int(Analysis(A, facto).sizes()[4])
+        Lf = np.zeros(coefnbr)
+        Uf = np.zeros(coefnbr) if facto == "getrf" else None
+    out = np.zeros(10)
+    nx, ny, nz = A.grid
+    rc = L.pb_simple(A.n, np.ascontiguousarray(A.colptr, dtype=np.int64), np.ascontiguousarray(A.rowind, dtype=np.int64),
+                     np.ascontiguousarray(A.values, dtype=np.float64).ctypes.data_as(_P), 1 if A.symmetric else 0,
+                     FACTO[facto], nx, ny, nz, SCHEDULERS[scheduler], nthreads, REFINEMENTS[refinement],
+                     epsilon_magn_ctrl, b.shape[1], b.ctypes.data_as(_P), x.ctypes.data_as(_P),
+                     Lf.ctypes.data_as(_P) if Lf is not None else None,
+                     Uf.ctypes.data_as(_P) if Uf is not None else None, out.ctypes.data_as(_P))
+    return dict(rc=int(rc), x=x, L=Lf, U=Uf, fact_time=out[0], solve_time=out[1], refine_time=out[2],
+                threshold=out[3], nbpivots=int(out[4]), nbiter=int(out[5]), relative_error=out[6],
+                fact_gflops=out[7], anorm=out[8])
