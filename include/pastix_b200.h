@@ -12,8 +12,15 @@
  * 0 = PASTIX_SUCCESS, 2 = PASTIX_ERR_ALLOC, 3 = PASTIX_ERR_NOTIMPLEMENTED,
  * 4 = PASTIX_ERR_OUTOFMEMORY, 6 = PASTIX_ERR_INTERNAL, 7 = PASTIX_ERR_BADPARAMETER.
  *
- * Threading: one solver instance is not re-entrant (as a pastix_data_t);
- * separate instances may be used from separate host threads.
+ * Threading: the factorization, bcsc and structure calls of one solver instance are
+ * not re-entrant (as a pastix_data_t) and must not overlap with its solves.  The
+ * solve and refinement calls on DIFFERENT CUDA streams may run concurrently from
+ * different host threads on the same factor: every stream gets its own workspaces,
+ * tickets and status word on its first call (a device allocation then), so their
+ * work overlaps on the GPU.  Calls on the same stream are serialized by the caller.
+ * The host-pointer calls (b200_solve, b200_refine, b200_spmv, b200_trsm,
+ * b200_applyorder) all use the solver's own stream.  Separate instances may be used
+ * from separate host threads.
  */
 #ifndef PASTIX_B200_H
 #define PASTIX_B200_H
@@ -212,15 +219,16 @@ int b200_trace_kinds( b200_solver_t *solver, double *ms, double *flops, int nkin
  * not NULL).  Check b200_solve_status once the stream has been synchronized. */
 int b200_solve_device( b200_solver_t *solver, int64_t nrhs, double *d_b, int64_t ldb, void *stream );
 
-/* Status of the last solve or refinement of this instance, for the asynchronous
- * device entry points (b200_solve_device, b200_solve_device_noalloc,
- * b200_refine_device with a caller's stream): call it after synchronizing that
- * stream.  PASTIX_ERR_INTERNAL if a sweep gave up waiting for its inputs (the
- * result is not to be used), else PASTIX_SUCCESS.  Each solve or refinement call
- * clears the status when it starts; the host-pointer calls check it themselves.
- * Counterpart of the return code of pastix_task_solve
- * (sopalin/pastix_task_solve.c:550). */
-int b200_solve_status( b200_solver_t *solver );
+/* Status of the last solve or refinement of this instance on stream (NULL: the
+ * solver's own stream), for the asynchronous device entry points
+ * (b200_solve_device, b200_solve_device_noalloc, b200_refine_device): call it after
+ * synchronizing that stream.  PASTIX_ERR_INTERNAL if a sweep gave up waiting for its
+ * inputs (the result is not to be used), else PASTIX_SUCCESS.  Each solve or
+ * refinement call clears the status of its stream when it starts; the host-pointer
+ * calls check it themselves.  b200_solve_device_noalloc reports on the solver's own
+ * stream's status, whatever stream it ran on.  Counterpart of the return code of
+ * pastix_task_solve (sopalin/pastix_task_solve.c:550). */
+int b200_solve_status( b200_solver_t *solver, void *stream );
 
 /* Size of the fixed scratch of b200_solve_device_noalloc: 4,194,304 doubles
  * (32 MiB); a call needs 2 * n * nrhs of them. */

@@ -10,6 +10,7 @@
 //  solve_scale_diag_kernel  b /= D (solve_cblk_zdiag, kernels/solve_ztrsmsp.c:584-633)
 //  permute_kernel           bvec_zlapmr with peritab (bcsc/bvec_zcompute.c:875)
 //  convert_kernel           double <-> float copies of a vector block
+#include <atomic>
 #include "b200_internal.h"
 #include "kernels.h"
 #include "tile_ops.cuh"
@@ -838,10 +839,12 @@ void launch_solve_flow(const DevSym &s, const FlowItem *items, int nitems, const
                        int64_t ldx, int nrhs, int backward, int *ticket, int *cnt_a, int *cnt_b, int *abort_word,
                        int *err, cudaStream_t st) {
     if (nitems <= 0) return;
-    static int ctas[2] = {0, 0};
+    // resident CTAs of the launch, computed once (calls on several streams may race
+    // to compute it; they store the same value)
+    static std::atomic<int> ctas[2] = {{0}, {0}};
     const int bi = backward ? 1 : 0;
     const int smem = FlowSmem<T, V>::BYTES;
-    if (!ctas[bi]) {
+    if (!ctas[bi].load()) {
         int dev = 0, sms = 0, occ = 0;
         cudaGetDevice(&dev);
         cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
@@ -852,9 +855,9 @@ void launch_solve_flow(const DevSym &s, const FlowItem *items, int nitems, const
             cudaFuncSetAttribute(solve_flow_kernel<T, V, 0>, cudaFuncAttributeMaxDynamicSharedMemorySize, smem);
             cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ, solve_flow_kernel<T, V, 0>, FLOW_THREADS, smem);
         }
-        ctas[bi] = std::max(occ, 1) * std::max(sms, 1);
+        ctas[bi].store(std::max(occ, 1) * std::max(sms, 1));
     }
-    const int grid = std::min(nitems, ctas[bi]);
+    const int grid = std::min(nitems, ctas[bi].load());
     if (backward)
         solve_flow_kernel<T, V, 1><<<grid, FLOW_THREADS, smem, st>>>(s, items, nitems, leaf, flist, need, nprev, P, W,
                                                                     woff, x, aux, ldx, nrhs, ticket, cnt_a, cnt_b,

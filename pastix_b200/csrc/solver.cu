@@ -7,6 +7,7 @@
 #include <cstdio>
 #include <cstdlib>
 #include <cstring>
+#include <atomic>
 #include <map>
 #include <mutex>
 #include <vector>
@@ -57,6 +58,27 @@ int upload(T **p, const std::vector<T> &h, cudaStream_t st) {
 }
 
 }  // namespace
+
+// Scratch of the solve and refinement calls issued on one CUDA stream: the
+// workspace blocks, the per-column scalars, the dataflow sweeps' tickets and
+// counters, the sweep status word and the SpMV staging.  Every stream that solves
+// gets its own, so calls on different streams (from different host threads) never
+// share scratch and their work can overlap on the GPU.
+struct Lane {
+    cudaStream_t st = nullptr;
+    double *d_ws = nullptr;
+    size_t ws_cap = 0;
+    double *d_scal = nullptr;  // per-column scalars
+    int scal_cap = 0;
+    // [ticket f, ticket b, abort, pad][cnt_a f][cnt_b f][cnt_a b][cnt_b b], zeroed per solve
+    int *d_sflags = nullptr;
+    // bit 4 set by a dataflow sweep that gave up waiting; zeroed at the start of every
+    // call that runs sweeps (b200_solve_status reads it)
+    int *d_serr = nullptr;
+    double *d_xt = nullptr;    // n x 16 row-major staging of the multi-column SpMV (allocated on first use)
+    double t_solve = 0, t_refine = 0;
+    int launches_solve = 0;
+};
 
 struct b200_solver_s {
     int facto = 0, prec = 0;
@@ -115,9 +137,6 @@ struct b200_solver_s {
     FlowItem *d_fitem_f = nullptr, *d_fitem_b = nullptr;
     int n_fitem_f = 0, n_fitem_b = 0;
     int *d_flist = nullptr, *d_need_f = nullptr, *d_need_b = nullptr, *d_nprev_f = nullptr, *d_nprev_b = nullptr;
-    // [ticket f, ticket b, abort, pad][cnt_a f][cnt_b f][cnt_a b][cnt_b b], zeroed per solve
-    int *d_sflags = nullptr;
-    double *d_xt = nullptr;  // n x 16 row-major staging of the multi-column SpMV (allocated on first use)
     // wide POTRF / LDL^T cblks: one panel launch per level over their 64 x 64 tiles
     std::vector<int> lvl_pi0, lvl_pi1;  // items of each level's launch
     std::vector<int> lvl_prows;         // row-block form: rows of the blocks below the diagonal (0: tile items)
@@ -192,29 +211,25 @@ struct b200_solver_s {
     std::vector<double> last_berr;  // per-problem backward errors of the last refinement
     std::vector<unsigned long long> last_piv_sys;  // pivots replaced per system by the last numfact
 
-    // status of the solve sweeps: bit 4 set by a dataflow sweep that gave up waiting;
-    // zeroed at the start of every call that runs sweeps (b200_solve_status reads it)
-    int *d_serr = nullptr;
-
     // device of the instance and the address of the no-allocation scratch on it
     // (looked up when the instance is created)
     int device = 0;
     double *noalloc_scratch = nullptr;
 
-    // solve / refine workspaces
-    double *d_ws = nullptr;
-    size_t ws_cap = 0;
+    // per-stream scratch of the solves: main is the instance's own stream's; others
+    // are created on a stream's first solve (lane_mu guards the map)
+    Lane main;
+    std::map<cudaStream_t, Lane *> lanes;
+    std::mutex lane_mu;
     // device copies of the host vectors of b200_solve / b200_refine / b200_spmv,
     // sized on first use and grown only when a call needs more
     double *d_stage = nullptr;
     size_t stage_cap = 0;
-    std::map<int, cudaGraphExec_t> solve_graphs;  // keyed by nrhs, on the ws buffer
-    double *d_scal = nullptr;                     // per-column scalars
-    int scal_cap = 0;
 
-    double t_fact = 0, t_solve = 0, t_refine = 0;
-    int launches_fact = 0, launches_solve = 0;
-    long long kernel_launches = 0;      // kernels this instance has run (graph replays included)
+    double t_fact = 0;
+    int launches_fact = 0;
+    std::atomic<long long> kernel_launches{0};  // kernels this instance has run (graph replays included)
+    std::mutex berr_mu;                           // last_berr, written by refinements on any stream
     std::vector<std::pair<int, double>> trace_detail;  // per-launch times of the last trace
     cudaEvent_t ev0 = nullptr, ev1 = nullptr;
 
@@ -233,7 +248,7 @@ struct b200_solver_s {
 };
 
 extern "C" {
-static int sweep_status(b200_solver_t *s);
+static int sweep_status(Lane *ln);
 }
 
 namespace {
@@ -624,7 +639,7 @@ int build_schedule(b200_solver_t *s) {
         RET(s->dupload(&s->d_need_b, need_b));
         RET(s->dupload(&s->d_nprev_f, nprev_f));
         RET(s->dupload(&s->d_nprev_b, nprev_b));
-        RET(s->dmalloc(&s->d_sflags, (size_t)4 * N + 4));
+        RET(dalloc(&s->main.d_sflags, (size_t)4 * N + 4));  // freed with the main lane
     }
     RET(s->dupload(&s->d_diag_list, diag_list));
     {
@@ -677,15 +692,55 @@ int build_schedule(b200_solver_t *s) {
     return ERR_SUCCESS;
 }
 
-int ensure_ws(b200_solver_t *s, size_t doubles) {
-    if (doubles <= s->ws_cap) return ERR_SUCCESS;
-    for (auto &kv : s->solve_graphs) cudaGraphExecDestroy(kv.second);
-    s->solve_graphs.clear();
-    if (s->d_ws) cudaFree(s->d_ws);
-    s->d_ws = nullptr;
-    s->ws_cap = 0;
-    RET(dalloc(&s->d_ws, doubles));
-    s->ws_cap = doubles;
+int ensure_ws(Lane *ln, size_t doubles) {
+    if (doubles <= ln->ws_cap) return ERR_SUCCESS;
+    if (ln->d_ws) {
+        CU(cudaStreamSynchronize(ln->st));
+        cudaFree(ln->d_ws);
+    }
+    ln->d_ws = nullptr;
+    ln->ws_cap = 0;
+    RET(dalloc(&ln->d_ws, doubles));
+    ln->ws_cap = doubles;
+    return ERR_SUCCESS;
+}
+
+void free_lane(Lane *ln) {
+    if (ln->d_ws) cudaFree(ln->d_ws);
+    if (ln->d_scal) cudaFree(ln->d_scal);
+    if (ln->d_sflags) cudaFree(ln->d_sflags);
+    if (ln->d_serr) cudaFree(ln->d_serr);
+    if (ln->d_xt) cudaFree(ln->d_xt);
+    *ln = Lane{};
+}
+
+// The scratch of the solves issued on stream st (NULL or the instance's own stream:
+// the main lane, allocated when the instance was created).  Another stream's lane is
+// created on its first call: tickets, counters and status word here, workspaces as
+// its calls need them.
+int lane_for(b200_solver_t *s, cudaStream_t st, Lane **out) {
+    if (!st || st == s->st) {
+        *out = &s->main;
+        return ERR_SUCCESS;
+    }
+    std::lock_guard<std::mutex> lock(s->lane_mu);
+    auto it = s->lanes.find(st);
+    if (it != s->lanes.end()) {
+        *out = it->second;
+        return ERR_SUCCESS;
+    }
+    Lane *ln = new Lane();
+    ln->st = st;
+    int rc = dalloc(&ln->d_sflags, (size_t)4 * s->cblknbr + 4);
+    if (!rc) rc = dalloc(&ln->d_serr, 1);
+    if (!rc && cudaMemsetAsync(ln->d_serr, 0, sizeof(int), st) != cudaSuccess) rc = ERR_INTERNAL;
+    if (rc) {
+        free_lane(ln);
+        delete ln;
+        return rc;
+    }
+    s->lanes[st] = ln;
+    *out = ln;
     return ERR_SUCCESS;
 }
 
@@ -705,12 +760,15 @@ int ensure_stage(b200_solver_t *s, size_t doubles) {
     return ERR_SUCCESS;
 }
 
-int ensure_scal(b200_solver_t *s, int count) {
-    if (count <= s->scal_cap) return ERR_SUCCESS;
-    if (s->d_scal) cudaFree(s->d_scal);
-    s->d_scal = nullptr;
-    RET(dalloc(&s->d_scal, (size_t)count));
-    s->scal_cap = count;
+int ensure_scal(Lane *ln, int count) {
+    if (count <= ln->scal_cap) return ERR_SUCCESS;
+    if (ln->d_scal) {
+        CU(cudaStreamSynchronize(ln->st));
+        cudaFree(ln->d_scal);
+    }
+    ln->d_scal = nullptr;
+    RET(dalloc(&ln->d_scal, (size_t)count));
+    ln->scal_cap = count;
     return ERR_SUCCESS;
 }
 
@@ -890,14 +948,14 @@ bool flow_withheld() {
 }
 
 template <typename T>
-int enqueue_sweeps(b200_solver_t *s, T *x, T *aux, int64_t ldx, int nrhs, cudaStream_t st, int *launches,
+int enqueue_sweeps(b200_solver_t *s, Lane *ln, T *x, T *aux, int64_t ldx, int nrhs, cudaStream_t st, int *launches,
                    Trace *tr = nullptr, int parts = SWEEP_BOTH) {
     const T *L = (const T *)s->dL;
     const T *Ub = (s->facto == FACTO_GETRF) ? (const T *)s->dU : L;
     const T *WL = (const T *)s->dWL;
     const T *WB = (s->facto == FACTO_GETRF) ? (const T *)s->dWU : WL;
     const int N = s->cblknbr, nlev = (int)s->levels.size(), fl0 = s->flow_level;
-    int *fl = s->d_sflags, *abort_word = fl + 2;
+    int *fl = ln->d_sflags, *abort_word = fl + 2;
     CU(cudaMemsetAsync(fl, 0, ((size_t)4 * N + 4) * sizeof(int), st));
     if (flow_withheld()) CU(cudaMemsetAsync(fl, 1, 1, st));  // forward ticket = 1
     // the diagonal products accumulate their K chunks: zero their outputs (aux now, x
@@ -923,7 +981,7 @@ int enqueue_sweeps(b200_solver_t *s, T *x, T *aux, int64_t ldx, int nrhs, cudaSt
     if (fl0 < nlev) {
         if (tr) tr->begin(st);
         launch_solve_flow<T, T>(s->ds, s->d_fitem_f, s->n_fitem_f, s->d_leaf, s->d_flist, s->d_need_f, s->d_nprev_f,
-                                L, WL, s->d_woff, x, aux, ldx, nrhs, 0, fl, fl + 4, fl + 4 + N, abort_word, s->d_serr,
+                                L, WL, s->d_woff, x, aux, ldx, nrhs, 0, fl, fl + 4, fl + 4 + N, abort_word, ln->d_serr,
                                 st);
         if (tr) tr->end(1, st);
         *launches += 1;
@@ -941,7 +999,7 @@ int enqueue_sweeps(b200_solver_t *s, T *x, T *aux, int64_t ldx, int nrhs, cudaSt
         if (tr) tr->begin(st);
         launch_solve_flow<T, T>(s->ds, s->d_fitem_b, s->n_fitem_b, s->d_leaf, s->d_flist, s->d_need_b, s->d_nprev_b,
                                 Ub, WB, s->d_woff, x, aux, ldx, nrhs, 1, fl + 1, fl + 4 + 2 * N, fl + 4 + 3 * N,
-                                abort_word, s->d_serr, st);
+                                abort_word, ln->d_serr, st);
         if (tr) tr->end(2, st);
         *launches += 1;
     }
@@ -969,12 +1027,12 @@ int enqueue_sweeps(b200_solver_t *s, T *x, T *aux, int64_t ldx, int nrhs, cudaSt
 // aux (n x nrhs doubles).  An FP32 factor runs the sweeps in FP32 -- they apply the
 // preconditioner of an FP64 refinement -- on two n x nrhs float blocks held in aux,
 // converted from and back to x.
-int sweeps(b200_solver_t *s, double *x, double *aux, int64_t ldx, int nrhs, cudaStream_t st, int *launches,
-           Trace *tr = nullptr) {
-    if (!s->f32) return enqueue_sweeps<double>(s, x, aux, ldx, nrhs, st, launches, tr);
+int sweeps(b200_solver_t *s, Lane *ln, double *x, double *aux, int64_t ldx, int nrhs, cudaStream_t st,
+           int *launches, Trace *tr = nullptr) {
+    if (!s->f32) return enqueue_sweeps<double>(s, ln, x, aux, ldx, nrhs, st, launches, tr);
     float *xf = reinterpret_cast<float *>(aux), *af = xf + (size_t)s->n * nrhs;
     launch_convert<double, float>(s->n, nrhs, x, ldx, xf, s->n, st);
-    RET(enqueue_sweeps<float>(s, xf, af, s->n, nrhs, st, launches, tr));
+    RET(enqueue_sweeps<float>(s, ln, xf, af, s->n, nrhs, st, launches, tr));
     launch_convert<float, double>(s->n, nrhs, xf, s->n, x, ldx, st);
     *launches += 2;
     return ERR_SUCCESS;
@@ -986,14 +1044,15 @@ int sweeps(b200_solver_t *s, double *x, double *aux, int64_t ldx, int nrhs, cuda
 // contributions of the others), 1 the backward sweep (L^T or U, reading the Schur
 // rows of x as given), 2 x <- D^{-1} x (LDL^T).  aux: n x nrhs doubles of scratch.
 template <typename T>
-int sweep_step_t(b200_solver_t *s, T *x, T *aux, int64_t ldx, int nrhs, int step, cudaStream_t st, int *launches) {
+int sweep_step_t(b200_solver_t *s, Lane *ln, T *x, T *aux, int64_t ldx, int nrhs, int step, cudaStream_t st,
+                 int *launches) {
     const size_t pitch = (size_t)ldx * sizeof(T);
     if (step == 0) {
-        RET(enqueue_sweeps<T>(s, x, aux, ldx, nrhs, st, launches, nullptr, SWEEP_FORWARD));
+        RET(enqueue_sweeps<T>(s, ln, x, aux, ldx, nrhs, st, launches, nullptr, SWEEP_FORWARD));
         if (s->n1 > 0) CU(cudaMemcpy2DAsync(x, pitch, aux, pitch, (size_t)s->n1 * sizeof(T), nrhs, cudaMemcpyDeviceToDevice, st));
     } else if (step == 1) {
         if (s->n1 > 0) CU(cudaMemcpy2DAsync(aux, pitch, x, pitch, (size_t)s->n1 * sizeof(T), nrhs, cudaMemcpyDeviceToDevice, st));
-        RET(enqueue_sweeps<T>(s, x, aux, ldx, nrhs, st, launches, nullptr, SWEEP_BACKWARD));
+        RET(enqueue_sweeps<T>(s, ln, x, aux, ldx, nrhs, st, launches, nullptr, SWEEP_BACKWARD));
     } else if (s->facto == FACTO_SYTRF) {
         launch_solve_scale_diag<T>(s->ds, s->d_lvl_cblk, s->n_active, (const T *)s->dL, x, ldx, nrhs, st);
         *launches += 1;
@@ -1001,30 +1060,30 @@ int sweep_step_t(b200_solver_t *s, T *x, T *aux, int64_t ldx, int nrhs, int step
     return ERR_SUCCESS;
 }
 
-int sweep_step(b200_solver_t *s, double *x, double *aux, int64_t ldx, int nrhs, int step, cudaStream_t st,
+int sweep_step(b200_solver_t *s, Lane *ln, double *x, double *aux, int64_t ldx, int nrhs, int step, cudaStream_t st,
                int *launches) {
-    if (!s->f32) return sweep_step_t<double>(s, x, aux, ldx, nrhs, step, st, launches);
+    if (!s->f32) return sweep_step_t<double>(s, ln, x, aux, ldx, nrhs, step, st, launches);
     float *xf = reinterpret_cast<float *>(aux), *af = xf + (size_t)s->n * nrhs;
     launch_convert<double, float>(s->n, nrhs, x, ldx, xf, s->n, st);
-    RET(sweep_step_t<float>(s, xf, af, s->n, nrhs, step, st, launches));
+    RET(sweep_step_t<float>(s, ln, xf, af, s->n, nrhs, step, st, launches));
     launch_convert<float, double>(s->n, nrhs, xf, s->n, x, ldx, st);
     *launches += 2;
     return ERR_SUCCESS;
 }
 
-// Full solve of device b (original ordering): permute, sweeps, permute back.
-// Uses ws[0 : n*nrhs] as the permuted block; replayed from a CUDA graph per nrhs
-// when the call runs on the solver's own stream.
-int solve_device(b200_solver_t *s, int nrhs, double *b, int64_t ldb, cudaStream_t st) {
+// Full solve of device b (original ordering) on the lane of stream st: permute,
+// sweeps, permute back, with the lane's ws[0 : 2 n nrhs] as the permuted block and
+// the sweeps' scratch.
+int solve_device(b200_solver_t *s, Lane *ln, int nrhs, double *b, int64_t ldb, cudaStream_t st) {
     const int n = s->n;
-    RET(ensure_ws(s, (size_t)2 * n * nrhs));
-    double *xp = s->d_ws, *aux = s->d_ws + (size_t)n * nrhs;
+    RET(ensure_ws(ln, (size_t)2 * n * nrhs));
+    double *xp = ln->d_ws, *aux = ln->d_ws + (size_t)n * nrhs;
     int launches = 2;
     launch_permute(n, nrhs, s->d_peri, b, ldb, xp, n, 1, st);
-    RET(sweeps(s, xp, aux, n, nrhs, st, &launches));
+    RET(sweeps(s, ln, xp, aux, n, nrhs, st, &launches));
     launch_permute(n, nrhs, s->d_peri, xp, n, b, ldb, 0, st);
     CU(cudaGetLastError());
-    s->launches_solve = launches;
+    ln->launches_solve = launches;
     s->kernel_launches += launches;
     return ERR_SUCCESS;
 }
@@ -1033,6 +1092,7 @@ int solve_device(b200_solver_t *s, int nrhs, double *b, int64_t ldb, cudaStream_
 
 struct RefineCtx {
     b200_solver_t *s;
+    Lane *ln;
     cudaStream_t st;
     int n, nrhs;
     // independent problems: one per right-hand side column, or in a batch one per
@@ -1044,8 +1104,8 @@ struct RefineCtx {
     // A x in the permuted basis with the bcsc
     int spmv(const double *x, double *y, double alpha, double beta) {
         const double *vals = (s->facto == FACTO_GETRF) ? s->d_Uv : s->d_Lv;
-        if (nrhs > 1 && !s->d_xt) RET(dalloc(&s->d_xt, (size_t)n * 16));
-        launch_spmv(n, nrhs, s->d_colptr, s->d_rowtab, vals, x, n, y, n, alpha, beta, st, s->d_xt);
+        if (nrhs > 1 && !ln->d_xt) RET(dalloc(&ln->d_xt, (size_t)n * 16));
+        launch_spmv(n, nrhs, s->d_colptr, s->d_rowtab, vals, x, n, y, n, alpha, beta, st, ln->d_xt);
         s->kernel_launches += nrhs > 1 ? 2 * ((nrhs + 15) / 16) : 1;
         return ERR_SUCCESS;
     }
@@ -1053,27 +1113,27 @@ struct RefineCtx {
     double *aux = nullptr;  // n x nrhs scratch of the sweeps
     int spsv(double *z) {
         int l = 0;
-        int rc = sweeps(s, z, aux, n, nrhs, st, &l);
+        int rc = sweeps(s, ln, z, aux, n, nrhs, st, &l);
         s->kernel_launches += l;
         return rc;
     }
     // one BLAS-1 kernel launched by the caller
     void count(int k = 1) { s->kernel_launches += k; }
     int dots(const double *x, const double *y, std::vector<double> &out) {
-        if (segid) launch_seg_dots(nseg, seg, nrhs, x, n, y, n, s->d_scal, st);
-        else launch_dots(n, nrhs, x, n, y, n, s->d_scal, st);
+        if (segid) launch_seg_dots(nseg, seg, nrhs, x, n, y, n, ln->d_scal, st);
+        else launch_dots(n, nrhs, x, n, y, n, ln->d_scal, st);
         s->kernel_launches++;
         out.resize(np());
-        CU(cudaMemcpyAsync(out.data(), s->d_scal, np() * sizeof(double), cudaMemcpyDeviceToHost, st));
+        CU(cudaMemcpyAsync(out.data(), ln->d_scal, np() * sizeof(double), cudaMemcpyDeviceToHost, st));
         CU(cudaStreamSynchronize(st));
         return ERR_SUCCESS;
     }
     int set_scal(const std::vector<double> &v, int slot) {
-        CU(cudaMemcpyAsync(s->d_scal + (size_t)slot * np(), v.data(), np() * sizeof(double), cudaMemcpyHostToDevice,
+        CU(cudaMemcpyAsync(ln->d_scal + (size_t)slot * np(), v.data(), np() * sizeof(double), cudaMemcpyHostToDevice,
                            st));
         return ERR_SUCCESS;
     }
-    double *scal(int slot) { return s->d_scal + (size_t)slot * np(); }
+    double *scal(int slot) { return ln->d_scal + (size_t)slot * np(); }
     // vector operations over n x nrhs blocks with per-problem scalars from slot
     void copy(const double *x, double *y) {
         launch_copy(n, nrhs, x, n, y, n, st);
@@ -1098,7 +1158,7 @@ struct RefineCtx {
 int refine_sr(RefineCtx &c, const double *b, double *x, int itermax, double eps, int64_t *niter,
               std::vector<double> &berr) {
     const int n = c.n, R = c.np();
-    double *r = c.s->d_ws + (size_t)2 * n * c.nrhs, *dx = r + (size_t)n * c.nrhs;
+    double *r = c.ln->d_ws + (size_t)2 * n * c.nrhs, *dx = r + (size_t)n * c.nrhs;
     std::vector<double> nb, nr, last(R, 0.0), mask(R, 1.0);
     RET(c.dots(b, b, nb));
     for (auto &v : nb) v = std::sqrt(v);
@@ -1138,7 +1198,7 @@ int refine_cg(RefineCtx &c, const double *b, double *x, int itermax, double eps,
               std::vector<double> &berr) {
     const int n = c.n, R = c.np();
     const size_t blk = (size_t)n * c.nrhs;
-    double *gr = c.s->d_ws + 2 * blk, *gp = gr + blk, *gz = gp + blk, *g2 = gz + blk;
+    double *gr = c.ln->d_ws + 2 * blk, *gp = gr + blk, *gz = gp + blk, *g2 = gz + blk;
     std::vector<double> nb, nx, nr, beta, alpha, tmp;
     RET(c.dots(b, b, nb));
     RET(c.dots(x, x, nx));
@@ -1194,7 +1254,7 @@ int refine_gmres(RefineCtx &c, const double *b, double *x, int itermax, int im, 
                  std::vector<double> &berr) {
     const int n = c.n, R = c.np();
     const size_t blk = (size_t)n * c.nrhs;
-    double *V = c.s->d_ws + 2 * blk;               // (im+1) blocks
+    double *V = c.ln->d_ws + 2 * blk;              // (im+1) blocks
     double *W = V + (size_t)(im + 1) * blk;         // im blocks
     const int im1 = im + 1;
     std::vector<double> nb, nr, h, tmp;
@@ -1292,8 +1352,8 @@ int refine_gmres(RefineCtx &c, const double *b, double *x, int itermax, int im, 
     return ERR_SUCCESS;
 }
 
-int refine_device(b200_solver_t *s, int nrhs, const double *b, int64_t ldb, double *x, int64_t ldx, int method,
-                  double eps, int64_t itermax, int64_t im, int64_t *niter, double *berr, cudaStream_t st) {
+int refine_device(b200_solver_t *s, Lane *ln, int nrhs, const double *b, int64_t ldb, double *x, int64_t ldx,
+                  int method, double eps, int64_t itermax, int64_t im, int64_t *niter, double *berr, cudaStream_t st) {
     const int n = s->n;
     if (im < 1) im = 25;
     const size_t blk = (size_t)n * nrhs;
@@ -1303,20 +1363,20 @@ int refine_device(b200_solver_t *s, int nrhs, const double *b, int64_t ldb, doub
     else need += (size_t)(2 * im + 1) * blk;
     const size_t aux_at = need;
     need += blk;  // scratch of the sweeps
-    RET(ensure_ws(s, need));
+    RET(ensure_ws(ln, need));
     const int nseg = s->nsys > 0 ? s->nsys : 1;
-    RET(ensure_scal(s, 2 * nrhs * nseg));
-    double *bp = s->d_ws, *xp = s->d_ws + blk;
+    RET(ensure_scal(ln, 2 * nrhs * nseg));
+    double *bp = ln->d_ws, *xp = ln->d_ws + blk;
     launch_permute(n, nrhs, s->d_peri, b, ldb, bp, n, 1, st);
     launch_permute(n, nrhs, s->d_peri, x, ldx, xp, n, 1, st);
     s->kernel_launches += 3;
-    RefineCtx c{s, st, n, nrhs};
+    RefineCtx c{s, ln, st, n, nrhs};
     if (s->nsys > 0) {
         c.nseg = s->nsys;
         c.seg = s->d_sys_col;
         c.segid = s->d_segid;
     }
-    c.aux = s->d_ws + aux_at;
+    c.aux = ln->d_ws + aux_at;
     std::vector<double> be;
     int64_t it = 0;
     int rc;
@@ -1327,7 +1387,10 @@ int refine_device(b200_solver_t *s, int nrhs, const double *b, int64_t ldb, doub
     launch_permute(n, nrhs, s->d_peri, xp, n, x, ldx, 0, st);
     CU(cudaGetLastError());
     if (niter) *niter = it;
-    s->last_berr = be;
+    {
+        std::lock_guard<std::mutex> lock(s->berr_mu);
+        s->last_berr = be;
+    }
     // per column: the largest backward error of its problems (its systems in a batch)
     if (berr)
         for (int j = 0; j < nrhs; j++) {
@@ -1544,8 +1607,9 @@ int b200_solver_create_schur(const b200_symbol_t *sym, int facto, int precision,
     if (!rc) rc = s->dmalloc(&s->d_thr, 1);
     if (!rc) rc = s->dmalloc(&s->d_npiv, 1);
     if (!rc) rc = s->dmalloc(&s->d_err, 1);
-    if (!rc) rc = s->dmalloc(&s->d_serr, 1);
-    if (!rc && cudaMemsetAsync(s->d_serr, 0, sizeof(int), s->st) != cudaSuccess) rc = ERR_INTERNAL;
+    s->main.st = s->st;
+    if (!rc) rc = dalloc(&s->main.d_serr, 1);
+    if (!rc && cudaMemsetAsync(s->main.d_serr, 0, sizeof(int), s->st) != cudaSuccess) rc = ERR_INTERNAL;
     s->device = dev;
     if (!rc) rc = noalloc_scratch(dev, &s->noalloc_scratch);
     if (!rc && cudaEventCreate(&s->ev0) != cudaSuccess) rc = ERR_INTERNAL;
@@ -1563,7 +1627,11 @@ int b200_solver_destroy(b200_solver_t *s) {
     if (!s) return ERR_SUCCESS;
     if (s->st) cudaStreamSynchronize(s->st);
     if (s->fact_graph) cudaGraphExecDestroy(s->fact_graph);
-    for (auto &kv : s->solve_graphs) cudaGraphExecDestroy(kv.second);
+    for (auto &kv : s->lanes) {
+        free_lane(kv.second);
+        delete kv.second;
+    }
+    s->lanes.clear();
     for (void *p : s->dev_allocs) cudaFree(p);
     if (s->dL) cudaFree(s->dL);
     if (s->dU) cudaFree(s->dU);
@@ -1579,10 +1647,8 @@ int b200_solver_destroy(b200_solver_t *s) {
     if (s->d_umap) cudaFree(s->d_umap);
     if (s->d_spmv) cudaFree(s->d_spmv);
     if (s->d_dest) cudaFree(s->d_dest);
-    if (s->d_ws) cudaFree(s->d_ws);
+    free_lane(&s->main);
     if (s->d_stage) cudaFree(s->d_stage);
-    if (s->d_scal) cudaFree(s->d_scal);
-    if (s->d_xt) cudaFree(s->d_xt);
     if (s->ev0) cudaEventDestroy(s->ev0);
     if (s->ev1) cudaEventDestroy(s->ev1);
     if (s->own_stream && s->st) cudaStreamDestroy(s->st);
@@ -1636,11 +1702,13 @@ int b200_spm_values_device(b200_solver_t *s, const double *d_values, double anor
     if (s->facto == FACTO_GETRF) launch_gather_values(s->nnz, s->d_umap, d_values, s->d_Uv, st);
     if (anorm < 0.0) {
         // ||A||_F over the expanded bcsc (both triangles), as spmNorm(SpmFrobeniusNorm)
-        RET(ensure_scal(s, 4));
-        CU(cudaMemsetAsync(s->d_scal, 0, sizeof(double), st));
-        launch_dots((int)s->nnz, 1, s->d_Lv, s->nnz, s->d_Lv, s->nnz, s->d_scal, st);
+        Lane *ln = nullptr;
+        RET(lane_for(s, st, &ln));
+        RET(ensure_scal(ln, 4));
+        CU(cudaMemsetAsync(ln->d_scal, 0, sizeof(double), st));
+        launch_dots((int)s->nnz, 1, s->d_Lv, s->nnz, s->d_Lv, s->nnz, ln->d_scal, st);
         double ss = 0.0;
-        CU(cudaMemcpyAsync(&ss, s->d_scal, sizeof(double), cudaMemcpyDeviceToHost, st));
+        CU(cudaMemcpyAsync(&ss, ln->d_scal, sizeof(double), cudaMemcpyDeviceToHost, st));
         CU(cudaStreamSynchronize(st));
         anorm = std::sqrt(ss);
     }
@@ -1658,10 +1726,10 @@ int b200_get_diag(b200_solver_t *s, double *D, int64_t incD) {
     if (!s || !D || incD <= 0) return ERR_BADPARAM;
     if (!s->factored) return ERR_BADPARAM;  // pastixGetDiag requires the numerical factorization
     const int n = s->n;
-    RET(ensure_ws(s, (size_t)n));
-    if (s->f32) launch_get_diag<float>(s->ds, (const float *)s->dL, s->d_ws, s->st);
-    else launch_get_diag<double>(s->ds, (const double *)s->dL, s->d_ws, s->st);
-    CU(cudaMemcpy2DAsync(D, incD * sizeof(double), s->d_ws, sizeof(double), sizeof(double), n, cudaMemcpyDeviceToHost,
+    RET(ensure_ws(&s->main, (size_t)n));
+    if (s->f32) launch_get_diag<float>(s->ds, (const float *)s->dL, s->main.d_ws, s->st);
+    else launch_get_diag<double>(s->ds, (const double *)s->dL, s->main.d_ws, s->st);
+    CU(cudaMemcpy2DAsync(D, incD * sizeof(double), s->main.d_ws, sizeof(double), sizeof(double), n, cudaMemcpyDeviceToHost,
                          s->st));
     CU(cudaStreamSynchronize(s->st));
     return ERR_SUCCESS;
@@ -1768,8 +1836,8 @@ int b200_applyorder(b200_solver_t *s, int dir, int64_t nrhs, double *b, int64_t 
     if (!s || (dir != 0 && dir != 1) || nrhs < 0 || ldb < s->n || (!b && nrhs)) return ERR_BADPARAM;
     if (nrhs == 0) return ERR_SUCCESS;
     const int n = s->n;
-    RET(ensure_ws(s, (size_t)2 * n * nrhs));
-    double *d = s->d_ws, *p = s->d_ws + (size_t)n * nrhs;
+    RET(ensure_ws(&s->main, (size_t)2 * n * nrhs));
+    double *d = s->main.d_ws, *p = s->main.d_ws + (size_t)n * nrhs;
     CU(cudaMemcpy2DAsync(d, n * sizeof(double), b, ldb * sizeof(double), n * sizeof(double), nrhs,
                          cudaMemcpyHostToDevice, s->st));
     launch_permute(n, (int)nrhs, s->d_peri, d, n, p, n, dir == 0 ? 1 : 0, s->st);
@@ -1783,18 +1851,18 @@ int b200_trsm(b200_solver_t *s, int step, int64_t nrhs, double *b, int64_t ldb) 
     if (!s || !s->factored || step < 0 || step > 2 || nrhs < 0 || ldb < s->n || (!b && nrhs)) return ERR_BADPARAM;
     if (nrhs == 0) return ERR_SUCCESS;
     const int n = s->n;
-    RET(ensure_ws(s, (size_t)2 * n * nrhs));
-    double *x = s->d_ws, *aux = s->d_ws + (size_t)n * nrhs;
-    CU(cudaMemsetAsync(s->d_serr, 0, sizeof(int), s->st));
+    RET(ensure_ws(&s->main, (size_t)2 * n * nrhs));
+    double *x = s->main.d_ws, *aux = s->main.d_ws + (size_t)n * nrhs;
+    CU(cudaMemsetAsync(s->main.d_serr, 0, sizeof(int), s->st));
     CU(cudaMemcpy2DAsync(x, n * sizeof(double), b, ldb * sizeof(double), n * sizeof(double), nrhs,
                          cudaMemcpyHostToDevice, s->st));
     int launches = 0;
-    RET(sweep_step(s, x, aux, n, (int)nrhs, step, s->st, &launches));
+    RET(sweep_step(s, &s->main, x, aux, n, (int)nrhs, step, s->st, &launches));
     s->kernel_launches += launches;
     CU(cudaMemcpy2DAsync(b, ldb * sizeof(double), x, n * sizeof(double), n * sizeof(double), nrhs,
                          cudaMemcpyDeviceToHost, s->st));
     CU(cudaStreamSynchronize(s->st));
-    return sweep_status(s);
+    return sweep_status(&s->main);
 }
 
 int b200_spm_values(b200_solver_t *s, const double *values, double anorm) {
@@ -1951,15 +2019,15 @@ int b200_numfact_trace(b200_solver_t *s, double epsilon_magn_ctrl, double *ms, d
 int b200_solve_trace(b200_solver_t *s, int64_t nrhs, double *ms, double *bytes) {
     if (!s || !s->factored || nrhs <= 0 || !ms) return ERR_BADPARAM;
     const int n = s->n;
-    RET(ensure_ws(s, (size_t)2 * n * nrhs));
-    double *xp = s->d_ws, *aux = s->d_ws + (size_t)n * nrhs;
+    RET(ensure_ws(&s->main, (size_t)2 * n * nrhs));
+    double *xp = s->main.d_ws, *aux = s->main.d_ws + (size_t)n * nrhs;
     CU(cudaMemsetAsync(xp, 0, (size_t)n * nrhs * sizeof(double), s->st));
     Trace tr;
     tr.detail = &s->trace_detail;
     int launches = 0;
     tr.begin(s->st);
     tr.end(0, s->st);
-    int rc = sweeps(s, xp, aux, n, (int)nrhs, s->st, &launches, &tr);
+    int rc = sweeps(s, &s->main, xp, aux, n, (int)nrhs, s->st, &launches, &tr);
     if (rc) return rc;
     CU(cudaStreamSynchronize(s->st));
     s->kernel_launches += launches;
@@ -2007,8 +2075,10 @@ int b200_solve_device(b200_solver_t *s, int64_t nrhs, double *d_b, int64_t ldb, 
     if (!s || !s->factored || nrhs < 0 || ldb < s->n) return ERR_BADPARAM;
     if (nrhs == 0) return ERR_SUCCESS;
     cudaStream_t st = stream ? (cudaStream_t)stream : s->st;
-    CU(cudaMemsetAsync(s->d_serr, 0, sizeof(int), st));
-    return solve_device(s, (int)nrhs, d_b, ldb, st);
+    Lane *ln = nullptr;
+    RET(lane_for(s, st, &ln));
+    CU(cudaMemsetAsync(ln->d_serr, 0, sizeof(int), st));
+    return solve_device(s, ln, (int)nrhs, d_b, ldb, st);
 }
 
 int b200_solve_device_noalloc(b200_solver_t *s, int64_t nrhs, double *d_b, int64_t ldb, void *stream) {
@@ -2027,26 +2097,29 @@ int b200_solve_device_noalloc(b200_solver_t *s, int64_t nrhs, double *d_b, int64
     if (!xp) return ERR_INTERNAL;
     double *aux = xp + (size_t)n * nrhs;
     cudaStream_t st = stream ? (cudaStream_t)stream : s->st;
-    CU(cudaMemsetAsync(s->d_serr, 0, sizeof(int), st));
+    // the sweeps' tickets, counters and status word: the main lane's, whatever the
+    // stream (allocated with the instance; a stream's own lane would be allocated here)
+    Lane *ln = &s->main;
+    CU(cudaMemsetAsync(ln->d_serr, 0, sizeof(int), st));
     // every entry of the scratch used here is written before it is read: the first half
     // by the permutation, the second by the forward diagonal products (for an FP32
     // factor, the two float blocks of the sweeps by the conversion and the products)
     int launches = 2;
     launch_permute(n, (int)nrhs, s->d_peri, d_b, ldb, xp, n, 1, st);
-    RET(sweeps(s, xp, aux, n, (int)nrhs, st, &launches));
+    RET(sweeps(s, ln, xp, aux, n, (int)nrhs, st, &launches));
     launch_permute(n, (int)nrhs, s->d_peri, xp, n, d_b, ldb, 0, st);
     CU(cudaGetLastError());
     s->kernel_launches += launches;
     return ERR_SUCCESS;
 }
 
-// Bit 4 of the sweep status word: a dataflow sweep of the last solve / refinement
-// call gave up waiting for its inputs (its result is not to be used).  Every call
-// that runs sweeps clears the word first.  Read after the stream has been
-// synchronized.
-static int sweep_status(b200_solver_t *s) {
+// Bit 4 of a lane's sweep status word: a dataflow sweep of the last solve /
+// refinement call on that stream gave up waiting for its inputs (its result is not
+// to be used).  Every call that runs sweeps clears the word first.  Read after the
+// stream has been synchronized.
+static int sweep_status(Lane *ln) {
     int err = 0;
-    if (cudaMemcpy(&err, s->d_serr, sizeof(int), cudaMemcpyDeviceToHost) != cudaSuccess) return ERR_INTERNAL;
+    if (cudaMemcpy(&err, ln->d_serr, sizeof(int), cudaMemcpyDeviceToHost) != cudaSuccess) return ERR_INTERNAL;
     if (err & 16) {
         fprintf(stderr, "pastix_b200: a solve sweep timed out waiting for its inputs\n");
         return ERR_INTERNAL;
@@ -2054,9 +2127,11 @@ static int sweep_status(b200_solver_t *s) {
     return ERR_SUCCESS;
 }
 
-int b200_solve_status(b200_solver_t *s) {
+int b200_solve_status(b200_solver_t *s, void *stream) {
     if (!s) return ERR_BADPARAM;
-    return sweep_status(s);
+    Lane *ln = nullptr;
+    RET(lane_for(s, stream ? (cudaStream_t)stream : s->st, &ln));
+    return sweep_status(ln);
 }
 
 int b200_solve(b200_solver_t *s, int64_t nrhs, double *b, int64_t ldb) {
@@ -2067,21 +2142,21 @@ int b200_solve(b200_solver_t *s, int64_t nrhs, double *b, int64_t ldb) {
     RET(ensure_stage(s, (size_t)n * nrhs));
     double *db = s->d_stage;
     int rc = ERR_SUCCESS;
-    if (cudaMemsetAsync(s->d_serr, 0, sizeof(int), s->st) != cudaSuccess) rc = ERR_INTERNAL;
+    if (cudaMemsetAsync(s->main.d_serr, 0, sizeof(int), s->st) != cudaSuccess) rc = ERR_INTERNAL;
     if (!rc && cudaMemcpy2DAsync(db, n * sizeof(double), b, ldb * sizeof(double), n * sizeof(double), nrhs,
                                  cudaMemcpyHostToDevice, s->st) != cudaSuccess) rc = ERR_INTERNAL;
     if (!rc) {
         cudaEventRecord(s->ev0, s->st);
-        rc = solve_device(s, (int)nrhs, db, n, s->st);
+        rc = solve_device(s, &s->main, (int)nrhs, db, n, s->st);
         cudaEventRecord(s->ev1, s->st);
     }
     if (!rc && cudaMemcpy2DAsync(b, ldb * sizeof(double), db, n * sizeof(double), n * sizeof(double), nrhs,
                                  cudaMemcpyDeviceToHost, s->st) != cudaSuccess) rc = ERR_INTERNAL;
     if (cudaStreamSynchronize(s->st) != cudaSuccess) rc = ERR_INTERNAL;
-    if (!rc) rc = sweep_status(s);
+    if (!rc) rc = sweep_status(&s->main);
     float ms = 0;
     if (!rc) cudaEventElapsedTime(&ms, s->ev0, s->ev1);
-    s->t_solve = ms;
+    s->main.t_solve = ms;
     return rc;
 }
 
@@ -2093,11 +2168,13 @@ int b200_refine_device(b200_solver_t *s, int64_t nrhs, const double *d_b, int64_
     if (nrhs == 0) return ERR_SUCCESS;
     cudaStream_t st = stream ? (cudaStream_t)stream : s->st;
     auto t0 = std::chrono::steady_clock::now();
-    CU(cudaMemsetAsync(s->d_serr, 0, sizeof(int), st));
-    int rc = refine_device(s, (int)nrhs, d_b, ldb, d_x, ldx, method, eps, itermax, gmres_im, niter, berr, st);
+    Lane *ln = nullptr;
+    RET(lane_for(s, st, &ln));
+    CU(cudaMemsetAsync(ln->d_serr, 0, sizeof(int), st));
+    int rc = refine_device(s, ln, (int)nrhs, d_b, ldb, d_x, ldx, method, eps, itermax, gmres_im, niter, berr, st);
     if (!rc && cudaStreamSynchronize(st) != cudaSuccess) rc = ERR_INTERNAL;
-    if (!rc) rc = sweep_status(s);
-    s->t_refine = std::chrono::duration<double, std::milli>(std::chrono::steady_clock::now() - t0).count();
+    if (!rc) rc = sweep_status(ln);
+    ln->t_refine = std::chrono::duration<double, std::milli>(std::chrono::steady_clock::now() - t0).count();
     return rc;
 }
 
@@ -2138,8 +2215,9 @@ int b200_spmv(b200_solver_t *s, int64_t nrhs, double alpha, const double *x, int
         launch_permute(n, (int)nrhs, s->d_peri, dx, n, px, n, 1, s->st);
         launch_permute(n, (int)nrhs, s->d_peri, dy, n, py, n, 1, s->st);
         const double *vals = (s->facto == FACTO_GETRF) ? s->d_Uv : s->d_Lv;
-        if (nrhs > 1 && !s->d_xt && dalloc(&s->d_xt, (size_t)n * 16)) rc = ERR_OOM;
-        if (!rc) launch_spmv(n, (int)nrhs, s->d_colptr, s->d_rowtab, vals, px, n, py, n, alpha, beta, s->st, s->d_xt);
+        if (nrhs > 1 && !s->main.d_xt && dalloc(&s->main.d_xt, (size_t)n * 16)) rc = ERR_OOM;
+        if (!rc)
+            launch_spmv(n, (int)nrhs, s->d_colptr, s->d_rowtab, vals, px, n, py, n, alpha, beta, s->st, s->main.d_xt);
         launch_permute(n, (int)nrhs, s->d_peri, py, n, dy, n, 0, s->st);
         if (cudaMemcpy2DAsync(y, ldy * sizeof(double), dy, n * sizeof(double), n * sizeof(double), nrhs,
                               cudaMemcpyDeviceToHost, s->st) != cudaSuccess) rc = ERR_INTERNAL;
@@ -2156,13 +2234,15 @@ int b200_spmv_device(b200_solver_t *s, int64_t nrhs, double alpha, const double 
     const int n = s->n;
     const size_t blk = (size_t)n * nrhs;
     cudaStream_t st = stream ? (cudaStream_t)stream : s->st;
-    RET(ensure_ws(s, 2 * blk));
-    double *px = s->d_ws, *py = s->d_ws + blk;
-    if (nrhs > 1 && !s->d_xt) RET(dalloc(&s->d_xt, (size_t)n * 16));
+    Lane *ln = nullptr;
+    RET(lane_for(s, st, &ln));
+    RET(ensure_ws(ln, 2 * blk));
+    double *px = ln->d_ws, *py = ln->d_ws + blk;
+    if (nrhs > 1 && !ln->d_xt) RET(dalloc(&ln->d_xt, (size_t)n * 16));
     const double *vals = (s->facto == FACTO_GETRF) ? s->d_Uv : s->d_Lv;
     launch_permute(n, (int)nrhs, s->d_peri, d_x, ldx, px, n, 1, st);
     launch_permute(n, (int)nrhs, s->d_peri, d_y, ldy, py, n, 1, st);
-    launch_spmv(n, (int)nrhs, s->d_colptr, s->d_rowtab, vals, px, n, py, n, alpha, beta, st, s->d_xt);
+    launch_spmv(n, (int)nrhs, s->d_colptr, s->d_rowtab, vals, px, n, py, n, alpha, beta, st, ln->d_xt);
     launch_permute(n, (int)nrhs, s->d_peri, py, n, d_y, ldy, 0, st);
     CU(cudaGetLastError());
     s->kernel_launches += 3 + (nrhs > 1 ? 2 * ((nrhs + 15) / 16) : 1);
@@ -2200,17 +2280,17 @@ int b200_factor_download(b200_solver_t *s, double *L, double *U) {
 int b200_stats(b200_solver_t *s, double *out) {
     if (!s || !out) return ERR_BADPARAM;
     out[0] = s->t_fact;
-    out[1] = s->t_solve;
-    out[2] = s->t_refine;
+    out[1] = s->main.t_solve;
+    out[2] = s->main.t_refine;
     out[3] = (double)s->last_npiv;
     out[4] = s->thr_used;
     out[5] = ((double)s->arena + s->winv_elems) * s->esz * (s->dU ? 2 : 1);
     out[6] = (double)s->levels.size();
     out[7] = s->launches_fact;
-    out[8] = s->launches_solve;
+    out[8] = s->main.launches_solve;
     out[9] = (double)s->coefnbr;
     out[10] = (double)s->kernel_launches;
-    out[11] = (double)s->ws_cap * sizeof(double);
+    out[11] = (double)s->main.ws_cap * sizeof(double);
     out[12] = (double)s->stage_cap * sizeof(double);
     return ERR_SUCCESS;
 }

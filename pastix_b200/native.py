@@ -76,7 +76,7 @@ def lib():
         L.b200_trace_kinds.argtypes = [_P, _P, _P, C.c_int]
         L.b200_solve_device.argtypes = [_P, _I64, _P, _I64, _P]
         L.b200_solve_device_noalloc.argtypes = [_P, _I64, _P, _I64, _P]
-        L.b200_solve_status.argtypes = [_P]
+        L.b200_solve_status.argtypes = [_P, _P]
         L.b200_refine.argtypes = [_P, _I64, _P, _I64, _P, _I64, C.c_int, C.c_double, _I64, _I64,
                                   C.POINTER(_I64), _P]
         L.b200_refine_device.argtypes = [_P, _I64, _P, _I64, _P, _I64, C.c_int, C.c_double, _I64, _I64,
@@ -321,10 +321,10 @@ class Solver:
         check(lib().b200_factor_download(self.h, _p(L), _p(U)), "b200_factor_download")
         return L, U
 
-    def solve_status(self):
-        """Raise if a sweep of the last solve / refinement gave up waiting (call it
-        after synchronizing the stream of a device solve)."""
-        check(lib().b200_solve_status(self.h), "b200_solve_status")
+    def solve_status(self, stream: int | None = None):
+        """Raise if a sweep of the last solve / refinement on stream (None: the
+        solver's own) gave up waiting (call it after synchronizing that stream)."""
+        check(lib().b200_solve_status(self.h, _P(stream) if stream else None), "b200_solve_status")
 
     def stats(self) -> dict:
         out = np.zeros(13)

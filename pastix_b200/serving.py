@@ -253,3 +253,357 @@ def torch_batcher(server: SolveServer) -> ContinuousBatcher:
 
     return ContinuousBatcher(server.solve, server.max_nrhs, lambda bs: torch.cat(bs, dim=0), split,
                              refactor=server.refactor)
+
+
+# ====================================================================== real-time serving loop
+
+class _Req:
+    __slots__ = ("idx", "arrival", "item", "epoch", "cols")
+
+    def __init__(self, idx, arrival, item, epoch, cols):
+        self.idx, self.arrival, self.item, self.epoch, self.cols = idx, arrival, item, epoch, cols
+
+
+class ServingLoop:
+    """Continuous batching of solve requests that arrive in real time, on resident
+    factors, with batches running concurrently on the GPU.
+
+    The reference answers requests one PaStiX instance call at a time
+    (``pastix_task_solve`` + ``pastix_task_refine``, sopalin/pastix_task_solve.c:550,
+    refinement/pastix_task_refine.c:226) and refactors in place
+    (``pastix_task_numfact`` on the kept analysis, sopalin/pastix_task_sopalin.c:563).
+    Here:
+
+    * ``submit`` may be called from any thread (a producer) while batches run;
+      requests carry their own right-hand-side block.
+    * ``lanes`` batches run at once, each on its own CUDA stream with its own
+      buffers and solver workspaces (the C ABI keeps scratch per stream), so their
+      sweeps, SpMVs and refinement launches overlap on the device.  Whenever a lane
+      is idle, the dispatcher admits the pending requests in arrival order while
+      their columns fit the lane's ``max_cols`` slots, as one multi-RHS solve +
+      refinement (each column keeps its own stopping rule).
+    * A ``Refactor`` item starts an epoch: requests submitted before it are served
+      by the old factor, those after it by the new one.  The refactorization runs
+      at once into a standby factor instance if the device has room for one (the
+      backend's ``standby_ok``, by HBM footprint) -- concurrently with the batches
+      still served by the old factor, which becomes the next standby when they are
+      done; without room it runs in place once the old epoch's work has drained.
+
+    The backend (``GpuServingBackend`` on the GPU, any object with the same methods
+    elsewhere) provides ``lanes``, ``max_cols``, ``slots`` (factor instances, 1 or 2),
+    ``standby_ok(slot)`` (the instance exists), ``refactor(slot, values)`` and
+    ``solve(slot, lane, blocks)`` -> (list of x blocks, list of per-column berr,
+    info); the initial factor is slot 0's."""
+
+    def __init__(self, backend, clock=time.perf_counter):
+        import collections
+        import threading
+        self.b = backend
+        self.clock = clock
+        self.cv = threading.Condition()
+        self.pending = collections.deque()    # _Req in arrival order (requests only)
+        self.epoch = 0                         # epoch of the next submitted request
+        self.slot_of = {0: 0}                  # epoch -> factor slot, once its factor is ready
+        self.busy = {}                         # slot -> batches in flight
+        self.refactors = collections.deque()   # (epoch, values) not yet started
+        self.results = {}
+        self.batches = []
+        self.n_submitted = 0
+        self.closed = False
+        self.error = None
+        self.idle_lanes = list(range(backend.lanes))
+        self.t0 = clock()
+        self.threads = [threading.Thread(target=self._dispatch, daemon=True),
+                        threading.Thread(target=self._refactor_worker, daemon=True)]
+        for t in self.threads:
+            t.start()
+
+    # ------------------------------------------------------------ producer side
+    def submit(self, item) -> int:
+        """A request (a right-hand-side block with ``shape[0]`` columns) or a
+        ``Refactor``.  Returns the item's index; arrival = now."""
+        with self.cv:
+            idx = self.n_submitted
+            self.n_submitted += 1
+            t = self.clock() - self.t0
+            if isinstance(item, Refactor):
+                self.epoch += 1
+                self.refactors.append((self.epoch, item.values, idx, t))
+            else:
+                k = int(item.shape[0])
+                if k > self.b.max_cols:
+                    raise ValueError(f"request of {k} columns above {self.b.max_cols} slots")
+                self.pending.append(_Req(idx, t, item, self.epoch, k))
+            self.cv.notify_all()
+            return idx
+
+    def drain(self, timeout: float = 600.0) -> dict:
+        """Wait until every submitted item is done; returns {index: result}."""
+        end = time.monotonic() + timeout
+        with self.cv:
+            while len(self.results) < self.n_submitted and self.error is None:
+                left = end - time.monotonic()
+                if left <= 0:
+                    raise TimeoutError(f"{self.n_submitted - len(self.results)} items not done")
+                self.cv.wait(min(left, 0.5))
+            if self.error is not None:
+                raise self.error
+            return dict(self.results)
+
+    def close(self):
+        with self.cv:
+            self.closed = True
+            self.cv.notify_all()
+        for t in self.threads:
+            t.join(timeout=30)
+
+    # ------------------------------------------------------------ internals
+    def _fail(self, exc):
+        with self.cv:
+            if self.error is None:
+                self.error = exc
+            self.cv.notify_all()
+
+    def _epoch_drained(self, e) -> bool:
+        """No request of epoch e waits and none is on the GPU."""
+        if any(r.epoch == e for r in self.pending):
+            return False
+        return not any(b["epoch"] == e and b["done"] is None for b in self.batches)
+
+    def _free_slot(self, e):
+        """A factor slot that epoch e may refactor into, or None for now: a slot no
+        undrained earlier epoch uses and nothing runs on -- the standby if the backend
+        holds one, else the previous epoch's own slot once that epoch has drained."""
+        in_use = {self.slot_of[q] for q in self.slot_of if q < e and not self._epoch_drained(q)}
+        for s in range(self.b.slots):
+            if s not in in_use and not self.busy.get(s, 0) and self.b.standby_ok(s):
+                return s
+        return None
+
+    def _refactor_worker(self):
+        try:
+            while True:
+                with self.cv:
+                    while not self.refactors and not self.closed:
+                        self.cv.wait(0.5)
+                    if self.closed and not self.refactors:
+                        return
+                    e, values, idx, t_arr = self.refactors[0]
+                    # the previous epoch's factor must exist before this one is placed
+                    while (e - 1) not in self.slot_of:
+                        self.cv.wait(0.5)
+                    slot = self._free_slot(e)
+                    while slot is None:
+                        self.cv.wait(0.05)
+                        slot = self._free_slot(e)
+                    self.busy[slot] = self.busy.get(slot, 0) + 1
+                    self.refactors.popleft()
+                t0 = self.clock() - self.t0
+                info = self.b.refactor(slot, values)
+                t1 = self.clock() - self.t0
+                with self.cv:
+                    self.busy[slot] -= 1
+                    self.slot_of[e] = slot
+                    self.results[idx] = dict(refactor=info, slot=slot, epoch=e, arrival=t_arr, start=t0, done=t1,
+                                             latency=t1 - t_arr,
+                                             standby=slot != self.slot_of[e - 1])
+                    self.cv.notify_all()
+        except BaseException as exc:  # noqa: BLE001 -- reported by drain()
+            self._fail(exc)
+
+    def _dispatch(self):
+        import threading
+        try:
+            while True:
+                with self.cv:
+                    while True:
+                        if self.closed:
+                            return
+                        if self.pending and self.idle_lanes and self.pending[0].epoch in self.slot_of:
+                            break
+                        self.cv.wait(0.5)
+                    e = self.pending[0].epoch
+                    slot = self.slot_of[e]
+                    take, cols = [], 0
+                    while self.pending and self.pending[0].epoch == e and cols + self.pending[0].cols <= self.b.max_cols:
+                        r = self.pending.popleft()
+                        take.append(r)
+                        cols += r.cols
+                    lane = self.idle_lanes.pop(0)
+                    self.busy[slot] = self.busy.get(slot, 0) + 1
+                    rec = dict(requests=[r.idx for r in take], cols=cols, lane=lane, slot=slot, epoch=e,
+                               start=self.clock() - self.t0, done=None)
+                    self.batches.append(rec)
+                threading.Thread(target=self._run_batch, args=(rec, take, slot, lane), daemon=True).start()
+        except BaseException as exc:  # noqa: BLE001
+            self._fail(exc)
+
+    def _run_batch(self, rec, take, slot, lane):
+        try:
+            xs, berrs, info = self.b.solve(slot, lane, [r.item for r in take])
+            t1 = self.clock() - self.t0
+            with self.cv:
+                rec["done"] = t1
+                rec["service"] = t1 - rec["start"]
+                rec["iters"] = info.get("iters")
+                for r, x, be in zip(take, xs, berrs):
+                    self.results[r.idx] = dict(x=x, berr=be, arrival=r.arrival, start=rec["start"], done=t1,
+                                               latency=t1 - r.arrival, batch=len(self.batches) - 1, lane=lane,
+                                               slot=slot, epoch=r.epoch)
+                self.busy[slot] -= 1
+                self.idle_lanes.append(lane)
+                self.cv.notify_all()
+        except BaseException as exc:  # noqa: BLE001
+            self._fail(exc)
+
+
+def replay(loop: ServingLoop, trace, clock=time.perf_counter):
+    """Producer: submit trace = [(offset_s, item)] at those wall-clock offsets from
+    now, from a thread of its own; returns the thread (join it, then drain)."""
+    import threading
+
+    def run():
+        t0 = clock()
+        for off, item in sorted(trace, key=lambda p: p[0]):
+            dt = off - (clock() - t0)
+            if dt > 0:
+                time.sleep(dt)
+            loop.submit(item)
+
+    th = threading.Thread(target=run, daemon=True)
+    th.start()
+    return th
+
+
+def poisson_offsets(n: int, rate: float, seed: int = 0) -> np.ndarray:
+    """Arrival offsets (s) of a Poisson process of the given rate (requests/s)."""
+    return np.cumsum(np.random.default_rng(seed).exponential(1.0 / rate, n))
+
+
+class GpuServingBackend:
+    """The GPU side of ``ServingLoop``: factor instances (slot 0, and a standby
+    slot 1 created when the device has room for a second one), and lanes, each a
+    CUDA stream with its own request buffers (max_cols x n) and, inside the
+    library, its own solve workspaces on every factor instance.  Requests are device
+    blocks of shape (k, n) (torch tensors, column-major n x k blocks)."""
+
+    def __init__(self, analysis, precision: str = "tf32x3", method: str = "cg", eps: float = 1e-12,
+                 itermax: int = 250, gmres_im: int = 25, lanes: int = 2, max_cols: int = 256,
+                 standby: bool = True, device: int = 0, values=None):
+        import threading
+        import torch
+        self.torch = torch
+        self.dev = torch.device("cuda", device)
+        self.an = analysis
+        self.st = analysis.structure()
+        self.n = self.st.n
+        self.precision, self.method, self.eps, self.itermax, self.im = precision, method, eps, itermax, gmres_im
+        self.lanes = int(lanes)
+        self.max_cols = bucket(max_cols)
+        self.slots = 2 if standby else 1
+        self.nnz, self.lmap, self.umap = analysis.spm_maps()
+        self.lock = threading.Lock()
+        self.streams = [torch.cuda.Stream(device=self.dev) for _ in range(self.lanes)]
+        self.ref_stream = torch.cuda.Stream(device=self.dev)
+        self.d_b = [torch.zeros((self.max_cols, self.n), dtype=torch.float64, device=self.dev)
+                    for _ in range(self.lanes)]
+        self.d_x = [torch.zeros_like(b) for b in self.d_b]
+        self.d_vals = torch.empty(self.nnz, dtype=torch.float64, device=self.dev)
+        self.solvers = [None] * self.slots
+        torch.cuda.synchronize(self.dev)
+        free0, _ = torch.cuda.mem_get_info(self.dev)
+        self._make(0)
+        self.refactor(0, analysis.A.values if values is None else values)
+        self._warm(0)
+        free1, _ = torch.cuda.mem_get_info(self.dev)
+        self.footprint = max(free0 - free1, 1)   # one factor instance with its lane workspaces
+        # the standby instance, if the device holds a second one (by the first one's
+        # footprint, with 10 % to spare); created and warmed here, before serving, so
+        # that its warm-up never meets a batch in the lanes' buffers
+        self.standby_created = False
+        if self.slots == 2:
+            if free1 > 1.1 * self.footprint:
+                self._make(1)
+                self.refactor(1, analysis.A.values if values is None else values)
+                self._warm(1)
+                self.standby_created = True
+            else:
+                self.slots = 1
+
+    def _make(self, slot):
+        from . import native
+        s = native.Solver(self.st, self.an.facto_name, self.precision)
+        s.bcsc_load(self.an.bcsc())
+        s.spm_map(self.nnz, self.lmap, self.umap)
+        self.solvers[slot] = s
+
+    def _warm(self, slot):
+        """Size every lane's workspace on this instance for the largest batch."""
+        for lane in range(self.lanes):
+            z = self.torch.zeros((1, self.n), dtype=self.torch.float64, device=self.dev)
+            self.solve(slot, lane, [z], cols=self.max_cols)
+
+    def standby_ok(self, slot) -> bool:
+        """Whether factor slot exists (slot 1 only when HBM held a second instance)."""
+        return slot < len(self.solvers) and self.solvers[slot] is not None
+
+    def refactor(self, slot, values) -> dict:
+        t = self.torch
+        with self.lock:
+            if self.solvers[slot] is None:
+                raise RuntimeError(f"factor slot {slot} does not exist")
+            v = values if isinstance(values, t.Tensor) else t.from_numpy(np.ascontiguousarray(values, dtype=np.float64))
+            t0 = time.perf_counter()
+            with t.cuda.stream(self.ref_stream):
+                self.d_vals.copy_(v, non_blocking=False)
+                self.solvers[slot].spm_values_device(self.d_vals.data_ptr(), -1.0, self.ref_stream.cuda_stream)
+            npiv = self.solvers[slot].numfact(0.0)
+            ms = (time.perf_counter() - t0) * 1e3
+        return dict(ms=ms, nbpivots=npiv, numfact_ms=self.solvers[slot].stats()["numfact_ms"], slot=slot)
+
+    def solve(self, slot, lane, blocks, cols=None):
+        """One batch on a lane: the blocks' columns side by side (padded with zero
+        columns to a bucket size), solve + refinement on the lane's stream."""
+        t = self.torch
+        s = self.solvers[slot]
+        st = self.streams[lane]
+        ks = [int(b.shape[0]) for b in blocks]
+        k = sum(ks)
+        nb = bucket(cols or k)
+        d_b, d_x = self.d_b[lane], self.d_x[lane]
+        with t.cuda.stream(st):
+            c0 = 0
+            for b, kk in zip(blocks, ks):
+                d_b[c0:c0 + kk].copy_(b)
+                c0 += kk
+            if nb > k:
+                d_b[k:nb].zero_()
+            d_x[:nb].copy_(d_b[:nb])
+        s.solve_device(d_x.data_ptr(), nb, self.n, stream=st.cuda_stream)
+        it, berr = s.refine_device(d_b.data_ptr(), d_x.data_ptr(), nb, self.method, self.eps, self.itermax, self.im,
+                                   stream=st.cuda_stream)
+        with t.cuda.stream(st):
+            xs, c0 = [], 0
+            for kk in ks:
+                xs.append(d_x[c0:c0 + kk].clone())
+                c0 += kk
+        st.synchronize()
+        bes, c0 = [], 0
+        for kk in ks:
+            bes.append(np.asarray(berr[c0:c0 + kk]))
+            c0 += kk
+        return xs, bes, dict(iters=it, cols=k, padded=nb)
+
+    def matvec(self, slot, x):
+        """A x with slot's current values, for a device block x of shape (k, n)."""
+        y = self.torch.empty_like(x)
+        self.torch.cuda.synchronize(self.dev)
+        self.solvers[slot].spmv_device(x.data_ptr(), y.data_ptr(), x.shape[0], 1.0, 0.0)
+        self.torch.cuda.synchronize(self.dev)
+        return y
+
+    def close(self):
+        for s in self.solvers:
+            if s is not None:
+                s.close()
+        self.solvers = [None] * self.slots

@@ -1,0 +1,145 @@
+"""The real-time serving loop on the GPU (ServingLoop + GpuServingBackend).
+
+Requests are submitted from a producer thread at Poisson wall-clock times while
+batches run; idle lanes (CUDA streams with their own buffers and solve workspaces)
+admit the pending requests, so batches overlap on the device; refactorizations go
+into a standby factor.  Latencies are measured (completion minus submission, wall
+clock), not modelled."""
+import numpy as np
+import pytest
+
+from pastix_b200 import matrices as M
+from pastix_b200.refhost import Analysis
+from pastix_b200.serving import GpuServingBackend, Refactor, ServingLoop, poisson_offsets, replay
+
+pytestmark = pytest.mark.gpu
+
+BERR_TARGET = 1e-12
+
+
+def _rhs(backend, k, seed):
+    import torch
+    g = torch.Generator(device="cuda").manual_seed(seed)
+    xt = torch.rand((k, backend.n), generator=g, dtype=torch.float64, device="cuda") * 2 - 1
+    return backend.matvec(0, xt)
+
+
+def test_serving_loop_same_alone_and_in_the_mix():
+    """Each request's result in an overlapping mix (two lanes, arrivals faster than
+    service) equals its result served alone (arrivals spaced out, one request per
+    batch): both refined to <= 1e-12 and within 1e-9 of each other (two solutions at
+    backward error <= 1e-12 differ by at most ~cond(A) 2e-12, cond ~ 66 for the 24^3
+    27-point operator)."""
+    import torch
+    A = M.laplacian(24, 24, 24, 27, 26.0, shift=1e-3)
+    an = Analysis(A, "potrf")
+    be = GpuServingBackend(an, "tf32x3", "cg", BERR_TARGET, lanes=2, max_cols=64)
+    rng = np.random.default_rng(8)
+    ks = rng.integers(1, 24, 12)
+    bs = [_rhs(be, int(k), 100 + i) for i, k in enumerate(ks)]
+    alone = ServingLoop(be)
+    th = replay(alone, [(0.05 * i, b) for i, b in enumerate(bs)])
+    th.join()
+    ra = alone.drain(60)
+    alone.close()
+    mix = ServingLoop(be)
+    th = replay(mix, [(float(t), b) for t, b in zip(np.cumsum(rng.exponential(0.0003, len(bs))), bs)])
+    th.join()
+    rm = mix.drain(60)
+    mix.close()
+    overlap = any(b1["start"] < b2["done"] and b2["start"] < b1["done"] and b1["lane"] != b2["lane"]
+                  for i, b1 in enumerate(mix.batches) for b2 in mix.batches[i + 1:])
+    print(f"\nalone: {len(alone.batches)} batches; mix: {len(mix.batches)} batches of "
+          f"{[b['cols'] for b in mix.batches]} columns on lanes {[b['lane'] for b in mix.batches]}, "
+          f"overlapping {overlap}")
+    assert len(mix.batches) < len(bs)
+    assert overlap
+    for i, b in enumerate(bs):
+        assert ra[i]["berr"].max() <= BERR_TARGET and rm[i]["berr"].max() <= BERR_TARGET
+        d = (torch.linalg.vector_norm(rm[i]["x"] - ra[i]["x"]) / torch.linalg.vector_norm(ra[i]["x"])).item()
+        assert d <= 1e-9, (i, d)
+        r = b - be.matvec(0, rm[i]["x"])
+        berr = (torch.linalg.vector_norm(r, dim=1) / torch.linalg.vector_norm(b, dim=1)).max().item()
+        assert berr <= 1.01 * BERR_TARGET
+    be.close()
+
+
+def _residuals(A_vals, A, x, b):
+    """Backward errors of a device solution against the matrix with values A_vals (host)."""
+    import scipy.sparse as sp
+    Af = M.CSC(A.n, A.colptr, A.rowind, A_vals, A.symmetric, A.grid, A.name).full()
+    S = sp.csc_matrix((Af.values, Af.rowind, Af.colptr), shape=(A.n, A.n))
+    xh = x.cpu().numpy().T
+    bh = b.cpu().numpy().T
+    r = bh - S @ xh
+    return np.linalg.norm(r, axis=0) / np.linalg.norm(bh, axis=0)
+
+
+def test_serving_100cube_measured_latency():
+    """The serving workload at full size: 7-point Laplacian on 100^3 (n = 1e6)
+    resident; 100 requests with nrhs log-uniform in [1, 256] submitted at Poisson
+    times of rate 20 requests/s from a producer thread; a same-pattern
+    refactorization after every 50 requests with the matrix scaled D A D by d_i
+    uniform in [0.9, 1.1]; every request refined to <= 1e-12.  Mixed (FP32 factor,
+    3xTF32 updates) and FP64 factors, two lanes, standby factor.  Reports measured
+    p50 / p99 latency, throughput and the refactorizations' overlap with serving."""
+    import torch
+    A = M.laplacian(100, 100, 100, 7, 6.0)
+    an = Analysis(A, "potrf")
+    rng = np.random.default_rng(5)
+    nreq, rate = 100, 20.0
+    nrhs = np.floor(np.exp(rng.uniform(0.0, np.log(257.0), nreq))).astype(int).clip(1, 256)
+    col = np.repeat(np.arange(A.n), np.diff(A.colptr))
+    vals = [A.values]
+    for r in range(1, nreq // 50):
+        d = rng.uniform(0.9, 1.1, A.n)
+        vals.append(A.values * d[A.rowind] * d[col])
+    offs = poisson_offsets(nreq + len(vals) - 1, rate, seed=9)
+    report = {}
+    for prec in ("tf32x3", "fp64"):
+        be = GpuServingBackend(an, prec, "cg", BERR_TARGET, lanes=2, max_cols=256)
+        pool = _rhs(be, 256, 1234)  # right-hand sides: request i takes columns of the pool
+        trace, owner, pos = [], [], 0
+        for i in range(nreq):
+            if i and i % 50 == 0:
+                trace.append((float(offs[pos]), Refactor(vals[i // 50])))
+                owner.append(None)
+                pos += 1
+            c0 = int(rng.integers(0, 257 - nrhs[i]))
+            trace.append((float(offs[pos]), pool[c0:c0 + nrhs[i]]))
+            owner.append((i, c0))
+            pos += 1
+        loop = ServingLoop(be)
+        th = replay(loop, trace)
+        th.join()
+        res = loop.drain(600)
+        loop.close()
+        reqs = [res[j] for j, o in enumerate(owner) if o is not None]
+        refs = [res[j] for j, o in enumerate(owner) if o is None]
+        lat = np.array([r["latency"] for r in reqs]) * 1e3
+        berr = max(float(r["berr"].max()) for r in reqs)
+        span = max(r["done"] for r in reqs) - min(r["arrival"] for r in reqs)
+        # independent host residuals of a few requests of each epoch, against that epoch's matrix
+        checked = 0
+        for j, o in enumerate(owner):
+            if o is None or o[0] % 17:
+                continue
+            r = res[j]
+            bres = _residuals(vals[r["epoch"]], A, r["x"], trace[j][1])
+            assert bres.max() <= 1.05 * BERR_TARGET, (prec, o, bres.max())
+            checked += 1
+        overlapped = [rf["start"] < max(q["done"] for q in reqs if q["epoch"] == rf["epoch"] - 1) for rf in refs]
+        report[prec] = dict(
+            requests=nreq, rate_per_s=rate, columns=int(nrhs.sum()), batches=len(loop.batches),
+            mean_batch_cols=round(float(np.mean([b["cols"] for b in loop.batches])), 1),
+            latency_p50_ms=round(float(np.percentile(lat, 50)), 1),
+            latency_p99_ms=round(float(np.percentile(lat, 99)), 1),
+            throughput_req_per_s=round(nreq / span, 2), rhs_per_s=round(nrhs.sum() / span, 1),
+            berr_max=berr, refactor_ms=[round(rf["refactor"]["ms"], 1) for rf in refs],
+            refactor_standby=[bool(rf["standby"]) for rf in refs], refactor_overlapped_serving=overlapped,
+            standby_instance=be.standby_created, host_checked=checked)
+        assert berr <= BERR_TARGET
+        be.close()
+        del pool
+        torch.cuda.empty_cache()
+    print(f"\nserving 100^3 (measured): {report}")

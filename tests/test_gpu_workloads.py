@@ -1,6 +1,6 @@
-"""Full-size checks of the nonsymmetric LU workload and of the serving workload,
-through size-independent properties (backward error after refinement, agreement of
-the mixed and FP64 solutions, forward error against x_true)."""
+"""Full-size check of the nonsymmetric LU workload through size-independent
+properties (backward error after refinement, agreement of the mixed and FP64
+solutions, forward error against x_true), and the virtual-time continuous batcher."""
 import numpy as np
 import pytest
 
@@ -8,7 +8,7 @@ from pastix_b200 import matrices as M
 from pastix_b200 import native
 from pastix_b200.api import backward_error, forward_error
 from pastix_b200.refhost import Analysis
-from pastix_b200.serving import SolveServer, fifo_latencies
+from pastix_b200.serving import SolveServer
 
 pytestmark = pytest.mark.gpu
 
@@ -46,60 +46,6 @@ def test_full_size_convection_diffusion_lu():
     assert backward_error(A, xd, b).max() <= BERR_TARGET
     assert agree <= 1e-9
     assert fe.max() <= 1e-9
-
-
-def test_serving_resident_factor_100cube():
-    """The serving workload at full size: 7-point Laplacian on 100^3 (n = 1e6)
-    resident, requests with nrhs log-uniform in [1, 256] and x_true uniform[-1, 1]
-    solved and refined to <= 1e-12, a same-pattern refactorization every 50 requests
-    with the matrix scaled D A D by d_i uniform in [0.9, 1.1] (a symmetric
-    diagonal scaling keeps it SPD); mixed (3xTF32) and FP64 factors.  Service
-    times are measured; latencies under Poisson arrivals at 70 % of the measured
-    capacity follow from a FIFO queue of those service times."""
-    import torch
-    A = M.laplacian(100, 100, 100, 7, 6.0)
-    an = Analysis(A, "potrf")
-    rng = np.random.default_rng(5)
-    nreq = 100
-    nrhs = np.floor(np.exp(rng.uniform(0.0, np.log(257.0), nreq))).astype(int).clip(1, 256)
-    col = np.repeat(np.arange(A.n), np.diff(A.colptr))
-    scaled = []
-    for r in range(nreq // 50):
-        d = rng.uniform(0.9, 1.1, A.n)
-        scaled.append(A.values * d[A.rowind] * d[col] if r else A.values)
-    report = {}
-    for prec in ("tf32x3", "fp64"):
-        srv = SolveServer(an, prec, "cg", BERR_TARGET, max_nrhs=256)
-        refs = [srv.refactor(scaled[0])]
-        srv.warm_up()
-        g = torch.Generator(device="cuda").manual_seed(1234)
-        service, iters = [], []
-        for i in range(nreq):
-            if i and i % 50 == 0:
-                refs.append(srv.refactor(scaled[i // 50]))
-            xt = torch.rand((int(nrhs[i]), A.n), generator=g, dtype=torch.float64, device="cuda") * 2 - 1
-            b = srv.matvec(xt)
-            x, info = srv.solve(b)
-            assert info["berr"].max() <= BERR_TARGET, (prec, i, info)
-            r = b - srv.matvec(x)
-            be = (torch.linalg.vector_norm(r, dim=1) / torch.linalg.vector_norm(b, dim=1)).max().item()
-            assert be <= 1.01 * BERR_TARGET, (prec, i, be)
-            service.append(info["ms"])
-            iters.append(info["iters"])
-        srv.close()
-        torch.cuda.empty_cache()
-        service = np.array(service) / 1e3
-        cap = nreq / service.sum()
-        arrivals = np.cumsum(np.random.default_rng(9).exponential(1.0 / (0.7 * cap), nreq))
-        lat = fifo_latencies(arrivals, service) * 1e3
-        report[prec] = dict(
-            numfact_ms=[round(x["numfact_ms"], 1) for x in refs], refactor_ms=[round(x["ms"], 1) for x in refs],
-            solves_per_s=round(cap, 2), rhs_per_s=round(nrhs.sum() / service.sum(), 1),
-            service_p50_ms=round(float(np.percentile(service * 1e3, 50)), 2),
-            service_p99_ms=round(float(np.percentile(service * 1e3, 99)), 2),
-            latency_p50_ms=round(float(np.percentile(lat, 50)), 2), latency_p99_ms=round(float(np.percentile(lat, 99)), 2),
-            iters_mean=round(float(np.mean(iters)), 2))
-    print(f"\nserving 100^3, {nreq} requests, nrhs total {nrhs.sum()}: {report}")
 
 
 def test_continuous_batching_same_alone_and_in_the_mix():
