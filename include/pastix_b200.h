@@ -65,6 +65,33 @@ typedef struct b200_symbol_s {
 
 typedef struct b200_solver_s b200_solver_t;
 
+/* Kernel choices of one solver instance, as an autotuner picks them (no
+ * counterpart in PaStiX, whose GEMM kernels take fixed blockings,
+ * kernels/gpus/kepler/gemm_config/dgemm_param_nt.h:35,64, with per-kernel cost models
+ * in common/models.c).  update[w][h] selects the kernel of the GEMM-scatter updates
+ * of an FP32 factor (precisions FP32, TF32, TF32X3) whose width K (the source cblk's
+ * columns) falls in width class w and whose height M (rows of the source panel from
+ * the facing block down) in height class h:
+ *   width classes  K: [1,16) [16,32) [32,48) [48,64) [64,128) [128,inf)
+ *   height classes M: [1,64) [64,128) [128,256) [256,512) [512,inf)
+ * B200_UPD_DEFAULT keeps the built-in rule (tensor cores for K >= 32 and M >= 64,
+ * 128-column tiles for updates wider than 64 columns), B200_UPD_SIMT the CUDA-core
+ * kernels, B200_UPD_TC the tensor cores with the built-in tile width, B200_UPD_TC64
+ * the tensor cores with 64-column tiles.  Updates the tensor-core kernel does not
+ * handle (LDL^T's D-scaled operands, K not a multiple of 32 past the first K chunk)
+ * stay on the CUDA cores whatever the table says.  flow_min: the solve sweeps take
+ * one dataflow launch for the levels from the first one with fewer than flow_min
+ * cblks (0: the default, 8).  panel_tiles: 1 forces the 64 x 64 tile-item form of
+ * the wide-cblk panel launches. */
+#define B200_TUNE_WCLASSES 6
+#define B200_TUNE_HCLASSES 5
+enum { B200_UPD_DEFAULT = 0, B200_UPD_SIMT = 1, B200_UPD_TC = 2, B200_UPD_TC64 = 3 };
+typedef struct b200_tuning_s {
+    int32_t update[B200_TUNE_WCLASSES][B200_TUNE_HCLASSES];
+    int32_t flow_min;
+    int32_t panel_tiles;
+} b200_tuning_t;
+
 /* Upload the structure and build the device-side schedules.  Replaces the
  * structure walk PaStiX does in coeftabInit / solverBackupInit
  * (sopalin/coeftab.c:70-140, blend/solver_backup.c:60-100) and selects the
@@ -83,6 +110,11 @@ int b200_solver_destroy( b200_solver_t *solver );
  * b200_refine* refuse such an instance (PASTIX_ERR_BADPARAMETER). */
 int b200_solver_create_schur( const b200_symbol_t *symbol, int facto, int precision, void *stream,
                               int64_t cblkschur, b200_solver_t **solver );
+
+/* b200_solver_create_schur with a tuning table (NULL: the defaults); cblkschur =
+ * symbol->cblknbr for no Schur complement. */
+int b200_solver_create_tuned( const b200_symbol_t *symbol, int facto, int precision, void *stream,
+                              int64_t cblkschur, const b200_tuning_t *tuning, b200_solver_t **solver );
 
 /* Load the permuted blocked CSC (bcsc/bcsc.h:28-53; pastix_subtask_spm2bcsc,
  * sopalin/pastix_task_sopalin.c:82).  colptr has n+1 entries in the permuted

@@ -230,16 +230,20 @@ class BatchSolver:
     them, PaStiX's analyses reused), where the threshold sqrt(eps_64) ||A_i||_F
     replaces far fewer pivots: a system goes to FP64 when its FP32 factor replaced
     more than ``fp64_pivot_frac`` of its pivots, or when its refinement with the FP32
-    factor misses the target.  The reference factors each system separately
+    factor misses the target within ``fp32_restarts`` GMRES restarts (or as many
+    iterations of the other methods, gmres_im each): the forest's refinement sweeps
+    every system each iteration, so a few slow systems would otherwise hold the whole
+    batch for the full iteration budget.  The reference factors each system separately
     (pastix_task_numfact / _solve / _refine per instance,
     sopalin/pastix_task_sopalin.c:563, refinement/pastix_task_refine.c:226)."""
 
     def __init__(self, ba: BatchAnalysis, precision: str = "fp32", fp64_pivot_frac: float = 0.1,
-                 stream=None):
+                 fp32_restarts: int = 2, stream=None):
         from . import native
         self.ba = ba
         self.precision = precision
         self.frac = float(fp64_pivot_frac)
+        self.restarts = int(fp32_restarts)
         self.stream = stream
         self.s = native.Solver(ba.structure(), ba.facto_name, precision, stream=stream)
         self.s.batch_set(ba.sys_cblk)
@@ -296,7 +300,8 @@ class BatchSolver:
         bf = b.copy(order="F")
         bf[rows] = 0.0
         x = self.s.solve(bf)
-        x, it, _ = self.s.refine(bf, x, method, eps, itermax, gmres_im)
+        it_fp32 = itermax if self.precision == "fp64" else min(itermax, self.restarts * gmres_im)
+        x, it, _ = self.s.refine(bf, x, method, eps, it_fp32, gmres_im)
         berr = self.s.batch_berr(nrhs)
         late = (berr.max(axis=1) > eps) & ~fp64
         fp64 |= late

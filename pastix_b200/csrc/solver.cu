@@ -156,7 +156,7 @@ struct b200_solver_s {
     // FP32 updates on the tensor cores (precision TF32 / TF32X3); updates below the
     // size thresholds stay on the SIMT kernel
     bool use_tc = false;
-    int tc_min_k = 32, tc_min_m = 64;
+    b200_tuning_t tuning{};             // kernel choices (b200_solver_create_tuned)
     Upd *d_tcupd = nullptr;
     std::vector<int> lvl_tc_u0, lvl_tc_u1, lvl_tc_tiles, lvl_tc_m0, lvl_tc_wtiles, lvl_tc_mw0;
     int2 *d_tcmapw = nullptr;             // 128-column tiles
@@ -298,9 +298,19 @@ int build_schedule(b200_solver_t *s) {
     s->lvl_tc_m0.assign(nlev, 0);
     s->lvl_tc_mw0.assign(nlev, 0);
     s->lvl_tc_wtiles.assign(nlev, 0);
-    auto tc_ok = [&](const Upd &u) {
-        return s->use_tc && !(u.flags & UPD_SCALE_D) && u.K >= s->tc_min_k && u.M >= s->tc_min_m &&
-               (u.colK0 == 0 || u.K % 32 == 0);
+    // kernel of an FP32 update by the tuning table: 0 CUDA cores, 64 or 128 the
+    // tensor cores with tiles of that many columns
+    auto tc_choice = [&](const Upd &u) -> int {
+        if (!s->use_tc || (u.flags & UPD_SCALE_D) || !(u.colK0 == 0 || u.K % 32 == 0)) return 0;
+        const int w = u.K < 16 ? 0 : u.K < 32 ? 1 : u.K < 48 ? 2 : u.K < 64 ? 3 : u.K < 128 ? 4 : 5;
+        const int h = u.M < 64 ? 0 : u.M < 128 ? 1 : u.M < 256 ? 2 : u.M < 512 ? 3 : 4;
+        const int wide = u.N > 64 ? 128 : 64;
+        switch (s->tuning.update[w][h]) {
+            case B200_UPD_SIMT: return 0;
+            case B200_UPD_TC: return wide;
+            case B200_UPD_TC64: return 64;
+            default: return (u.K >= 32 && u.M >= 64) ? wide : 0;
+        }
     };
     // tensor-core tiles: 128 x 64
     // useful flops of an update: the lower triangle of the diagonal square when symmetric
@@ -312,9 +322,8 @@ int build_schedule(b200_solver_t *s) {
     // base: first update of the launch the update belongs to (map entries are relative)
     // updates more than 64 columns wide take 128-column tiles (half the operand
     // traffic per flop of the 64-column tiles)
-    auto push_tc = [&](Upd u, int &t0, int &t0w, int base) {
+    auto push_tc = [&](Upd u, int bn, int &t0, int &t0w, int base) {
         s->flops_kind[6] += upd_flops(u);
-        const int bn = u.N > 64 ? 128 : 64;
         u.tiles_m = (u.M + 127) / 128;
         u.tiles_n = (u.N + bn - 1) / bn;
         const int ui = (int)tcupds.size() - base;
@@ -504,8 +513,8 @@ int build_schedule(b200_solver_t *s) {
                                                           : (double)u.M * u.N;
                     flops += (int64_t)(2.0 * mn * u.K);
                     s->flops_class[3] += 2.0 * mn * u.K;
-                    if (tc_ok(u)) {
-                        push_tc(u, tc_tile0, tc_tilew, s->lvl_tc_u0[l]);
+                    if (const int bn = tc_choice(u)) {
+                        push_tc(u, bn, tc_tile0, tc_tilew, s->lvl_tc_u0[l]);
                         ext_wanted[k] = 1;
                         continue;
                     }
@@ -576,8 +585,9 @@ int build_schedule(b200_solver_t *s) {
             }
         };
         std::vector<std::vector<FlowItem>> lvl_bwd(nlev);
-        // first level with fewer than flow_min cblks (environment B200_FLOW_MIN)
-        int flow_min = 8;
+        // first level with fewer than flow_min cblks (tuning table; environment
+        // B200_FLOW_MIN overrides it, for tests of both sweep forms)
+        int flow_min = s->tuning.flow_min > 0 ? s->tuning.flow_min : 8;
         if (const char *e = getenv("B200_FLOW_MIN")) flow_min = atoi(e);
         s->flow_level = nlev;
         for (int l = 0; l < nlev; l++)
@@ -1459,6 +1469,15 @@ int b200_solver_create(const b200_symbol_t *sym, int facto, int precision, void 
 
 int b200_solver_create_schur(const b200_symbol_t *sym, int facto, int precision, void *stream, int64_t cblkschur,
                              b200_solver_t **out) {
+    return b200_solver_create_tuned(sym, facto, precision, stream, cblkschur, nullptr, out);
+}
+
+int b200_solver_create_tuned(const b200_symbol_t *sym, int facto, int precision, void *stream, int64_t cblkschur,
+                             const b200_tuning_t *tuning, b200_solver_t **out) {
+    if (tuning)
+        for (int w = 0; w < B200_TUNE_WCLASSES; w++)
+            for (int h = 0; h < B200_TUNE_HCLASSES; h++)
+                if (tuning->update[w][h] < 0 || tuning->update[w][h] > B200_UPD_TC64) return ERR_BADPARAM;
     if (!sym || !out || facto < 0 || facto > 2 || precision < 0 || precision > 3) return ERR_BADPARAM;
     if (sym->n <= 0 || sym->cblknbr <= 0 || sym->n >= (1LL << 31) || sym->bloknbr >= (1LL << 31)) return ERR_BADPARAM;
     if (cblkschur < 1 || cblkschur > sym->cblknbr) return ERR_BADPARAM;
@@ -1471,8 +1490,8 @@ int b200_solver_create_schur(const b200_symbol_t *sym, int facto, int precision,
     s->f32 = precision != B200_PREC_FP64;
     s->esz = s->f32 ? 4 : 8;
     s->use_tc = precision == B200_PREC_TF32 || precision == B200_PREC_TF32X3;
-    if (const char *e = getenv("B200_TC_MIN_K")) s->tc_min_k = std::max(1, atoi(e));
-    if (const char *e = getenv("B200_TC_MIN_M")) s->tc_min_m = std::max(1, atoi(e));
+    if (tuning) s->tuning = *tuning;
+    s->panel_steps_only = s->tuning.panel_tiles != 0;
     if (const char *e = getenv("B200_PANEL_TILES")) s->panel_steps_only = atoi(e) != 0;
     if (const char *e = getenv("B200_TEST_WITHHOLD"))
         s->test_withhold = !strcmp(e, "panel") ? 1 : !strcmp(e, "flow") ? 2 : 0;

@@ -23,7 +23,8 @@ _I64 = C.c_int64
 _lib = None
 
 # exported symbols, in the order of include/pastix_b200.h
-SYMBOLS = ["b200_solver_create", "b200_solver_destroy", "b200_solver_create_schur", "b200_bcsc_load",
+SYMBOLS = ["b200_solver_create", "b200_solver_destroy", "b200_solver_create_schur", "b200_solver_create_tuned",
+           "b200_bcsc_load",
            "b200_bcsc_values", "b200_get_schur", "b200_applyorder", "b200_trsm", "b200_get_diag", "b200_batch_set",
            "b200_batch_thresholds", "b200_batch_pivots", "b200_batch_berr", "b200_spm_map", "b200_spm_values",
            "b200_spm_values_device", "b200_numfact", "b200_numfact_trace", "b200_solve", "b200_solve_trace",
@@ -38,6 +39,30 @@ class Symbol(C.Structure):
         (f, _P) for f in ("cblk_fcolnum", "cblk_lcolnum", "cblk_fblok", "cblk_stride", "cblk_lcolidx",
                           "cblk_brownum", "blok_frownum", "blok_lrownum", "blok_lcblknm", "blok_fcblknm",
                           "browtab", "peritab")]
+
+
+WCLASSES, HCLASSES = 6, 5
+UPD = {"default": 0, "simt": 1, "tc": 2, "tc64": 3}
+
+
+class Tuning(C.Structure):
+    """b200_tuning_t: kernel choice per (update width class, height class)."""
+    _fields_ = [("update", (C.c_int32 * HCLASSES) * WCLASSES), ("flow_min", C.c_int32), ("panel_tiles", C.c_int32)]
+
+
+def tuning_table(default: int = 0) -> dict:
+    """A tuning table as a dict (every class set to ``default``)."""
+    return {"update": [[int(default)] * HCLASSES for _ in range(WCLASSES)], "flow_min": 0, "panel_tiles": 0}
+
+
+def _tuning_struct(t: dict) -> Tuning:
+    out = Tuning()
+    for w in range(WCLASSES):
+        for h in range(HCLASSES):
+            out.update[w][h] = int(t["update"][w][h])
+    out.flow_min = int(t.get("flow_min", 0))
+    out.panel_tiles = int(t.get("panel_tiles", 0))
+    return out
 
 
 class B200Error(RuntimeError):
@@ -62,6 +87,7 @@ def lib():
         L.b200_bcsc_values.argtypes = [_P, _P, _P, C.c_double]
         L.b200_spm_map.argtypes = [_P, _I64, _P, _P]
         L.b200_solver_create_schur.argtypes = [_P, C.c_int, C.c_int, _P, _I64, _P]
+        L.b200_solver_create_tuned.argtypes = [_P, C.c_int, C.c_int, _P, _I64, _P, _P]
         L.b200_get_schur.argtypes = [_P, _P, _I64]
         L.b200_applyorder.argtypes = [_P, C.c_int, _I64, _P, _I64]
         L.b200_trsm.argtypes = [_P, C.c_int, _I64, _P, _I64]
@@ -103,7 +129,9 @@ class Solver:
     """One factorization instance on the GPU (the B200 counterpart of a
     pastix_data_t after analysis)."""
 
-    def __init__(self, st, facto="potrf", precision="fp64", stream=None):
+    def __init__(self, st, facto="potrf", precision="fp64", stream=None, tuning: dict | None = None):
+        """tuning: a tuning table (``tuning_table`` / ``pastix_b200.tuner``), None for
+        the built-in kernel choices."""
         self.st = st
         self.facto = FACTO[facto] if isinstance(facto, str) else int(facto)
         self.precision = PREC[precision] if isinstance(precision, str) else int(precision)
@@ -116,13 +144,15 @@ class Solver:
         h = _P()
         cs = int(getattr(st, "cblkschur", -1))
         self.nschur = 0
+        self.tuning = tuning
         if 0 <= cs < st.cblknbr:
             self.nschur = int(st.n - st.cblk_fcolnum[cs])
-            check(lib().b200_solver_create_schur(C.byref(sym), self.facto, self.precision, stream, cs, C.byref(h)),
-                  "b200_solver_create_schur")
         else:
-            check(lib().b200_solver_create(C.byref(sym), self.facto, self.precision, stream, C.byref(h)),
-                  "b200_solver_create")
+            cs = st.cblknbr
+        tu = _tuning_struct(tuning) if tuning is not None else None
+        check(lib().b200_solver_create_tuned(C.byref(sym), self.facto, self.precision, stream, cs,
+                                             C.byref(tu) if tu is not None else None, C.byref(h)),
+              "b200_solver_create_tuned")
         self.h = h
 
     def close(self):

@@ -37,11 +37,11 @@ def factor_rel_diff(st, facto, bc, thr, s):
     return d
 
 
-def run_case(A, facto, prec, method, nrhs=3):
+def run_case(A, facto, prec, method, nrhs=3, tuning=None):
     an = Analysis(A, facto)
     st = an.structure()
     bc = an.bcsc()
-    s = native.Solver(st, facto, prec)
+    s = native.Solver(st, facto, prec, tuning=tuning)
     s.bcsc_load(bc)
     s.numfact_trace(0.0)
     cls, _ = s.trace_launches()
@@ -88,10 +88,12 @@ def test_tf32_updates_refine_to_fp64_accuracy(facto, make, method):
     ("getrf", lambda: M.convection_diffusion(9, 7, 5, seed=2), "gmres"),
     ("potrf", lambda: M.laplacian(13, 11, 3, 7, 6.0), "sr"),
 ])
-def test_every_update_on_tensor_cores(monkeypatch, facto, make, method):
-    monkeypatch.setenv("B200_TC_MIN_K", "1")
-    monkeypatch.setenv("B200_TC_MIN_M", "1")
-    d, be, fe, n_tc = run_case(make(), facto, "tf32x3", method)
+def test_every_update_on_tensor_cores(facto, make, method):
+    """A tuning table that sends every update class to the tensor cores: tiny and
+    ragged tiles, 64-column tiles for narrow classes, atomics."""
+    tuning = native.tuning_table(default=native.UPD["tc"])
+    tuning["update"][0][0] = native.UPD["tc64"]
+    d, be, fe, n_tc = run_case(make(), facto, "tf32x3", method, tuning=tuning)
     assert n_tc > 0
     assert d <= 2e-5, d
     assert be <= BERR_TARGET
