@@ -50,6 +50,12 @@ def parse():
                     help="precision of the mixed path (fp32, tf32, tf32x3; auto = tf32x3: FP32 factor with 3xTF32 "
                          "tensor-core updates)")
     ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--no-tune", action="store_true", help="built-in kernel choices instead of the autotuned table")
+    ap.add_argument("--tune-budget", type=float, default=150.0,
+                    help="seconds the autotuner may spend on a structure not in its cache")
+    ap.add_argument("--no-serving", action="store_true", help="skip the measured serving section (100^3)")
+    ap.add_argument("--serving-requests", type=int, default=60)
+    ap.add_argument("--serving-rate", type=float, default=12.0, help="requests per second (Poisson)")
     ap.add_argument("--numfact-once", default=None, metavar="PREC",
                     help="profiling aid: one factorization of the workload in precision PREC (fp64, fp32, tf32, "
                          "tf32x3) through the library, then exit")
@@ -256,6 +262,24 @@ def solve_latency(solver, A, b, stream, device_b, device_x, nrhs, reps=50):
     return float(np.percentile(ts, 50)), float(np.percentile(ts, 99))
 
 
+def serving_section(args, paths):
+    """The serving workload measured in real time (``serving.serving_workload``): a
+    7-point Laplacian on 100^3 (n = 1e6) resident, Poisson arrivals at the stated
+    rate, nrhs log-uniform in [1, 256], a D A D refactorization after 50 requests,
+    two lanes and a standby factor; per path p50/p99 latency and throughput."""
+    from pastix_b200 import matrices as M
+    from pastix_b200.refhost import Analysis
+    from pastix_b200.serving import serving_workload
+    A = M.laplacian(100, 100, 100, 7, 6.0)
+    an = Analysis(A, "potrf")
+    out = {"workload": "7-point 3D Laplacian 100^3 (n=1000000), POTRF, requests nrhs log-uniform [1,256], "
+                       f"Poisson {args.serving_rate:g}/s, D A D refactorization every 50 requests, CG to 1e-12",
+           "paths": {}}
+    for prec in paths:
+        out["paths"][prec] = serving_workload(an, A, prec, nreq=args.serving_requests, rate=args.serving_rate)
+    return out
+
+
 def max_over_ranks(vals, dist, device):
     """Each entry's largest value over the ranks (every rank calls it once, at the same
     point); the values themselves without a process group."""
@@ -408,8 +432,19 @@ def main():
     traces = {}
     solvers = {}
     kinds_trace, kinds_launches = {}, {}
+    tunings = {}
     for prec, refine in (("fp64", False), (mixed_prec, True)):
-        s = native.Solver(st, "potrf", prec, stream=stream.cuda_stream)
+        tuning = None
+        if not args.no_tune:
+            # the autotuned kernel choices of this structure (cached by structure,
+            # precision and device; tuned within the budget when not cached)
+            from pastix_b200 import tuner
+            tuning, entry = tuner.load_or_tune(st, "potrf", prec, bc, budget_s=args.tune_budget)
+            tunings[prec] = {k: entry.get(k) for k in ("numfact_ms", "baseline_ms", "solve_ms", "baseline_solve_ms",
+                                                       "seconds")}
+            tunings[prec]["changes"] = [t["change"] for t in entry.get("trials", [])
+                                        if t["change"] != "baseline"]
+        s = native.Solver(st, "potrf", prec, stream=stream.cuda_stream, tuning=tuning)
         s.bcsc_load(bc)
         solvers[prec] = (s, refine)
         traces[prec] = s.numfact_trace(0.0)
@@ -437,6 +472,14 @@ def main():
     hs, _ = solvers[head["prec"]]
     p50, p99 = solve_latency(hs, A, b, stream, device_b, device_x, nrhs)
     e2e_s, h2d, d2h, e2e_phases = e2e_path(hs, an, A, b, head["prec"], head["prec"] != "fp64", nrhs, reps=5)
+    # the same end-to-end step on the other path, for the wall-time comparison
+    e2e_other = {}
+    for prec, (s_, refine_) in solvers.items():
+        if prec == head["prec"]:
+            continue
+        es, hb, db, ph = e2e_path(s_, an, A, b, prec, refine_, nrhs, reps=5)
+        e2e_other[prec] = {"seconds_per_step": es, "value": world * st.thflops / es / 1e9,
+                           "h2d_bytes_per_step": hb, "d2h_bytes_per_step": db, "phases_ms": ph}
     # a replica job is as slow as its slowest rank
     step_ms, e2e_s = max_over_ranks([head["step_ms"], e2e_s], dist, "cuda")
     value = world * st.thflops / (step_ms * 1e-3) / 1e9
@@ -485,6 +528,16 @@ def main():
     except Exception as exc:  # an auxiliary figure: the line stands without it
         solve_roofline = {"unavailable": str(exc)}
 
+    serving = None
+    if not args.no_serving and rank == 0:
+        for s_, _r in solvers.values():
+            s_.close()
+        solvers = {}
+        torch.cuda.empty_cache()
+        try:
+            serving = serving_section(args, (mixed_prec, "fp64"))
+        except Exception as exc:  # an auxiliary section: the line stands without it
+            serving = {"unavailable": f"{type(exc).__name__}: {exc}"}
     if rank == 0:
         line = {
             "metric": METRIC, "value": value, "unit": "GFLOP/s", "n_gpus": world, "steps": args.steps,
@@ -507,6 +560,9 @@ def main():
             "e2e": {"value": e2e_value, "unit": "GFLOP/s", "h2d_bytes_per_step": h2d, "d2h_bytes_per_step": d2h,
                     "seconds_per_step": e2e_s, "host_buffers": "pinned", "phases_ms": e2e_phases,
                     "step": "b200_spm_values (bcsc built on the GPU) + b200_numfact + host copy x=b + b200_solve + b200_refine"},
+            "e2e_paths": e2e_other,
+            "tuning": tunings,
+            "serving": serving,
             "gpu_launches": int(sum(r["launches"] for r in results.values())),
             "clocks": clocks,
             "wall_s_timed_region": wall,

@@ -607,3 +607,75 @@ class GpuServingBackend:
             if s is not None:
                 s.close()
         self.solvers = [None] * self.slots
+
+
+def serving_workload(an, A, precision: str, nreq: int = 100, rate: float = 12.0, refactor_every: int = 50,
+                     method: str = "cg", eps: float = 1e-12, lanes: int = 2, max_cols: int = 256, seed: int = 5,
+                     check=None) -> dict:
+    """The serving workload on one resident factor, measured in real time: nreq
+    requests with nrhs log-uniform in [1, 256] (right-hand sides taken from a pool of
+    256 columns b = A x_true, x_true uniform[-1, 1]) submitted at Poisson times of
+    the given rate (requests/s) from a producer thread, and a same-pattern
+    refactorization after every ``refactor_every`` requests with the matrix scaled
+    D A D, d_i uniform in [0.9, 1.1].  ``check(values, x, b)`` may verify a result
+    against the matrix values of its epoch.  Returns the measured figures."""
+    import torch
+    rng = np.random.default_rng(seed)
+    nrhs = np.floor(np.exp(rng.uniform(0.0, np.log(257.0), nreq))).astype(int).clip(1, 256)
+    col = np.repeat(np.arange(A.n), np.diff(A.colptr))
+    vals = [A.values]
+    for _ in range(1, (nreq - 1) // refactor_every + 1):
+        d = rng.uniform(0.9, 1.1, A.n)
+        vals.append(A.values * d[A.rowind] * d[col])
+    offs = poisson_offsets(nreq + len(vals) - 1, rate, seed=seed + 4)
+    be = GpuServingBackend(an, precision, method, eps, lanes=lanes, max_cols=max_cols)
+    try:
+        g = torch.Generator(device="cuda").manual_seed(seed + 1229)
+        xt = torch.rand((256, A.n), generator=g, dtype=torch.float64, device="cuda") * 2 - 1
+        pool = be.matvec(0, xt)
+        del xt
+        trace, owner, pos = [], [], 0
+        for i in range(nreq):
+            if i and i % refactor_every == 0:
+                trace.append((float(offs[pos]), Refactor(vals[i // refactor_every])))
+                owner.append(None)
+                pos += 1
+            c0 = int(rng.integers(0, 257 - nrhs[i]))
+            trace.append((float(offs[pos]), pool[c0:c0 + nrhs[i]]))
+            owner.append(i)
+            pos += 1
+        loop = ServingLoop(be)
+        th = replay(loop, trace)
+        th.join()
+        res = loop.drain(900)
+        loop.close()
+        reqs = [res[j] for j, o in enumerate(owner) if o is not None]
+        refs = [res[j] for j, o in enumerate(owner) if o is None]
+        checked = 0
+        if check is not None:
+            for j, o in enumerate(owner):
+                if o is not None and o % 17 == 0:
+                    check(vals[res[j]["epoch"]], res[j]["x"], trace[j][1])
+                    checked += 1
+        lat = np.array([r["latency"] for r in reqs]) * 1e3
+        span = max(r["done"] for r in reqs) - min(r["arrival"] for r in reqs)
+        svc = np.array([b["service"] for b in loop.batches]) * 1e3
+        overlapped = [rf["start"] < max(q["done"] for q in reqs if q["epoch"] == rf["epoch"] - 1) for rf in refs]
+        out = dict(
+            precision=precision, requests=nreq, rate_per_s=rate, columns=int(nrhs.sum()), lanes=lanes,
+            batches=len(loop.batches), mean_batch_cols=round(float(np.mean([b["cols"] for b in loop.batches])), 1),
+            latency_p50_ms=round(float(np.percentile(lat, 50)), 1),
+            latency_p99_ms=round(float(np.percentile(lat, 99)), 1),
+            batch_service_p50_ms=round(float(np.percentile(svc, 50)), 1),
+            throughput_req_per_s=round(nreq / span, 2), rhs_per_s=round(float(nrhs.sum()) / span, 1),
+            berr_max=float(max(float(r["berr"].max()) for r in reqs)),
+            refactor_ms=[round(rf["refactor"]["ms"], 1) for rf in refs],
+            refactor_numfact_ms=[round(rf["refactor"]["numfact_ms"], 1) for rf in refs],
+            refactor_into_standby=[bool(rf["standby"]) for rf in refs],
+            refactor_overlapped_serving=overlapped, standby_instance=be.standby_created,
+            checked=checked)
+        del pool
+        return out
+    finally:
+        be.close()
+        torch.cuda.empty_cache()

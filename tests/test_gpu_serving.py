@@ -78,68 +78,25 @@ def _residuals(A_vals, A, x, b):
 def test_serving_100cube_measured_latency():
     """The serving workload at full size: 7-point Laplacian on 100^3 (n = 1e6)
     resident; 100 requests with nrhs log-uniform in [1, 256] submitted at Poisson
-    times of rate 20 requests/s from a producer thread; a same-pattern
+    times of rate 12 requests/s from a producer thread (about 70 % of the capacity
+    measured at 20 requests/s, where the queue grew); a same-pattern
     refactorization after every 50 requests with the matrix scaled D A D by d_i
-    uniform in [0.9, 1.1]; every request refined to <= 1e-12.  Mixed (FP32 factor,
-    3xTF32 updates) and FP64 factors, two lanes, standby factor.  Reports measured
-    p50 / p99 latency, throughput and the refactorizations' overlap with serving."""
-    import torch
+    uniform in [0.9, 1.1]; every request refined to <= 1e-12, and some checked
+    against their epoch's matrix on the host.  Mixed (FP32 factor, 3xTF32 updates)
+    and FP64 factors, two lanes, standby factor.  Reports measured p50 / p99
+    latency, throughput and the refactorizations' overlap with serving."""
+    from pastix_b200.serving import serving_workload
     A = M.laplacian(100, 100, 100, 7, 6.0)
     an = Analysis(A, "potrf")
-    rng = np.random.default_rng(5)
-    nreq, rate = 100, 20.0
-    nrhs = np.floor(np.exp(rng.uniform(0.0, np.log(257.0), nreq))).astype(int).clip(1, 256)
-    col = np.repeat(np.arange(A.n), np.diff(A.colptr))
-    vals = [A.values]
-    for r in range(1, nreq // 50):
-        d = rng.uniform(0.9, 1.1, A.n)
-        vals.append(A.values * d[A.rowind] * d[col])
-    offs = poisson_offsets(nreq + len(vals) - 1, rate, seed=9)
+
+    def check(vals, x, b):
+        assert _residuals(vals, A, x, b).max() <= 1.05 * BERR_TARGET
+
     report = {}
     for prec in ("tf32x3", "fp64"):
-        be = GpuServingBackend(an, prec, "cg", BERR_TARGET, lanes=2, max_cols=256)
-        pool = _rhs(be, 256, 1234)  # right-hand sides: request i takes columns of the pool
-        trace, owner, pos = [], [], 0
-        for i in range(nreq):
-            if i and i % 50 == 0:
-                trace.append((float(offs[pos]), Refactor(vals[i // 50])))
-                owner.append(None)
-                pos += 1
-            c0 = int(rng.integers(0, 257 - nrhs[i]))
-            trace.append((float(offs[pos]), pool[c0:c0 + nrhs[i]]))
-            owner.append((i, c0))
-            pos += 1
-        loop = ServingLoop(be)
-        th = replay(loop, trace)
-        th.join()
-        res = loop.drain(600)
-        loop.close()
-        reqs = [res[j] for j, o in enumerate(owner) if o is not None]
-        refs = [res[j] for j, o in enumerate(owner) if o is None]
-        lat = np.array([r["latency"] for r in reqs]) * 1e3
-        berr = max(float(r["berr"].max()) for r in reqs)
-        span = max(r["done"] for r in reqs) - min(r["arrival"] for r in reqs)
-        # independent host residuals of a few requests of each epoch, against that epoch's matrix
-        checked = 0
-        for j, o in enumerate(owner):
-            if o is None or o[0] % 17:
-                continue
-            r = res[j]
-            bres = _residuals(vals[r["epoch"]], A, r["x"], trace[j][1])
-            assert bres.max() <= 1.05 * BERR_TARGET, (prec, o, bres.max())
-            checked += 1
-        overlapped = [rf["start"] < max(q["done"] for q in reqs if q["epoch"] == rf["epoch"] - 1) for rf in refs]
-        report[prec] = dict(
-            requests=nreq, rate_per_s=rate, columns=int(nrhs.sum()), batches=len(loop.batches),
-            mean_batch_cols=round(float(np.mean([b["cols"] for b in loop.batches])), 1),
-            latency_p50_ms=round(float(np.percentile(lat, 50)), 1),
-            latency_p99_ms=round(float(np.percentile(lat, 99)), 1),
-            throughput_req_per_s=round(nreq / span, 2), rhs_per_s=round(nrhs.sum() / span, 1),
-            berr_max=berr, refactor_ms=[round(rf["refactor"]["ms"], 1) for rf in refs],
-            refactor_standby=[bool(rf["standby"]) for rf in refs], refactor_overlapped_serving=overlapped,
-            standby_instance=be.standby_created, host_checked=checked)
-        assert berr <= BERR_TARGET
-        be.close()
-        del pool
-        torch.cuda.empty_cache()
+        r = serving_workload(an, A, prec, nreq=100, rate=12.0, check=check)
+        report[prec] = r
+        assert r["berr_max"] <= BERR_TARGET
+        assert r["checked"] >= 5
+        assert r["standby_instance"] and all(r["refactor_into_standby"])
     print(f"\nserving 100^3 (measured): {report}")
