@@ -75,6 +75,7 @@ struct Upd {
     int tiles_m, tiles_n;
     int tile0;    // first tile index of this update inside its launch
     int flags;
+    int nb;       // tensor-core updates: columns per tile (a multiple of 32, at most the launch's tile width)
 };
 
 // Off-diagonal row tile of a cblk panel (TRSM and solve tasks).

@@ -322,14 +322,19 @@ int build_schedule(b200_solver_t *s) {
     // base: first update of the launch the update belongs to (map entries are relative)
     // updates more than 64 columns wide take 128-column tiles (half the operand
     // traffic per flop of the 64-column tiles)
+    // the launch's tile width bn (64 or 128) bounds the columns of a tile; within it
+    // each update takes the narrowest multiple of 32 that keeps its tile count, so the
+    // column tiles split N evenly (N = 278: 3 tiles of 96, not 3 of 128)
     auto push_tc = [&](Upd u, int bn, int &t0, int &t0w, int base) {
         s->flops_kind[6] += upd_flops(u);
+        const int ntn = (u.N + bn - 1) / bn;
+        u.nb = std::min(bn, ((u.N + ntn - 1) / ntn + 31) / 32 * 32);
         u.tiles_m = (u.M + 127) / 128;
-        u.tiles_n = (u.N + bn - 1) / bn;
+        u.tiles_n = (u.N + u.nb - 1) / u.nb;
         const int ui = (int)tcupds.size() - base;
         for (int nt = 0; nt < u.tiles_n; nt++)
             for (int mt = 0; mt < u.tiles_m; mt++) {
-                if ((u.flags & UPD_SYM) && mt * 128 + 127 < nt * bn) continue;  // above the diagonal
+                if ((u.flags & UPD_SYM) && mt * 128 + 127 < nt * u.nb) continue;  // above the diagonal
                 (bn == 128 ? tcmapw : tcmap).push_back(make_int2(ui, mt | (nt << 16)));
                 (bn == 128 ? t0w : t0)++;
             }

@@ -13,16 +13,19 @@
 // bits cleared (exact in TF32) and lo = x - hi (exact); D += hi_A hi_B + hi_A lo_B +
 // lo_A hi_B keeps close to FP32 accuracy.  TF32 keeps x once and D += A B.
 //
-// update_tc_kernel is persistent (one CTA per SM, tiles of 128 rows x BN = 64 or
-// 128 columns striding over the launch's tile list) and warp-specialised:
+// update_tc_kernel is persistent (one CTA per SM, tiles of 128 rows x at most BN = 64
+// or 128 columns striding over the launch's tile list) and warp-specialised:
 //  * warp 0 (one lane): TMA producer.  One 2D tensor map per panel copy (K
-//    innermost, boxes of 32 K x 64 rows, 128-byte swizzle: exactly the canonical
-//    K-major UMMA layout), a ring of [A hi][B hi]([A lo][B lo]) stages in shared
-//    memory, K in chunks of 32.
+//    innermost, boxes of 32 K x 32 rows, 128-byte swizzle: stacked, exactly the
+//    canonical K-major UMMA layout), a ring of [A hi][B hi]([A lo][B lo]) stages in
+//    shared memory, K in chunks of 32.  A tile's B operand is its update's nb rows
+//    (nb = the narrowest multiple of 32 that keeps the update's column-tile count, so
+//    the tiles split N evenly); only those are loaded.
 //  * warp 1 (one lane): allocates 2 BN TMEM columns (two 128 x BN FP32
-//    accumulators) and issues tcgen05.mma (M = 128, N = BN, K = 8); each stage is
-//    released to the producer and each accumulator to the epilogue by
-//    tcgen05.commit on an mbarrier.
+//    accumulators) and issues tcgen05.mma (M = 128, N = nb, K = 8; the N field of the
+//    instruction descriptor is set per tile), skipping the K steps of a chunk's
+//    zero-filled tail; each stage is released to the producer and each accumulator
+//    to the epilogue by tcgen05.commit on an mbarrier.
 //  * warps 2-9: epilogue.  Thread = accumulator row (TMEM lane quarter = warp % 4),
 //    two warps per quarter with BN / 2 columns each; tcgen05.ld, release the
 //    accumulator, scatter-add into f with reductions (red.global.add), overlapping
@@ -52,10 +55,12 @@ struct TcCfg {
     static constexpr int NST = (192 * 1024) / STAGE;
     static constexpr int SMEM = NST * STAGE + 1024;  // + alignment slack
     static constexpr uint32_t TMEM_COLS = 2 * BN;    // two accumulators
-    // instruction descriptor: D F32, A/B TF32, both K-major, M = 128, N = BN
-    static constexpr uint32_t IDESC = (1u << 4) | (2u << 7) | (2u << 10) | ((uint32_t)(BN >> 3) << 17) |
-                                      ((uint32_t)(TC_BM >> 4) << 24);
 };
+
+// instruction descriptor: D F32, A/B TF32, both K-major, M = 128, N = n (a multiple of 16)
+__device__ __forceinline__ uint32_t tc_idesc(int n) {
+    return (1u << 4) | (2u << 7) | (2u << 10) | ((uint32_t)(n >> 3) << 17) | ((uint32_t)(TC_BM >> 4) << 24);
+}
 
 __device__ __forceinline__ uint32_t smem_addr(const void *p) {
     return static_cast<uint32_t>(__cvta_generic_to_shared(p));
@@ -117,13 +122,13 @@ __device__ __forceinline__ uint64_t umma_desc(uint32_t addr) {
     return d;
 }
 
-template <uint32_t IDESC>
-__device__ __forceinline__ void umma_tf32(uint32_t tmem, uint64_t da, uint64_t db, uint32_t accumulate) {
+__device__ __forceinline__ void umma_tf32(uint32_t tmem, uint64_t da, uint64_t db, uint32_t idesc,
+                                          uint32_t accumulate) {
     asm volatile(
         "{\n\t.reg .pred p;\n\t"
         "setp.ne.b32 p, %4, 0;\n\t"
         "tcgen05.mma.cta_group::1.kind::tf32 [%0], %1, %2, %3, {%5, %6, %7, %8}, p;\n\t}\n" ::"r"(tmem),
-        "l"(da), "l"(db), "r"(IDESC), "r"(accumulate), "r"(0), "r"(0), "r"(0), "r"(0)
+        "l"(da), "l"(db), "r"(idesc), "r"(accumulate), "r"(0), "r"(0), "r"(0), "r"(0)
         : "memory");
 }
 
@@ -271,8 +276,10 @@ __global__ void __launch_bounds__(TC_THREADS, 1) update_tc_kernel(DevSym s, cons
                 const int side_a = (u.flags & UPD_A_U) ? 1 : 0, side_b = (u.flags & UPD_B_U) ? 1 : 0;
                 const CUtensorMap *ma = maps + (size_t)(side_a * 2) * N + u.k;
                 const CUtensorMap *mb = maps + (size_t)(side_b * 2) * N + u.k;
-                const int ya = u.rowA0 + tt.mt * TC_BM, yb = u.rowB0 + tt.nt * TC_BN;
+                const int nb = u.nb;  // this update's tile width: nb / 32 boxes of B rows
+                const int ya = u.rowA0 + tt.mt * TC_BM, yb = u.rowB0 + tt.nt * nb;
                 const int nk = (u.K + TC_BK - 1) / TC_BK;
+                const uint32_t tx = (uint32_t)(TC_A_BYTES + nb * TC_BK * 4) * (SPLIT ? 2u : 1u);
                 for (int kc = 0; kc < nk; kc++, it++) {
                     const int st = it % NST;
                     if (it >= NST && !mbar_wait(smem_addr(&empty_bar[st]), ((it / NST) - 1) & 1, &abort_sh)) {
@@ -280,21 +287,19 @@ __global__ void __launch_bounds__(TC_THREADS, 1) update_tc_kernel(DevSym s, cons
                         break;
                     }
                     const uint32_t bar = smem_addr(&full_bar[st]);
-                    mbar_expect_tx(bar, Cfg::STAGE);
+                    mbar_expect_tx(bar, tx);
                     last_ph[st] = (it / NST) & 1;
                     const uint32_t base = smem_addr(smem + (size_t)st * Cfg::STAGE);
                     const int x = kc * TC_BK + u.colK0;
-                    tma_load_2d(base, ma, x, ya, bar);
-                    tma_load_2d(base + TC_A_BYTES / 2, ma, x, ya + 64, bar);
 #pragma unroll
-                    for (int g = 0; g < BN / 64; g++) tma_load_2d(base + TC_A_BYTES + g * 8192, mb, x, yb + 64 * g, bar);
+                    for (int g = 0; g < TC_BM / 32; g++) tma_load_2d(base + g * 4096, ma, x, ya + 32 * g, bar);
+                    for (int g = 0; g < nb / 32; g++) tma_load_2d(base + TC_A_BYTES + g * 4096, mb, x, yb + 32 * g, bar);
                     if (SPLIT) {
                         const uint32_t lb = base + TC_A_BYTES + TC_B_BYTES;
-                        tma_load_2d(lb, ma + N, x, ya, bar);
-                        tma_load_2d(lb + TC_A_BYTES / 2, ma + N, x, ya + 64, bar);
 #pragma unroll
-                        for (int g = 0; g < BN / 64; g++)
-                            tma_load_2d(lb + TC_A_BYTES + g * 8192, mb + N, x, yb + 64 * g, bar);
+                        for (int g = 0; g < TC_BM / 32; g++) tma_load_2d(lb + g * 4096, ma + N, x, ya + 32 * g, bar);
+                        for (int g = 0; g < nb / 32; g++)
+                            tma_load_2d(lb + TC_A_BYTES + g * 4096, mb + N, x, yb + 32 * g, bar);
                     }
                 }
             }
@@ -319,6 +324,7 @@ __global__ void __launch_bounds__(TC_THREADS, 1) update_tc_kernel(DevSym s, cons
                 asm volatile("tcgen05.fence::after_thread_sync;\n" ::: "memory");
                 const uint32_t acc = tmem + (uint32_t)(a * TC_BN);
                 const int nk = (tt.u.K + TC_BK - 1) / TC_BK;
+                const uint32_t idesc = tc_idesc(tt.u.nb);
                 for (int kc = 0; kc < nk; kc++, it++) {
                     const int st = it % NST;
                     if (!mbar_wait(smem_addr(&full_bar[st]), (it / NST) & 1, &abort_sh)) {
@@ -329,14 +335,18 @@ __global__ void __launch_bounds__(TC_THREADS, 1) update_tc_kernel(DevSym s, cons
                     const uint32_t base = smem_addr(smem + (size_t)st * Cfg::STAGE);
                     const uint32_t a_hi = base, b_hi = base + TC_A_BYTES;
                     const uint32_t a_lo = base + TC_A_BYTES + TC_B_BYTES, b_lo = a_lo + TC_A_BYTES;
+                    // K steps of 8 holding data: the chunk's zero-filled tail (K past the
+                    // cblk's columns, read as zeros by the TMA) contributes nothing
+                    const int k8n = min(TC_BK / 8, (tt.u.K - kc * TC_BK + 7) / 8);
 #pragma unroll
                     for (int k8 = 0; k8 < TC_BK / 8; k8++) {
+                        if (k8 >= k8n) break;
                         // K step: 8 values = 32 bytes into each row line
                         const uint64_t dah = umma_desc(a_hi + 32 * k8), dbh = umma_desc(b_hi + 32 * k8);
-                        umma_tf32<Cfg::IDESC>(acc, dah, dbh, (kc > 0 || k8 > 0) ? 1u : 0u);
+                        umma_tf32(acc, dah, dbh, idesc, (kc > 0 || k8 > 0) ? 1u : 0u);
                         if (SPLIT) {
-                            umma_tf32<Cfg::IDESC>(acc, dah, umma_desc(b_lo + 32 * k8), 1u);
-                            umma_tf32<Cfg::IDESC>(acc, umma_desc(a_lo + 32 * k8), dbh, 1u);
+                            umma_tf32(acc, dah, umma_desc(b_lo + 32 * k8), idesc, 1u);
+                            umma_tf32(acc, umma_desc(a_lo + 32 * k8), dbh, idesc, 1u);
                         }
                     }
                     umma_commit(smem_addr(&empty_bar[st]));
@@ -392,10 +402,12 @@ __global__ void __launch_bounds__(TC_THREADS, 1) update_tc_kernel(DevSym s, cons
                 // consecutive rows of a warp merge into one L2 transaction per column
                 float *C = ((u.flags & UPD_C_U) ? U : L) + s.off[u.f];
                 const size_t ldf = (size_t)s.ld[u.f];
-                const int cmax = min(TC_BN, u.N - tt.nt * TC_BN) - c0;
-                const int csym = (u.flags & UPD_SYM) ? lr - tt.nt * TC_BN - c0 : ECOLS - 1;  // last column kept
+                // columns of this warp's half inside the tile's nb (TMEM columns past nb
+                // hold another tile's values and are never stored)
+                const int cmax = min(u.nb, u.N - tt.nt * u.nb) - c0;
+                const int csym = (u.flags & UPD_SYM) ? lr - tt.nt * u.nb - c0 : ECOLS - 1;  // last column kept
                 const int cend = min(cmax, csym + 1);
-                float *p = C + d + (size_t)(u.colbase + tt.nt * TC_BN + c0) * ldf;
+                float *p = C + d + (size_t)(u.colbase + tt.nt * u.nb + c0) * ldf;
 #pragma unroll
                 for (int c = 0; c < ECOLS; c++)
                     if (c < cend) atomicAdd(p + (size_t)c * ldf, -__uint_as_float(v[c]));
@@ -447,7 +459,7 @@ int configure_tc_kernels() {
 }
 
 // One 2D tensor map per operand copy (FP32, K innermost: ncols x stride with row
-// pitch kp = ncols rounded up to 4), boxes of 32 K x 64 rows with 128-byte swizzle;
+// pitch kp = ncols rounded up to 4), boxes of 32 K x 32 rows with 128-byte swizzle;
 // elements past ncols or stride read as zero.
 typedef CUresult (*EncodeTiledFn)(CUtensorMap *, CUtensorMapDataType, cuuint32_t, void *, const cuuint64_t *,
                                   const cuuint64_t *, const cuuint32_t *, const cuuint32_t *, CUtensorMapInterleave,
@@ -472,7 +484,7 @@ int encode_operand_maps(const std::vector<int64_t> &toff, const std::vector<int>
         const int kp = (ncols[k] + 3) & ~3;
         cuuint64_t dims[2] = {(cuuint64_t)ncols[k], (cuuint64_t)stride[k]};
         cuuint64_t strides[1] = {(cuuint64_t)kp * sizeof(float)};
-        cuuint32_t box[2] = {32, 64};
+        cuuint32_t box[2] = {32, 32};
         cuuint32_t estr[2] = {1, 1};
         CUresult r = encode(&maps[k], CU_TENSOR_MAP_DATA_TYPE_FLOAT32, 2, arena + toff[k], dims, strides, box, estr,
                             CU_TENSOR_MAP_INTERLEAVE_NONE, CU_TENSOR_MAP_SWIZZLE_128B,

@@ -21,8 +21,10 @@ def test_tuned_table_is_faster_and_correct(tmp_path):
     print(f"\ntuner: baseline {entry['baseline_ms']:.3f} ms -> {entry['numfact_ms']:.3f} ms, solve "
           f"{entry['baseline_solve_ms']:.3f} -> {entry['solve_ms']:.3f} ms, {len(entry['trials'])} trials in "
           f"{entry['seconds']} s: {[t['change'] for t in entry['trials']]}")
+    # changes are kept only when faster by more than the 2 % noise margin
     assert entry["numfact_ms"] <= entry["baseline_ms"]
     assert entry["solve_ms"] <= entry["baseline_solve_ms"]
+    assert entry["baseline_solve_ms"] > 0.05  # the solve is timed on the stream it runs on
     s = native.Solver(st, "potrf", "tf32x3", tuning=table)
     s.bcsc_load(bc)
     s.numfact(0.0)
