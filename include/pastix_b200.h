@@ -296,6 +296,16 @@ int b200_refine( b200_solver_t *solver, int64_t nrhs, const double *b, int64_t l
                  int64_t ldx, int method, double eps, int64_t itermax, int64_t gmres_im,
                  int64_t *niter, double *berr );
 
+/* pastix_task_solve / pastix_task_refine with single-precision vectors, as PaStiX
+ * takes them for a float matrix (the call dispatches on the bcsc's flttype,
+ * sopalin/pastix_task_solve.c:550, refinement/pastix_task_refine.c:226): host
+ * arrays of float, widened to double on the GPU for the solve and the refinement,
+ * narrowed back into b (solve) or x (refinement). */
+int b200_solve_float( b200_solver_t *solver, int64_t nrhs, float *b, int64_t ldb );
+int b200_refine_float( b200_solver_t *solver, int64_t nrhs, const float *b, int64_t ldb, float *x,
+                       int64_t ldx, int method, double eps, int64_t itermax, int64_t gmres_im,
+                       int64_t *niter, double *berr );
+
 /* Same on device memory (b and x on the device). */
 int b200_refine_device( b200_solver_t *solver, int64_t nrhs, const double *d_b, int64_t ldb,
                         double *d_x, int64_t ldx, int method, double eps, int64_t itermax,

@@ -2184,6 +2184,63 @@ int b200_solve(b200_solver_t *s, int64_t nrhs, double *b, int64_t ldb) {
     return rc;
 }
 
+// Single-precision host vectors (a float matrix's b and x, as pastix_task_solve /
+// pastix_task_refine take them for PastixFloat, sopalin/pastix_task_solve.c:550):
+// uploaded as floats, widened to double on the device, solved or refined there in
+// double and narrowed back.
+int b200_solve_float(b200_solver_t *s, int64_t nrhs, float *b, int64_t ldb) {
+    if (s && s->cblkschur < s->cblknbr) return ERR_BADPARAM;
+    if (!s || !s->factored || nrhs < 0 || ldb < s->n || (!b && nrhs)) return ERR_BADPARAM;
+    if (nrhs == 0) return ERR_SUCCESS;
+    const int n = s->n;
+    const size_t blk = (size_t)n * nrhs;
+    RET(ensure_stage(s, blk + (blk + 1) / 2));
+    double *db = s->d_stage;
+    float *fb = reinterpret_cast<float *>(s->d_stage + blk);
+    int rc = ERR_SUCCESS;
+    if (cudaMemsetAsync(s->main.d_serr, 0, sizeof(int), s->st) != cudaSuccess) rc = ERR_INTERNAL;
+    if (!rc && cudaMemcpy2DAsync(fb, n * sizeof(float), b, ldb * sizeof(float), n * sizeof(float), nrhs,
+                                 cudaMemcpyHostToDevice, s->st) != cudaSuccess) rc = ERR_INTERNAL;
+    if (!rc) {
+        launch_convert<float, double>(n, (int)nrhs, fb, n, db, n, s->st);
+        rc = solve_device(s, &s->main, (int)nrhs, db, n, s->st);
+    }
+    if (!rc) launch_convert<double, float>(n, (int)nrhs, db, n, fb, n, s->st);
+    if (!rc && cudaMemcpy2DAsync(b, ldb * sizeof(float), fb, n * sizeof(float), n * sizeof(float), nrhs,
+                                 cudaMemcpyDeviceToHost, s->st) != cudaSuccess) rc = ERR_INTERNAL;
+    if (cudaStreamSynchronize(s->st) != cudaSuccess) rc = ERR_INTERNAL;
+    if (!rc) rc = sweep_status(&s->main);
+    s->kernel_launches += 2;
+    return rc;
+}
+
+int b200_refine_float(b200_solver_t *s, int64_t nrhs, const float *b, int64_t ldb, float *x, int64_t ldx, int method,
+                      double eps, int64_t itermax, int64_t gmres_im, int64_t *niter, double *berr) {
+    if (!s || !s->factored || nrhs < 0 || ldb < s->n || ldx < s->n) return ERR_BADPARAM;
+    if (nrhs == 0) return ERR_SUCCESS;
+    const int n = s->n;
+    const size_t blk = (size_t)n * nrhs;
+    RET(ensure_stage(s, 3 * blk));
+    double *db = s->d_stage, *dx = s->d_stage + blk;
+    float *fb = reinterpret_cast<float *>(s->d_stage + 2 * blk), *fx = fb + blk;
+    int rc = ERR_SUCCESS;
+    if (cudaMemcpy2DAsync(fb, n * sizeof(float), b, ldb * sizeof(float), n * sizeof(float), nrhs,
+                          cudaMemcpyHostToDevice, s->st) != cudaSuccess) rc = ERR_INTERNAL;
+    if (!rc && cudaMemcpy2DAsync(fx, n * sizeof(float), x, ldx * sizeof(float), n * sizeof(float), nrhs,
+                                 cudaMemcpyHostToDevice, s->st) != cudaSuccess) rc = ERR_INTERNAL;
+    if (!rc) {
+        launch_convert<float, double>(n, (int)nrhs, fb, n, db, n, s->st);
+        launch_convert<float, double>(n, (int)nrhs, fx, n, dx, n, s->st);
+        rc = b200_refine_device(s, nrhs, db, n, dx, n, method, eps, itermax, gmres_im, niter, berr, s->st);
+    }
+    if (!rc) launch_convert<double, float>(n, (int)nrhs, dx, n, fx, n, s->st);
+    if (!rc && cudaMemcpy2DAsync(x, ldx * sizeof(float), fx, n * sizeof(float), n * sizeof(float), nrhs,
+                                 cudaMemcpyDeviceToHost, s->st) != cudaSuccess) rc = ERR_INTERNAL;
+    if (cudaStreamSynchronize(s->st) != cudaSuccess) rc = ERR_INTERNAL;
+    s->kernel_launches += 3;
+    return rc;
+}
+
 int b200_refine_device(b200_solver_t *s, int64_t nrhs, const double *d_b, int64_t ldb, double *d_x, int64_t ldx,
                        int method, double eps, int64_t itermax, int64_t gmres_im, int64_t *niter, double *berr,
                        void *stream) {

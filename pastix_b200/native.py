@@ -30,7 +30,8 @@ SYMBOLS = ["b200_solver_create", "b200_solver_destroy", "b200_solver_create_schu
            "b200_spm_values_device", "b200_numfact", "b200_numfact_trace", "b200_solve", "b200_solve_trace",
            "b200_trace_launches", "b200_trace_kinds", "b200_solve_device", "b200_solve_status",
            "b200_solve_device_noalloc",
-           "b200_refine", "b200_refine_device", "b200_spmv", "b200_spmv_device", "b200_factor_download",
+           "b200_refine", "b200_solve_float", "b200_refine_float", "b200_refine_device", "b200_spmv",
+           "b200_spmv_device", "b200_factor_download",
            "b200_stats", "b200_strerror"]
 
 
@@ -105,6 +106,9 @@ def lib():
         L.b200_solve_status.argtypes = [_P, _P]
         L.b200_refine.argtypes = [_P, _I64, _P, _I64, _P, _I64, C.c_int, C.c_double, _I64, _I64,
                                   C.POINTER(_I64), _P]
+        L.b200_solve_float.argtypes = [_P, _I64, _P, _I64]
+        L.b200_refine_float.argtypes = [_P, _I64, _P, _I64, _P, _I64, C.c_int, C.c_double, _I64, _I64,
+                                        C.POINTER(_I64), _P]
         L.b200_refine_device.argtypes = [_P, _I64, _P, _I64, _P, _I64, C.c_int, C.c_double, _I64, _I64,
                                          C.POINTER(_I64), _P, _P]
         L.b200_spmv.argtypes = [_P, _I64, C.c_double, _P, _I64, C.c_double, _P, _I64]
@@ -296,6 +300,23 @@ class Solver:
             x = np.array(b, dtype=np.float64, order="F", copy=True).reshape(self.n, -1, order="F")
         check(lib().b200_solve(self.h, x.shape[1], _p(x), self.n), "b200_solve")
         return x.reshape(np.shape(b), order="F")
+
+    def solve_float(self, b) -> np.ndarray:
+        """x = A^{-1} b for single-precision vectors (b200_solve_float), on a copy."""
+        x = np.array(b, dtype=np.float32, order="F", copy=True).reshape(self.n, -1, order="F")
+        check(lib().b200_solve_float(self.h, x.shape[1], _p(x), self.n), "b200_solve_float")
+        return x.reshape(np.shape(b), order="F")
+
+    def refine_float(self, b, x, method="gmres", eps=1e-6, itermax=250, gmres_im=25):
+        """Refinement of single-precision vectors (b200_refine_float), on a copy of x."""
+        b2 = np.array(b, dtype=np.float32, order="F", copy=True).reshape(self.n, -1, order="F")
+        x2 = np.array(x, dtype=np.float32, order="F", copy=True).reshape(self.n, -1, order="F")
+        nit = _I64(0)
+        berr = np.zeros(b2.shape[1])
+        m = REFINE[method] if isinstance(method, str) else int(method)
+        check(lib().b200_refine_float(self.h, b2.shape[1], _p(b2), self.n, _p(x2), self.n, m, eps, itermax,
+                                      gmres_im, C.byref(nit), _p(berr)), "b200_refine_float")
+        return x2.reshape(np.shape(x), order="F"), int(nit.value), berr
 
     def solve_device(self, d_ptr: int, nrhs: int, ld: int, stream: int | None = None):
         check(lib().b200_solve_device(self.h, nrhs, _P(d_ptr), ld, _P(stream) if stream else None),

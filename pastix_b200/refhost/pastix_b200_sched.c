@@ -332,9 +332,14 @@ pastix_b200_task_solve( pastix_data_t *pastix_data, pastix_int_t nrhs, void *b, 
         return PASTIX_ERR_BADPARAMETER;
     }
     t0 = b200_wtime();
-    d  = b200_vec_in( pastix_data, b, n, nrhs, ldb, &ldd );
-    rc = b200_solve( e->solver, nrhs, d, ldd );
-    b200_vec_out( pastix_data, d, b, n, nrhs, ldb, rc == PASTIX_SUCCESS );
+    if ( pastix_data->bcsc->flttype == PastixFloat ) {
+        rc = b200_solve_float( e->solver, nrhs, b, ldb );
+    }
+    else {
+        d  = b200_vec_in( pastix_data, b, n, nrhs, ldb, &ldd );
+        rc = b200_solve( e->solver, nrhs, d, ldd );
+        b200_vec_out( pastix_data, d, b, n, nrhs, ldb, rc == PASTIX_SUCCESS );
+    }
     pastix_data->dparm[DPARM_SOLV_TIME] = b200_wtime() - t0;
     if ( rc == PASTIX_SUCCESS ) {
         pastix_data->steps |= STEP_SOLVE;
@@ -431,14 +436,21 @@ pastix_b200_task_refine( pastix_data_t *pastix_data, pastix_int_t n, pastix_int_
     }
     t0   = b200_wtime();
     berr = malloc( (nrhs > 0 ? nrhs : 1) * sizeof(double) );
-    db   = b200_vec_in( pastix_data, b, gN, nrhs, ldb, &ldbd );
-    dx   = b200_vec_in( pastix_data, x, gN, nrhs, ldx, &ldxd );
     /* GMRES = 0, CG = 1, SR = 2 in both enums (include/pastix/api.h:241-246) */
-    rc = b200_refine( e->solver, nrhs, db, ldbd, dx, ldxd, (int)method,
-                      pastix_data->dparm[DPARM_EPSILON_REFINEMENT], pastix_data->iparm[IPARM_ITERMAX],
-                      pastix_data->iparm[IPARM_GMRES_IM], &niter, berr );
-    b200_vec_out( pastix_data, db, (void *)b, gN, nrhs, ldb, 0 );
-    b200_vec_out( pastix_data, dx, x, gN, nrhs, ldx, rc == PASTIX_SUCCESS );
+    if ( pastix_data->bcsc->flttype == PastixFloat ) {
+        rc = b200_refine_float( e->solver, nrhs, b, ldb, x, ldx, (int)method,
+                                pastix_data->dparm[DPARM_EPSILON_REFINEMENT], pastix_data->iparm[IPARM_ITERMAX],
+                                pastix_data->iparm[IPARM_GMRES_IM], &niter, berr );
+    }
+    else {
+        db = b200_vec_in( pastix_data, b, gN, nrhs, ldb, &ldbd );
+        dx = b200_vec_in( pastix_data, x, gN, nrhs, ldx, &ldxd );
+        rc = b200_refine( e->solver, nrhs, db, ldbd, dx, ldxd, (int)method,
+                          pastix_data->dparm[DPARM_EPSILON_REFINEMENT], pastix_data->iparm[IPARM_ITERMAX],
+                          pastix_data->iparm[IPARM_GMRES_IM], &niter, berr );
+        b200_vec_out( pastix_data, db, (void *)b, gN, nrhs, ldb, 0 );
+        b200_vec_out( pastix_data, dx, x, gN, nrhs, ldx, rc == PASTIX_SUCCESS );
+    }
     for ( j = 0; j < nrhs; j++ ) {
         emax = berr[j] > emax ? berr[j] : emax;
     }
