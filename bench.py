@@ -318,7 +318,7 @@ def e2e_path(solver, an, A, b, prec, refine, nrhs, reps=3):
         t.append(time.perf_counter())
         solver.numfact(0.0)
         t.append(time.perf_counter())
-        np.copyto(xp, bp)
+        _tx.copy_(_tb)  # x = b on the host (torch's CPU copy runs on all host threads)
         t.append(time.perf_counter())
         solver.solve(xp, inplace=True)
         t.append(time.perf_counter())

@@ -322,13 +322,13 @@ int build_schedule(b200_solver_t *s) {
     // base: first update of the launch the update belongs to (map entries are relative)
     // updates more than 64 columns wide take 128-column tiles (half the operand
     // traffic per flop of the 64-column tiles)
-    // the launch's tile width bn (64 or 128) bounds the columns of a tile; within it
-    // each update takes the narrowest multiple of 32 that keeps its tile count, so the
-    // column tiles split N evenly (N = 278: 3 tiles of 96, not 3 of 128)
+    // tiles of the launch's width bn (64 or 128 columns).  Narrower tiles that split N
+    // evenly (N = 278: 3 of 96 instead of 3 of 128) issue 30 % fewer MMAs at 80^3 but
+    // ran 5 % slower: the kernel is bound by the TMA round trips and barrier hand-offs
+    // per K chunk and per tile, which a narrower tile does not shorten
     auto push_tc = [&](Upd u, int bn, int &t0, int &t0w, int base) {
         s->flops_kind[6] += upd_flops(u);
-        const int ntn = (u.N + bn - 1) / bn;
-        u.nb = std::min(bn, ((u.N + ntn - 1) / ntn + 31) / 32 * 32);
+        u.nb = bn;
         u.tiles_m = (u.M + 127) / 128;
         u.tiles_n = (u.N + u.nb - 1) / u.nb;
         const int ui = (int)tcupds.size() - base;

@@ -16,16 +16,14 @@
 // update_tc_kernel is persistent (one CTA per SM, tiles of 128 rows x at most BN = 64
 // or 128 columns striding over the launch's tile list) and warp-specialised:
 //  * warp 0 (one lane): TMA producer.  One 2D tensor map per panel copy (K
-//    innermost, boxes of 32 K x 32 rows, 128-byte swizzle: stacked, exactly the
+//    innermost, boxes of 32 K x 64 rows, 128-byte swizzle: stacked, exactly the
 //    canonical K-major UMMA layout), a ring of [A hi][B hi]([A lo][B lo]) stages in
-//    shared memory, K in chunks of 32.  A tile's B operand is its update's nb rows
-//    (nb = the narrowest multiple of 32 that keeps the update's column-tile count, so
-//    the tiles split N evenly); only those are loaded.
+//    shared memory, K in chunks of 32.
 //  * warp 1 (one lane): allocates 2 BN TMEM columns (two 128 x BN FP32
-//    accumulators) and issues tcgen05.mma (M = 128, N = nb, K = 8; the N field of the
-//    instruction descriptor is set per tile), skipping the K steps of a chunk's
-//    zero-filled tail; each stage is released to the producer and each accumulator
-//    to the epilogue by tcgen05.commit on an mbarrier.
+//    accumulators) and issues tcgen05.mma (M = 128, N = the update's tile width, K =
+//    8; the N field of the instruction descriptor is set per tile), skipping the K
+//    steps of a chunk's zero-filled tail; each stage is released to the producer and
+//    each accumulator to the epilogue by tcgen05.commit on an mbarrier.
 //  * warps 2-9: epilogue.  Thread = accumulator row (TMEM lane quarter = warp % 4),
 //    two warps per quarter with BN / 2 columns each; tcgen05.ld, release the
 //    accumulator, scatter-add into f with reductions (red.global.add), overlapping
@@ -276,7 +274,7 @@ __global__ void __launch_bounds__(TC_THREADS, 1) update_tc_kernel(DevSym s, cons
                 const int side_a = (u.flags & UPD_A_U) ? 1 : 0, side_b = (u.flags & UPD_B_U) ? 1 : 0;
                 const CUtensorMap *ma = maps + (size_t)(side_a * 2) * N + u.k;
                 const CUtensorMap *mb = maps + (size_t)(side_b * 2) * N + u.k;
-                const int nb = u.nb;  // this update's tile width: nb / 32 boxes of B rows
+                const int nb = u.nb;  // this update's tile width: nb / 64 boxes of B rows
                 const int ya = u.rowA0 + tt.mt * TC_BM, yb = u.rowB0 + tt.nt * nb;
                 const int nk = (u.K + TC_BK - 1) / TC_BK;
                 const uint32_t tx = (uint32_t)(TC_A_BYTES + nb * TC_BK * 4) * (SPLIT ? 2u : 1u);
@@ -292,14 +290,14 @@ __global__ void __launch_bounds__(TC_THREADS, 1) update_tc_kernel(DevSym s, cons
                     const uint32_t base = smem_addr(smem + (size_t)st * Cfg::STAGE);
                     const int x = kc * TC_BK + u.colK0;
 #pragma unroll
-                    for (int g = 0; g < TC_BM / 32; g++) tma_load_2d(base + g * 4096, ma, x, ya + 32 * g, bar);
-                    for (int g = 0; g < nb / 32; g++) tma_load_2d(base + TC_A_BYTES + g * 4096, mb, x, yb + 32 * g, bar);
+                    for (int g = 0; g < TC_BM / 64; g++) tma_load_2d(base + g * 8192, ma, x, ya + 64 * g, bar);
+                    for (int g = 0; g < nb / 64; g++) tma_load_2d(base + TC_A_BYTES + g * 8192, mb, x, yb + 64 * g, bar);
                     if (SPLIT) {
                         const uint32_t lb = base + TC_A_BYTES + TC_B_BYTES;
 #pragma unroll
-                        for (int g = 0; g < TC_BM / 32; g++) tma_load_2d(lb + g * 4096, ma + N, x, ya + 32 * g, bar);
-                        for (int g = 0; g < nb / 32; g++)
-                            tma_load_2d(lb + TC_A_BYTES + g * 4096, mb + N, x, yb + 32 * g, bar);
+                        for (int g = 0; g < TC_BM / 64; g++) tma_load_2d(lb + g * 8192, ma + N, x, ya + 64 * g, bar);
+                        for (int g = 0; g < nb / 64; g++)
+                            tma_load_2d(lb + TC_A_BYTES + g * 8192, mb + N, x, yb + 64 * g, bar);
                     }
                 }
             }
@@ -459,7 +457,7 @@ int configure_tc_kernels() {
 }
 
 // One 2D tensor map per operand copy (FP32, K innermost: ncols x stride with row
-// pitch kp = ncols rounded up to 4), boxes of 32 K x 32 rows with 128-byte swizzle;
+// pitch kp = ncols rounded up to 4), boxes of 32 K x 64 rows with 128-byte swizzle;
 // elements past ncols or stride read as zero.
 typedef CUresult (*EncodeTiledFn)(CUtensorMap *, CUtensorMapDataType, cuuint32_t, void *, const cuuint64_t *,
                                   const cuuint64_t *, const cuuint32_t *, const cuuint32_t *, CUtensorMapInterleave,
@@ -484,7 +482,7 @@ int encode_operand_maps(const std::vector<int64_t> &toff, const std::vector<int>
         const int kp = (ncols[k] + 3) & ~3;
         cuuint64_t dims[2] = {(cuuint64_t)ncols[k], (cuuint64_t)stride[k]};
         cuuint64_t strides[1] = {(cuuint64_t)kp * sizeof(float)};
-        cuuint32_t box[2] = {32, 32};
+        cuuint32_t box[2] = {32, 64};
         cuuint32_t estr[2] = {1, 1};
         CUresult r = encode(&maps[k], CU_TENSOR_MAP_DATA_TYPE_FLOAT32, 2, arena + toff[k], dims, strides, box, estr,
                             CU_TENSOR_MAP_INTERLEAVE_NONE, CU_TENSOR_MAP_SWIZZLE_128B,
