@@ -49,6 +49,9 @@ def parse():
     ap.add_argument("--mixed", default="auto",
                     help="precision of the mixed path (fp32, tf32, tf32x3; auto = tf32x3: FP32 factor with 3xTF32 "
                          "tensor-core updates)")
+    ap.add_argument("--extra-paths", default="bf16x3",
+                    help="comma-separated further FP32-factor precisions measured beside fp64 and the mixed path "
+                         "(refined to the same target; the headline takes the fastest path that meets it)")
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--no-tune", action="store_true", help="built-in kernel choices instead of the autotuned table")
     ap.add_argument("--tune-budget", type=float, default=150.0,
@@ -433,7 +436,9 @@ def main():
     solvers = {}
     kinds_trace, kinds_launches = {}, {}
     tunings = {}
-    for prec, refine in (("fp64", False), (mixed_prec, True)):
+    paths = [("fp64", False), (mixed_prec, True)]
+    paths += [(p, True) for p in args.extra_paths.split(",") if p and p not in (mixed_prec, "fp64")]
+    for prec, refine in paths:
         tuning = None
         if not args.no_tune:
             # the autotuned kernel choices of this structure (cached by structure,

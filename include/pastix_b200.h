@@ -42,8 +42,13 @@ enum { B200_FACTO_POTRF = 0, B200_FACTO_SYTRF = 1, B200_FACTO_GETRF = 2 };
  *           with FP32 accumulation.
  *  TF32X3 : as TF32 with split (big + small) operands, three TF32 products per
  *           update, for close-to-FP32 accuracy.
+ *  BF16X3 : factor in float, wide updates on tcgen05 tensor cores with split BF16
+ *           operands (x = hi + lo, both BF16; three BF16 products accumulated in
+ *           FP32, about 2^-17 relative per product): half the operand bytes and
+ *           twice the MMA rate of TF32, a less accurate factor for the refinement
+ *           to correct.
  * The solve and refinement vectors are always double. */
-enum { B200_PREC_FP64 = 0, B200_PREC_FP32 = 1, B200_PREC_TF32 = 2, B200_PREC_TF32X3 = 3 };
+enum { B200_PREC_FP64 = 0, B200_PREC_FP32 = 1, B200_PREC_TF32 = 2, B200_PREC_TF32X3 = 3, B200_PREC_BF16X3 = 4 };
 
 /* Refinement methods, numbered as PaStiX's pastix_refine_t
  * (include/pastix/api.h, IPARM_REFINEMENT): GMRES, CG, simple refinement. */

@@ -59,15 +59,16 @@ int configure_factor_kernels();
 // columns listed by tmap ({update index, row tile | column tile << 16}); maps: 4 x cblknbr
 // tensor maps of the operand arenas, [(side * 2 + part) * cblknbr + k] with side
 // 0 L / 1 U and part 0 hi / 1 lo; split: 3xTF32.
+// op: operand format of the copies, 0 FP32 read as TF32 (kind::tf32), 1 BF16 (kind::f16, always split)
 void launch_update_tc(const DevSym &s, const Upd *upds, const int2 *tmap, int ntiles, const void *maps, float *L,
-                      float *U, int split, int bn, int *err, cudaStream_t st);
+                      float *U, int split, int bn, int op, int *err, cudaStream_t st);
 int configure_tc_kernels();
 // copy panel tiles row-major into the operand arena (hi, and lo = x - hi when lo is given)
 void launch_panel_split(const DevSym &s, const SplitTask *tasks, int ntasks, const float *P, const int64_t *toff,
-                        float *hi, float *lo, cudaStream_t st);
+                        void *hi, void *lo, int op, cudaStream_t st);
 // tensor maps of the operand copies of the cblks with wanted[k] != 0 (maps: cblknbr entries)
 int encode_operand_maps(const std::vector<int64_t> &toff, const std::vector<int> &stride,
-                        const std::vector<int> &ncols, const std::vector<char> &wanted, float *arena,
+                        const std::vector<int> &ncols, const std::vector<char> &wanted, void *arena, int op,
                         CUtensorMap *maps);
 
 // solve (solve_kernels.cu); x is the permuted right-hand side block, n x nrhs, leading

@@ -156,6 +156,7 @@ struct b200_solver_s {
     // FP32 updates on the tensor cores (precision TF32 / TF32X3); updates below the
     // size thresholds stay on the SIMT kernel
     bool use_tc = false;
+    int op = 0;                         // operand format of the tensor-core updates: 0 TF32, 1 BF16
     b200_tuning_t tuning{};             // kernel choices (b200_solver_create_tuned)
     Upd *d_tcupd = nullptr;
     std::vector<int> lvl_tc_u0, lvl_tc_u1, lvl_tc_tiles, lvl_tc_m0, lvl_tc_wtiles, lvl_tc_mw0;
@@ -164,8 +165,8 @@ struct b200_solver_s {
     Upd *d_smallupd = nullptr;            // updates with K <= 16, N <= 32 (one warp each)
     std::vector<int> lvl_us0, lvl_us1;
     std::vector<char> tc_wanted;          // cblks whose panels the tensor-core updates read
-    std::vector<int64_t> toff;            // operand copy of cblk k: row-major, pitch ncols rounded up to 4
-    int64_t tsize = 0;                    // floats of one operand arena
+    std::vector<int64_t> toff;            // operand copy of cblk k: row-major, pitch ncols rounded up to 16 bytes
+    int64_t tsize = 0;                    // elements of one operand arena
     void *d_tarena = nullptr;             // [L hi][L lo][U hi][U lo] (lo only for TF32X3, U only for LU)
     int64_t *d_toffT = nullptr;
     void *d_maps = nullptr;               // 4 x cblknbr tensor maps
@@ -696,11 +697,12 @@ int build_schedule(b200_solver_t *s) {
     RET(s->dupload(&s->d_split, splits));
     s->toff.assign(N, 0);
     int64_t tp = 0;
+    const int oesz = s->op ? 2 : 4, pad = 16 / oesz;  // operand element bytes; pitch in 16-byte units
     for (int k = 0; k < N; k++) {
         if (!s->tc_wanted[k]) continue;
         s->toff[k] = tp;
-        tp += (int64_t)s->stride[k] * ((s->ncols[k] + 3) & ~3);
-        tp = (tp + 63) / 64 * 64;  // 256-byte starts
+        tp += (int64_t)s->stride[k] * ((s->ncols[k] + pad - 1) / pad * pad);
+        tp = (tp + 256 / oesz - 1) / (256 / oesz) * (256 / oesz);  // 256-byte starts
     }
     s->tsize = tp;
     RET(s->dupload(&s->d_toffT, s->toff));
@@ -831,14 +833,15 @@ struct Trace {
 
 // Row-major (split) copies of the panel tiles sp0..sp1 for the tensor-core updates.
 void enqueue_split(b200_solver_t *s, int sp0, int sp1, cudaStream_t st) {
-    const bool split = s->prec == B200_PREC_TF32X3;
-    float *a = (float *)s->d_tarena;
+    const bool split = s->prec == B200_PREC_TF32X3 || s->prec == B200_PREC_BF16X3;
+    char *a = (char *)s->d_tarena;
+    const size_t part_bytes = (size_t)s->tsize * (s->op ? 2 : 4);
     const int parts = split ? 2 : 1;
     for (int side = 0; side < (s->facto == FACTO_GETRF ? 2 : 1); side++) {
-        float *hi = a + (size_t)(side * parts) * s->tsize;
-        float *lo = split ? hi + s->tsize : nullptr;
+        char *hi = a + (size_t)(side * parts) * part_bytes;
+        char *lo = split ? hi + part_bytes : nullptr;
         launch_panel_split(s->ds, s->d_split + sp0, sp1 - sp0, (const float *)(side ? s->dU : s->dL), s->d_toffT, hi,
-                           lo, st);
+                           lo, s->op, st);
     }
 }
 
@@ -919,11 +922,11 @@ int enqueue_numfact(b200_solver_t *s, cudaStream_t st, Trace *tr = nullptr) {
             launches += 1 + (s->facto == FACTO_GETRF);
             if (tr) tr->end(7, st);
             if (tr) tr->begin(st);
-            const int split = s->prec == B200_PREC_TF32X3;
+            const int split = s->prec == B200_PREC_TF32X3 || s->prec == B200_PREC_BF16X3;
             launch_update_tc(s->ds, s->d_tcupd + s->lvl_tc_u0[l], s->d_tcmap + s->lvl_tc_m0[l], s->lvl_tc_tiles[l],
-                             s->d_maps, (float *)L, (float *)U, split, 64, s->d_err, st);
+                             s->d_maps, (float *)L, (float *)U, split, 64, s->op, s->d_err, st);
             launch_update_tc(s->ds, s->d_tcupd + s->lvl_tc_u0[l], s->d_tcmapw + s->lvl_tc_mw0[l],
-                             s->lvl_tc_wtiles[l], s->d_maps, (float *)L, (float *)U, split, 128, s->d_err, st);
+                             s->lvl_tc_wtiles[l], s->d_maps, (float *)L, (float *)U, split, 128, s->op, s->d_err, st);
             launches += (s->lvl_tc_tiles[l] > 0) + (s->lvl_tc_wtiles[l] > 0);
             if (tr) tr->end(6, st);
         }
@@ -1483,7 +1486,7 @@ int b200_solver_create_tuned(const b200_symbol_t *sym, int facto, int precision,
         for (int w = 0; w < B200_TUNE_WCLASSES; w++)
             for (int h = 0; h < B200_TUNE_HCLASSES; h++)
                 if (tuning->update[w][h] < 0 || tuning->update[w][h] > B200_UPD_TC64) return ERR_BADPARAM;
-    if (!sym || !out || facto < 0 || facto > 2 || precision < 0 || precision > 3) return ERR_BADPARAM;
+    if (!sym || !out || facto < 0 || facto > 2 || precision < 0 || precision > 4) return ERR_BADPARAM;
     if (sym->n <= 0 || sym->cblknbr <= 0 || sym->n >= (1LL << 31) || sym->bloknbr >= (1LL << 31)) return ERR_BADPARAM;
     if (cblkschur < 1 || cblkschur > sym->cblknbr) return ERR_BADPARAM;
     int dev = 0;
@@ -1494,7 +1497,8 @@ int b200_solver_create_tuned(const b200_symbol_t *sym, int facto, int precision,
     s->prec = precision;
     s->f32 = precision != B200_PREC_FP64;
     s->esz = s->f32 ? 4 : 8;
-    s->use_tc = precision == B200_PREC_TF32 || precision == B200_PREC_TF32X3;
+    s->use_tc = precision == B200_PREC_TF32 || precision == B200_PREC_TF32X3 || precision == B200_PREC_BF16X3;
+    s->op = precision == B200_PREC_BF16X3 ? 1 : 0;
     if (tuning) s->tuning = *tuning;
     s->panel_steps_only = s->tuning.panel_tiles != 0;
     if (const char *e = getenv("B200_PANEL_TILES")) s->panel_steps_only = atoi(e) != 0;
@@ -1610,13 +1614,14 @@ int b200_solver_create_tuned(const b200_symbol_t *sym, int facto, int precision,
     if (!rc && facto == FACTO_GETRF) rc = dalloc((char **)&s->dWU, (size_t)s->winv_elems * s->esz);
     if (!rc && s->use_tc) {
         // operand arenas and their tensor maps
-        const int parts = precision == B200_PREC_TF32X3 ? 2 : 1, sides = facto == FACTO_GETRF ? 2 : 1;
-        rc = dalloc((char **)&s->d_tarena, (size_t)std::max<int64_t>(s->tsize, 64) * parts * sides * sizeof(float));
+        const int parts = (precision == B200_PREC_TF32X3 || precision == B200_PREC_BF16X3) ? 2 : 1;
+        const int sides = facto == FACTO_GETRF ? 2 : 1, oesz = s->op ? 2 : 4;
+        rc = dalloc((char **)&s->d_tarena, (size_t)std::max<int64_t>(s->tsize, 128) * parts * sides * oesz);
         std::vector<CUtensorMap> maps((size_t)4 * N);
         for (int side = 0; side < sides && !rc; side++)
             for (int part = 0; part < parts && !rc; part++) {
-                float *arena = (float *)s->d_tarena + (size_t)(side * parts + part) * s->tsize;
-                if (encode_operand_maps(s->toff, s->stride, s->ncols, s->tc_wanted, arena,
+                char *arena = (char *)s->d_tarena + (size_t)(side * parts + part) * s->tsize * oesz;
+                if (encode_operand_maps(s->toff, s->stride, s->ncols, s->tc_wanted, arena, s->op,
                                         maps.data() + (size_t)(side * 2 + part) * N)) {
                     fprintf(stderr, "pastix_b200: cannot encode the tensor maps of the operand copies\n");
                     rc = ERR_INTERNAL;

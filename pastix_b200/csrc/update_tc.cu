@@ -8,10 +8,14 @@
 // Operand copies.  kind::tf32 reads its operands K-major (the MN-major form leaves
 // the accumulator untouched on sm_100a) while the factor panels are column-major,
 // so once a panel is final (after its TRSM) panel_split_kernel writes it row-major
-// (row r of cblk k at toff[k] + r * kp_k, kp_k = ncols_k rounded up to 4) into an
-// operand arena, split for TF32X3: x = hi + lo with hi = x with its 13 low mantissa
-// bits cleared (exact in TF32) and lo = x - hi (exact); D += hi_A hi_B + hi_A lo_B +
-// lo_A hi_B keeps close to FP32 accuracy.  TF32 keeps x once and D += A B.
+// (row r of cblk k at toff[k] + r * kp_k, kp_k = ncols_k rounded up to 16 bytes)
+// into an operand arena, split for TF32X3: x = hi + lo with hi = x with its 13 low
+// mantissa bits cleared (exact in TF32) and lo = x - hi (exact); D += hi_A hi_B +
+// hi_A lo_B + lo_A hi_B keeps close to FP32 accuracy.  TF32 keeps x once and D += A B.
+// BF16X3 (kind::f16, both operands BF16, FP32 accumulation): hi = x rounded to BF16,
+// lo = (x - hi) rounded to BF16, the same three products -- x = hi + lo to about 2^-17
+// relative, half the bytes per operand and twice the MMA rate of TF32; a 128-byte
+// operand row then holds 64 K values instead of 32.
 //
 // update_tc_kernel is persistent (one CTA per SM, tiles of 128 rows x at most BN = 64
 // or 128 columns striding over the launch's tile list) and warp-specialised:
@@ -32,14 +36,24 @@
 //    up; the kernel then records bit 2 of err, waits (bounded) for its TMA loads and
 //    MMAs in flight, frees its TMEM and returns.
 #include <cuda.h>
+#include <cuda_bf16.h>
 
 #include "b200_internal.h"
 #include "kernels.h"
 
 namespace b200 {
 
-constexpr int TC_BM = 128, TC_BK = 32;
-constexpr int TC_A_BYTES = TC_BM * TC_BK * 4;  // 16 KB
+constexpr int TC_BM = 128, TC_BK = 32;          // TC_BK: K of a 128-byte row of FP32 (TF32) operands
+constexpr int TC_A_BYTES = TC_BM * TC_BK * 4;  // 16 KB: 128 rows of 128 bytes, for either format
+
+// operand formats: OP_TF32 (FP32 storage, kind::tf32) and OP_BF16 (kind::f16 on BF16)
+enum { OP_TF32 = 0, OP_BF16 = 1 };
+template <int OP>
+struct OpFmt {
+    static constexpr int BK = OP == OP_BF16 ? 64 : 32;     // K values per 128-byte operand row (a stage)
+    static constexpr int KSTEP = OP == OP_BF16 ? 16 : 8;   // K of one MMA: 32 bytes of the row
+    static constexpr uint32_t FMT = OP == OP_BF16 ? 1u : 2u;  // A/B format in the instruction descriptor
+};
 constexpr long long TC_WAIT_CYCLES = 1000000000LL;  // about 0.5 s at the maximum SM clock
 constexpr int TC_THREADS = 320;  // producer, MMA, 8 epilogue warps
 constexpr int TC_EPI_WARPS = 8;
@@ -55,9 +69,10 @@ struct TcCfg {
     static constexpr uint32_t TMEM_COLS = 2 * BN;    // two accumulators
 };
 
-// instruction descriptor: D F32, A/B TF32, both K-major, M = 128, N = n (a multiple of 16)
-__device__ __forceinline__ uint32_t tc_idesc(int n) {
-    return (1u << 4) | (2u << 7) | (2u << 10) | ((uint32_t)(n >> 3) << 17) | ((uint32_t)(TC_BM >> 4) << 24);
+// instruction descriptor: D F32, A and B of the same format fmt (TF32 = 2 for
+// kind::tf32, BF16 = 1 for kind::f16), both K-major, M = 128, N = n (a multiple of 16)
+__device__ __forceinline__ uint32_t tc_idesc(int n, uint32_t fmt) {
+    return (1u << 4) | (fmt << 7) | (fmt << 10) | ((uint32_t)(n >> 3) << 17) | ((uint32_t)(TC_BM >> 4) << 24);
 }
 
 __device__ __forceinline__ uint32_t smem_addr(const void *p) {
@@ -120,14 +135,23 @@ __device__ __forceinline__ uint64_t umma_desc(uint32_t addr) {
     return d;
 }
 
-__device__ __forceinline__ void umma_tf32(uint32_t tmem, uint64_t da, uint64_t db, uint32_t idesc,
-                                          uint32_t accumulate) {
-    asm volatile(
-        "{\n\t.reg .pred p;\n\t"
-        "setp.ne.b32 p, %4, 0;\n\t"
-        "tcgen05.mma.cta_group::1.kind::tf32 [%0], %1, %2, %3, {%5, %6, %7, %8}, p;\n\t}\n" ::"r"(tmem),
-        "l"(da), "l"(db), "r"(idesc), "r"(accumulate), "r"(0), "r"(0), "r"(0), "r"(0)
-        : "memory");
+template <int OP>
+__device__ __forceinline__ void umma_op(uint32_t tmem, uint64_t da, uint64_t db, uint32_t idesc,
+                                        uint32_t accumulate) {
+    if (OP == OP_BF16)
+        asm volatile(
+            "{\n\t.reg .pred p;\n\t"
+            "setp.ne.b32 p, %4, 0;\n\t"
+            "tcgen05.mma.cta_group::1.kind::f16 [%0], %1, %2, %3, {%5, %6, %7, %8}, p;\n\t}\n" ::"r"(tmem),
+            "l"(da), "l"(db), "r"(idesc), "r"(accumulate), "r"(0), "r"(0), "r"(0), "r"(0)
+            : "memory");
+    else
+        asm volatile(
+            "{\n\t.reg .pred p;\n\t"
+            "setp.ne.b32 p, %4, 0;\n\t"
+            "tcgen05.mma.cta_group::1.kind::tf32 [%0], %1, %2, %3, {%5, %6, %7, %8}, p;\n\t}\n" ::"r"(tmem),
+            "l"(da), "l"(db), "r"(idesc), "r"(accumulate), "r"(0), "r"(0), "r"(0), "r"(0)
+            : "memory");
 }
 
 __device__ __forceinline__ void umma_commit(uint32_t bar) {
@@ -169,14 +193,33 @@ __device__ __forceinline__ void tc_decode(const Upd *__restrict__ upds, const in
 
 // ---------------------------------------------------------------- operand copies
 
-// One 32 x 32 tile of a panel to the row-major operand arena(s).
+__device__ __forceinline__ void split_store(float *dh, float *dl, size_t i, float x) {
+    if (dl) {
+        const float h = __uint_as_float(__float_as_uint(x) & 0xFFFFE000u);
+        dh[i] = h;
+        dl[i] = x - h;
+    } else {
+        dh[i] = x;
+    }
+}
+
+__device__ __forceinline__ void split_store(__nv_bfloat16 *dh, __nv_bfloat16 *dl, size_t i, float x) {
+    const __nv_bfloat16 h = __float2bfloat16_rn(x);
+    dh[i] = h;
+    if (dl) dl[i] = __float2bfloat16_rn(x - __bfloat162float(h));
+}
+
+// One 32 x 32 tile of a panel to the row-major operand arena(s) of element type E
+// (float for TF32 operands, BF16); the row pitch kp is ncols rounded up to 16 bytes.
+template <typename E>
 __global__ void __launch_bounds__(256) panel_split_kernel(DevSym s, const SplitTask *__restrict__ tasks,
                                                           const float *__restrict__ P,
-                                                          const int64_t *__restrict__ toff, float *hi, float *lo) {
+                                                          const int64_t *__restrict__ toff, E *hi, E *lo) {
     __shared__ float t[32][33];
+    constexpr int PAD = 16 / sizeof(E);
     const SplitTask tk = tasks[blockIdx.x];
     const int k = tk.k, tx = threadIdx.x & 31, ty = threadIdx.x >> 5;
-    const int stride = s.stride[k], nc = s.ncols[k], ld = s.ld[k], kp = (nc + 3) & ~3;
+    const int stride = s.stride[k], nc = s.ncols[k], ld = s.ld[k], kp = (nc + PAD - 1) / PAD * PAD;
     const float *src = P + s.off[k];
 #pragma unroll
     for (int i = 0; i < 4; i++) {
@@ -184,38 +227,37 @@ __global__ void __launch_bounds__(256) panel_split_kernel(DevSym s, const SplitT
         t[ty + 8 * i][tx] = (r < stride && c < nc) ? src[r + (size_t)c * ld] : 0.f;
     }
     __syncthreads();
-    float *dh = hi + toff[k];
-    float *dl = lo ? lo + toff[k] : nullptr;
+    E *dh = hi + toff[k];
+    E *dl = lo ? lo + toff[k] : nullptr;
 #pragma unroll
     for (int i = 0; i < 4; i++) {
         const int r = tk.row0 + ty + 8 * i, c = tk.col0 + tx;
-        if (r < stride && c < kp) {
-            const float x = t[tx][ty + 8 * i];
-            if (dl) {
-                const float h = __uint_as_float(__float_as_uint(x) & 0xFFFFE000u);
-                dh[(size_t)r * kp + c] = h;
-                dl[(size_t)r * kp + c] = x - h;
-            } else {
-                dh[(size_t)r * kp + c] = x;
-            }
-        }
+        if (r < stride && c < kp) split_store(dh, dl, (size_t)r * kp + c, t[tx][ty + 8 * i]);
     }
 }
 
 void launch_panel_split(const DevSym &s, const SplitTask *tasks, int ntasks, const float *P, const int64_t *toff,
-                        float *hi, float *lo, cudaStream_t st) {
-    if (ntasks > 0) panel_split_kernel<<<ntasks, 256, 0, st>>>(s, tasks, P, toff, hi, lo);
+                        void *hi, void *lo, int op, cudaStream_t st) {
+    if (ntasks <= 0) return;
+    if (op == OP_BF16)
+        panel_split_kernel<__nv_bfloat16><<<ntasks, 256, 0, st>>>(
+            s, tasks, P, toff, static_cast<__nv_bfloat16 *>(hi), static_cast<__nv_bfloat16 *>(lo));
+    else
+        panel_split_kernel<float><<<ntasks, 256, 0, st>>>(s, tasks, P, toff, static_cast<float *>(hi),
+                                                          static_cast<float *>(lo));
 }
 
 // ---------------------------------------------------------------- GEMM-scatter
 
 // maps[(side * 2 + part) * cblknbr + k]: side 0 L / 1 U, part 0 hi / 1 lo
-template <int SPLIT, int BN>
+template <int SPLIT, int BN, int OP>
 __global__ void __launch_bounds__(TC_THREADS, 1) update_tc_kernel(DevSym s, const Upd *__restrict__ upds,
                                                                   const int2 *__restrict__ tmap, int ntiles,
                                                                   const CUtensorMap *__restrict__ maps,
                                                                   float *L, float *U, int *err) {
     using Cfg = TcCfg<SPLIT, BN>;
+    using Fmt = OpFmt<OP>;
+    constexpr int BK = Fmt::BK;  // K values per stage (one 128-byte operand row)
     constexpr int TC_B_BYTES = Cfg::B_BYTES;
     constexpr int TC_BN = BN;
     constexpr uint32_t TC_TMEM_COLS = Cfg::TMEM_COLS;
@@ -276,8 +318,8 @@ __global__ void __launch_bounds__(TC_THREADS, 1) update_tc_kernel(DevSym s, cons
                 const CUtensorMap *mb = maps + (size_t)(side_b * 2) * N + u.k;
                 const int nb = u.nb;  // this update's tile width: nb / 64 boxes of B rows
                 const int ya = u.rowA0 + tt.mt * TC_BM, yb = u.rowB0 + tt.nt * nb;
-                const int nk = (u.K + TC_BK - 1) / TC_BK;
-                const uint32_t tx = (uint32_t)(TC_A_BYTES + nb * TC_BK * 4) * (SPLIT ? 2u : 1u);
+                const int nk = (u.K + BK - 1) / BK;
+                const uint32_t tx = (uint32_t)(TC_A_BYTES + nb * 128) * (SPLIT ? 2u : 1u);
                 for (int kc = 0; kc < nk; kc++, it++) {
                     const int st = it % NST;
                     if (it >= NST && !mbar_wait(smem_addr(&empty_bar[st]), ((it / NST) - 1) & 1, &abort_sh)) {
@@ -288,7 +330,7 @@ __global__ void __launch_bounds__(TC_THREADS, 1) update_tc_kernel(DevSym s, cons
                     mbar_expect_tx(bar, tx);
                     last_ph[st] = (it / NST) & 1;
                     const uint32_t base = smem_addr(smem + (size_t)st * Cfg::STAGE);
-                    const int x = kc * TC_BK + u.colK0;
+                    const int x = kc * BK + u.colK0;
 #pragma unroll
                     for (int g = 0; g < TC_BM / 64; g++) tma_load_2d(base + g * 8192, ma, x, ya + 64 * g, bar);
                     for (int g = 0; g < nb / 64; g++) tma_load_2d(base + TC_A_BYTES + g * 8192, mb, x, yb + 64 * g, bar);
@@ -321,8 +363,8 @@ __global__ void __launch_bounds__(TC_THREADS, 1) update_tc_kernel(DevSym s, cons
                 }
                 asm volatile("tcgen05.fence::after_thread_sync;\n" ::: "memory");
                 const uint32_t acc = tmem + (uint32_t)(a * TC_BN);
-                const int nk = (tt.u.K + TC_BK - 1) / TC_BK;
-                const uint32_t idesc = tc_idesc(tt.u.nb);
+                const int nk = (tt.u.K + BK - 1) / BK;
+                const uint32_t idesc = tc_idesc(tt.u.nb, Fmt::FMT);
                 for (int kc = 0; kc < nk; kc++, it++) {
                     const int st = it % NST;
                     if (!mbar_wait(smem_addr(&full_bar[st]), (it / NST) & 1, &abort_sh)) {
@@ -333,18 +375,18 @@ __global__ void __launch_bounds__(TC_THREADS, 1) update_tc_kernel(DevSym s, cons
                     const uint32_t base = smem_addr(smem + (size_t)st * Cfg::STAGE);
                     const uint32_t a_hi = base, b_hi = base + TC_A_BYTES;
                     const uint32_t a_lo = base + TC_A_BYTES + TC_B_BYTES, b_lo = a_lo + TC_A_BYTES;
-                    // K steps of 8 holding data: the chunk's zero-filled tail (K past the
+                    // K steps holding data: the chunk's zero-filled tail (K past the
                     // cblk's columns, read as zeros by the TMA) contributes nothing
-                    const int k8n = min(TC_BK / 8, (tt.u.K - kc * TC_BK + 7) / 8);
+                    const int ksn = min(4, (tt.u.K - kc * BK + Fmt::KSTEP - 1) / Fmt::KSTEP);
 #pragma unroll
-                    for (int k8 = 0; k8 < TC_BK / 8; k8++) {
-                        if (k8 >= k8n) break;
-                        // K step: 8 values = 32 bytes into each row line
-                        const uint64_t dah = umma_desc(a_hi + 32 * k8), dbh = umma_desc(b_hi + 32 * k8);
-                        umma_tf32(acc, dah, dbh, idesc, (kc > 0 || k8 > 0) ? 1u : 0u);
+                    for (int ks = 0; ks < 4; ks++) {
+                        if (ks >= ksn) break;
+                        // K step: 32 bytes into each row line (8 TF32 or 16 BF16 values)
+                        const uint64_t dah = umma_desc(a_hi + 32 * ks), dbh = umma_desc(b_hi + 32 * ks);
+                        umma_op<OP>(acc, dah, dbh, idesc, (kc > 0 || ks > 0) ? 1u : 0u);
                         if (SPLIT) {
-                            umma_tf32(acc, dah, umma_desc(b_lo + 32 * k8), idesc, 1u);
-                            umma_tf32(acc, umma_desc(a_lo + 32 * k8), dbh, idesc, 1u);
+                            umma_op<OP>(acc, dah, umma_desc(b_lo + 32 * ks), idesc, 1u);
+                            umma_op<OP>(acc, umma_desc(a_lo + 32 * ks), dbh, idesc, 1u);
                         }
                     }
                     umma_commit(smem_addr(&empty_bar[st]));
@@ -424,27 +466,34 @@ __global__ void __launch_bounds__(TC_THREADS, 1) update_tc_kernel(DevSym s, cons
 
 static int g_num_sms = 0;
 
+template <int SPLIT, int BN, int OP>
+static void launch_tc(const DevSym &s, const Upd *upds, const int2 *tmap, int ntiles, const CUtensorMap *m, float *L,
+                      float *U, int *err, cudaStream_t st) {
+    const int grid = ntiles < g_num_sms ? ntiles : g_num_sms;
+    update_tc_kernel<SPLIT, BN, OP><<<grid, TC_THREADS, TcCfg<SPLIT, BN>::SMEM, st>>>(s, upds, tmap, ntiles, m, L, U,
+                                                                                    err);
+}
+
 void launch_update_tc(const DevSym &s, const Upd *upds, const int2 *tmap, int ntiles, const void *maps, float *L,
-                      float *U, int split, int bn, int *err, cudaStream_t st) {
+                      float *U, int split, int bn, int op, int *err, cudaStream_t st) {
     if (ntiles <= 0) return;
     const CUtensorMap *m = static_cast<const CUtensorMap *>(maps);
-    const int grid = ntiles < g_num_sms ? ntiles : g_num_sms;
-    if (bn == 128) {
-        if (split)
-            update_tc_kernel<1, 128><<<grid, TC_THREADS, TcCfg<1, 128>::SMEM, st>>>(s, upds, tmap, ntiles, m, L, U, err);
-        else
-            update_tc_kernel<0, 128><<<grid, TC_THREADS, TcCfg<0, 128>::SMEM, st>>>(s, upds, tmap, ntiles, m, L, U, err);
+    if (op == OP_BF16) {
+        // BF16 operands are always split (hi + lo): three products
+        if (bn == 128) launch_tc<1, 128, OP_BF16>(s, upds, tmap, ntiles, m, L, U, err, st);
+        else launch_tc<1, 64, OP_BF16>(s, upds, tmap, ntiles, m, L, U, err, st);
+    } else if (bn == 128) {
+        if (split) launch_tc<1, 128, OP_TF32>(s, upds, tmap, ntiles, m, L, U, err, st);
+        else launch_tc<0, 128, OP_TF32>(s, upds, tmap, ntiles, m, L, U, err, st);
     } else {
-        if (split)
-            update_tc_kernel<1, 64><<<grid, TC_THREADS, TcCfg<1, 64>::SMEM, st>>>(s, upds, tmap, ntiles, m, L, U, err);
-        else
-            update_tc_kernel<0, 64><<<grid, TC_THREADS, TcCfg<0, 64>::SMEM, st>>>(s, upds, tmap, ntiles, m, L, U, err);
+        if (split) launch_tc<1, 64, OP_TF32>(s, upds, tmap, ntiles, m, L, U, err, st);
+        else launch_tc<0, 64, OP_TF32>(s, upds, tmap, ntiles, m, L, U, err, st);
     }
 }
 
-template <int SPLIT, int BN>
+template <int SPLIT, int BN, int OP>
 static int tc_set_smem() {
-    return (int)cudaFuncSetAttribute(update_tc_kernel<SPLIT, BN>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+    return (int)cudaFuncSetAttribute(update_tc_kernel<SPLIT, BN, OP>, cudaFuncAttributeMaxDynamicSharedMemorySize,
                                      TcCfg<SPLIT, BN>::SMEM);
 }
 
@@ -452,19 +501,20 @@ int configure_tc_kernels() {
     int dev = 0, rc = 0;
     rc |= (int)cudaGetDevice(&dev);
     rc |= (int)cudaDeviceGetAttribute(&g_num_sms, cudaDevAttrMultiProcessorCount, dev);
-    rc |= tc_set_smem<0, 64>() | tc_set_smem<1, 64>() | tc_set_smem<0, 128>() | tc_set_smem<1, 128>();
+    rc |= tc_set_smem<0, 64, OP_TF32>() | tc_set_smem<1, 64, OP_TF32>() | tc_set_smem<0, 128, OP_TF32>() |
+          tc_set_smem<1, 128, OP_TF32>() | tc_set_smem<1, 64, OP_BF16>() | tc_set_smem<1, 128, OP_BF16>();
     return rc == 0 && g_num_sms > 0 ? 0 : -1;
 }
 
-// One 2D tensor map per operand copy (FP32, K innermost: ncols x stride with row
-// pitch kp = ncols rounded up to 4), boxes of 32 K x 64 rows with 128-byte swizzle;
-// elements past ncols or stride read as zero.
+// One 2D tensor map per operand copy (K innermost: ncols x stride with row pitch kp =
+// ncols rounded up to 16 bytes), boxes of one 128-byte row (32 FP32 or 64 BF16 values)
+// x 64 rows with 128-byte swizzle; elements past ncols or stride read as zero.
 typedef CUresult (*EncodeTiledFn)(CUtensorMap *, CUtensorMapDataType, cuuint32_t, void *, const cuuint64_t *,
                                   const cuuint64_t *, const cuuint32_t *, const cuuint32_t *, CUtensorMapInterleave,
                                   CUtensorMapSwizzle, CUtensorMapL2promotion, CUtensorMapFloatOOBfill);
 
 int encode_operand_maps(const std::vector<int64_t> &toff, const std::vector<int> &stride,
-                        const std::vector<int> &ncols, const std::vector<char> &wanted, float *arena,
+                        const std::vector<int> &ncols, const std::vector<char> &wanted, void *arena, int op,
                         CUtensorMap *maps) {
     static EncodeTiledFn encode = nullptr;
     if (!encode) {
@@ -476,15 +526,17 @@ int encode_operand_maps(const std::vector<int64_t> &toff, const std::vector<int>
         encode = reinterpret_cast<EncodeTiledFn>(fn);
     }
     const size_t n = toff.size();
+    const int esz = op == OP_BF16 ? 2 : 4, pad = 16 / esz;
     for (size_t k = 0; k < n; k++) {
         maps[k] = CUtensorMap{};
         if (!wanted[k] || !arena) continue;
-        const int kp = (ncols[k] + 3) & ~3;
+        const int kp = (ncols[k] + pad - 1) / pad * pad;
         cuuint64_t dims[2] = {(cuuint64_t)ncols[k], (cuuint64_t)stride[k]};
-        cuuint64_t strides[1] = {(cuuint64_t)kp * sizeof(float)};
-        cuuint32_t box[2] = {32, 64};
+        cuuint64_t strides[1] = {(cuuint64_t)kp * esz};
+        cuuint32_t box[2] = {(cuuint32_t)(128 / esz), 64};
         cuuint32_t estr[2] = {1, 1};
-        CUresult r = encode(&maps[k], CU_TENSOR_MAP_DATA_TYPE_FLOAT32, 2, arena + toff[k], dims, strides, box, estr,
+        CUresult r = encode(&maps[k], op == OP_BF16 ? CU_TENSOR_MAP_DATA_TYPE_BFLOAT16 : CU_TENSOR_MAP_DATA_TYPE_FLOAT32,
+                            2, static_cast<char *>(arena) + toff[k] * esz, dims, strides, box, estr,
                             CU_TENSOR_MAP_INTERLEAVE_NONE, CU_TENSOR_MAP_SWIZZLE_128B,
                             CU_TENSOR_MAP_L2_PROMOTION_L2_256B, CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE);
         if (r != CUDA_SUCCESS) return -2;

@@ -74,6 +74,29 @@ def test_tf32x3_updates_keep_fp32_accuracy(facto, make, method):
     assert fe <= 1e-8
 
 
+@pytest.mark.parametrize("facto,make,method", CASES)
+def test_bf16x3_updates_refine_to_fp64_accuracy(facto, make, method):
+    """Split-BF16 tensor-core updates (kind::f16, three BF16 products per update
+    accumulated in FP32): a factor within about 2^-16 of the FP64 one, refined to
+    <= 1e-12."""
+    d, be, fe, n_tc = run_case(make(), facto, "bf16x3", method)
+    print(f"\nbf16x3 {facto}: factor diff {d:.2e}, berr {be:.2e}, ferr {fe:.2e}")
+    assert n_tc > 0
+    assert d <= 1e-4, d
+    assert be <= BERR_TARGET
+    assert fe <= 1e-8
+
+
+def test_bf16x3_every_update_on_tensor_cores():
+    tuning = native.tuning_table(default=native.UPD["tc"])
+    tuning["update"][0][0] = native.UPD["tc64"]
+    d, be, fe, n_tc = run_case(M.laplacian(12, 12, 12, 27, 26.0, shift=1e-3), "potrf", "bf16x3", "cg",
+                               tuning=tuning)
+    assert n_tc > 0
+    assert d <= 1e-4, d
+    assert be <= BERR_TARGET
+
+
 @pytest.mark.parametrize("facto,make,method", CASES[:2])
 def test_tf32_updates_refine_to_fp64_accuracy(facto, make, method):
     d, be, fe, n_tc = run_case(make(), facto, "tf32", method)
