@@ -83,35 +83,23 @@ __device__ __forceinline__ void load4(const T *p, T v[4]) {
 }
 
 // Factor the wd x wd diagonal tile a (pitch LP, lower triangle) in place, by
-// 8-column leaves, left-looking between leaves:
-//   update (warp w = leaf column b + w): a_ij -= sum_{k < b} l_ik (d_k) l_jk over the
-//          factored columns, k ascending (the order of the right-looking kernel);
+// 8-column leaves, right-looking between leaves:
 //   leaf   (warp 0): every lane factors the leaf's 8 x 8 diagonal block in registers
 //          (the same values in every lane, no broadcasts), then its two rows below
 //          it column by column; static pivoting replaces a pivot below thr in
 //          magnitude by +-thr.  The pivot's square root is p * rsqrt(p) (within an
 //          ulp of sqrt(p); rsqrt(p) scales the column).
+//   update (all warps, warp w = trailing columns j = b + 8 + w, b + 16 + w, ...):
+//          a_ij -= l_ik (d_k) l_jk for the leaf's columns k, k ascending.  Every entry
+//          receives the factored columns' terms one by one in ascending k, leaf after
+//          leaf: the same operations in the same order as a left-looking sum over all
+//          earlier columns, spread over the CTA's warps instead of one chain per column.
 // LDL^T keeps D on the diagonal and unit L below.  Called by all PT threads.
 template <typename T, int FACTO, int LP>
 __device__ void factor_tile64(T *a, int wd, double thr, int *s_piv, int *s_err) {
-    const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
+    const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5, nwarp = blockDim.x >> 5;
     for (int b = 0; b < wd; b += 8) {
         const int bw = min(8, wd - b);
-        if (b > 0) {
-            if (warp < bw) {
-                const int j = b + warp;
-                for (int i = j + lane; i < wd; i += 32) {
-                    T acc = a[i + j * LP];
-                    for (int k = 0; k < b; k++) {
-                        const T lik = a[i + k * LP], ljk = a[j + k * LP];
-                        if (FACTO == FACTO_SYTRF) acc -= (lik * a[k * (LP + 1)]) * ljk;
-                        else acc -= lik * ljk;
-                    }
-                    a[i + j * LP] = acc;
-                }
-            }
-            __syncthreads();
-        }
         if (warp == 0) {
             T g[36];  // the leaf's diagonal block, lower part: g[r (r + 1) / 2 + c]
 #pragma unroll
@@ -194,6 +182,30 @@ __device__ void factor_tile64(T *a, int wd, double thr, int *s_piv, int *s_err) 
             }
         }
         __syncthreads();
+        if (b + 8 < wd) {
+            // rank-bw update of the trailing lower triangle with the leaf's columns
+            T dk[8];
+#pragma unroll
+            for (int c = 0; c < 8; c++) dk[c] = (FACTO == FACTO_SYTRF && c < bw) ? a[(b + c) * (LP + 1)] : (T)1;
+            for (int j = b + 8 + warp; j < wd; j += nwarp) {
+                T ljk[8];
+#pragma unroll
+                for (int c = 0; c < 8; c++) ljk[c] = (c < bw) ? a[j + (b + c) * LP] : (T)0;
+                for (int i = j + lane; i < wd; i += 32) {
+                    T acc = a[i + j * LP];
+#pragma unroll
+                    for (int c = 0; c < 8; c++) {
+                        if (c < bw) {
+                            const T lik = a[i + (b + c) * LP];
+                            if (FACTO == FACTO_SYTRF) acc -= (lik * dk[c]) * ljk[c];
+                            else acc -= lik * ljk[c];
+                        }
+                    }
+                    a[i + j * LP] = acc;
+                }
+            }
+            __syncthreads();
+        }
     }
 }
 
