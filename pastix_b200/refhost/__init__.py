@@ -23,7 +23,7 @@ _lib = None
 
 IPARM_NAMES = ["MIN_BLOCKSIZE", "MAX_BLOCKSIZE", "SCHEDULER", "THREAD_NBR", "TASKS2D_LEVEL",
                "REFINEMENT", "ITERMAX", "GMRES_IM", "FACTORIZATION", "NBITER", "STATIC_PIVOTING",
-               "NNZEROS", "IPARM_SIZE"]
+               "NNZEROS", "IO_STRATEGY", "IPARM_SIZE"]
 DPARM_NAMES = ["EPSILON_REFINEMENT", "EPSILON_MAGN_CTRL", "A_NORM", "FACT_TIME", "SOLV_TIME",
                "REFINE_TIME", "FACT_THFLOPS", "RELATIVE_ERROR", "DPARM_SIZE"]
 
@@ -50,6 +50,11 @@ def lib():
         L.rh_analyze_schur.argtypes = [C.c_int64, _I64P, _I64P, _P, C.c_int, C.c_int, C.c_int, C.c_int64,
                                        C.c_int64, C.c_int64, C.c_int, C.c_int, C.c_int, _P, C.c_int64, _P,
                                        C.POINTER(C.c_int)]
+        L.rh_analyze_load.restype = _P
+        L.rh_analyze_load.argtypes = [C.c_int64, _I64P, _I64P, _P, C.c_int, C.c_int, C.c_int, C.c_int, C.c_int,
+                                      C.c_int, _P, C.POINTER(C.c_int)]
+        L.rh_io_dir.restype = C.c_char_p
+        L.rh_io_dir.argtypes = [_P]
         L.rh_sizes.argtypes = [_P, _I64P]
         L.rh_export_solver.argtypes = [_P] + [_I64P] * 7 + [_I32P] + [_I64P] * 7
         L.rh_export_perm.argtypes = [_P, _I64P, _I64P]
@@ -136,11 +141,16 @@ class Analysis:
     """One PaStiX instance after ``pastix_task_analyze`` (grid ND ordering)."""
 
     def __init__(self, A, facto: str = "potrf", nthreads: int = 1, verbose: bool = False,
-                 iparm: dict | None = None, flttype: int = 3, schur=None):
+                 iparm: dict | None = None, flttype: int = 3, schur=None, load_dir: str | None = None):
         """schur: unknowns (0-based, original numbering) of a Schur complement
         (pastixSetSchurUnknownList); they must be the last ones of the grid ordering
-        (``schur_candidates`` gives them)."""
+        (``schur_candidates`` gives them).  load_dir: start from PaStiX's own saved
+        analysis files in that directory (``save_pastix_analysis``) instead of
+        computing the ordering and the symbolic factorization."""
         L = lib()
+        if load_dir is not None:
+            self._load(A, facto, nthreads, verbose, iparm, flttype, load_dir)
+            return
         self.A = A
         self.facto_name = facto
         self.facto = FACTO[facto]
@@ -163,6 +173,37 @@ class Analysis:
                                     sl.ctypes.data_as(C.c_void_p) if sl.size else None, C.byref(info))
         if info.value != 0:
             raise RuntimeError(f"PaStiX analysis failed: {info.value}")
+        self._bcsc_done = False
+
+    def _load(self, A, facto, nthreads, verbose, iparm, flttype, load_dir):
+        L = lib()
+        self.A = A
+        self.facto_name = facto
+        self.facto = FACTO[facto]
+        self.flttype = flttype
+        ip, _ = param_ids()
+        kv = []
+        for k, v in (iparm or {}).items():
+            kv += [ip[k], int(v)]
+        kva = np.array(kv, dtype=np.int64) if kv else np.zeros(2, dtype=np.int64)
+        vals = np.ascontiguousarray(A.values, dtype=np.float32 if flttype == 2 else np.float64)
+        self._vals = vals
+        missing = [f for f in ("ordername", "symbname") if not os.path.isfile(os.path.join(load_dir, f))]
+        if missing:  # PaStiX's order loader aborts the process on a missing file
+            raise RuntimeError(f"PaStiX analysis files missing in {load_dir}: {', '.join(missing)}")
+        info = C.c_int(0)
+        cwd = os.getcwd()
+        os.chdir(load_dir)  # PaStiX's loaders open "ordername" and "symbname" where they run
+        try:
+            self.h = L.rh_analyze_load(A.n, np.ascontiguousarray(A.colptr, dtype=np.int64),
+                                       np.ascontiguousarray(A.rowind, dtype=np.int64),
+                                       vals.ctypes.data_as(C.c_void_p), 0 if not A.symmetric else 1, flttype,
+                                       self.facto, nthreads, 1 if verbose else 0, len(kv) // 2,
+                                       kva.ctypes.data_as(C.c_void_p), C.byref(info))
+        finally:
+            os.chdir(cwd)
+        if info.value != 0:
+            raise RuntimeError(f"PaStiX analysis from saved files failed: {info.value}")
         self._bcsc_done = False
 
     def __del__(self):
@@ -302,3 +343,33 @@ def pastix_simple(A, facto: str, scheduler: str, b, nthreads: int = 1, refinemen
     return dict(rc=int(rc), x=x, L=Lf, U=Uf, fact_time=out[0], solve_time=out[1], refine_time=out[2],
                 threshold=out[3], nbpivots=int(out[4]), nbiter=int(out[5]), relative_error=out[6],
                 fact_gflops=out[7], anorm=out[8])
+
+
+def save_pastix_analysis(A, facto: str, path: str, nthreads: int = 1, iparm: dict | None = None) -> Analysis:
+    """PaStiX's analysis of A (grid nested dissection) run with IPARM_IO_STRATEGY =
+    PastixIOSave: PaStiX writes its symbolic factorization (pastixSymbolSave,
+    symbol/symbol_io.c:146) into a pastix-XXXXXX directory, and ``rh_analyze`` writes
+    the reordered ordering there in pastixOrderLoad's format (PaStiX's own
+    pastixOrderSave writes nothing in a single-process run, order/order_io.c:321).  Both
+    end in ``path`` under the names PaStiX's loaders read (``ordername``,
+    ``symbname``).  ``Analysis(A, facto, load_dir=path)`` -- or any PaStiX program run
+    there with PastixIOLoad -- starts from them.  Returns the analysis that wrote them."""
+    import shutil
+    path = os.path.abspath(path)
+    os.makedirs(path, exist_ok=True)
+    ip = dict(iparm or {})
+    ip["IO_STRATEGY"] = 2  # PastixIOSave
+    cwd = os.getcwd()
+    os.chdir(path)
+    try:
+        an = Analysis(A, facto, nthreads=nthreads, iparm=ip)
+        d = lib().rh_io_dir(an.h)
+    finally:
+        os.chdir(cwd)
+    if not d:
+        raise RuntimeError("PaStiX wrote no analysis files")
+    src = os.path.join(path, d.decode())
+    for gen, name in (("ordergen", "ordername"), ("symbgen", "symbname")):
+        shutil.move(os.path.join(src, gen), os.path.join(path, name))
+    shutil.rmtree(src, ignore_errors=True)
+    return an

@@ -20,6 +20,8 @@
 #include "common.h"
 #include "spm.h"
 #include "blend/solver.h"
+#include "graph/graph.h"
+#include "symbol/symbol.h"
 #include "bcsc/bcsc.h"
 #include "pastix/order.h"
 #include <string.h>
@@ -47,6 +49,8 @@ rh_analyze_schur( int64_t n, const int64_t *colptr, const int64_t *rowind, const
                   int mtxtype, int flttype, int facto, int64_t nx, int64_t ny, int64_t nz,
                   int nthreads, int verbose, int nkv, const int64_t *kv, int64_t nschur,
                   const int64_t *schur_list, int *info );
+
+int rh_write_order( const pastix_order_t *o, const char *path );
 
 void *
 rh_analyze( int64_t n, const int64_t *colptr, const int64_t *rowind, const void *values,
@@ -110,6 +114,14 @@ rh_analyze_schur( int64_t n, const int64_t *colptr, const int64_t *rowind, const
     if ( rc == PASTIX_SUCCESS ) rc = pastix_subtask_order( h->pastix_data, &h->spm, ord );
     if ( rc == PASTIX_SUCCESS ) rc = pastix_subtask_symbfact( h->pastix_data );
     if ( rc == PASTIX_SUCCESS ) rc = pastix_subtask_reordering( h->pastix_data );
+    if ( (rc == PASTIX_SUCCESS) && (h->iparm[IPARM_IO_STRATEGY] & PastixIOSave) &&
+         (h->pastix_data->dir_global != NULL) ) {
+        /* the reordered ordering, beside the symbol file the reordering step saved
+         * (before blend, which splits the ordering's column blocks) */
+        char path[4096];
+        snprintf( path, sizeof(path), "%s/ordergen", h->pastix_data->dir_global );
+        rc = rh_write_order( h->pastix_data->ordemesh, path );
+    }
     if ( rc == PASTIX_SUCCESS ) rc = pastix_subtask_blend( h->pastix_data );
     if ( ord ) {
         pastixOrderExit( ord );
@@ -119,10 +131,173 @@ rh_analyze_schur( int64_t n, const int64_t *colptr, const int64_t *rowind, const
     return h;
 }
 
+/* The symbolic-factorization step of an analysis loaded from files: what
+ * pastix_subtask_symbfact does under PastixIOLoad (symbol/pastix_subtask_symbfact.c:157-165,
+ * then :248-330), with two gaps of that path filled.  Its symbol structure is
+ * malloc'ed and never initialised (:150-155; pastixSymbolInit sets dof, schurfcol and
+ * the row tables), and pastixSymbolLoad (symbol/symbol_io.c:50-130) does not restore
+ * the blocks' lcblknm, which pastixSymbolCheck (symbol/symbol_check.c:88-95) and the
+ * solver build read.  Here the structure is initialised, lcblknm is set from the
+ * column blocks' block ranges and the Schur start from the graph, then the steps after
+ * the fax follow (rebase, row tables, selevtx, NNZ and flop counts, step bits). */
+static int
+rh_symbol_load( pastix_data_t *pd, const char *path )
+{
+    symbol_matrix_t *s;
+    FILE *f;
+    pastix_int_t k, b;
+
+    if ( !(pd->steps & STEP_ORDERING) || (pd->graph == NULL) || (pd->ordemesh == NULL) ) {
+        return PASTIX_ERR_BADPARAMETER;
+    }
+    pastixOrderBase( pd->ordemesh, 0 );
+    s = malloc( sizeof(symbol_matrix_t) );
+    pastixSymbolInit( NULL, NULL, s );
+    f = fopen( path, "r" );
+    if ( f == NULL ) {
+        free( s );
+        return PASTIX_ERR_FILE;
+    }
+    if ( pastixSymbolLoad( s, f ) != 0 ) {
+        fclose( f );
+        free( s );
+        return PASTIX_ERR_FILE;
+    }
+    fclose( f );
+    if ( s->nodenbr != pd->graph->gN ) {
+        pastixSymbolExit( s );
+        free( s );
+        return PASTIX_ERR_BADPARAMETER;
+    }
+    for ( k = 0; k < s->cblknbr; k++ ) {
+        for ( b = s->cblktab[k].bloknum; b < s->cblktab[k + 1].bloknum; b++ ) {
+            s->bloktab[b - s->baseval].lcblknm = k + s->baseval;
+        }
+    }
+    s->schurfcol = pd->graph->gN - pd->schur_n + s->baseval;
+    pastixSymbolBase( s, 0 );
+    pastixSymbolBuildRowtab( s );
+    pastixSymbolRealloc( s );
+    if ( pd->ordemesh->selevtx != NULL ) {
+        for ( k = 0; k < s->cblknbr; k++ ) {
+            s->cblktab[k].selevtx = pd->ordemesh->selevtx[k];
+        }
+    }
+    if ( pastixSymbolCheck( s ) != 0 ) {
+        pastixSymbolExit( s );
+        free( s );
+        return PASTIX_ERR_BADPARAMETER;
+    }
+    pd->symbmtx = s;
+    pd->iparm[IPARM_NNZEROS] = pastixSymbolGetNNZ( s );
+    pastixSymbolGetFlops( s, pd->iparm[IPARM_FLOAT], pd->iparm[IPARM_FACTORIZATION],
+                          &(pd->dparm[DPARM_FACT_THFLOPS]), &(pd->dparm[DPARM_FACT_RLFLOPS]) );
+    pd->steps &= ~( STEP_ANALYSE | STEP_CSC2BCSC | STEP_BCSC2CTAB | STEP_NUMFACT | STEP_SOLVE | STEP_REFINE );
+    pd->steps |= STEP_SYMBFACT;
+    return PASTIX_SUCCESS;
+}
+
+/* The analysis from PaStiX's own saved files: the working directory holds
+ * "ordername" and "symbname" as written by an analysis run with IPARM_IO_STRATEGY =
+ * PastixIOSave ("ordergen" and "symbgen" of its pastix-XXXXXX directory, renamed to
+ * the names the loaders read).  pastix_subtask_order loads the ordering
+ * (order/pastix_subtask_order.c:310-315), rh_symbol_load the symbol matrix, and blend
+ * builds the SolverMatrix; the reordering step is not run again, the saved
+ * ordering and symbol being the reordered ones (symbol/pastix_subtask_reordering.c:102-106).
+ * No ordering or symbolic factorization is computed. */
+void *
+rh_analyze_load( int64_t n, const int64_t *colptr, const int64_t *rowind, const void *values,
+                 int mtxtype, int flttype, int facto, int nthreads, int verbose, int nkv, const int64_t *kv,
+                 int *info )
+{
+    rh_t *h = calloc( 1, sizeof(rh_t) );
+    int64_t nnz = colptr[n] - colptr[0];
+    size_t  esz = (flttype == 2) ? sizeof(float) : sizeof(double);
+    int rc;
+
+    spmInit( &h->spm );
+    h->spm.mtxtype = (mtxtype == 0) ? SpmGeneral : SpmSymmetric;
+    h->spm.flttype = (flttype == 2) ? SpmFloat : SpmDouble;
+    h->spm.fmttype = SpmCSC;
+    h->spm.n       = n;
+    h->spm.nnz     = nnz;
+    h->spm.dof     = 1;
+    h->spm.colptr  = malloc( (n + 1) * sizeof(spm_int_t) );
+    h->spm.rowptr  = malloc( nnz * sizeof(spm_int_t) );
+    h->spm.values  = malloc( nnz * esz );
+    memcpy( h->spm.colptr, colptr, (n + 1) * sizeof(int64_t) );
+    memcpy( h->spm.rowptr, rowind, nnz * sizeof(int64_t) );
+    if ( values ) {
+        memcpy( h->spm.values, values, nnz * esz );
+    }
+    else {
+        memset( h->spm.values, 0, nnz * esz );
+    }
+    spmUpdateComputedFields( &h->spm );
+
+    pastixInitParam( h->iparm, h->dparm );
+    h->iparm[IPARM_VERBOSE]       = verbose ? PastixVerboseYes : PastixVerboseNot;
+    h->iparm[IPARM_FACTORIZATION] = facto;
+    h->iparm[IPARM_THREAD_NBR]    = nthreads > 0 ? nthreads : 1;
+    h->iparm[IPARM_ORDERING]      = PastixOrderPersonal;
+    for ( int i = 0; i < nkv; i++ ) {
+        h->iparm[kv[2 * i]] = kv[2 * i + 1];
+    }
+    h->iparm[IPARM_IO_STRATEGY] = PastixIOLoad;
+    pastixInit( &h->pastix_data, MPI_COMM_WORLD, h->iparm, h->dparm );
+    rc = pastix_subtask_order( h->pastix_data, &h->spm, NULL );
+    if ( rc == PASTIX_SUCCESS ) rc = rh_symbol_load( h->pastix_data, "symbname" );
+    if ( rc == PASTIX_SUCCESS ) rc = pastix_subtask_blend( h->pastix_data );
+    h->iparm[IPARM_IO_STRATEGY] = PastixIONo;
+    *info = rc;
+    return h;
+}
+
+/* Write an ordering (rangtab, permtab, treetab) to path in the text format
+ * pastixOrderLoad reads (order/order_io.c:40-110: version 1, cblknbr, vertnbr, then
+ * the three arrays).  PaStiX's own pastixOrderSave writes only when procnbr == 0
+ * (order/order_io.c:321), which never holds, so an analysis run with PastixIOSave
+ * leaves its symbol file but not its ordering; rh_analyze writes it instead. */
+int
+rh_write_order( const pastix_order_t *o, const char *path )
+{
+    FILE *f;
+    pastix_int_t i;
+    if ( (o == NULL) || (o->permtab == NULL) || (o->rangtab == NULL) || (o->treetab == NULL) ) {
+        return PASTIX_ERR_BADPARAMETER;
+    }
+    f = fopen( path, "w" );
+    if ( f == NULL ) {
+        return PASTIX_ERR_FILE;
+    }
+    fprintf( f, "1\n%ld\t%ld\n", (long)o->cblknbr, (long)o->vertnbr );
+    for ( i = 0; i <= o->cblknbr; i++ ) {
+        fprintf( f, "%ld%c", (long)o->rangtab[i], ((i & 7) == 7) ? '\n' : '\t' );
+    }
+    fputc( '\n', f );
+    for ( i = 0; i < o->vertnbr; i++ ) {
+        fprintf( f, "%ld%c", (long)o->permtab[i], ((i & 7) == 7) ? '\n' : '\t' );
+    }
+    fputc( '\n', f );
+    for ( i = 0; i < o->cblknbr; i++ ) {
+        fprintf( f, "%ld%c", (long)o->treetab[i], ((i & 7) == 7) ? '\n' : '\t' );
+    }
+    fputc( '\n', f );
+    return fclose( f ) == 0 ? PASTIX_SUCCESS : PASTIX_ERR_FILE;
+}
+
+/* The directory where an analysis run with PastixIOSave wrote its files (NULL if
+ * none). */
+const char *
+rh_io_dir( void *vh )
+{
+    return ((rh_t *)vh)->pastix_data->dir_global;
+}
+
 /* Index of the iparm/dparm entries a host program sets or reads, in a fixed
  * order: MIN_BLOCKSIZE, MAX_BLOCKSIZE, SCHEDULER, THREAD_NBR, TASKS2D_LEVEL,
  * REFINEMENT, ITERMAX, GMRES_IM, FACTORIZATION, NBITER, STATIC_PIVOTING,
- * NNZEROS, IPARM_SIZE | DPARM_EPSILON_REFINEMENT, DPARM_EPSILON_MAGN_CTRL,
+ * NNZEROS, IO_STRATEGY, IPARM_SIZE | DPARM_EPSILON_REFINEMENT, DPARM_EPSILON_MAGN_CTRL,
  * DPARM_A_NORM, DPARM_FACT_TIME, DPARM_SOLV_TIME, DPARM_REFINE_TIME,
  * DPARM_FACT_THFLOPS, DPARM_RELATIVE_ERROR, DPARM_SIZE. */
 void
@@ -131,7 +306,7 @@ rh_param_ids( int64_t *ids )
     int64_t v[] = { IPARM_MIN_BLOCKSIZE, IPARM_MAX_BLOCKSIZE, IPARM_SCHEDULER, IPARM_THREAD_NBR,
                     IPARM_TASKS2D_LEVEL, IPARM_REFINEMENT, IPARM_ITERMAX, IPARM_GMRES_IM,
                     IPARM_FACTORIZATION, IPARM_NBITER, IPARM_STATIC_PIVOTING, IPARM_NNZEROS,
-                    IPARM_SIZE,
+                    IPARM_IO_STRATEGY, IPARM_SIZE,
                     DPARM_EPSILON_REFINEMENT, DPARM_EPSILON_MAGN_CTRL, DPARM_A_NORM,
                     DPARM_FACT_TIME, DPARM_SOLV_TIME, DPARM_REFINE_TIME, DPARM_FACT_THFLOPS,
                     DPARM_RELATIVE_ERROR, DPARM_SIZE };
