@@ -62,7 +62,9 @@ def _pastix(A, b, flttype):
 
 def test_pastix_reruns_match_fixture():
     """PaStiX rerun here on one system it fails in FP32 (n = 12,544) and the
-    smallest recorded one: same pivot counts, same FP32 outcome, FP64 clean."""
+    smallest recorded one: the same FP32 pivot counts within 0.5 % (the FP32 pivots
+    that sit at the threshold flip with the BLAS kernels the host CPU selects), the
+    same FP32 outcome, FP64 clean."""
     d = fixture()
     by_side = sorted(d["systems"], key=lambda s: s["side"])
     failing = [s for s in d["systems"] if s["pastix_fp32"]["berr_after_refine"] > 1e-6]
@@ -70,7 +72,7 @@ def test_pastix_reruns_match_fixture():
         A = M.shifted_laplacian_2d(s["side"], s["sigma"])
         xt, b = M.rhs_from_xtrue(A, 1, seed=s["system"])
         st32, be32 = _pastix(A, b, 2)
-        assert st32["nbpivots"] == s["pastix_fp32"]["pivots"]
+        assert abs(st32["nbpivots"] - s["pastix_fp32"]["pivots"]) <= max(2, 0.005 * s["pastix_fp32"]["pivots"])
         assert (be32 > 1e-6) == (s["pastix_fp32"]["berr_after_refine"] > 1e-6)
         assert be32 == pytest.approx(s["pastix_fp32"]["berr_after_refine"], rel=0.5)
         st64, be64 = _pastix(A, b, 3)
