@@ -159,22 +159,6 @@ __device__ __forceinline__ void umma_commit(uint32_t bar) {
                  : "memory");
 }
 
-__device__ __forceinline__ int tc_dest_row(const DevSym &s, int k, int f, int prow) {
-    int lo = s.fblok[k], hi = s.fblok[k + 1] - 1;
-    while (lo < hi) {
-        const int mid = (lo + hi + 1) >> 1;
-        if (s.rowoff[mid] <= prow) lo = mid; else hi = mid - 1;
-    }
-    const int grow = s.frow[lo] + (prow - s.rowoff[lo]);
-    int flo = s.fblok[f], fhi = s.fblok[f + 1] - 1;
-    while (flo < fhi) {
-        const int mid = (flo + fhi + 1) >> 1;
-        if (s.frow[mid] <= grow) flo = mid; else fhi = mid - 1;
-    }
-    if (grow > s.lrow[flo]) return -1;
-    return s.rowoff[flo] + (grow - s.frow[flo]);
-}
-
 // Tile t of the launch from the host-built tile map {update, row tile | column
 // tile << 16} (tiles entirely above the diagonal of a symmetric update are not
 // listed): two loads instead of a search.
@@ -412,7 +396,7 @@ __global__ void __launch_bounds__(TC_THREADS, 1) update_tc_kernel(DevSym s, cons
             const Upd &u = tt.u;
             const int a = tl & 1;
             const int lr = tt.mt * TC_BM + row;
-            const int d = lr < u.M ? tc_dest_row(s, u.k, u.f, u.rowA0 + lr) : -1;
+            const int d = lr < u.M ? __ldg(s.rmap + u.rm0 + lr) : -1;  // destination row in f
             if (!mbar_wait(smem_addr(&tfull_bar[a]), (tl >> 1) & 1, &abort_sh)) {
                 abort_sh = 1;
                 break;
