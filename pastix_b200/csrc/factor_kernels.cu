@@ -72,145 +72,80 @@ __global__ void scatter_kernel(int64_t nnz, const int64_t *__restrict__ dest, co
 // ------------------------------------------------------------------ diagonal blocks
 
 
-// Unblocked factorization of a pb x pb tile by one warp, in shared memory (lane =
-// row); low register use for the many-CTA diagonal kernel.
+// Unblocked factorization of a pb x pb tile by one warp, held in registers: lane
+// i owns row i (r[j] = t[i][j]), columns are broadcast with warp shuffles.
 // POTRF: core_zpotf2sp (kernels/core_zpotrfsp.c:66-100)
 // GETRF: core_zgetf2sp (kernels/core_zgetrfsp.c:64-110)
 // SYTRF: core_zsytf2sp (kernels/core_zsytrfsp.c:63-103)
-template <typename T, int FACTO>
-__device__ void factor_tile_smem(T *t, int pb, int lane, double thr, int *piv, int *err) {
-    for (int c = 0; c < pb; c++) {
-        if (lane == 0) {
-            T d = t[c * (TP + 1)];
-            if (fabs((double)d) < thr) {
-                if (FACTO == FACTO_POTRF) d = (T)thr;
-                else d = (d < (T)0) ? (T)(-thr) : (T)thr;
-                (*piv)++;
-            }
-            if (FACTO == FACTO_POTRF) {
-                if (d < (T)0) { *err = 1; d = -d; }
-                d = sqrt(d);
-            }
-            t[c * (TP + 1)] = d;
-        }
-        __syncwarp();
-        const T d = t[c * (TP + 1)];
-        const T inv = (T)1 / d;
-        if (lane > c && lane < pb) {
-            const T v = t[lane + c * TP];
-            if (FACTO == FACTO_SYTRF) t[c + lane * TP] = v;  // D L^T copy in the upper part
-            t[lane + c * TP] = v * inv;
-        }
-        __syncwarp();
-        if (lane > c && lane < pb) {
-            const T lic = t[lane + c * TP];
-            if (FACTO == FACTO_GETRF) {
-                for (int j = c + 1; j < pb; j++) t[lane + j * TP] -= lic * t[c + j * TP];
-            } else if (FACTO == FACTO_POTRF) {
-                for (int j = c + 1; j <= lane; j++) t[lane + j * TP] -= lic * t[j + c * TP];
-            } else {
-                const T a = -d * lic;
-                for (int j = c + 1; j <= lane; j++) t[lane + j * TP] += a * t[j + c * TP];
-            }
-        }
-        __syncwarp();
-    }
-}
-
-// Inverse of the lower triangle of a pb x pb tile by one warp (lane = column of
-// the row being formed): W[i][i] = 1/T[i][i] (1 if unit), W[i][j] =
-// -(1/T[i][i]) sum_{j<=m<i} T[i][m] W[m][j], rows in order.  trans = 1 reads the
-// tile transposed (the lower triangle of T^T is the upper triangle of T).
-template <typename T>
-__device__ void invert_lower_tile_smem(const T *t, T *w, int pb, int lane, int unit, int trans) {
-    for (int i = 0; i < 32; i++) {
-        if (lane <= i) {
-            const int j = lane;
-            T v = 0;
-            if (i < pb) {
-                const T dii = unit ? (T)1 : (trans ? t[i * TP + i] : t[i + i * TP]);
-                if (j == i) {
-                    v = (T)1 / dii;
-                } else {
-                    T acc = 0;
-                    for (int m = j; m < i; m++) acc += (trans ? t[m + i * TP] : t[i + m * TP]) * w[m + j * TP];
-                    v = -acc / dii;
-                }
-            }
-            w[i + j * TP] = v;
-        } else {
-            w[i + lane * TP] = 0;
-        }
-        __syncwarp();
-    }
-}
-
-// Unblocked factorization of a pb x pb tile by one warp, held in registers: lane
-// i owns row i (r[j] = t[i][j]), columns are broadcast with warp shuffles.  Same
-// algorithm and pivot rule as factor_tile_smem; the reciprocal of each pivot comes
-// from rsqrt (POTRF) or one division computed beside the pivot, off the critical
-// path of the trailing updates.
+// The reciprocal of each pivot comes from rsqrt (POTRF) or one division computed
+// beside the pivot, off the critical path of the trailing updates.  Every register
+// index is a compile-time constant (static_for): a column loop left rolled by the
+// compiler would move r[] to local memory (four times slower on a 32 x 32 tile).
 template <typename T, int FACTO>
 __device__ void factor_tile(T *t, int pb, int lane, double thr, int *piv, int *err) {
     T r[32];
-#pragma unroll
-    for (int j = 0; j < 32; j++) r[j] = t[lane + j * TP];
+    static_for<32>([&](auto jj) {
+        constexpr int j = decltype(jj)::value;
+        r[j] = t[lane + j * TP];
+    });
     const bool row_in = lane < pb;
     // Columns >= pb run too (no branch, so the compiler can overlap consecutive
     // columns): they only touch padding rows (lane >= pb) and count nothing.
-#pragma unroll
-    for (int c = 0; c < 32; c++) {
-        {
-            const bool col_in = c < pb;
-            T a = __shfl_sync(0xffffffffu, r[c], c);
-            const bool rep = fabs((double)a) < thr;
-            if (rep) a = (FACTO == FACTO_POTRF) ? (T)thr : ((a < (T)0) ? (T)(-thr) : (T)thr);
-            bool neg = false;
-            T d, inv;
-            if (FACTO == FACTO_POTRF) {
-                if (a < (T)0) { neg = true; a = -a; }
-                d = sqrt(a);
-                inv = rsqrt(a);
-            } else {
-                d = a;
-                inv = (T)1 / a;
-            }
-            if (lane == 0 && col_in) {
-                if (rep) (*piv)++;
-                if (neg) *err = 1;
-            }
-            const bool below = lane > c && row_in;
-            if (lane == c) r[c] = d;
-            if (below) {
-                if (FACTO == FACTO_SYTRF) t[c + lane * TP] = r[c];  // D L^T copy in the upper part
-                r[c] *= inv;
-            }
-            const T li = r[c];
-            if (FACTO == FACTO_GETRF) {
-#pragma unroll
-                for (int j = c + 1; j < 32; j++) {
+    static_for<32>([&](auto cc) {
+        constexpr int c = decltype(cc)::value;
+        const bool col_in = c < pb;
+        T a = __shfl_sync(0xffffffffu, r[c], c);
+        const bool rep = fabs((double)a) < thr;
+        if (rep) a = (FACTO == FACTO_POTRF) ? (T)thr : ((a < (T)0) ? (T)(-thr) : (T)thr);
+        bool neg = false;
+        T d, inv;
+        if (FACTO == FACTO_POTRF) {
+            if (a < (T)0) { neg = true; a = -a; }
+            d = sqrt(a);
+            inv = rsqrt(a);
+        } else {
+            d = a;
+            inv = (T)1 / a;
+        }
+        if (lane == 0 && col_in) {
+            if (rep) (*piv)++;
+            if (neg) *err = 1;
+        }
+        const bool below = lane > c && row_in;
+        if (lane == c) r[c] = d;
+        if (below) {
+            if (FACTO == FACTO_SYTRF) t[c + lane * TP] = r[c];  // D L^T copy in the upper part
+            r[c] *= inv;
+        }
+        const T li = r[c];
+        if (FACTO == FACTO_GETRF) {
+            static_for<32>([&](auto jj) {
+                constexpr int j = decltype(jj)::value;
+                if constexpr (j > c) {
                     const T ucj = __shfl_sync(0xffffffffu, r[j], c);  // row c of U
                     if (below && j < pb) r[j] -= li * ucj;
                 }
-            } else {
-                const T m = (FACTO == FACTO_SYTRF) ? -d * li : li;
-#pragma unroll
-                for (int j = c + 1; j < 32; j++) {
+            });
+        } else {
+            const T m = (FACTO == FACTO_SYTRF) ? -d * li : li;
+            static_for<32>([&](auto jj) {
+                constexpr int j = decltype(jj)::value;
+                if constexpr (j > c) {
                     const T lj = __shfl_sync(0xffffffffu, r[c], j);  // l_j
                     if (below && j <= lane) {
                         if (FACTO == FACTO_SYTRF) r[j] += m * lj;
                         else r[j] -= m * lj;
                     }
                 }
-            }
+            });
         }
-    }
+    });
     __syncwarp();
-#pragma unroll
-    for (int j = 0; j < 32; j++) {
+    static_for<32>([&](auto jj) {
+        constexpr int j = decltype(jj)::value;
         // LDL^T keeps the D L^T copies of the upper part written above
         if (FACTO != FACTO_SYTRF || j <= lane) t[lane + j * TP] = r[j];
-    }
+    });
     __syncwarp();
 }
 
@@ -296,16 +231,19 @@ __device__ void warp_tile_update(float *A, int ld, int n, int p, int pb, int r0,
 }
 
 // One CTA (256 threads) factors the diagonal block of one cblk, blocked by 32
-// columns.  Per panel: one warp factors the 32x32 diagonal tile and a second
-// inverts it (lower, and for LU the upper triangle too); the rows (and, for LU,
+// columns.  Per panel: warp 0 factors the 32x32 diagonal tile in registers and then
+// inverts it (warp 1 inverts the upper triangle for LU); the rows (and, for LU,
 // columns) below the tile inside the diagonal block are solved as products with
 // those inverses; every warp then updates its own 32x32 tiles of the trailing
 // block (FP64 tensor cores for double).  The tile inverses are also stored in
 // tinv for the panel TRSM.  For LU the diagonal block of the U arena is first
 // added transposed into L (core_zgeadd) and afterwards receives the transposed
-// factor (core_zgetmo).
+// factor (core_zgetmo).  At most 128 registers per thread, so that two CTAs share an
+// SM: the levels of many 33-96 column cblks are latency-bound, and the second CTA's
+// warps cover the first one's single-warp tile steps (the spills this costs are
+// cheaper than the idle SMs).
 template <typename T, int FACTO>
-__global__ void __launch_bounds__(256) diag_factor_kernel(DevSym s, const int *__restrict__ cblks, T *L,
+__global__ void __launch_bounds__(256, 2) diag_factor_kernel(DevSym s, const int *__restrict__ cblks, T *L,
                                                           T *U, T *tinv, const int64_t *__restrict__ tinv_off,
                                                           const double *__restrict__ thr_ptr,
                                                           unsigned long long *npiv, int *err) {
@@ -337,10 +275,10 @@ __global__ void __launch_bounds__(256) diag_factor_kernel(DevSym s, const int *_
             tile[i + j * TP] = (i < pb && j < pb) ? Ap[i + (size_t)j * ld] : (T)0;
         }
         __syncthreads();
-        if (warp == 0) factor_tile_smem<T, FACTO>(tile, pb, lane, thr, &s_piv, &s_err);
+        if (warp == 0) factor_tile<T, FACTO>(tile, pb, lane, thr, &s_piv, &s_err);
         __syncthreads();
-        if (warp == 0) invert_lower_tile_smem<T>(tile, wl, pb, lane, FACTO != FACTO_POTRF, 0);
-        if (FACTO == FACTO_GETRF && warp == 1) invert_lower_tile_smem<T>(tile, wu, pb, lane, 0, 1);  // inv(U^T)
+        if (warp == 0) invert_lower_tile<T>(tile, wl, pb, lane, FACTO != FACTO_POTRF, 0);
+        if (FACTO == FACTO_GETRF && warp == 1) invert_lower_tile<T>(tile, wu, pb, lane, 0, 1);  // inv(U^T)
         __syncthreads();
         // store the factored tile and its inverse(s)
         for (int idx = tid; idx < 32 * 32; idx += nth) {

@@ -2,7 +2,21 @@
 // leading dimension TP (conflict-free column and row access).
 #pragma once
 
+#include <utility>
+
 namespace b200 {
+
+// f(std::integral_constant<int, I>) for I = 0 .. N-1, each index a compile-time
+// constant: register arrays indexed by it stay in registers whatever the unroller
+// decides (a loop that is not fully unrolled moves such arrays to local memory).
+template <typename F, int... Is>
+__device__ __forceinline__ void static_for_seq(F &&f, std::integer_sequence<int, Is...>) {
+    (f(std::integral_constant<int, Is>{}), ...);
+}
+template <int N, typename F>
+__device__ __forceinline__ void static_for(F &&f) {
+    static_for_seq(f, std::make_integer_sequence<int, N>{});
+}
 
 constexpr int TP = 33;  // padded leading dimension of 32x32 shared tiles
 
