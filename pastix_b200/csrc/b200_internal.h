@@ -36,7 +36,7 @@ struct DevSym {
     const int *csys;      // [cblknbr] system of each cblk of a batch; nullptr: one system
     const int64_t *rbase; // [cblknbr] first entry of cblk k in prow
     const int *prow;      // [sum of strides] global row of every panel row, cblk after cblk
-    const int *rmap;      // tensor-core updates: destination row in f of each row of the update (Upd::rm0)
+    const int *rmap;      // destination row in f of each row of every update (from Upd::rm0)
 };
 
 #ifdef __CUDACC__
@@ -77,7 +77,7 @@ struct Upd {
     int tile0;    // first tile index of this update inside its launch
     int flags;
     int nb;       // tensor-core updates: columns per tile (a multiple of 32, at most the launch's tile width)
-    int rm0;      // tensor-core updates: first entry of its row map (M entries: row rowA0 + i of k -> row of f, or -1)
+    int rm0;      // first entry of its row map (M entries: row rowA0 + i of k -> row of f, or -1)
 };
 
 // Off-diagonal row tile of a cblk panel (TRSM and solve tasks).

@@ -34,26 +34,6 @@ __device__ __forceinline__ void cp_async_commit() { asm volatile("cp.async.commi
 template <int N>
 __device__ __forceinline__ void cp_async_wait() { asm volatile("cp.async.wait_group %0;\n" ::"n"(N)); }
 
-// Panel row -> destination panel row in the facing cblk f.
-// Block i of k holds panel rows [rowoff[i], rowoff[i]+rows); its global rows
-// start at frow[i].  In f the global row lies in the block fb with
-// frow[fb] <= grow <= lrow[fb]  (is_block_inside_fblock, blend/solver.h:358).
-__device__ __forceinline__ int dest_row(const DevSym &s, int k, int f, int prow) {
-    int lo = s.fblok[k], hi = s.fblok[k + 1] - 1;
-    while (lo < hi) {
-        int mid = (lo + hi + 1) >> 1;
-        if (s.rowoff[mid] <= prow) lo = mid; else hi = mid - 1;
-    }
-    const int grow = s.frow[lo] + (prow - s.rowoff[lo]);
-    int flo = s.fblok[f], fhi = s.fblok[f + 1] - 1;
-    while (flo < fhi) {
-        int mid = (flo + fhi + 1) >> 1;
-        if (s.frow[mid] <= grow) flo = mid; else fhi = mid - 1;
-    }
-    if (grow > s.lrow[flo]) return -1;  // not in the structure of f (cannot happen for a valid symbol)
-    return s.rowoff[flo] + (grow - s.frow[flo]);
-}
-
 // ------------------------------------------------------------------ scatter
 
 template <typename T>
@@ -622,7 +602,7 @@ __global__ void __launch_bounds__(128) update_f64_kernel(DevSym s, const Upd *__
         }
     }
     cp_async_wait<0>();
-    if (tid < UT_M) drow[tid] = (m0 + tid < u.M) ? dest_row(s, k, u.f, u.rowA0 + m0 + tid) : -1;
+    if (tid < UT_M) drow[tid] = (m0 + tid < u.M) ? __ldg(s.rmap + u.rm0 + m0 + tid) : -1;
     __syncthreads();
     double *C = ((u.flags & UPD_C_U) ? U : L) + s.off[u.f];
     const int ldf = s.ld[u.f];
@@ -705,7 +685,7 @@ __global__ void __launch_bounds__(256) update_simt_f32_kernel(DevSym s, const Up
         }
         __syncthreads();
     }
-    if (tid < UT_M) drow[tid] = (m0 + tid < u.M) ? dest_row(s, k, u.f, u.rowA0 + m0 + tid) : -1;
+    if (tid < UT_M) drow[tid] = (m0 + tid < u.M) ? __ldg(s.rmap + u.rm0 + m0 + tid) : -1;
     __syncthreads();
     float *C = ((u.flags & UPD_C_U) ? U : L) + s.off[u.f];
     const int ldf = s.ld[u.f];
@@ -836,7 +816,7 @@ __global__ void __launch_bounds__(32 * US_WARPS) update_small_kernel(DevSym s, c
             const T dq = __shfl_sync(0xffffffffu, dk, q);
             a[q] = (in && q < u.K) ? Ap[i + (size_t)q * ldk] * dq : (T)0;
         }
-        const int d = in ? dest_row(s, k, u.f, u.rowA0 + i) : -1;
+        const int d = in ? __ldg(s.rmap + u.rm0 + i) : -1;
         T *crow = C + d + (size_t)u.colbase * ldf;
         for (int c = 0; c < u.N; c++) {
             T acc = 0;

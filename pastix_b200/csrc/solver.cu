@@ -284,11 +284,32 @@ int build_schedule(b200_solver_t *s) {
     std::vector<PanelCblk> pcbs;
     std::vector<PanelItem> pitems;
     std::vector<Upd> tcupds;
-    // destination rows of the tensor-core updates: for update u, entry u.rm0 + i is
-    // the panel row of f receiving row rowA0 + i of k (the block of f that contains
-    // it, core_zgemmsp_2d2d's facing-block walk, kernels/core_zgemmsp.c:420-440), so
-    // that the epilogue reads one entry instead of searching the block tables
+    // destination rows of the updates: for update u, entry u.rm0 + i is the panel row
+    // of f receiving row rowA0 + i of k (the block of f that contains it,
+    // is_block_inside_fblock, blend/solver.h:358, as core_zgemmsp_2d2d's facing-block
+    // walk, kernels/core_zgemmsp.c:420-440), so that
+    // the update kernels read one entry instead of searching the block tables
     std::vector<int> rmap;
+    auto map_rows = [&](Upd &u) -> bool {
+        if (rmap.size() + (size_t)u.M > (size_t)INT32_MAX) return false;
+        u.rm0 = (int)rmap.size();
+        rmap.resize(rmap.size() + u.M, -1);
+        int bf = s->fblok[u.f];
+        const int bfe = s->fblok[u.f + 1];
+        for (int b = s->fblok[u.k] + 1; b < s->fblok[u.k + 1]; b++) {
+            const int r0 = s->rowoff[b], nbr = s->lrow[b] - s->frow[b] + 1;
+            if (r0 + nbr <= u.rowA0) continue;
+            for (int t = 0; t < nbr; t++) {
+                const int prow = r0 + t, grow = s->frow[b] + t;
+                if (prow < u.rowA0) continue;
+                while (bf < bfe && s->lrow[bf] < grow) bf++;
+                int d = -1;
+                if (bf < bfe && grow >= s->frow[bf] && grow <= s->lrow[bf]) d = s->rowoff[bf] + (grow - s->frow[bf]);
+                rmap[(size_t)u.rm0 + (prow - u.rowA0)] = d;
+            }
+        }
+        return true;
+    };
     std::vector<int2> tcmap, tcmapw;  // tile maps of the 64- and 128-column tensor-core launches
     std::vector<Upd> smallupds;
     s->lvl_us0.assign(nlev, 0);
@@ -345,25 +366,7 @@ int build_schedule(b200_solver_t *s) {
                 (bn == 128 ? t0w : t0)++;
             }
         s->tc_wanted[u.k] = 1;
-        if (rmap.size() + (size_t)u.M > (size_t)INT32_MAX) return false;
-        u.rm0 = (int)rmap.size();
-        rmap.resize(rmap.size() + u.M, -1);
-        {
-            int bf = s->fblok[u.f];
-            const int bfe = s->fblok[u.f + 1];
-            for (int b = s->fblok[u.k] + 1; b < s->fblok[u.k + 1]; b++) {
-                const int r0 = s->rowoff[b], nbr = s->lrow[b] - s->frow[b] + 1;
-                if (r0 + nbr <= u.rowA0) continue;
-                for (int t = 0; t < nbr; t++) {
-                    const int prow = r0 + t, grow = s->frow[b] + t;
-                    if (prow < u.rowA0) continue;
-                    while (bf < bfe && s->lrow[bf] < grow) bf++;
-                    int d = -1;
-                    if (bf < bfe && grow >= s->frow[bf] && grow <= s->lrow[bf]) d = s->rowoff[bf] + (grow - s->frow[bf]);
-                    rmap[(size_t)u.rm0 + (prow - u.rowA0)] = d;
-                }
-            }
-        }
+        if (!map_rows(u)) return false;
         tcupds.push_back(u);
         return true;
     };
@@ -549,6 +552,7 @@ int build_schedule(b200_solver_t *s) {
                         ext_wanted[k] = 1;
                         continue;
                     }
+                    if (!map_rows(u)) return ERR_NOTIMPL;
                     if (u.K <= 16 && u.N <= 32) {
                         s->flops_kind[3] += upd_flops(u);
                         smallupds.push_back(u);
