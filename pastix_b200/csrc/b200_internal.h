@@ -117,7 +117,7 @@ struct PanelItem {
     int p, j, b;
 };
 
-// 32 x 32 tile of a panel copied to the row-major operand arena of the tensor-core
+// 64 x 64 tile of a panel copied to the row-major operand arena of the tensor-core
 // updates.
 struct SplitTask {
     int k;

@@ -580,8 +580,11 @@ int build_schedule(b200_solver_t *s) {
         for (int i = L.c0; i < L.c1; i++) {
             const int k = lvl_cblk[i];
             if (!ext_wanted[k]) continue;
-            for (int r0 = s->ncols[k]; r0 < s->stride[k]; r0 += 32)
-                for (int c0 = 0; c0 < s->ncols[k]; c0 += 32) splits.push_back({k, r0, c0});
+            // 64 x 64 tiles from the first off-diagonal row rounded down to a multiple
+            // of 4 (16-byte column loads; the few diagonal-block rows copied with them
+            // are never read by the updates)
+            for (int r0 = s->ncols[k] & ~3; r0 < s->stride[k]; r0 += 64)
+                for (int c0 = 0; c0 < s->ncols[k]; c0 += 64) splits.push_back({k, r0, c0});
         }
         s->lvl_sp1[l] = (int)splits.size();
         L.flops = flops;

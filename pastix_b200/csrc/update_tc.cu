@@ -177,46 +177,82 @@ __device__ __forceinline__ void tc_decode(const Upd *__restrict__ upds, const in
 
 // ---------------------------------------------------------------- operand copies
 
-__device__ __forceinline__ void split_store(float *dh, float *dl, size_t i, float x) {
-    if (dl) {
-        const float h = __uint_as_float(__float_as_uint(x) & 0xFFFFE000u);
-        dh[i] = h;
-        dl[i] = x - h;
-    } else {
-        dh[i] = x;
+// 16 bytes of one operand row (4 FP32 or 8 BF16 values), split into hi and lo and
+// stored as one vector each.
+__device__ __forceinline__ void split_store16(float *dh, float *dl, size_t i, const float (&x)[4]) {
+    float h[4], l[4];
+#pragma unroll
+    for (int j = 0; j < 4; j++) {
+        h[j] = dl ? __uint_as_float(__float_as_uint(x[j]) & 0xFFFFE000u) : x[j];
+        l[j] = x[j] - h[j];
     }
+    *reinterpret_cast<float4 *>(dh + i) = make_float4(h[0], h[1], h[2], h[3]);
+    if (dl) *reinterpret_cast<float4 *>(dl + i) = make_float4(l[0], l[1], l[2], l[3]);
 }
 
-__device__ __forceinline__ void split_store(__nv_bfloat16 *dh, __nv_bfloat16 *dl, size_t i, float x) {
-    const __nv_bfloat16 h = __float2bfloat16_rn(x);
-    dh[i] = h;
-    if (dl) dl[i] = __float2bfloat16_rn(x - __bfloat162float(h));
+__device__ __forceinline__ void split_store16(__nv_bfloat16 *dh, __nv_bfloat16 *dl, size_t i, const float (&x)[8]) {
+    __align__(16) __nv_bfloat16 h[8], l[8];
+#pragma unroll
+    for (int j = 0; j < 8; j++) {
+        h[j] = __float2bfloat16_rn(x[j]);
+        l[j] = __float2bfloat16_rn(x[j] - __bfloat162float(h[j]));
+    }
+    *reinterpret_cast<uint4 *>(dh + i) = *reinterpret_cast<const uint4 *>(h);
+    if (dl) *reinterpret_cast<uint4 *>(dl + i) = *reinterpret_cast<const uint4 *>(l);
 }
 
-// One 32 x 32 tile of a panel to the row-major operand arena(s) of element type E
-// (float for TF32 operands, BF16); the row pitch kp is ncols rounded up to 16 bytes.
+// One 64 x 64 tile of a panel (rows row0 .., a multiple of 4; columns col0 ..) to the
+// row-major operand arena(s) of element type E (float for TF32 operands, BF16); the row
+// pitch kp is ncols rounded up to 16 bytes, columns ncols .. kp - 1 written as zeros.
+// Loads: four consecutive rows of one column as one 16-byte vector (panels start on
+// 256-byte boundaries and their leading dimension is a multiple of 4); stores: 16 bytes
+// of one row per thread and part (4 FP32 or 8 BF16 columns), through a padded transpose.
 template <typename E>
 __global__ void __launch_bounds__(256) panel_split_kernel(DevSym s, const SplitTask *__restrict__ tasks,
                                                           const float *__restrict__ P,
                                                           const int64_t *__restrict__ toff, E *hi, E *lo) {
-    __shared__ float t[32][33];
+    __shared__ float t[64][65];  // t[column][row]
     constexpr int PAD = 16 / sizeof(E);
     const SplitTask tk = tasks[blockIdx.x];
-    const int k = tk.k, tx = threadIdx.x & 31, ty = threadIdx.x >> 5;
+    const int k = tk.k, tid = threadIdx.x;
     const int stride = s.stride[k], nc = s.ncols[k], ld = s.ld[k], kp = (nc + PAD - 1) / PAD * PAD;
     const float *src = P + s.off[k];
+    float4 v[4];
 #pragma unroll
-    for (int i = 0; i < 4; i++) {
-        const int r = tk.row0 + tx, c = tk.col0 + ty + 8 * i;
-        t[ty + 8 * i][tx] = (r < stride && c < nc) ? src[r + (size_t)c * ld] : 0.f;
+    for (int u = 0; u < 4; u++) {
+        const int idx = tid + 256 * u, r = tk.row0 + 4 * (idx & 15), c = tk.col0 + (idx >> 4);
+        const float *p = src + r + (size_t)c * ld;
+        if (c < nc && r + 3 < stride) {
+            v[u] = __ldg(reinterpret_cast<const float4 *>(p));
+        } else {
+            v[u].x = (c < nc && r < stride) ? p[0] : 0.f;
+            v[u].y = (c < nc && r + 1 < stride) ? p[1] : 0.f;
+            v[u].z = (c < nc && r + 2 < stride) ? p[2] : 0.f;
+            v[u].w = 0.f;
+        }
+    }
+#pragma unroll
+    for (int u = 0; u < 4; u++) {
+        const int idx = tid + 256 * u, r4 = 4 * (idx & 15), c = idx >> 4;
+        t[c][r4] = v[u].x;
+        t[c][r4 + 1] = v[u].y;
+        t[c][r4 + 2] = v[u].z;
+        t[c][r4 + 3] = v[u].w;
     }
     __syncthreads();
     E *dh = hi + toff[k];
     E *dl = lo ? lo + toff[k] : nullptr;
+    constexpr int VE = 16 / sizeof(E), G = 64 / VE;  // values per 16-byte unit, units per tile row
 #pragma unroll
-    for (int i = 0; i < 4; i++) {
-        const int r = tk.row0 + ty + 8 * i, c = tk.col0 + tx;
-        if (r < stride && c < kp) split_store(dh, dl, (size_t)r * kp + c, t[tx][ty + 8 * i]);
+    for (int u = 0; u < 64 * G / 256; u++) {
+        const int idx = tid + 256 * u, g = idx % G, rr = idx / G;
+        const int r = tk.row0 + rr, c0 = tk.col0 + VE * g;
+        if (r < stride && c0 < kp) {
+            float x[VE];
+#pragma unroll
+            for (int j = 0; j < VE; j++) x[j] = t[VE * g + j][rr];
+            split_store16(dh, dl, (size_t)r * kp + c0, x);
+        }
     }
 }
 
