@@ -693,6 +693,9 @@ int build_schedule(b200_solver_t *s) {
     {
         std::vector<int> small, big;
         for (int k = 0; k < cs; k++) (s->ncols[k] <= 32 && !is_big(k) ? small : big).push_back(k);
+        // widest first: their inverses take the longest, so they start before the many
+        // narrow ones instead of forming the launch's tail
+        std::stable_sort(big.begin(), big.end(), [&](int a, int b) { return s->ncols[a] > s->ncols[b]; });
         s->n_inv_small = (int)small.size();
         s->n_inv_big = (int)big.size();
         RET(s->dupload(&s->d_inv_small, small));
