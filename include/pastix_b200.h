@@ -51,8 +51,9 @@ enum { B200_FACTO_POTRF = 0, B200_FACTO_SYTRF = 1, B200_FACTO_GETRF = 2 };
 enum { B200_PREC_FP64 = 0, B200_PREC_FP32 = 1, B200_PREC_TF32 = 2, B200_PREC_TF32X3 = 3, B200_PREC_BF16X3 = 4 };
 
 /* Refinement methods, numbered as PaStiX's pastix_refine_t
- * (include/pastix/api.h, IPARM_REFINEMENT): GMRES, CG, simple refinement. */
-enum { B200_REFINE_GMRES = 0, B200_REFINE_CG = 1, B200_REFINE_SR = 2 };
+ * (include/pastix/api.h:241-246, IPARM_REFINEMENT): GMRES, CG, simple refinement,
+ * BiCGSTAB. */
+enum { B200_REFINE_GMRES = 0, B200_REFINE_CG = 1, B200_REFINE_SR = 2, B200_REFINE_BICGSTAB = 3 };
 
 /* The SolverMatrix integer structure (blend/solver.h:83-213), 0-based.
  * cblk arrays hold cblknbr+1 entries (the last is PaStiX's sentinel cblk, whose

@@ -19,7 +19,7 @@ from .refhost import BCSC, Analysis, SolverStructure
 
 DEFAULT_IPARM = {
     "FACTORIZATION": "potrf",   # IPARM_FACTORIZATION: potrf / sytrf / getrf
-    "REFINEMENT": "gmres",      # IPARM_REFINEMENT: gmres / cg / sr
+    "REFINEMENT": "gmres",      # IPARM_REFINEMENT: gmres / cg / sr / bicgstab
     "ITERMAX": 250,             # IPARM_ITERMAX
     "GMRES_IM": 25,             # IPARM_GMRES_IM
     "MIN_BLOCKSIZE": 160,       # IPARM_MIN_BLOCKSIZE

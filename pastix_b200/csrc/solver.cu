@@ -1305,6 +1305,76 @@ int refine_cg(RefineCtx &c, const double *b, double *x, int itermax, double eps,
     return ERR_SUCCESS;
 }
 
+// z_bicgstab_smp (refinement/z_refine_bicgstab.c:46-200): preconditioned
+// BiCGSTAB in PaStiX's order, three applications of the preconditioner per iteration
+// (to p, to s, and to t for the ratio w = (M^-1 t, M^-1 s) / (M^-1 t, M^-1 t)); every
+// right-hand side (every (column, system) of a batch) with its own scalars and
+// stopping rule, a stopped one kept unchanged by zero steps.
+int refine_bicgstab(RefineCtx &c, const double *b, double *x, int itermax, double eps, int64_t *niter,
+                    std::vector<double> &berr) {
+    const int n = c.n, R = c.np();
+    const size_t blk = (size_t)n * c.nrhs;
+    double *gr = c.ln->d_ws + 2 * blk, *gr2 = gr + blk, *gp = gr2 + blk, *gy = gp + blk, *gv = gy + blk;
+    double *gs = gv + blk, *gz = gs + blk, *gt = gz + blk, *g2 = gt + blk;
+    std::vector<double> nb, nr, vr2, rr2, v1, v2, alpha(R), w(R), beta(R);
+    RET(c.dots(b, b, nb));
+    for (auto &v : nb) v = std::sqrt(v);
+    c.copy(b, gr);  // r = b - A x
+    RET(c.spmv(x, gr, -1.0, 1.0));
+    RET(c.dots(gr, gr, nr));
+    c.copy(gr, gr2);
+    c.copy(gr, gp);
+    std::vector<double> resid(R), active(R, 1.0);
+    bool any = false;
+    for (int j = 0; j < R; j++) {
+        resid[j] = std::sqrt(nr[j]) / (nb[j] > 0 ? nb[j] : 1.0);
+        if (resid[j] > eps) any = true; else active[j] = 0.0;
+    }
+    int iter = 0;
+    while (any && iter < itermax) {
+        iter++;
+        c.copy(gp, gy);  // y = M^-1 p
+        RET(c.spsv(gy));
+        RET(c.spmv(gy, gv, 1.0, 0.0));  // v = A y
+        RET(c.dots(gv, gr2, vr2));      // alpha = (r, r2) / (v, r2)
+        RET(c.dots(gr, gr2, rr2));
+        for (int j = 0; j < R; j++) alpha[j] = (active[j] != 0.0 && vr2[j] != 0.0) ? rr2[j] / vr2[j] : 0.0;
+        RET(c.set_scal(alpha, 0));
+        c.copy(gr, gs);  // s = r - alpha v
+        c.axpys(0, -1.0, gv, gs);
+        c.copy(gs, gz);  // z = M^-1 s
+        RET(c.spsv(gz));
+        RET(c.spmv(gz, gt, 1.0, 0.0));  // t = A z
+        c.copy(gt, g2);                 // M^-1 t
+        RET(c.spsv(g2));
+        RET(c.dots(g2, gz, v1));
+        RET(c.dots(g2, g2, v2));
+        for (int j = 0; j < R; j++) w[j] = (active[j] != 0.0 && v2[j] != 0.0) ? v1[j] / v2[j] : 0.0;
+        RET(c.set_scal(alpha, 0));  // slot 0 again: dots() returns its results through it
+        c.axpys(0, 1.0, gy, x);     // x += alpha y + w z
+        RET(c.set_scal(w, 1));
+        c.axpys(1, 1.0, gz, x);
+        c.copy(gs, gr);  // r = s - w t
+        c.axpys(1, -1.0, gt, gr);
+        RET(c.dots(gr, gr2, v1));  // beta = (r', r2) / (r, r2) * (alpha / w)
+        for (int j = 0; j < R; j++)
+            beta[j] = (active[j] != 0.0 && rr2[j] != 0.0 && w[j] != 0.0) ? v1[j] / rr2[j] * (alpha[j] / w[j]) : 0.0;
+        c.axpys(1, -1.0, gv, gp);  // p = r + beta (p - w v)
+        RET(c.set_scal(beta, 0));
+        c.xpbys(gr, 0, gp);
+        RET(c.dots(gr, gr, nr));
+        any = false;
+        for (int j = 0; j < R; j++) {
+            if (active[j] == 0.0) continue;
+            resid[j] = std::sqrt(nr[j]) / (nb[j] > 0 ? nb[j] : 1.0);
+            if (resid[j] > eps) any = true; else active[j] = 0.0;
+        }
+    }
+    berr = resid;
+    *niter = iter;
+    return ERR_SUCCESS;
+}
+
 // z_gmres_smp (refinement/z_refine_gmres.c:46-352): right-preconditioned
 // restarted GMRES(im) with Givens rotations; the Gram-Schmidt projections of all
 // right-hand sides are computed together.
@@ -1418,6 +1488,7 @@ int refine_device(b200_solver_t *s, Lane *ln, int nrhs, const double *b, int64_t
     size_t need = 2 * blk;
     if (method == B200_REFINE_SR) need += 2 * blk;
     else if (method == B200_REFINE_CG) need += 4 * blk;
+    else if (method == B200_REFINE_BICGSTAB) need += 9 * blk;
     else need += (size_t)(2 * im + 1) * blk;
     const size_t aux_at = need;
     need += blk;  // scratch of the sweeps
@@ -1440,6 +1511,7 @@ int refine_device(b200_solver_t *s, Lane *ln, int nrhs, const double *b, int64_t
     int rc;
     if (method == B200_REFINE_SR) rc = refine_sr(c, bp, xp, (int)itermax, eps, &it, be);
     else if (method == B200_REFINE_CG) rc = refine_cg(c, bp, xp, (int)itermax, eps, &it, be);
+    else if (method == B200_REFINE_BICGSTAB) rc = refine_bicgstab(c, bp, xp, (int)itermax, eps, &it, be);
     else rc = refine_gmres(c, bp, xp, (int)itermax, (int)im, eps, &it, be);
     if (rc) return rc;
     launch_permute(n, nrhs, s->d_peri, xp, n, x, ldx, 0, st);
@@ -2290,7 +2362,7 @@ int b200_refine_device(b200_solver_t *s, int64_t nrhs, const double *d_b, int64_
                        int method, double eps, int64_t itermax, int64_t gmres_im, int64_t *niter, double *berr,
                        void *stream) {
     if (s && s->cblkschur < s->cblknbr) return ERR_BADPARAM;
-    if (!s || !s->factored || nrhs < 0 || ldb < s->n || ldx < s->n || method < 0 || method > 2) return ERR_BADPARAM;
+    if (!s || !s->factored || nrhs < 0 || ldb < s->n || ldx < s->n || method < 0 || method > 3) return ERR_BADPARAM;
     if (nrhs == 0) return ERR_SUCCESS;
     cudaStream_t st = stream ? (cudaStream_t)stream : s->st;
     auto t0 = std::chrono::steady_clock::now();

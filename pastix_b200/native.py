@@ -16,7 +16,7 @@ LIBPATH = os.path.join(HERE, "lib", "libpastix_b200.so")
 
 FACTO = {"potrf": 0, "sytrf": 1, "getrf": 2}
 PREC = {"fp64": 0, "fp32": 1, "tf32": 2, "tf32x3": 3, "bf16x3": 4}
-REFINE = {"gmres": 0, "cg": 1, "sr": 2}
+REFINE = {"gmres": 0, "cg": 1, "sr": 2, "bicgstab": 3}
 
 _P = C.c_void_p
 _I64 = C.c_int64

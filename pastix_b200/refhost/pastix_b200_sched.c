@@ -429,14 +429,14 @@ pastix_b200_task_refine( pastix_data_t *pastix_data, pastix_int_t n, pastix_int_
     if ( e == NULL ) {
         return PASTIX_ERR_BADPARAMETER;
     }
-    if ( (method != PastixRefineGMRES) && (method != PastixRefineCG) && (method != PastixRefineSR) ) {
-        errorPrint( "pastix_b200: refinement method %ld is not available on the B200 backend (GMRES, CG, SR)",
-                    (long)method );
-        return PASTIX_ERR_NOTIMPLEMENTED;
+    if ( (method != PastixRefineGMRES) && (method != PastixRefineCG) && (method != PastixRefineSR) &&
+         (method != PastixRefineBiCGSTAB) ) {
+        errorPrint( "pastix_b200: unknown refinement method %ld", (long)method );
+        return PASTIX_ERR_BADPARAMETER;
     }
     t0   = b200_wtime();
     berr = malloc( (nrhs > 0 ? nrhs : 1) * sizeof(double) );
-    /* GMRES = 0, CG = 1, SR = 2 in both enums (include/pastix/api.h:241-246) */
+    /* GMRES = 0, CG = 1, SR = 2, BiCGSTAB = 3 in both enums (include/pastix/api.h:241-246) */
     if ( pastix_data->bcsc->flttype == PastixFloat ) {
         rc = b200_refine_float( e->solver, nrhs, b, ldb, x, ldx, (int)method,
                                 pastix_data->dparm[DPARM_EPSILON_REFINEMENT], pastix_data->iparm[IPARM_ITERMAX],

@@ -160,6 +160,8 @@ def check_fp64_case(facto, make):
     ("potrf", lambda: M.laplacian(20, 20, 20, 7, 6.0), "sr"),
     ("getrf", lambda: M.convection_diffusion(16, 16, 16, seed=5), "gmres"),
     ("sytrf", lambda: M.shifted_laplacian_2d(40, 0.8), "gmres"),
+    ("getrf", lambda: M.convection_diffusion(16, 16, 16, seed=5), "bicgstab"),
+    ("potrf", lambda: M.laplacian(20, 20, 20, 27, 26.0, shift=1e-3), "bicgstab"),
 ])
 def test_fp32_factor_with_fp64_refinement(facto, make, method):
     A = make()

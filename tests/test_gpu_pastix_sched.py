@@ -66,7 +66,7 @@ def test_b200_scheduler_matches_sequential(facto, make, eps, refine):
     assert gpu["fact_time"] > 0 and gpu["fact_gflops"] > 0 and gpu["solve_time"] > 0
 
 
-@pytest.mark.parametrize("facto,make,eps,refine", [CASES[1], CASES[2]])
+@pytest.mark.parametrize("facto,make,eps,refine", [CASES[1], CASES[2], CASES[1][:3] + ("bicgstab",)])
 def test_b200_mixed_scheduler_refines_to_target(facto, make, eps, refine):
     A = make()
     xt, b = M.rhs_from_xtrue(A, 2, seed=12)
