@@ -46,3 +46,18 @@ def test_max_over_ranks_without_process_group():
     sys.path.insert(0, REPO)
     import bench
     assert bench.max_over_ranks([3, 4.5], None, "cpu") == [3.0, 4.5]
+
+
+def test_peaks_fall_back_when_file_absent(tmp_path, monkeypatch):
+    """Without a peaks file the roofline denominators are the labelled fallback;
+    with one, its figures are used as written."""
+    sys.path.insert(0, REPO)
+    import json
+    import bench
+    monkeypatch.setattr(bench, "REPO", str(tmp_path))
+    got = bench.measured_peaks()
+    assert got == bench.FALLBACK_PEAKS and got is not bench.FALLBACK_PEAKS
+    (tmp_path / "MEASURED_PEAKS.json").write_text(json.dumps({"hbm_gbs": 7000.0, "bf16_tflops": 1600.0}))
+    assert bench.measured_peaks() == {"hbm_gbs": 7000.0, "bf16_tflops": 1600.0}
+    (tmp_path / "MEASURED_PEAKS.json").write_text("{not json")
+    assert bench.measured_peaks()["source"] == "fallback"
