@@ -513,7 +513,8 @@ def main():
     achieved = dk["flops"] / (dk["ms"] * 1e-3) / 1e12 if dk["ms"] > 0 else 0.0
     kname = {"update": "update_f64_kernel" if head["prec"] == "fp64" else "update_simt_f32_kernel",
              "panel": "panel_kernel",
-             "tc_update": "update_tc_kernel<%d>" % (1 if head["prec"] == "tf32x3" else 0)}[dom]
+             "tc_update": "update_tc_kernel<%d>" % (1 if head["prec"] == "tf32x3" else 0),
+             "tree_bottom": "dag_bottom_kernel"}[dom]
     traffic = ncu_traffic(kname)
     roofline = {"bound": "tensor", "achieved": achieved, "peak": peak, "unit": "TFLOP/s",
                 "frac": (achieved / peak) if peak else None,

@@ -241,14 +241,17 @@ int b200_solve_trace( b200_solver_t *solver, int64_t nrhs, double *ms, double *b
  * factorizations of the wide cblks (diagonal block, panel solve and the updates
  * inside the panel, one launch per level), 5 inverses of the diagonal blocks,
  * 6 GEMM-scatter updates on the tensor cores, 7 the row-major operand copies they
- * read.  Returns the launch count (or a negative error code).
+ * read, 8 the tree-bottom launch (every cblk of the bottom levels, at most 32
+ * columns each: diagonal block, panel solve and updates, ordered by dependency
+ * counters instead of level by level).  Returns the launch count (or a negative
+ * error code).
  * Counterpart of PaStiX's kernel trace (kernels/kernels_trace.h). */
 int64_t b200_trace_launches( b200_solver_t *solver, double *ms, int32_t *cls, int64_t cap );
 
 /* Per-kind totals of the last b200_numfact_trace: ms[i] the device time and
  * flops[i] the algorithmic flops (useful products of the GEMM-scatter updates,
  * PaStiX's counting; panels: their diagonal and solve flops; 0 where not
- * counted) of kind i < min(nkinds, 8), kinds as
+ * counted; kind 8: its updates' useful products) of kind i < min(nkinds, 9), kinds as
  * in b200_trace_launches.  Returns the number of kinds filled.  Counterpart of
  * the per-kernel flop counters of kernels/kernels_trace.h. */
 int b200_trace_kinds( b200_solver_t *solver, double *ms, double *flops, int nkinds );

@@ -61,17 +61,18 @@ __global__ void scatter_kernel(int64_t nnz, const int64_t *__restrict__ dest, co
 // beside the pivot, off the critical path of the trailing updates.  Every register
 // index is a compile-time constant (static_for): a column loop left rolled by the
 // compiler would move r[] to local memory (four times slower on a 32 x 32 tile).
-template <typename T, int FACTO>
+// NB >= pb bounds the columns (8, 16 or 32): a narrow tile skips the padding.
+template <typename T, int FACTO, int NB = 32>
 __device__ void factor_tile(T *t, int pb, int lane, double thr, int *piv, int *err) {
-    T r[32];
-    static_for<32>([&](auto jj) {
+    T r[NB];
+    static_for<NB>([&](auto jj) {
         constexpr int j = decltype(jj)::value;
         r[j] = t[lane + j * TP];
     });
     const bool row_in = lane < pb;
     // Columns >= pb run too (no branch, so the compiler can overlap consecutive
     // columns): they only touch padding rows (lane >= pb) and count nothing.
-    static_for<32>([&](auto cc) {
+    static_for<NB>([&](auto cc) {
         constexpr int c = decltype(cc)::value;
         const bool col_in = c < pb;
         T a = __shfl_sync(0xffffffffu, r[c], c);
@@ -99,7 +100,7 @@ __device__ void factor_tile(T *t, int pb, int lane, double thr, int *piv, int *e
         }
         const T li = r[c];
         if (FACTO == FACTO_GETRF) {
-            static_for<32>([&](auto jj) {
+            static_for<NB>([&](auto jj) {
                 constexpr int j = decltype(jj)::value;
                 if constexpr (j > c) {
                     const T ucj = __shfl_sync(0xffffffffu, r[j], c);  // row c of U
@@ -108,7 +109,7 @@ __device__ void factor_tile(T *t, int pb, int lane, double thr, int *piv, int *e
             });
         } else {
             const T m = (FACTO == FACTO_SYTRF) ? -d * li : li;
-            static_for<32>([&](auto jj) {
+            static_for<NB>([&](auto jj) {
                 constexpr int j = decltype(jj)::value;
                 if constexpr (j > c) {
                     const T lj = __shfl_sync(0xffffffffu, r[c], j);  // l_j
@@ -121,7 +122,7 @@ __device__ void factor_tile(T *t, int pb, int lane, double thr, int *piv, int *e
         }
     });
     __syncwarp();
-    static_for<32>([&](auto jj) {
+    static_for<NB>([&](auto jj) {
         constexpr int j = decltype(jj)::value;
         // LDL^T keeps the D L^T copies of the upper part written above
         if (FACTO != FACTO_SYTRF || j <= lane) t[lane + j * TP] = r[j];
@@ -717,33 +718,68 @@ void launch_scatter(int64_t nnz, const int64_t *dest, const double *Lv, const do
     scatter_kernel<T><<<(unsigned)((nnz + bs - 1) / bs), bs, 0, st>>>(nnz, dest, Lv, Uv, L, U);
 }
 
-// Diagonal blocks of cblks with at most 32 columns, one warp per cblk (the bottom
-// levels of the tree hold tens of thousands): the single-panel case of
-// diag_factor_kernel -- geadd of U^T for LU, factor_tile, the tile inverse(s) for
-// the panel TRSM, write-back (and U^T for LU).
-constexpr int DS_WARPS = 4;
+constexpr int DS_WARPS = 4;  // warps (cblks) per CTA of diag_small_kernel
 
-template <typename T, int FACTO>
-__global__ void __launch_bounds__(32 * DS_WARPS) diag_small_kernel(DevSym s, const int *__restrict__ cblks, int ncblk,
-                                                                   T *L, T *U, T *tinv,
-                                                                   const int64_t *__restrict__ tinv_off,
-                                                                   const double *__restrict__ thr_ptr,
-                                                                   unsigned long long *npiv, int *err) {
-    extern __shared__ __align__(16) unsigned char ds_smem[];
-    const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
-    constexpr int NT = (FACTO == FACTO_GETRF) ? 3 : 2;
-    T *tile = reinterpret_cast<T *>(ds_smem) + (size_t)warp * NT * 32 * TP;
-    T *wl = tile + 32 * TP;
-    T *wu = wl + 32 * TP;
-    __shared__ int s_piv[DS_WARPS], s_err[DS_WARPS];
-    const int ci = blockIdx.x * DS_WARPS + warp;
-    if (ci >= ncblk) return;
-    const int k = cblks[ci];
+// Rows below the diagonal block of cblk k (at most 32 columns), lane = row: POTRF
+// X = A L^{-T} with the tile inverse wl; LU (lower side) and LDL^T by substitution
+// against the upper part of the factored tile (U; D L^T), dividing by its diagonal;
+// LU upper side (the transposed U panel) against the unit lower part.  NB >= ncols
+// (8, 16 or 32) bounds the columns.
+template <typename T, int FACTO, int NB>
+__device__ void small_trsm_warp(const DevSym &s, int k, T *L, T *U, const T *tile, const T *wl, int lane) {
+    const int n = s.ncols[k], ld = s.ld[k], stride = s.stride[k];
+    for (int side = 0; side < (FACTO == FACTO_GETRF ? 2 : 1); side++) {
+        T *P = (side ? U : L) + s.off[k];
+        for (int r0 = n; r0 < stride; r0 += 32) {
+            const int row = r0 + lane;
+            if (row >= stride) continue;
+            T *rp = P + row;
+            T a[NB];
+#pragma unroll
+            for (int c = 0; c < NB; c++) a[c] = (c < n) ? rp[(size_t)c * ld] : (T)0;
+            if (FACTO == FACTO_POTRF) {
+                // x_c = sum_{l <= c} a_l inv(L)[c][l], in place from the last column
+#pragma unroll
+                for (int c = NB - 1; c >= 0; c--) {
+                    if (c < n) {
+                        T v = 0;
+#pragma unroll
+                        for (int l = 0; l <= c; l++) v += a[l] * wl[c + l * TP];
+                        a[c] = v;
+                    }
+                }
+            } else {
+#pragma unroll
+                for (int c = 0; c < NB; c++) {
+                    if (c < n) {
+                        T v = a[c];
+#pragma unroll
+                        for (int l = 0; l < c; l++) v -= a[l] * (side ? tile[c + l * TP] : tile[l + c * TP]);
+                        a[c] = side ? v : v / tile[c * (TP + 1)];
+                    }
+                }
+            }
+#pragma unroll
+            for (int c = 0; c < NB; c++)
+                if (c < n) rp[(size_t)c * ld] = a[c];
+        }
+    }
+}
+
+// One warp factors the diagonal block of cblk k (at most NB <= 32 columns): tile,
+// wl and (LU) wu are the warp's shared-memory tiles of NB columns (pitch TP), *piv /
+// *ferr its counters in shared memory.  On return the factored tile is still in tile
+// (the panel solve, small_trsm_warp, reads it from there).
+template <typename T, int FACTO, int NB>
+__device__ __forceinline__ void small_diag_warp(const DevSym &s, int k, T *L, T *U, T *tinv,
+                                                const int64_t *__restrict__ tinv_off, const double *__restrict__ thr_ptr,
+                                                unsigned long long *npiv, int *err, T *tile, T *wl, T *wu, int *piv,
+                                                int *ferr, int lane) {
     const int n = s.ncols[k], ld = s.ld[k];
     const double thr = cblk_threshold(s, thr_ptr, k);
     T *A = L + s.off[k];
-    if (lane == 0) { s_piv[warp] = 0; s_err[warp] = 0; }
-    stage_n<32, T>(
+    if (lane == 0) { *piv = 0; *ferr = 0; }
+    stage_n<NB, T>(
         [&](int j) {
             T v = 0;
             if (lane < n && j < n) {
@@ -754,11 +790,11 @@ __global__ void __launch_bounds__(32 * DS_WARPS) diag_small_kernel(DevSym s, con
         },
         [&](int j, T v) { tile[lane + j * TP] = v; });
     __syncwarp();
-    factor_tile<T, FACTO>(tile, n, lane, thr, &s_piv[warp], &s_err[warp]);
-    invert_lower_tile<T>(tile, wl, n, lane, FACTO != FACTO_POTRF, 0);
-    if (FACTO == FACTO_GETRF) invert_lower_tile<T>(tile, wu, n, lane, 0, 1);  // inv(U^T)
+    factor_tile<T, FACTO, NB>(tile, n, lane, thr, piv, ferr);
+    invert_lower_tile<T, NB>(tile, wl, n, lane, FACTO != FACTO_POTRF, 0);
+    if (FACTO == FACTO_GETRF) invert_lower_tile<T, NB>(tile, wu, n, lane, 0, 1);  // inv(U^T)
     T *tp = tinv + tinv_off[k];
-    for (int idx = lane; idx < 32 * 32; idx += 32) {
+    for (int idx = lane; idx < 32 * NB; idx += 32) {
         const int i = idx & 31, j = idx >> 5;
         if (i < n && j < n && (FACTO != FACTO_POTRF || i >= j)) {
             A[i + (size_t)j * ld] = tile[i + j * TP];
@@ -771,9 +807,37 @@ __global__ void __launch_bounds__(32 * DS_WARPS) diag_small_kernel(DevSym s, con
     }
     __syncwarp();
     if (lane == 0) {
-        if (s_piv[warp]) atomicAdd(cblk_pivot_counter(s, npiv, k), (unsigned long long)s_piv[warp]);
-        if (s_err[warp]) atomicOr(err, 1);
+        if (*piv) atomicAdd(cblk_pivot_counter(s, npiv, k), (unsigned long long)*piv);
+        if (*ferr) atomicOr(err, 1);
     }
+}
+
+// Cblks with at most 32 columns, one warp per cblk (the bottom levels of the tree
+// hold tens of thousands): the single-panel case of diag_factor_kernel -- geadd of
+// U^T for LU, factor_tile, the tile inverse(s), write-back (and U^T for LU) -- and
+// the panel solve of the rows below (small_trsm_warp), so that these cblks need no
+// TRSM launch.  One instance per width class NB (8, 16, 32 columns): the narrow
+// classes, most of the cblks, need a fraction of the registers and shared memory, so
+// more warps share an SM.
+template <typename T, int FACTO, int NB>
+__global__ void __launch_bounds__(32 * DS_WARPS) diag_small_kernel(DevSym s, const int *__restrict__ cblks, int ncblk,
+                                                                   T *L, T *U, T *tinv,
+                                                                   const int64_t *__restrict__ tinv_off,
+                                                                   const double *__restrict__ thr_ptr,
+                                                                   unsigned long long *npiv, int *err) {
+    extern __shared__ __align__(16) unsigned char ds_smem[];
+    const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+    constexpr int NT = (FACTO == FACTO_GETRF) ? 3 : 2;
+    T *tile = reinterpret_cast<T *>(ds_smem) + (size_t)warp * NT * NB * TP;
+    T *wl = tile + NB * TP;
+    T *wu = wl + NB * TP;
+    __shared__ int s_piv[DS_WARPS], s_err[DS_WARPS];
+    const int ci = blockIdx.x * DS_WARPS + warp;
+    if (ci >= ncblk) return;
+    const int k = cblks[ci];
+    small_diag_warp<T, FACTO, NB>(s, k, L, U, tinv, tinv_off, thr_ptr, npiv, err, tile, wl, wu, &s_piv[warp],
+                                  &s_err[warp], lane);
+    small_trsm_warp<T, FACTO, NB>(s, k, L, U, tile, wl, lane);
 }
 
 // Small GEMM-scatter updates (K <= 16, N <= 32: the bottom levels of the tree,
@@ -847,6 +911,153 @@ __global__ void __launch_bounds__(32 * US_WARPS) update_small_kernel(DevSym s, c
     }
 }
 
+// ------------------------------------------------------------------ tree-bottom launch
+
+// The bottom levels of the elimination tree (every cblk of at most 32 columns, no
+// update on the tensor cores) in one launch, as PaStiX's dynamic scheduler runs
+// them: a cblk starts as soon as the cblks that update it are done, without level
+// barriers (cpucblk_zincoming_deps / cpucblk_zrelease_deps,
+// kernels/cpucblk_zmpi_coeftab.c:482-562; sequential_zpotrf.c's dynamic driver,
+// sopalin/sequential_zpotrf.c:129-234).  One warp per cblk, taken from an atomic
+// ticket in level order: the warp waits until the cblk's counter (the number of
+// updates it receives from the launch's cblks, ctrbcnt) is 0, factors the diagonal
+// block (small_diag_warp), solves the rows below it against the factored tile still
+// in shared memory (core_ztrsmsp, kernels/core_ztrsmsp.c:147-181), applies each of
+// its updates with atomics (the facing cblk may receive others at the same time;
+// core_zgemmsp_2d2d, kernels/core_zgemmsp.c:396-465) and decrements the facing
+// cblk's counter after each.  A warp only waits for cblks of earlier tickets, which
+// running warps hold, so the launch completes whatever the number of resident
+// warps.  Every wait is bounded: on expiry the warp sets bit 5 of err and an abort
+// word that ends the other warps' waits.
+constexpr int DG_WARPS = 4;
+constexpr long long DAG_WAIT_CYCLES = 1000000000LL;  // about 0.5 s at the maximum SM clock
+
+__device__ __forceinline__ int dag_ld_acquire(const int *p) {
+    int v;
+    asm volatile("ld.acquire.gpu.global.b32 %0, [%1];\n" : "=r"(v) : "l"(p) : "memory");
+    return v;
+}
+
+// Bounded wait (one lane) until *cnt <= 0; false on expiry or abort.
+__device__ bool dag_wait(const int *cnt, const int *abort_word) {
+    const long long t0 = clock64();
+    for (int it = 0;; it++) {
+        if (dag_ld_acquire(cnt) <= 0) return true;
+        if ((it & 15) == 15) {
+            if (dag_ld_acquire(abort_word)) return false;
+            if (clock64() - t0 > DAG_WAIT_CYCLES) return false;
+        }
+        __nanosleep(64);
+    }
+}
+
+// One update with K <= KB columns by one warp, every sum accumulated with atomics:
+// C[d(i)][colbase + c] -= sum_q A[i][q] (D_q) B[c][q] (c <= i when symmetric), B in
+// chunks of 32 rows staged in bs (32 x TP).
+template <typename T, int KB>
+__device__ void warp_update(const DevSym &s, const Upd &u, T *L, T *U, T *bs, int lane) {
+    const int k = u.k, ldk = s.ld[k];
+    const T *Ap = ((u.flags & UPD_A_U) ? U : L) + s.off[k] + u.rowA0 + (size_t)u.colK0 * ldk;
+    const T *Bp = ((u.flags & UPD_B_U) ? U : L) + s.off[k] + u.rowB0 + (size_t)u.colK0 * ldk;
+    const T *Dp = L + s.off[k] + (size_t)u.colK0 * (ldk + 1);
+    const bool scale = (u.flags & UPD_SCALE_D) != 0, sym = (u.flags & UPD_SYM) != 0;
+    T *C = ((u.flags & UPD_C_U) ? U : L) + s.off[u.f];
+    const int ldf = s.ld[u.f];
+    const T dk = (scale && lane < u.K) ? Dp[(size_t)lane * (ldk + 1)] : (T)1;
+    for (int n0 = 0; n0 < u.N; n0 += 32) {
+        const int nw = min(32, u.N - n0);
+        __syncwarp();
+#pragma unroll
+        for (int q = 0; q < KB; q++)
+            bs[lane * TP + q] = (lane < nw && q < u.K) ? Bp[(n0 + lane) + (size_t)q * ldk] : (T)0;
+        __syncwarp();
+        // symmetric: rows above n0 lie above the diagonal for every column of the chunk
+        for (int r0 = sym ? n0 : 0; r0 < u.M; r0 += 32) {
+            const int i = r0 + lane;
+            const bool in = i < u.M;
+            T a[KB];
+#pragma unroll
+            for (int q = 0; q < KB; q++) {
+                const T dq = __shfl_sync(0xffffffffu, dk, q);
+                a[q] = (in && q < u.K) ? Ap[i + (size_t)q * ldk] * dq : (T)0;
+            }
+            const int d = in ? __ldg(s.rmap + u.rm0 + i) : -1;
+            if (d < 0) continue;
+            T *crow = C + d + (size_t)(u.colbase + n0) * ldf;
+            for (int c = 0; c < nw; c++) {
+                T acc = 0;
+#pragma unroll
+                for (int q = 0; q < KB; q++) acc += a[q] * bs[c * TP + q];
+                if (!(sym && i < n0 + c)) atomicAdd(crow + (size_t)c * ldf, -acc);
+            }
+        }
+    }
+    __syncwarp();
+}
+
+template <typename T, int FACTO>
+__global__ void __launch_bounds__(32 * DG_WARPS) dag_bottom_kernel(DevSym s, const int *__restrict__ cblks,
+                                                                   int ncblk, const int *__restrict__ uoff,
+                                                                   const Upd *__restrict__ upds, int *cnt,
+                                                                   int *ticket, int *abort_word, T *L, T *U,
+                                                                   T *tinv, const int64_t *__restrict__ tinv_off,
+                                                                   const double *__restrict__ thr_ptr,
+                                                                   unsigned long long *npiv, int *err) {
+    extern __shared__ __align__(16) unsigned char dg_smem[];
+    const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+    constexpr int NT = (FACTO == FACTO_GETRF) ? 3 : 2;
+    T *tile = reinterpret_cast<T *>(dg_smem) + (size_t)warp * NT * 32 * TP;
+    T *wl = tile + 32 * TP;
+    T *wu = wl + 32 * TP;
+    __shared__ int s_piv[DG_WARPS], s_err[DG_WARPS];
+    for (;;) {
+        __syncwarp();
+        int t = 0;
+        if (lane == 0) t = atomicAdd(ticket, 1);
+        t = __shfl_sync(0xffffffffu, t, 0);
+        if (t >= ncblk) return;
+        const int k = cblks[t];
+        int ok = 1;
+        if (lane == 0) ok = dag_wait(cnt + k, abort_word);
+        ok = __shfl_sync(0xffffffffu, ok, 0);
+        if (!ok) {
+            if (lane == 0) {
+                atomicOr(err, 32);
+                atomicExch(abort_word, 1);
+            }
+            return;
+        }
+        __syncwarp();  // the other lanes' reads of k's panel come after lane 0's acquire
+        const int n = s.ncols[k];
+        if (n <= 8) {
+            small_diag_warp<T, FACTO, 8>(s, k, L, U, tinv, tinv_off, thr_ptr, npiv, err, tile, wl, wu, &s_piv[warp],
+                                         &s_err[warp], lane);
+            small_trsm_warp<T, FACTO, 8>(s, k, L, U, tile, wl, lane);
+        } else if (n <= 16) {
+            small_diag_warp<T, FACTO, 16>(s, k, L, U, tinv, tinv_off, thr_ptr, npiv, err, tile, wl, wu, &s_piv[warp],
+                                          &s_err[warp], lane);
+            small_trsm_warp<T, FACTO, 16>(s, k, L, U, tile, wl, lane);
+        } else {
+            small_diag_warp<T, FACTO, 32>(s, k, L, U, tinv, tinv_off, thr_ptr, npiv, err, tile, wl, wu, &s_piv[warp],
+                                          &s_err[warp], lane);
+            small_trsm_warp<T, FACTO, 32>(s, k, L, U, tile, wl, lane);
+        }
+        __syncwarp();  // the panel is final before any lane reads it for the updates
+        for (int q = uoff[t]; q < uoff[t + 1]; q++) {
+            const Upd u = upds[q];
+            if (n <= 8) warp_update<T, 8>(s, u, L, U, wl, lane);
+            else if (n <= 16) warp_update<T, 16>(s, u, L, U, wl, lane);
+            else warp_update<T, 32>(s, u, L, U, wl, lane);
+            __threadfence();  // this lane's contributions before the release below
+            __syncwarp();
+            if (lane == 0) {
+                __threadfence();
+                atomicSub(cnt + u.f, 1);
+            }
+        }
+    }
+}
+
 // pastixGetDiag / coeftab_zgetdiag (sopalin/diag.c:55, sopalin/coeftab_z.c:462-492):
 // the diagonal of every cblk's diagonal block in cblk order (the permuted
 // numbering): L_kk's diagonal for Cholesky, D for LDL^T, U_kk's for LU.
@@ -873,27 +1084,88 @@ void launch_update_small(const DevSym &s, const Upd *upds, int nupd, T *L, T *U,
 template void launch_update_small<double>(const DevSym &, const Upd *, int, double *, double *, cudaStream_t);
 template void launch_update_small<float>(const DevSym &, const Upd *, int, float *, float *, cudaStream_t);
 
+template <typename T, int NB>
+static void launch_diag_small_nb(int facto, const DevSym &s, const int *cblks, int ncblk, T *L, T *U, T *tinv,
+                                 const int64_t *tinv_off, const double *thr, unsigned long long *npiv, int *err,
+                                 cudaStream_t st) {
+    const int grid = (ncblk + DS_WARPS - 1) / DS_WARPS;
+    const size_t smem = (size_t)DS_WARPS * (facto == FACTO_GETRF ? 3 : 2) * NB * TP * sizeof(T);
+    if (facto == FACTO_POTRF)
+        diag_small_kernel<T, FACTO_POTRF, NB><<<grid, 32 * DS_WARPS, smem, st>>>(s, cblks, ncblk, L, U, tinv, tinv_off,
+                                                                               thr, npiv, err);
+    else if (facto == FACTO_GETRF)
+        diag_small_kernel<T, FACTO_GETRF, NB><<<grid, 32 * DS_WARPS, smem, st>>>(s, cblks, ncblk, L, U, tinv, tinv_off,
+                                                                               thr, npiv, err);
+    else
+        diag_small_kernel<T, FACTO_SYTRF, NB><<<grid, 32 * DS_WARPS, smem, st>>>(s, cblks, ncblk, L, U, tinv, tinv_off,
+                                                                               thr, npiv, err);
+}
+
 template <typename T>
-void launch_diag_small(int facto, const DevSym &s, const int *cblks, int ncblk, T *L, T *U, T *tinv,
+void launch_diag_small(int facto, const DevSym &s, const int *cblks, int ncblk, int nb, T *L, T *U, T *tinv,
                        const int64_t *tinv_off, const double *thr, unsigned long long *npiv, int *err,
                        cudaStream_t st) {
     if (ncblk <= 0) return;
-    const int grid = (ncblk + DS_WARPS - 1) / DS_WARPS;
-    const size_t smem = (size_t)DS_WARPS * (facto == FACTO_GETRF ? 3 : 2) * 32 * TP * sizeof(T);
-    if (facto == FACTO_POTRF)
-        diag_small_kernel<T, FACTO_POTRF><<<grid, 32 * DS_WARPS, smem, st>>>(s, cblks, ncblk, L, U, tinv, tinv_off, thr,
-                                                                           npiv, err);
-    else if (facto == FACTO_GETRF)
-        diag_small_kernel<T, FACTO_GETRF><<<grid, 32 * DS_WARPS, smem, st>>>(s, cblks, ncblk, L, U, tinv, tinv_off, thr,
-                                                                           npiv, err);
+    if (nb <= 8)
+        launch_diag_small_nb<T, 8>(facto, s, cblks, ncblk, L, U, tinv, tinv_off, thr, npiv, err, st);
+    else if (nb <= 16)
+        launch_diag_small_nb<T, 16>(facto, s, cblks, ncblk, L, U, tinv, tinv_off, thr, npiv, err, st);
     else
-        diag_small_kernel<T, FACTO_SYTRF><<<grid, 32 * DS_WARPS, smem, st>>>(s, cblks, ncblk, L, U, tinv, tinv_off, thr,
-                                                                           npiv, err);
+        launch_diag_small_nb<T, 32>(facto, s, cblks, ncblk, L, U, tinv, tinv_off, thr, npiv, err, st);
 }
-template void launch_diag_small<double>(int, const DevSym &, const int *, int, double *, double *, double *,
+template void launch_diag_small<double>(int, const DevSym &, const int *, int, int, double *, double *, double *,
                                         const int64_t *, const double *, unsigned long long *, int *, cudaStream_t);
-template void launch_diag_small<float>(int, const DevSym &, const int *, int, float *, float *, float *,
+template void launch_diag_small<float>(int, const DevSym &, const int *, int, int, float *, float *, float *,
                                        const int64_t *, const double *, unsigned long long *, int *, cudaStream_t);
+
+static size_t dag_bottom_smem(int facto, size_t esz) {
+    return (size_t)DG_WARPS * (facto == FACTO_GETRF ? 3 : 2) * 32 * TP * esz;
+}
+
+template <typename T>
+void launch_dag_bottom(int facto, const DevSym &s, int grid, const int *cblks, int ncblk, const int *uoff,
+                       const Upd *upds, int *cnt, int *ticket, int *abort_word, T *L, T *U, T *tinv,
+                       const int64_t *tinv_off, const double *thr, unsigned long long *npiv, int *err,
+                       cudaStream_t st) {
+    if (ncblk <= 0 || grid <= 0) return;
+    const size_t smem = dag_bottom_smem(facto, sizeof(T));
+    if (facto == FACTO_POTRF)
+        dag_bottom_kernel<T, FACTO_POTRF><<<grid, 32 * DG_WARPS, smem, st>>>(
+            s, cblks, ncblk, uoff, upds, cnt, ticket, abort_word, L, U, tinv, tinv_off, thr, npiv, err);
+    else if (facto == FACTO_GETRF)
+        dag_bottom_kernel<T, FACTO_GETRF><<<grid, 32 * DG_WARPS, smem, st>>>(
+            s, cblks, ncblk, uoff, upds, cnt, ticket, abort_word, L, U, tinv, tinv_off, thr, npiv, err);
+    else
+        dag_bottom_kernel<T, FACTO_SYTRF><<<grid, 32 * DG_WARPS, smem, st>>>(
+            s, cblks, ncblk, uoff, upds, cnt, ticket, abort_word, L, U, tinv, tinv_off, thr, npiv, err);
+}
+template void launch_dag_bottom<double>(int, const DevSym &, int, const int *, int, const int *, const Upd *, int *,
+                                        int *, int *, double *, double *, double *, const int64_t *, const double *,
+                                        unsigned long long *, int *, cudaStream_t);
+template void launch_dag_bottom<float>(int, const DevSym &, int, const int *, int, const int *, const Upd *, int *,
+                                       int *, int *, float *, float *, float *, const int64_t *, const double *,
+                                       unsigned long long *, int *, cudaStream_t);
+
+// Grid of the tree-bottom launch: the CTAs resident at once (more would only queue
+// behind them), at most one warp per cblk.
+int dag_bottom_grid(int facto, bool f32, int ncblk) {
+    if (ncblk <= 0) return 0;
+    int dev = 0, sms = 0, per_sm = 0;
+    cudaGetDevice(&dev);
+    cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
+    const size_t smem = dag_bottom_smem(facto, f32 ? 4 : 8);
+    cudaError_t e;
+    if (f32)
+        e = facto == FACTO_POTRF   ? cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, dag_bottom_kernel<float, FACTO_POTRF>, 32 * DG_WARPS, smem)
+            : facto == FACTO_GETRF ? cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, dag_bottom_kernel<float, FACTO_GETRF>, 32 * DG_WARPS, smem)
+                                   : cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, dag_bottom_kernel<float, FACTO_SYTRF>, 32 * DG_WARPS, smem);
+    else
+        e = facto == FACTO_POTRF   ? cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, dag_bottom_kernel<double, FACTO_POTRF>, 32 * DG_WARPS, smem)
+            : facto == FACTO_GETRF ? cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, dag_bottom_kernel<double, FACTO_GETRF>, 32 * DG_WARPS, smem)
+                                   : cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, dag_bottom_kernel<double, FACTO_SYTRF>, 32 * DG_WARPS, smem);
+    if (e != cudaSuccess || per_sm <= 0 || sms <= 0) return -1;
+    return std::min(per_sm * sms, (ncblk + DG_WARPS - 1) / DG_WARPS);
+}
 
 template <typename T>
 void launch_diag(int facto, const DevSym &s, const int *cblks, int ncblk, T *L, T *U, T *tinv,
@@ -942,13 +1214,29 @@ static int raise_smem(K kernel) {
     return dyn;
 }
 
+// every instance of one width class (GETRF in FP64 needs more than the default 48 KB
+// from 16 columns on)
+template <int NB>
+static int raise_diag_small_smem() {
+    if (raise_smem(diag_small_kernel<double, FACTO_POTRF, NB>) < 0 ||
+        raise_smem(diag_small_kernel<double, FACTO_SYTRF, NB>) < 0 ||
+        raise_smem(diag_small_kernel<double, FACTO_GETRF, NB>) < 0 ||
+        raise_smem(diag_small_kernel<float, FACTO_POTRF, NB>) < 0 ||
+        raise_smem(diag_small_kernel<float, FACTO_SYTRF, NB>) < 0 ||
+        raise_smem(diag_small_kernel<float, FACTO_GETRF, NB>) < 0)
+        return -1;
+    return 0;
+}
+
 int configure_factor_kernels() {
     int lim = 1 << 30;
     int v;
     if ((v = raise_smem(update_f64_kernel)) < UPD_F64_SMEM) return -1;
-    if (raise_smem(diag_small_kernel<double, FACTO_POTRF>) < 0 || raise_smem(diag_small_kernel<double, FACTO_SYTRF>) < 0 ||
-        raise_smem(diag_small_kernel<double, FACTO_GETRF>) < 0 || raise_smem(diag_small_kernel<float, FACTO_POTRF>) < 0 ||
-        raise_smem(diag_small_kernel<float, FACTO_SYTRF>) < 0 || raise_smem(diag_small_kernel<float, FACTO_GETRF>) < 0)
+    if (raise_diag_small_smem<8>() < 0 || raise_diag_small_smem<16>() < 0 || raise_diag_small_smem<32>() < 0)
+        return -1;
+    if (raise_smem(dag_bottom_kernel<double, FACTO_POTRF>) < 0 || raise_smem(dag_bottom_kernel<double, FACTO_SYTRF>) < 0 ||
+        raise_smem(dag_bottom_kernel<double, FACTO_GETRF>) < 0 || raise_smem(dag_bottom_kernel<float, FACTO_POTRF>) < 0 ||
+        raise_smem(dag_bottom_kernel<float, FACTO_SYTRF>) < 0 || raise_smem(dag_bottom_kernel<float, FACTO_GETRF>) < 0)
         return -1;
     if ((v = raise_smem(panel_trsm_kernel<double>)) < 0) return -1;
     lim = std::min(lim, v);

@@ -15,9 +15,10 @@ void launch_scatter(int64_t nnz, const int64_t *dest, const double *Lv, const do
 template <typename T>
 void launch_diag(int facto, const DevSym &s, const int *cblks, int ncblk, T *L, T *U, T *tinv,
                  const int64_t *tinv_off, const double *thr, unsigned long long *npiv, int *err, cudaStream_t st);
-// the same for cblks of at most 32 columns, one warp per cblk
+// the same for cblks of at most nb (8, 16 or 32) columns, one warp per cblk, with the
+// panel solve of their rows below (no TRSM task for them)
 template <typename T>
-void launch_diag_small(int facto, const DevSym &s, const int *cblks, int ncblk, T *L, T *U, T *tinv,
+void launch_diag_small(int facto, const DevSym &s, const int *cblks, int ncblk, int nb, T *L, T *U, T *tinv,
                        const int64_t *tinv_off, const double *thr, unsigned long long *npiv, int *err,
                        cudaStream_t st);
 // X op(T) = B: mode 0 upper / 1 lower-transposed for the left-looking part; which = 0 (inv L) or 1 (inv U^T)
@@ -53,6 +54,18 @@ void launch_update_f64(const DevSym &s, const Upd *upds, int nupd, int ntiles, d
                        cudaStream_t st);
 void launch_update_f32(const DevSym &s, const Upd *upds, int nupd, int ntiles, float *L, float *U,
                        cudaStream_t st);
+// the bottom levels of the tree in one launch (cblks of at most 32 columns, in level
+// order): one warp per cblk from *ticket, started when cnt[k] (the updates k receives
+// from the launch's cblks) reaches 0; uoff[t] .. uoff[t + 1] are the updates of the
+// t-th cblk, all accumulated with atomics.  cnt, *ticket and *abort_word are reset
+// before every factorization; a wait that runs out sets bit 5 of err.
+template <typename T>
+void launch_dag_bottom(int facto, const DevSym &s, int grid, const int *cblks, int ncblk, const int *uoff,
+                       const Upd *upds, int *cnt, int *ticket, int *abort_word, T *L, T *U, T *tinv,
+                       const int64_t *tinv_off, const double *thr, unsigned long long *npiv, int *err,
+                       cudaStream_t st);
+// its grid: the CTAs resident at once on this device, capped by the cblks (-1 on error)
+int dag_bottom_grid(int facto, bool f32, int ncblk);
 // returns the dynamic shared memory (bytes) the panel TRSM may use, or -1
 int configure_factor_kernels();
 // FP32 updates on the tensor cores (update_tc.cu).  Tiles of 128 rows x bn (64 or 128)

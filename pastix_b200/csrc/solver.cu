@@ -128,6 +128,18 @@ struct b200_solver_s {
     int n_inv_small = 0, n_inv_big = 0;
     std::vector<int> lvl_ds0, lvl_ds1;
     std::vector<int> lvl_dsm0, lvl_dsm1;  // cblks of <= 32 columns (one warp each)
+    std::vector<int> lvl_dsm8, lvl_dsm16; // ends of their <= 8 and <= 16 column classes
+    // tree-bottom launch: levels 0 .. dag_levels - 1 (every cblk of at most 32
+    // columns, no tensor-core update) factored in one launch by dependency counters
+    // instead of level by level, when the environment sets B200_TREE_DAG=1 and the
+    // tree has at least two such levels (off by default: at 80^3 it ran slower than
+    // the level launches it replaces, whose update kernels keep more warps in flight)
+    int dag_levels = 0, dag_ncblk = 0, dag_grid = 0;
+    int *d_dag_cblk = nullptr;   // the launch's cblks in level order (its ticket order)
+    int *d_dag_uoff = nullptr;   // [dag_ncblk + 1] first update of each
+    Upd *d_dag_upd = nullptr;
+    int *d_dag_cnt0 = nullptr;   // [cblknbr] updates each cblk receives from the launch's cblks
+    int *d_dag_cnt = nullptr;    // [cblknbr] working copy, then the ticket and the abort word
     // dataflow solve sweeps: items of the forward and backward launches, the facing
     // lists, and per cblk the counts that complete x (need_f / need_b) and aux
     // (nprev_f: diagonal items, nprev_b: off-diagonal items)
@@ -142,11 +154,13 @@ struct b200_solver_s {
     std::vector<int> lvl_prows;         // row-block form: rows of the blocks below the diagonal (0: tile items)
     std::vector<int> lvl_pns;           // most 64-column steps of a cblk of the level
     bool panel_steps_only = false;      // environment B200_PANEL_TILES=1: always the tile-item form
-    // failure-path tests (environment B200_TEST_WITHHOLD=panel|flow): the first item of
-    // every panel launch / of the forward dataflow sweep is never taken, so the waits
-    // that depend on it run out and the error path is exercised.  "panel" is read when
-    // the instance is created (the factorization graph is captured once); "flow" is
-    // read by every solve, so one instance can fail a solve and then run a good one
+    // failure-path tests (environment B200_TEST_WITHHOLD=panel|flow|dag): the first item
+    // of every panel launch / of the forward dataflow sweep is never taken, and the last
+    // cblk of the tree-bottom launch waits for one update more than it receives, so the
+    // waits that depend on them run out and the error path is exercised.  "panel" and
+    // "dag" are read when the instance is created (the factorization graph is captured
+    // once); "flow" is read by every solve, so one instance can fail a solve and then
+    // run a good one
     int test_withhold = 0;
     PanelCblk *d_pcb = nullptr;
     PanelItem *d_pitem = nullptr;
@@ -177,7 +191,8 @@ struct b200_solver_s {
     int64_t total_tiles = 0;
     int trsm_smem = 0;                  // dynamic shared memory available to the panel TRSM
     double flops_class[4] = {0, 0, 0, 0};  // algorithmic flops per kernel class (see Trace)
-    double flops_kind[8] = {};             // algorithmic flops of the kinds 3 (updates), 4 (panels), 6 (TC updates)
+    double flops_kind[9] = {};             // algorithmic flops of the kinds 3 (updates), 4 (panels), 6 (TC updates),
+                                           // 8 (the tree-bottom launch's updates)
     double bytes_scatter = 0;
 
     // bcsc
@@ -373,6 +388,8 @@ int build_schedule(b200_solver_t *s) {
     s->lvl_ds0.assign(nlev, 0);
     s->lvl_ds1.assign(nlev, 0);
     s->lvl_dsm0.assign(nlev, 0);
+    s->lvl_dsm8.assign(nlev, 0);
+    s->lvl_dsm16.assign(nlev, 0);
     s->lvl_dsm1.assign(nlev, 0);
     s->lvl_pi0.assign(nlev, 0);
     s->lvl_pi1.assign(nlev, 0);
@@ -393,6 +410,31 @@ int build_schedule(b200_solver_t *s) {
     s->levels.assign(nlev, Level{});
     s->lvl_tr.assign(nlev, 64);
     std::vector<int> src_count(N, 0), src_last(N, -1);
+    // the update of block j of cblk k (side 0; for LU side 1, the upper side, from the
+    // U panel rows below block j): false when the block has no such update
+    auto make_upd = [&](int k, int j, int side, int atomic, Upd &u) -> bool {
+        u = Upd{};
+        u.k = k;
+        u.j = j;
+        u.f = s->fcblk[j];
+        u.rowB0 = s->rowoff[j];
+        if (side == 0) {
+            u.rowA0 = s->rowoff[j];
+            u.flags = atomic;
+            if (s->facto != FACTO_GETRF) u.flags |= UPD_SYM;
+            if (s->facto == FACTO_SYTRF) u.flags |= UPD_SCALE_D;
+            if (s->facto == FACTO_GETRF) u.flags |= UPD_B_U;
+        } else {
+            if (j + 1 >= s->fblok[k + 1]) return false;
+            u.rowA0 = s->rowoff[j + 1];
+            u.flags = atomic | UPD_A_U | UPD_C_U;
+        }
+        u.M = s->stride[k] - u.rowA0;
+        u.N = s->lrow[j] - s->frow[j] + 1;
+        u.K = s->ncols[k];
+        u.colbase = s->frow[j] - s->fcol[u.f];
+        return true;
+    };
     const size_t trsm_smem = (size_t)s->trsm_smem;
     for (int l = 0; l < nlev; l++) {
         Level &L = s->levels[l];
@@ -418,9 +460,16 @@ int build_schedule(b200_solver_t *s) {
         for (int i = L.c0; i < L.c1; i++)
             if (!is_big(lvl_cblk[i]) && s->ncols[lvl_cblk[i]] > 32) diag_list.push_back(lvl_cblk[i]);
         s->lvl_ds1[l] = (int)diag_list.size();
+        // cblks of at most 32 columns by width class (8, 16, 32: one kernel instance each)
         s->lvl_dsm0[l] = (int)diag_list.size();
         for (int i = L.c0; i < L.c1; i++)
-            if (s->ncols[lvl_cblk[i]] <= 32) diag_list.push_back(lvl_cblk[i]);
+            if (s->ncols[lvl_cblk[i]] <= 8) diag_list.push_back(lvl_cblk[i]);
+        s->lvl_dsm8[l] = (int)diag_list.size();
+        for (int i = L.c0; i < L.c1; i++)
+            if (s->ncols[lvl_cblk[i]] > 8 && s->ncols[lvl_cblk[i]] <= 16) diag_list.push_back(lvl_cblk[i]);
+        s->lvl_dsm16[l] = (int)diag_list.size();
+        for (int i = L.c0; i < L.c1; i++)
+            if (s->ncols[lvl_cblk[i]] > 16 && s->ncols[lvl_cblk[i]] <= 32) diag_list.push_back(lvl_cblk[i]);
         s->lvl_dsm1[l] = (int)diag_list.size();
         {
             // wide cblks: items (step j, row block b >= j) of the level's panel launch,
@@ -470,7 +519,8 @@ int build_schedule(b200_solver_t *s) {
         s->lvl_lf0[l] = (int)leaf.size();
         for (int i = L.c0; i < L.c1; i++) {
             const int k = lvl_cblk[i];
-            if (!is_big(k))
+            // (cblks of at most 32 columns solve their rows in the one-warp diagonal kernel)
+            if (!is_big(k) && s->ncols[k] > 32)
                 for (int r0 = s->ncols[k]; r0 < s->stride[k]; r0 += TR) trsm.push_back({k, r0});
             if (s->ncols[k] <= 32) {
                 // small cblk: both parts of each sweep in the one-warp kernel
@@ -520,28 +570,9 @@ int build_schedule(b200_solver_t *s) {
             for (int j = s->fblok[k] + 1; j < s->fblok[k + 1]; j++) {
                 const int f = s->fcblk[j];
                 const int atomic = src_count[f] > 1 ? UPD_ATOMIC : 0;
-                const int nj = s->lrow[j] - s->frow[j] + 1;
                 for (int side = 0; side < (s->facto == FACTO_GETRF ? 2 : 1); side++) {
                     Upd u{};
-                    u.k = k;
-                    u.j = j;
-                    u.f = f;
-                    u.rowB0 = s->rowoff[j];
-                    if (side == 0) {
-                        u.rowA0 = s->rowoff[j];
-                        u.flags = atomic;
-                        if (s->facto != FACTO_GETRF) u.flags |= UPD_SYM;
-                        if (s->facto == FACTO_SYTRF) u.flags |= UPD_SCALE_D;
-                        if (s->facto == FACTO_GETRF) u.flags |= UPD_B_U;
-                    } else {
-                        if (j + 1 >= s->fblok[k + 1]) continue;
-                        u.rowA0 = s->rowoff[j + 1];
-                        u.flags = atomic | UPD_A_U | UPD_C_U;
-                    }
-                    u.M = s->stride[k] - u.rowA0;
-                    u.N = nj;
-                    u.K = nc;
-                    u.colbase = s->frow[j] - s->fcol[f];
+                    if (!make_upd(k, j, side, atomic, u)) continue;
                     // useful work: the lower triangle of the diagonal square for symmetric updates
                     const double mn = (u.flags & UPD_SYM) ? (double)u.N * (u.M - u.N) + 0.5 * u.N * (u.N + 1.0)
                                                           : (double)u.M * u.N;
@@ -598,6 +629,53 @@ int build_schedule(b200_solver_t *s) {
             }
         }
         s->nmax_all = std::max(s->nmax_all, L.nmax);
+    }
+    // tree-bottom launch: the first levels whose cblks all have at most 32 columns and
+    // whose updates all stay off the tensor cores, when there are at least two of them
+    {
+        bool on = false;
+        if (const char *e = getenv("B200_TREE_DAG")) on = atoi(e) != 0;
+        int lb = 0;
+        while (on && lb < nlev) {
+            const Level &L = s->levels[lb];
+            if (L.nmax > 32 || s->lvl_tc_tiles[lb] + s->lvl_tc_wtiles[lb] > 0 || s->lvl_sp1[lb] > s->lvl_sp0[lb] ||
+                s->lvl_pi1[lb] > s->lvl_pi0[lb] || s->lvl_ds1[lb] > s->lvl_ds0[lb])
+                break;
+            lb++;
+        }
+        const int ndag = lb >= 2 ? s->levels[lb - 1].c1 : 0;
+        const int grid = ndag > 0 ? dag_bottom_grid(s->facto, s->f32, ndag) : 0;
+        if (grid > 0) {
+            std::vector<int> dcblk, duoff;
+            std::vector<Upd> dupd;
+            std::vector<int> cnt0(N, 0);
+            for (int i = 0; i < ndag; i++) {
+                const int k = lvl_cblk[i];
+                dcblk.push_back(k);
+                duoff.push_back((int)dupd.size());
+                for (int j = s->fblok[k] + 1; j < s->fblok[k + 1]; j++)
+                    for (int side = 0; side < (s->facto == FACTO_GETRF ? 2 : 1); side++) {
+                        Upd u{};
+                        if (!make_upd(k, j, side, UPD_ATOMIC, u)) continue;
+                        if (!map_rows(u)) return ERR_NOTIMPL;
+                        // the same updates the level launches would have run on CUDA cores
+                        s->flops_kind[3] -= upd_flops(u);
+                        s->flops_kind[8] += upd_flops(u);
+                        dupd.push_back(u);
+                        cnt0[u.f]++;
+                    }
+            }
+            duoff.push_back((int)dupd.size());
+            if (s->test_withhold & 4) cnt0[dcblk.back()]++;  // an update that never comes
+            RET(s->dupload(&s->d_dag_cblk, dcblk));
+            RET(s->dupload(&s->d_dag_uoff, duoff));
+            RET(s->dupload(&s->d_dag_upd, dupd));
+            RET(s->dupload(&s->d_dag_cnt0, cnt0));
+            RET(s->dmalloc(&s->d_dag_cnt, (size_t)N + 2));
+            s->dag_levels = lb;
+            s->dag_ncblk = ndag;
+            s->dag_grid = grid;
+        }
     }
     RET(s->dupload(&s->d_lvl_cblk, lvl_cblk));
     RET(s->dupload(&s->d_trsm, trsm));
@@ -836,9 +914,11 @@ int ensure_scal(Lane *ln, int count) {
 // blocks, 2 panel TRSM, 3 GEMM-scatter updates.
 // Fine kernel kinds recorded in the per-launch detail; ids 0-3 are the classes
 // above, 4 panel factorizations of wide cblks, 5 diagonal-block inverses, 6 updates
-// on the tensor cores, 7 operand copies for them (summed into classes 1, 1, 3, 3).
+// on the tensor cores, 7 operand copies for them, 8 the tree-bottom launch (diagonal
+// blocks, panel solves and updates of the bottom levels) (summed into classes 1, 1,
+// 3, 3, 3).
 struct Trace {
-    static constexpr int NK = 8;
+    static constexpr int NK = 9;
     static int coarse(int c) { return c < 4 ? c : c < 6 ? 1 : 3; }
     std::vector<std::pair<cudaEvent_t, cudaEvent_t>> ev[NK];
     cudaEvent_t open = nullptr;
@@ -901,14 +981,32 @@ int enqueue_numfact(b200_solver_t *s, cudaStream_t st, Trace *tr = nullptr) {
     launch_scatter<T>(s->nnz, s->d_dest, s->d_Lv, s->d_Uv, L, U, st);
     if (tr) tr->end(0, st);
     launches++;
-    for (size_t l = 0; l < s->levels.size(); l++) {
+    if (s->dag_levels > 0) {
+        // the bottom levels in one launch, ordered by dependency counters
+        if (tr) tr->begin(st);
+        const int N = s->cblknbr;
+        CU(cudaMemcpyAsync(s->d_dag_cnt, s->d_dag_cnt0, (size_t)N * sizeof(int), cudaMemcpyDeviceToDevice, st));
+        CU(cudaMemsetAsync(s->d_dag_cnt + N, 0, 2 * sizeof(int), st));
+        launch_dag_bottom<T>(s->facto, s->ds, s->dag_grid, s->d_dag_cblk, s->dag_ncblk, s->d_dag_uoff, s->d_dag_upd,
+                             s->d_dag_cnt, s->d_dag_cnt + N, s->d_dag_cnt + N + 1, L, U, (T *)s->dTinv, s->d_toff,
+                             s->d_thr, s->d_npiv, s->d_err, st);
+        launches++;
+        if (tr) tr->end(8, st);
+    }
+    for (size_t l = (size_t)s->dag_levels; l < s->levels.size(); l++) {
         const Level &Lv = s->levels[l];
         if (tr) tr->begin(st);
         launch_diag<T>(s->facto, s->ds, s->d_diag_list + s->lvl_ds0[l], s->lvl_ds1[l] - s->lvl_ds0[l], L, U,
                        (T *)s->dTinv, s->d_toff, s->d_thr, s->d_npiv, s->d_err, st);
-        launch_diag_small<T>(s->facto, s->ds, s->d_diag_list + s->lvl_dsm0[l], s->lvl_dsm1[l] - s->lvl_dsm0[l], L, U,
-                             (T *)s->dTinv, s->d_toff, s->d_thr, s->d_npiv, s->d_err, st);
-        launches += (s->lvl_dsm1[l] > s->lvl_dsm0[l]);
+        {
+            const int b[4] = {s->lvl_dsm0[l], s->lvl_dsm8[l], s->lvl_dsm16[l], s->lvl_dsm1[l]};
+            const int nb[3] = {8, 16, 32};
+            for (int c = 0; c < 3; c++) {
+                launch_diag_small<T>(s->facto, s->ds, s->d_diag_list + b[c], b[c + 1] - b[c], nb[c], L, U,
+                                     (T *)s->dTinv, s->d_toff, s->d_thr, s->d_npiv, s->d_err, st);
+                launches += (b[c + 1] > b[c]);
+            }
+        }
         if (tr) tr->end(1, st);
         launches++;
         const int nt = Lv.t1 - Lv.t0;
@@ -1615,7 +1713,7 @@ int b200_solver_create_tuned(const b200_symbol_t *sym, int facto, int precision,
     s->panel_steps_only = s->tuning.panel_tiles != 0;
     if (const char *e = getenv("B200_PANEL_TILES")) s->panel_steps_only = atoi(e) != 0;
     if (const char *e = getenv("B200_TEST_WITHHOLD"))
-        s->test_withhold = !strcmp(e, "panel") ? 1 : !strcmp(e, "flow") ? 2 : 0;
+        s->test_withhold = !strcmp(e, "panel") ? 1 : !strcmp(e, "flow") ? 2 : !strcmp(e, "dag") ? 4 : 0;
     if (stream) {
         s->st = (cudaStream_t)stream;
     } else {
@@ -2133,6 +2231,7 @@ int b200_numfact(b200_solver_t *s, double epsilon_magn_ctrl, int64_t *nbpivots) 
     if (nbpivots) *nbpivots = (int64_t)piv;
     if (err & 2) fprintf(stderr, "pastix_b200: a tensor-core update timed out waiting for its operands\n");
     if (err & 8) fprintf(stderr, "pastix_b200: a panel factorization timed out waiting for a tile\n");
+    if (err & 32) fprintf(stderr, "pastix_b200: the tree-bottom launch timed out waiting for a cblk's updates\n");
     if (err & 1) fprintf(stderr, "pastix_b200: negative diagonal term in the Cholesky factorization\n");
     if (err) return ERR_INTERNAL;
     s->factored = true;
@@ -2190,7 +2289,7 @@ int b200_solve_trace(b200_solver_t *s, int64_t nrhs, double *ms, double *bytes) 
 
 int b200_trace_kinds(b200_solver_t *s, double *ms, double *flops, int nkinds) {
     if (!s || nkinds < 0) return -ERR_BADPARAM;
-    const int nk = std::min(nkinds, 8);
+    const int nk = std::min(nkinds, 9);
     for (int i = 0; i < nk; i++) {
         if (ms) ms[i] = 0.0;
         if (flops) flops[i] = s->flops_kind[i];

@@ -37,24 +37,31 @@ __device__ __forceinline__ void stage_n(Load load, Store store) {
 // / T[m][m] (T[m][m] = 1 if unit), with row m of T broadcast by warp shuffles and
 // the reciprocals of the diagonal formed first.  trans = 1 inverts the lower
 // triangle of T^T (the upper triangle of T read transposed).  Rows and columns
-// >= pb of W are zero.  Called by a whole warp.
-template <typename T>
+// >= pb of W are zero.  NB >= pb bounds the substitution (8, 16 or 32: narrow
+// tiles skip the columns that are padding); T is read and W written in their first
+// NB columns only (NB x TP elements each; W's rows 0..31).  Called by a whole warp.
+template <typename T, int NB = 32>
 __device__ void invert_lower_tile(const T *t, T *w, int pb, int lane, int unit, int trans) {
-    T r[32];  // row `lane` of the triangle to invert
+    T r[NB];  // row `lane` of the triangle to invert (lanes >= NB: padding, never read)
 #pragma unroll
-    for (int p = 0; p < 32; p++) r[p] = trans ? t[p + lane * TP] : t[lane + p * TP];
-    const T rd = unit ? (T)1 : (T)1 / r[lane];  // reciprocal of this lane's diagonal entry
-    T x[32];
+    for (int p = 0; p < NB; p++) r[p] = lane >= NB ? (T)0 : trans ? t[p + lane * TP] : t[lane + p * TP];
+    // reciprocal of this lane's diagonal entry (the same entry, transposed or not)
+    const T rd = (unit || lane >= pb) ? (T)1 : (T)1 / t[lane * (TP + 1)];
+    T x[NB];
 #pragma unroll
-    for (int m = 0; m < 32; m++) {
+    for (int m = 0; m < NB; m++) {
         T acc = (lane == m) ? (T)1 : (T)0;
 #pragma unroll
         for (int p = 0; p < m; p++) acc -= __shfl_sync(0xffffffffu, r[p], m) * x[p];
         const T rm = __shfl_sync(0xffffffffu, rd, m);
         x[m] = (m < pb && lane < pb) ? acc * rm : (T)0;
     }
+    if (lane < NB) {  // W has NB columns (pitch TP), its rows >= NB zero
 #pragma unroll
-    for (int m = 0; m < 32; m++) w[m + lane * TP] = x[m];
+        for (int m = 0; m < NB; m++) w[m + lane * TP] = x[m];
+#pragma unroll
+        for (int m = NB; m < 32; m++) w[m + lane * TP] = (T)0;
+    }
     __syncwarp();
 }
 

@@ -279,7 +279,7 @@ class Solver:
         lib().b200_trace_launches(self.h, _p(ms), _p(cls), cnt)
         return cls[:cnt], ms[:cnt]
 
-    KIND_NAMES = ["scatter", "diag", "trsm", "update", "panel", "inverse", "tc_update", "tc_split"]
+    KIND_NAMES = ["scatter", "diag", "trsm", "update", "panel", "inverse", "tc_update", "tc_split", "tree_bottom"]
 
     def trace_kinds(self) -> dict:
         """Per-kind device time and algorithmic flops of the last numfact trace."""

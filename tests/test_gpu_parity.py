@@ -129,6 +129,53 @@ def test_solve_sweep_forms(monkeypatch, flow_min, facto, make):
     s.close()
 
 
+TREE_KIND = native.Solver.KIND_NAMES.index("tree_bottom")
+
+
+@pytest.mark.parametrize("prec,facto,make", [("fp64",) + CASES[0], ("fp64",) + CASES[2], ("fp64",) + CASES[3],
+                                             ("fp64",) + CASES[6], ("fp32",) + CASES[0], ("fp32",) + CASES[2]])
+def test_tree_bottom_launch_matches_level_launches(monkeypatch, prec, facto, make):
+    """The bottom levels of the tree (cblks of at most 32 columns) in one launch
+    ordered by dependency counters (B200_TREE_DAG=1) give the factor of the
+    level-by-level launches (the default): the same replaced pivots, factors apart
+    by rounding only -- the atomics vary the summation order, and on the indefinite
+    2D LDL^T two FP64 summation orders land ~1e-12 apart, hence 1e-11 -- and the
+    oracle's pivots and backward error."""
+    A = make()
+    an = Analysis(A, facto)
+    st = an.structure()
+    bc = an.bcsc()
+    xt, b = M.rhs_from_xtrue(A, 3, seed=5)
+
+    def run(flag):
+        monkeypatch.setenv("B200_TREE_DAG", flag)
+        s = native.Solver(st, facto, prec)
+        s.bcsc_load(bc)
+        piv = s.numfact(0.0)
+        x = s.solve(b)
+        s.numfact_trace(0.0)
+        cls, _ = s.trace_launches()
+        launches = s.stats()["launches_numfact"]
+        Lg, Ug = s.factor()
+        thr = s.stats()["threshold"]
+        s.close()
+        return piv, thr, Lg, Ug, x, int(np.sum(cls == TREE_KIND)), launches
+
+    p1, thr, L1, U1, x1, n1, l1 = run("1")
+    p0, _, L0, U0, x0, n0, l0 = run("0")
+    assert (n1, n0) == (1, 0)
+    assert l1 < l0
+    assert p1 == p0
+    orc = oracle.Oracle(st)
+    assert factor_diff(orc, an.facto, L1, U1, L0, U0) <= (1e-11 if prec == "fp64" else 1e-4)
+    if prec == "fp64":
+        orc, L, U, opiv = oracle_factor(st, bc, an.facto, thr)
+        assert p1 == opiv
+        assert backward_error(A, x1, b).max() <= BERR_FP64
+    else:
+        assert np.linalg.norm(x1 - x0) / np.linalg.norm(x0) <= 1e-3
+
+
 def check_fp64_case(facto, make):
     A = make()
     an = Analysis(A, facto)
@@ -484,10 +531,10 @@ def test_schur_complement_and_solve_around_it(facto, make):
 
 
 def test_bounded_waits_report_errors(monkeypatch):
-    """The dependency-counter waits of the panel launches and of the dataflow sweeps
-    are bounded: with the first item withheld (a counter nothing raises), the launch
-    gives up within about a second, b200_numfact / b200_solve report the error, and a
-    fresh instance works."""
+    """The dependency-counter waits of the panel launches, of the tree-bottom launch
+    and of the dataflow sweeps are bounded: with an item withheld (a counter nothing
+    raises), the launch gives up within about a second, b200_numfact / b200_solve
+    report the error, and a fresh instance works."""
     import time
     A = M.laplacian(20, 20, 20, 7, 6.0)
     an = Analysis(A, "potrf")
@@ -495,6 +542,16 @@ def test_bounded_waits_report_errors(monkeypatch):
     bc = an.bcsc()
     assert np.max(st.cblk_lcolnum[:-1] - st.cblk_fcolnum[:-1] + 1) > 96  # wide cblks: panel launches
     xt, b = M.rhs_from_xtrue(A, 2, seed=4)
+    monkeypatch.setenv("B200_TEST_WITHHOLD", "dag")
+    monkeypatch.setenv("B200_TREE_DAG", "1")
+    s = native.Solver(st, "potrf", "fp64")
+    s.bcsc_load(bc)
+    t0 = time.perf_counter()
+    with pytest.raises(native.B200Error):
+        s.numfact(0.0)
+    assert time.perf_counter() - t0 < 30.0
+    s.close()
+    monkeypatch.delenv("B200_TREE_DAG")
     monkeypatch.setenv("B200_TEST_WITHHOLD", "panel")
     s = native.Solver(st, "potrf", "fp64")
     s.bcsc_load(bc)
