@@ -80,6 +80,14 @@ struct Upd {
     int rm0;      // first entry of its row map (M entries: row rowA0 + i of k -> row of f, or -1)
 };
 
+// Item of the tree-bottom launch, in ticket order: fact = 1 factors cblk k (diagonal
+// block and panel solve) once its counter is 0, then marks it factored; fact = 0 waits
+// for that mark.  Either then applies updates q0 .. q1 - 1 of the launch's list, on the
+// rows [r0, r1) of their M-range (one update split by rows, or whole updates).
+struct DagItem {
+    int k, q0, q1, r0, r1, fact;
+};
+
 // Off-diagonal row tile of a cblk panel (TRSM and solve tasks).
 struct RowTask {
     int k;

@@ -918,17 +918,19 @@ __global__ void __launch_bounds__(32 * US_WARPS) update_small_kernel(DevSym s, c
 // them: a cblk starts as soon as the cblks that update it are done, without level
 // barriers (cpucblk_zincoming_deps / cpucblk_zrelease_deps,
 // kernels/cpucblk_zmpi_coeftab.c:482-562; sequential_zpotrf.c's dynamic driver,
-// sopalin/sequential_zpotrf.c:129-234).  One warp per cblk, taken from an atomic
-// ticket in level order: the warp waits until the cblk's counter (the number of
-// updates it receives from the launch's cblks, ctrbcnt) is 0, factors the diagonal
-// block (small_diag_warp), solves the rows below it against the factored tile still
-// in shared memory (core_ztrsmsp, kernels/core_ztrsmsp.c:147-181), applies each of
-// its updates with atomics (the facing cblk may receive others at the same time;
-// core_zgemmsp_2d2d, kernels/core_zgemmsp.c:396-465) and decrements the facing
-// cblk's counter after each.  A warp only waits for cblks of earlier tickets, which
-// running warps hold, so the launch completes whatever the number of resident
-// warps.  Every wait is bounded: on expiry the warp sets bit 5 of err and an abort
-// word that ends the other warps' waits.
+// sopalin/sequential_zpotrf.c:129-234).  Items (DagItem) are taken by warps from an
+// atomic ticket, level by level: the level's factor items, then its update items.  A
+// factor item waits until its cblk's counter (the update items it receives from the
+// launch's cblks, ctrbcnt) is 0, factors the diagonal block (small_diag_warp), solves
+// the rows below it against the factored tile still in shared memory (core_ztrsmsp,
+// kernels/core_ztrsmsp.c:147-181), runs the cblk's updates itself when they are few,
+// and marks the cblk factored (counter -1).  An update item waits for that mark and
+// applies its updates (or rows of one) with atomics, the facing cblk receiving
+// others at the same time (core_zgemmsp_2d2d, kernels/core_zgemmsp.c:396-465); every
+// item then decrements the facing cblks' counters, once per update.  An item only
+// waits for earlier items, which running warps hold, so the launch completes whatever
+// the number of resident warps.  Every wait is bounded: on expiry the warp sets bit 5
+// of err and an abort word that ends the other warps' waits.
 constexpr int DG_WARPS = 4;
 constexpr long long DAG_WAIT_CYCLES = 1000000000LL;  // about 0.5 s at the maximum SM clock
 
@@ -938,11 +940,11 @@ __device__ __forceinline__ int dag_ld_acquire(const int *p) {
     return v;
 }
 
-// Bounded wait (one lane) until *cnt <= 0; false on expiry or abort.
-__device__ bool dag_wait(const int *cnt, const int *abort_word) {
+// Bounded wait (one lane) until *cnt <= target; false on expiry or abort.
+__device__ bool dag_wait(const int *cnt, int target, const int *abort_word) {
     const long long t0 = clock64();
     for (int it = 0;; it++) {
-        if (dag_ld_acquire(cnt) <= 0) return true;
+        if (dag_ld_acquire(cnt) <= target) return true;
         if ((it & 15) == 15) {
             if (dag_ld_acquire(abort_word)) return false;
             if (clock64() - t0 > DAG_WAIT_CYCLES) return false;
@@ -951,11 +953,12 @@ __device__ bool dag_wait(const int *cnt, const int *abort_word) {
     }
 }
 
-// One update with K <= KB columns by one warp, every sum accumulated with atomics:
+// One update with K <= KB columns by one warp on the rows [rb, re) of its M-range
+// (rb a multiple of 32), every sum accumulated with atomics:
 // C[d(i)][colbase + c] -= sum_q A[i][q] (D_q) B[c][q] (c <= i when symmetric), B in
 // chunks of 32 rows staged in bs (32 x TP).
 template <typename T, int KB>
-__device__ void warp_update(const DevSym &s, const Upd &u, T *L, T *U, T *bs, int lane) {
+__device__ void warp_update(const DevSym &s, const Upd &u, T *L, T *U, T *bs, int lane, int rb, int re) {
     const int k = u.k, ldk = s.ld[k];
     const T *Ap = ((u.flags & UPD_A_U) ? U : L) + s.off[k] + u.rowA0 + (size_t)u.colK0 * ldk;
     const T *Bp = ((u.flags & UPD_B_U) ? U : L) + s.off[k] + u.rowB0 + (size_t)u.colK0 * ldk;
@@ -972,9 +975,10 @@ __device__ void warp_update(const DevSym &s, const Upd &u, T *L, T *U, T *bs, in
             bs[lane * TP + q] = (lane < nw && q < u.K) ? Bp[(n0 + lane) + (size_t)q * ldk] : (T)0;
         __syncwarp();
         // symmetric: rows above n0 lie above the diagonal for every column of the chunk
-        for (int r0 = sym ? n0 : 0; r0 < u.M; r0 += 32) {
+        const int rend = min(u.M, re);
+        for (int r0 = sym ? max(n0, rb) : rb; r0 < rend; r0 += 32) {
             const int i = r0 + lane;
-            const bool in = i < u.M;
+            const bool in = i < rend;
             T a[KB];
 #pragma unroll
             for (int q = 0; q < KB; q++) {
@@ -996,9 +1000,8 @@ __device__ void warp_update(const DevSym &s, const Upd &u, T *L, T *U, T *bs, in
 }
 
 template <typename T, int FACTO>
-__global__ void __launch_bounds__(32 * DG_WARPS) dag_bottom_kernel(DevSym s, const int *__restrict__ cblks,
-                                                                   int ncblk, const int *__restrict__ uoff,
-                                                                   const Upd *__restrict__ upds, int *cnt,
+__global__ void __launch_bounds__(32 * DG_WARPS) dag_bottom_kernel(DevSym s, const DagItem *__restrict__ items,
+                                                                   int nitems, const Upd *__restrict__ upds, int *cnt,
                                                                    int *ticket, int *abort_word, T *L, T *U,
                                                                    T *tinv, const int64_t *__restrict__ tinv_off,
                                                                    const double *__restrict__ thr_ptr,
@@ -1015,10 +1018,11 @@ __global__ void __launch_bounds__(32 * DG_WARPS) dag_bottom_kernel(DevSym s, con
         int t = 0;
         if (lane == 0) t = atomicAdd(ticket, 1);
         t = __shfl_sync(0xffffffffu, t, 0);
-        if (t >= ncblk) return;
-        const int k = cblks[t];
+        if (t >= nitems) return;
+        const DagItem it = items[t];
+        const int k = it.k;
         int ok = 1;
-        if (lane == 0) ok = dag_wait(cnt + k, abort_word);
+        if (lane == 0) ok = dag_wait(cnt + k, it.fact ? 0 : -1, abort_word);
         ok = __shfl_sync(0xffffffffu, ok, 0);
         if (!ok) {
             if (lane == 0) {
@@ -1029,30 +1033,35 @@ __global__ void __launch_bounds__(32 * DG_WARPS) dag_bottom_kernel(DevSym s, con
         }
         __syncwarp();  // the other lanes' reads of k's panel come after lane 0's acquire
         const int n = s.ncols[k];
-        if (n <= 8) {
-            small_diag_warp<T, FACTO, 8>(s, k, L, U, tinv, tinv_off, thr_ptr, npiv, err, tile, wl, wu, &s_piv[warp],
-                                         &s_err[warp], lane);
-            small_trsm_warp<T, FACTO, 8>(s, k, L, U, tile, wl, lane);
-        } else if (n <= 16) {
-            small_diag_warp<T, FACTO, 16>(s, k, L, U, tinv, tinv_off, thr_ptr, npiv, err, tile, wl, wu, &s_piv[warp],
-                                          &s_err[warp], lane);
-            small_trsm_warp<T, FACTO, 16>(s, k, L, U, tile, wl, lane);
-        } else {
-            small_diag_warp<T, FACTO, 32>(s, k, L, U, tinv, tinv_off, thr_ptr, npiv, err, tile, wl, wu, &s_piv[warp],
-                                          &s_err[warp], lane);
-            small_trsm_warp<T, FACTO, 32>(s, k, L, U, tile, wl, lane);
+        if (it.fact) {
+            if (n <= 8) {
+                small_diag_warp<T, FACTO, 8>(s, k, L, U, tinv, tinv_off, thr_ptr, npiv, err, tile, wl, wu,
+                                             &s_piv[warp], &s_err[warp], lane);
+                small_trsm_warp<T, FACTO, 8>(s, k, L, U, tile, wl, lane);
+            } else if (n <= 16) {
+                small_diag_warp<T, FACTO, 16>(s, k, L, U, tinv, tinv_off, thr_ptr, npiv, err, tile, wl, wu,
+                                              &s_piv[warp], &s_err[warp], lane);
+                small_trsm_warp<T, FACTO, 16>(s, k, L, U, tile, wl, lane);
+            } else {
+                small_diag_warp<T, FACTO, 32>(s, k, L, U, tinv, tinv_off, thr_ptr, npiv, err, tile, wl, wu,
+                                              &s_piv[warp], &s_err[warp], lane);
+                small_trsm_warp<T, FACTO, 32>(s, k, L, U, tile, wl, lane);
+            }
+            __syncwarp();  // the panel is final before any lane reads it for the updates
         }
-        __syncwarp();  // the panel is final before any lane reads it for the updates
-        for (int q = uoff[t]; q < uoff[t + 1]; q++) {
+        for (int q = it.q0; q < it.q1; q++) {
             const Upd u = upds[q];
-            if (n <= 8) warp_update<T, 8>(s, u, L, U, wl, lane);
-            else if (n <= 16) warp_update<T, 16>(s, u, L, U, wl, lane);
-            else warp_update<T, 32>(s, u, L, U, wl, lane);
-            __threadfence();  // this lane's contributions before the release below
+            if (n <= 8) warp_update<T, 8>(s, u, L, U, wl, lane, it.r0, it.r1);
+            else if (n <= 16) warp_update<T, 16>(s, u, L, U, wl, lane, it.r0, it.r1);
+            else warp_update<T, 32>(s, u, L, U, wl, lane, it.r0, it.r1);
+        }
+        if (it.q1 > it.q0 || it.fact) {
+            __threadfence();  // this lane's writes before the releases below
             __syncwarp();
             if (lane == 0) {
                 __threadfence();
-                atomicSub(cnt + u.f, 1);
+                for (int q = it.q0; q < it.q1; q++) atomicSub(cnt + upds[q].f, 1);
+                if (it.fact) atomicExch(cnt + k, -1);  // factored: its update items may start
             }
         }
     }
@@ -1123,31 +1132,30 @@ static size_t dag_bottom_smem(int facto, size_t esz) {
 }
 
 template <typename T>
-void launch_dag_bottom(int facto, const DevSym &s, int grid, const int *cblks, int ncblk, const int *uoff,
-                       const Upd *upds, int *cnt, int *ticket, int *abort_word, T *L, T *U, T *tinv,
-                       const int64_t *tinv_off, const double *thr, unsigned long long *npiv, int *err,
-                       cudaStream_t st) {
-    if (ncblk <= 0 || grid <= 0) return;
+void launch_dag_bottom(int facto, const DevSym &s, int grid, const DagItem *items, int nitems, const Upd *upds,
+                       int *cnt, int *ticket, int *abort_word, T *L, T *U, T *tinv, const int64_t *tinv_off,
+                       const double *thr, unsigned long long *npiv, int *err, cudaStream_t st) {
+    if (nitems <= 0 || grid <= 0) return;
     const size_t smem = dag_bottom_smem(facto, sizeof(T));
     if (facto == FACTO_POTRF)
         dag_bottom_kernel<T, FACTO_POTRF><<<grid, 32 * DG_WARPS, smem, st>>>(
-            s, cblks, ncblk, uoff, upds, cnt, ticket, abort_word, L, U, tinv, tinv_off, thr, npiv, err);
+            s, items, nitems, upds, cnt, ticket, abort_word, L, U, tinv, tinv_off, thr, npiv, err);
     else if (facto == FACTO_GETRF)
         dag_bottom_kernel<T, FACTO_GETRF><<<grid, 32 * DG_WARPS, smem, st>>>(
-            s, cblks, ncblk, uoff, upds, cnt, ticket, abort_word, L, U, tinv, tinv_off, thr, npiv, err);
+            s, items, nitems, upds, cnt, ticket, abort_word, L, U, tinv, tinv_off, thr, npiv, err);
     else
         dag_bottom_kernel<T, FACTO_SYTRF><<<grid, 32 * DG_WARPS, smem, st>>>(
-            s, cblks, ncblk, uoff, upds, cnt, ticket, abort_word, L, U, tinv, tinv_off, thr, npiv, err);
+            s, items, nitems, upds, cnt, ticket, abort_word, L, U, tinv, tinv_off, thr, npiv, err);
 }
-template void launch_dag_bottom<double>(int, const DevSym &, int, const int *, int, const int *, const Upd *, int *,
-                                        int *, int *, double *, double *, double *, const int64_t *, const double *,
+template void launch_dag_bottom<double>(int, const DevSym &, int, const DagItem *, int, const Upd *, int *, int *,
+                                        int *, double *, double *, double *, const int64_t *, const double *,
                                         unsigned long long *, int *, cudaStream_t);
-template void launch_dag_bottom<float>(int, const DevSym &, int, const int *, int, const int *, const Upd *, int *,
-                                       int *, int *, float *, float *, float *, const int64_t *, const double *,
+template void launch_dag_bottom<float>(int, const DevSym &, int, const DagItem *, int, const Upd *, int *, int *,
+                                       int *, float *, float *, float *, const int64_t *, const double *,
                                        unsigned long long *, int *, cudaStream_t);
 
 // Grid of the tree-bottom launch: the CTAs resident at once (more would only queue
-// behind them), at most one warp per cblk.
+// behind them), at most one warp per item.
 int dag_bottom_grid(int facto, bool f32, int ncblk) {
     if (ncblk <= 0) return 0;
     int dev = 0, sms = 0, per_sm = 0;

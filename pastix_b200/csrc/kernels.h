@@ -54,17 +54,18 @@ void launch_update_f64(const DevSym &s, const Upd *upds, int nupd, int ntiles, d
                        cudaStream_t st);
 void launch_update_f32(const DevSym &s, const Upd *upds, int nupd, int ntiles, float *L, float *U,
                        cudaStream_t st);
-// the bottom levels of the tree in one launch (cblks of at most 32 columns, in level
-// order): one warp per cblk from *ticket, started when cnt[k] (the updates k receives
-// from the launch's cblks) reaches 0; uoff[t] .. uoff[t + 1] are the updates of the
-// t-th cblk, all accumulated with atomics.  cnt, *ticket and *abort_word are reset
-// before every factorization; a wait that runs out sets bit 5 of err.
+// the bottom levels of the tree in one launch (cblks of at most 32 columns): items
+// (factor items, then update items, level by level) taken by warps from *ticket; a
+// factor item starts when cnt[k] (the update items k receives from the launch's cblks)
+// reaches 0 and sets it to -1 when k is factored, which its update items wait for;
+// updates (upds, indexed by the items) accumulate with atomics.  cnt, *ticket and
+// *abort_word are reset before every factorization; a wait that runs out sets bit 5
+// of err.
 template <typename T>
-void launch_dag_bottom(int facto, const DevSym &s, int grid, const int *cblks, int ncblk, const int *uoff,
-                       const Upd *upds, int *cnt, int *ticket, int *abort_word, T *L, T *U, T *tinv,
-                       const int64_t *tinv_off, const double *thr, unsigned long long *npiv, int *err,
-                       cudaStream_t st);
-// its grid: the CTAs resident at once on this device, capped by the cblks (-1 on error)
+void launch_dag_bottom(int facto, const DevSym &s, int grid, const DagItem *items, int nitems, const Upd *upds,
+                       int *cnt, int *ticket, int *abort_word, T *L, T *U, T *tinv, const int64_t *tinv_off,
+                       const double *thr, unsigned long long *npiv, int *err, cudaStream_t st);
+// its grid: the CTAs resident at once on this device, capped by the items (-1 on error)
 int dag_bottom_grid(int facto, bool f32, int ncblk);
 // returns the dynamic shared memory (bytes) the panel TRSM may use, or -1
 int configure_factor_kernels();

@@ -134,11 +134,10 @@ struct b200_solver_s {
     // instead of level by level, when the environment sets B200_TREE_DAG=1 and the
     // tree has at least two such levels (off by default: at 80^3 it ran slower than
     // the level launches it replaces, whose update kernels keep more warps in flight)
-    int dag_levels = 0, dag_ncblk = 0, dag_grid = 0;
-    int *d_dag_cblk = nullptr;   // the launch's cblks in level order (its ticket order)
-    int *d_dag_uoff = nullptr;   // [dag_ncblk + 1] first update of each
+    int dag_levels = 0, dag_nitems = 0, dag_grid = 0;
+    DagItem *d_dag_item = nullptr;  // the launch's items in ticket order
     Upd *d_dag_upd = nullptr;
-    int *d_dag_cnt0 = nullptr;   // [cblknbr] updates each cblk receives from the launch's cblks
+    int *d_dag_cnt0 = nullptr;   // [cblknbr] update items each cblk receives from the launch's cblks
     int *d_dag_cnt = nullptr;    // [cblknbr] working copy, then the ticket and the abort word
     // dataflow solve sweeps: items of the forward and backward launches, the facing
     // lists, and per cblk the counts that complete x (need_f / need_b) and aux
@@ -646,35 +645,78 @@ int build_schedule(b200_solver_t *s) {
         const int ndag = lb >= 2 ? s->levels[lb - 1].c1 : 0;
         const int grid = ndag > 0 ? dag_bottom_grid(s->facto, s->f32, ndag) : 0;
         if (grid > 0) {
-            std::vector<int> dcblk, duoff;
+            // items level by level: the level's factor items, then the update items of
+            // its cblks whose updates are not run by the factor item itself (every
+            // dependency of an item is an earlier item).  Item sizes in multiply-adds:
+            // a cblk's updates up to kInline run in its factor item; the others are
+            // grouped into items of about kChunk, an update above kChunk split by rows
+            constexpr double kInline = 16384.0, kChunk = 16384.0;
+            std::vector<DagItem> items, upd_items;
             std::vector<Upd> dupd;
             std::vector<int> cnt0(N, 0);
-            for (int i = 0; i < ndag; i++) {
-                const int k = lvl_cblk[i];
-                dcblk.push_back(k);
-                duoff.push_back((int)dupd.size());
-                for (int j = s->fblok[k] + 1; j < s->fblok[k + 1]; j++)
-                    for (int side = 0; side < (s->facto == FACTO_GETRF ? 2 : 1); side++) {
-                        Upd u{};
-                        if (!make_upd(k, j, side, UPD_ATOMIC, u)) continue;
-                        if (!map_rows(u)) return ERR_NOTIMPL;
-                        // the same updates the level launches would have run on CUDA cores
-                        s->flops_kind[3] -= upd_flops(u);
-                        s->flops_kind[8] += upd_flops(u);
-                        dupd.push_back(u);
-                        cnt0[u.f]++;
+            auto fma = [&](const Upd &u) { return 0.5 * upd_flops(u); };
+            int last_fact = -1;
+            for (int l = 0; l < lb; l++) {
+                upd_items.clear();
+                for (int i = s->levels[l].c0; i < s->levels[l].c1; i++) {
+                    const int k = lvl_cblk[i];
+                    const int q0 = (int)dupd.size();
+                    double work = 0.0;
+                    for (int j = s->fblok[k] + 1; j < s->fblok[k + 1]; j++)
+                        for (int side = 0; side < (s->facto == FACTO_GETRF ? 2 : 1); side++) {
+                            Upd u{};
+                            if (!make_upd(k, j, side, UPD_ATOMIC, u)) continue;
+                            if (!map_rows(u)) return ERR_NOTIMPL;
+                            // the same updates the level launches would have run on CUDA cores
+                            s->flops_kind[3] -= upd_flops(u);
+                            s->flops_kind[8] += upd_flops(u);
+                            work += fma(u);
+                            dupd.push_back(u);
+                        }
+                    const int q1 = (int)dupd.size();
+                    last_fact = (int)items.size();
+                    if (work <= kInline) {
+                        items.push_back({k, q0, q1, 0, INT32_MAX, 1});
+                        continue;
                     }
+                    items.push_back({k, q0, q0, 0, INT32_MAX, 1});
+                    double acc = 0.0;
+                    int qa = q0;
+                    for (int q = q0; q < q1; q++) {
+                        const double w = fma(dupd[q]);
+                        if (w > kChunk) {
+                            if (qa < q) upd_items.push_back({k, qa, q, 0, INT32_MAX, 0});
+                            const int M = dupd[q].M;
+                            const int pieces = std::min((M + 31) / 32, (int)std::ceil(w / kChunk));
+                            const int R = ((M + pieces - 1) / pieces + 31) / 32 * 32;
+                            for (int r0 = 0; r0 < M; r0 += R) upd_items.push_back({k, q, q + 1, r0, std::min(M, r0 + R), 0});
+                            qa = q + 1;
+                            acc = 0.0;
+                            continue;
+                        }
+                        if (acc + w > kChunk && qa < q) {
+                            upd_items.push_back({k, qa, q, 0, INT32_MAX, 0});
+                            qa = q;
+                            acc = 0.0;
+                        }
+                        acc += w;
+                    }
+                    if (qa < q1) upd_items.push_back({k, qa, q1, 0, INT32_MAX, 0});
+                }
+                items.insert(items.end(), upd_items.begin(), upd_items.end());
             }
-            duoff.push_back((int)dupd.size());
-            if (s->test_withhold & 4) cnt0[dcblk.back()]++;  // an update that never comes
-            RET(s->dupload(&s->d_dag_cblk, dcblk));
-            RET(s->dupload(&s->d_dag_uoff, duoff));
+            // every item decrements the counter of each update's facing cblk once
+            for (const DagItem &it : items)
+                for (int q = it.q0; q < it.q1; q++) cnt0[dupd[q].f]++;
+            if (s->test_withhold & 4) cnt0[items[last_fact].k]++;  // an update that never comes
+            RET(s->dupload(&s->d_dag_item, items));
             RET(s->dupload(&s->d_dag_upd, dupd));
             RET(s->dupload(&s->d_dag_cnt0, cnt0));
             RET(s->dmalloc(&s->d_dag_cnt, (size_t)N + 2));
             s->dag_levels = lb;
-            s->dag_ncblk = ndag;
-            s->dag_grid = grid;
+            s->dag_nitems = (int)items.size();
+            s->dag_grid = dag_bottom_grid(s->facto, s->f32, s->dag_nitems);
+            if (s->dag_grid <= 0) return ERR_INTERNAL;
         }
     }
     RET(s->dupload(&s->d_lvl_cblk, lvl_cblk));
@@ -987,7 +1029,7 @@ int enqueue_numfact(b200_solver_t *s, cudaStream_t st, Trace *tr = nullptr) {
         const int N = s->cblknbr;
         CU(cudaMemcpyAsync(s->d_dag_cnt, s->d_dag_cnt0, (size_t)N * sizeof(int), cudaMemcpyDeviceToDevice, st));
         CU(cudaMemsetAsync(s->d_dag_cnt + N, 0, 2 * sizeof(int), st));
-        launch_dag_bottom<T>(s->facto, s->ds, s->dag_grid, s->d_dag_cblk, s->dag_ncblk, s->d_dag_uoff, s->d_dag_upd,
+        launch_dag_bottom<T>(s->facto, s->ds, s->dag_grid, s->d_dag_item, s->dag_nitems, s->d_dag_upd,
                              s->d_dag_cnt, s->d_dag_cnt + N, s->d_dag_cnt + N + 1, L, U, (T *)s->dTinv, s->d_toff,
                              s->d_thr, s->d_npiv, s->d_err, st);
         launches++;
