@@ -844,11 +844,13 @@ __global__ void __launch_bounds__(32 * DS_WARPS) diag_small_kernel(DevSym s, con
 // far below a 64 x 64 tile), one warp each: lane = row of the M-range (32 rows per
 // pass), C[d(i)][colbase + c] -= sum_k A[i][k] (D[k]) B[c][k] for c < N (c <= i when
 // symmetric).  Same operation as the tile kernels (core_zgemmsp_2d2d,
-// kernels/core_zgemmsp.c:396-465).
+// kernels/core_zgemmsp.c:396-465).  Each warp waits mostly on its loads, so the
+// launch bounds ask for 4 (FP32) / 3 (FP64) CTAs per SM: 64 / 80 registers, a few
+// bytes of spill, a third to a half more warps in flight.
 constexpr int US_WARPS = 8;
 
 template <typename T>
-__global__ void __launch_bounds__(32 * US_WARPS) update_small_kernel(DevSym s, const Upd *__restrict__ upds, int nupd,
+__global__ void __launch_bounds__(32 * US_WARPS, sizeof(T) == 4 ? 4 : 3) update_small_kernel(DevSym s, const Upd *__restrict__ upds, int nupd,
                                                                      T *L, T *U) {
     const int lane = threadIdx.x & 31;
     const int ui = blockIdx.x * US_WARPS + (threadIdx.x >> 5);
